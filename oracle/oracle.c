@@ -1,0 +1,510 @@
+/*
+ * CPU restatement of the AUSAXS Debye hot path -- TEST INFRASTRUCTURE ONLY.
+ *
+ * This file is the checker for the CUDA path: only tests/, the smoke check
+ * and bench.py's CPU-baseline leg load it.  It restates, in plain C and in
+ * the reference's operation order, the functions listed below; each cites the
+ * reference file:line it follows.  Its own correctness is pinned against the
+ * reference compiled from source (oracle/_ref, see oracle/Makefile) and
+ * against the reference's known-answer tests (tests/golden/).
+ *
+ * Build: gcc -O2 -ffp-contract=off -fPIC -shared (no fast-math: the pair
+ * distance must be evaluated with the reference's SIMD rounding sequence).
+ *
+ * Conventions
+ *   point     : 4 x 32-bit {x, y, z, w|ff} exactly as the reference's
+ *               CompactCoordinatesXYZW / XYZFF records
+ *               (include/core/hist/detail/data/CompactCoordinatesXYZW.h:131-134).
+ *   ff types  : the reference's form_factor_t enum values (0 = excluded volume,
+ *               1 = water/OH, ...), max 15 (include/core/form_factor/FormFactorType.h:14-37).
+ *   histograms: row-major FP64 [rows][nbins].
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define NFF 15 /* settings::form_factor::max_ff_types (include/core/settings/FormFactorSettings.h:12) */
+
+typedef struct {
+    float x, y, z;
+    union {
+        float w;
+        int32_t ff;
+    } v;
+} opoint;
+
+/* ---------------------------------------------------------------------------
+ * Pair evaluation.
+ * SIMD evaluators (CompactCoordinatesXYZW.h:382-423, :491-535, :602-655):
+ *   d2 = (dx*dx + dy*dy) + dz*dz, d = sqrt(d2), bin = cvt_rn(d * inv_w)
+ * with each operation rounded separately and ties to even.
+ * Scalar tail evaluator (CompactCoordinatesXYZW.h:303-307): same distance,
+ * bin = std::round(inv_w * d) (ties away from zero).
+ * ------------------------------------------------------------------------- */
+static inline float pair_distance(const opoint* a, const opoint* b) {
+    float dx = a->x - b->x, dy = a->y - b->y, dz = a->z - b->z;
+    float sx = dx * dx, sy = dy * dy, sz = dz * dz;
+    return sqrtf((sx + sy) + sz);
+}
+
+static inline int32_t pair_bin(float d, float inv_w, int tail) {
+    float x = d * inv_w;
+    return tail ? (int32_t)roundf(x) : (int32_t)rintf(x);
+}
+
+/* The j-loops of every reference driver are unrolled 16/8/4 and finish with
+ * single evaluations (SimpleCalculator.h:117-141, HistogramManagerMTFFAvg.cpp:216-232):
+ * the last (len mod 4) partners of a row go through the scalar evaluator. */
+static inline int32_t tail_start(int32_t j0, int32_t n) { return n - ((n - j0) & 3); }
+
+/* Row selection for one pair, by the histogram shape the reference increments. */
+enum {
+    ROW_SINGLE = 0, /* 1D histogram (ww, xx, wx, Simple)                               */
+    ROW_FFPAIR = 1, /* [ff_i][ff_j]  (increment_linear_index, CompactCoordinatesXYZFF.h:187-188) */
+    ROW_FFOUTER = 2 /* [ff_i]        (aw / ax by the outer atom's type)                */
+};
+
+typedef struct {
+    double* counts; /* [rows][nbins]: += factor per pair                                 */
+    double* dsum;   /* [nbins]: += factor * d (the bin_center sums of the rows that feed */
+                    /*          the weighted d-axis)                                     */
+    double* dcnt;   /* [nbins]: += factor (their counts)                                 */
+    double* wsum;   /* [nbins] or NULL: += factor * (w_i * w_j) (XYZW weights)           */
+    int64_t overflow;
+} job_out;
+
+/*
+ * One pair-binning pass.  Outer set A (index i), inner set B (index j).
+ * self != 0: A == B and only j > i is visited (SimpleCalculator.h:117-141).
+ * FFAvg also increments the excluded-volume rows of every atom-atom pair
+ * (HistogramManagerMTFFAvg.cpp:27-35): exv_rows = 2 adds [ff_i][exv] and
+ * [exv][exv]; for atom-water pairs exv_rows = 1 adds [exv] (:111-117).
+ */
+static void pair_job(const opoint* A, int32_t na, const opoint* B, int32_t nb, int self, int row_mode, int exv_rows,
+                     double factor, float inv_w, int32_t nbins, job_out* o) {
+    for (int32_t i = 0; i < na; ++i) {
+        int32_t j0 = self ? i + 1 : 0;
+        int32_t ts = tail_start(j0, nb);
+        for (int32_t j = j0; j < nb; ++j) {
+            float d = pair_distance(&A[i], &B[j]);
+            int32_t bin = pair_bin(d, inv_w, j >= ts);
+            if (!(bin >= 0 && bin < nbins)) {
+                o->overflow++;
+                continue;
+            }
+            int32_t row = 0;
+            if (row_mode == ROW_FFPAIR) row = A[i].v.ff * NFF + B[j].v.ff;
+            else if (row_mode == ROW_FFOUTER) row = A[i].v.ff;
+            o->counts[(size_t)row * nbins + bin] += factor;
+            if (exv_rows == 2) {
+                o->counts[(size_t)(A[i].v.ff * NFF + 0) * nbins + bin] += factor;
+                o->counts[(size_t)0 * nbins + bin] += factor;
+            } else if (exv_rows == 1) {
+                o->counts[(size_t)0 * nbins + bin] += factor;
+            }
+            /* WeightedEntry::add/increment: bin_center += N*distance with N*distance in
+             * float (include/core/hist/distribution/detail/WeightedEntry.h:63-81). */
+            if (o->dsum) {
+                o->dsum[bin] += (double)((float)factor * d);
+                o->dcnt[bin] += factor;
+            }
+            if (o->wsum) o->wsum[bin] += factor * (double)(A[i].v.w * B[j].v.w);
+        }
+    }
+}
+
+/* ---------------------------------------------------------------------------
+ * Manager post-processing helpers.
+ * ------------------------------------------------------------------------- */
+
+/* max_bin: last bin >= 10 whose total is non-zero, +1; minimum 10
+ * (HistogramManagerMT.cpp:47-58, HistogramManagerMTFFAvg.cpp:339-346). */
+static int32_t find_max_bin(const double* tot, int32_t nbins) {
+    for (int32_t i = nbins - 1; i >= 10; --i)
+        if (tot[i] != 0) return i + 1;
+    return 10;
+}
+
+/* WeightedDistribution1D::get_weighted_axis (source/core/hist/distribution/WeightedDistribution1D.cpp:51-58):
+ * mean distance of each bin, or the bin's lower value i*width when empty. */
+static void weighted_axis(const double* dsum, const double* dcnt, int32_t n, double bin_width, double* out) {
+    double w = ((double)n * bin_width) / n; /* Axis(0, n*bin_width, n).width() */
+    for (int32_t i = 0; i < n; ++i) {
+        double dv = 0 + i * w;
+        double bc = dsum[i];
+        uint32_t c = (uint32_t)dcnt[i];
+        out[i] = ((double)(bc == 0) * dv + bc) / (double)((c == 0) + c);
+    }
+}
+
+/*
+ * HistogramManagerMT<weighted_bins, vbw>::calculate_all (source/core/hist/histogram_manager/HistogramManagerMT.cpp:23-75)
+ * over SimpleCalculator (include/core/hist/distance_calculator/SimpleCalculator.h:94-215):
+ * aa self (factor 2), ww self (factor 2), aw cross with waters outer / atoms inner (factor 2),
+ * diagonal sum(w*w) into bin 0, truncation, and the weighted axis of p_tot.
+ *
+ * Outputs (first *max_bin entries used, capacity nbins): aa, aw, ww, tot = weighted counts;
+ * d_axis = weighted bin centres (or i*width when !weighted), d_axis[0] = 0.
+ * Returns the number of pairs whose bin fell outside [0, nbins).
+ */
+int64_t oracle_hist_simple(const opoint* atoms, int32_t na, const opoint* waters, int32_t nw, double bin_width,
+                           int32_t nbins, int weighted, int32_t* max_bin, double* aa, double* aw, double* ww,
+                           double* tot, double* d_axis) {
+    float inv_w = (float)(1.0 / bin_width);
+    size_t nbytes = sizeof(double) * (size_t)nbins;
+    double *ca = calloc(nbins, 8), *cw = calloc(nbins, 8), *cx = calloc(nbins, 8);
+    double *da = calloc(nbins, 8), *dw = calloc(nbins, 8), *dx = calloc(nbins, 8);
+    double *na_ = calloc(nbins, 8), *nw_ = calloc(nbins, 8), *nx_ = calloc(nbins, 8);
+    double *wa = calloc(nbins, 8), *ww_ = calloc(nbins, 8), *wx = calloc(nbins, 8);
+    job_out oa = {ca, da, na_, wa, 0}, ow = {cw, dw, nw_, ww_, 0}, ox = {cx, dx, nx_, wx, 0};
+    pair_job(atoms, na, atoms, na, 1, ROW_SINGLE, 0, 2.0, inv_w, nbins, &oa);
+    pair_job(waters, nw, waters, nw, 1, ROW_SINGLE, 0, 2.0, inv_w, nbins, &ow);
+    pair_job(waters, nw, atoms, na, 0, ROW_SINGLE, 0, 2.0, inv_w, nbins, &ox);
+    /* self-correlation: scaling * sum(float(w*w)) (SimpleCalculator.h:146-160) */
+    double twa = 0, tww = 0;
+    for (int32_t i = 0; i < na; ++i) twa += atoms[i].v.w * atoms[i].v.w;
+    for (int32_t i = 0; i < nw; ++i) tww += waters[i].v.w * waters[i].v.w;
+    wa[0] += twa;
+    ww_[0] += tww;
+    na_[0] += (double)(uint32_t)twa;
+    nw_[0] += (double)(uint32_t)tww;
+    double* ptot = calloc(nbins, 8);
+    double* pdsum = calloc(nbins, 8);
+    double* pdcnt = calloc(nbins, 8);
+    for (int32_t b = 0; b < nbins; ++b) {
+        ptot[b] = wa[b] + ww_[b] + wx[b];
+        pdsum[b] = da[b] + dw[b] + dx[b];
+        pdcnt[b] = (double)((uint32_t)na_[b] + (uint32_t)nw_[b] + (uint32_t)nx_[b]);
+    }
+    int32_t mb = find_max_bin(ptot, nbins);
+    *max_bin = mb;
+    memcpy(aa, wa, sizeof(double) * mb);
+    memcpy(aw, wx, sizeof(double) * mb);
+    memcpy(ww, ww_, sizeof(double) * mb);
+    memcpy(tot, ptot, sizeof(double) * mb);
+    if (weighted) {
+        weighted_axis(pdsum, pdcnt, mb, bin_width, d_axis);
+    } else {
+        double w = ((double)mb * bin_width) / mb;
+        for (int32_t i = 0; i < mb; ++i) d_axis[i] = i * w;
+    }
+    d_axis[0] = 0; /* DistanceHistogram::initialize (DistanceHistogram.cpp:44-47) */
+    int64_t of = oa.overflow + ow.overflow + ox.overflow;
+    (void)nbytes;
+    free(ca); free(cw); free(cx); free(da); free(dw); free(dx);
+    free(na_); free(nw_); free(nx_); free(wa); free(ww_); free(wx);
+    free(ptot); free(pdsum); free(pdcnt);
+    return of;
+}
+
+/*
+ * Form-factor managers.
+ *   kind 0: HistogramManagerMTFFAvg     (source/core/hist/histogram_manager/HistogramManagerMTFFAvg.cpp:194-372)
+ *   kind 1: HistogramManagerMTFFExplicit (HistogramManagerMTFFExplicit.cpp:216-437)
+ *   kind 2: HistogramManagerMTFFGrid     (HistogramManagerMTFFGrid.cpp:43-234): FFAvg plus the
+ *           excluded-volume dummies exv[] (ax, wx, xx) replacing the exv rows.
+ * Atoms must carry ff >= 1.  Outputs (capacity nbins, first *max_bin used per row):
+ *   aa [15][15][mb], aw [15][mb], ww [mb], tot [mb] (p_tot counts), d_axis [mb];
+ *   for kind 2 also d_axis_ax, d_axis_xx [mb].
+ * z_exv: the average excluded-volume charge V_grid * rho_w / N_atoms (kind 0 only).
+ */
+int64_t oracle_hist_ff(int kind, const opoint* atoms, int32_t na, const opoint* waters, int32_t nw, const opoint* exv,
+                       int32_t nx, double bin_width, int32_t nbins, double z_exv, int32_t* max_bin, double* aa,
+                       double* aw, double* ww, double* tot, double* d_axis, double* d_axis_ax, double* d_axis_xx) {
+    float inv_w = (float)(1.0 / bin_width);
+    size_t nb = (size_t)nbins;
+    double* caa = calloc(NFF * NFF * nb, 8);
+    double* caw = calloc(NFF * nb, 8);
+    double* cww = calloc(nb, 8);
+    double* dsum = calloc(nb, 8);
+    double* dcnt = calloc(nb, 8);
+    /* FFExplicit has no exv rows (HistogramManagerMTFFExplicit.cpp:27-35 increments only [ff_i][ff_j]) */
+    int exv_aa = kind == 1 ? 0 : 2, exv_aw = kind == 1 ? 0 : 1;
+    job_out o1 = {caa, dsum, dcnt, NULL, 0};
+    pair_job(atoms, na, atoms, na, 1, ROW_FFPAIR, exv_aa, 2.0, inv_w, nbins, &o1);
+    job_out o2 = {caw, dsum, dcnt, NULL, 0};
+    pair_job(atoms, na, waters, nw, 0, ROW_FFOUTER, exv_aw, 1.0, inv_w, nbins, &o2);
+    job_out o3 = {cww, dsum, dcnt, NULL, 0};
+    pair_job(waters, nw, waters, nw, 1, ROW_SINGLE, 0, 2.0, inv_w, nbins, &o3);
+    int64_t of = o1.overflow + o2.overflow + o3.overflow;
+
+    /* self-correlations (HistogramManagerMTFFAvg.cpp:310-323) */
+    for (int32_t i = 0; i < na; ++i) {
+        int32_t f = atoms[i].v.ff;
+        caa[(size_t)(f * NFF + f) * nb + 0] += 1;
+        dcnt[0] += 1;
+    }
+    if (kind != 1) caa[0] += na; /* [exv][exv][0] += N_a, not part of p_tot */
+    cww[0] += nw;
+    dcnt[0] += nw;
+
+    /* p_tot = sum over ff >= 1 of aa and aw, plus ww (HistogramManagerMTFFAvg.cpp:325-337) */
+    double* ptot = calloc(nb, 8);
+    for (int f1 = 1; f1 < NFF; ++f1)
+        for (int f2 = 1; f2 < NFF; ++f2)
+            for (size_t b = 0; b < nb; ++b) ptot[b] += caa[(size_t)(f1 * NFF + f2) * nb + b];
+    for (int f1 = 1; f1 < NFF; ++f1)
+        for (size_t b = 0; b < nb; ++b) ptot[b] += caw[(size_t)f1 * nb + b];
+    for (size_t b = 0; b < nb; ++b) ptot[b] += cww[b];
+    int32_t mb = find_max_bin(ptot, nbins);
+
+    if (kind == 0) {
+        /* Z_exv scaling of the exv rows (HistogramManagerMTFFAvg.cpp:355-364) */
+        for (int f1 = 1; f1 < NFF; ++f1)
+            for (int32_t b = 0; b < mb; ++b) caa[(size_t)(f1 * NFF + 0) * nb + b] *= z_exv;
+        for (int32_t b = 0; b < mb; ++b) caa[b] *= z_exv * z_exv;
+        for (int32_t b = 0; b < mb; ++b) caw[b] *= z_exv;
+    }
+
+    if (kind == 2) {
+        /* grid excluded volume (HistogramManagerMTFFGrid.cpp:68-233) */
+        double* cax = calloc(NFF * nb, 8);
+        double* cwx = calloc(nb, 8);
+        double* cxx = calloc(nb, 8);
+        double* dax = calloc(nb, 8);
+        double* nax = calloc(nb, 8);
+        double* dxx = calloc(nb, 8);
+        double* nxx = calloc(nb, 8);
+        job_out ox = {cxx, dxx, nxx, NULL, 0};
+        pair_job(exv, nx, exv, nx, 1, ROW_SINGLE, 0, 2.0, inv_w, nbins, &ox);
+        job_out oax = {cax, dax, nax, NULL, 0};
+        pair_job(atoms, na, exv, nx, 0, ROW_FFOUTER, 0, 1.0, inv_w, nbins, &oax);
+        job_out owx = {cwx, dax, nax, NULL, 0};
+        pair_job(waters, nw, exv, nx, 0, ROW_SINGLE, 0, 1.0, inv_w, nbins, &owx);
+        of += ox.overflow + oax.overflow + owx.overflow;
+        cxx[0] += nx;
+        nxx[0] += nx;
+        int32_t mbx = 10;
+        for (int32_t i = nbins - 1; i >= 10; --i)
+            if (cxx[i] != 0 || cwx[i] != 0) {
+                mbx = i + 1;
+                break;
+            }
+        if (mbx > mb) mb = mbx;
+        for (int f1 = 0; f1 < NFF; ++f1)
+            for (int32_t b = 0; b < mb; ++b) caa[(size_t)(f1 * NFF + 0) * nb + b] = cax[(size_t)f1 * nb + b];
+        for (int32_t b = 0; b < mb; ++b) caw[b] = cwx[b];
+        for (int32_t b = 0; b < mb; ++b) caa[b] = cxx[b];
+        /* ax / xx axes keep their weighted value in bin 0 (CompositeDistanceHistogramFFGrid.cpp:129-134) */
+        weighted_axis(dax, nax, mb, bin_width, d_axis_ax);
+        weighted_axis(dxx, nxx, mb, bin_width, d_axis_xx);
+        free(cax); free(cwx); free(cxx); free(dax); free(nax); free(dxx); free(nxx);
+    }
+
+    *max_bin = mb;
+    for (int r = 0; r < NFF * NFF; ++r) memcpy(aa + (size_t)r * mb, caa + (size_t)r * nb, sizeof(double) * mb);
+    for (int r = 0; r < NFF; ++r) memcpy(aw + (size_t)r * mb, caw + (size_t)r * nb, sizeof(double) * mb);
+    memcpy(ww, cww, sizeof(double) * mb);
+    memcpy(tot, ptot, sizeof(double) * mb);
+    weighted_axis(dsum, dcnt, mb, bin_width, d_axis);
+    d_axis[0] = 0;
+    free(caa); free(caw); free(cww); free(dsum); free(dcnt); free(ptot);
+    return of;
+}
+
+/* ---------------------------------------------------------------------------
+ * Debye transform (FP64), generalised to arbitrary q.
+ * ------------------------------------------------------------------------- */
+
+/* VectorDebyeTable::initialize (source/core/table/VectorDebyeTable.cpp:24-40) */
+static double sinc_ref(double qd) {
+    if (qd < 1e-3) {
+        double qd2 = qd * qd;
+        return 1 - qd2 * (1.0 / 6) + qd2 * qd2 * (1.0 / 120);
+    }
+    return sin(qd) / qd;
+}
+
+/* sinqd[r][q] = sum_b p[r][b] * sinc(q * d[b])  (std::inner_product order,
+ * CompositeDistanceHistogramFFAvgBase.cpp:427-467) */
+void oracle_sinqd(const double* p, int32_t rows, int32_t nbins, const double* d_axis, const double* q, int32_t nq,
+                  double* out) {
+    double* s = malloc(sizeof(double) * (size_t)nbins);
+    for (int32_t k = 0; k < nq; ++k) {
+        for (int32_t b = 0; b < nbins; ++b) s[b] = sinc_ref(q[k] * d_axis[b]);
+        for (int32_t r = 0; r < rows; ++r) {
+            double acc = 0;
+            const double* pr = p + (size_t)r * nbins;
+            for (int32_t b = 0; b < nbins; ++b) acc = acc + pr[b] * s[b];
+            out[(size_t)r * nq + k] = acc;
+        }
+    }
+    free(s);
+}
+
+/* Five-Gaussian atomic form factors: f(q) = sum_i a_i exp(-b_i q^2) + c, with
+ * b given in s = q/(4 pi) units and converted by 1/(16 pi^2)
+ * (include/core/form_factor/FormFactorTable.h:8-21, FormFactor.h:33-39).
+ * Coefficients: Waasmaier & Kirfel (1995) for C, N, O, S and argon (OTHER);
+ * International Tables for H; Grudinin, Garkavenko & Kazennov (2017) for the
+ * united-atom groups (FormFactorTable.h:24-186).  Index = form_factor_t. */
+typedef struct {
+    double a[5], b[5], c;
+} ff5;
+
+static const ff5 FF_TABLE[NFF] = {
+    /* 0 EXCLUDED_VOLUME: a={1}, b={r^2/2} with r = 1.62 (FormFactorTable.h, excluded_volume) */
+    {{1, 0, 0, 0, 0}, {-1, 0, 0, 0, 0}, 0},
+    /* 1 WATER = OH (OH_alc) */
+    {{0.456221, 3.219608, 0.812773, 2.666928, 1.380927}, {21.503498, 13.397134, 34.547137, 5.826620, 0.412902}, 0.463202},
+    /* 2 H */
+    {{0.489918, 0.262003, 0.196767, 0.049879, 0}, {20.6593, 7.74039, 49.5519, 2.20159, 0}, 0.001305},
+    /* 3 C */
+    {{2.657506, 1.078079, 1.490909, -4.241070, 0.713791}, {14.780758, 0.776775, 42.086843, -0.000294, 0.239535}, 4.297983},
+    /* 4 CH (CH_sp3) */
+    {{2.909530, 0.485267, 1.516151, 0.206905, 1.541626}, {13.933084, 23.221524, 41.990403, 4.974183, 0.679266}, 0.337670},
+    /* 5 CH2 (CH2_sp3) */
+    {{3.275723, 0.870037, 1.534606, 0.395078, 1.544562}, {13.408502, 23.785175, 41.922444, 5.019072, 0.724439}, 0.377096},
+    /* 6 CH3 (CH3_sp3) */
+    {{3.681341, 1.228691, 1.549320, 0.574033, 1.554377}, {13.026207, 24.131974, 41.869426, 4.984373, 0.765769}, 0.409294},
+    /* 7 N */
+    {{11.893780, 3.277479, 1.858092, 0.858927, 0.912985}, {0.000158, 10.232723, 30.344690, 0.656065, 0.217287}, -11.804902},
+    /* 8 NH */
+    {{1.650531, 0.429639, 2.144736, 1.851894, 1.408921}, {10.603730, 6.987283, 29.939901, 10.573859, 0.611678}, 0.510589},
+    /* 9 NH2 */
+    {{1.904157, 1.942536, 2.435585, 0.730512, 1.379728}, {10.803702, 10.792421, 29.610479, 6.847755, 0.709687}, 0.603738},
+    /* 10 NH3 (NH3_plus) */
+    {{1.882162, 1.933200, 2.465843, 0.927311, 1.190889}, {10.975157, 10.956008, 29.208572, 6.663555, 0.843650}, 0.597322},
+    /* 11 O */
+    {{2.960427, 2.508818, 0.637853, 0.722838, 1.142756}, {14.182259, 5.936858, 0.112726, 34.958481, 0.390240}, 0.027014},
+    /* 12 S */
+    {{6.362157, 5.154568, 1.473732, 1.635073, 1.209372}, {1.514347, 22.092528, 0.061373, 55.445176, 0.646925}, 0.154722},
+    /* 13 SH */
+    {{0.570042, 6.337416, 1.641643, 5.398549, 1.527982}, {11.447986, 1.197657, 55.401032, 22.420955, 2.356552}, 1.523944},
+    /* 14 OTHER (argon) */
+    {{7.188004, 6.638454, 0.454180, 1.929593, 1.523654}, {0.956221, 15.339877, 15.339862, 39.043824, 0.062409}, 0.265954},
+};
+
+static const double PI_ = 3.14159265358979323846;
+
+/* raw FormFactor::evaluate(q) with q0 = 1 (FormFactor.h:33-39) */
+double oracle_ff_raw(int type, double q) {
+    const ff5* f = &FF_TABLE[type];
+    double s_to_q = 1. / (4 * 4 * PI_ * PI_);
+    double sum = 0;
+    for (int i = 0; i < 5; ++i) {
+        double b = (type == 0) ? (i == 0 ? 1.62 * 1.62 / 2 : 0) : f->b[i] * s_to_q;
+        sum += f->a[i] * exp(-b * q * q);
+    }
+    return sum + f->c;
+}
+
+/* ExvFormFactor(V).evaluate(q) = V rho_w exp(-V^(2/3)/(4 pi) q^2)
+ * (include/core/form_factor/ExvFormFactor.h:20-33), rho_w = 0.334 e/A^3 (Constants.h:114) */
+double oracle_ff_exv_volume(double volume, double q) {
+    double e = pow(volume, 2. / 3) / (4 * PI_);
+    return volume * 0.334 * exp(-e * q * q);
+}
+
+/*
+ * FFAvg / FFGrid intensity (CompositeDistanceHistogramFFAvgBase.cpp:57-76, 333-374, 470-558;
+ * CompositeDistanceHistogramFFGrid.cpp:37-119).
+ *   kind 0 (FFAvg): products of raw form factors, F(ff, exv) uses the raw excluded_volume entry.
+ *   kind 2 (FFGrid): F(ff, exv) = f_ff * ExvFormFactor(width^3), F(exv, exv) likewise, and ax/wx
+ *                    use d_axis_ax, xx uses d_axis_xx.
+ * Inputs: the histograms as returned by oracle_hist_ff (mb bins).  Outputs profiles[6][nq]
+ * = {aa, ax, aw, xx, wx, ww} and Iq = aa - ax + aw + xx - wx + ww.
+ */
+void oracle_debye_ff(int kind, const double* aa, const double* aw, const double* ww, int32_t mb, const double* d_axis,
+                     const double* d_axis_ax, const double* d_axis_xx, const double* q, int32_t nq, double cw,
+                     double cx, double crho, double dw_atomic, double dw_exv, double grid_width, double* profiles,
+                     double* Iq) {
+    double* s_aa = malloc(sizeof(double) * (size_t)NFF * NFF * nq);
+    double* s_aw = malloc(sizeof(double) * (size_t)NFF * nq);
+    double* s_ww = malloc(sizeof(double) * (size_t)nq);
+    const double* dax = kind == 2 ? d_axis_ax : d_axis;
+    const double* dxx = kind == 2 ? d_axis_xx : d_axis;
+    /* aa rows: ff1 >= 1 and ff2 >= 1 with the aa axis; [ff][exv] with the ax axis; [exv][exv] with xx */
+    for (int f1 = 0; f1 < NFF; ++f1) {
+        for (int f2 = 0; f2 < NFF; ++f2) {
+            const double* ax = (f1 == 0 && f2 == 0) ? dxx : (f2 == 0 ? dax : d_axis);
+            oracle_sinqd(aa + (size_t)(f1 * NFF + f2) * mb, 1, mb, ax, q, nq, s_aa + (size_t)(f1 * NFF + f2) * nq);
+        }
+        oracle_sinqd(aw + (size_t)f1 * mb, 1, mb, f1 == 0 ? dax : d_axis, q, nq, s_aw + (size_t)f1 * nq);
+    }
+    oracle_sinqd(ww, 1, mb, d_axis, q, nq, s_ww);
+
+    double Vg = grid_width * grid_width * grid_width;
+    for (int32_t k = 0; k < nq; ++k) {
+        double qq = q[k];
+        double fa[NFF];
+        for (int t = 0; t < NFF; ++t) fa[t] = oracle_ff_raw(t, qq);
+        double fx = kind == 2 ? oracle_ff_exv_volume(Vg, qq) : fa[0];
+        double paa = 0, pax = 0, paw = 0, pxx = 0, pwx = 0, pww = 0;
+        for (int f1 = 1; f1 < NFF; ++f1)
+            for (int f2 = 1; f2 < NFF; ++f2) paa += s_aa[(size_t)(f1 * NFF + f2) * nq + k] * (fa[f1] * fa[f2]);
+        double cxq = cx; /* exv_factor(q) = cx for FFAvg / FFGrid */
+        for (int f1 = 1; f1 < NFF; ++f1) pax += 2 * crho * cxq * s_aa[(size_t)(f1 * NFF + 0) * nq + k] * (fa[f1] * fx);
+        pxx = pow(cxq * crho, 2) * s_aa[k] * (fx * fx);
+        for (int f1 = 1; f1 < NFF; ++f1) paw += 2 * cw * s_aw[(size_t)f1 * nq + k] * (fa[f1] * fa[1]);
+        pww = cw * cw * s_ww[k] * (fa[1] * fa[1]);
+        pwx = 2 * crho * cxq * cw * s_aw[k] * (fx * fa[1]);
+        if (dw_atomic != 0 || dw_exv != 0) {
+            double ba = exp(-qq * qq * dw_atomic * dw_atomic * 0.5);
+            double bx = exp(-qq * qq * dw_exv * dw_exv * 0.5);
+            paa *= ba * ba;
+            pxx *= bx * bx;
+            pax *= ba * bx;
+            paw *= ba;
+            pwx *= bx;
+        }
+        profiles[0 * nq + k] = paa;
+        profiles[1 * nq + k] = pax;
+        profiles[2 * nq + k] = paw;
+        profiles[3 * nq + k] = pxx;
+        profiles[4 * nq + k] = pwx;
+        profiles[5 * nq + k] = pww;
+        double I = 0;
+        I += paa;
+        I -= pax;
+        I += paw;
+        I += pxx;
+        I -= pwx;
+        I += pww;
+        Iq[k] = I;
+    }
+    free(s_aa);
+    free(s_aw);
+    free(s_ww);
+}
+
+/* Simple composite intensity: exp(-q^2) * sum_b (aa + k aw + k^2 ww) sinc(q d)
+ * (DistanceHistogram.cpp:54-87, CompositeDistanceHistogram.cpp:55-57). */
+void oracle_debye_simple(const double* aa, const double* aw, const double* ww, int32_t mb, const double* d_axis,
+                         const double* q, int32_t nq, double cw, double* Iq) {
+    double* p = malloc(sizeof(double) * (size_t)mb);
+    for (int32_t b = 0; b < mb; ++b) p[b] = aa[b] + cw * aw[b] + cw * cw * ww[b];
+    oracle_sinqd(p, 1, mb, d_axis, q, nq, Iq);
+    for (int32_t k = 0; k < nq; ++k) Iq[k] *= exp(-q[k] * q[k]);
+    free(p);
+}
+
+/* fitter::detail::LinearLeastSquares::fit_params_only + chi2
+ * (source/core/fitter/detail/LinearLeastSquares.cpp:26-44, :71-78):
+ * fit model ~ a * data + b with weights 1/err^2.  out = {a, b, a_err, b_err, chi2}. */
+void oracle_linear_lsq(const double* data, const double* model, const double* err, int32_t n, double* out) {
+    double S = 0, Sx = 0, Sy = 0, Sxx = 0, Sxy = 0;
+    for (int32_t i = 0; i < n; ++i) {
+        double is = 1. / err[i];
+        double w = is * is;
+        S += w;
+        Sx += data[i] * w;
+        Sy += model[i] * w;
+        Sxx += pow(data[i], 2) * w;
+        Sxy += data[i] * model[i] * w;
+    }
+    double delta = S * Sxx - Sx * Sx;
+    double a = (S * Sxy - Sx * Sy) / delta;
+    double b = (Sxx * Sy - Sx * Sxy) / delta;
+    double chi2 = 0;
+    for (int32_t i = 0; i < n; ++i) {
+        double r = (model[i] - (a * data[i] + b)) / err[i];
+        chi2 += r * r;
+    }
+    out[0] = a;
+    out[1] = b;
+    out[2] = S / delta;
+    out[3] = Sxx / delta;
+    out[4] = chi2;
+}

@@ -1,0 +1,352 @@
+"""ctypes front for the oracle -- TEST INFRASTRUCTURE ONLY.
+
+Two libraries sit behind this module:
+
+* ``liboracle.so``   -- the plain-C restatement in ``oracle/oracle.c``;
+* ``_ref/libausaxs_ref.so`` -- the reference itself, compiled from its own
+  sources by ``oracle/Makefile`` (only present where the reference sources
+  were available at build time, or where the built file was carried along).
+
+Only ``tests/``, ``__graft_entry__.smoke`` and ``bench.py``'s CPU-baseline leg
+use this module, as the checker.  The product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+NFF = 15
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+
+_lib = None
+_ref = None
+
+
+def build_oracle() -> str:
+    """Compile the C restatement (gcc, no fast-math, no FMA contraction)."""
+    out = os.path.join(HERE, "liboracle.so")
+    src = os.path.join(HERE, "oracle.c")
+    if not os.path.exists(out) or os.path.getmtime(out) < os.path.getmtime(src):
+        subprocess.check_call(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", out, src, "-lm"])
+    return out
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build_oracle()
+        L = C.CDLL(path)
+        L.oracle_hist_simple.restype = C.c_int64
+        L.oracle_hist_simple.argtypes = [_f32p, C.c_int32, _f32p, C.c_int32, C.c_double, C.c_int32, C.c_int,
+                                         C.POINTER(C.c_int32), _f64p, _f64p, _f64p, _f64p, _f64p]
+        L.oracle_hist_ff.restype = C.c_int64
+        L.oracle_hist_ff.argtypes = [C.c_int, _f32p, C.c_int32, _f32p, C.c_int32, _f32p, C.c_int32, C.c_double,
+                                     C.c_int32, C.c_double, C.POINTER(C.c_int32), _f64p, _f64p, _f64p, _f64p, _f64p,
+                                     _f64p, _f64p]
+        L.oracle_debye_ff.restype = None
+        L.oracle_debye_ff.argtypes = [C.c_int, _f64p, _f64p, _f64p, C.c_int32, _f64p, _f64p, _f64p, _f64p, C.c_int32,
+                                      C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, _f64p,
+                                      _f64p]
+        L.oracle_debye_simple.restype = None
+        L.oracle_debye_simple.argtypes = [_f64p, _f64p, _f64p, C.c_int32, _f64p, _f64p, C.c_int32, C.c_double, _f64p]
+        L.oracle_sinqd.restype = None
+        L.oracle_sinqd.argtypes = [_f64p, C.c_int32, C.c_int32, _f64p, _f64p, C.c_int32, _f64p]
+        L.oracle_ff_raw.restype = C.c_double
+        L.oracle_ff_raw.argtypes = [C.c_int, C.c_double]
+        L.oracle_ff_exv_volume.restype = C.c_double
+        L.oracle_ff_exv_volume.argtypes = [C.c_double, C.c_double]
+        L.oracle_linear_lsq.restype = None
+        L.oracle_linear_lsq.argtypes = [_f64p, _f64p, _f64p, C.c_int32, _f64p]
+        _lib = L
+    return _lib
+
+
+def pack_points(xyz: np.ndarray, fourth: np.ndarray, as_int: bool) -> np.ndarray:
+    """float32 [n,4] records {x, y, z, w|ff} as the reference's compact coordinates."""
+    n = len(xyz)
+    out = np.zeros((n, 4), np.float32)
+    out[:, :3] = np.asarray(xyz, np.float64).astype(np.float32)
+    if as_int:
+        out[:, 3] = np.asarray(fourth, np.int32).view(np.float32)
+    else:
+        out[:, 3] = np.asarray(fourth, np.float64).astype(np.float32)
+    return np.ascontiguousarray(out)
+
+
+@dataclass
+class SimpleHist:
+    aa: np.ndarray
+    aw: np.ndarray
+    ww: np.ndarray
+    tot: np.ndarray
+    d_axis: np.ndarray
+    overflow: int = 0
+
+
+@dataclass
+class FFHist:
+    aa: np.ndarray  # [15,15,mb]
+    aw: np.ndarray  # [15,mb]
+    ww: np.ndarray  # [mb]
+    tot: np.ndarray
+    d_axis: np.ndarray
+    d_axis_ax: Optional[np.ndarray] = None
+    d_axis_xx: Optional[np.ndarray] = None
+    overflow: int = 0
+
+
+def hist_simple(atoms4, waters4, bin_width, nbins, weighted=True) -> SimpleHist:
+    L = lib()
+    mb = C.c_int32(0)
+    bufs = [np.zeros(nbins) for _ in range(5)]
+    of = L.oracle_hist_simple(np.ascontiguousarray(atoms4, np.float32), len(atoms4),
+                              np.ascontiguousarray(waters4, np.float32), len(waters4), bin_width, nbins,
+                              int(weighted), C.byref(mb), *bufs)
+    m = mb.value
+    return SimpleHist(*(b[:m].copy() for b in bufs), overflow=int(of))
+
+
+def hist_ff(kind, atoms4, waters4, exv4=None, bin_width=0.25, nbins=8000, z_exv=0.0) -> FFHist:
+    """kind: 0 FFAvg, 1 FFExplicit, 2 FFGrid."""
+    L = lib()
+    mb = C.c_int32(0)
+    if exv4 is None:
+        exv4 = np.zeros((0, 4), np.float32)
+    aa = np.zeros(NFF * NFF * nbins)
+    aw = np.zeros(NFF * nbins)
+    ww, tot, d, dax, dxx = (np.zeros(nbins) for _ in range(5))
+    of = L.oracle_hist_ff(kind, np.ascontiguousarray(atoms4, np.float32), len(atoms4),
+                          np.ascontiguousarray(waters4, np.float32), len(waters4),
+                          np.ascontiguousarray(exv4, np.float32), len(exv4), bin_width, nbins, z_exv, C.byref(mb),
+                          aa, aw, ww, tot, d, dax, dxx)
+    m = mb.value
+    return FFHist(aa[: NFF * NFF * m].reshape(NFF, NFF, m).copy(), aw[: NFF * m].reshape(NFF, m).copy(), ww[:m].copy(),
+                  tot[:m].copy(), d[:m].copy(), dax[:m].copy() if kind == 2 else None,
+                  dxx[:m].copy() if kind == 2 else None, overflow=int(of))
+
+
+def debye_ff(kind, h: FFHist, q, cw=1.0, cx=1.0, crho=1.0, dw_atomic=0.0, dw_exv=0.0, grid_width=1.0):
+    L = lib()
+    q = np.ascontiguousarray(q, np.float64)
+    nq = len(q)
+    mb = len(h.d_axis)
+    prof = np.zeros(6 * nq)
+    I = np.zeros(nq)
+    dax = h.d_axis_ax if h.d_axis_ax is not None else h.d_axis
+    dxx = h.d_axis_xx if h.d_axis_xx is not None else h.d_axis
+    L.oracle_debye_ff(kind, np.ascontiguousarray(h.aa.reshape(-1)), np.ascontiguousarray(h.aw.reshape(-1)),
+                      np.ascontiguousarray(h.ww), mb, np.ascontiguousarray(h.d_axis), np.ascontiguousarray(dax),
+                      np.ascontiguousarray(dxx), q, nq, cw, cx, crho, dw_atomic, dw_exv, grid_width, prof, I)
+    return I, prof.reshape(6, nq)
+
+
+def debye_simple(h: SimpleHist, q, cw=1.0):
+    L = lib()
+    q = np.ascontiguousarray(q, np.float64)
+    I = np.zeros(len(q))
+    L.oracle_debye_simple(h.aa, h.aw, h.ww, len(h.d_axis), np.ascontiguousarray(h.d_axis), q, len(q), cw, I)
+    return I
+
+
+def sinqd(p, d_axis, q):
+    L = lib()
+    p = np.ascontiguousarray(np.atleast_2d(p), np.float64)
+    out = np.zeros((p.shape[0], len(q)))
+    L.oracle_sinqd(p, p.shape[0], p.shape[1], np.ascontiguousarray(d_axis, np.float64),
+                   np.ascontiguousarray(q, np.float64), len(q), out)
+    return out
+
+
+def ff_raw(t, q):
+    return np.array([lib().oracle_ff_raw(int(t), float(x)) for x in np.atleast_1d(q)])
+
+
+def linear_lsq(data, model, err):
+    out = np.zeros(5)
+    lib().oracle_linear_lsq(np.ascontiguousarray(data, np.float64), np.ascontiguousarray(model, np.float64),
+                            np.ascontiguousarray(err, np.float64), len(data), out)
+    return out
+
+
+# ---------------------------------------------------------------------------
+# The reference compiled from source (oracle/_ref/libausaxs_ref.so)
+# ---------------------------------------------------------------------------
+
+def ref_path() -> str:
+    return os.path.join(HERE, "_ref", "libausaxs_ref.so")
+
+
+def ref_available() -> bool:
+    return os.path.exists(ref_path())
+
+
+def ref(threads: int = 0):
+    """Load the compiled reference once; threads sizes its global pool (first call only)."""
+    global _ref
+    if _ref is None:
+        R = C.CDLL(ref_path())
+        vp = C.c_void_p
+        R.ref_last_error.restype = C.c_char_p
+        R.ref_init.argtypes = [C.c_int]
+        R.ref_set_axes.argtypes = [C.c_double, C.c_int, C.c_double, C.c_double]
+        R.ref_set_simple_exv.argtypes = [C.c_int]
+        R.ref_molecule_new.restype = vp
+        R.ref_molecule_new.argtypes = [_f64p, C.c_int, _f64p, C.c_int, _i32p, C.c_int, C.c_double]
+        R.ref_molecule_free.argtypes = [vp]
+        R.ref_body_move.argtypes = [vp, C.c_int, _f64p, _f64p]
+        R.ref_manager_set.argtypes = [vp, C.c_int, C.c_int, _f64p, C.c_int]
+        R.ref_manager_calculate.restype = vp
+        R.ref_manager_calculate.argtypes = [vp, C.POINTER(C.c_double)]
+        R.ref_hist_free.argtypes = [vp]
+        R.ref_hist_bins.argtypes = [vp]
+        R.ref_hist_total.argtypes = [vp, _f64p, _f64p]
+        R.ref_hist_simple.argtypes = [vp, _f64p, _f64p, _f64p]
+        R.ref_hist_ff.argtypes = [vp, _f64p, _f64p, _f64p]
+        R.ref_hist_grid_axes.argtypes = [vp, _f64p, _f64p]
+        R.ref_hist_grid_axis_sizes.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        R.ref_debye.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, _f64p, _f64p, _f64p,
+                                C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        R.ref_exact_debye.argtypes = [vp, _f64p, C.c_int, _f64p]
+        R.ref_linear_lsq.argtypes = [_f64p, _f64p, _f64p, C.c_int, _f64p]
+        n = threads if threads > 0 else max(1, (os.cpu_count() or 2) - 1)
+        _check(R, R.ref_init(n))
+        _ref = R
+    return _ref
+
+
+def _check(R, rc):
+    if rc != 0:
+        raise RuntimeError("reference: " + R.ref_last_error().decode())
+
+
+MANAGERS = {"single": 0, "mt": 1, "ffavg": 2, "ffexplicit": 3, "ffgrid": 4, "partial": 5}
+
+
+class RefMolecule:
+    """A reference data::Molecule built from arrays (atoms: x y z w ff; waters: x y z w)."""
+
+    def __init__(self, atoms_xyz, atoms_w, atoms_ff, waters_xyz, waters_w, body_sizes=None, volume=-1.0):
+        R = ref()
+        na = len(atoms_xyz)
+        a = np.zeros((na, 5))
+        a[:, :3] = atoms_xyz
+        a[:, 3] = atoms_w
+        a[:, 4] = atoms_ff
+        nw = len(waters_xyz)
+        w = np.zeros((max(nw, 1), 4))
+        if nw:
+            w[:nw, :3] = waters_xyz
+            w[:nw, 3] = waters_w
+        bs = np.asarray(body_sizes if body_sizes is not None else [na], np.int32)
+        self.h = R.ref_molecule_new(np.ascontiguousarray(a.reshape(-1)) if na else np.zeros(5), na,
+                                    np.ascontiguousarray(w.reshape(-1)), nw, bs, len(bs), float(volume))
+        if not self.h:
+            raise RuntimeError("reference: " + R.ref_last_error().decode())
+
+    def __del__(self):
+        if getattr(self, "h", None) and _ref is not None:
+            _ref.ref_molecule_free(self.h)
+            self.h = None
+
+    def set_manager(self, name, weighted_bins=True, exv_xyz=None):
+        R = ref()
+        x = np.zeros(3) if exv_xyz is None or len(exv_xyz) == 0 else np.ascontiguousarray(np.asarray(exv_xyz, np.float64).reshape(-1))
+        nx = 0 if exv_xyz is None else len(exv_xyz)
+        _check(R, R.ref_manager_set(self.h, MANAGERS[name], int(weighted_bins), x, nx))
+
+    def move_body(self, body, Rm, t):
+        R = ref()
+        _check(R, R.ref_body_move(self.h, body, np.ascontiguousarray(np.asarray(Rm, np.float64).reshape(9)),
+                                  np.ascontiguousarray(np.asarray(t, np.float64).reshape(3))))
+
+    def calculate(self):
+        R = ref()
+        secs = C.c_double(0)
+        hp = R.ref_manager_calculate(self.h, C.byref(secs))
+        if not hp:
+            raise RuntimeError("reference: " + R.ref_last_error().decode())
+        return RefHist(hp, secs.value)
+
+    def exact_debye(self, q):
+        R = ref()
+        q = np.ascontiguousarray(q, np.float64)
+        out = np.zeros(len(q))
+        _check(R, R.ref_exact_debye(self.h, q, len(q), out))
+        return out
+
+
+class RefHist:
+    def __init__(self, h, seconds):
+        self.h = h
+        self.seconds = seconds
+
+    def __del__(self):
+        if getattr(self, "h", None) and _ref is not None:
+            _ref.ref_hist_free(self.h)
+            self.h = None
+
+    @property
+    def bins(self):
+        return ref().ref_hist_bins(self.h)
+
+    def total(self):
+        n = self.bins
+        c, d = np.zeros(n), np.zeros(n)
+        _check(ref(), ref().ref_hist_total(self.h, c, d))
+        return c, d
+
+    def simple(self):
+        n = self.bins
+        a, b, c = np.zeros(n), np.zeros(n), np.zeros(n)
+        _check(ref(), ref().ref_hist_simple(self.h, a, b, c))
+        return a, b, c
+
+    def ff(self):
+        n = self.bins
+        a, b, c = np.zeros(NFF * NFF * n), np.zeros(NFF * n), np.zeros(n)
+        _check(ref(), ref().ref_hist_ff(self.h, a, b, c))
+        return a.reshape(NFF, NFF, n), b.reshape(NFF, n), c
+
+    def grid_axes(self):
+        na, nx = C.c_int(0), C.c_int(0)
+        _check(ref(), ref().ref_hist_grid_axis_sizes(self.h, C.byref(na), C.byref(nx)))
+        a, x = np.zeros(na.value), np.zeros(nx.value)
+        _check(ref(), ref().ref_hist_grid_axes(self.h, a, x))
+        return a, x
+
+    def debye(self, cw=1.0, cx=1.0, crho=1.0, dw_atomic=0.0, dw_exv=0.0):
+        R = ref()
+        q, I, prof = np.zeros(200), np.zeros(200), np.zeros(6 * 200)
+        nq = C.c_int(0)
+        secs = C.c_double(0)
+        _check(R, R.ref_debye(self.h, cw, cx, crho, dw_atomic, dw_exv, q, I, prof, C.byref(nq), C.byref(secs)))
+        n = nq.value
+        return q[:n].copy(), I[:n].copy(), prof[: 6 * n].reshape(6, n).copy(), secs.value
+
+
+def ref_set_axes(bin_width=0.25, bin_count=8000, qmin=1e-4, qmax=0.5):
+    R = ref()
+    _check(R, R.ref_set_axes(bin_width, bin_count, qmin, qmax))
+
+
+def ref_set_simple_exv(enable: bool):
+    R = ref()
+    _check(R, R.ref_set_simple_exv(int(enable)))
+
+
+def ref_linear_lsq(data, model, err):
+    R = ref()
+    out = np.zeros(5)
+    _check(R, R.ref_linear_lsq(np.ascontiguousarray(data, np.float64), np.ascontiguousarray(model, np.float64),
+                               np.ascontiguousarray(err, np.float64), len(data), out))
+    return out

@@ -1,0 +1,361 @@
+// C entry points over the reference implementation, compiled from the
+// reference's own sources by oracle/Makefile into oracle/_ref/libausaxs_ref.so.
+//
+// Test infrastructure only: the parity tests call it (through ctypes) to pin
+// the C restatement in oracle/oracle.c and the CUDA path, and bench.py's
+// reference arm times it as the CPU baseline.  Nothing in the product links it.
+//
+// Every function drives the reference's public C++ API exactly as its own
+// tests do (tests/feature/hist/hist_test_helper.h:19-27 for the volume-scaled
+// molecule; histogram_manager.cpp:74-190 for the managers).  Arrays are
+// row-major FP64, sizes are explicit, errors come back as a non-zero int with
+// the message in ref_last_error().
+#include <data/Body.h>
+#include <data/Molecule.h>
+#include <data/atoms/AtomFF.h>
+#include <data/atoms/Water.h>
+#include <dataset/SimpleDataset.h>
+#include <fitter/detail/LinearLeastSquares.h>
+#include <grid/detail/GridExcludedVolume.h>
+#include <hist/detail/SimpleExvModel.h>
+#include <hist/distribution/Distribution1D.h>
+#include <hist/distribution/Distribution2D.h>
+#include <hist/distribution/Distribution3D.h>
+#include <hist/histogram_manager/HistogramManager.h>
+#include <hist/histogram_manager/HistogramManagerMT.h>
+#include <hist/histogram_manager/HistogramManagerMTFFAvg.h>
+#include <hist/histogram_manager/HistogramManagerMTFFExplicit.h>
+#include <hist/histogram_manager/HistogramManagerMTFFGrid.h>
+#include <hist/histogram_manager/PartialHistogramManagerMT.h>
+#include <hist/intensity_calculator/CompositeDistanceHistogramFFGrid.h>
+#include <hist/intensity_calculator/DistanceHistogram.h>
+#include <hist/intensity_calculator/ExactDebyeCalculator.h>
+#include <hist/intensity_calculator/ICompositeDistanceHistogram.h>
+#include <hist/intensity_calculator/ICompositeDistanceHistogramExv.h>
+#include <math/Matrix.h>
+#include <settings/ExvSettings.h>
+#include <settings/Flags.h>
+#include <settings/GeneralSettings.h>
+#include <settings/HistogramSettings.h>
+
+#include <chrono>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+using namespace ausaxs;
+
+namespace {
+thread_local std::string g_err;
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        f();
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+    } catch (...) {
+        g_err = "unknown exception";
+    }
+    return 1;
+}
+
+// A molecule whose excluded volume is given instead of derived from the
+// reference's voxel grid, as the reference's own DebugMolecule does.
+class FixedVolumeMolecule : public data::Molecule {
+  public:
+    using Molecule::Molecule;
+    double get_volume_grid() const override { return volume >= 0 ? volume : data::Molecule::get_volume_grid(); }
+    double volume = -1;
+};
+
+// The grid manager with its excluded-volume dummies supplied by the caller
+// (HistogramManagerMTFFGrid::get_exv is the one virtual hook for them).
+template <bool vbw>
+class GivenExvGridManager : public hist::HistogramManagerMTFFGrid<vbw> {
+  public:
+    GivenExvGridManager(observer_ptr<const data::Molecule> m, std::vector<Vector3<double>> x)
+        : hist::HistogramManagerMTFFGrid<vbw>(m), exv(std::move(x)) {}
+
+  private:
+    grid::exv::GridExcludedVolume get_exv() const override {
+        grid::exv::GridExcludedVolume g;
+        g.interior = exv;
+        return g;
+    }
+    std::vector<Vector3<double>> exv;
+};
+
+struct Result {
+    std::unique_ptr<hist::ICompositeDistanceHistogram> h;
+    int kind = 0;
+};
+
+bool custom_width() { return settings::flags::custom_bin_width; }
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error() { return g_err.c_str(); }
+
+// Must be called before any other entry point: sizes the reference's global
+// thread pool (settings::general::threads, read once at first use).
+int ref_init(int threads) {
+    return guarded([&] {
+        settings::general::threads = threads > 0 ? threads : 1;
+        settings::flags::init_histogram_manager = false;
+        settings::general::verbose = false;
+    });
+}
+
+int ref_set_axes(double bin_width, int bin_count, double qmin, double qmax) {
+    return guarded([&] {
+        settings::axes::bin_count = static_cast<unsigned int>(bin_count);
+        settings::axes::bin_width = bin_width;
+        settings::axes::qmin = qmin;
+        settings::axes::qmax = qmax;
+    });
+}
+
+int ref_set_simple_exv(int enable) {
+    return guarded([&] {
+        if (enable) hist::detail::SimpleExvModel::enable();
+        else hist::detail::SimpleExvModel::disable();
+    });
+}
+
+// atoms: n_a rows of {x, y, z, weight, ff_type}; waters: n_w rows of {x, y, z, weight}.
+// body_sizes splits the atoms into consecutive bodies (n_bodies >= 1); all
+// waters go to the first body.  volume < 0 keeps the reference's own grid volume.
+void* ref_molecule_new(const double* atoms, int n_a, const double* waters, int n_w,
+                       const int* body_sizes, int n_bodies, double volume) {
+    FixedVolumeMolecule* out = nullptr;
+    int rc = guarded([&] {
+        std::vector<data::Body> bodies;
+        int off = 0;
+        int nb = n_bodies > 0 ? n_bodies : 1;
+        for (int b = 0; b < nb; ++b) {
+            int sz = n_bodies > 0 ? body_sizes[b] : n_a;
+            std::vector<data::AtomFF> a;
+            a.reserve(sz);
+            for (int i = off; i < off + sz; ++i) {
+                const double* r = atoms + 5 * static_cast<size_t>(i);
+                a.emplace_back(Vector3<double>(r[0], r[1], r[2]), static_cast<form_factor::form_factor_t>(static_cast<int>(r[4])), r[3]);
+            }
+            off += sz;
+            std::vector<data::Water> w;
+            if (b == 0) {
+                w.reserve(n_w);
+                for (int i = 0; i < n_w; ++i) {
+                    const double* r = waters + 4 * static_cast<size_t>(i);
+                    data::Water x(Vector3<double>(r[0], r[1], r[2]));
+                    x.weight() = r[3];
+                    w.push_back(x);
+                }
+            }
+            bodies.emplace_back(std::move(a), std::move(w));
+        }
+        out = new FixedVolumeMolecule(std::move(bodies));
+        out->volume = volume;
+    });
+    return rc == 0 ? out : nullptr;
+}
+
+void ref_molecule_free(void* m) { delete static_cast<FixedVolumeMolecule*>(m); }
+
+// Rigid move of one body: x <- R x + t, through Body::rotate / Body::translate
+// (source/core/data/Body.cpp:135-156), which also signal the partial managers.
+int ref_body_move(void* m, int body, const double* R, const double* t) {
+    return guarded([&] {
+        auto* mol = static_cast<FixedVolumeMolecule*>(m);
+        auto& b = mol->get_body(body);
+        Matrix<double> M{{R[0], R[1], R[2]}, {R[3], R[4], R[5]}, {R[6], R[7], R[8]}};
+        b.rotate(M);
+        b.translate(Vector3<double>(t[0], t[1], t[2]));
+    });
+}
+
+// manager: 0 HistogramManager (1 thread), 1 HistogramManagerMT, 2 MTFFAvg,
+// 3 MTFFExplicit, 4 MTFFGrid (exv dummies given), 5 PartialHistogramManagerMT.
+// The manager is installed in the molecule (Molecule::set_histogram_manager,
+// which binds the body signallers the partial manager listens to);
+// ref_manager_calculate then runs Molecule::get_histogram().
+int ref_manager_set(void* m, int manager, int weighted_bins, const double* exv, int n_x) {
+    return guarded([&] {
+        hist::IHistogramManager* out = nullptr;
+        auto* mol = static_cast<FixedVolumeMolecule*>(m);
+        bool vbw = custom_width();
+        bool wb = weighted_bins != 0;
+        std::vector<Vector3<double>> x;
+        for (int i = 0; i < n_x; ++i) x.emplace_back(exv[3 * i], exv[3 * i + 1], exv[3 * i + 2]);
+#define PICK(T)                                                                   \
+    if (wb) out = vbw ? (hist::IHistogramManager*)new T<true, true>(mol)          \
+                      : (hist::IHistogramManager*)new T<true, false>(mol);        \
+    else out = vbw ? (hist::IHistogramManager*)new T<false, true>(mol)            \
+                   : (hist::IHistogramManager*)new T<false, false>(mol);
+        switch (manager) {
+            case 0: PICK(hist::HistogramManager); break;
+            case 1: PICK(hist::HistogramManagerMT); break;
+            case 2: PICK(hist::HistogramManagerMTFFAvg); break;
+            case 3: PICK(hist::HistogramManagerMTFFExplicit); break;
+            case 4:
+                out = vbw ? (hist::IHistogramManager*)new GivenExvGridManager<true>(mol, std::move(x))
+                          : (hist::IHistogramManager*)new GivenExvGridManager<false>(mol, std::move(x));
+                break;
+            case 5: PICK(hist::PartialHistogramManagerMT); break;
+            default: throw std::runtime_error("unknown manager");
+        }
+#undef PICK
+        mol->set_histogram_manager(std::unique_ptr<hist::IHistogramManager>(out));
+    });
+}
+
+void* ref_manager_calculate(void* m, double* seconds) {
+    Result* out = nullptr;
+    int rc = guarded([&] {
+        auto t0 = std::chrono::steady_clock::now();
+        auto h = static_cast<FixedVolumeMolecule*>(m)->get_histogram();
+        auto t1 = std::chrono::steady_clock::now();
+        if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+        out = new Result{std::move(h), 0};
+    });
+    return rc == 0 ? out : nullptr;
+}
+
+void ref_hist_free(void* r) { delete static_cast<Result*>(r); }
+
+int ref_hist_bins(void* r) { return static_cast<int>(static_cast<Result*>(r)->h->get_d_axis().size()); }
+
+int ref_hist_total(void* r, double* counts, double* d_axis) {
+    return guarded([&] {
+        auto* h = static_cast<Result*>(r)->h.get();
+        const auto& c = h->get_weighted_counts();
+        const auto& d = h->get_d_axis();
+        std::memcpy(counts, c.data(), c.size() * sizeof(double));
+        std::memcpy(d_axis, d.data(), d.size() * sizeof(double));
+    });
+}
+
+// Simple (weights) composite: aa, aw, ww weighted counts, each bins long.
+int ref_hist_simple(void* r, double* aa, double* aw, double* ww) {
+    return guarded([&] {
+        auto* h = static_cast<Result*>(r)->h.get();
+        const auto& a = h->get_aa_counts();
+        const auto& b = h->get_aw_counts();
+        const auto& c = h->get_ww_counts();
+        for (size_t i = 0; i < a.size(); ++i) aa[i] = a.index(i);
+        for (size_t i = 0; i < b.size(); ++i) aw[i] = b.index(i);
+        for (size_t i = 0; i < c.size(); ++i) ww[i] = c.index(i);
+    });
+}
+
+// Form-factor composites: raw aa [15][15][bins], aw [15][bins], ww [bins].
+int ref_hist_ff(void* r, double* aa, double* aw, double* ww) {
+    return guarded([&] {
+        auto* h = dynamic_cast<hist::ICompositeDistanceHistogramExv*>(static_cast<Result*>(r)->h.get());
+        if (!h) throw std::runtime_error("not a form-factor histogram");
+        const auto& a = h->get_raw_aa_counts_by_ff();
+        const auto& b = h->get_raw_aw_counts_by_ff();
+        const auto& c = h->get_raw_ww_counts_by_ff();
+        size_t nb = c.size();
+        for (size_t i = 0; i < 15; ++i)
+            for (size_t j = 0; j < 15; ++j)
+                for (size_t k = 0; k < nb; ++k) aa[(i * 15 + j) * nb + k] = a.index(i, j, k);
+        for (size_t i = 0; i < 15; ++i)
+            for (size_t k = 0; k < nb; ++k) aw[i * nb + k] = b.index(i, k);
+        for (size_t k = 0; k < nb; ++k) ww[k] = c.index(k);
+    });
+}
+
+// Grid composite: the extra ax and xx weighted distance axes (bins long).
+int ref_hist_grid_axes(void* r, double* ax, double* xx) {
+    return guarded([&] {
+        auto* h = dynamic_cast<hist::CompositeDistanceHistogramFFGrid*>(static_cast<Result*>(r)->h.get());
+        if (!h) throw std::runtime_error("not a grid histogram");
+        const auto& a = h->get_d_axis_ax();
+        const auto& x = h->get_d_axis_xx();
+        std::memcpy(ax, a.data(), a.size() * sizeof(double));
+        std::memcpy(xx, x.data(), x.size() * sizeof(double));
+    });
+}
+
+int ref_hist_grid_axis_sizes(void* r, int* n_ax, int* n_xx) {
+    return guarded([&] {
+        auto* h = dynamic_cast<hist::CompositeDistanceHistogramFFGrid*>(static_cast<Result*>(r)->h.get());
+        if (!h) throw std::runtime_error("not a grid histogram");
+        *n_ax = static_cast<int>(h->get_d_axis_ax().size());
+        *n_xx = static_cast<int>(h->get_d_axis_xx().size());
+    });
+}
+
+// debye_transform() on the reference's default q axis restricted to
+// [qmin, qmax].  For form-factor histograms the six partial profiles
+// {aa, ax, aw, xx, wx, ww} are written to profiles (6 x nq) when non-null;
+// for the Simple histogram {aa, aw, ww} go to rows 0, 2, 5.
+int ref_debye(void* r, double cw, double cx, double crho, double dw_atomic, double dw_exv,
+              double* q_out, double* Iq, double* profiles, int* nq, double* seconds) {
+    return guarded([&] {
+        auto* h = static_cast<Result*>(r)->h.get();
+        h->apply_water_scaling_factor(cw);
+        auto* x = dynamic_cast<hist::ICompositeDistanceHistogramExv*>(h);
+        if (x) {
+            x->apply_excluded_volume_scaling_factor(cx);
+            x->apply_solvent_density_scaling_factor(crho);
+            x->apply_atomic_debye_waller_factor(dw_atomic);
+            x->apply_exv_debye_waller_factor(dw_exv);
+        }
+        auto t0 = std::chrono::steady_clock::now();
+        auto I = h->debye_transform();
+        auto t1 = std::chrono::steady_clock::now();
+        if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+        const auto& c = I.get_counts();
+        auto qv = I.get_axis().as_vector();
+        *nq = static_cast<int>(c.size());
+        if (Iq) std::memcpy(Iq, c.data(), c.size() * sizeof(double));
+        if (q_out) std::memcpy(q_out, qv.data(), qv.size() * sizeof(double));
+        if (profiles) {
+            size_t n = c.size();
+            auto put = [&](int row, const hist::ScatteringProfile& p) {
+                const auto& v = p.get_counts();
+                std::memcpy(profiles + row * n, v.data(), n * sizeof(double));
+            };
+            std::memset(profiles, 0, 6 * n * sizeof(double));
+            put(0, h->get_profile_aa());
+            put(2, h->get_profile_aw());
+            put(5, h->get_profile_ww());
+            if (x) {
+                put(1, x->get_profile_ax());
+                put(3, x->get_profile_xx());
+                put(4, x->get_profile_wx());
+            }
+        }
+    });
+}
+
+// hist::exact_debye_transform (source/core/hist/intensity_calculator/ExactDebyeCalculator.cpp:13-58).
+int ref_exact_debye(void* m, const double* q, int nq, double* Iq) {
+    return guarded([&] {
+        std::vector<double> qv(q, q + nq);
+        auto I = hist::exact_debye_transform(*static_cast<FixedVolumeMolecule*>(m), qv);
+        std::memcpy(Iq, I.data(), I.size() * sizeof(double));
+    });
+}
+
+// fitter::detail::LinearLeastSquares::fit (source/core/fitter/detail/LinearLeastSquares.cpp:26-55):
+// out = {a, b, sigma_a, sigma_b, chi2}.
+int ref_linear_lsq(const double* data, const double* model, const double* err, int n, double* out) {
+    return guarded([&] {
+        std::vector<double> d(data, data + n), m(model, model + n), e(err, err + n);
+        fitter::detail::LinearLeastSquares f(d, m, e);
+        auto r = f.fit();
+        out[0] = r->get_parameter(0u).value;
+        out[1] = r->get_parameter(1u).value;
+        out[2] = r->get_parameter(0u).error.max;
+        out[3] = r->get_parameter(1u).error.max;
+        out[4] = r->fval;
+    });
+}
+
+}  // extern "C"
