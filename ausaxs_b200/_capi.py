@@ -1,0 +1,213 @@
+"""ctypes binding of the C ABI in include/ausaxs_b200.h.
+
+The library is the in-tree ``ausaxs_b200/_lib/libausaxs_b200.so`` built by ``ausaxs_b200.build``.
+There is no CPU fallback: importing a GPU entry point without the library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libausaxs_b200.so")
+
+OK = 0
+ERR_ARGUMENT = 1
+ERR_CUDA = 2
+ERR_BIN_OVERFLOW = 3
+ERR_FORM_FACTOR = 4
+ERR_CAPACITY = 5
+ERR_TIMEOUT = 6
+ERR_NOT_FOUND = 7
+
+MANAGER_MT = 1
+MANAGER_FFAVG = 2
+MANAGER_FFEXPLICIT = 3
+MANAGER_FFGRID = 4
+
+# every symbol include/ausaxs_b200.h declares
+EXPORTED = [
+    "ausaxs_gpu_ctx_create", "ausaxs_gpu_ctx_destroy", "ausaxs_gpu_ctx_set_stream", "ausaxs_gpu_ctx_launch_count",
+    "ausaxs_gpu_last_error", "ausaxs_gpu_ctx_enable_timing", "ausaxs_gpu_ctx_kernel_time", "ausaxs_gpu_histogram", "ausaxs_gpu_debye", "ausaxs_gpu_profile",
+    "ausaxs_gpu_structure_create", "ausaxs_gpu_structure_destroy", "ausaxs_gpu_structure_profile",
+    "ausaxs_gpu_structure_histogram",
+]
+
+
+class AusaxsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class HistConfig(C.Structure):
+    _fields_ = [("manager", C.c_int32), ("weighted_bins", C.c_int32), ("bin_width", C.c_double),
+                ("bin_count", C.c_int32), ("z_exv", C.c_double)]
+
+
+class HistResult(C.Structure):
+    _fields_ = [("max_bin", C.c_int32), ("pairs", C.c_int64), ("overflow_pairs", C.c_int64),
+                ("aa", C.POINTER(C.c_double)), ("aw", C.POINTER(C.c_double)), ("ww", C.POINTER(C.c_double)),
+                ("tot", C.POINTER(C.c_double)), ("d_axis", C.POINTER(C.c_double)),
+                ("d_axis_ax", C.POINTER(C.c_double)), ("d_axis_xx", C.POINTER(C.c_double))]
+
+
+class DebyeParams(C.Structure):
+    _fields_ = [("cw", C.c_double), ("cx", C.c_double), ("crho", C.c_double), ("dw_atomic", C.c_double),
+                ("dw_exv", C.c_double), ("grid_width", C.c_double), ("precision", C.c_int32),
+                ("tolerance", C.c_double)]
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load():
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m ausaxs_b200.build` (needs nvcc)")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        f32 = C.POINTER(C.c_float)
+        f64 = C.POINTER(C.c_double)
+        L.ausaxs_gpu_last_error.restype = C.c_char_p
+        L.ausaxs_gpu_ctx_create.argtypes = [C.c_int, C.POINTER(vp)]
+        L.ausaxs_gpu_ctx_destroy.argtypes = [vp]
+        L.ausaxs_gpu_ctx_set_stream.argtypes = [vp, vp]
+        L.ausaxs_gpu_ctx_launch_count.argtypes = [vp]
+        L.ausaxs_gpu_ctx_launch_count.restype = C.c_int64
+        L.ausaxs_gpu_ctx_enable_timing.argtypes = [vp, C.c_int32]
+        L.ausaxs_gpu_ctx_kernel_time.argtypes = [vp, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+        L.ausaxs_gpu_histogram.argtypes = [vp, C.POINTER(HistConfig), f32, C.c_int32, f32, C.c_int32, f32, C.c_int32,
+                                           C.POINTER(HistResult)]
+        L.ausaxs_gpu_debye.argtypes = [vp, C.POINTER(HistConfig), C.POINTER(HistResult), f64, C.c_int32,
+                                       C.POINTER(DebyeParams), f64, f64]
+        L.ausaxs_gpu_profile.argtypes = [vp, C.POINTER(HistConfig), f32, C.c_int32, f32, C.c_int32, f32, C.c_int32,
+                                         f64, C.c_int32, C.POINTER(DebyeParams), f64, f64]
+        L.ausaxs_gpu_structure_create.argtypes = [vp, C.c_int32, f32, C.c_int32, f32, C.c_int32, f32, C.c_int32,
+                                                  C.c_int32, C.POINTER(vp)]
+        L.ausaxs_gpu_structure_destroy.argtypes = [vp]
+        L.ausaxs_gpu_structure_profile.argtypes = [vp, vp, C.POINTER(HistConfig), f64, C.c_int32,
+                                                   C.POINTER(DebyeParams), f64, f64]
+        L.ausaxs_gpu_structure_histogram.argtypes = [vp, vp, C.POINTER(HistConfig), C.POINTER(HistResult)]
+        _lib = L
+        return L
+
+
+def check(rc: int):
+    if rc != OK:
+        raise AusaxsError(rc, load().ausaxs_gpu_last_error().decode())
+
+
+def fptr(a: np.ndarray | None, ctype=C.c_float):
+    if a is None:
+        return C.cast(0, C.POINTER(ctype))
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def dptr(a: np.ndarray | None):
+    return fptr(a, C.c_double)
+
+
+def devptr(x, ctype=C.c_double):
+    """Pointer of a device buffer (an integer address or anything with data_ptr())."""
+    addr = x.data_ptr() if hasattr(x, "data_ptr") else int(x)
+    return C.cast(C.c_void_p(addr), C.POINTER(ctype))
+
+
+class Context:
+    """One CUDA context handle of the library (its own stream and workspace)."""
+
+    def __init__(self, device: int = 0):
+        L = load()
+        h = C.c_void_p()
+        check(L.ausaxs_gpu_ctx_create(device, C.byref(h)))
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().ausaxs_gpu_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int | None):
+        check(load().ausaxs_gpu_ctx_set_stream(self.h, C.c_void_p(stream_ptr or 0)))
+
+    @property
+    def launches(self) -> int:
+        return int(load().ausaxs_gpu_ctx_launch_count(self.h))
+
+    def enable_timing(self, on: bool = True):
+        check(load().ausaxs_gpu_ctx_enable_timing(self.h, int(on)))
+
+    def kernel_time(self, cls: int):
+        """(total ms, launches) of a kernel class: 0 pair histograms, 1 finalisation, 2 Debye."""
+        ms = C.c_double(0)
+        n = C.c_int64(0)
+        check(load().ausaxs_gpu_ctx_kernel_time(self.h, cls, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+
+_default = {}
+
+
+def default_context(device: int = 0) -> Context:
+    if device not in _default:
+        _default[device] = Context(device)
+    return _default[device]
+
+
+class Structure:
+    """A device-resident structure (ausaxs_gpu_structure_*): upload once, profile many times."""
+
+    def __init__(self, ctx: Context, atoms, waters, exv=None, ff_typed: bool = True):
+        self.ctx = ctx
+        self._a = np.ascontiguousarray(atoms, np.float32)
+        self._w = np.ascontiguousarray(waters, np.float32)
+        self._x = None if exv is None else np.ascontiguousarray(exv, np.float32)
+        h = C.c_void_p()
+        check(load().ausaxs_gpu_structure_create(ctx.h, int(ff_typed), fptr(self._a), len(self._a), fptr(self._w),
+                                                 len(self._w), fptr(self._x), 0 if self._x is None else len(self._x),
+                                                 1, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().ausaxs_gpu_structure_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def profile_device(self, cfg: HistConfig, q_dev, nq: int, params: DebyeParams, I_dev, prof_dev=None):
+        """Enqueue coordinates -> I(q) on the context's stream; q/I/profiles are device addresses."""
+        check(load().ausaxs_gpu_structure_profile(self.ctx.h, self.h, C.byref(cfg), devptr(q_dev), nq,
+                                                  C.byref(params), devptr(I_dev),
+                                                  devptr(prof_dev) if prof_dev is not None else C.cast(0, C.POINTER(C.c_double))))
+
+    def histogram(self, cfg: HistConfig, bin_count: int):
+        ff = cfg.manager != MANAGER_MT
+        bufs = {k: np.zeros(n) for k, n in [("aa", (225 if ff else 1) * bin_count), ("aw", (15 if ff else 1) * bin_count),
+                                             ("ww", bin_count), ("tot", bin_count), ("d_axis", bin_count),
+                                             ("d_axis_ax", bin_count), ("d_axis_xx", bin_count)]}
+        r = HistResult()
+        for k, v in bufs.items():
+            setattr(r, k, dptr(v))
+        check(load().ausaxs_gpu_structure_histogram(self.ctx.h, self.h, C.byref(cfg), C.byref(r)))
+        return r, bufs

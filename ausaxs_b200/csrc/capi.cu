@@ -1,0 +1,247 @@
+// The C ABI (include/ausaxs_b200.h): status codes and last-error text instead of exceptions, the
+// convention of the reference's own C API (include/api/api/api_helper.h:15-45).
+#include <cstring>
+#include <string>
+
+#include "engine.cuh"
+
+using namespace ausaxs_b200;
+
+namespace {
+thread_local std::string g_last_error;
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        f();
+        return AUSAXS_OK;
+    } catch (const Error& e) {
+        g_last_error = e.msg;
+        return e.code;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return AUSAXS_ERR_CUDA;
+    } catch (...) {
+        g_last_error = "unknown failure";
+        return AUSAXS_ERR_CUDA;
+    }
+}
+
+Structure& scratch(Ctx& C) {
+    if (!C.scratch) {
+        C.scratch = std::make_unique<Structure>();
+        C.scratch->ctx = &C;
+    }
+    return *C.scratch;
+}
+
+bool ff_manager(int m) { return m == AUSAXS_MANAGER_FFAVG || m == AUSAXS_MANAGER_FFEXPLICIT || m == AUSAXS_MANAGER_FFGRID; }
+
+void check_cfg(const ausaxs_hist_config* cfg) {
+    if (!cfg) throw Error{AUSAXS_ERR_ARGUMENT, "null configuration"};
+}
+
+ausaxs_debye_params default_params(const ausaxs_debye_params* p) {
+    if (p) return *p;
+    ausaxs_debye_params d{};
+    d.cw = d.cx = d.crho = 1.0;
+    d.grid_width = 1.0;
+    d.precision = 0;
+    d.tolerance = 1e-5;
+    return d;
+}
+}  // namespace
+
+extern "C" {
+
+const char* ausaxs_gpu_last_error(void) { return g_last_error.c_str(); }
+
+int ausaxs_gpu_ctx_create(int device, ausaxs_gpu_ctx** out) {
+    return guarded([&] {
+        if (!out) throw Error{AUSAXS_ERR_ARGUMENT, "null output"};
+        *out = nullptr;
+        int n = 0;
+        AUSAXS_CUDA(cudaGetDeviceCount(&n));
+        if (device < 0 || device >= n) throw Error{AUSAXS_ERR_ARGUMENT, "no such CUDA device"};
+        AUSAXS_CUDA(cudaSetDevice(device));
+        auto* c = new ausaxs_gpu_ctx();
+        Ctx& C = c->impl;
+        C.device = device;
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) C.sm_count = prop.multiProcessorCount;
+        if (cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete c;
+            throw Error{AUSAXS_ERR_CUDA, "cudaStreamCreate failed"};
+        }
+        C.own_stream = true;
+        if (cudaMallocHost(&C.h_stats, sizeof(PrepStats)) != cudaSuccess) {
+            cudaStreamDestroy(C.stream);
+            delete c;
+            throw Error{AUSAXS_ERR_CUDA, "cudaMallocHost failed"};
+        }
+        *out = c;
+    });
+}
+
+int ausaxs_gpu_ctx_destroy(ausaxs_gpu_ctx* ctx) {
+    return guarded([&] {
+        if (!ctx) return;
+        Ctx& C = ctx->impl;
+        cudaSetDevice(C.device);
+        cudaStreamSynchronize(C.stream);
+        C.scratch.reset();
+        if (C.h_stats) cudaFreeHost(C.h_stats);
+        if (C.own_stream) cudaStreamDestroy(C.stream);
+        delete ctx;
+    });
+}
+
+int ausaxs_gpu_ctx_set_stream(ausaxs_gpu_ctx* ctx, void* stream) {
+    return guarded([&] {
+        if (!ctx) throw Error{AUSAXS_ERR_ARGUMENT, "null context"};
+        Ctx& C = ctx->impl;
+        if (C.own_stream) {
+            cudaStreamSynchronize(C.stream);
+            cudaStreamDestroy(C.stream);
+            C.own_stream = false;
+        }
+        if (stream) {
+            C.stream = static_cast<cudaStream_t>(stream);
+        } else {
+            AUSAXS_CUDA(cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking));
+            C.own_stream = true;
+        }
+    });
+}
+
+int64_t ausaxs_gpu_ctx_launch_count(const ausaxs_gpu_ctx* ctx) { return ctx ? ctx->impl.launches : 0; }
+
+int ausaxs_gpu_ctx_enable_timing(ausaxs_gpu_ctx* ctx, int32_t enable) {
+    return guarded([&] {
+        if (!ctx) throw Error{AUSAXS_ERR_ARGUMENT, "null context"};
+        Ctx& C = ctx->impl;
+        C.time_collect();
+        for (auto& t : C.timed) t.ms = 0, t.count = 0;
+        C.timing = enable != 0;
+    });
+}
+
+int ausaxs_gpu_ctx_kernel_time(ausaxs_gpu_ctx* ctx, int32_t kernel_class, double* ms, int64_t* launches) {
+    return guarded([&] {
+        if (!ctx || kernel_class < 0 || kernel_class > 2) throw Error{AUSAXS_ERR_ARGUMENT, "bad argument"};
+        Ctx& C = ctx->impl;
+        C.time_collect();
+        if (ms) *ms = C.timed[kernel_class].ms;
+        if (launches) *launches = C.timed[kernel_class].count;
+    });
+}
+
+int ausaxs_gpu_histogram(ausaxs_gpu_ctx* ctx, const ausaxs_hist_config* cfg, const float* atoms, int32_t n_atoms,
+                         const float* waters, int32_t n_waters, const float* exv, int32_t n_exv,
+                         ausaxs_hist_result* out) {
+    return guarded([&] {
+        if (!ctx || !out) throw Error{AUSAXS_ERR_ARGUMENT, "null argument"};
+        check_cfg(cfg);
+        Ctx& C = ctx->impl;
+        AUSAXS_CUDA(cudaSetDevice(C.device));
+        Structure& S = scratch(C);
+        const bool grid = cfg->manager == AUSAXS_MANAGER_FFGRID;
+        S.load(atoms, n_atoms, waters, n_waters, grid ? exv : nullptr, grid ? n_exv : 0, ff_manager(cfg->manager), true);
+        S.enqueue_histogram(*cfg);
+        S.read_histogram(*cfg, out);
+    });
+}
+
+int ausaxs_gpu_debye(ausaxs_gpu_ctx* ctx, const ausaxs_hist_config* cfg, const ausaxs_hist_result* hist,
+                     const double* q, int32_t n_q, const ausaxs_debye_params* params, double* Iq, double* profiles) {
+    return guarded([&] {
+        if (!ctx || !hist || !q || !Iq || n_q < 0) throw Error{AUSAXS_ERR_ARGUMENT, "null argument"};
+        check_cfg(cfg);
+        Ctx& C = ctx->impl;
+        AUSAXS_CUDA(cudaSetDevice(C.device));
+        ausaxs_debye_params p = default_params(params);
+        debye_of_host_histogram(C, *cfg, *hist, q, n_q, p, Iq, profiles);
+    });
+}
+
+int ausaxs_gpu_profile(ausaxs_gpu_ctx* ctx, const ausaxs_hist_config* cfg, const float* atoms, int32_t n_atoms,
+                       const float* waters, int32_t n_waters, const float* exv, int32_t n_exv, const double* q,
+                       int32_t n_q, const ausaxs_debye_params* params, double* Iq, double* profiles) {
+    return guarded([&] {
+        if (!ctx || !q || !Iq || n_q < 0) throw Error{AUSAXS_ERR_ARGUMENT, "null argument"};
+        check_cfg(cfg);
+        Ctx& C = ctx->impl;
+        AUSAXS_CUDA(cudaSetDevice(C.device));
+        Structure& S = scratch(C);
+        const bool grid = cfg->manager == AUSAXS_MANAGER_FFGRID;
+        S.load(atoms, n_atoms, waters, n_waters, grid ? exv : nullptr, grid ? n_exv : 0, ff_manager(cfg->manager), true);
+        ausaxs_debye_params p = default_params(params);
+        size_t need = (size_t)n_q * 8 * 8 + 256;
+        C.io.ensure(need);
+        double* dq = C.io.as<double>();
+        double* dI = dq + n_q;
+        double* dP = dI + n_q;
+        AUSAXS_CUDA(cudaMemcpyAsync(dq, q, (size_t)n_q * 8, cudaMemcpyHostToDevice, C.stream));
+        S.enqueue_histogram(*cfg);
+        S.enqueue_debye(*cfg, dq, n_q, p, dI, profiles ? dP : nullptr);
+        AUSAXS_CUDA(cudaMemcpyAsync(Iq, dI, (size_t)n_q * 8, cudaMemcpyDeviceToHost, C.stream));
+        if (profiles) AUSAXS_CUDA(cudaMemcpyAsync(profiles, dP, (size_t)n_q * 6 * 8, cudaMemcpyDeviceToHost, C.stream));
+        unsigned long long overflow = 0;
+        AUSAXS_CUDA(cudaMemcpyAsync(&overflow, S.plan.dev.as<char>() + S.plan.off_overflow, 8, cudaMemcpyDeviceToHost, C.stream));
+        AUSAXS_CUDA(cudaStreamSynchronize(C.stream));
+        if (overflow) throw Error{AUSAXS_ERR_BIN_OVERFLOW, "pair distances beyond bin_count * bin_width; increase settings::axes::bin_count"};
+    });
+}
+
+int ausaxs_gpu_structure_create(ausaxs_gpu_ctx* ctx, int32_t ff_typed, const float* atoms, int32_t n_atoms,
+                                const float* waters, int32_t n_waters, const float* exv, int32_t n_exv,
+                                int32_t host_pointers, ausaxs_gpu_structure** out) {
+    return guarded([&] {
+        if (!ctx || !out) throw Error{AUSAXS_ERR_ARGUMENT, "null argument"};
+        *out = nullptr;
+        Ctx& C = ctx->impl;
+        AUSAXS_CUDA(cudaSetDevice(C.device));
+        auto* h = new ausaxs_gpu_structure();
+        h->impl.ctx = &C;
+        try {
+            h->impl.load(atoms, n_atoms, waters, n_waters, exv, n_exv, ff_typed ? 1 : 0, host_pointers != 0);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int ausaxs_gpu_structure_destroy(ausaxs_gpu_structure* s) {
+    return guarded([&] {
+        if (!s) return;
+        cudaStreamSynchronize(s->impl.ctx->stream);
+        delete s;
+    });
+}
+
+int ausaxs_gpu_structure_profile(ausaxs_gpu_ctx* ctx, ausaxs_gpu_structure* s, const ausaxs_hist_config* cfg,
+                                 const double* q, int32_t n_q, const ausaxs_debye_params* params, double* Iq,
+                                 double* profiles) {
+    return guarded([&] {
+        if (!ctx || !s || !q || !Iq || n_q < 0) throw Error{AUSAXS_ERR_ARGUMENT, "null argument"};
+        check_cfg(cfg);
+        if (s->impl.ctx != &ctx->impl) throw Error{AUSAXS_ERR_ARGUMENT, "structure belongs to another context"};
+        ausaxs_debye_params p = default_params(params);
+        s->impl.enqueue_histogram(*cfg);
+        s->impl.enqueue_debye(*cfg, q, n_q, p, Iq, profiles);
+    });
+}
+
+int ausaxs_gpu_structure_histogram(ausaxs_gpu_ctx* ctx, ausaxs_gpu_structure* s, const ausaxs_hist_config* cfg,
+                                   ausaxs_hist_result* out) {
+    return guarded([&] {
+        if (!ctx || !s || !out) throw Error{AUSAXS_ERR_ARGUMENT, "null argument"};
+        check_cfg(cfg);
+        s->impl.enqueue_histogram(*cfg);
+        s->impl.read_histogram(*cfg, out);
+    });
+}
+
+}  // extern "C"

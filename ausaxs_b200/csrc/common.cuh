@@ -1,0 +1,80 @@
+// Shared device helpers of the ausaxs_b200 kernels (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ausaxs_b200 {
+
+constexpr int kNff = 15;        // settings::form_factor::max_ff_types (include/core/settings/FormFactorSettings.h:12)
+constexpr int kExv = 0;         // form_factor::exv_bin   (include/core/form_factor/FormFactorType.h:33)
+constexpr int kWater = 1;       // form_factor::water_bin (FormFactorType.h:34)
+constexpr int kMaxTypes = 15;   // distinct atom form-factor types one structure may use
+constexpr float kMagic = 12582912.0f;      // 1.5 * 2^23: x + kMagic rounds x to an integer, ties to even
+constexpr int32_t kMagicBits = 0x4B400000; // bit pattern of kMagic
+constexpr int32_t kResBias = 1 << 20;      // bias of the fixed-point in-bin offset (see pair_eval)
+
+// ---------------------------------------------------------------------------------------------
+// Pair evaluation with the reference's rounding sequence.
+// SIMD evaluators (include/core/hist/detail/data/CompactCoordinatesXYZW.h:382-423, :491-535,
+// :602-655): d2 = (dx*dx + dy*dy) + dz*dz, d = sqrt(d2), bin = cvt_rn(d * inv_w); every operation
+// rounded on its own (the squares are formed before lane shuffles, so nothing contracts), ties to
+// even.  The scalar evaluator used for the last (len mod 4) partners of each row
+// (CompactCoordinatesXYZW.h:303-307, IntrinsicHelpers.h:9-14) is contracted by the reference's
+// release build (GCC -O3 -ffast-math -march=x86-64-v3) to fma(dz, dz, fma(dx, dx, dy*dy)) and
+// rounds ties away from zero (std::round).
+// ---------------------------------------------------------------------------------------------
+struct PairBin {
+    float d;    // distance (float, as the reference accumulates it)
+    float xr;   // bin index as float
+    int32_t bin;
+};
+
+__device__ __forceinline__ PairBin pair_eval(float4 a, float4 b, float inv_w, bool tail) {
+    float dx = __fsub_rn(a.x, b.x);
+    float dy = __fsub_rn(a.y, b.y);
+    float dz = __fsub_rn(a.z, b.z);
+    float s = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+    if (tail) s = __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
+    PairBin r;
+    r.d = __fsqrt_rn(s);
+    float x = __fmul_rn(r.d, inv_w);
+    float xm = __fadd_rn(x, kMagic);               // exact rint for 0 <= x < 2^22
+    r.bin = __float_as_int(xm) - kMagicBits;
+    r.xr = __fsub_rn(xm, kMagic);
+    if (tail && __fsub_rn(x, r.xr) == 0.5f) {      // std::round: ties away from zero
+        r.bin += 1;
+        r.xr = __fadd_rn(r.xr, 1.0f);
+    }
+    // NaN / inf / huge distances: make the bin fail every range check
+    if (!(x < 4194304.0f)) r.bin = 0x7fffffff;
+    return r;
+}
+
+// Fixed-point in-bin offset of a pair: the distance is d = bin*c + r with |r| <= c/2 (c = 1/inv_w
+// rounded to float), r is stored as rint(r * scale) + kResBias in [0, 2^21).  Sums of these are
+// exact integers, so the per-bin mean distance does not depend on summation order; the
+// quantisation step is c * 2^-20 (below 2.4e-7 A at the default 0.25 A bins).
+__device__ __forceinline__ uint32_t pair_residual(const PairBin& p, float c, float scale) {
+    float r = __fmaf_rn(-p.xr, c, p.d);
+    float t = __fadd_rn(__fmul_rn(r, scale), kMagic);
+    return static_cast<uint32_t>(__float_as_int(t) - kMagicBits + kResBias);
+}
+
+// In the reference's j-loops (SimpleCalculator.h:117-141, HistogramManagerMTFFAvg.cpp:216-232)
+// the last (len mod 4) partners of each outer point go through the scalar evaluator.
+__device__ __forceinline__ int32_t tail_start(int32_t j0, int32_t n) { return n - ((n - j0) & 3); }
+
+// ---------------------------------------------------------------------------------------------
+// Five-Gaussian atomic form factors f(q) = sum_i a_i exp(-b_i q^2) + c, with b tabulated in
+// s = q / (4 pi) units (converted by 1 / (16 pi^2)), indexed by form_factor_t
+// (include/core/form_factor/FormFactorTable.h:8-186, FormFactor.h:33-39).
+// Published coefficients: Waasmaier & Kirfel, Acta Cryst. A51 (1995) for C, N, O, S and Ar
+// (OTHER); International Tables for H; Grudinin, Garkavenko & Kazennov, Acta Cryst. D73 (2017)
+// for the united-atom groups.  Entry 0 is the reference's average excluded-volume form factor
+// a = {1}, b = {r^2/2} with r = 1.62 A, not converted (FormFactorTable.h, excluded_volume).
+// ---------------------------------------------------------------------------------------------
+struct FormFactor5 {
+    double a[5], b[5], c;
+};
+
+}  // namespace ausaxs_b200

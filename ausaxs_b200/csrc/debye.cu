@@ -1,0 +1,206 @@
+// Debye transform, FP64 per-q reduction and profile assembly (the K5 stage).
+//
+// For every q: sinqd[r] = sum_b H[r][b] sinc(q d_{g(r)}[b]) and
+//   aa = sum F(ta,tb) sinqd_aa,   ax = sum 2 crho cx F(ta,exv) sinqd_ax,   xx = (cx crho)^2 F(x,x) sinqd_xx,
+//   aw = sum 2 cw F(ta,w) sinqd_aw, wx = 2 crho cx cw F(x,w) sinqd_wx,     ww = cw^2 F(w,w) sinqd_ww,
+//   I  = aa - ax + aw + xx - wx + ww,
+// with Debye-Waller factors, as CompositeDistanceHistogramFFAvgBase::debye_transform
+// (source/core/hist/intensity_calculator/CompositeDistanceHistogramFFAvgBase.cpp:57-76, 333-374,
+// 427-558) and CompositeDistanceHistogramFFGrid (CompositeDistanceHistogramFFGrid.cpp:37-119), or
+// I = exp(-q^2) sum_b (aa + cw aw + cw^2 ww) sinc for the Simple histogram (DistanceHistogram.cpp:54-87).
+//
+// When the split-BF16 tensor-core contraction (debye_tc.cu) has produced sinqd for all q, this kernel
+// only re-evaluates in FP64 the q values whose error estimate exceeds the tolerance: that is where
+// cancellation between bins (and between profiles) bites, typically the high-q WAXS tail.
+#include "debye.cuh"
+
+namespace ausaxs_b200 {
+
+namespace {
+
+__constant__ FormFactor5 c_ff[kNff] = {
+    {{1, 0, 0, 0, 0}, {0, 0, 0, 0, 0}, 0},  // EXCLUDED_VOLUME (b set in ff_raw)
+    {{0.456221, 3.219608, 0.812773, 2.666928, 1.380927}, {21.503498, 13.397134, 34.547137, 5.826620, 0.412902}, 0.463202},  // WATER = OH_alc
+    {{0.489918, 0.262003, 0.196767, 0.049879, 0}, {20.6593, 7.74039, 49.5519, 2.20159, 0}, 0.001305},  // H
+    {{2.657506, 1.078079, 1.490909, -4.241070, 0.713791}, {14.780758, 0.776775, 42.086843, -0.000294, 0.239535}, 4.297983},  // C
+    {{2.909530, 0.485267, 1.516151, 0.206905, 1.541626}, {13.933084, 23.221524, 41.990403, 4.974183, 0.679266}, 0.337670},  // CH
+    {{3.275723, 0.870037, 1.534606, 0.395078, 1.544562}, {13.408502, 23.785175, 41.922444, 5.019072, 0.724439}, 0.377096},  // CH2
+    {{3.681341, 1.228691, 1.549320, 0.574033, 1.554377}, {13.026207, 24.131974, 41.869426, 4.984373, 0.765769}, 0.409294},  // CH3
+    {{11.893780, 3.277479, 1.858092, 0.858927, 0.912985}, {0.000158, 10.232723, 30.344690, 0.656065, 0.217287}, -11.804902},  // N
+    {{1.650531, 0.429639, 2.144736, 1.851894, 1.408921}, {10.603730, 6.987283, 29.939901, 10.573859, 0.611678}, 0.510589},  // NH
+    {{1.904157, 1.942536, 2.435585, 0.730512, 1.379728}, {10.803702, 10.792421, 29.610479, 6.847755, 0.709687}, 0.603738},  // NH2
+    {{1.882162, 1.933200, 2.465843, 0.927311, 1.190889}, {10.975157, 10.956008, 29.208572, 6.663555, 0.843650}, 0.597322},  // NH3
+    {{2.960427, 2.508818, 0.637853, 0.722838, 1.142756}, {14.182259, 5.936858, 0.112726, 34.958481, 0.390240}, 0.027014},  // O
+    {{6.362157, 5.154568, 1.473732, 1.635073, 1.209372}, {1.514347, 22.092528, 0.061373, 55.445176, 0.646925}, 0.154722},  // S
+    {{0.570042, 6.337416, 1.641643, 5.398549, 1.527982}, {11.447986, 1.197657, 55.401032, 22.420955, 2.356552}, 1.523944},  // SH
+    {{7.188004, 6.638454, 0.454180, 1.929593, 1.523654}, {0.956221, 15.339877, 15.339862, 39.043824, 0.062409}, 0.265954},  // OTHER (Ar)
+};
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kRhoWater = 0.334;        // e / A^3 (include/core/constants/Constants.h:114)
+constexpr double kAvgRadius = 1.62;        // A (Constants.h:90)
+constexpr int kChunk = 512;
+constexpr int kThreads = 256;
+constexpr int kMaxRows = 264;
+
+__device__ double ff_raw(int t, double q) {
+    const FormFactor5& f = c_ff[t];
+    const double s_to_q = 1.0 / (4 * 4 * kPi * kPi);
+    double sum = 0;
+    for (int i = 0; i < 5; ++i) {
+        double b = t == kExv ? (i == 0 ? kAvgRadius * kAvgRadius / 2 : 0.0) : f.b[i] * s_to_q;
+        sum += f.a[i] * exp(-b * q * q);
+    }
+    return sum + f.c;
+}
+
+// VectorDebyeTable::initialize (source/core/table/VectorDebyeTable.cpp:24-40)
+__device__ __forceinline__ double sinc64(double x) {
+    if (x < 1e-3) {
+        double x2 = x * x;
+        return 1 - x2 * (1.0 / 6) + x2 * x2 * (1.0 / 120);
+    }
+    return sin(x) / x;
+}
+
+struct QFactors {
+    double f[kNff];  // raw atomic form factors at q
+    double fx;       // excluded-volume form factor at q
+    double ba, bx;   // Debye-Waller factors
+    double eq2;      // exp(-q^2)
+};
+
+__device__ double row_coef(const DebyeArgs& A, const RowDesc& r, const QFactors& F, int& profile) {
+    switch (r.kind) {
+        case kRowAA: profile = 0; return (F.f[r.ta] * F.f[r.tb]) * F.ba * F.ba;
+        case kRowAX: profile = 1; return 2 * A.crho * A.cx * (F.f[r.ta] * F.fx) * F.ba * F.bx;
+        case kRowXX: profile = 3; return (A.cx * A.crho) * (A.cx * A.crho) * (F.fx * F.fx) * F.bx * F.bx;
+        case kRowAW: profile = 2; return 2 * A.cw * (F.f[r.ta] * F.f[kWater]) * F.ba;
+        case kRowWX: profile = 4; return 2 * A.crho * A.cx * A.cw * (F.fx * F.f[kWater]) * F.bx;
+        case kRowWW: profile = 5; return A.cw * A.cw * (F.f[kWater] * F.f[kWater]);
+        case kRowSAA: profile = 0; return F.eq2;
+        case kRowSAW: profile = 2; return F.eq2;
+        case kRowSWW: profile = 5; return F.eq2;
+    }
+    profile = 0;
+    return 0;
+}
+
+__global__ void __launch_bounds__(kThreads) debye_kernel(DebyeArgs A) {
+    const int k = blockIdx.x;
+    if (k >= A.nq) return;
+    const double q = A.q[k];
+    const int R = A.R;
+    const int mb = *A.max_bin;
+    __shared__ double s_sinc[3][kChunk];
+    __shared__ double s_acc[kMaxRows];
+    __shared__ QFactors s_F;
+    __shared__ int s_fp64;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = kThreads >> 5;
+
+    if (threadIdx.x < kNff) s_F.f[threadIdx.x] = ff_raw(threadIdx.x, q);
+    if (threadIdx.x == 32) {
+        if (A.exv_model == 1) {
+            double e = pow(A.grid_volume, 2.0 / 3) / (4 * kPi);  // ExvFormFactor (ExvFormFactor.h:20-33)
+            s_F.fx = A.grid_volume * kRhoWater * exp(-e * q * q);
+        } else {
+            s_F.fx = ff_raw(kExv, q);
+        }
+        s_F.ba = (A.dw_atomic != 0 || A.dw_exv != 0) ? exp(-q * q * A.dw_atomic * A.dw_atomic * 0.5) : 1.0;
+        s_F.bx = (A.dw_atomic != 0 || A.dw_exv != 0) ? exp(-q * q * A.dw_exv * A.dw_exv * 0.5) : 1.0;
+        s_F.eq2 = exp(-q * q);
+    }
+    for (int r = threadIdx.x; r < R; r += kThreads) s_acc[r] = 0;
+    __syncthreads();
+
+    // With tensor-core values: keep this q unless the estimated error is above tolerance.
+    if (threadIdx.x == 0) s_fp64 = 1;
+    __syncthreads();
+    if (A.sinqd_tc && warp == 0) {
+        double I = 0, err = 0;
+        for (int r = lane; r < R; r += 32) {
+            int p;
+            double cf = row_coef(A, A.rows[r], s_F, p);
+            double sgn = (p == 1 || p == 4) ? -1.0 : 1.0;
+            double v = A.sinqd_tc[static_cast<size_t>(r) * A.nq + k];
+            double bnd = A.bound_tc[static_cast<size_t>(r) * A.nq + k];
+            if (A.rows[r].kind == kRowSAW) cf *= A.cw;
+            if (A.rows[r].kind == kRowSWW) cf *= A.cw * A.cw;
+            I += sgn * cf * v;
+            // split-BF16 operands carry 16 significant bits each; FP32 accumulation adds
+            // ~sqrt(K) 2^-24 relative: 2^-14 of the absolute-value sum bounds both
+            err += fabs(cf) * bnd * (1.0 / 16384.0);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            I += __shfl_xor_sync(0xffffffffu, I, o);
+            err += __shfl_xor_sync(0xffffffffu, err, o);
+        }
+        if (lane == 0) {
+            bool ok = err <= A.tolerance * fabs(I);
+            s_fp64 = ok ? 0 : 1;
+            if (!ok && A.fp64_columns) atomicAdd(A.fp64_columns, 1);
+        }
+    }
+    __syncthreads();
+
+    if (s_fp64) {
+        int used_groups = 1;
+        for (int r = 0; r < R; ++r) used_groups = max(used_groups, A.rows[r].group + 1);
+        for (int c0 = 0; c0 < mb; c0 += kChunk) {
+            const int cn = min(kChunk, mb - c0);
+            for (int t = threadIdx.x; t < cn; t += kThreads) {
+                s_sinc[0][t] = sinc64(q * A.axis0[c0 + t]);
+                if (used_groups > 1) s_sinc[1][t] = sinc64(q * A.axis1[c0 + t]);
+                if (used_groups > 2) s_sinc[2][t] = sinc64(q * A.axis2[c0 + t]);
+            }
+            __syncthreads();
+            for (int r = warp; r < R; r += nwarps) {
+                const double* h = A.H + static_cast<size_t>(r) * A.nb + c0;
+                const double* s = s_sinc[A.rows[r].group];
+                double acc = 0;
+                for (int t = lane; t < cn; t += 32) acc += h[t] * s[t];
+                for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                if (lane == 0) s_acc[r] += acc;
+            }
+            __syncthreads();
+        }
+    } else {
+        for (int r = threadIdx.x; r < R; r += kThreads) s_acc[r] = A.sinqd_tc[static_cast<size_t>(r) * A.nq + k];
+        __syncthreads();
+    }
+
+    if (warp == 0) {
+        double prof[6] = {0, 0, 0, 0, 0, 0};
+        for (int r = lane; r < R; r += 32) {
+            int p;
+            double cf = row_coef(A, A.rows[r], s_F, p);
+            prof[p] += cf * s_acc[r];
+        }
+        for (int p = 0; p < 6; ++p)
+            for (int o = 16; o > 0; o >>= 1) prof[p] += __shfl_xor_sync(0xffffffffu, prof[p], o);
+        if (lane == 0) {
+            double I;
+            if (A.rows[0].kind >= kRowSAA) {
+                I = prof[0] + A.cw * prof[2] + A.cw * A.cw * prof[5];
+            } else {
+                I = 0;
+                I += prof[0];
+                I -= prof[1];
+                I += prof[2];
+                I += prof[3];
+                I -= prof[4];
+                I += prof[5];
+            }
+            if (A.overflow && *A.overflow) I = __longlong_as_double(0x7ff8000000000000ll);
+            A.Iq[k] = I;
+            if (A.profiles)
+                for (int p = 0; p < 6; ++p) A.profiles[static_cast<size_t>(p) * A.nq + k] = prof[p];
+        }
+    }
+}
+
+}  // namespace
+
+void debye_fp64_launch(const DebyeArgs& A, cudaStream_t s) { debye_kernel<<<A.nq, kThreads, 0, s>>>(A); }
+
+}  // namespace ausaxs_b200

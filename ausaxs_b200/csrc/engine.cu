@@ -1,0 +1,620 @@
+// Host-side engine of the Debye hot path: structure upload, plan construction and kernel enqueue.
+//
+// The reference runs a histogram manager's calculate_all() as thread-pool tasks over 800-row
+// chunks (SimpleCalculator.h:117-141, GeneralSettings.cpp:50) and keeps all results in host
+// memory.  Here a structure is uploaded once; a Plan lays out every accumulator and output of a
+// (structure, configuration) pair in one device allocation and records the launch shapes, so a
+// profile is a fixed sequence of kernels with no allocation and no host round trip.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "engine.cuh"
+
+namespace ausaxs_b200 {
+
+void DevBuf::ensure(size_t bytes) {
+    if (bytes <= n) return;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    if (bytes == 0) return;
+    AUSAXS_CUDA(cudaMalloc(&p, bytes));
+    n = bytes;
+}
+
+DevBuf::~DevBuf() {
+    if (p) cudaFree(p);
+}
+
+void Ctx::check_launch(const char* what) {
+    ++launches;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw Error{AUSAXS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
+}
+
+static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+void Ctx::time_begin(int cls, cudaEvent_t* ev) {
+    *ev = nullptr;
+    if (!timing) return;
+    AUSAXS_CUDA(cudaEventCreate(ev));
+    AUSAXS_CUDA(cudaEventRecord(*ev, stream));
+    (void)cls;
+}
+
+void Ctx::time_end(int cls, cudaEvent_t start) {
+    if (!timing || !start) return;
+    cudaEvent_t stop;
+    AUSAXS_CUDA(cudaEventCreate(&stop));
+    AUSAXS_CUDA(cudaEventRecord(stop, stream));
+    timed[cls].pending.emplace_back(start, stop);
+}
+
+void Ctx::time_collect() {
+    AUSAXS_CUDA(cudaStreamSynchronize(stream));
+    for (auto& t : timed) {
+        for (auto& e : t.pending) {
+            float ms = 0;
+            AUSAXS_CUDA(cudaEventElapsedTime(&ms, e.first, e.second));
+            t.ms += ms;
+            t.count += 1;
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+        t.pending.clear();
+    }
+}
+
+void Structure::load(const float* atoms, int n_atoms, const float* waters, int n_waters, const float* exv, int n_exv,
+                     int ff_typed_, bool host) {
+    if (n_atoms < 0 || n_waters < 0 || n_exv < 0) throw Error{AUSAXS_ERR_ARGUMENT, "negative point count"};
+    if ((n_atoms && !atoms) || (n_waters && !waters) || (n_exv && !exv)) throw Error{AUSAXS_ERR_ARGUMENT, "null point array"};
+    Ctx& C = *ctx;
+    cudaStream_t s = C.stream;
+    ff_typed = ff_typed_;
+    n_a = n_atoms;
+    n_w = n_waters;
+    n_x = n_exv;
+    raw_a.ensure(align_up(std::max(1, n_a) * 16, 256));
+    raw_w.ensure(align_up(std::max(1, n_w) * 16, 256));
+    raw_x.ensure(align_up(std::max(1, n_x) * 16, 256));
+    cudaMemcpyKind kind = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    if (n_a) AUSAXS_CUDA(cudaMemcpyAsync(raw_a.p, atoms, (size_t)n_a * 16, kind, s));
+    if (n_w) AUSAXS_CUDA(cudaMemcpyAsync(raw_w.p, waters, (size_t)n_w * 16, kind, s));
+    if (n_x) AUSAXS_CUDA(cudaMemcpyAsync(raw_x.p, exv, (size_t)n_x * 16, kind, s));
+
+    PrepStats init{};
+    for (int k = 0; k < 3; ++k) init.lo[k] = 0xffffffffu, init.hi[k] = 0;
+    *C.h_stats = init;
+    C.stats.ensure(sizeof(PrepStats));
+    AUSAXS_CUDA(cudaMemcpyAsync(C.stats.p, C.h_stats, sizeof(PrepStats), cudaMemcpyHostToDevice, s));
+    census_launch(raw_a.as<float4>(), n_a, ff_typed, C.stats.as<PrepStats>(), C.sm_count, s);
+    census_launch(raw_w.as<float4>(), n_w, 0, C.stats.as<PrepStats>(), C.sm_count, s);
+    census_launch(raw_x.as<float4>(), n_x, 0, C.stats.as<PrepStats>(), C.sm_count, s);
+    C.check_launch("census");
+    AUSAXS_CUDA(cudaMemcpyAsync(C.h_stats, C.stats.p, sizeof(PrepStats), cudaMemcpyDeviceToHost, s));
+    AUSAXS_CUDA(cudaStreamSynchronize(s));
+    const PrepStats st = *C.h_stats;
+    if (st.bad & 1u)
+        throw Error{AUSAXS_ERR_FORM_FACTOR,
+                    "an atom has a form-factor type outside [1, 15) (UNKNOWN or excluded volume); form factor "
+                    "information is required for the selected excluded volume model"};
+    if (st.bad & 2u) throw Error{AUSAXS_ERR_ARGUMENT, "non-finite coordinate"};
+    if (n_a + n_w + n_x > 0) {
+        double d2 = 0;
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = ordered_to_float(st.lo[k]);
+            hi[k] = ordered_to_float(st.hi[k]);
+            double e = (double)hi[k] - (double)lo[k];
+            d2 += e * e;
+        }
+        dmax = (float)(std::sqrt(d2) * (1 + 1e-6) + 1e-3);
+    } else {
+        dmax = 0;
+    }
+    int T_new = 0;
+    for (int f = 0; f < kNff; ++f) ff_to_type[f] = -1;
+    if (ff_typed) {
+        for (int f = 1; f < kNff; ++f)
+            if (st.mask & (1u << f)) {
+                type_ff[T_new] = f;
+                type_count[T_new] = st.count[f];
+                ff_to_type[f] = T_new;
+                ++T_new;
+            }
+    }
+    T = T_new;
+    meta.ensure(256);
+    int32_t hmeta[2 * kNff];
+    for (int k = 0; k < kNff; ++k) hmeta[k] = k < T ? type_count[k] : 0, hmeta[kNff + k] = ff_to_type[k];
+    AUSAXS_CUDA(cudaMemcpyAsync(meta.p, hmeta, sizeof(hmeta), cudaMemcpyHostToDevice, s));
+    if (ff_typed) {
+        dense_a.ensure(align_up(std::max(1, n_a) * 16, 256));
+        to_dense_launch(raw_a.as<float4>(), dense_a.as<float4>(), n_a, meta.as<int32_t>(kNff * 4), C.sm_count, s);
+        C.check_launch("to_dense");
+    }
+    AUSAXS_CUDA(cudaStreamSynchronize(s));  // hmeta lives on this stack frame
+}
+
+static long long tri(long long t) { return t * (t + 1) / 2; }
+
+Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
+    Plan& P = plan;
+    if (cfg.bin_width <= 0 || cfg.bin_count <= 0) throw Error{AUSAXS_ERR_ARGUMENT, "bin_width and bin_count must be positive"};
+    const bool ff = cfg.manager == AUSAXS_MANAGER_FFAVG || cfg.manager == AUSAXS_MANAGER_FFEXPLICIT ||
+                    cfg.manager == AUSAXS_MANAGER_FFGRID;
+    if (!ff && cfg.manager != AUSAXS_MANAGER_MT) throw Error{AUSAXS_ERR_ARGUMENT, "unknown manager"};
+    if (ff != (ff_typed != 0))
+        throw Error{AUSAXS_ERR_ARGUMENT, ff ? "form-factor managers need form-factor typed atoms"
+                                            : "the weighted manager needs weighted atoms"};
+    const int weighted = cfg.weighted_bins ? 1 : 0;
+    const float inv_w = (float)(1.0 / cfg.bin_width);
+    int nb = (int)std::ceil((double)dmax * inv_w) + 2;
+    nb = std::max(nb, 11);
+    nb = std::min(nb, cfg.bin_count);
+    if (P.manager == cfg.manager && P.weighted == weighted && P.bin_count == cfg.bin_count &&
+        P.bin_width == cfg.bin_width && P.n_a == n_a && P.n_w == n_w && P.n_x == n_x && P.T == T && P.nb >= nb &&
+        P.nb <= nb + 64)
+        return P;
+
+    Ctx& C = *ctx;
+    P.manager = cfg.manager;
+    P.weighted = weighted;
+    P.bin_count = cfg.bin_count;
+    P.bin_width = cfg.bin_width;
+    P.n_a = n_a;
+    P.n_w = n_w;
+    P.n_x = n_x;
+    P.T = T;
+    P.nb = nb;
+    P.inv_w = inv_w;
+    P.c = (float)(1.0 / (double)inv_w);
+    P.scale = (float)(1048576.0 / (double)P.c);
+    const bool grid = cfg.manager == AUSAXS_MANAGER_FFGRID;
+    const bool mt = cfg.manager == AUSAXS_MANAGER_MT;
+    const int n_x_eff = grid ? n_x : 0;
+
+    long long biggest = std::max<long long>({(long long)n_a, (long long)n_w, (long long)n_x_eff});
+    P.tile = biggest >= 16384 ? 512 : 256;
+    const int tile = P.tile;
+    auto nt = [tile](int n) { return (n + tile - 1) / tile; };
+
+    // job list: {A, na, B, nb, self, row mode, rows, counts slot, dsum slot, wsum slot}
+    struct J {
+        const float4* A;
+        int na;
+        const float4* B;
+        int nbp;
+        int self, rmode, rows;
+        int slot;  // accumulator slot (aa, aw, ww, ax, wx, xx)
+    };
+    std::vector<J> js;
+    const float4* A = atoms_for_pairs();
+    const float4* W = raw_w.as<float4>();
+    const float4* X = raw_x.as<float4>();
+    if (mt) {
+        js.push_back({A, n_a, A, n_a, 1, kRowSingle, 1, 0});
+        js.push_back({W, n_w, A, n_a, 0, kRowSingle, 1, 1});  // waters outer, atoms inner (SimpleCalculator.h:187-205)
+        js.push_back({W, n_w, W, n_w, 1, kRowSingle, 1, 2});
+    } else {
+        js.push_back({A, n_a, A, n_a, 1, kRowPair, T * T, 0});
+        js.push_back({A, n_a, W, n_w, 0, kRowOuter, T, 1});  // atoms outer, waters inner (HistogramManagerMTFFAvg.cpp:236-254)
+        js.push_back({W, n_w, W, n_w, 1, kRowSingle, 1, 2});
+        if (grid) {
+            js.push_back({A, n_a, X, n_x, 0, kRowOuter, T, 3});  // HistogramManagerMTFFGrid.cpp:86-104
+            js.push_back({W, n_w, X, n_x, 0, kRowSingle, 1, 4});  // :106-124
+            js.push_back({X, n_x, X, n_x, 1, kRowSingle, 1, 5});  // :66-84
+        }
+    }
+    const int slots = 6;
+    int slot_rows[slots] = {0, 0, 0, 0, 0, 0};
+    for (auto& j : js) slot_rows[j.slot] = std::max(slot_rows[j.slot], j.rows);
+
+    // on-chip budget: split rows of a job into groups when its [rows][nb] counts do not fit
+    const size_t smem_cap = 232448 - 1024;
+    int max_group_rows = 1;
+    while (max_group_rows < 4096 && pairhist_smem_bytes(max_group_rows + 1, nb, weighted && mt, tile) <= smem_cap) ++max_group_rows;
+    if (pairhist_smem_bytes(1, nb, weighted && mt, tile) > smem_cap)
+        throw Error{AUSAXS_ERR_CAPACITY, "too many distance bins for the on-chip histogram"};
+
+    // layout
+    size_t off = 0;
+    P.off_jobs = off;
+    std::vector<PairJob> jobs;
+    off += align_up(sizeof(PairJob) * 64, 256);
+    P.off_acc = off;
+    size_t slot_cnt[slots], slot_ds[slots], slot_ws[slots];
+    for (int k = 0; k < slots; ++k) {
+        slot_cnt[k] = off;
+        off += align_up((size_t)std::max(1, slot_rows[k]) * nb * 8, 256);
+        slot_ds[k] = off;
+        off += align_up((size_t)nb * 8, 256);
+        slot_ws[k] = off;
+        off += align_up((size_t)nb * 8, 256);
+    }
+    P.off_counter = off;
+    off += 256;
+    P.off_overflow = off;
+    off += 256;
+    P.off_maxbin = off;
+    off += 256;
+    P.off_wscale = off;
+    off += 256;
+    P.off_self = off;
+    off += 256;
+    P.off_fp64cols = off;
+    off += 256;
+    P.acc_bytes = off - P.off_acc;
+    const int R = mt ? 3 : ff_rows(T);
+    P.R = R;
+    P.off_H = off;
+    off += align_up((size_t)R * nb * 8, 256);
+    P.off_tot = off;
+    off += align_up((size_t)nb * 8, 256);
+    P.off_d = off;
+    off += align_up((size_t)nb * 8, 256);
+    P.off_dax = off;
+    off += align_up((size_t)nb * 8, 256);
+    P.off_dxx = off;
+    off += align_up((size_t)nb * 8, 256);
+    P.off_rows = off;
+    off += align_up(sizeof(RowDesc) * R, 256);
+    P.off_expand_aa = off;
+    off += align_up((size_t)kNff * kNff * nb * 8, 256);
+    P.off_expand_aw = off;
+    off += align_up((size_t)kNff * nb * 8, 256);
+    P.dev.ensure(off);
+    char* base = P.dev.as<char>();
+
+    long long tb = 0;
+    P.pairs = 0;
+    P.smem_rows = 1;
+    for (auto& j : js) {
+        if (j.na == 0 || j.nbp == 0) continue;
+        long long tiles = j.self ? tri(nt(j.na)) : (long long)nt(j.na) * nt(j.nbp);
+        long long pairs = j.self ? (long long)j.na * (j.na - 1) / 2 : (long long)j.na * j.nbp;
+        if (pairs == 0) continue;
+        P.pairs += pairs;
+        for (int r0 = 0; r0 < j.rows; r0 += max_group_rows) {
+            int r1 = std::min(j.rows, r0 + max_group_rows);
+            PairJob pj{};
+            pj.A = j.A;
+            pj.B = j.B;
+            pj.na = j.na;
+            pj.nb = j.nbp;
+            pj.self = j.self;
+            pj.row_mode = j.rmode;
+            pj.types = T;
+            pj.row_lo = r0;
+            pj.row_hi = r1;
+            pj.nbins = nb;
+            pj.tiles_i = nt(j.na);
+            pj.tiles_j = nt(j.nbp);
+            pj.tile_begin = tb;
+            pj.tile_count = tiles;
+            pj.inv_w = P.inv_w;
+            pj.c = P.c;
+            pj.scale = P.scale;
+            pj.counts = reinterpret_cast<unsigned long long*>(base + slot_cnt[j.slot]) + (size_t)r0 * nb;
+            // offset sums only feed the weighted d-axis; weight sums are the Simple histogram's values
+            pj.dsum = (r0 == 0 && weighted) ? reinterpret_cast<unsigned long long*>(base + slot_ds[j.slot]) : nullptr;
+            pj.wsum = (mt && r0 == 0) ? reinterpret_cast<long long*>(base + slot_ws[j.slot]) : nullptr;
+            pj.wscale = 0;  // read from device memory by weighted launches (see below)
+            jobs.push_back(pj);
+            tb += tiles;
+            P.smem_rows = std::max(P.smem_rows, r1 - r0);
+        }
+    }
+    if (jobs.size() > 64) throw Error{AUSAXS_ERR_CAPACITY, "too many row groups"};
+    P.n_jobs = (int)jobs.size();
+    P.total_tiles = tb;
+    const bool w_launch = mt;  // Simple histograms always carry weight sums (values)
+    P.smem = pairhist_smem_bytes(P.smem_rows, nb, w_launch, tile);
+    int per_sm = std::max(1, std::min((int)(233472 / (P.smem + 1024)), 2048 / tile));
+    long long want = std::max<long long>(1, P.total_tiles);
+    P.grid = (int)std::min<long long>((long long)C.sm_count * per_sm, want);
+    P.chunk = (int)std::max<long long>(1, std::min<long long>(8, P.total_tiles / ((long long)P.grid * 8)));
+    if (!jobs.empty()) AUSAXS_CUDA(cudaMemcpy(base + P.off_jobs, jobs.data(), sizeof(PairJob) * jobs.size(), cudaMemcpyHostToDevice));
+
+    PairLaunch& L = P.launch;
+    L.jobs = reinterpret_cast<const PairJob*>(base + P.off_jobs);
+    L.n_jobs = P.n_jobs;
+    L.total_tiles = P.total_tiles;
+    L.chunk = P.chunk;
+    L.smem_rows = P.smem_rows;
+    L.smem_bins = nb;
+    L.tile_counter = reinterpret_cast<unsigned long long*>(base + P.off_counter);
+    L.overflow = reinterpret_cast<unsigned long long*>(base + P.off_overflow);
+    L.weighted = w_launch;
+    L.wscale = reinterpret_cast<const float*>(base + P.off_wscale);
+
+    // finalisation
+    auto cnt = [&](int k) { return reinterpret_cast<const unsigned long long*>(base + slot_cnt[k]); };
+    auto ds = [&](int k) { return reinterpret_cast<const unsigned long long*>(base + slot_ds[k]); };
+    if (mt) {
+        FinalizeMT& F = P.fin_mt;
+        F.nb = nb;
+        F.c_aa = cnt(0);
+        F.c_aw = cnt(1);
+        F.c_ww = cnt(2);
+        F.ds_aa = ds(0);
+        F.ds_aw = ds(1);
+        F.ds_ww = ds(2);
+        F.w_aa = reinterpret_cast<const long long*>(base + slot_ws[0]);
+        F.w_aw = reinterpret_cast<const long long*>(base + slot_ws[1]);
+        F.w_ww = reinterpret_cast<const long long*>(base + slot_ws[2]);
+        F.wscale = reinterpret_cast<const float*>(base + P.off_wscale);
+        F.self_aa = reinterpret_cast<const double*>(base + P.off_self);
+        F.self_ww = reinterpret_cast<const double*>(base + P.off_self) + 1;
+        F.bin_width = cfg.bin_width;
+        F.c = P.c;
+        F.scale = P.scale;
+        F.weighted = weighted;
+        F.max_bin = reinterpret_cast<int32_t*>(base + P.off_maxbin);
+        F.H = reinterpret_cast<double*>(base + P.off_H);
+        F.tot = reinterpret_cast<double*>(base + P.off_tot);
+        F.d_axis = reinterpret_cast<double*>(base + P.off_d);
+    } else {
+        FinalizeFF& F = P.fin_ff;
+        F.kind = cfg.manager;
+        F.T = T;
+        F.nb = nb;
+        F.n_a = n_a;
+        F.n_w = n_w;
+        F.n_x = n_x_eff;
+        F.type_count = meta.as<int32_t>();
+        F.ff_to_type = meta.as<int32_t>(kNff * 4);
+        F.cnt_aa = cnt(0);
+        F.cnt_aw = cnt(1);
+        F.cnt_ww = cnt(2);
+        F.cnt_ax = cnt(3);
+        F.cnt_wx = cnt(4);
+        F.cnt_xx = cnt(5);
+        F.ds_aa = ds(0);
+        F.ds_aw = ds(1);
+        F.ds_ww = ds(2);
+        F.ds_ax = ds(3);
+        F.ds_wx = ds(4);
+        F.ds_xx = ds(5);
+        F.z_exv = cfg.z_exv;
+        F.bin_width = cfg.bin_width;
+        F.c = P.c;
+        F.scale = P.scale;
+        F.weighted = weighted;
+        F.max_bin = reinterpret_cast<int32_t*>(base + P.off_maxbin);
+        F.H = reinterpret_cast<double*>(base + P.off_H);
+        F.tot = reinterpret_cast<double*>(base + P.off_tot);
+        F.d_axis = reinterpret_cast<double*>(base + P.off_d);
+        F.d_axis_ax = grid ? reinterpret_cast<double*>(base + P.off_dax) : nullptr;
+        F.d_axis_xx = grid ? reinterpret_cast<double*>(base + P.off_dxx) : nullptr;
+    }
+
+    // row descriptors of the Debye transform
+    std::vector<RowDesc> rd(R);
+    if (mt) {
+        rd[0] = {0, kRowSAA, 0, 0};
+        rd[1] = {0, kRowSAW, 0, 0};
+        rd[2] = {0, kRowSWW, 0, 0};
+    } else {
+        int g_ax = grid ? 1 : 0, g_xx = grid ? 2 : 0;
+        for (int a = 0; a < T; ++a)
+            for (int b = 0; b < T; ++b) rd[a * T + b] = {0, kRowAA, type_ff[a], type_ff[b]};
+        for (int a = 0; a < T; ++a) rd[T * T + a] = {g_ax, kRowAX, type_ff[a], kExv};
+        rd[T * T + T] = {g_xx, kRowXX, kExv, kExv};
+        for (int a = 0; a < T; ++a) rd[T * T + T + 1 + a] = {0, kRowAW, type_ff[a], kWater};
+        rd[T * T + 2 * T + 1] = {g_ax, kRowWX, kExv, kWater};
+        rd[T * T + 2 * T + 2] = {0, kRowWW, kWater, kWater};
+    }
+    AUSAXS_CUDA(cudaMemcpy(base + P.off_rows, rd.data(), sizeof(RowDesc) * R, cudaMemcpyHostToDevice));
+    return P;
+}
+
+void Structure::enqueue_histogram(const ausaxs_hist_config& cfg) {
+    Plan& P = plan_for(cfg);
+    Ctx& C = *ctx;
+    cudaStream_t s = C.stream;
+    char* base = P.dev.as<char>();
+    AUSAXS_CUDA(cudaMemsetAsync(base + P.off_acc, 0, P.acc_bytes, s));
+    const bool mt = cfg.manager == AUSAXS_MANAGER_MT;
+    if (mt) {
+        weight_scale_launch(raw_a.as<float4>(), n_a, raw_w.as<float4>(), n_w, reinterpret_cast<float*>(base + P.off_wscale), s);
+        weight_square_sum_launch(raw_a.as<float4>(), n_a, reinterpret_cast<double*>(base + P.off_self), s);
+        weight_square_sum_launch(raw_w.as<float4>(), n_w, reinterpret_cast<double*>(base + P.off_self) + 1, s);
+        C.check_launch("weights");
+    }
+    if (P.total_tiles > 0) {
+        cudaEvent_t ev;
+        C.time_begin(0, &ev);
+        pairhist_launch(P.launch, P.tile, P.grid, P.smem, s);
+        C.check_launch("pairhist");
+        C.time_end(0, ev);
+    }
+    cudaEvent_t evf;
+    C.time_begin(1, &evf);
+    if (mt) mt_finalize_launch(P.fin_mt, s);
+    else ff_finalize_launch(P.fin_ff, s);
+    C.check_launch("finalize");
+    C.launches += 1;  // finalize is two kernels
+    C.time_end(1, evf);
+}
+
+void Structure::enqueue_debye(const ausaxs_hist_config& cfg, const double* q_dev, int nq, const ausaxs_debye_params& p,
+                              double* Iq_dev, double* prof_dev) {
+    Plan& P = plan;
+    if (cfg.manager == AUSAXS_MANAGER_FFEXPLICIT)
+        throw Error{AUSAXS_ERR_ARGUMENT, "the Debye transform of FFEXPLICIT histograms needs per-type excluded-volume tables, which this build does not carry"};
+    char* base = P.dev.as<char>();
+    DebyeArgs A{};
+    A.R = P.R;
+    A.nb = P.nb;
+    A.H = reinterpret_cast<const double*>(base + P.off_H);
+    A.axis0 = reinterpret_cast<const double*>(base + P.off_d);
+    const bool grid = cfg.manager == AUSAXS_MANAGER_FFGRID;
+    A.axis1 = grid ? reinterpret_cast<const double*>(base + P.off_dax) : A.axis0;
+    A.axis2 = grid ? reinterpret_cast<const double*>(base + P.off_dxx) : A.axis0;
+    A.max_bin = reinterpret_cast<const int32_t*>(base + P.off_maxbin);
+    A.rows = reinterpret_cast<const RowDesc*>(base + P.off_rows);
+    A.overflow = reinterpret_cast<const unsigned long long*>(base + P.off_overflow);
+    A.exv_model = grid ? 1 : 0;
+    A.cw = p.cw;
+    A.cx = p.cx;
+    A.crho = p.crho;
+    A.dw_atomic = p.dw_atomic;
+    A.dw_exv = p.dw_exv;
+    A.grid_volume = p.grid_width * p.grid_width * p.grid_width;
+    A.q = q_dev;
+    A.nq = nq;
+    A.sinqd_tc = nullptr;
+    A.bound_tc = nullptr;
+    A.tolerance = p.tolerance > 0 ? p.tolerance : 1e-5;
+    A.fp64_columns = reinterpret_cast<int32_t*>(base + P.off_fp64cols);
+    A.Iq = Iq_dev;
+    A.profiles = prof_dev;
+    if (nq > 0) {
+        cudaEvent_t ev;
+        ctx->time_begin(2, &ev);
+        debye_fp64_launch(A, ctx->stream);
+        ctx->check_launch("debye");
+        ctx->time_end(2, ev);
+    }
+}
+
+void Structure::read_histogram(const ausaxs_hist_config& cfg, ausaxs_hist_result* out) {
+    Plan& P = plan;
+    Ctx& C = *ctx;
+    cudaStream_t s = C.stream;
+    char* base = P.dev.as<char>();
+    struct {
+        int32_t mb;
+        int32_t pad;
+        unsigned long long overflow;
+    } hdr;
+    AUSAXS_CUDA(cudaMemcpyAsync(&hdr.mb, base + P.off_maxbin, 4, cudaMemcpyDeviceToHost, s));
+    AUSAXS_CUDA(cudaMemcpyAsync(&hdr.overflow, base + P.off_overflow, 8, cudaMemcpyDeviceToHost, s));
+    AUSAXS_CUDA(cudaStreamSynchronize(s));
+    const int mb = hdr.mb;
+    const size_t nb = P.nb;
+    out->max_bin = mb;
+    out->pairs = P.pairs;
+    out->overflow_pairs = (int64_t)hdr.overflow;
+    const double* H = reinterpret_cast<const double*>(base + P.off_H);
+    auto d2h = [&](double* dst, const void* src, size_t n) {
+        if (dst && n) AUSAXS_CUDA(cudaMemcpyAsync(dst, src, n * 8, cudaMemcpyDeviceToHost, s));
+    };
+    if (cfg.manager == AUSAXS_MANAGER_MT) {
+        d2h(out->aa, H, mb);
+        d2h(out->aw, H + nb, mb);
+        d2h(out->ww, H + 2 * nb, mb);
+    } else {
+        double* eaa = reinterpret_cast<double*>(base + P.off_expand_aa);
+        double* eaw = reinterpret_cast<double*>(base + P.off_expand_aw);
+        ff_expand_launch(P.fin_ff, eaa, eaw, mb, s);
+        C.check_launch("expand");
+        d2h(out->aa, eaa, (size_t)kNff * kNff * mb);
+        d2h(out->aw, eaw, (size_t)kNff * mb);
+        d2h(out->ww, H + (size_t)(ff_rows(P.T) - 1) * nb, mb);
+        if (cfg.manager == AUSAXS_MANAGER_FFGRID) {
+            d2h(out->d_axis_ax, base + P.off_dax, mb);
+            d2h(out->d_axis_xx, base + P.off_dxx, mb);
+        }
+    }
+    d2h(out->tot, base + P.off_tot, mb);
+    d2h(out->d_axis, base + P.off_d, mb);
+    AUSAXS_CUDA(cudaStreamSynchronize(s));
+    if (hdr.overflow)
+        throw Error{AUSAXS_ERR_BIN_OVERFLOW, "pair distances beyond bin_count * bin_width; increase settings::axes::bin_count"};
+}
+
+void debye_of_host_histogram(Ctx& C, const ausaxs_hist_config& cfg, const ausaxs_hist_result& h, const double* q,
+                             int nq, const ausaxs_debye_params& p, double* Iq, double* profiles) {
+    const int mb = h.max_bin;
+    if (mb <= 0 || !h.d_axis || !h.aa || !h.aw || !h.ww) throw Error{AUSAXS_ERR_ARGUMENT, "incomplete histogram"};
+    if (cfg.manager == AUSAXS_MANAGER_FFEXPLICIT)
+        throw Error{AUSAXS_ERR_ARGUMENT, "the Debye transform of FFEXPLICIT histograms needs per-type excluded-volume tables, which this build does not carry"};
+    const bool mt = cfg.manager == AUSAXS_MANAGER_MT;
+    const bool grid = cfg.manager == AUSAXS_MANAGER_FFGRID;
+    if (grid && (!h.d_axis_ax || !h.d_axis_xx)) throw Error{AUSAXS_ERR_ARGUMENT, "grid histogram without ax/xx axes"};
+    std::vector<double> H;
+    std::vector<RowDesc> rd;
+    auto row = [&](const double* src, RowDesc d) {
+        H.insert(H.end(), src, src + mb);
+        rd.push_back(d);
+    };
+    if (mt) {
+        row(h.aa, {0, kRowSAA, 0, 0});
+        row(h.aw, {0, kRowSAW, 0, 0});
+        row(h.ww, {0, kRowSWW, 0, 0});
+    } else {
+        auto nonzero = [mb](const double* r) {
+            for (int b = 0; b < mb; ++b)
+                if (r[b] != 0) return true;
+            return false;
+        };
+        std::vector<int> types;
+        for (int f = 1; f < kNff; ++f) {
+            bool used = nonzero(h.aw + (size_t)f * mb) || nonzero(h.aa + (size_t)(f * kNff) * mb);
+            for (int g = 1; g < kNff && !used; ++g) used = nonzero(h.aa + (size_t)(f * kNff + g) * mb) || nonzero(h.aa + (size_t)(g * kNff + f) * mb);
+            if (used) types.push_back(f);
+        }
+        int g_ax = grid ? 1 : 0, g_xx = grid ? 2 : 0;
+        for (int a : types)
+            for (int b : types) row(h.aa + (size_t)(a * kNff + b) * mb, {0, kRowAA, a, b});
+        for (int a : types) row(h.aa + (size_t)(a * kNff + kExv) * mb, {g_ax, kRowAX, a, kExv});
+        row(h.aa, {g_xx, kRowXX, kExv, kExv});
+        for (int a : types) row(h.aw + (size_t)a * mb, {0, kRowAW, a, kWater});
+        row(h.aw, {g_ax, kRowWX, kExv, kWater});
+        row(h.ww, {0, kRowWW, kWater, kWater});
+    }
+    const int R = (int)rd.size();
+    if (R > 264) throw Error{AUSAXS_ERR_CAPACITY, "too many histogram rows"};
+    size_t off_H = 0, off_ax0 = align_up((size_t)R * mb * 8, 256);
+    size_t off_ax1 = off_ax0 + align_up((size_t)mb * 8, 256), off_ax2 = off_ax1 + align_up((size_t)mb * 8, 256);
+    size_t off_rows = off_ax2 + align_up((size_t)mb * 8, 256), off_mb = off_rows + align_up(sizeof(RowDesc) * R, 256);
+    size_t off_q = off_mb + 256, off_I = off_q + align_up((size_t)nq * 8, 256), off_P = off_I + align_up((size_t)nq * 8, 256);
+    size_t total = off_P + align_up((size_t)nq * 6 * 8, 256);
+    C.io.ensure(total);
+    char* base = C.io.as<char>();
+    cudaStream_t s = C.stream;
+    AUSAXS_CUDA(cudaMemcpyAsync(base + off_H, H.data(), H.size() * 8, cudaMemcpyHostToDevice, s));
+    AUSAXS_CUDA(cudaMemcpyAsync(base + off_ax0, h.d_axis, (size_t)mb * 8, cudaMemcpyHostToDevice, s));
+    if (grid) {
+        AUSAXS_CUDA(cudaMemcpyAsync(base + off_ax1, h.d_axis_ax, (size_t)mb * 8, cudaMemcpyHostToDevice, s));
+        AUSAXS_CUDA(cudaMemcpyAsync(base + off_ax2, h.d_axis_xx, (size_t)mb * 8, cudaMemcpyHostToDevice, s));
+    }
+    AUSAXS_CUDA(cudaMemcpyAsync(base + off_rows, rd.data(), sizeof(RowDesc) * R, cudaMemcpyHostToDevice, s));
+    int32_t mbv = mb;
+    AUSAXS_CUDA(cudaMemcpyAsync(base + off_mb, &mbv, 4, cudaMemcpyHostToDevice, s));
+    AUSAXS_CUDA(cudaMemcpyAsync(base + off_q, q, (size_t)nq * 8, cudaMemcpyHostToDevice, s));
+    DebyeArgs A{};
+    A.R = R;
+    A.nb = mb;
+    A.H = reinterpret_cast<const double*>(base + off_H);
+    A.axis0 = reinterpret_cast<const double*>(base + off_ax0);
+    A.axis1 = grid ? reinterpret_cast<const double*>(base + off_ax1) : A.axis0;
+    A.axis2 = grid ? reinterpret_cast<const double*>(base + off_ax2) : A.axis0;
+    A.max_bin = reinterpret_cast<const int32_t*>(base + off_mb);
+    A.rows = reinterpret_cast<const RowDesc*>(base + off_rows);
+    A.overflow = nullptr;
+    A.exv_model = grid ? 1 : 0;
+    A.cw = p.cw;
+    A.cx = p.cx;
+    A.crho = p.crho;
+    A.dw_atomic = p.dw_atomic;
+    A.dw_exv = p.dw_exv;
+    A.grid_volume = p.grid_width * p.grid_width * p.grid_width;
+    A.q = reinterpret_cast<const double*>(base + off_q);
+    A.nq = nq;
+    A.tolerance = p.tolerance > 0 ? p.tolerance : 1e-5;
+    A.Iq = reinterpret_cast<double*>(base + off_I);
+    A.profiles = profiles ? reinterpret_cast<double*>(base + off_P) : nullptr;
+    if (nq > 0) {
+        debye_fp64_launch(A, s);
+        C.check_launch("debye");
+        AUSAXS_CUDA(cudaMemcpyAsync(Iq, base + off_I, (size_t)nq * 8, cudaMemcpyDeviceToHost, s));
+        if (profiles) AUSAXS_CUDA(cudaMemcpyAsync(profiles, base + off_P, (size_t)nq * 6 * 8, cudaMemcpyDeviceToHost, s));
+    }
+    AUSAXS_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace ausaxs_b200

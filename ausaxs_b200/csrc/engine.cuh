@@ -1,0 +1,132 @@
+// Host-side engine: device-resident structures and the launch plans of the Debye hot path.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/ausaxs_b200.h"
+#include "debye.cuh"
+#include "finalize.cuh"
+#include "pairhist.cuh"
+#include "prep.cuh"
+
+namespace ausaxs_b200 {
+
+// Error raised inside the engine; the C ABI turns it into a status code plus last-error text.
+struct Error {
+    int code;
+    std::string msg;
+};
+
+#define AUSAXS_CUDA(call)                                                                              \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) throw ::ausaxs_b200::Error{AUSAXS_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)}; \
+    } while (0)
+
+// A growable device allocation (grows, never shrinks; freed with its owner).
+struct DevBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    void ensure(size_t bytes);
+    ~DevBuf();
+    template <typename T>
+    T* as(size_t byte_offset = 0) const { return reinterpret_cast<T*>(static_cast<char*>(p) + byte_offset); }
+};
+
+struct Ctx;
+
+// Launch plan of one structure under one histogram configuration: job table, accumulator and
+// output layout, kernel shapes.  Built once, then enqueued any number of times without
+// allocation or synchronisation (so it can be captured in a CUDA graph).
+struct Plan {
+    // key
+    int manager = 0, weighted = 0, bin_count = 0;
+    double bin_width = 0;
+    int n_a = -1, n_w = -1, n_x = -1, T = -1;
+    // shapes
+    int nb = 0, tile = 256, grid = 0, chunk = 1, smem_rows = 0;
+    size_t smem = 0;
+    int n_jobs = 0;
+    long long total_tiles = 0, pairs = 0;
+    int R = 0;
+    float inv_w = 0, c = 0, scale = 0;
+    // device layout
+    DevBuf dev;
+    size_t off_jobs = 0, off_acc = 0, acc_bytes = 0, off_counter = 0, off_overflow = 0, off_maxbin = 0, off_wscale = 0,
+           off_self = 0, off_fp64cols = 0, off_H = 0, off_tot = 0, off_d = 0, off_dax = 0, off_dxx = 0, off_rows = 0,
+           off_expand_aa = 0, off_expand_aw = 0;
+    FinalizeFF fin_ff{};
+    FinalizeMT fin_mt{};
+    PairLaunch launch{};
+    // tensor-core scratch
+    DevBuf tc;
+    int tc_nq = 0;
+};
+
+struct Structure {
+    Ctx* ctx = nullptr;
+    int ff_typed = 0;
+    int n_a = 0, n_w = 0, n_x = 0;
+    DevBuf raw_a, raw_w, raw_x, dense_a, meta;
+    int T = 0;
+    int type_ff[kNff] = {};
+    int type_count[kNff] = {};
+    int ff_to_type[kNff] = {};
+    float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    float dmax = 0;
+    Plan plan;
+
+    // copy in (host or device pointers), census, validation and dense-type conversion (one sync)
+    void load(const float* atoms, int n_atoms, const float* waters, int n_waters, const float* exv, int n_exv,
+              int ff_typed_, bool host);
+    const float4* atoms_for_pairs() const { return ff_typed ? dense_a.as<float4>() : raw_a.as<float4>(); }
+    Plan& plan_for(const ausaxs_hist_config& cfg);
+    void enqueue_histogram(const ausaxs_hist_config& cfg);
+    void enqueue_debye(const ausaxs_hist_config& cfg, const double* q_dev, int nq, const ausaxs_debye_params& p,
+                       double* Iq_dev, double* prof_dev);
+    // histogram in the reference's layouts into host buffers (synchronises)
+    void read_histogram(const ausaxs_hist_config& cfg, ausaxs_hist_result* out);
+};
+
+struct Ctx {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    long long launches = 0;
+    // optional per-kernel-class timing with CUDA events on the context's stream
+    // (class 0: pair histograms, 1: finalisation, 2: Debye transform)
+    bool timing = false;
+    struct Timed {
+        std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+        double ms = 0;
+        long long count = 0;
+    } timed[3];
+    void time_begin(int cls, cudaEvent_t* ev);
+    void time_end(int cls, cudaEvent_t ev);
+    void time_collect();
+    DevBuf stats;
+    PrepStats* h_stats = nullptr;  // pinned
+    std::unique_ptr<Structure> scratch;
+    DevBuf io;                     // q / I(q) / profiles of one-shot host calls
+    void check_launch(const char* what);
+};
+
+// CompositeDistanceHistogram*::debye_transform() of a histogram given in the reference's host
+// layouts (ausaxs_hist_result): compacts the rows of the form-factor types present, uploads them
+// and runs the transform (synchronises).
+void debye_of_host_histogram(Ctx& C, const ausaxs_hist_config& cfg, const ausaxs_hist_result& h, const double* q,
+                             int nq, const ausaxs_debye_params& p, double* Iq, double* profiles);
+
+}  // namespace ausaxs_b200
+
+struct ausaxs_gpu_ctx {
+    ausaxs_b200::Ctx impl;
+};
+
+struct ausaxs_gpu_structure {
+    ausaxs_b200::Structure impl;
+};

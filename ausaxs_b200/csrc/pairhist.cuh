@@ -1,0 +1,65 @@
+// Pair-distance histogram kernels (the O(N^2) stage of the Debye hot path).
+#pragma once
+#include "common.cuh"
+
+namespace ausaxs_b200 {
+
+// Row selection of a pair job, by the histogram shape the reference increments.
+enum RowMode : int32_t {
+    kRowSingle = 0,  // one row (ww, xx, wx, and every Simple/weighted job)
+    kRowPair = 1,    // [t_i][t_j] over dense atom types (increment_linear_index, CompactCoordinatesXYZFF.h:187-188)
+    kRowOuter = 2    // [t_i] of the outer point (aw by atom type, HistogramManagerMTFFAvg.cpp:111-117; ax)
+};
+
+// One pass of pair binning: outer set A (index i) against inner set B (index j); self jobs visit
+// only j > i (SimpleCalculator.h:117-141).  The host splits the pass into square tiles of
+// kTile x kTile pairs; tiles of all jobs of a launch are numbered consecutively.
+struct PairJob {
+    const float4* A;
+    const float4* B;
+    int32_t na, nb;
+    int32_t self;
+    int32_t row_mode;
+    int32_t types;        // dense type count T (kRowPair: rows = T*T, kRowOuter: rows = T)
+    int32_t row_lo, row_hi;  // rows of this job kept by this pass (row-group split when the full set
+                             // of rows does not fit on chip)
+    int32_t nbins;        // bins on chip / in the global accumulators
+    int32_t tiles_i, tiles_j;
+    int64_t tile_begin;   // first global tile id of the job
+    int64_t tile_count;
+    float inv_w;          // float(1 / bin_width), the reference's multiplier
+    float c;              // 1 / inv_w (float): bin pitch of the fixed-point offsets
+    float scale;          // 2^20 / c
+    unsigned long long* counts;  // [row_hi-row_lo][nbins] global pair counts (factor not applied)
+    unsigned long long* dsum;    // [nbins] biased fixed-point offset sums, or null
+    long long* wsum;             // [nbins] fixed-point weight-product sums, or null (weighted jobs)
+    float wscale;                // unused (the launch-wide scale lives in device memory)
+};
+
+struct PairLaunch {
+    const PairJob* jobs;
+    int32_t n_jobs;
+    int64_t total_tiles;
+    int32_t chunk;                  // tiles taken per grab from the global counter
+    int32_t smem_rows;              // rows of the on-chip count array
+    int32_t smem_bins;              // bins of the on-chip arrays (>= every job's nbins)
+    unsigned long long* tile_counter;
+    unsigned long long* overflow;   // pairs whose bin fell outside the job's nbins
+    int32_t weighted;
+    const float* wscale;            // device: 2^k with max|w_i w_j| * 2^k <= 2^30 (weighted launches)
+};
+
+// Bytes of dynamic shared memory a launch needs.
+inline size_t pairhist_smem_bytes(int rows, int bins, bool weighted, int tile) {
+    size_t pad = (size_t)bins + 1;
+    size_t b = (size_t)rows * pad * 4;          // u32 counts
+    b = (b + 15) & ~(size_t)15;
+    b += pad * 8;                               // u64 offset sums
+    if (weighted) b += pad * 8;                 // i64 weight sums
+    b += (size_t)tile * 16;                     // inner tile of points
+    return b + 64;
+}
+
+void pairhist_launch(const PairLaunch& L, int tile, int grid, size_t smem, cudaStream_t s);
+
+}  // namespace ausaxs_b200

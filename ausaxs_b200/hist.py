@@ -1,0 +1,337 @@
+"""Host-side mirror of the reference's histogram-manager and composite-histogram interfaces.
+
+Names, arguments and results follow the reference so that code written against
+``hist::IHistogramManager`` / ``ICompositeDistanceHistogram(Exv)`` reads the same:
+
+* ``HistogramManagerMT`` / ``HistogramManagerMTFFAvg`` / ``HistogramManagerMTFFExplicit`` /
+  ``HistogramManagerMTFFGrid`` -- ``calculate_all()`` as in
+  source/core/hist/histogram_manager/HistogramManager{MT,MTFFAvg,MTFFExplicit,MTFFGrid}.cpp;
+* ``CompositeDistanceHistogram`` (Simple, source/core/hist/intensity_calculator/CompositeDistanceHistogram.cpp)
+  and ``CompositeDistanceHistogramFFAvg`` / ``...FFGrid`` (CompositeDistanceHistogramFFAvgBase.cpp,
+  CompositeDistanceHistogramFFGrid.cpp) with ``apply_*_factor``, ``debye_transform`` and
+  ``get_profile_*``.
+
+All computation runs in the CUDA library through the C ABI (include/ausaxs_b200.h); this module
+only marshals arrays.  Settings the reference reads from globals (bin width/count, weighted bins,
+q range) are explicit arguments here.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _capi
+from ._capi import AusaxsError, DebyeParams, HistConfig, HistResult, check, dptr, fptr, load
+
+NFF = 15
+RHO_WATER = 0.334  # e/A^3, constants::charge::density::water (include/core/constants/Constants.h:114)
+
+
+def default_q_axis(qmin: float = 1e-4, qmax: float = 0.5) -> np.ndarray:
+    """constants::axes::q_axis = Axis(1e-4, 1, 200) restricted by sub_axis(qmin, qmax)
+    (include/core/constants/ConstantsAxes.h:14, source/core/utility/Axis.cpp:40-59)."""
+    lo, hi, bins = 1e-4, 1.0, 200
+    w = (hi - lo) / bins
+
+    def get_bin(v):
+        if v <= lo:
+            return 0
+        if v >= hi:
+            return bins
+        return int(np.floor((v + 1e-6 - lo) / w))
+
+    b0, b1 = get_bin(qmin), get_bin(qmax)
+    new_min, new_max = lo + b0 * w, lo + b1 * w
+    n = b1 - b0
+    ww = (new_max - new_min) / n
+    return np.array([new_min + i * ww for i in range(n)])
+
+
+def pack(xyz, fourth, as_int: bool) -> np.ndarray:
+    """float32 [n, 4] compact records {x, y, z, w | ff} (CompactCoordinatesXYZW.h:131-134)."""
+    xyz = np.asarray(xyz, dtype=np.float64).reshape(-1, 3)
+    out = np.empty((len(xyz), 4), np.float32)
+    out[:, :3] = xyz.astype(np.float32)
+    if as_int:
+        out[:, 3] = np.asarray(fourth, np.int32).reshape(-1).view(np.float32)
+    else:
+        out[:, 3] = np.asarray(fourth, np.float64).reshape(-1).astype(np.float32)
+    return np.ascontiguousarray(out)
+
+
+@dataclass
+class Molecule:
+    """The inputs of the hot path a data::Molecule provides: atoms with form-factor type and
+    weight, hydration waters, optional grid excluded-volume dummies, and the molecular volume
+    used for the average excluded-volume charge (Molecule::get_volume_grid)."""
+
+    atoms: np.ndarray                       # [n, 3] coordinates
+    ff_types: Optional[np.ndarray] = None   # [n] form_factor_t
+    weights: Optional[np.ndarray] = None    # [n] effective charges
+    waters: Optional[np.ndarray] = None     # [m, 3]
+    water_weights: Optional[np.ndarray] = None
+    exv: Optional[np.ndarray] = None        # [k, 3] grid dummies (FFGrid)
+    volume: float = 0.0
+
+    def size_atom(self) -> int:
+        return len(self.atoms)
+
+    def size_water(self) -> int:
+        return 0 if self.waters is None else len(self.waters)
+
+    def get_volume_grid(self) -> float:
+        return float(self.volume)
+
+    def compact_ff(self):
+        a = pack(self.atoms, self.ff_types, True)
+        w = pack(self.waters if self.waters is not None else np.zeros((0, 3)), np.ones(self.size_water(), np.int32), True)
+        x = pack(self.exv if self.exv is not None else np.zeros((0, 3)), np.zeros(0 if self.exv is None else len(self.exv), np.int32), True)
+        return a, w, x
+
+    def compact_w(self):
+        a = pack(self.atoms, self.weights, False)
+        ww = self.water_weights if self.water_weights is not None else np.zeros(self.size_water())
+        w = pack(self.waters if self.waters is not None else np.zeros((0, 3)), ww, False)
+        return a, w
+
+
+class _Composite:
+    """Common part of the composite histograms returned by the managers."""
+
+    kind = 0
+
+    def __init__(self, cfg: HistConfig, res: dict, ctx):
+        self._cfg = cfg
+        self._r = res
+        self._ctx = ctx
+        self.max_bin = int(res["max_bin"])
+        self.pairs = int(res["pairs"])
+        self.free = dict(cw=1.0, cx=1.0, crho=1.0, dw_atomic=0.0, dw_exv=0.0)
+        self.grid_width = 1.0
+
+    # DistanceHistogram interface
+    def get_d_axis(self) -> np.ndarray:
+        return self._r["d_axis"]
+
+    def get_counts(self) -> np.ndarray:
+        return self._r["tot"]
+
+    def apply_water_scaling_factor(self, k: float):
+        self.free["cw"] = float(k)
+
+    def _result(self) -> HistResult:
+        r = HistResult()
+        r.max_bin = self.max_bin
+        self._keep = {k: np.ascontiguousarray(v) for k, v in self._r.items() if isinstance(v, np.ndarray)}
+        for name in ("aa", "aw", "ww", "tot", "d_axis", "d_axis_ax", "d_axis_xx"):
+            setattr(r, name, dptr(self._keep.get(name)))
+        return r
+
+    def _transform(self, q, precision: int = 1):
+        q = default_q_axis() if q is None else np.ascontiguousarray(q, np.float64)
+        p = DebyeParams(self.free["cw"], self.free["cx"], self.free["crho"], self.free["dw_atomic"],
+                        self.free["dw_exv"], self.grid_width, precision, 1e-5)
+        I = np.zeros(len(q))
+        prof = np.zeros(6 * len(q))
+        r = self._result()
+        check(load().ausaxs_gpu_debye(self._ctx.h, C.byref(self._cfg), C.byref(r), dptr(q), len(q), C.byref(p),
+                                      dptr(I), dptr(prof)))
+        return q, I, prof.reshape(6, len(q))
+
+    def debye_transform(self, q: Optional[Sequence[float]] = None):
+        """I(q) at q (default: the reference's default q axis within [qmin, qmax])."""
+        q, I, _ = self._transform(q)
+        return q, I
+
+    def profiles(self, q=None) -> np.ndarray:
+        """[6][nq] partial profiles {aa, ax, aw, xx, wx, ww}."""
+        return self._transform(q)[2]
+
+    def get_profile_aa(self, q=None):
+        return self.profiles(q)[0]
+
+    def get_profile_aw(self, q=None):
+        return self.profiles(q)[2]
+
+    def get_profile_ww(self, q=None):
+        return self.profiles(q)[5]
+
+
+class CompositeDistanceHistogram(_Composite):
+    """Simple (weights) composite histogram: aa, aw, ww weighted counts."""
+
+    def get_aa_counts(self):
+        return self._r["aa"]
+
+    def get_aw_counts(self):
+        return self._r["aw"]
+
+    def get_ww_counts(self):
+        return self._r["ww"]
+
+
+class CompositeDistanceHistogramFFAvg(_Composite):
+    def get_raw_aa_counts_by_ff(self):
+        return self._r["aa"]
+
+    def get_raw_aw_counts_by_ff(self):
+        return self._r["aw"]
+
+    def get_raw_ww_counts_by_ff(self):
+        return self._r["ww"]
+
+    def apply_excluded_volume_scaling_factor(self, k: float):
+        self.free["cx"] = float(k)
+
+    def apply_solvent_density_scaling_factor(self, k: float):
+        self.free["crho"] = float(k)
+
+    def apply_atomic_debye_waller_factor(self, s: float):
+        self.free["dw_atomic"] = float(s)
+
+    def apply_exv_debye_waller_factor(self, s: float):
+        self.free["dw_exv"] = float(s)
+
+    def get_profile_ax(self, q=None):
+        return self.profiles(q)[1]
+
+    def get_profile_xx(self, q=None):
+        return self.profiles(q)[3]
+
+    def get_profile_wx(self, q=None):
+        return self.profiles(q)[4]
+
+
+class CompositeDistanceHistogramFFExplicit(CompositeDistanceHistogramFFAvg):
+    pass
+
+
+class CompositeDistanceHistogramFFGrid(CompositeDistanceHistogramFFAvg):
+    def get_d_axis_ax(self):
+        return self._r["d_axis_ax"]
+
+    def get_d_axis_xx(self):
+        return self._r["d_axis_xx"]
+
+
+class _Manager:
+    manager = 0
+    composite = _Composite
+
+    def __init__(self, protein: Molecule, weighted_bins: bool = True, bin_width: float = 0.25, bin_count: int = 8000,
+                 ctx: Optional[_capi.Context] = None):
+        self.protein = protein
+        self.weighted_bins = weighted_bins
+        self.bin_width = bin_width
+        self.bin_count = bin_count
+        self.ctx = ctx or _capi.default_context()
+
+    def config(self) -> HistConfig:
+        z = 0.0
+        if self.manager == _capi.MANAGER_FFAVG and self.protein.size_atom():
+            z = self.protein.get_volume_grid() * RHO_WATER / self.protein.size_atom()
+        return HistConfig(self.manager, int(self.weighted_bins), float(self.bin_width), int(self.bin_count), z)
+
+    def _inputs(self):
+        raise NotImplementedError
+
+    def calculate_all(self):
+        cfg = self.config()
+        a, w, x = self._inputs()
+        nb = self.bin_count
+        ff = self.manager != _capi.MANAGER_MT
+        bufs = {
+            "aa": np.zeros(NFF * NFF * nb if ff else nb),
+            "aw": np.zeros(NFF * nb if ff else nb),
+            "ww": np.zeros(nb),
+            "tot": np.zeros(nb),
+            "d_axis": np.zeros(nb),
+            "d_axis_ax": np.zeros(nb),
+            "d_axis_xx": np.zeros(nb),
+        }
+        r = HistResult()
+        for k, v in bufs.items():
+            setattr(r, k, dptr(v))
+        check(load().ausaxs_gpu_histogram(self.ctx.h, C.byref(cfg), fptr(a), len(a), fptr(w), len(w), fptr(x),
+                                          0 if x is None else len(x), C.byref(r)))
+        m = r.max_bin
+        res = {"max_bin": m, "pairs": r.pairs}
+        if ff:
+            res["aa"] = bufs["aa"][: NFF * NFF * m].reshape(NFF, NFF, m).copy()
+            res["aw"] = bufs["aw"][: NFF * m].reshape(NFF, m).copy()
+        else:
+            res["aa"] = bufs["aa"][:m].copy()
+            res["aw"] = bufs["aw"][:m].copy()
+        for k in ("ww", "tot", "d_axis"):
+            res[k] = bufs[k][:m].copy()
+        if self.manager == _capi.MANAGER_FFGRID:
+            res["d_axis_ax"] = bufs["d_axis_ax"][:m].copy()
+            res["d_axis_xx"] = bufs["d_axis_xx"][:m].copy()
+        return self.composite(cfg, res, self.ctx)
+
+    def calculate(self):
+        return self.calculate_all()
+
+
+class HistogramManagerMT(_Manager):
+    """Weights (Simple excluded volume); HistogramManagerMT.cpp:23-75."""
+
+    manager = _capi.MANAGER_MT
+    composite = CompositeDistanceHistogram
+
+    def _inputs(self):
+        a, w = self.protein.compact_w()
+        return a, w, None
+
+
+class HistogramManagerMTFFAvg(_Manager):
+    """Form factors with the average excluded volume; HistogramManagerMTFFAvg.cpp:194-372."""
+
+    manager = _capi.MANAGER_FFAVG
+    composite = CompositeDistanceHistogramFFAvg
+
+    def _inputs(self):
+        a, w, _ = self.protein.compact_ff()
+        return a, w, None
+
+
+class HistogramManagerMTFFExplicit(_Manager):
+    """Form factors, no excluded-volume rows; HistogramManagerMTFFExplicit.cpp:216-437."""
+
+    manager = _capi.MANAGER_FFEXPLICIT
+    composite = CompositeDistanceHistogramFFExplicit
+
+    def _inputs(self):
+        a, w, _ = self.protein.compact_ff()
+        return a, w, None
+
+
+class HistogramManagerMTFFGrid(_Manager):
+    """Form factors with grid excluded-volume dummies; HistogramManagerMTFFGrid.cpp:43-234.
+    The dummies (RawGridExv::create in the reference) come from Molecule.exv."""
+
+    manager = _capi.MANAGER_FFGRID
+    composite = CompositeDistanceHistogramFFGrid
+
+    def __init__(self, protein: Molecule, bin_width: float = 0.25, bin_count: int = 8000, ctx=None):
+        super().__init__(protein, True, bin_width, bin_count, ctx)
+
+    def _inputs(self):
+        return self.protein.compact_ff()
+
+
+def profile(manager: _Manager, q, cw=1.0, cx=1.0, crho=1.0, dw_atomic=0.0, dw_exv=0.0, grid_width=1.0,
+            precision: int = 1, with_profiles: bool = False):
+    """Coordinates -> I(q) in one call (Molecule::get_histogram()->debye_transform()): only I(q) leaves the device."""
+    cfg = manager.config()
+    a, w, x = manager._inputs()
+    q = np.ascontiguousarray(q, np.float64)
+    I = np.zeros(len(q))
+    prof = np.zeros(6 * len(q)) if with_profiles else None
+    p = DebyeParams(cw, cx, crho, dw_atomic, dw_exv, grid_width, precision, 1e-5)
+    check(load().ausaxs_gpu_profile(manager.ctx.h, C.byref(cfg), fptr(a), len(a), fptr(w), len(w), fptr(x),
+                                    0 if x is None else len(x), dptr(q), len(q), C.byref(p), dptr(I), dptr(prof)))
+    return (I, prof.reshape(6, len(q))) if with_profiles else I

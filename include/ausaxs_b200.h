@@ -1,0 +1,196 @@
+/*
+ * ausaxs_b200 -- C ABI of the B200 (sm_100a) Debye hot path.
+ *
+ * The two stages of AUSAXS's hot path sit behind these entry points:
+ *
+ *   1. pair-distance histograms, i.e. what
+ *        hist::IHistogramManager::calculate_all()
+ *      returns (include/core/hist/histogram_manager/IHistogramManager.h:16-29) for the
+ *      managers HistogramManagerMT, HistogramManagerMTFFAvg, HistogramManagerMTFFExplicit and
+ *      HistogramManagerMTFFGrid (source/core/hist/histogram_manager/*.cpp);
+ *   2. the Debye transform, i.e.
+ *        ICompositeDistanceHistogram::debye_transform() and get_profile_*()
+ *      (include/core/hist/intensity_calculator/ICompositeDistanceHistogram.h:24-71,
+ *       ICompositeDistanceHistogramExv.h:12-107), evaluated at caller-given q.
+ *
+ * Conventions (all entry points):
+ *   - every function returns an int status: AUSAXS_OK (0) or one of the AUSAXS_ERR_* codes; the
+ *     message of the last failure on the calling thread is returned by ausaxs_gpu_last_error().
+ *     This mirrors the reference's C API, where exceptions become a non-zero *status plus a
+ *     last-error string (include/api/api/api_helper.h:15-45).  No exception crosses this ABI.
+ *   - point arrays are the reference's compact 16-byte records, n x {float x, y, z; w | ff}
+ *     (include/core/hist/detail/data/CompactCoordinatesXYZW.h:131-134 for weights,
+ *     CompactCoordinatesXYZFF.h for the int32 form-factor type, form_factor_t numbering
+ *     include/core/form_factor/FormFactorType.h:14-37).  A caller holding
+ *     hist::detail::CompactCoordinates can pass get_data().data() directly.
+ *   - ausaxs_gpu_histogram / _debye / _profile take host pointers and copy inside; the
+ *     ausaxs_gpu_structure_* entry points work on device-resident structures.
+ *   - output buffers are always caller-allocated.
+ *   - a context is not thread-safe; use one context per host thread.
+ */
+#ifndef AUSAXS_B200_H
+#define AUSAXS_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define AUSAXS_API __attribute__((visibility("default")))
+#else
+#define AUSAXS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    AUSAXS_OK = 0,
+    AUSAXS_ERR_ARGUMENT = 1,     /* invalid argument (null pointer, negative size, ...)           */
+    AUSAXS_ERR_CUDA = 2,         /* a CUDA runtime call failed                                     */
+    AUSAXS_ERR_BIN_OVERFLOW = 3, /* a pair distance fell outside bin_count bins (the reference's   */
+                                 /* HistogramSettings.cpp:51-61 only warns; here it is an error)    */
+    AUSAXS_ERR_FORM_FACTOR = 4,  /* a form-factor type outside [0, 15) (CompactCoordinatesFF.h:24) */
+    AUSAXS_ERR_CAPACITY = 5,     /* request exceeds a capacity (memory budget, slots, ...)          */
+    AUSAXS_ERR_TIMEOUT = 6,      /* a bounded wait ran out                                          */
+    AUSAXS_ERR_NOT_FOUND = 7     /* unknown handle / request id                                     */
+};
+
+/* settings::hist::HistogramManagerChoice (include/core/settings/HistogramSettings.h) */
+enum {
+    AUSAXS_MANAGER_MT = 1,         /* HistogramManagerMT: weights, Simple excluded volume       */
+    AUSAXS_MANAGER_FFAVG = 2,      /* HistogramManagerMTFFAvg: form factors, average exv         */
+    AUSAXS_MANAGER_FFEXPLICIT = 3, /* HistogramManagerMTFFExplicit: form factors, no exv rows    */
+    AUSAXS_MANAGER_FFGRID = 4      /* HistogramManagerMTFFGrid: form factors, grid exv dummies   */
+};
+
+typedef struct ausaxs_gpu_ctx ausaxs_gpu_ctx;
+
+/* Create a context on a CUDA device (its own stream and device workspace). */
+AUSAXS_API int ausaxs_gpu_ctx_create(int device, ausaxs_gpu_ctx** out);
+AUSAXS_API int ausaxs_gpu_ctx_destroy(ausaxs_gpu_ctx* ctx);
+/* Use an existing CUDA stream (cudaStream_t passed as void*) for all later work; NULL = own stream. */
+AUSAXS_API int ausaxs_gpu_ctx_set_stream(ausaxs_gpu_ctx* ctx, void* stream);
+/* Number of kernels this context has launched (instrumentation for benchmarks). */
+AUSAXS_API int64_t ausaxs_gpu_ctx_launch_count(const ausaxs_gpu_ctx* ctx);
+AUSAXS_API const char* ausaxs_gpu_last_error(void);
+/*
+ * Optional kernel timing (instrumentation, no counterpart in the reference): with timing enabled,
+ * every later launch of a kernel class is bracketed by CUDA events on the context's stream.
+ * ausaxs_gpu_ctx_kernel_time synchronises the stream and returns the accumulated device time (ms)
+ * and number of launches of one class: 0 = pair histograms, 1 = finalisation, 2 = Debye transform.
+ */
+AUSAXS_API int ausaxs_gpu_ctx_enable_timing(ausaxs_gpu_ctx* ctx, int32_t enable);
+AUSAXS_API int ausaxs_gpu_ctx_kernel_time(ausaxs_gpu_ctx* ctx, int32_t kernel_class, double* ms, int64_t* launches);
+
+/*
+ * Histogram configuration: the global settings the reference reads during calculate_all().
+ *   bin_width, bin_count : settings::axes::bin_width / bin_count (HistogramSettings.cpp:38-80);
+ *                          the pair bin is round(float(d) * float(1/bin_width))
+ *                          (include/core/hist/detail/data/WidthControllers.h:10-26)
+ *   weighted_bins        : settings::hist::weighted_bins (mean distance per bin as d-axis)
+ *   z_exv                : FFAvg only, V_grid * rho_w / N_atoms (HistogramManagerMTFFAvg.cpp:351-364)
+ */
+typedef struct {
+    int32_t manager;
+    int32_t weighted_bins;
+    double bin_width;
+    int32_t bin_count;
+    double z_exv;
+} ausaxs_hist_config;
+
+/*
+ * Histogram result, in the reference's layouts, truncated to max_bin bins
+ * (HistogramManagerMT.cpp:47-58): every row below is written with stride max_bin.
+ * All pointers are caller-allocated host buffers with room for bin_count bins per row.
+ *   MT    : aa, aw, ww, tot = weighted counts (get_aa_counts/get_aw_counts/get_ww_counts/get_counts)
+ *   FF*   : aa = [15][15] rows (get_raw_aa_counts_by_ff), aw = [15] rows (get_raw_aw_counts_by_ff),
+ *           ww (get_raw_ww_counts_by_ff), tot = p_tot counts
+ *   d_axis: DistanceHistogram::get_d_axis() (weighted bin centres, bin 0 pinned to 0)
+ *   FFGRID: d_axis_ax / d_axis_xx = CompositeDistanceHistogramFFGrid::get_d_axis_ax/_xx
+ */
+typedef struct {
+    int32_t max_bin;
+    int64_t pairs;          /* pair evaluations performed                         */
+    int64_t overflow_pairs; /* pairs whose bin fell outside bin_count (then ERR 3) */
+    double* aa;
+    double* aw;
+    double* ww;
+    double* tot;
+    double* d_axis;
+    double* d_axis_ax;
+    double* d_axis_xx;
+} ausaxs_hist_result;
+
+/*
+ * IHistogramManager::calculate_all() for one structure (host buffers).
+ * atoms: n_atoms records, waters: n_waters records, exv: n_exv excluded-volume dummies (FFGRID only;
+ * RawGridExv::create supplies these in the reference, source/core/grid/exv/RawGridExv.cpp:10-59).
+ * FF managers read the int32 form-factor type from the 4th word, MT reads the float weight.
+ */
+AUSAXS_API int ausaxs_gpu_histogram(ausaxs_gpu_ctx* ctx, const ausaxs_hist_config* cfg, const float* atoms, int32_t n_atoms,
+                         const float* waters, int32_t n_waters, const float* exv, int32_t n_exv,
+                         ausaxs_hist_result* out);
+
+/*
+ * Free parameters of the composite histograms
+ * (CompositeDistanceHistogramFFAvgBase.cpp:216-238: cw = water scaling, cx = excluded-volume
+ * scaling, crho = solvent density scaling, Debye-Waller sigmas for atoms and exv).
+ * grid_width: settings::grid::exv::width, the FFGRID dummy volume is grid_width^3.
+ * precision: 0 = split-BF16 tensor-core contraction with FP64 recomputation of every q whose
+ *            estimated error exceeds tolerance; 1 = FP64 on CUDA cores for every q.
+ */
+typedef struct {
+    double cw, cx, crho, dw_atomic, dw_exv;
+    double grid_width;
+    int32_t precision;
+    double tolerance; /* relative I(q) error target for precision 0 (default 1e-5 when <= 0) */
+} ausaxs_debye_params;
+
+/*
+ * debye_transform() of a histogram previously returned by ausaxs_gpu_histogram (host buffers),
+ * evaluated at the caller's q values (the generalised-q form of
+ * CompositeDistanceHistogramFFAvgBase::debye_transform, :57-76).
+ * Iq: n_q values; profiles (optional, 6 x n_q): {aa, ax, aw, xx, wx, ww} as get_profile_*().
+ */
+AUSAXS_API int ausaxs_gpu_debye(ausaxs_gpu_ctx* ctx, const ausaxs_hist_config* cfg, const ausaxs_hist_result* hist,
+                     const double* q, int32_t n_q, const ausaxs_debye_params* params, double* Iq, double* profiles);
+
+/*
+ * Coordinates -> I(q) in one call (Molecule::get_histogram()->debye_transform(), host buffers):
+ * histogram and transform stay on the device; only I(q) (and optional profiles) come back.
+ */
+AUSAXS_API int ausaxs_gpu_profile(ausaxs_gpu_ctx* ctx, const ausaxs_hist_config* cfg, const float* atoms, int32_t n_atoms,
+                       const float* waters, int32_t n_waters, const float* exv, int32_t n_exv, const double* q,
+                       int32_t n_q, const ausaxs_debye_params* params, double* Iq, double* profiles);
+
+/*
+ * Device-resident structures.  A structure keeps its points in device memory; its first profile
+ * under a configuration builds a launch plan (allocation, one synchronisation), every later
+ * profile is a fixed sequence of kernels on the context's stream with no allocation, copy or
+ * synchronisation (so it can be captured in a CUDA graph).  This is the analogue of the
+ * reference's Molecule owning its histogram manager (source/core/data/Molecule.cpp:67-75, 236).
+ *
+ * ausaxs_gpu_structure_create: points as in ausaxs_gpu_histogram; host_pointers != 0 means the
+ *   arrays are host memory, otherwise device memory of the context's device.  ff_typed != 0: the
+ *   4th word is the int32 form-factor type (FF managers), else the float weight (MT).  One
+ *   synchronisation (point census: bounding box, type counts, validation).
+ * ausaxs_gpu_structure_profile: q, Iq and profiles are device pointers.  A histogram that lost
+ *   pairs to bin overflow yields NaN in Iq.
+ * ausaxs_gpu_structure_histogram: host result as ausaxs_gpu_histogram (synchronises).
+ */
+typedef struct ausaxs_gpu_structure ausaxs_gpu_structure;
+
+AUSAXS_API int ausaxs_gpu_structure_create(ausaxs_gpu_ctx* ctx, int32_t ff_typed, const float* atoms, int32_t n_atoms,
+                                const float* waters, int32_t n_waters, const float* exv, int32_t n_exv,
+                                int32_t host_pointers, ausaxs_gpu_structure** out);
+AUSAXS_API int ausaxs_gpu_structure_destroy(ausaxs_gpu_structure* s);
+AUSAXS_API int ausaxs_gpu_structure_profile(ausaxs_gpu_ctx* ctx, ausaxs_gpu_structure* s, const ausaxs_hist_config* cfg,
+                                 const double* q, int32_t n_q, const ausaxs_debye_params* params, double* Iq,
+                                 double* profiles);
+AUSAXS_API int ausaxs_gpu_structure_histogram(ausaxs_gpu_ctx* ctx, ausaxs_gpu_structure* s, const ausaxs_hist_config* cfg,
+                                   ausaxs_hist_result* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AUSAXS_B200_H */

@@ -38,12 +38,19 @@ typedef struct {
  * Pair evaluation.
  * SIMD evaluators (CompactCoordinatesXYZW.h:382-423, :491-535, :602-655):
  *   d2 = (dx*dx + dy*dy) + dz*dz, d = sqrt(d2), bin = cvt_rn(d * inv_w)
- * with each operation rounded separately and ties to even.
- * Scalar tail evaluator (CompactCoordinatesXYZW.h:303-307): same distance,
- * bin = std::round(inv_w * d) (ties away from zero).
+ * with each operation rounded separately and ties to even (the squares are
+ * formed before the lane shuffles, so no contraction is possible).
+ * Scalar tail evaluator (CompactCoordinatesXYZW.h:303-307, IntrinsicHelpers.h:9-14):
+ * dx*dx + dy*dy + dz*dz under the reference's release flags
+ * (-O3 -ffast-math -march=x86-64-v3, cmake/setup_compile_commands.cmake:100-103)
+ * is contracted by GCC to fma(dz, dz, fma(dx, dx, dy*dy)) -- established by
+ * compiling that helper with those flags and comparing all candidate
+ * contractions on 1e6 random pairs -- and bin = std::round(inv_w * d), ties
+ * away from zero.
  * ------------------------------------------------------------------------- */
-static inline float pair_distance(const opoint* a, const opoint* b) {
+static inline float pair_distance(const opoint* a, const opoint* b, int tail) {
     float dx = a->x - b->x, dy = a->y - b->y, dz = a->z - b->z;
+    if (tail) return sqrtf(fmaf(dz, dz, fmaf(dx, dx, dy * dy)));
     float sx = dx * dx, sy = dy * dy, sz = dz * dz;
     return sqrtf((sx + sy) + sz);
 }
@@ -87,8 +94,9 @@ static void pair_job(const opoint* A, int32_t na, const opoint* B, int32_t nb, i
         int32_t j0 = self ? i + 1 : 0;
         int32_t ts = tail_start(j0, nb);
         for (int32_t j = j0; j < nb; ++j) {
-            float d = pair_distance(&A[i], &B[j]);
-            int32_t bin = pair_bin(d, inv_w, j >= ts);
+            const int tail = j >= ts;
+            float d = pair_distance(&A[i], &B[j], tail);
+            int32_t bin = pair_bin(d, inv_w, tail);
             if (!(bin >= 0 && bin < nbins)) {
                 o->overflow++;
                 continue;

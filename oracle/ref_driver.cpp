@@ -107,6 +107,7 @@ int ref_init(int threads) {
         settings::general::threads = threads > 0 ? threads : 1;
         settings::flags::init_histogram_manager = false;
         settings::general::verbose = false;
+        settings::general::warnings = false;
     });
 }
 

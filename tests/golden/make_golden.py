@@ -1,0 +1,97 @@
+"""Regenerate the golden fixtures from the reference compiled from its own sources.
+
+Run (needs oracle/_ref/libausaxs_ref.so, i.e. a machine where the reference sources were
+available to ``make -C oracle``):
+
+    python tests/golden/make_golden.py
+
+Each fixture stores the inputs (coordinates as float64, form-factor types, weights, waters,
+exv dummies, volume, settings) and the reference's outputs: the raw histograms of
+calculate_all(), the distance axes, and debye_transform() with its partial profiles on the
+reference's default q axis.  Cases:
+
+* ``cube_*``  : the reference's SimpleCube known-answer structure (tests/feature/hist/hist_test_helper.h:87-162)
+                for every manager;
+* ``random_*``: seeded random molecules (ragged sizes, all four elements, non-default bin width).
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import py as O  # noqa: E402
+
+CUBE = np.array([[-1, -1, -1], [-1, 1, -1], [1, -1, -1], [1, 1, -1], [-1, -1, 1], [-1, 1, 1], [1, -1, 1], [1, 1, 1]], float)
+
+
+def run_case(name, atoms, ff, w, waters, ww, exv, volume, bin_width, manager, cw=1.0, cx=1.0, crho=1.0, dwa=0.0, dwx=0.0,
+             simple_exv=False):
+    O.ref_set_axes(bin_width, 8000, 1e-4, 0.5)
+    O.ref_set_simple_exv(simple_exv)
+    m = O.RefMolecule(atoms, w, ff, waters, ww, volume=volume)
+    m.set_manager(manager, exv_xyz=exv if manager == "ffgrid" else None)
+    h = m.calculate()
+    out = dict(atoms=atoms, ff=ff.astype(np.int32), w=w, waters=waters, ww=ww, exv=exv, volume=volume,
+               bin_width=bin_width, manager=manager, params=np.array([cw, cx, crho, dwa, dwx]),
+               simple_exv=simple_exv)
+    tot, d = h.total()
+    out["tot"], out["d_axis"] = tot, d
+    if manager in ("mt", "single"):
+        out["aa"], out["aw"], out["ww_h"] = h.simple()
+    else:
+        out["aa"], out["aw"], out["ww_h"] = h.ff()
+        if manager == "ffgrid":
+            ax, xx = h.grid_axes()
+            out["d_axis_ax"], out["d_axis_xx"] = ax[: len(d)], xx[: len(d)]
+    if manager != "ffexplicit":
+        q, I, prof, _ = h.debye(cw, cx, crho, dwa, dwx)
+        out["q"], out["Iq"], out["profiles"] = q, I, prof
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, "bins", len(d), "I" if "Iq" in out else "")
+
+
+def main():
+    O.ref()
+    # SimpleCube: 8 corners + centre as atoms (carbon), 8 corner waters
+    atoms = np.vstack([CUBE, [[0, 0, 0]]])
+    ff = np.full(9, 3)
+    w = np.ones(9)
+    waters = CUBE.copy()
+    ww = np.ones(8)
+    for mgr in ("mt", "ffavg", "ffexplicit"):
+        run_case(f"cube_{mgr}", atoms, ff, w, waters, ww, np.zeros((0, 3)), 100.0, 0.25, mgr)
+    run_case("cube_ffgrid", atoms, ff, w, waters, ww, CUBE * 2.0, 100.0, 0.25, "ffgrid")
+
+    rng = np.random.default_rng(20240601)
+    elements = np.array([3, 7, 11, 12])
+    charge = {3: 5.997198, 7: 6.996361, 11: 7.999706, 12: 15.989624}
+    for k, (na, nw, nx, bw) in enumerate([(257, 63, 0, 0.25), (401, 97, 0, 0.1), (130, 0, 0, 0.25),
+                                          (333, 71, 250, 0.1)]):
+        xyz = rng.normal(0, 7, (na, 3))
+        f = rng.choice(elements, na, p=[0.63, 0.17, 0.19, 0.01])
+        wt = np.array([charge[t] for t in f]) * rng.uniform(0.8, 1.2, na)
+        wat = rng.normal(0, 9, (nw, 3))
+        wwt = np.full(nw, 8.999659)
+        exv = np.round(rng.uniform(-9, 9, (nx, 3)))
+        vol = 40.0 * na
+        run_case(f"random{k}_mt", xyz, f, wt, wat, wwt, exv, vol, bw, "mt", cw=1.3)
+        run_case(f"random{k}_ffavg", xyz, f, wt, wat, wwt, exv, vol, bw, "ffavg", cw=1.1, cx=0.97, crho=1.02,
+                 dwa=0.4, dwx=0.2)
+        run_case(f"random{k}_ffexplicit", xyz, f, wt, wat, wwt, exv, vol, bw, "ffexplicit")
+        if nx:
+            run_case(f"random{k}_ffgrid", xyz, f, wt, wat, wwt, exv, vol, bw, "ffgrid", cw=0.9, cx=1.05)
+    # Simple excluded volume enabled (weights shifted by -rho_w V / N, SimpleExvModel.cpp:23-28)
+    xyz = rng.normal(0, 6, (120, 3))
+    f = rng.choice(elements, 120)
+    wt = np.array([charge[t] for t in f])
+    run_case("random_simple_exv_mt", xyz, f, wt, np.zeros((0, 3)), np.zeros(0), np.zeros((0, 3)), 900.0, 0.25, "mt",
+             simple_exv=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,44 @@
+"""Shared test helpers: golden fixtures and oracle runs."""
+import glob
+import os
+
+import numpy as np
+
+from oracle import py as O
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+RHO_W = 0.334
+
+
+def golden_cases(prefix=""):
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, prefix + "*.npz")))
+
+
+def load_golden(name):
+    with np.load(os.path.join(GOLDEN, name + ".npz"), allow_pickle=False) as z:
+        return {k: z[k] for k in z.files}
+
+
+def simple_exv_weights(w, volume, n_atoms):
+    """CompactCoordinatesTemplate::implicit_excluded_volume: w += -(rho_w * V / N), in double, stored as float."""
+    return (np.asarray(w, np.float32).astype(np.float64) - RHO_W * volume / n_atoms).astype(np.float32)
+
+
+def oracle_for(g):
+    """Run the C restatement on a golden fixture's inputs."""
+    mgr = str(g["manager"])
+    bw = float(g["bin_width"])
+    atoms, waters = g["atoms"], g["waters"]
+    if mgr == "mt":
+        w = g["w"]
+        if bool(g["simple_exv"]):
+            w = simple_exv_weights(w, float(g["volume"]), len(atoms))
+        A = O.pack_points(atoms, w, False)
+        W = O.pack_points(waters, g["ww"], False)
+        return O.hist_simple(A, W, bw, 8000)
+    kind = {"ffavg": 0, "ffexplicit": 1, "ffgrid": 2}[mgr]
+    A = O.pack_points(atoms, g["ff"], True)
+    W = O.pack_points(waters, np.ones(len(waters), np.int32), True)
+    X = O.pack_points(g["exv"], np.zeros(len(g["exv"]), np.int32), True)
+    z = float(g["volume"]) * RHO_W / len(atoms)
+    return O.hist_ff(kind, A, W, X if kind == 2 else None, bw, 8000, z)
