@@ -95,10 +95,10 @@ __global__ void __launch_bounds__(TILE) pairhist_kernel(PairLaunch L) {
     uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem);
     size_t off = (static_cast<size_t>(L.smem_rows) * pad * 4 + 15) & ~static_cast<size_t>(15);
     unsigned long long* s_dsum = reinterpret_cast<unsigned long long*>(smem + off);
-    off += static_cast<size_t>(pad) * 8;
+    off += (static_cast<size_t>(pad) * 8 + 15) & ~static_cast<size_t>(15);
     long long* s_wsum = reinterpret_cast<long long*>(smem + off);
-    if (WEIGHTED) off += static_cast<size_t>(pad) * 8;
-    float4* s_pts = reinterpret_cast<float4*>(smem + off);
+    if (WEIGHTED) off += (static_cast<size_t>(pad) * 8 + 15) & ~static_cast<size_t>(15);
+    float4* s_pts = reinterpret_cast<float4*>(smem + off);  // 16-byte aligned: every offset above is
     __shared__ long long s_grab;
 
     // zero the on-chip histograms once; flushes keep them zero afterwards

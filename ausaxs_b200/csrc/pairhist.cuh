@@ -54,9 +54,9 @@ inline size_t pairhist_smem_bytes(int rows, int bins, bool weighted, int tile) {
     size_t pad = (size_t)bins + 1;
     size_t b = (size_t)rows * pad * 4;          // u32 counts
     b = (b + 15) & ~(size_t)15;
-    b += pad * 8;                               // u64 offset sums
-    if (weighted) b += pad * 8;                 // i64 weight sums
-    b += (size_t)tile * 16;                     // inner tile of points
+    b += (pad * 8 + 15) & ~(size_t)15;          // u64 offset sums
+    if (weighted) b += (pad * 8 + 15) & ~(size_t)15;  // i64 weight sums
+    b += (size_t)tile * 16;                     // inner tile of points (16-byte aligned)
     return b + 64;
 }
 
