@@ -87,7 +87,8 @@ __global__ void ff_rows_kernel(FinalizeFF F) {
         }
         if (b == 0) tot += static_cast<unsigned long long>(F.n_a);
         double xx = 0;
-        if (F.kind == kKindAvg) xx = (xx_sum + (b == 0 ? F.n_a : 0)) * F.z_exv * F.z_exv;
+        // val * (Z * Z): the reference's release build hoists Z*Z (HistogramManagerMTFFAvg.cpp:361-362)
+        if (F.kind == kKindAvg) xx = (xx_sum + (b == 0 ? F.n_a : 0)) * (F.z_exv * F.z_exv);
         else if (F.kind == kKindGrid) xx = 2.0 * static_cast<double>(F.cnt_xx[b]) + (b == 0 ? F.n_x : 0);
         F.H[static_cast<size_t>(T * T + T) * nb + b] = xx;
         // atom-water rows (factor 1) and their exv marginal

@@ -261,6 +261,8 @@ int64_t oracle_hist_ff(int kind, const opoint* atoms, int32_t na, const opoint* 
         /* Z_exv scaling of the exv rows (HistogramManagerMTFFAvg.cpp:355-364) */
         for (int f1 = 1; f1 < NFF; ++f1)
             for (int32_t b = 0; b < mb; ++b) caa[(size_t)(f1 * NFF + 0) * nb + b] *= z_exv;
+        /* val * (Z * Z): the reference release build (-ffast-math) hoists Z*Z out of the loop of
+         * HistogramManagerMTFFAvg.cpp:361-362; checked against its output (tests/golden) */
         for (int32_t b = 0; b < mb; ++b) caa[b] *= z_exv * z_exv;
         for (int32_t b = 0; b < mb; ++b) caw[b] *= z_exv;
     }
