@@ -197,12 +197,19 @@ __global__ void weight_scale_kernel(const float4* a, int na, const float4* b, in
     }
 }
 
+// Weighted sum of one job in bin b: the pair kernel adds rint(w_i w_j * wscale) + 2^30 per pair
+// (unsigned, wrapping); the bias is removed with n pairs counted in the bin.
+__device__ __forceinline__ double weight_sum(const long long* w, const unsigned long long* n, int b, double inv) {
+    unsigned long long raw = static_cast<unsigned long long>(w[b]) - n[b] * (1ull << 30);
+    return static_cast<double>(static_cast<long long>(raw)) * inv;
+}
+
 __global__ void mt_maxbin_kernel(FinalizeMT F) {
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(F.max_bin, 10);  // minimum size (HistogramManagerMT.cpp:48)
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < F.nb; b += gridDim.x * blockDim.x) {
         double inv = 1.0 / static_cast<double>(*F.wscale);
-        double v = 2.0 * static_cast<double>(F.w_aa[b]) * inv + 2.0 * static_cast<double>(F.w_ww[b]) * inv +
-                   2.0 * static_cast<double>(F.w_aw[b]) * inv;
+        double v = 2.0 * weight_sum(F.w_aa, F.c_aa, b, inv) + 2.0 * weight_sum(F.w_ww, F.c_ww, b, inv) +
+                   2.0 * weight_sum(F.w_aw, F.c_aw, b, inv);
         if (b == 0) v += *F.self_aa + *F.self_ww;
         if (v != 0 && b >= 10) atomicMax(F.max_bin, b + 1);
     }
@@ -220,9 +227,9 @@ __global__ void mt_rows_kernel(FinalizeMT F) {
             F.d_axis[b] = 0;
             continue;
         }
-        double aa = 2.0 * static_cast<double>(F.w_aa[b]) * inv;
-        double aw = 2.0 * static_cast<double>(F.w_aw[b]) * inv;
-        double ww = 2.0 * static_cast<double>(F.w_ww[b]) * inv;
+        double aa = 2.0 * weight_sum(F.w_aa, F.c_aa, b, inv);
+        double aw = 2.0 * weight_sum(F.w_aw, F.c_aw, b, inv);
+        double ww = 2.0 * weight_sum(F.w_ww, F.c_ww, b, inv);
         unsigned int c_aa = 2u * static_cast<unsigned int>(F.c_aa[b]);
         unsigned int c_aw = 2u * static_cast<unsigned int>(F.c_aw[b]);
         unsigned int c_ww = 2u * static_cast<unsigned int>(F.c_ww[b]);

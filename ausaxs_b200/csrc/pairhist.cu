@@ -54,50 +54,112 @@ __device__ __forceinline__ void tile_coords(const PairJob& J, long long t, int& 
     tj = static_cast<int>(r + (t - start(r)));
 }
 
+// On-chip privatised histograms of one CTA.  Sums that can exceed 32 bits are kept as two u32
+// words, value = hi * 2^32 + lo, with exact carry propagation: every add uses the old value the
+// atomic returns, and exactly the add that wraps lo increments hi.  (A 64-bit shared-memory atomic
+// costs about three times as much per pair on sm_100a as two 32-bit ones.)
+struct Onchip {
+    uint32_t* cnt;  // [rows][pad] pair counts
+    uint32_t* dlo;  // [pad] biased fixed-point in-bin offsets
+    uint32_t* dhi;
+    uint32_t* wlo;  // [pad] biased fixed-point weight products (weighted launches)
+    uint32_t* whi;
+    int pad;
+};
+
+__device__ __forceinline__ void add_carry(uint32_t* lo, uint32_t* hi, int b, uint32_t v) {
+    const uint32_t old = atomicAdd(&lo[b], v);
+    if (old + v < old) atomicAdd(&hi[b], 1u);
+}
+
 template <int TILE, bool WEIGHTED>
-__device__ __forceinline__ void flush_hist(const PairJob& J, int pad, uint32_t* s_cnt, unsigned long long* s_dsum,
-                                           long long* s_wsum) {
+__device__ __forceinline__ void flush_hist(const PairJob& J, const Onchip& S) {
     __syncthreads();
     const int rows = J.row_hi - J.row_lo;
     const int nb = J.nbins;
     const int n = rows * nb;
     for (int idx = threadIdx.x; idx < n; idx += TILE) {
         int r = idx / nb, b = idx - r * nb;
-        uint32_t v = s_cnt[r * pad + b];
+        uint32_t v = S.cnt[r * S.pad + b];
         if (v) {
             atomicAdd(&J.counts[static_cast<size_t>(r) * nb + b], static_cast<unsigned long long>(v));
-            s_cnt[r * pad + b] = 0;
+            S.cnt[r * S.pad + b] = 0;
         }
     }
     for (int b = threadIdx.x; b < nb; b += TILE) {
         if (J.dsum) {
-            unsigned long long v = s_dsum[b];
+            unsigned long long v = (static_cast<unsigned long long>(S.dhi[b]) << 32) | S.dlo[b];
             if (v) {
                 atomicAdd(&J.dsum[b], v);
-                s_dsum[b] = 0;
+                S.dlo[b] = S.dhi[b] = 0;
             }
         }
         if (WEIGHTED && J.wsum) {
-            long long v = s_wsum[b];
+            unsigned long long v = (static_cast<unsigned long long>(S.whi[b]) << 32) | S.wlo[b];
             if (v) {
-                atomicAdd(reinterpret_cast<unsigned long long*>(&J.wsum[b]), static_cast<unsigned long long>(v));
-                s_wsum[b] = 0;
+                atomicAdd(reinterpret_cast<unsigned long long*>(&J.wsum[b]), v);
+                S.wlo[b] = S.whi[b] = 0;
             }
         }
     }
     __syncthreads();
 }
 
+// All pairs of one outer point against the staged inner tile.  GENERAL handles the diagonal tiles
+// of self jobs (j > i only) and the tiles that contain the scalar-tail partners; every other tile
+// takes the lean path.
+template <bool GENERAL, bool WEIGHTED>
+__device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, const float4* s_pts, const float4 a, int i,
+                                           int j0, int jn, bool diag, float wsc, unsigned long long& overflow) {
+    const float inv_w = J.inv_w, c = J.c, scale = J.scale;
+    const unsigned nbins = static_cast<unsigned>(J.nbins);
+    const int rmode = J.row_mode, rlo = J.row_lo, rhi = J.row_hi;
+    const int ts = tail_start(J.self ? i + 1 : 0, J.nb);
+    const int ta = __float_as_int(a.w);
+    const int rowbase = rmode == kRowPair ? ta * J.types : (rmode == kRowOuter ? ta : 0);
+    const bool pair_rows = rmode == kRowPair;
+    const int full_rows = pair_rows ? J.types * J.types : (rmode == kRowOuter ? J.types : 1);
+    const bool all_rows = rlo == 0 && rhi >= full_rows;
+    const bool do_d = J.dsum != nullptr;
+    const bool do_w = WEIGHTED && J.wsum != nullptr;
+#pragma unroll 4
+    for (int jj = 0; jj < jn; ++jj) {
+        const float4 b = s_pts[jj];
+        const int j = j0 + jj;
+        if (GENERAL && diag && j <= i) continue;
+        const PairBin p = pair_eval(a, b, inv_w, GENERAL && j >= ts);
+        if (static_cast<unsigned>(p.bin) >= nbins) {
+            ++overflow;
+            continue;
+        }
+        const int row = pair_rows ? rowbase + __float_as_int(b.w) : rowbase;
+        if (all_rows || (row >= rlo && row < rhi)) atomicAdd(&S.cnt[(row - rlo) * S.pad + p.bin], 1u);
+        if (do_d) add_carry(S.dlo, S.dhi, p.bin, pair_residual(p, c, scale));
+        if (do_w) {
+            const float wp = __fmul_rn(a.w, b.w);
+            const int wq = __float2int_rn(__fmul_rn(wp, wsc));  // |wq| <= 2^30
+            add_carry(S.wlo, S.whi, p.bin, static_cast<uint32_t>(wq + (1 << 30)));
+        }
+    }
+}
+
 template <int TILE, bool WEIGHTED>
 __global__ void __launch_bounds__(TILE) pairhist_kernel(PairLaunch L) {
     extern __shared__ __align__(16) unsigned char smem[];
-    const int pad = L.smem_bins + 1;
-    uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem);
-    size_t off = (static_cast<size_t>(L.smem_rows) * pad * 4 + 15) & ~static_cast<size_t>(15);
-    unsigned long long* s_dsum = reinterpret_cast<unsigned long long*>(smem + off);
-    off += (static_cast<size_t>(pad) * 8 + 15) & ~static_cast<size_t>(15);
-    long long* s_wsum = reinterpret_cast<long long*>(smem + off);
-    if (WEIGHTED) off += (static_cast<size_t>(pad) * 8 + 15) & ~static_cast<size_t>(15);
+    Onchip S;
+    S.pad = L.smem_bins + 1;
+    const size_t row_bytes = (static_cast<size_t>(S.pad) * 4 + 15) & ~static_cast<size_t>(15);
+    size_t off = 0;
+    S.cnt = reinterpret_cast<uint32_t*>(smem);
+    off += (static_cast<size_t>(L.smem_rows) * S.pad * 4 + 15) & ~static_cast<size_t>(15);
+    S.dlo = reinterpret_cast<uint32_t*>(smem + off);
+    off += row_bytes;
+    S.dhi = reinterpret_cast<uint32_t*>(smem + off);
+    off += row_bytes;
+    S.wlo = reinterpret_cast<uint32_t*>(smem + off);
+    if (WEIGHTED) off += row_bytes;
+    S.whi = reinterpret_cast<uint32_t*>(smem + off);
+    if (WEIGHTED) off += row_bytes;
     float4* s_pts = reinterpret_cast<float4*>(smem + off);  // 16-byte aligned: every offset above is
     __shared__ long long s_grab;
 
@@ -122,8 +184,9 @@ __global__ void __launch_bounds__(TILE) pairhist_kernel(PairLaunch L) {
         const long long g1 = min(g0 + static_cast<long long>(L.chunk), static_cast<long long>(L.total_tiles));
         for (long long g = g0; g < g1; ++g) {
             const int jb = find_job(L.jobs, L.n_jobs, g);
+            // u32 counts stay exact below 2^32 pairs per bin between flushes
             if (jb != cur || pairs_since_flush > (1ll << 31)) {
-                if (cur >= 0) flush_hist<TILE, WEIGHTED>(L.jobs[cur], pad, s_cnt, s_dsum, s_wsum);
+                if (cur >= 0) flush_hist<TILE, WEIGHTED>(L.jobs[cur], S);
                 cur = jb;
                 pairs_since_flush = 0;
             }
@@ -139,38 +202,14 @@ __global__ void __launch_bounds__(TILE) pairhist_kernel(PairLaunch L) {
             const float4 a = active ? J.A[i] : make_float4(0.f, 0.f, 0.f, 0.f);
             __syncthreads();
             pairs_since_flush += static_cast<long long>(TILE) * TILE;
-
-            const float inv_w = J.inv_w, c = J.c, scale = J.scale;
-            const int nbins = J.nbins;
-            const int rmode = J.row_mode, rlo = J.row_lo, rhi = J.row_hi;
-            const bool diag = J.self && ti == tj;
-            const int ts = tail_start(J.self ? i + 1 : 0, J.nb);
-            const int rowbase = rmode == kRowPair ? __float_as_int(a.w) * J.types : (rmode == kRowOuter ? __float_as_int(a.w) : 0);
-            const bool do_d = J.dsum != nullptr;
-            const bool do_w = WEIGHTED && J.wsum != nullptr;
             if (!active) continue;
-#pragma unroll 4
-            for (int jj = 0; jj < jn; ++jj) {
-                const float4 b = s_pts[jj];
-                const int j = j0 + jj;
-                if (diag && j <= i) continue;
-                const PairBin p = pair_eval(a, b, inv_w, j >= ts);
-                if (static_cast<unsigned>(p.bin) >= static_cast<unsigned>(nbins)) {
-                    ++overflow;
-                    continue;
-                }
-                const int row = rmode == kRowPair ? rowbase + __float_as_int(b.w) : rowbase;
-                if (row >= rlo && row < rhi) atomicAdd(&s_cnt[(row - rlo) * pad + p.bin], 1u);
-                if (do_d) atomicAdd(&s_dsum[p.bin], static_cast<unsigned long long>(pair_residual(p, c, scale)));
-                if (do_w) {
-                    const float wp = __fmul_rn(a.w, b.w);
-                    const long long wq = __float2ll_rn(__fmul_rn(wp, wsc));
-                    atomicAdd(reinterpret_cast<unsigned long long*>(&s_wsum[p.bin]), static_cast<unsigned long long>(wq));
-                }
-            }
+            const bool diag = J.self && ti == tj;
+            const bool has_tail = j0 + jn > J.nb - 3;  // scalar-tail partners are among the last 3 inner points
+            if (diag || has_tail) tile_pairs<true, WEIGHTED>(J, S, s_pts, a, i, j0, jn, diag, wsc, overflow);
+            else tile_pairs<false, WEIGHTED>(J, S, s_pts, a, i, j0, jn, false, wsc, overflow);
         }
     }
-    if (cur >= 0) flush_hist<TILE, WEIGHTED>(L.jobs[cur], pad, s_cnt, s_dsum, s_wsum);
+    if (cur >= 0) flush_hist<TILE, WEIGHTED>(L.jobs[cur], S);
     // warp-aggregated overflow report
     for (int o = 16; o > 0; o >>= 1) overflow += __shfl_xor_sync(0xffffffffu, overflow, o);
     if ((threadIdx.x & 31) == 0 && overflow) atomicAdd(L.overflow, overflow);

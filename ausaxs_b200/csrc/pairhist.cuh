@@ -32,7 +32,8 @@ struct PairJob {
     float scale;          // 2^20 / c
     unsigned long long* counts;  // [row_hi-row_lo][nbins] global pair counts (factor not applied)
     unsigned long long* dsum;    // [nbins] biased fixed-point offset sums, or null
-    long long* wsum;             // [nbins] fixed-point weight-product sums, or null (weighted jobs)
+    long long* wsum;             // [nbins] biased fixed-point weight-product sums, or null (weighted jobs):
+                                 //         per pair rint(w_i w_j * wscale) + 2^30
     float wscale;                // unused (the launch-wide scale lives in device memory)
 };
 
@@ -46,17 +47,17 @@ struct PairLaunch {
     unsigned long long* tile_counter;
     unsigned long long* overflow;   // pairs whose bin fell outside the job's nbins
     int32_t weighted;
-    const float* wscale;            // device: 2^k with max|w_i w_j| * 2^k <= 2^30 (weighted launches)
+    const float* wscale;            // device: 2^k with max|w_i w_j| * 2^k < 2^30 (weighted launches)
 };
 
-// Bytes of dynamic shared memory a launch needs.
+// Bytes of dynamic shared memory a launch needs (layout of pairhist_kernel).
 inline size_t pairhist_smem_bytes(int rows, int bins, bool weighted, int tile) {
     size_t pad = (size_t)bins + 1;
-    size_t b = (size_t)rows * pad * 4;          // u32 counts
-    b = (b + 15) & ~(size_t)15;
-    b += (pad * 8 + 15) & ~(size_t)15;          // u64 offset sums
-    if (weighted) b += (pad * 8 + 15) & ~(size_t)15;  // i64 weight sums
-    b += (size_t)tile * 16;                     // inner tile of points (16-byte aligned)
+    size_t row = (pad * 4 + 15) & ~(size_t)15;
+    size_t b = ((size_t)rows * pad * 4 + 15) & ~(size_t)15;  // u32 counts
+    b += 2 * row;                                            // offset sums (lo, hi)
+    if (weighted) b += 2 * row;                              // weight sums (lo, hi)
+    b += (size_t)tile * 16;                                  // inner tile of points (16-byte aligned)
     return b + 64;
 }
 

@@ -202,4 +202,9 @@ def test_all_pairs_in_one_bin(gpu_ctx):
     h = hist.HistogramManagerMTFFAvg(m, True, 0.25, 8000, gpu_ctx).calculate_all()
     aa = h.get_raw_aa_counts_by_ff()
     assert aa[3, 3, 0] == n * (n - 1) + n
-    assert aa.sum() - aa[3, 3, 0] - aa[3, 0, 0] - aa[0, 0, 0] == 0
+    rest = aa.copy()
+    rest[3, 3, 0] = rest[3, 0, 0] = rest[0, 0, 0] = 0
+    assert not rest.any()
+    z = 1.0 * 0.334 / n
+    assert aa[3, 0, 0] == n * (n - 1) * z
+    assert aa[0, 0, 0] == (n * (n - 1) + n) * (z * z)
