@@ -170,7 +170,8 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
     P.nb = nb;
     P.inv_w = inv_w;
     P.c = (float)(1.0 / (double)inv_w);
-    P.scale = (float)(1048576.0 / (double)P.c);
+    // offsets r in [-c/2 (1 + 2^-10), c/2 (1 + 2^-10)] map into [0, 2^16)
+    P.scale = (float)(32768.0 / (double)P.c * (1.0 - 1.0 / 256));
     const bool grid = cfg.manager == AUSAXS_MANAGER_FFGRID;
     const bool mt = cfg.manager == AUSAXS_MANAGER_MT;
     const int n_x_eff = grid ? n_x : 0;
@@ -267,9 +268,13 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
     P.dev.ensure(off);
     char* base = P.dev.as<char>();
 
-    long long tb = 0;
+    // Jobs split into launch groups by the rows they keep on chip: one-row jobs (ww, xx, wx and all
+    // Simple jobs) run with a small footprint and high occupancy, multi-row jobs (aa, aw, ax) get the
+    // shared memory they need.  Tiles are numbered per group.
     P.pairs = 0;
-    P.smem_rows = 1;
+    std::vector<PairJob> group_jobs[2];
+    long long group_tiles[2] = {0, 0};
+    int group_rows[2] = {1, 1};
     for (auto& j : js) {
         if (j.na == 0 || j.nbp == 0) continue;
         long long tiles = j.self ? tri(nt(j.na)) : (long long)nt(j.na) * nt(j.nbp);
@@ -278,6 +283,7 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
         P.pairs += pairs;
         for (int r0 = 0; r0 < j.rows; r0 += max_group_rows) {
             int r1 = std::min(j.rows, r0 + max_group_rows);
+            const int g = (r1 - r0) == 1 ? 0 : 1;
             PairJob pj{};
             pj.A = j.A;
             pj.B = j.B;
@@ -291,7 +297,7 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
             pj.nbins = nb;
             pj.tiles_i = nt(j.na);
             pj.tiles_j = nt(j.nbp);
-            pj.tile_begin = tb;
+            pj.tile_begin = group_tiles[g];
             pj.tile_count = tiles;
             pj.inv_w = P.inv_w;
             pj.c = P.c;
@@ -301,33 +307,39 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
             pj.dsum = (r0 == 0 && weighted) ? reinterpret_cast<unsigned long long*>(base + slot_ds[j.slot]) : nullptr;
             pj.wsum = (mt && r0 == 0) ? reinterpret_cast<long long*>(base + slot_ws[j.slot]) : nullptr;
             pj.wscale = 0;  // read from device memory by weighted launches (see below)
-            jobs.push_back(pj);
-            tb += tiles;
-            P.smem_rows = std::max(P.smem_rows, r1 - r0);
+            group_jobs[g].push_back(pj);
+            group_tiles[g] += tiles;
+            group_rows[g] = std::max(group_rows[g], r1 - r0);
         }
     }
-    if (jobs.size() > 64) throw Error{AUSAXS_ERR_CAPACITY, "too many row groups"};
-    P.n_jobs = (int)jobs.size();
-    P.total_tiles = tb;
+    if (group_jobs[0].size() + group_jobs[1].size() > 64) throw Error{AUSAXS_ERR_CAPACITY, "too many row groups"};
     const bool w_launch = mt;  // Simple histograms always carry weight sums (values)
-    P.smem = pairhist_smem_bytes(P.smem_rows, nb, w_launch, tile);
-    int per_sm = std::max(1, std::min((int)(233472 / (P.smem + 1024)), 2048 / tile));
-    long long want = std::max<long long>(1, P.total_tiles);
-    P.grid = (int)std::min<long long>((long long)C.sm_count * per_sm, want);
-    P.chunk = (int)std::max<long long>(1, std::min<long long>(8, P.total_tiles / ((long long)P.grid * 8)));
-    if (!jobs.empty()) AUSAXS_CUDA(cudaMemcpy(base + P.off_jobs, jobs.data(), sizeof(PairJob) * jobs.size(), cudaMemcpyHostToDevice));
-
-    PairLaunch& L = P.launch;
-    L.jobs = reinterpret_cast<const PairJob*>(base + P.off_jobs);
-    L.n_jobs = P.n_jobs;
-    L.total_tiles = P.total_tiles;
-    L.chunk = P.chunk;
-    L.smem_rows = P.smem_rows;
-    L.smem_bins = nb;
-    L.tile_counter = reinterpret_cast<unsigned long long*>(base + P.off_counter);
-    L.overflow = reinterpret_cast<unsigned long long*>(base + P.off_overflow);
-    L.weighted = w_launch;
-    L.wscale = reinterpret_cast<const float*>(base + P.off_wscale);
+    P.n_launch = 0;
+    P.total_tiles = 0;
+    size_t job_off = P.off_jobs;
+    for (int g = 0; g < 2; ++g) {
+        if (group_jobs[g].empty()) continue;
+        Plan::Group& G = P.group[P.n_launch++];
+        G.tile = tile;
+        G.smem = pairhist_smem_bytes(group_rows[g], nb, w_launch, tile);
+        int per_sm = std::max(1, std::min((int)(233472 / (G.smem + 1024)), 2048 / tile));
+        G.grid = (int)std::min<long long>((long long)C.sm_count * per_sm, std::max<long long>(1, group_tiles[g]));
+        PairLaunch& L = G.launch;
+        L.jobs = reinterpret_cast<const PairJob*>(base + job_off);
+        L.n_jobs = (int)group_jobs[g].size();
+        L.total_tiles = group_tiles[g];
+        L.chunk = (int)std::max<long long>(1, std::min<long long>(8, group_tiles[g] / ((long long)G.grid * 8)));
+        L.smem_rows = group_rows[g];
+        L.smem_bins = nb;
+        L.tile_counter = reinterpret_cast<unsigned long long*>(base + P.off_counter) + g;
+        L.overflow = reinterpret_cast<unsigned long long*>(base + P.off_overflow);
+        L.weighted = w_launch;
+        L.wscale = reinterpret_cast<const float*>(base + P.off_wscale);
+        AUSAXS_CUDA(cudaMemcpy(base + job_off, group_jobs[g].data(), sizeof(PairJob) * group_jobs[g].size(),
+                               cudaMemcpyHostToDevice));
+        job_off += sizeof(PairJob) * group_jobs[g].size();
+        P.total_tiles += group_tiles[g];
+    }
 
     // finalisation
     auto cnt = [&](int k) { return reinterpret_cast<const unsigned long long*>(base + slot_cnt[k]); };
@@ -423,10 +435,11 @@ void Structure::enqueue_histogram(const ausaxs_hist_config& cfg) {
         weight_square_sum_launch(raw_w.as<float4>(), n_w, reinterpret_cast<double*>(base + P.off_self) + 1, s);
         C.check_launch("weights");
     }
-    if (P.total_tiles > 0) {
+    for (int g = 0; g < P.n_launch; ++g) {
+        const Plan::Group& G = P.group[g];
         cudaEvent_t ev;
         C.time_begin(0, &ev);
-        pairhist_launch(P.launch, P.tile, P.grid, P.smem, s);
+        pairhist_launch(G.launch, G.tile, G.grid, G.smem, s);
         C.check_launch("pairhist");
         C.time_end(0, ev);
     }

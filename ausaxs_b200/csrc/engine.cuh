@@ -47,9 +47,13 @@ struct Plan {
     double bin_width = 0;
     int n_a = -1, n_w = -1, n_x = -1, T = -1;
     // shapes
-    int nb = 0, tile = 256, grid = 0, chunk = 1, smem_rows = 0;
-    size_t smem = 0;
-    int n_jobs = 0;
+    int nb = 0, tile = 256;
+    struct Group {  // one pair-kernel launch
+        PairLaunch launch{};
+        int tile = 256, grid = 0;
+        size_t smem = 0;
+    } group[2];
+    int n_launch = 0;
     long long total_tiles = 0, pairs = 0;
     int R = 0;
     float inv_w = 0, c = 0, scale = 0;
@@ -60,7 +64,6 @@ struct Plan {
            off_expand_aa = 0, off_expand_aw = 0;
     FinalizeFF fin_ff{};
     FinalizeMT fin_mt{};
-    PairLaunch launch{};
     // tensor-core scratch
     DevBuf tc;
     int tc_nq = 0;

@@ -54,22 +54,39 @@ __device__ __forceinline__ void tile_coords(const PairJob& J, long long t, int& 
     tj = static_cast<int>(r + (t - start(r)));
 }
 
-// On-chip privatised histograms of one CTA.  Sums that can exceed 32 bits are kept as two u32
-// words, value = hi * 2^32 + lo, with exact carry propagation: every add uses the old value the
-// atomic returns, and exactly the add that wraps lo increments hi.  (A 64-bit shared-memory atomic
-// costs about three times as much per pair on sm_100a as two 32-bit ones.)
+// On-chip privatised histograms of one CTA.
+//   counts   : u32 per (row, bin), one atomic per pair.
+//   offsets  : the in-bin distance offset of a pair is quantised to 16 bits (kResBits) and added
+//              with a 32-bit atomic to dacc; every kSegment inner points (at most 2^16 pairs per
+//              bin, so dacc cannot wrap) the threads drain dacc into the u64 sums d64 without
+//              atomics.  (A 64-bit shared-memory atomic costs about three times as much per pair on
+//              sm_100a; this keeps one cheap 32-bit atomic per pair and an exact integer sum.)
+//   weights  : weighted (Simple) jobs add rint(w_i w_j wscale) + 2^30 to wlo with exact carry
+//              propagation into whi (the old value returned by the atomic detects the wrap).
 struct Onchip {
-    uint32_t* cnt;  // [rows][pad] pair counts
-    uint32_t* dlo;  // [pad] biased fixed-point in-bin offsets
-    uint32_t* dhi;
-    uint32_t* wlo;  // [pad] biased fixed-point weight products (weighted launches)
-    uint32_t* whi;
+    uint32_t* cnt;                // [rows][pad]
+    uint32_t* dacc;               // [pad]
+    unsigned long long* d64;      // [pad]
+    uint32_t* wlo;                // [pad] (weighted launches)
+    uint32_t* whi;                // [pad]
     int pad;
 };
 
 __device__ __forceinline__ void add_carry(uint32_t* lo, uint32_t* hi, int b, uint32_t v) {
     const uint32_t old = atomicAdd(&lo[b], v);
     if (old + v < old) atomicAdd(&hi[b], 1u);
+}
+
+// dacc -> d64 for the bins of a job; callers synchronise before (atomics done) and after.
+template <int TILE>
+__device__ __forceinline__ void drain_offsets(const Onchip& S, int nb) {
+    for (int b = threadIdx.x; b < nb; b += TILE) {
+        uint32_t v = S.dacc[b];
+        if (v) {
+            S.d64[b] += v;
+            S.dacc[b] = 0;
+        }
+    }
 }
 
 template <int TILE, bool WEIGHTED>
@@ -88,10 +105,10 @@ __device__ __forceinline__ void flush_hist(const PairJob& J, const Onchip& S) {
     }
     for (int b = threadIdx.x; b < nb; b += TILE) {
         if (J.dsum) {
-            unsigned long long v = (static_cast<unsigned long long>(S.dhi[b]) << 32) | S.dlo[b];
+            unsigned long long v = S.d64[b];
             if (v) {
                 atomicAdd(&J.dsum[b], v);
-                S.dlo[b] = S.dhi[b] = 0;
+                S.d64[b] = 0;
             }
         }
         if (WEIGHTED && J.wsum) {
@@ -105,25 +122,25 @@ __device__ __forceinline__ void flush_hist(const PairJob& J, const Onchip& S) {
     __syncthreads();
 }
 
-// All pairs of one outer point against the staged inner tile.  GENERAL handles the diagonal tiles
-// of self jobs (j > i only) and the tiles that contain the scalar-tail partners; every other tile
-// takes the lean path.
-template <bool GENERAL, bool WEIGHTED>
+// Pairs of one outer point against inner points [k0, k1) of the staged tile.  GENERAL handles the
+// diagonal tiles of self jobs (j > i only) and the tiles that contain scalar-tail partners; SINGLE
+// is a one-row job whose count index is the bin itself.
+template <bool GENERAL, bool WEIGHTED, bool SINGLE>
 __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, const float4* s_pts, const float4 a, int i,
-                                           int j0, int jn, bool diag, float wsc, unsigned long long& overflow) {
+                                           int j0, int k0, int k1, bool diag, float wsc, unsigned long long& overflow) {
     const float inv_w = J.inv_w, c = J.c, scale = J.scale;
     const unsigned nbins = static_cast<unsigned>(J.nbins);
     const int rmode = J.row_mode, rlo = J.row_lo, rhi = J.row_hi;
     const int ts = tail_start(J.self ? i + 1 : 0, J.nb);
     const int ta = __float_as_int(a.w);
-    const int rowbase = rmode == kRowPair ? ta * J.types : (rmode == kRowOuter ? ta : 0);
     const bool pair_rows = rmode == kRowPair;
+    const int rowbase = pair_rows ? ta * J.types : (rmode == kRowOuter ? ta : 0);
     const int full_rows = pair_rows ? J.types * J.types : (rmode == kRowOuter ? J.types : 1);
     const bool all_rows = rlo == 0 && rhi >= full_rows;
     const bool do_d = J.dsum != nullptr;
     const bool do_w = WEIGHTED && J.wsum != nullptr;
 #pragma unroll 4
-    for (int jj = 0; jj < jn; ++jj) {
+    for (int jj = k0; jj < k1; ++jj) {
         const float4 b = s_pts[jj];
         const int j = j0 + jj;
         if (GENERAL && diag && j <= i) continue;
@@ -132,9 +149,13 @@ __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, co
             ++overflow;
             continue;
         }
-        const int row = pair_rows ? rowbase + __float_as_int(b.w) : rowbase;
-        if (all_rows || (row >= rlo && row < rhi)) atomicAdd(&S.cnt[(row - rlo) * S.pad + p.bin], 1u);
-        if (do_d) add_carry(S.dlo, S.dhi, p.bin, pair_residual(p, c, scale));
+        if (SINGLE) {
+            atomicAdd(&S.cnt[p.bin], 1u);
+        } else {
+            const int row = pair_rows ? rowbase + __float_as_int(b.w) : rowbase;
+            if (all_rows || (row >= rlo && row < rhi)) atomicAdd(&S.cnt[(row - rlo) * S.pad + p.bin], 1u);
+        }
+        if (do_d) atomicAdd(&S.dacc[p.bin], pair_residual(p, c, scale));
         if (do_w) {
             const float wp = __fmul_rn(a.w, b.w);
             const int wq = __float2int_rn(__fmul_rn(wp, wsc));  // |wq| <= 2^30
@@ -148,22 +169,23 @@ __global__ void __launch_bounds__(TILE) pairhist_kernel(PairLaunch L) {
     extern __shared__ __align__(16) unsigned char smem[];
     Onchip S;
     S.pad = L.smem_bins + 1;
-    const size_t row_bytes = (static_cast<size_t>(S.pad) * 4 + 15) & ~static_cast<size_t>(15);
+    const size_t w32 = (static_cast<size_t>(S.pad) * 4 + 15) & ~static_cast<size_t>(15);
+    const size_t w64 = (static_cast<size_t>(S.pad) * 8 + 15) & ~static_cast<size_t>(15);
     size_t off = 0;
     S.cnt = reinterpret_cast<uint32_t*>(smem);
     off += (static_cast<size_t>(L.smem_rows) * S.pad * 4 + 15) & ~static_cast<size_t>(15);
-    S.dlo = reinterpret_cast<uint32_t*>(smem + off);
-    off += row_bytes;
-    S.dhi = reinterpret_cast<uint32_t*>(smem + off);
-    off += row_bytes;
+    S.d64 = reinterpret_cast<unsigned long long*>(smem + off);
+    off += w64;
+    S.dacc = reinterpret_cast<uint32_t*>(smem + off);
+    off += w32;
     S.wlo = reinterpret_cast<uint32_t*>(smem + off);
-    if (WEIGHTED) off += row_bytes;
+    if (WEIGHTED) off += w32;
     S.whi = reinterpret_cast<uint32_t*>(smem + off);
-    if (WEIGHTED) off += row_bytes;
+    if (WEIGHTED) off += w32;
     float4* s_pts = reinterpret_cast<float4*>(smem + off);  // 16-byte aligned: every offset above is
     __shared__ long long s_grab;
 
-    // zero the on-chip histograms once; flushes keep them zero afterwards
+    // zero the on-chip histograms once; drains and flushes keep them zero afterwards
     {
         uint32_t* z = reinterpret_cast<uint32_t*>(smem);
         size_t words = off / 4;
@@ -202,11 +224,27 @@ __global__ void __launch_bounds__(TILE) pairhist_kernel(PairLaunch L) {
             const float4 a = active ? J.A[i] : make_float4(0.f, 0.f, 0.f, 0.f);
             __syncthreads();
             pairs_since_flush += static_cast<long long>(TILE) * TILE;
-            if (!active) continue;
             const bool diag = J.self && ti == tj;
             const bool has_tail = j0 + jn > J.nb - 3;  // scalar-tail partners are among the last 3 inner points
-            if (diag || has_tail) tile_pairs<true, WEIGHTED>(J, S, s_pts, a, i, j0, jn, diag, wsc, overflow);
-            else tile_pairs<false, WEIGHTED>(J, S, s_pts, a, i, j0, jn, false, wsc, overflow);
+            const bool general = diag || has_tail;
+            const bool single = J.row_mode == kRowSingle && J.row_lo == 0 && J.row_hi >= 1;
+            for (int k0 = 0; k0 < jn; k0 += kSegment) {
+                const int k1 = min(jn, k0 + kSegment);
+                if (active) {
+                    if (general) {
+                        if (single) tile_pairs<true, WEIGHTED, true>(J, S, s_pts, a, i, j0, k0, k1, diag, wsc, overflow);
+                        else tile_pairs<true, WEIGHTED, false>(J, S, s_pts, a, i, j0, k0, k1, diag, wsc, overflow);
+                    } else {
+                        if (single) tile_pairs<false, WEIGHTED, true>(J, S, s_pts, a, i, j0, k0, k1, false, wsc, overflow);
+                        else tile_pairs<false, WEIGHTED, false>(J, S, s_pts, a, i, j0, k0, k1, false, wsc, overflow);
+                    }
+                }
+                if (J.dsum) {
+                    __syncthreads();
+                    drain_offsets<TILE>(S, J.nbins);
+                    __syncthreads();
+                }
+            }
         }
     }
     if (cur >= 0) flush_hist<TILE, WEIGHTED>(L.jobs[cur], S);

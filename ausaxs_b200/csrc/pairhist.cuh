@@ -55,7 +55,7 @@ inline size_t pairhist_smem_bytes(int rows, int bins, bool weighted, int tile) {
     size_t pad = (size_t)bins + 1;
     size_t row = (pad * 4 + 15) & ~(size_t)15;
     size_t b = ((size_t)rows * pad * 4 + 15) & ~(size_t)15;  // u32 counts
-    b += 2 * row;                                            // offset sums (lo, hi)
+    b += ((pad * 8 + 15) & ~(size_t)15) + row;               // offset sums: u64 + u32 accumulator
     if (weighted) b += 2 * row;                              // weight sums (lo, hi)
     b += (size_t)tile * 16;                                  // inner tile of points (16-byte aligned)
     return b + 64;
