@@ -33,7 +33,7 @@ EXPORTED = [
     "ausaxs_gpu_ctx_create", "ausaxs_gpu_ctx_destroy", "ausaxs_gpu_ctx_set_stream", "ausaxs_gpu_ctx_launch_count",
     "ausaxs_gpu_last_error", "ausaxs_gpu_ctx_enable_timing", "ausaxs_gpu_ctx_kernel_time", "ausaxs_gpu_histogram", "ausaxs_gpu_debye", "ausaxs_gpu_profile",
     "ausaxs_gpu_structure_create", "ausaxs_gpu_structure_destroy", "ausaxs_gpu_structure_profile",
-    "ausaxs_gpu_structure_histogram",
+    "ausaxs_gpu_structure_histogram", "ausaxs_gpu_histogram_mt_noalloc",
 ]
 
 

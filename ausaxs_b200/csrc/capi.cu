@@ -52,6 +52,11 @@ ausaxs_debye_params default_params(const ausaxs_debye_params* p) {
 }
 }  // namespace
 
+namespace ausaxs_b200 {
+// Lets entry points outside this file report through ausaxs_gpu_last_error().
+void set_last_error(const char* msg) { g_last_error = msg; }
+}  // namespace ausaxs_b200
+
 extern "C" {
 
 const char* ausaxs_gpu_last_error(void) { return g_last_error.c_str(); }

@@ -190,6 +190,31 @@ AUSAXS_API int ausaxs_gpu_structure_profile(ausaxs_gpu_ctx* ctx, ausaxs_gpu_stru
 AUSAXS_API int ausaxs_gpu_structure_histogram(ausaxs_gpu_ctx* ctx, ausaxs_gpu_structure* s, const ausaxs_hist_config* cfg,
                                    ausaxs_hist_result* out);
 
+/*
+ * Allocation-free Simple (weighted) histogram.  No counterpart in the reference: it exists for
+ * callers that cannot allocate device memory while they run (a memory-pool-managed or real-time
+ * section, or an embedding application that forbids cudaMalloc after start-up, since allocation can
+ * synchronise the device).  It computes what ausaxs_gpu_histogram returns for AUSAXS_MANAGER_MT, but
+ * from device inputs into device outputs, and calls no cudaMalloc, cudaFree or allocating library
+ * routine: its temporaries live in one file-scope device array (about 640 KiB per device, held
+ * until the process exits).
+ *   atoms, waters   : device arrays of n x {float x, y, z, w} (weights in the 4th word)
+ *   bin_count       : at most 8192 (AUSAXS_ERR_CAPACITY above that); every pair distance must fall
+ *                     below bin_count * bin_width
+ *   hist_out        : device, 5 * bin_count doubles: rows {aa, aw, ww, tot, d_axis}, each with stride
+ *                     bin_count, zero beyond *max_bin_out
+ *   max_bin_out     : device int32
+ *   overflow_out    : device u64 (may be NULL): pairs that fell beyond bin_count
+ *   stream          : cudaStream_t as void* (NULL = legacy default stream); the call only enqueues.
+ * All calls share the one scratch array, which keeps the last call's contents (each call clears
+ * what must start at zero); calls that overlap on the GPU race and give wrong results.  The first
+ * call on a device looks up the array's address and caches it: make it before any stream capture.
+ */
+AUSAXS_API int ausaxs_gpu_histogram_mt_noalloc(const float* atoms, int32_t n_atoms, const float* waters,
+                                               int32_t n_waters, double bin_width, int32_t bin_count,
+                                               int32_t weighted_bins, double* hist_out, int32_t* max_bin_out,
+                                               unsigned long long* overflow_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
