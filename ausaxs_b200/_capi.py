@@ -33,7 +33,7 @@ EXPORTED = [
     "ausaxs_gpu_ctx_create", "ausaxs_gpu_ctx_destroy", "ausaxs_gpu_ctx_set_stream", "ausaxs_gpu_ctx_launch_count",
     "ausaxs_gpu_last_error", "ausaxs_gpu_ctx_enable_timing", "ausaxs_gpu_ctx_kernel_time", "ausaxs_gpu_histogram", "ausaxs_gpu_debye", "ausaxs_gpu_profile",
     "ausaxs_gpu_structure_create", "ausaxs_gpu_structure_destroy", "ausaxs_gpu_structure_profile",
-    "ausaxs_gpu_structure_histogram", "ausaxs_gpu_histogram_mt_noalloc",
+    "ausaxs_gpu_structure_histogram", "ausaxs_gpu_histogram_mt_noalloc", "ausaxs_gpu_linear_lsq",
 ]
 
 
@@ -97,6 +97,7 @@ def load():
         L.ausaxs_gpu_structure_profile.argtypes = [vp, vp, C.POINTER(HistConfig), f64, C.c_int32,
                                                    C.POINTER(DebyeParams), f64, f64]
         L.ausaxs_gpu_structure_histogram.argtypes = [vp, vp, C.POINTER(HistConfig), C.POINTER(HistResult)]
+        L.ausaxs_gpu_linear_lsq.argtypes = [vp, f64, f64, f64, C.c_int32, f64]
         _lib = L
         return L
 
@@ -159,6 +160,14 @@ class Context:
         n = C.c_int64(0)
         check(load().ausaxs_gpu_ctx_kernel_time(self.h, cls, C.byref(ms), C.byref(n)))
         return ms.value, n.value
+
+
+def linear_lsq(ctx: "Context", data, model, err) -> np.ndarray:
+    """{a, b, sigma_a, sigma_b, chi2} of model ~ a * data + b (fitter::detail::LinearLeastSquares::fit)."""
+    data, model, err = (np.ascontiguousarray(x, np.float64) for x in (data, model, err))
+    out = np.zeros(5)
+    check(load().ausaxs_gpu_linear_lsq(ctx.h, dptr(data), dptr(model), dptr(err), len(data), dptr(out)))
+    return out
 
 
 _default = {}

@@ -4,6 +4,7 @@
 #include <string>
 
 #include "engine.cuh"
+#include "lsq.cuh"
 
 using namespace ausaxs_b200;
 
@@ -195,6 +196,25 @@ int ausaxs_gpu_profile(ausaxs_gpu_ctx* ctx, const ausaxs_hist_config* cfg, const
         AUSAXS_CUDA(cudaMemcpyAsync(&overflow, S.plan.dev.as<char>() + S.plan.off_overflow, 8, cudaMemcpyDeviceToHost, C.stream));
         AUSAXS_CUDA(cudaStreamSynchronize(C.stream));
         if (overflow) throw Error{AUSAXS_ERR_BIN_OVERFLOW, "pair distances beyond bin_count * bin_width; increase settings::axes::bin_count"};
+    });
+}
+
+int ausaxs_gpu_linear_lsq(ausaxs_gpu_ctx* ctx, const double* data, const double* model, const double* err,
+                          int32_t n, double* out) {
+    return guarded([&] {
+        if (!ctx || !data || !model || !err || !out || n < 2) throw Error{AUSAXS_ERR_ARGUMENT, "invalid argument"};
+        Ctx& C = ctx->impl;
+        AUSAXS_CUDA(cudaSetDevice(C.device));
+        C.io.ensure((size_t)n * 3 * 8 + 256);
+        double* d = C.io.as<double>();
+        AUSAXS_CUDA(cudaMemcpyAsync(d, data, (size_t)n * 8, cudaMemcpyHostToDevice, C.stream));
+        AUSAXS_CUDA(cudaMemcpyAsync(d + n, model, (size_t)n * 8, cudaMemcpyHostToDevice, C.stream));
+        AUSAXS_CUDA(cudaMemcpyAsync(d + 2 * n, err, (size_t)n * 8, cudaMemcpyHostToDevice, C.stream));
+        double* o = d + 3 * (size_t)n;
+        lsq_launch(d, d + n, d + 2 * n, n, o, C.stream);
+        C.check_launch("lsq");
+        AUSAXS_CUDA(cudaMemcpyAsync(out, o, 5 * 8, cudaMemcpyDeviceToHost, C.stream));
+        AUSAXS_CUDA(cudaStreamSynchronize(C.stream));
     });
 }
 

@@ -272,9 +272,14 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
     // Simple jobs) run with a small footprint and high occupancy, multi-row jobs (aa, aw, ax) get the
     // shared memory they need.  Tiles are numbered per group.
     P.pairs = 0;
-    std::vector<PairJob> group_jobs[2];
-    long long group_tiles[2] = {0, 0};
-    int group_rows[2] = {1, 1};
+    // Large structures: one launch per row class (1, T, T*T rows) so each gets the occupancy its
+    // footprint allows; small ones: everything in one launch (launch latency dominates).
+    long long all_pairs = 0;
+    for (auto& j : js) all_pairs += j.self ? (long long)j.na * (j.na - 1) / 2 : (long long)j.na * j.nbp;
+    const bool split = all_pairs >= 2000000000LL;
+    std::vector<PairJob> group_jobs[3];
+    long long group_tiles[3] = {0, 0, 0};
+    int group_rows[3] = {1, 1, 1};
     for (auto& j : js) {
         if (j.na == 0 || j.nbp == 0) continue;
         long long tiles = j.self ? tri(nt(j.na)) : (long long)nt(j.na) * nt(j.nbp);
@@ -283,7 +288,7 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
         P.pairs += pairs;
         for (int r0 = 0; r0 < j.rows; r0 += max_group_rows) {
             int r1 = std::min(j.rows, r0 + max_group_rows);
-            const int g = (r1 - r0) == 1 ? 0 : 1;
+            const int g = !split ? 0 : ((r1 - r0) == 1 ? 0 : ((r1 - r0) <= T ? 1 : 2));
             PairJob pj{};
             pj.A = j.A;
             pj.B = j.B;
@@ -312,12 +317,13 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
             group_rows[g] = std::max(group_rows[g], r1 - r0);
         }
     }
-    if (group_jobs[0].size() + group_jobs[1].size() > 64) throw Error{AUSAXS_ERR_CAPACITY, "too many row groups"};
+    if (group_jobs[0].size() + group_jobs[1].size() + group_jobs[2].size() > 64)
+        throw Error{AUSAXS_ERR_CAPACITY, "too many row groups"};
     const bool w_launch = mt;  // Simple histograms always carry weight sums (values)
     P.n_launch = 0;
     P.total_tiles = 0;
     size_t job_off = P.off_jobs;
-    for (int g = 0; g < 2; ++g) {
+    for (int g = 0; g < 3; ++g) {
         if (group_jobs[g].empty()) continue;
         Plan::Group& G = P.group[P.n_launch++];
         G.tile = tile;

@@ -52,7 +52,7 @@ struct Plan {
         PairLaunch launch{};
         int tile = 256, grid = 0;
         size_t smem = 0;
-    } group[2];
+    } group[3];
     int n_launch = 0;
     long long total_tiles = 0, pairs = 0;
     int R = 0;

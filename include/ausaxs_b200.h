@@ -191,6 +191,16 @@ AUSAXS_API int ausaxs_gpu_structure_histogram(ausaxs_gpu_ctx* ctx, ausaxs_gpu_st
                                    ausaxs_hist_result* out);
 
 /*
+ * Weighted linear least squares of a model against data plus chi-square, on the device:
+ * fitter::detail::LinearLeastSquares::fit (source/core/fitter/detail/LinearLeastSquares.cpp:26-55),
+ * fitting model ~ a * data + b with weights 1/err^2 as LinearFitter sets it up (the measured
+ * intensities as data, the model on the measured q as model; source/core/fitter/LinearFitter.cpp:14-21).
+ * Host pointers; out[5] = {a, b, sigma_a, sigma_b, chi2}.
+ */
+AUSAXS_API int ausaxs_gpu_linear_lsq(ausaxs_gpu_ctx* ctx, const double* data, const double* model, const double* err,
+                                     int32_t n, double* out);
+
+/*
  * Allocation-free Simple (weighted) histogram.  No counterpart in the reference: it exists for
  * callers that cannot allocate device memory while they run (a memory-pool-managed or real-time
  * section, or an embedding application that forbids cudaMalloc after start-up, since allocation can

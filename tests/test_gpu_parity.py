@@ -171,6 +171,18 @@ def test_cfg0_vs_oracle(gpu_ctx):
     np.testing.assert_allclose(I, Io, rtol=1e-6)
 
 
+def test_linear_lsq_vs_oracle(gpu_ctx):
+    rng = np.random.default_rng(4)
+    n = 400
+    target = 1e4 * np.exp(-np.linspace(0.005, 0.5, n) * 20)
+    err = 0.01 * target
+    model = 3.2 * target + 7.0 + rng.normal(0, 1, n) * err
+    g = _capi.linear_lsq(gpu_ctx, target, model, err)
+    o = O.linear_lsq(target, model, err)
+    np.testing.assert_allclose(g[[0, 1, 4]], o[[0, 1, 4]], rtol=1e-9)
+    np.testing.assert_allclose(g[[2, 3]], np.sqrt(o[[2, 3]]), rtol=1e-9)
+
+
 # ---- error behaviour -----------------------------------------------------------------------
 
 def test_unknown_form_factor_is_an_error(gpu_ctx):
