@@ -31,7 +31,8 @@ MANAGER_FFGRID = 4
 # every symbol include/ausaxs_b200.h declares
 EXPORTED = [
     "ausaxs_gpu_ctx_create", "ausaxs_gpu_ctx_destroy", "ausaxs_gpu_ctx_set_stream", "ausaxs_gpu_ctx_launch_count",
-    "ausaxs_gpu_last_error", "ausaxs_gpu_ctx_enable_timing", "ausaxs_gpu_ctx_kernel_time", "ausaxs_gpu_histogram", "ausaxs_gpu_debye", "ausaxs_gpu_profile",
+    "ausaxs_gpu_last_error", "ausaxs_gpu_ctx_enable_timing", "ausaxs_gpu_ctx_kernel_time",
+    "ausaxs_gpu_ctx_fp64_columns", "ausaxs_gpu_ctx_tc_error_estimate", "ausaxs_gpu_histogram", "ausaxs_gpu_debye", "ausaxs_gpu_profile",
     "ausaxs_gpu_structure_create", "ausaxs_gpu_structure_destroy", "ausaxs_gpu_structure_profile",
     "ausaxs_gpu_structure_histogram", "ausaxs_gpu_histogram_mt_noalloc", "ausaxs_gpu_linear_lsq",
 ]
@@ -85,6 +86,8 @@ def load():
         L.ausaxs_gpu_ctx_launch_count.restype = C.c_int64
         L.ausaxs_gpu_ctx_enable_timing.argtypes = [vp, C.c_int32]
         L.ausaxs_gpu_ctx_kernel_time.argtypes = [vp, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+        L.ausaxs_gpu_ctx_fp64_columns.argtypes = [vp, C.POINTER(C.c_int32)]
+        L.ausaxs_gpu_ctx_tc_error_estimate.argtypes = [vp, C.POINTER(C.c_double), C.c_int32]
         L.ausaxs_gpu_histogram.argtypes = [vp, C.POINTER(HistConfig), f32, C.c_int32, f32, C.c_int32, f32, C.c_int32,
                                            C.POINTER(HistResult)]
         L.ausaxs_gpu_debye.argtypes = [vp, C.POINTER(HistConfig), C.POINTER(HistResult), f64, C.c_int32,
@@ -154,8 +157,19 @@ class Context:
     def enable_timing(self, on: bool = True):
         check(load().ausaxs_gpu_ctx_enable_timing(self.h, int(on)))
 
+    def fp64_columns(self) -> int:
+        n = C.c_int32(0)
+        check(load().ausaxs_gpu_ctx_fp64_columns(self.h, C.byref(n)))
+        return n.value
+
+    def tc_error_estimate(self, nq: int):
+        out = np.zeros(nq)
+        check(load().ausaxs_gpu_ctx_tc_error_estimate(self.h, out.ctypes.data_as(C.POINTER(C.c_double)), nq))
+        return out
+
     def kernel_time(self, cls: int):
-        """(total ms, launches) of a kernel class: 0 pair histograms, 1 finalisation, 2 Debye."""
+        """(total ms, launches) of a kernel class: 0 pair histograms, 1 finalisation, 2 FP64 Debye,
+        3 tensor-core Debye."""
         ms = C.c_double(0)
         n = C.c_int64(0)
         check(load().ausaxs_gpu_ctx_kernel_time(self.h, cls, C.byref(ms), C.byref(n)))

@@ -134,11 +134,27 @@ int ausaxs_gpu_ctx_enable_timing(ausaxs_gpu_ctx* ctx, int32_t enable) {
 
 int ausaxs_gpu_ctx_kernel_time(ausaxs_gpu_ctx* ctx, int32_t kernel_class, double* ms, int64_t* launches) {
     return guarded([&] {
-        if (!ctx || kernel_class < 0 || kernel_class > 2) throw Error{AUSAXS_ERR_ARGUMENT, "bad argument"};
+        if (!ctx || kernel_class < 0 || kernel_class > 3) throw Error{AUSAXS_ERR_ARGUMENT, "bad argument"};
         Ctx& C = ctx->impl;
         C.time_collect();
         if (ms) *ms = C.timed[kernel_class].ms;
         if (launches) *launches = C.timed[kernel_class].count;
+    });
+}
+
+int ausaxs_gpu_ctx_fp64_columns(ausaxs_gpu_ctx* ctx, int32_t* n) {
+    return guarded([&] {
+        if (!ctx || !n) throw Error{AUSAXS_ERR_ARGUMENT, "null argument"};
+        *n = ctx->impl.last_fp64_columns;
+    });
+}
+
+int ausaxs_gpu_ctx_tc_error_estimate(ausaxs_gpu_ctx* ctx, double* out, int32_t nq) {
+    return guarded([&] {
+        if (!ctx || (nq > 0 && !out)) throw Error{AUSAXS_ERR_ARGUMENT, "null argument"};
+        const auto& e = ctx->impl.last_tc_err;
+        if ((size_t)nq != e.size()) throw Error{AUSAXS_ERR_ARGUMENT, "nq differs from the last precision-0 transform"};
+        std::copy(e.begin(), e.end(), out);
     });
 }
 

@@ -114,22 +114,42 @@ __global__ void __launch_bounds__(kThreads) debye_kernel(DebyeArgs A) {
     __syncthreads();
 
     // With tensor-core values: keep this q unless the estimated error is above tolerance.
-    if (threadIdx.x == 0) s_fp64 = 1;
+    if (threadIdx.x == 0) {
+        s_fp64 = 1;
+        if (A.tc_err_est) A.tc_err_est[k] = INFINITY;  // overwritten below when tensor-core values exist
+    }
     __syncthreads();
-    if (A.sinqd_tc && warp == 0) {
+    if (A.sinqd_tc && !(A.tc_error && *A.tc_error) && warp == 0) {
+        // Error bound of the tensor-core values, per row: c_rel * sum_b |H||S| + c_abs * sum_b |H|.
+        //  * c_rel, operand representation: H to FP32 (2^-24), FP32 sinc value (sinf 2 ulp, the
+        //    division 2^-24), the BF16 products dropped by the split (< 2^-25), the main+correction
+        //    sum and the FP32 partial (2^-24 each): < 2^-21 in total;
+        //  * c_rel, accumulation: at most one rounding of the main accumulator per 16-bin K step
+        //    (truncation allowed: 2^-23 of a magnitude no larger than twice the bound), the
+        //    correction accumulator's terms are 2^-8 smaller;
+        //  * c_abs: the FP32 argument q*d carries 3 roundings, i.e. |dx| <= 3 * 2^-24 x, and
+        //    |d sinc/dx| <= 2/x, so |d sinc| <= 1.5 * 2^-22 for every x;
+        //  * 10 % slack for the FP32 bound and row sums themselves.
+        const int per = debye_tc_split_bins(mb, A.tc_splits);
+        const double c_rel = (0x1p-21 + (per / 16 + 1) * 0x1p-22) * 1.1;
+        const double c_abs = 0x1p-21 * 1.1;
+        const size_t plane = static_cast<size_t>(R) * A.nq;
         double I = 0, err = 0;
         for (int r = lane; r < R; r += 32) {
             int p;
             double cf = row_coef(A, A.rows[r], s_F, p);
             double sgn = (p == 1 || p == 4) ? -1.0 : 1.0;
-            double v = A.sinqd_tc[static_cast<size_t>(r) * A.nq + k];
-            double bnd = A.bound_tc[static_cast<size_t>(r) * A.nq + k];
+            double v = 0, bnd = 0, ha = 0;
+            for (int z = 0; z < A.tc_splits; ++z) {
+                v += A.sinqd_tc[z * plane + static_cast<size_t>(r) * A.nq + k];
+                bnd += A.bound_tc[z * plane + static_cast<size_t>(r) * A.nq + k];
+                ha += A.habs_tc[static_cast<size_t>(z) * R + r];
+            }
+            s_acc[r] = v;
             if (A.rows[r].kind == kRowSAW) cf *= A.cw;
             if (A.rows[r].kind == kRowSWW) cf *= A.cw * A.cw;
             I += sgn * cf * v;
-            // split-BF16 operands carry 16 significant bits each; FP32 accumulation adds
-            // ~sqrt(K) 2^-24 relative: 2^-14 of the absolute-value sum bounds both
-            err += fabs(cf) * bnd * (1.0 / 16384.0);
+            err += fabs(cf) * (c_rel * bnd + c_abs * ha);
         }
         for (int o = 16; o > 0; o >>= 1) {
             I += __shfl_xor_sync(0xffffffffu, I, o);
@@ -139,11 +159,14 @@ __global__ void __launch_bounds__(kThreads) debye_kernel(DebyeArgs A) {
             bool ok = err <= A.tolerance * fabs(I);
             s_fp64 = ok ? 0 : 1;
             if (!ok && A.fp64_columns) atomicAdd(A.fp64_columns, 1);
+            if (A.tc_err_est) A.tc_err_est[k] = fabs(I) > 0 ? err / fabs(I) : INFINITY;
         }
     }
     __syncthreads();
 
     if (s_fp64) {
+        for (int r = threadIdx.x; r < R; r += kThreads) s_acc[r] = 0;
+        __syncthreads();
         int used_groups = 1;
         for (int r = 0; r < R; ++r) used_groups = max(used_groups, A.rows[r].group + 1);
         for (int c0 = 0; c0 < mb; c0 += kChunk) {
@@ -164,9 +187,6 @@ __global__ void __launch_bounds__(kThreads) debye_kernel(DebyeArgs A) {
             }
             __syncthreads();
         }
-    } else {
-        for (int r = threadIdx.x; r < R; r += kThreads) s_acc[r] = A.sinqd_tc[static_cast<size_t>(r) * A.nq + k];
-        __syncthreads();
     }
 
     if (warp == 0) {

@@ -37,10 +37,16 @@ struct DebyeArgs {
     double cw, cx, crho, dw_atomic, dw_exv, grid_volume;
     const double* q;
     int32_t nq;
-    const float* sinqd_tc;      // [R][nq] from the tensor-core contraction, or null (FP64 everywhere)
-    const float* bound_tc;      // [R][nq] sum_b |H| |sinc| estimate, or null
+    // tensor-core partial sums from debye_tc_launch, or null (FP64 for every q):
+    //   sinqd_tc [splits][R][nq], bound_tc [splits][R][nq] (sum_b |H| |sinc|), habs_tc [splits][R] (sum_b |H|)
+    const float* sinqd_tc;
+    const float* bound_tc;
+    const float* habs_tc;
+    int32_t tc_splits;          // K splits of the bin range
+    const int32_t* tc_error;    // non-zero: the tensor-core values are unusable (FP64 for every q)
     double tolerance;           // relative I(q) error target when sinqd_tc is given
     int32_t* fp64_columns;      // out: number of q recomputed in FP64 (may be null)
+    double* tc_err_est;         // out: [nq] estimated relative error of the tensor-core I(q) (may be null)
     double* Iq;                 // [nq]
     double* profiles;           // [6][nq] or null
 };
@@ -48,10 +54,10 @@ struct DebyeArgs {
 void debye_fp64_launch(const DebyeArgs& A, cudaStream_t s);
 
 // Split-BF16 tensor-core contraction sinqd[r][q] = sum_b H[r][b] sinc(q d_{g(r)}[b]) for all rows,
-// with a bound sum_b |H||sinc| per element; returns false when the launch could not be made
-// (then callers use the FP64 path).
+// with the bound sum_b |H||sinc| per element (debye_tc.cu).  Returns false when the launch could not
+// be made (callers then use FP64 for every q).
 struct TcArgs {
-    int32_t R, nb;
+    int32_t R, nb, nq;
     const double* H;
     const double* axis0;
     const double* axis1;
@@ -59,15 +65,21 @@ struct TcArgs {
     const RowDesc* rows;
     const int32_t* max_bin;
     const double* q;
-    int32_t nq;
-    float* sinqd;  // [R][nq]
-    float* bound;  // [R][nq]
-    // scratch
-    unsigned short* a_hi;  // [Mpad][Kpad] bf16 packed in UMMA layout
-    unsigned short* a_lo;
-    int32_t kpad, mpad;
+    int32_t groups_present;  // bit g: some row uses distance axis g
+    int32_t splits;          // K splits of the bin range (tc_splits)
+    float* sinqd;            // [splits][R][nq]
+    float* bound;            // [splits][R][nq]
+    float* habs;             // [splits][R]
+    int32_t* error_flag;
 };
-bool debye_tc_launch(const TcArgs& A, int bins_hint, cudaStream_t s);
-size_t debye_tc_scratch_bytes(int R, int bins_hint);
+bool debye_tc_launch(const TcArgs& A, cudaStream_t s);
+// K splits for a contraction of up to `bins` bins, R rows and nq q values (fills the SMs once)
+int debye_tc_splits(int R, int bins, int nq, int sms);
+// bins of one K split when max_bin bins are in use (multiple of the 64-bin staging chunk)
+__host__ __device__ inline int debye_tc_split_bins(int max_bin, int splits) {
+    const int chunks = (max_bin + 63) / 64;
+    return ((chunks + splits - 1) / splits) * 64;
+}
+size_t debye_tc_smem_bytes();
 
 }  // namespace ausaxs_b200

@@ -490,13 +490,63 @@ void Structure::enqueue_debye(const ausaxs_hist_config& cfg, const double* q_dev
     A.fp64_columns = reinterpret_cast<int32_t*>(base + P.off_fp64cols);
     A.Iq = Iq_dev;
     A.profiles = prof_dev;
-    if (nq > 0) {
+    int groups = 1;
+    if (grid) groups = 7;
+    run_debye(*ctx, A, groups, P.tc, p.precision);
+}
+
+void run_debye(Ctx& C, DebyeArgs& A, int groups_present, DevBuf& tc, int precision) {
+    if (A.nq <= 0) return;
+    cudaStream_t s = C.stream;
+    if (precision == 0) {
+        // split-BF16 tensor-core contraction for every q, FP64 re-evaluation of the flagged ones
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, C.device);
+        const int splits = debye_tc_splits(A.R, A.nb, A.nq, sms);
+        const size_t plane = (size_t)A.R * A.nq;
+        const size_t n = (size_t)splits * plane;
+        const size_t bytes_v = align_up(n * 4, 256), bytes_h = align_up((size_t)splits * A.R * 4, 256);
+        tc.ensure(2 * bytes_v + bytes_h + 256);
+        float* sq = tc.as<float>();
+        float* bd = reinterpret_cast<float*>(tc.as<char>() + bytes_v);
+        float* ha = reinterpret_cast<float*>(tc.as<char>() + 2 * bytes_v);
+        int32_t* flag = reinterpret_cast<int32_t*>(tc.as<char>() + 2 * bytes_v + bytes_h);
+        AUSAXS_CUDA(cudaMemsetAsync(flag, 0, 4, s));
+        TcArgs T{};
+        T.R = A.R;
+        T.nb = A.nb;
+        T.nq = A.nq;
+        T.H = A.H;
+        T.axis0 = A.axis0;
+        T.axis1 = A.axis1;
+        T.axis2 = A.axis2;
+        T.rows = A.rows;
+        T.max_bin = A.max_bin;
+        T.q = A.q;
+        T.groups_present = groups_present;
+        T.splits = splits;
+        T.sinqd = sq;
+        T.bound = bd;
+        T.habs = ha;
+        T.error_flag = flag;
         cudaEvent_t ev;
-        ctx->time_begin(2, &ev);
-        debye_fp64_launch(A, ctx->stream);
-        ctx->check_launch("debye");
-        ctx->time_end(2, ev);
+        C.time_begin(3, &ev);
+        const bool ok = debye_tc_launch(T, s);
+        if (ok) C.check_launch("debye_tc");
+        C.time_end(3, ev);
+        if (ok) {
+            A.sinqd_tc = sq;
+            A.bound_tc = bd;
+            A.habs_tc = ha;
+            A.tc_splits = splits;
+            A.tc_error = flag;
+        }
     }
+    cudaEvent_t ev;
+    C.time_begin(2, &ev);
+    debye_fp64_launch(A, s);
+    C.check_launch("debye");
+    C.time_end(2, ev);
 }
 
 void Structure::read_histogram(const ausaxs_hist_config& cfg, ausaxs_hist_result* out) {
@@ -591,7 +641,8 @@ void debye_of_host_histogram(Ctx& C, const ausaxs_hist_config& cfg, const ausaxs
     size_t off_ax1 = off_ax0 + align_up((size_t)mb * 8, 256), off_ax2 = off_ax1 + align_up((size_t)mb * 8, 256);
     size_t off_rows = off_ax2 + align_up((size_t)mb * 8, 256), off_mb = off_rows + align_up(sizeof(RowDesc) * R, 256);
     size_t off_q = off_mb + 256, off_I = off_q + align_up((size_t)nq * 8, 256), off_P = off_I + align_up((size_t)nq * 8, 256);
-    size_t total = off_P + align_up((size_t)nq * 6 * 8, 256);
+    size_t off_E = off_P + align_up((size_t)nq * 6 * 8, 256);
+    size_t total = off_E + align_up((size_t)nq * 8, 256);
     C.io.ensure(total);
     char* base = C.io.as<char>();
     cudaStream_t s = C.stream;
@@ -627,11 +678,21 @@ void debye_of_host_histogram(Ctx& C, const ausaxs_hist_config& cfg, const ausaxs
     A.tolerance = p.tolerance > 0 ? p.tolerance : 1e-5;
     A.Iq = reinterpret_cast<double*>(base + off_I);
     A.profiles = profiles ? reinterpret_cast<double*>(base + off_P) : nullptr;
+    int32_t* cols = reinterpret_cast<int32_t*>(base + off_mb) + 1;
+    AUSAXS_CUDA(cudaMemsetAsync(cols, 0, 4, s));
+    A.fp64_columns = cols;
+    A.tc_err_est = p.precision == 0 ? reinterpret_cast<double*>(base + off_E) : nullptr;
+    C.last_tc_err.assign(p.precision == 0 ? nq : 0, INFINITY);
     if (nq > 0) {
-        debye_fp64_launch(A, s);
-        C.check_launch("debye");
+        run_debye(C, A, grid ? 7 : 1, C.tc, p.precision);
+        int32_t ncols = 0;
+        AUSAXS_CUDA(cudaMemcpyAsync(&ncols, cols, 4, cudaMemcpyDeviceToHost, s));
         AUSAXS_CUDA(cudaMemcpyAsync(Iq, base + off_I, (size_t)nq * 8, cudaMemcpyDeviceToHost, s));
         if (profiles) AUSAXS_CUDA(cudaMemcpyAsync(profiles, base + off_P, (size_t)nq * 6 * 8, cudaMemcpyDeviceToHost, s));
+        if (p.precision == 0)
+            AUSAXS_CUDA(cudaMemcpyAsync(C.last_tc_err.data(), base + off_E, (size_t)nq * 8, cudaMemcpyDeviceToHost, s));
+        AUSAXS_CUDA(cudaStreamSynchronize(s));
+        C.last_fp64_columns = p.precision == 0 ? ncols : nq;
     }
     AUSAXS_CUDA(cudaStreamSynchronize(s));
 }

@@ -107,7 +107,7 @@ struct Ctx {
         std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
         double ms = 0;
         long long count = 0;
-    } timed[3];
+    } timed[4];
     void time_begin(int cls, cudaEvent_t* ev);
     void time_end(int cls, cudaEvent_t ev);
     void time_collect();
@@ -115,8 +115,14 @@ struct Ctx {
     PrepStats* h_stats = nullptr;  // pinned
     std::unique_ptr<Structure> scratch;
     DevBuf io;                     // q / I(q) / profiles of one-shot host calls
+    DevBuf tc;                     // tensor-core scratch of one-shot host calls
+    int last_fp64_columns = 0;     // q values the last host transform evaluated in FP64
+    std::vector<double> last_tc_err;  // per q: estimated relative error of its tensor-core value
     void check_launch(const char* what);
 };
+
+// Tensor-core contraction (precision 0) followed by the FP64 epilogue, or FP64 only (precision 1).
+void run_debye(Ctx& C, DebyeArgs& A, int groups_present, DevBuf& tc, int precision);
 
 // CompositeDistanceHistogram*::debye_transform() of a histogram given in the reference's host
 // layouts (ausaxs_hist_result): compacts the rows of the form-factor types present, uploads them

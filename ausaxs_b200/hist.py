@@ -111,6 +111,10 @@ class _Composite:
         self.pairs = int(res["pairs"])
         self.free = dict(cw=1.0, cx=1.0, crho=1.0, dw_atomic=0.0, dw_exv=0.0)
         self.grid_width = 1.0
+        # 0: split-BF16 tensor cores + FP64 for the q whose error estimate exceeds `tolerance`;
+        # 1: FP64 for every q
+        self.precision = 1
+        self.tolerance = 1e-5
 
     # DistanceHistogram interface
     def get_d_axis(self) -> np.ndarray:
@@ -130,10 +134,10 @@ class _Composite:
             setattr(r, name, dptr(self._keep.get(name)))
         return r
 
-    def _transform(self, q, precision: int = 1):
+    def _transform(self, q):
         q = default_q_axis() if q is None else np.ascontiguousarray(q, np.float64)
         p = DebyeParams(self.free["cw"], self.free["cx"], self.free["crho"], self.free["dw_atomic"],
-                        self.free["dw_exv"], self.grid_width, precision, 1e-5)
+                        self.free["dw_exv"], self.grid_width, self.precision, self.tolerance)
         I = np.zeros(len(q))
         prof = np.zeros(6 * len(q))
         r = self._result()
@@ -324,14 +328,14 @@ class HistogramManagerMTFFGrid(_Manager):
 
 
 def profile(manager: _Manager, q, cw=1.0, cx=1.0, crho=1.0, dw_atomic=0.0, dw_exv=0.0, grid_width=1.0,
-            precision: int = 1, with_profiles: bool = False):
+            precision: int = 1, with_profiles: bool = False, tolerance: float = 1e-5):
     """Coordinates -> I(q) in one call (Molecule::get_histogram()->debye_transform()): only I(q) leaves the device."""
     cfg = manager.config()
     a, w, x = manager._inputs()
     q = np.ascontiguousarray(q, np.float64)
     I = np.zeros(len(q))
     prof = np.zeros(6 * len(q)) if with_profiles else None
-    p = DebyeParams(cw, cx, crho, dw_atomic, dw_exv, grid_width, precision, 1e-5)
+    p = DebyeParams(cw, cx, crho, dw_atomic, dw_exv, grid_width, precision, tolerance)
     check(load().ausaxs_gpu_profile(manager.ctx.h, C.byref(cfg), fptr(a), len(a), fptr(w), len(w), fptr(x),
                                     0 if x is None else len(x), dptr(q), len(q), C.byref(p), dptr(I), dptr(prof)))
     return (I, prof.reshape(6, len(q))) if with_profiles else I

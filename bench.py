@@ -177,7 +177,9 @@ def run_ours(args, rank, world, local_rank):
     cfg = mgr.config()
     A, W, X = mgr._inputs()
     pairs = pair_count(m, grid)
-    params = _capi.DebyeParams(1.0, 1.0, 1.0, 0.0, 0.0, 1.0, 1, 1e-5)
+    # precision 0: split-BF16 tensor-core transform, FP64 for every q whose rigorous error bound
+    # exceeds the tolerance (the path's I(q) bar, 1e-4 relative to the FP64 transform)
+    params = _capi.DebyeParams(1.0, 1.0, 1.0, 0.0, 0.0, 1.0, args.precision, args.tolerance)
     nq = len(wl.q)
     q_dev = torch.tensor(wl.q, dtype=torch.float64, device=f"cuda:{local_rank}")
     I_dev = torch.zeros(nq, dtype=torch.float64, device=f"cuda:{local_rank}")
@@ -217,6 +219,11 @@ def run_ours(args, rank, world, local_rank):
         total_ms = float(t.item())
     value = world * args.steps / (total_ms / 1e3)
     I_gpu = I_dev.cpu().numpy()
+    # the same structure through the FP64 transform: deviation of the timed result
+    I_64 = torch.zeros_like(I_dev)
+    st.profile_device(cfg, q_dev, nq, _capi.DebyeParams(1.0, 1.0, 1.0, 0.0, 0.0, 1.0, 1, 1e-5), I_64)
+    torch.cuda.synchronize()
+    iq_dev_fp64 = float(np.max(np.abs(I_gpu / I_64.cpu().numpy() - 1)))
 
     # end to end through the host C ABI with pinned buffers
     pin_a = torch.from_numpy(A).pin_memory()
@@ -262,6 +269,8 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": wl.name, "atoms": m.size_atom(), "waters": m.size_water(),
                    "exv": 0 if m.exv is None or not grid else len(m.exv), "pairs_per_profile": pairs,
                    "bin_width": wl.bin_width, "q_points": nq, "manager": wl.manager,
+                   "transform": {"precision": args.precision, "tolerance": args.tolerance,
+                                 "max_rel_diff_vs_fp64_transform": iq_dev_fp64},
                    "l2": "256 MiB buffer written between timed steps (outside the events)",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(A.nbytes + W.nbytes + (X.nbytes if grid else 0) + pin_q.numel() * 8),
@@ -315,6 +324,8 @@ def main():
     ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--atomic-peak", action="store_true")
+    ap.add_argument("--precision", type=int, default=0, choices=[0, 1])
+    ap.add_argument("--tolerance", type=float, default=1e-4)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

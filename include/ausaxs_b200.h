@@ -77,10 +77,18 @@ AUSAXS_API const char* ausaxs_gpu_last_error(void);
  * Optional kernel timing (instrumentation, no counterpart in the reference): with timing enabled,
  * every later launch of a kernel class is bracketed by CUDA events on the context's stream.
  * ausaxs_gpu_ctx_kernel_time synchronises the stream and returns the accumulated device time (ms)
- * and number of launches of one class: 0 = pair histograms, 1 = finalisation, 2 = Debye transform.
+ * and number of launches of one class: 0 = pair histograms, 1 = finalisation, 2 = FP64 Debye
+ * epilogue, 3 = tensor-core Debye contraction.
+ * ausaxs_gpu_ctx_fp64_columns: how many q values the last ausaxs_gpu_debye call evaluated in FP64
+ * (all of them with precision 1; those whose tensor-core error estimate exceeded the tolerance with
+ * precision 0).
  */
 AUSAXS_API int ausaxs_gpu_ctx_enable_timing(ausaxs_gpu_ctx* ctx, int32_t enable);
 AUSAXS_API int ausaxs_gpu_ctx_kernel_time(ausaxs_gpu_ctx* ctx, int32_t kernel_class, double* ms, int64_t* launches);
+AUSAXS_API int ausaxs_gpu_ctx_fp64_columns(ausaxs_gpu_ctx* ctx, int32_t* n);
+/* Per q of the last ausaxs_gpu_debye call with precision 0: the rigorous bound on the relative error
+ * of the tensor-core I(q) (before any FP64 re-evaluation); INFINITY where none was formed. */
+AUSAXS_API int ausaxs_gpu_ctx_tc_error_estimate(ausaxs_gpu_ctx* ctx, double* out, int32_t nq);
 
 /*
  * Histogram configuration: the global settings the reference reads during calculate_all().

@@ -1,0 +1,102 @@
+"""Split-BF16 tensor-core Debye contraction (precision 0) against the FP64 path and the oracle.
+
+Bar: with precision 0 every q either keeps its tensor-core value, when the rigorous error bound the
+kernel forms is within the tolerance, or is re-evaluated in FP64; so I(q) is within the tolerance
+(1e-4 relative, the path's stated I(q) bar) of the FP64 result everywhere.  The bound itself is
+checked: with an infinite tolerance (tensor-core values only) the actual deviation from FP64 never
+exceeds it.
+"""
+import numpy as np
+import pytest
+
+from ausaxs_b200 import hist, synth
+from oracle import py as O
+from tests.helpers import golden_cases, load_golden
+from tests.test_gpu_parity import manager_for
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-4
+
+
+def _pair(h, q, ctx, tolerance):
+    h.precision, h.tolerance = 1, 1e-5
+    _, I64 = h.debye_transform(q)
+    p64 = h.profiles(q)
+    h.precision, h.tolerance = 0, tolerance
+    _, Itc = h.debye_transform(q)
+    return I64, p64, Itc
+
+
+def _cases(ctx):
+    out = []
+    for name in [c for c in golden_cases() if "ffexplicit" not in c]:
+        g = load_golden(name)
+        h = manager_for(g, ctx).calculate_all()
+        cw, cx, crho, dwa, dwx = g["params"]
+        h.apply_water_scaling_factor(cw)
+        if str(g["manager"]) != "mt":
+            h.apply_excluded_volume_scaling_factor(cx)
+            h.apply_solvent_density_scaling_factor(crho)
+            h.apply_atomic_debye_waller_factor(dwa)
+            h.apply_exv_debye_waller_factor(dwx)
+        out.append((name, h, np.asarray(g["q"])))
+    w = synth.cfg0()
+    out.append(("cfg0", hist.HistogramManagerMTFFAvg(w.molecules[0], True, 0.25, 8000, ctx).calculate_all(), w.q))
+    rng = np.random.default_rng(3)
+    xyz = rng.normal(0, 14, (3000, 3))
+    ff = rng.choice([3, 7, 11, 12], 3000).astype(np.int32)
+    m = hist.Molecule(atoms=xyz, ff_types=ff, waters=rng.normal(0, 16, (600, 3)),
+                      exv=np.round(rng.uniform(-14, 14, (4000, 3))), volume=1.0)
+    out.append(("ffgrid", hist.HistogramManagerMTFFGrid(m, 0.1, 8000, ctx).calculate_all(),
+                np.linspace(0.002, 1.0, 700)))
+    return out
+
+
+def test_tc_bound_covers_actual_error(gpu_ctx):
+    worst = 0.0
+    for name, h, q in _cases(gpu_ctx):
+        I64, _, Itc = _pair(h, q, gpu_ctx, 1e30)
+        assert gpu_ctx.fp64_columns() == 0, name
+        est = gpu_ctx.tc_error_estimate(len(q))
+        assert np.all(np.isfinite(est) | (Itc == 0)), name
+        dev = np.abs(Itc - I64) / np.maximum(np.abs(Itc), 1e-300)
+        ok = dev <= est
+        assert ok.all(), (name, np.flatnonzero(~ok)[:5], dev[~ok][:5], est[~ok][:5])
+        worst = max(worst, float(np.max(dev / np.maximum(est, 1e-300))))
+    print(f"largest actual/bound ratio {worst:.3g}")
+
+
+def test_tc_within_tolerance_of_fp64(gpu_ctx):
+    for name, h, q in _cases(gpu_ctx):
+        I64, _, Itc = _pair(h, q, gpu_ctx, TOL)
+        np.testing.assert_allclose(Itc, I64, rtol=TOL, atol=0, err_msg=name)
+        n64 = gpu_ctx.fp64_columns()
+        assert 0 <= n64 <= len(q)
+        print(f"{name}: {n64}/{len(q)} q in FP64")
+
+
+def test_tc_profile_vs_oracle_cfg0(gpu_ctx):
+    w = synth.cfg0()
+    m = w.molecules[0]
+    mgr = hist.HistogramManagerMTFFAvg(m, True, 0.25, 8000, gpu_ctx)
+    I = hist.profile(mgr, w.q, precision=0, tolerance=TOL)
+    A, W, _ = m.compact_ff()
+    o = O.hist_ff(0, A, W, None, 0.25, 8000, m.volume * 0.334 / m.size_atom())
+    Io, _ = O.debye_ff(0, o, w.q)
+    np.testing.assert_allclose(I, Io, rtol=TOL)
+
+
+def test_tc_large_counts_and_many_bins(gpu_ctx):
+    # 20,000 atoms at 0.1 A bins: counts up to ~1e5 per bin and ~1,500 bins in use
+    rng = np.random.default_rng(8)
+    xyz = rng.normal(0, 25, (20000, 3))
+    ff = rng.choice([3, 7, 11], 20000).astype(np.int32)
+    m = hist.Molecule(atoms=xyz, ff_types=ff, waters=rng.normal(0, 28, (2000, 3)), volume=20000 * 18.0)
+    h = hist.HistogramManagerMTFFAvg(m, True, 0.1, 8000, gpu_ctx).calculate_all()
+    q = np.linspace(1e-4, 1.0, 1000)
+    I64, _, Itc = _pair(h, q, gpu_ctx, TOL)
+    np.testing.assert_allclose(Itc, I64, rtol=TOL, atol=0)
+    I64, _, Itc = _pair(h, q, gpu_ctx, 1e30)
+    est = gpu_ctx.tc_error_estimate(len(q))
+    assert np.all(np.abs(Itc - I64) <= est * np.abs(Itc))
