@@ -86,8 +86,7 @@ __device__ double row_coef(const DebyeArgs& A, const RowDesc& r, const QFactors&
     return 0;
 }
 
-__global__ void __launch_bounds__(kThreads) debye_kernel(DebyeArgs A) {
-    const int k = blockIdx.x;
+__device__ void debye_body(const DebyeArgs& A, const int k) {
     if (k >= A.nq) return;
     const double q = A.q[k];
     const int R = A.R;
@@ -219,8 +218,15 @@ __global__ void __launch_bounds__(kThreads) debye_kernel(DebyeArgs A) {
     }
 }
 
+__global__ void __launch_bounds__(kThreads) debye_kernel(DebyeArgs A) { debye_body(A, blockIdx.x); }
+// batched: blockIdx.y selects the structure
+__global__ void __launch_bounds__(kThreads) debye_batch_kernel(const DebyeArgs* As) { debye_body(As[blockIdx.y], blockIdx.x); }
+
 }  // namespace
 
 void debye_fp64_launch(const DebyeArgs& A, cudaStream_t s) { debye_kernel<<<A.nq, kThreads, 0, s>>>(A); }
+void debye_fp64_batch_launch(const DebyeArgs* As_dev, int n, int max_nq, cudaStream_t s) {
+    debye_batch_kernel<<<dim3(max_nq, n), kThreads, 0, s>>>(As_dev);
+}
 
 }  // namespace ausaxs_b200

@@ -139,6 +139,43 @@ void Structure::load(const float* atoms, int n_atoms, const float* waters, int n
 
 static long long tri(long long t) { return t * (t + 1) / 2; }
 
+void append_pair_jobs(const Plan& P, int tile, bool by_class, std::vector<PairJob> (&jobs)[3], long long (&tiles)[3],
+                      int (&rows)[3]) {
+    auto nt = [tile](int n) { return (n + tile - 1) / tile; };
+    for (const JobSpec& j : P.specs) {
+        const long long t = j.self ? tri(nt(j.na)) : (long long)nt(j.na) * nt(j.nbp);
+        for (int r0 = 0; r0 < j.rows; r0 += P.max_group_rows) {
+            const int r1 = std::min(j.rows, r0 + P.max_group_rows);
+            const int g = !by_class ? 0 : ((r1 - r0) == 1 ? 0 : ((r1 - r0) <= P.T ? 1 : 2));
+            PairJob pj{};
+            pj.A = j.A;
+            pj.B = j.B;
+            pj.na = j.na;
+            pj.nb = j.nbp;
+            pj.self = j.self;
+            pj.row_mode = j.rmode;
+            pj.types = P.T;
+            pj.row_lo = r0;
+            pj.row_hi = r1;
+            pj.nbins = P.nb;
+            pj.tiles_i = nt(j.na);
+            pj.tiles_j = nt(j.nbp);
+            pj.tile_begin = tiles[g];
+            pj.tile_count = t;
+            pj.inv_w = P.inv_w;
+            pj.c = P.c;
+            pj.scale = P.scale;
+            pj.counts = j.counts + (size_t)r0 * P.nb;
+            pj.dsum = r0 == 0 ? j.dsum : nullptr;
+            pj.wsum = r0 == 0 ? j.wsum : nullptr;
+            pj.wscale = 0;  // read from device memory by weighted launches
+            jobs[g].push_back(pj);
+            tiles[g] += t;
+            rows[g] = std::max(rows[g], r1 - r0);
+        }
+    }
+}
+
 Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
     Plan& P = plan;
     if (cfg.bin_width <= 0 || cfg.bin_count <= 0) throw Error{AUSAXS_ERR_ARGUMENT, "bin_width and bin_count must be positive"};
@@ -215,8 +252,8 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
     // on-chip budget: split rows of a job into groups when its [rows][nb] counts do not fit
     const size_t smem_cap = 232448 - 1024;
     int max_group_rows = 1;
-    while (max_group_rows < 4096 && pairhist_smem_bytes(max_group_rows + 1, nb, weighted && mt, tile) <= smem_cap) ++max_group_rows;
-    if (pairhist_smem_bytes(1, nb, weighted && mt, tile) > smem_cap)
+    while (max_group_rows < 4096 && pairhist_smem_bytes(max_group_rows + 1, nb, weighted && mt, 512) <= smem_cap) ++max_group_rows;
+    if (pairhist_smem_bytes(1, nb, weighted && mt, 512) > smem_cap)
         throw Error{AUSAXS_ERR_CAPACITY, "too many distance bins for the on-chip histogram"};
 
     // layout
@@ -268,55 +305,40 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
     P.dev.ensure(off);
     char* base = P.dev.as<char>();
 
-    // Jobs split into launch groups by the rows they keep on chip: one-row jobs (ww, xx, wx and all
-    // Simple jobs) run with a small footprint and high occupancy, multi-row jobs (aa, aw, ax) get the
-    // shared memory they need.  Tiles are numbered per group.
+    // passes of this structure with their accumulators
+    P.specs.clear();
     P.pairs = 0;
-    // Large structures: one launch per row class (1, T, T*T rows) so each gets the occupancy its
-    // footprint allows; small ones: everything in one launch (launch latency dominates).
-    long long all_pairs = 0;
-    for (auto& j : js) all_pairs += j.self ? (long long)j.na * (j.na - 1) / 2 : (long long)j.na * j.nbp;
-    const bool split = all_pairs >= 2000000000LL;
-    std::vector<PairJob> group_jobs[3];
-    long long group_tiles[3] = {0, 0, 0};
-    int group_rows[3] = {1, 1, 1};
     for (auto& j : js) {
         if (j.na == 0 || j.nbp == 0) continue;
-        long long tiles = j.self ? tri(nt(j.na)) : (long long)nt(j.na) * nt(j.nbp);
         long long pairs = j.self ? (long long)j.na * (j.na - 1) / 2 : (long long)j.na * j.nbp;
         if (pairs == 0) continue;
         P.pairs += pairs;
-        for (int r0 = 0; r0 < j.rows; r0 += max_group_rows) {
-            int r1 = std::min(j.rows, r0 + max_group_rows);
-            const int g = !split ? 0 : ((r1 - r0) == 1 ? 0 : ((r1 - r0) <= T ? 1 : 2));
-            PairJob pj{};
-            pj.A = j.A;
-            pj.B = j.B;
-            pj.na = j.na;
-            pj.nb = j.nbp;
-            pj.self = j.self;
-            pj.row_mode = j.rmode;
-            pj.types = T;
-            pj.row_lo = r0;
-            pj.row_hi = r1;
-            pj.nbins = nb;
-            pj.tiles_i = nt(j.na);
-            pj.tiles_j = nt(j.nbp);
-            pj.tile_begin = group_tiles[g];
-            pj.tile_count = tiles;
-            pj.inv_w = P.inv_w;
-            pj.c = P.c;
-            pj.scale = P.scale;
-            pj.counts = reinterpret_cast<unsigned long long*>(base + slot_cnt[j.slot]) + (size_t)r0 * nb;
-            // offset sums only feed the weighted d-axis; weight sums are the Simple histogram's values
-            pj.dsum = (r0 == 0 && weighted) ? reinterpret_cast<unsigned long long*>(base + slot_ds[j.slot]) : nullptr;
-            pj.wsum = (mt && r0 == 0) ? reinterpret_cast<long long*>(base + slot_ws[j.slot]) : nullptr;
-            pj.wscale = 0;  // read from device memory by weighted launches (see below)
-            group_jobs[g].push_back(pj);
-            group_tiles[g] += tiles;
-            group_rows[g] = std::max(group_rows[g], r1 - r0);
-        }
+        JobSpec sp{};
+        sp.A = j.A;
+        sp.na = j.na;
+        sp.B = j.B;
+        sp.nbp = j.nbp;
+        sp.self = j.self;
+        sp.rmode = j.rmode;
+        sp.rows = j.rows;
+        sp.counts = reinterpret_cast<unsigned long long*>(base + slot_cnt[j.slot]);
+        // offset sums only feed the weighted d-axis; weight sums are the Simple histogram's values
+        sp.dsum = weighted ? reinterpret_cast<unsigned long long*>(base + slot_ds[j.slot]) : nullptr;
+        sp.wsum = mt ? reinterpret_cast<long long*>(base + slot_ws[j.slot]) : nullptr;
+        P.specs.push_back(sp);
     }
+    P.max_group_rows = max_group_rows;
+
+    // Jobs split into launch groups by the rows they keep on chip: one-row jobs (ww, xx, wx and all
+    // Simple jobs) run with a small footprint and high occupancy, multi-row jobs (aa, aw, ax) get the
+    // shared memory they need.  Large structures: one launch per row class (1, T, T*T rows) so each
+    // gets the occupancy its footprint allows; small ones: everything in one launch (launch latency
+    // dominates).  Tiles are numbered per group.
+    const bool split = P.pairs >= 2000000000LL;
+    std::vector<PairJob> group_jobs[3];
+    long long group_tiles[3] = {0, 0, 0};
+    int group_rows[3] = {1, 1, 1};
+    append_pair_jobs(P, tile, split, group_jobs, group_tiles, group_rows);
     if (group_jobs[0].size() + group_jobs[1].size() + group_jobs[2].size() > 64)
         throw Error{AUSAXS_ERR_CAPACITY, "too many row groups"};
     const bool w_launch = mt;  // Simple histograms always carry weight sums (values)

@@ -38,6 +38,19 @@ struct DevBuf {
 
 struct Ctx;
 
+// One pass of pair binning of a structure before it is cut into tiles: the two point sets, the
+// rows it increments, and where its global accumulators live.
+struct JobSpec {
+    const float4* A;
+    int na;
+    const float4* B;
+    int nbp;
+    int self, rmode, rows;
+    unsigned long long* counts;  // [rows][nb]
+    unsigned long long* dsum;    // [nb] or null
+    long long* wsum;             // [nb] or null
+};
+
 // Launch plan of one structure under one histogram configuration: job table, accumulator and
 // output layout, kernel shapes.  Built once, then enqueued any number of times without
 // allocation or synchronisation (so it can be captured in a CUDA graph).
@@ -64,6 +77,8 @@ struct Plan {
            off_expand_aa = 0, off_expand_aw = 0;
     FinalizeFF fin_ff{};
     FinalizeMT fin_mt{};
+    std::vector<JobSpec> specs;  // the structure's passes (tiled by append_pair_jobs)
+    int max_group_rows = 1;      // rows that fit on chip at once (for 512-point tiles)
     // tensor-core scratch
     DevBuf tc;
     int tc_nq = 0;
@@ -120,6 +135,12 @@ struct Ctx {
     std::vector<double> last_tc_err;  // per q: estimated relative error of its tensor-core value
     void check_launch(const char* what);
 };
+
+// Cuts the passes of a planned structure into tiles of `tile` points and appends them to launch
+// classes: 0 (one on-chip row), 1 (up to T rows), 2 (more), or all to class 0 when !by_class.
+// Tile ids continue from tiles[g]; rows[g] grows to the largest row group of class g.
+void append_pair_jobs(const Plan& P, int tile, bool by_class, std::vector<PairJob> (&jobs)[3], long long (&tiles)[3],
+                      int (&rows)[3]);
 
 // Tensor-core contraction (precision 0) followed by the FP64 epilogue, or FP64 only (precision 1).
 void run_debye(Ctx& C, DebyeArgs& A, int groups_present, DevBuf& tc, int precision);

@@ -30,7 +30,7 @@ __device__ __forceinline__ double weighted_bin(double dsum, double count, int b,
     return (static_cast<double>(dsum == 0) * dv + dsum) / static_cast<double>((cnt == 0) + cnt);
 }
 
-__global__ void ff_maxbin_kernel(FinalizeFF F) {
+__device__ void ff_maxbin_body(const FinalizeFF& F) {
     const int T = F.T;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(F.max_bin, 10);  // minimum size (HistogramManagerMT.cpp:48)
     for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < F.nb; b += gridDim.x * blockDim.x) {
@@ -48,7 +48,7 @@ __global__ void ff_maxbin_kernel(FinalizeFF F) {
     }
 }
 
-__global__ void ff_rows_kernel(FinalizeFF F) {
+__device__ void ff_rows_body(const FinalizeFF& F) {
     const int T = F.T;
     const int mb = *F.max_bin;
     const double width = (static_cast<double>(mb) * F.bin_width) / mb;  // Axis(0, mb*width, mb).width()
@@ -130,6 +130,12 @@ __global__ void ff_rows_kernel(FinalizeFF F) {
         }
     }
 }
+
+__global__ void ff_maxbin_kernel(FinalizeFF F) { ff_maxbin_body(F); }
+__global__ void ff_rows_kernel(FinalizeFF F) { ff_rows_body(F); }
+// batched: blockIdx.y selects the structure
+__global__ void ff_maxbin_batch_kernel(const FinalizeFF* Fs) { ff_maxbin_body(Fs[blockIdx.y]); }
+__global__ void ff_rows_batch_kernel(const FinalizeFF* Fs) { ff_rows_body(Fs[blockIdx.y]); }
 
 // Expansion of the compact rows to the reference's [15][15] / [15] layouts, stride max_bin.
 __global__ void ff_expand_kernel(FinalizeFF F, double* aa_out, double* aw_out) {
@@ -261,6 +267,13 @@ void ff_finalize_launch(const FinalizeFF& F, cudaStream_t s) {
     int blocks = (F.nb + threads - 1) / threads;
     ff_maxbin_kernel<<<blocks, threads, 0, s>>>(F);
     ff_rows_kernel<<<blocks, threads, 0, s>>>(F);
+}
+
+void ff_finalize_batch_launch(const FinalizeFF* Fs_dev, int n, int max_nb, cudaStream_t s) {
+    int threads = 256;
+    dim3 grid((max_nb + threads - 1) / threads, n);
+    ff_maxbin_batch_kernel<<<grid, threads, 0, s>>>(Fs_dev);
+    ff_rows_batch_kernel<<<grid, threads, 0, s>>>(Fs_dev);
 }
 
 void ff_expand_launch(const FinalizeFF& F, double* aa_out, double* aw_out, int nb_hint, cudaStream_t s) {

@@ -65,6 +65,8 @@ struct FinalizeMT {
 };
 
 void ff_finalize_launch(const FinalizeFF& F, cudaStream_t s);
+// the same for n structures at once (device array of descriptors; max_nb >= every nb)
+void ff_finalize_batch_launch(const FinalizeFF* Fs_dev, int n, int max_nb, cudaStream_t s);
 void ff_expand_launch(const FinalizeFF& F, double* aa_out, double* aw_out, int nb_hint, cudaStream_t s);
 void mt_finalize_launch(const FinalizeMT& F, cudaStream_t s);
 void weight_scale_launch(const float4* a, int na, const float4* b, int nb, float* wscale, cudaStream_t s);

@@ -28,6 +28,10 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
+# thread instructions per pair of the pair kernel and its DRAM bytes per profile, from an ncu capture
+# (--set full) of the three pair launches of the 50k-atom FFGrid profile
+INSTR_PER_PAIR = 45.5
+PAIR_TRAFFIC_BYTES = 7.3e6
 METRIC = "I(q) profiles/s & p99 latency vs plain GPU path at ≤1e-4 rel. I(q) error"
 UNIT = "profiles/s"
 
@@ -262,6 +266,14 @@ def run_ours(args, rank, world, local_rank):
     peaks, peak_kind = load_peaks()
     kernel_ms = k_ms / args.steps  # all pair-kernel launches of one profile
     pair_rate = pairs / (kernel_ms / 1e3)
+    clocks = clk.summary()
+    sm_mhz = clocks.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+    sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
+    # The pair kernel is bound by instruction issue (its inputs live in shared memory; DRAM traffic is
+    # ~7 MB per profile).  Issue peak: every SM sub-partition issues one warp instruction per cycle;
+    # INSTR_PER_PAIR thread instructions per pair evaluation were counted by ncu
+    # (smsp__inst_executed.sum x 32 / pairs, one-row launch of the 50k-atom FFGrid profile).
+    issue_peak = sms * 4 * sm_mhz * 1e6 * 32 / INSTR_PER_PAIR
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -277,11 +289,14 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": int(nq * 8 + 8), "p50_ms": 1e3 * float(np.percentile(lat, 50)),
                 "p99_ms": 1e3 * float(np.percentile(lat, 99)), "max_rel_diff_vs_resident": e2e_match},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "smem_atomic+fp32", "kernel": "pairhist_kernel",
-                     "achieved": pair_rate / 1e9, "unit": "Gpair/s", "peak": None, "frac": None,
-                     "traffic": None, "kernel_ms_per_step": kernel_ms, "kernel_launches_per_step": k_n / args.steps,
-                     "note": "pair binning is bound by shared-memory atomics and FP32 issue, not HBM or tensor pipes"},
-        "clocks": clk.summary(),
+        "roofline": {"bound": "issue", "kernel": "pairhist_kernel", "achieved": pair_rate / 1e9,
+                     "peak": issue_peak / 1e9, "unit": "Gpair/s", "frac": pair_rate / issue_peak,
+                     "traffic": PAIR_TRAFFIC_BYTES if wl.name.startswith("cfg1") else None,
+                     "peak_source": f"issue model: {sms} SMs x 4 x {sm_mhz:.0f} MHz x 32 / {INSTR_PER_PAIR} instr per pair",
+                     "kernel_ms_per_step": kernel_ms, "kernel_launches_per_step": k_n / args.steps,
+                     "hbm_frac": (PAIR_TRAFFIC_BYTES / (kernel_ms / 1e3)) / (peaks["hbm_gbs"] * 1e9),
+                     "note": "pair binning is bound by FP32 issue and shared-memory atomics, not HBM or tensor pipes"},
+        "clocks": clocks,
         "peaks_source": peak_kind,
     }
     if args.atomic_peak:
