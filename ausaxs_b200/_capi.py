@@ -35,6 +35,8 @@ EXPORTED = [
     "ausaxs_gpu_ctx_fp64_columns", "ausaxs_gpu_ctx_tc_error_estimate", "ausaxs_gpu_histogram", "ausaxs_gpu_debye", "ausaxs_gpu_profile",
     "ausaxs_gpu_structure_create", "ausaxs_gpu_structure_destroy", "ausaxs_gpu_structure_profile",
     "ausaxs_gpu_structure_histogram", "ausaxs_gpu_histogram_mt_noalloc", "ausaxs_gpu_linear_lsq",
+    "ausaxs_gpu_batch_create", "ausaxs_gpu_batch_destroy", "ausaxs_gpu_batch_autotune", "ausaxs_gpu_batch_candidate",
+    "ausaxs_gpu_batch_profile_device", "ausaxs_gpu_batch_profile", "ausaxs_gpu_batch_histogram",
 ]
 
 
@@ -101,6 +103,16 @@ def load():
                                                    C.POINTER(DebyeParams), f64, f64]
         L.ausaxs_gpu_structure_histogram.argtypes = [vp, vp, C.POINTER(HistConfig), C.POINTER(HistResult)]
         L.ausaxs_gpu_linear_lsq.argtypes = [vp, f64, f64, f64, C.c_int32, f64]
+        i64 = C.POINTER(C.c_int64)
+        i32 = C.POINTER(C.c_int32)
+        L.ausaxs_gpu_batch_create.argtypes = [vp, C.POINTER(HistConfig), C.c_int32, f32, i64, f32, i64, f32, i64, f64,
+                                              C.c_int32, C.POINTER(vp)]
+        L.ausaxs_gpu_batch_destroy.argtypes = [vp]
+        L.ausaxs_gpu_batch_autotune.argtypes = [vp, i32, f64, C.c_int32]
+        L.ausaxs_gpu_batch_candidate.argtypes = [C.c_int32, i32, i32, i32, i32]
+        L.ausaxs_gpu_batch_profile_device.argtypes = [vp, f64, C.c_int32, C.POINTER(DebyeParams), f64]
+        L.ausaxs_gpu_batch_profile.argtypes = [vp, f64, C.c_int32, C.POINTER(DebyeParams), f64]
+        L.ausaxs_gpu_batch_histogram.argtypes = [vp, C.c_int32, C.POINTER(HistResult)]
         _lib = L
         return L
 
@@ -233,4 +245,74 @@ class Structure:
         for k, v in bufs.items():
             setattr(r, k, dptr(v))
         check(load().ausaxs_gpu_structure_histogram(self.ctx.h, self.h, C.byref(cfg), C.byref(r)))
+        return r, bufs
+
+
+class Batch:
+    """Many device-resident structures profiled together (ausaxs_gpu_batch_*)."""
+
+    def __init__(self, ctx: Context, cfg: HistConfig, atoms: list, waters: list, exv: list | None = None,
+                 z_exv=None):
+        self.ctx = ctx
+        self.cfg = cfg
+        self.n = len(atoms)
+
+        def cat(parts):
+            parts = [np.ascontiguousarray(p, np.float32).reshape(-1, 4) for p in parts]
+            off = np.zeros(len(parts) + 1, np.int64)
+            off[1:] = np.cumsum([len(p) for p in parts])
+            data = np.ascontiguousarray(np.concatenate(parts) if off[-1] else np.zeros((1, 4), np.float32))
+            return data, off
+
+        self._a, self._ao = cat(atoms)
+        self._w, self._wo = cat(waters)
+        self._x, self._xo = (None, None) if exv is None else cat(exv)
+        self._z = None if z_exv is None else np.ascontiguousarray(z_exv, np.float64)
+        i64 = lambda a: None if a is None else a.ctypes.data_as(C.POINTER(C.c_int64))
+        h = C.c_void_p()
+        check(load().ausaxs_gpu_batch_create(ctx.h, C.byref(cfg), self.n, fptr(self._a), i64(self._ao), fptr(self._w),
+                                             i64(self._wo), fptr(self._x), i64(self._xo), dptr(self._z), 1, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().ausaxs_gpu_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def autotune(self):
+        """(chosen candidate, per-candidate milliseconds of the pair launches)."""
+        times = np.zeros(16)
+        c = C.c_int32(-1)
+        check(load().ausaxs_gpu_batch_autotune(self.h, C.byref(c), dptr(times), len(times)))
+        return c.value, times
+
+    @staticmethod
+    def candidate(index: int) -> dict:
+        v = [C.c_int32() for _ in range(4)]
+        check(load().ausaxs_gpu_batch_candidate(index, *[C.byref(x) for x in v]))
+        return dict(zip(("tile_small", "tile_large", "threshold", "by_class"), [x.value for x in v]))
+
+    def profile(self, q, params: DebyeParams) -> np.ndarray:
+        q = np.ascontiguousarray(q, np.float64)
+        out = np.zeros(self.n * len(q))
+        check(load().ausaxs_gpu_batch_profile(self.h, dptr(q), len(q), C.byref(params), dptr(out)))
+        return out.reshape(self.n, len(q))
+
+    def profile_device(self, q_dev, nq: int, params: DebyeParams, I_dev):
+        check(load().ausaxs_gpu_batch_profile_device(self.h, devptr(q_dev), nq, C.byref(params), devptr(I_dev)))
+
+    def histogram(self, index: int, bin_count: int):
+        bufs = {k: np.zeros(n) for k, n in [("aa", 225 * bin_count), ("aw", 15 * bin_count), ("ww", bin_count),
+                                             ("tot", bin_count), ("d_axis", bin_count), ("d_axis_ax", bin_count),
+                                             ("d_axis_xx", bin_count)]}
+        r = HistResult()
+        for k, v in bufs.items():
+            setattr(r, k, dptr(v))
+        check(load().ausaxs_gpu_batch_histogram(self.h, index, C.byref(r)))
         return r, bufs

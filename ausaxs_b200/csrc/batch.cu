@@ -1,0 +1,416 @@
+// Batched profiles: many independent structures through one persistent pair launch per tile/row
+// class, one batched finalisation and one batched FP64 transform, captured once as a CUDA graph
+// and replayed per call.
+//
+// The reference evaluates one structure per calculate_all() call
+// (source/core/hist/histogram_manager/HistogramManagerMTFFAvg.cpp:194-372); a batch here is the
+// same computation for n structures whose pair tiles share the GPU: every structure keeps its own
+// plan (accumulators, finalisation descriptors, Debye rows) and the batch concatenates their pair
+// jobs, largest structures first, into launch classes.  Tile shapes and class grouping are chosen
+// by timing candidates on the batch itself (autotune) and cached per batch shape.
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <numeric>
+#include <tuple>
+
+#include "engine.cuh"
+#include "guard.cuh"
+
+namespace ausaxs_b200 {
+namespace {
+
+struct ZeroRange {
+    unsigned long long* p;
+    long long words;
+};
+
+// y: range, x: chunk of the range
+__global__ void zero_ranges_kernel(const ZeroRange* ranges) {
+    const ZeroRange r = ranges[blockIdx.y];
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < r.words; k += (long long)gridDim.x * blockDim.x)
+        r.p[k] = 0;
+}
+
+// Pair-plan candidates of the autotuner: tile of small structures, tile of large ones, the point
+// count from which a structure is large, and whether jobs are split into row classes.
+struct Candidate {
+    int tile_small, tile_large, threshold, by_class;
+};
+constexpr Candidate kCandidates[] = {
+    {256, 256, 0, 0}, {256, 256, 0, 1}, {512, 512, 0, 0}, {512, 512, 0, 1},
+    {256, 512, 8192, 0}, {256, 512, 8192, 1}, {256, 512, 24576, 1},
+};
+constexpr int kNumCandidates = sizeof(kCandidates) / sizeof(kCandidates[0]);
+constexpr int kDefaultCandidate = 5;
+
+// choice per batch shape (structures, pairs, bins, SMs), shared by all batches of the process
+std::mutex g_tune_mutex;
+std::map<std::tuple<int, long long, int, int>, int> g_tuned;
+
+}  // namespace
+
+struct Batch {
+    Ctx* ctx = nullptr;
+    ausaxs_hist_config cfg{};
+    std::vector<std::unique_ptr<Structure>> items;
+    std::vector<ausaxs_hist_config> cfgs;  // per structure (z_exv)
+    std::vector<int> order;                // structures by pair count, largest first
+    int max_nb = 0;
+    long long pairs = 0;
+    struct Launch {
+        PairLaunch L{};
+        int tile = 256, grid = 0;
+        size_t smem = 0;
+    };
+    std::vector<Launch> launches;
+    int choice = -1;
+    DevBuf jobs, misc, zero, fin, args;  // misc: tile counters [16], overflow at [16]
+    int n_zero = 0;
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
+    // captured profile
+    cudaGraphExec_t exec = nullptr;
+    struct Key {
+        const double* q = nullptr;
+        int nq = -1;
+        double* I = nullptr;
+        int choice = -1;
+        cudaStream_t s = nullptr;
+        ausaxs_debye_params p{};
+    } key;
+
+    ~Batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        for (auto& st : side)
+            if (st) cudaStreamDestroy(st);
+        if (fork) cudaEventDestroy(fork);
+        for (auto& e : join)
+            if (e) cudaEventDestroy(e);
+    }
+
+    unsigned long long* overflow() const { return misc.as<unsigned long long>() + 16; }
+
+    void load(const ausaxs_hist_config& c, int n, const float* atoms, const int64_t* aoff, const float* waters,
+              const int64_t* woff, const float* exv, const int64_t* xoff, const double* z_exv, bool host) {
+        if (c.manager != AUSAXS_MANAGER_FFAVG && c.manager != AUSAXS_MANAGER_FFGRID)
+            throw Error{AUSAXS_ERR_ARGUMENT, "batched profiles support the FFAVG and FFGRID managers"};
+        if (n <= 0 || !aoff || !woff) throw Error{AUSAXS_ERR_ARGUMENT, "empty batch or missing offsets"};
+        const bool grid = c.manager == AUSAXS_MANAGER_FFGRID;
+        if (grid && !xoff) throw Error{AUSAXS_ERR_ARGUMENT, "FFGRID batches need excluded-volume offsets"};
+        cfg = c;
+        for (int i = 0; i < n; ++i) {
+            const int64_t na = aoff[i + 1] - aoff[i], nw = woff[i + 1] - woff[i];
+            const int64_t nx = grid ? xoff[i + 1] - xoff[i] : 0;
+            if (na < 0 || nw < 0 || nx < 0 || na > INT32_MAX || nw > INT32_MAX || nx > INT32_MAX)
+                throw Error{AUSAXS_ERR_ARGUMENT, "bad offsets"};
+            auto S = std::make_unique<Structure>();
+            S->ctx = ctx;
+            S->load(atoms ? atoms + 4 * aoff[i] : nullptr, (int)na, waters ? waters + 4 * woff[i] : nullptr, (int)nw,
+                    grid && exv ? exv + 4 * xoff[i] : nullptr, (int)nx, 1, host);
+            ausaxs_hist_config ci = c;
+            if (z_exv) ci.z_exv = z_exv[i];
+            S->plan_for(ci);
+            max_nb = std::max(max_nb, S->plan.nb);
+            pairs += S->plan.pairs;
+            cfgs.push_back(ci);
+            items.push_back(std::move(S));
+        }
+        order.resize(n);
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int a, int b) { return items[a]->plan.pairs > items[b]->plan.pairs; });
+        // accumulators to clear before each run (one range per structure) and the batch counters
+        std::vector<ZeroRange> zr;
+        for (auto& S : items) {
+            Plan& P = S->plan;
+            zr.push_back({P.dev.as<unsigned long long>(P.off_acc), (long long)(P.acc_bytes / 8)});
+        }
+        misc.ensure(256);
+        zr.push_back({misc.as<unsigned long long>(), 32});
+        n_zero = (int)zr.size();
+        zero.ensure(sizeof(ZeroRange) * zr.size());
+        AUSAXS_CUDA(cudaMemcpy(zero.p, zr.data(), sizeof(ZeroRange) * zr.size(), cudaMemcpyHostToDevice));
+        std::vector<FinalizeFF> fins;
+        for (auto& S : items) fins.push_back(S->plan.fin_ff);
+        fin.ensure(sizeof(FinalizeFF) * fins.size());
+        AUSAXS_CUDA(cudaMemcpy(fin.p, fins.data(), sizeof(FinalizeFF) * fins.size(), cudaMemcpyHostToDevice));
+        for (auto& st : side) AUSAXS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        AUSAXS_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+        for (auto& e : join) AUSAXS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        std::lock_guard<std::mutex> lk(g_tune_mutex);
+        auto it = g_tuned.find(shape());
+        build(it != g_tuned.end() ? it->second : kDefaultCandidate);
+    }
+
+    std::tuple<int, long long, int, int> shape() const { return {(int)items.size(), pairs, max_nb, ctx->sm_count}; }
+
+    // job tables and launch shapes of one candidate
+    void build(int c_idx) {
+        const Candidate& c = kCandidates[c_idx];
+        std::vector<PairJob> js[2][3];
+        long long tiles[2][3] = {{0, 0, 0}, {0, 0, 0}};
+        int rows[2][3] = {{1, 1, 1}, {1, 1, 1}};
+        const bool grid = cfg.manager == AUSAXS_MANAGER_FFGRID;
+        for (int i : order) {
+            const Structure& S = *items[i];
+            const int biggest = std::max({S.n_a, S.n_w, grid ? S.n_x : 0});
+            const int b = (c.tile_small != c.tile_large && biggest >= c.threshold) ? 1 : 0;
+            append_pair_jobs(S.plan, b ? c.tile_large : c.tile_small, c.by_class != 0, js[b], tiles[b], rows[b]);
+        }
+        size_t n_jobs = 0;
+        for (auto& bb : js)
+            for (auto& g : bb) n_jobs += g.size();
+        if (exec) {
+            cudaGraphExecDestroy(exec);
+            exec = nullptr;
+        }
+        jobs.ensure(sizeof(PairJob) * std::max<size_t>(1, n_jobs));
+        launches.clear();
+        size_t at = 0;
+        int counter = 0;
+        for (int b = 0; b < 2; ++b)
+            for (int g = 0; g < 3; ++g) {
+                if (js[b][g].empty()) continue;
+                Launch La;
+                La.tile = b ? c.tile_large : c.tile_small;
+                La.smem = pairhist_smem_bytes(rows[b][g], max_nb, false, La.tile);
+                if (La.smem > 232448 - 1024) throw Error{AUSAXS_ERR_CAPACITY, "too many distance bins for a batched launch"};
+                const int per_sm = std::max(1, std::min((int)(233472 / (La.smem + 1024)), 2048 / La.tile));
+                La.grid = (int)std::min<long long>((long long)ctx->sm_count * per_sm, std::max<long long>(1, tiles[b][g]));
+                PairLaunch& L = La.L;
+                L.jobs = jobs.as<PairJob>() + at;
+                L.n_jobs = (int)js[b][g].size();
+                L.total_tiles = tiles[b][g];
+                L.chunk = (int)std::max<long long>(1, std::min<long long>(8, tiles[b][g] / ((long long)La.grid * 8)));
+                L.smem_rows = rows[b][g];
+                L.smem_bins = max_nb;
+                L.tile_counter = misc.as<unsigned long long>() + counter++;
+                L.overflow = overflow();
+                L.weighted = 0;
+                L.wscale = nullptr;
+                AUSAXS_CUDA(cudaMemcpy(jobs.as<PairJob>() + at, js[b][g].data(), sizeof(PairJob) * js[b][g].size(),
+                                       cudaMemcpyHostToDevice));
+                at += js[b][g].size();
+                launches.push_back(La);
+            }
+        choice = c_idx;
+    }
+
+    // clear the accumulators, then the pair launches: the first on s, the others forked onto the
+    // side streams so a class's tail overlaps the next class
+    void enqueue_pairs(cudaStream_t s) {
+        Ctx& C = *ctx;
+        zero_ranges_kernel<<<dim3(16, n_zero), 256, 0, s>>>(zero.as<ZeroRange>());
+        C.check_launch("zero");
+        const int n = (int)launches.size();
+        if (n > 1) AUSAXS_CUDA(cudaEventRecord(fork, s));
+        for (int k = 0; k < n; ++k) {
+            cudaStream_t sk = k == 0 ? s : side[(k - 1) % 2];
+            if (k > 0 && k <= 2) AUSAXS_CUDA(cudaStreamWaitEvent(sk, fork, 0));
+            const Launch& La = launches[k];
+            pairhist_launch(La.L, La.tile, La.grid, La.smem, sk);
+            C.check_launch("pairhist");
+        }
+        for (int k = 1; k <= std::min(2, n - 1); ++k) {
+            AUSAXS_CUDA(cudaEventRecord(join[k - 1], side[k - 1]));
+            AUSAXS_CUDA(cudaStreamWaitEvent(s, join[k - 1], 0));
+        }
+    }
+
+    void enqueue_all(int nq, cudaStream_t s) {
+        enqueue_pairs(s);
+        ff_finalize_batch_launch(fin.as<FinalizeFF>(), (int)items.size(), max_nb, s);
+        ctx->check_launch("finalize");
+        debye_fp64_batch_launch(args.as<DebyeArgs>(), (int)items.size(), nq, s);
+        ctx->check_launch("debye");
+    }
+
+    // I[i * nq + k] for every structure i (FP64 transform for every q); replays the captured graph
+    void profile_device(const double* q, int nq, const ausaxs_debye_params& p, double* I) {
+        Ctx& C = *ctx;
+        cudaStream_t s = C.stream;
+        const ausaxs_debye_params& o = key.p;
+        const bool same_p = o.cw == p.cw && o.cx == p.cx && o.crho == p.crho && o.dw_atomic == p.dw_atomic &&
+                            o.dw_exv == p.dw_exv && o.grid_width == p.grid_width;
+        const bool same = exec && key.q == q && key.nq == nq && key.I == I && key.choice == choice && key.s == s && same_p;
+        if (!same) {
+            if (exec) {
+                cudaGraphExecDestroy(exec);
+                exec = nullptr;
+            }
+            std::vector<DebyeArgs> A;
+            for (size_t i = 0; i < items.size(); ++i) {
+                DebyeArgs a = items[i]->debye_args(cfgs[i], q, nq, p, I + i * (size_t)nq, nullptr);
+                a.overflow = overflow();  // the batch's launches share one overflow counter
+                a.fp64_columns = nullptr;
+                A.push_back(a);
+            }
+            args.ensure(sizeof(DebyeArgs) * A.size());
+            AUSAXS_CUDA(cudaMemcpyAsync(args.p, A.data(), sizeof(DebyeArgs) * A.size(), cudaMemcpyHostToDevice, s));
+            AUSAXS_CUDA(cudaStreamSynchronize(s));
+            cudaGraph_t g = nullptr;
+            AUSAXS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            try {
+                enqueue_all(nq, s);
+            } catch (...) {
+                cudaStreamEndCapture(s, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            AUSAXS_CUDA(cudaStreamEndCapture(s, &g));
+            cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                exec = nullptr;
+                throw Error{AUSAXS_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e)};
+            }
+            key.q = q;
+            key.nq = nq;
+            key.I = I;
+            key.choice = choice;
+            key.s = s;
+            key.p = p;
+        }
+        AUSAXS_CUDA(cudaGraphLaunch(exec, s));
+        C.launches += 4 + (long long)launches.size();
+    }
+
+    // times every candidate's pair launches on this batch (best of 2 after a warm-up) and keeps the fastest
+    int autotune(double* times_ms, int n_times) {
+        Ctx& C = *ctx;
+        cudaStream_t s = C.stream;
+        cudaEvent_t e0, e1;
+        AUSAXS_CUDA(cudaEventCreate(&e0));
+        AUSAXS_CUDA(cudaEventCreate(&e1));
+        int best = -1;
+        float best_ms = 0;
+        for (int c = 0; c < kNumCandidates; ++c) {
+            build(c);
+            enqueue_pairs(s);
+            float ms = 1e30f;
+            for (int rep = 0; rep < 2; ++rep) {
+                AUSAXS_CUDA(cudaEventRecord(e0, s));
+                enqueue_pairs(s);
+                AUSAXS_CUDA(cudaEventRecord(e1, s));
+                AUSAXS_CUDA(cudaEventSynchronize(e1));
+                float t = 0;
+                AUSAXS_CUDA(cudaEventElapsedTime(&t, e0, e1));
+                ms = std::min(ms, t);
+            }
+            if (times_ms && c < n_times) times_ms[c] = ms;
+            if (best < 0 || ms < best_ms) {
+                best = c;
+                best_ms = ms;
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        build(best);
+        std::lock_guard<std::mutex> lk(g_tune_mutex);
+        g_tuned[shape()] = best;
+        return best;
+    }
+};
+
+}  // namespace ausaxs_b200
+
+using namespace ausaxs_b200;
+
+struct ausaxs_gpu_batch {
+    Batch impl;
+};
+
+extern "C" {
+
+int ausaxs_gpu_batch_create(ausaxs_gpu_ctx* ctx, const ausaxs_hist_config* cfg, int32_t n_structures,
+                            const float* atoms, const int64_t* atom_offsets, const float* waters,
+                            const int64_t* water_offsets, const float* exv, const int64_t* exv_offsets,
+                            const double* z_exv, int32_t host_pointers, ausaxs_gpu_batch** out) {
+    return guarded([&] {
+        if (!ctx || !cfg || !out) throw Error{AUSAXS_ERR_ARGUMENT, "null argument"};
+        *out = nullptr;
+        AUSAXS_CUDA(cudaSetDevice(ctx->impl.device));
+        auto* b = new ausaxs_gpu_batch();
+        b->impl.ctx = &ctx->impl;
+        try {
+            b->impl.load(*cfg, n_structures, atoms, atom_offsets, waters, water_offsets, exv, exv_offsets, z_exv,
+                         host_pointers != 0);
+        } catch (...) {
+            delete b;
+            throw;
+        }
+        *out = b;
+    });
+}
+
+int ausaxs_gpu_batch_destroy(ausaxs_gpu_batch* b) {
+    return guarded([&] {
+        if (!b) return;
+        cudaStreamSynchronize(b->impl.ctx->stream);
+        delete b;
+    });
+}
+
+int ausaxs_gpu_batch_autotune(ausaxs_gpu_batch* b, int32_t* choice, double* times_ms, int32_t n_times) {
+    return guarded([&] {
+        if (!b) throw Error{AUSAXS_ERR_ARGUMENT, "null batch"};
+        AUSAXS_CUDA(cudaSetDevice(b->impl.ctx->device));
+        const int c = b->impl.autotune(times_ms, n_times);
+        if (choice) *choice = c;
+    });
+}
+
+int ausaxs_gpu_batch_candidate(int32_t index, int32_t* tile_small, int32_t* tile_large, int32_t* threshold,
+                               int32_t* by_class) {
+    return guarded([&] {
+        if (index < 0 || index >= kNumCandidates) throw Error{AUSAXS_ERR_ARGUMENT, "no such candidate"};
+        const Candidate& c = kCandidates[index];
+        if (tile_small) *tile_small = c.tile_small;
+        if (tile_large) *tile_large = c.tile_large;
+        if (threshold) *threshold = c.threshold;
+        if (by_class) *by_class = c.by_class;
+    });
+}
+
+int ausaxs_gpu_batch_profile_device(ausaxs_gpu_batch* b, const double* q, int32_t n_q,
+                                    const ausaxs_debye_params* params, double* Iq) {
+    return guarded([&] {
+        if (!b || !q || !Iq || n_q <= 0 || !params) throw Error{AUSAXS_ERR_ARGUMENT, "null argument"};
+        AUSAXS_CUDA(cudaSetDevice(b->impl.ctx->device));
+        b->impl.profile_device(q, n_q, *params, Iq);
+    });
+}
+
+int ausaxs_gpu_batch_profile(ausaxs_gpu_batch* b, const double* q, int32_t n_q, const ausaxs_debye_params* params,
+                             double* Iq) {
+    return guarded([&] {
+        if (!b || !q || !Iq || n_q <= 0 || !params) throw Error{AUSAXS_ERR_ARGUMENT, "null argument"};
+        Batch& B = b->impl;
+        Ctx& C = *B.ctx;
+        AUSAXS_CUDA(cudaSetDevice(C.device));
+        const size_t n = B.items.size();
+        const size_t bytes_q = ((size_t)n_q * 8 + 255) & ~(size_t)255;
+        C.io.ensure(bytes_q + n * n_q * 8 + 256);
+        double* dq = C.io.as<double>();
+        double* dI = C.io.as<double>(bytes_q);
+        AUSAXS_CUDA(cudaMemcpyAsync(dq, q, (size_t)n_q * 8, cudaMemcpyHostToDevice, C.stream));
+        B.profile_device(dq, n_q, *params, dI);
+        AUSAXS_CUDA(cudaMemcpyAsync(Iq, dI, n * n_q * 8, cudaMemcpyDeviceToHost, C.stream));
+        unsigned long long overflow = 0;
+        AUSAXS_CUDA(cudaMemcpyAsync(&overflow, B.overflow(), 8, cudaMemcpyDeviceToHost, C.stream));
+        AUSAXS_CUDA(cudaStreamSynchronize(C.stream));
+        if (overflow) throw Error{AUSAXS_ERR_BIN_OVERFLOW, "pair distances beyond bin_count * bin_width; increase settings::axes::bin_count"};
+    });
+}
+
+int ausaxs_gpu_batch_histogram(ausaxs_gpu_batch* b, int32_t index, ausaxs_hist_result* out) {
+    return guarded([&] {
+        if (!b || !out || index < 0 || index >= (int)b->impl.items.size()) throw Error{AUSAXS_ERR_ARGUMENT, "bad argument"};
+        AUSAXS_CUDA(cudaSetDevice(b->impl.ctx->device));
+        b->impl.items[index]->read_histogram(b->impl.cfgs[index], out);
+    });
+}
+
+}  // extern "C"

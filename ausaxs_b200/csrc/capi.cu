@@ -4,29 +4,13 @@
 #include <string>
 
 #include "engine.cuh"
+#include "guard.cuh"
 #include "lsq.cuh"
 
 using namespace ausaxs_b200;
 
 namespace {
 thread_local std::string g_last_error;
-
-template <typename F>
-int guarded(F&& f) {
-    try {
-        f();
-        return AUSAXS_OK;
-    } catch (const Error& e) {
-        g_last_error = e.msg;
-        return e.code;
-    } catch (const std::exception& e) {
-        g_last_error = e.what();
-        return AUSAXS_ERR_CUDA;
-    } catch (...) {
-        g_last_error = "unknown failure";
-        return AUSAXS_ERR_CUDA;
-    }
-}
 
 Structure& scratch(Ctx& C) {
     if (!C.scratch) {

@@ -480,8 +480,8 @@ void Structure::enqueue_histogram(const ausaxs_hist_config& cfg) {
     C.time_end(1, evf);
 }
 
-void Structure::enqueue_debye(const ausaxs_hist_config& cfg, const double* q_dev, int nq, const ausaxs_debye_params& p,
-                              double* Iq_dev, double* prof_dev) {
+DebyeArgs Structure::debye_args(const ausaxs_hist_config& cfg, const double* q_dev, int nq, const ausaxs_debye_params& p,
+                                double* Iq_dev, double* prof_dev) {
     Plan& P = plan;
     if (cfg.manager == AUSAXS_MANAGER_FFEXPLICIT)
         throw Error{AUSAXS_ERR_ARGUMENT, "the Debye transform of FFEXPLICIT histograms needs per-type excluded-volume tables, which this build does not carry"};
@@ -512,9 +512,13 @@ void Structure::enqueue_debye(const ausaxs_hist_config& cfg, const double* q_dev
     A.fp64_columns = reinterpret_cast<int32_t*>(base + P.off_fp64cols);
     A.Iq = Iq_dev;
     A.profiles = prof_dev;
-    int groups = 1;
-    if (grid) groups = 7;
-    run_debye(*ctx, A, groups, P.tc, p.precision);
+    return A;
+}
+
+void Structure::enqueue_debye(const ausaxs_hist_config& cfg, const double* q_dev, int nq, const ausaxs_debye_params& p,
+                              double* Iq_dev, double* prof_dev) {
+    DebyeArgs A = debye_args(cfg, q_dev, nq, p, Iq_dev, prof_dev);
+    run_debye(*ctx, A, cfg.manager == AUSAXS_MANAGER_FFGRID ? 7 : 1, plan.tc, p.precision);
 }
 
 void run_debye(Ctx& C, DebyeArgs& A, int groups_present, DevBuf& tc, int precision) {

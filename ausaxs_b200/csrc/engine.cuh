@@ -105,6 +105,9 @@ struct Structure {
     void enqueue_histogram(const ausaxs_hist_config& cfg);
     void enqueue_debye(const ausaxs_hist_config& cfg, const double* q_dev, int nq, const ausaxs_debye_params& p,
                        double* Iq_dev, double* prof_dev);
+    // arguments of the FP64 transform of the planned histogram (no launch)
+    DebyeArgs debye_args(const ausaxs_hist_config& cfg, const double* q_dev, int nq, const ausaxs_debye_params& p,
+                         double* Iq_dev, double* prof_dev);
     // histogram in the reference's layouts into host buffers (synchronises)
     void read_histogram(const ausaxs_hist_config& cfg, ausaxs_hist_result* out);
 };

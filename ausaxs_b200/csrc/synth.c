@@ -72,8 +72,10 @@ static void grid_add(grid_t* g, const double* pts, int i) {
     g->next[i] = g->head[id];
     g->head[id] = i;
 }
-/* smallest (|p - x_i| - rad_i) over points within reach cells; rad may be NULL (0) */
-static double grid_min_gap(const grid_t* g, const double* pts, const double* rad, const double* p, int reach) {
+/* smallest (|p - x_i| - rad_i) over points within reach cells (rad may be NULL: 0); returns early
+ * once it is below stop_below (the callers only need to know that) */
+static double grid_min_gap(const grid_t* g, const double* pts, const double* rad, const double* p, int reach,
+                           double stop_below) {
     int c[3];
     for (int k = 0; k < 3; ++k) c[k] = (int)floor((p[k] - g->lo[k]) / g->cell);
     double best = 1e30;
@@ -85,7 +87,10 @@ static double grid_min_gap(const grid_t* g, const double* pts, const double* rad
                 for (int i = g->head[(z * g->dim[1] + y) * g->dim[0] + x]; i >= 0; i = g->next[i]) {
                     double ex = p[0] - pts[3 * i], ey = p[1] - pts[3 * i + 1], ez = p[2] - pts[3 * i + 2];
                     double d = sqrt(ex * ex + ey * ey + ez * ez) - (rad ? rad[i] : 0.0);
-                    if (d < best) best = d;
+                    if (d < best) {
+                        best = d;
+                        if (best < stop_below) return best;
+                    }
                 }
             }
     return best;
@@ -132,7 +137,7 @@ int synth_globule(uint64_t seed, int n, double r_in, double r_out, double cone_c
             double rr = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
             if (rr < r_in || rr > r_out) continue;
             if (cone_cos > -1 && (rr == 0 || q[2] / rr < cone_cos)) continue;
-            if (grid_min_gap(&g, xyz, NULL, q, 1) < min_sep) continue;
+            if (grid_min_gap(&g, xyz, NULL, q, 1, min_sep) < min_sep) continue;
             memcpy(xyz + 3 * placed, q, sizeof(q));
             grid_add(&g, xyz, placed);
             cur = placed;
@@ -195,9 +200,9 @@ int synth_waters(uint64_t seed, const double* xyz, const int32_t* ff, int n, int
         double u = 2 * rng_u(&r) - 1, phi = 2 * M_PI * rng_u(&r), s = sqrt(1 - u * u);
         double dist = rad[a] + shell_min + (shell_max - shell_min) * rng_u(&r);
         double p[3] = {xyz[3 * a] + dist * s * cos(phi), xyz[3 * a + 1] + dist * s * sin(phi), xyz[3 * a + 2] + dist * u};
-        double gap = grid_min_gap(&g, xyz, rad, p, 1);
+        double gap = grid_min_gap(&g, xyz, rad, p, 1, shell_min);
         if (gap < shell_min || gap > shell_max) continue;
-        if (min_water_sep > 0 && placed && grid_min_gap(&gw, out, NULL, p, 1) < min_water_sep) continue;
+        if (min_water_sep > 0 && placed && grid_min_gap(&gw, out, NULL, p, 1, min_water_sep) < min_water_sep) continue;
         memcpy(out + 3 * placed, p, sizeof(p));
         grid_add(&gw, out, placed);
         ++placed;

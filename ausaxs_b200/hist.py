@@ -339,3 +339,46 @@ def profile(manager: _Manager, q, cw=1.0, cx=1.0, crho=1.0, dw_atomic=0.0, dw_ex
     check(load().ausaxs_gpu_profile(manager.ctx.h, C.byref(cfg), fptr(a), len(a), fptr(w), len(w), fptr(x),
                                     0 if x is None else len(x), dptr(q), len(q), C.byref(p), dptr(I), dptr(prof)))
     return (I, prof.reshape(6, len(q))) if with_profiles else I
+
+
+class BatchedProfiles:
+    """Profiles of many independent molecules at once (ausaxs_gpu_batch_*): for every molecule the
+    result of ``HistogramManagerMTFFAvg(m).calculate_all()->debye_transform()`` (or FFGrid), from
+    one captured graph of shared pair launches.  The reference has no batched form; each molecule's
+    result equals its single-structure one."""
+
+    def __init__(self, molecules: Sequence[Molecule], grid: bool = False, bin_width: float = 0.25,
+                 bin_count: int = 8000, ctx: Optional[_capi.Context] = None):
+        self.molecules = list(molecules)
+        self.ctx = ctx or _capi.default_context()
+        self.grid = grid
+        self.bin_count = bin_count
+        manager = _capi.MANAGER_FFGRID if grid else _capi.MANAGER_FFAVG
+        self.cfg = HistConfig(manager, 1, float(bin_width), int(bin_count), 0.0)
+        parts = [m.compact_ff() for m in self.molecules]
+        z = None if grid else [m.get_volume_grid() * RHO_WATER / m.size_atom() if m.size_atom() else 0.0
+                               for m in self.molecules]
+        self._b = _capi.Batch(self.ctx, self.cfg, [p[0] for p in parts], [p[1] for p in parts],
+                              [p[2] for p in parts] if grid else None, z)
+
+    def autotune(self):
+        return self._b.autotune()
+
+    def debye_transform(self, q=None, cw=1.0, cx=1.0, crho=1.0, dw_atomic=0.0, dw_exv=0.0, grid_width=1.0):
+        """[n][nq] I(q) of every molecule (FP64 transform)."""
+        q = default_q_axis() if q is None else np.ascontiguousarray(q, np.float64)
+        return self._b.profile(q, DebyeParams(cw, cx, crho, dw_atomic, dw_exv, grid_width, 1, 1e-5))
+
+    def histogram(self, i: int) -> dict:
+        """Molecule i's histograms from the last transform: raw aa/aw/ww counts by form factor and axes."""
+        r, bufs = self._b.histogram(i, self.bin_count)
+        m = r.max_bin
+        out = {"max_bin": m, "aa": bufs["aa"][: NFF * NFF * m].reshape(NFF, NFF, m),
+               "aw": bufs["aw"][: NFF * m].reshape(NFF, m), "ww": bufs["ww"][:m], "d_axis": bufs["d_axis"][:m]}
+        if self.grid:
+            out["d_axis_ax"] = bufs["d_axis_ax"][:m]
+            out["d_axis_xx"] = bufs["d_axis_xx"][:m]
+        return out
+
+    def close(self):
+        self._b.close()

@@ -172,10 +172,23 @@ def cfg2(seed: int = 21, subunit: int = 8333) -> Workload:
                     np.linspace(0.005, 1.0, 2000), "ffavg")
 
 
+def _molecule_args(args):
+    return _molecule(*args)
+
+
 def cfg3(seed: int = 31, count: int = 256, nmin: int = 500, nmax: int = 50000) -> Workload:
     rng = np.random.default_rng(seed)
     ns = np.exp(rng.uniform(np.log(nmin), np.log(nmax), count)).astype(int)
-    mols = [_molecule(seed * 1000 + i, int(n), int(round(0.2 * n))) for i, n in enumerate(ns)]
+    jobs = [(seed * 1000 + i, int(n), int(round(0.2 * n))) for i, n in enumerate(ns)]
+    workers = min(16, os.cpu_count() or 1)
+    if count >= 16 and workers > 1:
+        # spawn: safe after CUDA has been initialised in the parent
+        import concurrent.futures
+        import multiprocessing
+        with concurrent.futures.ProcessPoolExecutor(workers, mp_context=multiprocessing.get_context("spawn")) as ex:
+            mols = list(ex.map(_molecule_args, jobs, chunksize=4))
+    else:
+        mols = [_molecule(*j) for j in jobs]
     return Workload(f"cfg3: {count} globules, N log-uniform [{nmin}, {nmax}], FFAvg, 0.25 A bins, 400 q", mols, 0.25,
                     np.linspace(0.005, 0.8, 400), "ffavg")
 

@@ -47,7 +47,7 @@ def load_peaks():
 def workload(name: str):
     from ausaxs_b200 import synth
 
-    return {"cfg0": synth.cfg0, "cfg1": synth.cfg1, "cfg2": synth.cfg2}[name]()
+    return {"cfg0": synth.cfg0, "cfg1": synth.cfg1, "cfg2": synth.cfg2, "cfg3": synth.cfg3}[name]()
 
 
 def pair_count(m, grid: bool) -> int:
@@ -161,6 +161,185 @@ def time_reference(m, wl, steps: int, warmup: int, target_pairs: float = 4e9):
                                            f"pairs, debye_transform() time scaled by q count"),
               "kind": "reference"}
     return 1.0 / per, detail
+
+
+def time_reference_batch(wl, steps: int, warmup: int, target_pairs: float = 4e9):
+    """The reference on whole structures drawn at random from the batch until about target_pairs
+    pairs; the batch time is scaled by total pairs / sampled pairs.  Returns (profiles/s, details)."""
+    from oracle import py as O
+
+    if not O.ref_available():
+        return None, {"unavailable": "reference build oracle/_ref/libausaxs_ref.so not present"}
+    threads = max(1, (os.cpu_count() or 2) - 1)
+    O.ref(threads)
+    O.ref_set_axes(wl.bin_width, 8000, 1e-4, 1.0)
+    O.ref_set_simple_exv(False)
+    total = sum(pair_count(m, False) for m in wl.molecules)
+    rng = np.random.default_rng(5)
+    picked, got = [], 0
+    for i in rng.permutation(len(wl.molecules)):
+        if got >= target_pairs:
+            break
+        picked.append(int(i))
+        got += pair_count(wl.molecules[i], False)
+    times = []
+    for it in range(warmup + steps):
+        t = 0.0
+        for i in picked:
+            m = wl.molecules[i]
+            rm = O.RefMolecule(m.atoms, m.weights, m.ff_types, m.waters, m.water_weights, volume=m.volume)
+            rm.set_manager(wl.manager)
+            h = rm.calculate()
+            _, _, _, t_debye = h.debye()
+            t += h.seconds + t_debye * (len(wl.q) / 200.0)
+        if it >= warmup:
+            times.append(t * total / got)
+    per_batch = statistics.median(times)
+    detail = {"cores": threads, "kind": "reference",
+              "sample": (f"{len(picked)} whole structures of the {len(wl.molecules)} ({got / total:.4f} of the pairs); "
+                         f"batch time scaled by pairs, debye_transform() time by q count")}
+    return len(wl.molecules) / per_batch, detail
+
+
+def run_batch(args, rank, world, local_rank):
+    """Batched profiles of many structures (one graph replay per step) against one plain
+    single-structure call per structure."""
+    import ctypes as C
+
+    import torch
+
+    from ausaxs_b200 import _capi, hist
+
+    torch.cuda.set_device(local_rank)
+    dev = f"cuda:{local_rank}"
+    stream = torch.cuda.Stream(local_rank)
+    ctx = _capi.Context(local_rank)
+    ctx.set_stream(stream.cuda_stream)
+    wl = workload(args.workload)
+    mols = wl.molecules
+    n = len(mols)
+    nq = len(wl.q)
+    pairs = sum(pair_count(m, False) for m in mols)
+    params = _capi.DebyeParams(1.0, 1.0, 1.0, 0.0, 0.0, 1.0, 1, 1e-5)
+    B = hist.BatchedProfiles(mols, bin_width=wl.bin_width, bin_count=wl.bin_count, ctx=ctx)
+    choice, cand_ms = B.autotune()
+    q_dev = torch.tensor(wl.q, dtype=torch.float64, device=dev)
+    I_dev = torch.zeros(n * nq, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step():
+        B._b.profile_device(q_dev, nq, params, I_dev)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+            flush.fill_(1.0)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        launches0 = ctx.launches
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        with ClockSampler(local_rank) as clk:
+            torch.cuda.synchronize()
+            for k in range(args.steps):
+                starts[k].record(stream)
+                step()
+                ends[k].record(stream)
+                flush.fill_(float(k))
+            torch.cuda.synchronize()
+        launches = ctx.launches - launches0
+        step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * n * args.steps / (total_ms / 1e3)
+    I_batch = I_dev.cpu().numpy().reshape(n, nq)
+
+    # the plain path: one resident structure per call, called n times in sequence on the same stream
+    cfgs = []
+    sts = []
+    for m in mols:
+        mgr = hist.HistogramManagerMTFFAvg(m, True, wl.bin_width, wl.bin_count, ctx)
+        a, w, _ = mgr._inputs()
+        cfgs.append(mgr.config())
+        sts.append(_capi.Structure(ctx, a, w, None, ff_typed=True))
+    I_plain = torch.zeros(n * nq, dtype=torch.float64, device=dev)
+
+    def plain_pass():
+        for i in range(n):
+            sts[i].profile_device(cfgs[i], q_dev, nq, params, I_plain[i * nq:])
+
+    with torch.cuda.stream(stream):
+        plain_pass()
+        torch.cuda.synchronize()
+        plain_ms = []
+        for k in range(max(1, min(3, args.steps))):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            plain_pass()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            plain_ms.append(e0.elapsed_time(e1))
+            flush.fill_(float(k))
+    plain_value = n / (statistics.median(plain_ms) / 1e3)
+    plain_diff = float(np.max(np.abs(I_plain.cpu().numpy().reshape(n, nq) / I_batch - 1)))
+    for st in sts:
+        st.close()
+
+    # end to end through the host API: every step creates the batch from host points (H2D of all
+    # coordinates, census, plans), profiles it and reads every I(q) back
+    h2d = sum(a.nbytes for a in (B._b._a, B._b._w)) + nq * 8
+    lat = []
+    for k in range(args.warmup // 2 + args.steps):
+        t0 = time.perf_counter()
+        Bk = hist.BatchedProfiles(mols, bin_width=wl.bin_width, bin_count=wl.bin_count, ctx=ctx)
+        Ie = Bk.debye_transform(wl.q)
+        Bk.close()
+        if k >= args.warmup // 2:
+            lat.append(time.perf_counter() - t0)
+    e2e = world * n * len(lat) / sum(lat)
+    e2e_diff = float(np.max(np.abs(Ie / I_batch - 1)))
+
+    peaks, peak_kind = load_peaks()
+    pair_ms = cand_ms[choice]
+    clocks = clk.summary()
+    sm_mhz = clocks.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+    sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
+    issue_peak = sms * 4 * sm_mhz * 1e6 * 32 / INSTR_PER_PAIR
+    pair_rate = pairs / (pair_ms / 1e3)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 distances, u32/u64 integer bins, f64 transform", "data": "synthetic (seeded generator)",
+        "config": {"workload": wl.name, "structures": n, "atoms_total": int(sum(m.size_atom() for m in mols)),
+                   "pairs_per_step": pairs, "bin_width": wl.bin_width, "q_points": nq, "manager": wl.manager,
+                   "autotune": {"choice": choice, "candidate": _capi.Batch.candidate(choice),
+                                "pair_ms_per_candidate": [round(float(x), 3) for x in cand_ms[:7]]},
+                   "plain_sequential": {"value": plain_value, "unit": UNIT, "speedup": value / plain_value,
+                                        "max_rel_diff": plain_diff},
+                   "l2": "256 MiB buffer written between timed steps (outside the events)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(n * nq * 8 + 8),
+                "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+                "max_rel_diff_vs_resident": e2e_diff,
+                "note": "batch created from host points every step (upload, census, plans), profiled, I(q) read back"},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "issue", "kernel": "pairhist_kernel", "achieved": pair_rate / 1e9,
+                     "peak": issue_peak / 1e9, "unit": "Gpair/s", "frac": pair_rate / issue_peak, "traffic": None,
+                     "peak_source": f"issue model: {sms} SMs x 4 x {sm_mhz:.0f} MHz x 32 / {INSTR_PER_PAIR} instr per pair",
+                     "pair_ms_per_step": pair_ms},
+        "clocks": clocks,
+        "peaks_source": peak_kind,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, det = time_reference_batch(wl, steps=1, warmup=0)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, **det} if v is not None else det
+    B.close()
+    ctx.close()
+    return line
 
 
 def run_ours(args, rank, world, local_rank):
@@ -318,8 +497,10 @@ def atomic_peak_estimate(device):
 
 def run_reference(args, rank, world):
     wl = workload(args.workload)
-    m = wl.molecules[0]
-    v, det = time_reference(m, wl, steps=args.steps, warmup=args.warmup, target_pairs=2e9)
+    if args.workload == "cfg3":
+        v, det = time_reference_batch(wl, steps=args.steps, warmup=args.warmup, target_pairs=1e9)
+    else:
+        v, det = time_reference(wl.molecules[0], wl, steps=args.steps, warmup=args.warmup, target_pairs=2e9)
     if v is None:
         return {"impl": "reference", **det}
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -336,7 +517,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2"])
+    ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--atomic-peak", action="store_true")
     ap.add_argument("--precision", type=int, default=0, choices=[0, 1])
@@ -357,7 +538,7 @@ def main():
 
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    line = run_ours(args, rank, world, local_rank)
+    line = (run_batch if args.workload == "cfg3" else run_ours)(args, rank, world, local_rank)
     if world > 1:
         import torch
 

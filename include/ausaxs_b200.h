@@ -199,6 +199,44 @@ AUSAXS_API int ausaxs_gpu_structure_histogram(ausaxs_gpu_ctx* ctx, ausaxs_gpu_st
                                    ausaxs_hist_result* out);
 
 /*
+ * Batched profiles of many independent structures (FFAVG or FFGRID).  The reference computes one
+ * structure per HistogramManagerMTFFAvg::calculate_all() (HistogramManagerMTFFAvg.cpp:194-372) and
+ * debye_transform(); a batch gives every structure's I(q) from one replay of a captured CUDA graph:
+ * the pair jobs of all structures in shared persistent launches, one batched finalisation, one
+ * batched FP64 transform.
+ *
+ * ausaxs_gpu_batch_create: points of structure i are rows [off[i], off[i+1]) of the concatenated
+ *   {x, y, z, ff} arrays (offsets have n_structures + 1 entries; exv/exv_offsets only for FFGRID);
+ *   z_exv[i] (may be null: cfg->z_exv for all) is the FFAVG excluded-volume charge per atom.  One
+ *   synchronisation per structure (census) at creation.
+ * ausaxs_gpu_batch_autotune: times every pair-plan candidate on this batch, keeps the fastest and
+ *   remembers it for batches of the same shape; choice and per-candidate milliseconds are returned
+ *   (times_ms may be null).  ausaxs_gpu_batch_candidate describes a candidate.
+ * ausaxs_gpu_batch_profile_device: q and Iq[n_structures * n_q] are device pointers; enqueues one
+ *   graph launch on the context's stream (the graph is captured on the first call and again when
+ *   q, Iq, n_q or the parameters change).  The transform is FP64 for every q; params->precision is
+ *   not used.  Any bin overflow in the batch makes every Iq NaN.
+ * ausaxs_gpu_batch_profile: host q and Iq (synchronises; bin overflow is an error).
+ * ausaxs_gpu_batch_histogram: structure `index`'s histograms from the last profile, as
+ *   ausaxs_gpu_structure_histogram.
+ */
+typedef struct ausaxs_gpu_batch ausaxs_gpu_batch;
+
+AUSAXS_API int ausaxs_gpu_batch_create(ausaxs_gpu_ctx* ctx, const ausaxs_hist_config* cfg, int32_t n_structures,
+                                       const float* atoms, const int64_t* atom_offsets, const float* waters,
+                                       const int64_t* water_offsets, const float* exv, const int64_t* exv_offsets,
+                                       const double* z_exv, int32_t host_pointers, ausaxs_gpu_batch** out);
+AUSAXS_API int ausaxs_gpu_batch_destroy(ausaxs_gpu_batch* b);
+AUSAXS_API int ausaxs_gpu_batch_autotune(ausaxs_gpu_batch* b, int32_t* choice, double* times_ms, int32_t n_times);
+AUSAXS_API int ausaxs_gpu_batch_candidate(int32_t index, int32_t* tile_small, int32_t* tile_large, int32_t* threshold,
+                                          int32_t* by_class);
+AUSAXS_API int ausaxs_gpu_batch_profile_device(ausaxs_gpu_batch* b, const double* q, int32_t n_q,
+                                               const ausaxs_debye_params* params, double* Iq);
+AUSAXS_API int ausaxs_gpu_batch_profile(ausaxs_gpu_batch* b, const double* q, int32_t n_q,
+                                        const ausaxs_debye_params* params, double* Iq);
+AUSAXS_API int ausaxs_gpu_batch_histogram(ausaxs_gpu_batch* b, int32_t index, ausaxs_hist_result* out);
+
+/*
  * Weighted linear least squares of a model against data plus chi-square, on the device:
  * fitter::detail::LinearLeastSquares::fit (source/core/fitter/detail/LinearLeastSquares.cpp:26-55),
  * fitting model ~ a * data + b with weights 1/err^2 as LinearFitter sets it up (the measured
