@@ -153,11 +153,17 @@ struct Batch {
         long long tiles[2][3] = {{0, 0, 0}, {0, 0, 0}};
         int rows[2][3] = {{1, 1, 1}, {1, 1, 1}};
         const bool grid = cfg.manager == AUSAXS_MANAGER_FFGRID;
+        // on-chip rows that fit next to the batch-wide bin count
+        const size_t cap = 232448 - 1024;
+        if (pairhist_smem_bytes(1, max_nb, false, 512) > cap)
+            throw Error{AUSAXS_ERR_CAPACITY, "too many distance bins for a batched launch"};
+        int max_rows = 1;
+        while (max_rows < 4096 && pairhist_smem_bytes(max_rows + 1, max_nb, false, 512) <= cap) ++max_rows;
         for (int i : order) {
             const Structure& S = *items[i];
             const int biggest = std::max({S.n_a, S.n_w, grid ? S.n_x : 0});
             const int b = (c.tile_small != c.tile_large && biggest >= c.threshold) ? 1 : 0;
-            append_pair_jobs(S.plan, b ? c.tile_large : c.tile_small, c.by_class != 0, js[b], tiles[b], rows[b]);
+            append_pair_jobs(S.plan, b ? c.tile_large : c.tile_small, c.by_class != 0, js[b], tiles[b], rows[b], max_rows);
         }
         size_t n_jobs = 0;
         for (auto& bb : js)

@@ -140,12 +140,13 @@ void Structure::load(const float* atoms, int n_atoms, const float* waters, int n
 static long long tri(long long t) { return t * (t + 1) / 2; }
 
 void append_pair_jobs(const Plan& P, int tile, bool by_class, std::vector<PairJob> (&jobs)[3], long long (&tiles)[3],
-                      int (&rows)[3]) {
+                      int (&rows)[3], int max_rows) {
     auto nt = [tile](int n) { return (n + tile - 1) / tile; };
+    const int group_rows = max_rows > 0 ? max_rows : P.max_group_rows;
     for (const JobSpec& j : P.specs) {
         const long long t = j.self ? tri(nt(j.na)) : (long long)nt(j.na) * nt(j.nbp);
-        for (int r0 = 0; r0 < j.rows; r0 += P.max_group_rows) {
-            const int r1 = std::min(j.rows, r0 + P.max_group_rows);
+        for (int r0 = 0; r0 < j.rows; r0 += group_rows) {
+            const int r1 = std::min(j.rows, r0 + group_rows);
             const int g = !by_class ? 0 : ((r1 - r0) == 1 ? 0 : ((r1 - r0) <= P.T ? 1 : 2));
             PairJob pj{};
             pj.A = j.A;

@@ -141,9 +141,10 @@ struct Ctx {
 
 // Cuts the passes of a planned structure into tiles of `tile` points and appends them to launch
 // classes: 0 (one on-chip row), 1 (up to T rows), 2 (more), or all to class 0 when !by_class.
-// Tile ids continue from tiles[g]; rows[g] grows to the largest row group of class g.
+// Tile ids continue from tiles[g]; rows[g] grows to the largest row group of class g.  Row groups
+// hold at most max_rows rows (0: the plan's own limit).
 void append_pair_jobs(const Plan& P, int tile, bool by_class, std::vector<PairJob> (&jobs)[3], long long (&tiles)[3],
-                      int (&rows)[3]);
+                      int (&rows)[3], int max_rows = 0);
 
 // Tensor-core contraction (precision 0) followed by the FP64 epilogue, or FP64 only (precision 1).
 void run_debye(Ctx& C, DebyeArgs& A, int groups_present, DevBuf& tc, int precision);
