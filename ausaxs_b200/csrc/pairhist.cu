@@ -143,10 +143,11 @@ __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, co
     for (int jj = k0; jj < k1; ++jj) {
         const float4 b = s_pts[jj];
         PairBin p;
-        if (GENERAL) {
-            const int j = j0 + jj;
-            if (diag && j <= i) continue;
-            p = pair_eval(a, b, inv_w, j >= ts);
+        // Which evaluation a pair gets depends only on the reference's rule (scalar-tail partner or
+        // not), never on the tiling, so results do not depend on tile shapes or launch grouping.
+        if (GENERAL && (diag && j0 + jj <= i)) continue;
+        if (GENERAL && j0 + jj >= ts) {
+            p = pair_eval(a, b, inv_w, true);
             if (static_cast<unsigned>(p.bin) >= nbins) {
                 ++overflow;
                 continue;
