@@ -26,17 +26,10 @@ constexpr int kSegment = 128;             // inner points between drains: 512 x 
 // rounds ties away from zero (std::round).
 // ---------------------------------------------------------------------------------------------
 struct PairBin {
-    float x;    // d * inv_w (float, the reference's rounding)
-    float t;    // x - bin: the in-bin offset in bin units, exact, in [-1/2, 1/2]
+    float d;    // distance (float, as the reference accumulates it)
+    float xr;   // bin index as float
     int32_t bin;
 };
-
-// rint(x) by the magic-number addition (exact for 0 <= x < 2^22) and the offset from it
-__device__ __forceinline__ void pair_round(PairBin& r) {
-    const float xm = __fadd_rn(r.x, kMagic);
-    r.bin = __float_as_int(xm) - kMagicBits;
-    r.t = __fsub_rn(r.x, __fsub_rn(xm, kMagic));
-}
 
 __device__ __forceinline__ PairBin pair_eval(float4 a, float4 b, float inv_w, bool tail) {
     float dx = __fsub_rn(a.x, b.x);
@@ -45,49 +38,29 @@ __device__ __forceinline__ PairBin pair_eval(float4 a, float4 b, float inv_w, bo
     float s = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
     if (tail) s = __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
     PairBin r;
-    r.x = __fmul_rn(__fsqrt_rn(s), inv_w);
-    pair_round(r);
-    if (tail && r.t == 0.5f) {  // std::round: ties away from zero
+    r.d = __fsqrt_rn(s);
+    float x = __fmul_rn(r.d, inv_w);
+    float xm = __fadd_rn(x, kMagic);               // exact rint for 0 <= x < 2^22
+    r.bin = __float_as_int(xm) - kMagicBits;
+    r.xr = __fsub_rn(xm, kMagic);
+    if (tail && __fsub_rn(x, r.xr) == 0.5f) {      // std::round: ties away from zero
         r.bin += 1;
-        r.t = -0.5f;
+        r.xr = __fadd_rn(r.xr, 1.0f);
     }
     // NaN / inf / huge distances: make the bin fail every range check
-    if (!(r.x < 4194304.0f)) r.bin = 0x7fffffff;
+    if (!(x < 4194304.0f)) r.bin = 0x7fffffff;
     return r;
 }
 
-// The SIMD evaluator's result (rounding of pair_eval without the tail rule) at lower cost: the
-// distance from the approximate square root (sqrt.approx.f32, within 1 ulp of the correctly rounded
-// root on sm_100a for all normal inputs), so x carries at most ~2^-22 x of extra error.  When x is
-// farther than 2^-21 x from a rounding boundary (k + 1/2) the bin is the same as with the exact root
-// and the offset differs by at most ~2^-22 x bins; otherwise the exact evaluation is redone.
-// Returns false when the bin is not below nbins (NaN, infinite and huge distances included: their
-// magic-number bins are above 2^22).
-__device__ __forceinline__ bool pair_eval_fast(float4 a, float4 b, float inv_w, unsigned nbins, PairBin& r) {
-    const float dx = __fsub_rn(a.x, b.x);
-    const float dy = __fsub_rn(a.y, b.y);
-    const float dz = __fsub_rn(a.z, b.z);
-    const float s = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-    float d;
-    asm("sqrt.approx.f32 %0, %1;" : "=f"(d) : "f"(s));
-    r.x = __fmul_rn(d, inv_w);
-    pair_round(r);
-    if (__fmaf_rn(r.x, 0x1p-21f, fabsf(r.t)) >= 0.5f) {
-        r.x = __fmul_rn(__fsqrt_rn(s), inv_w);
-        pair_round(r);
-    }
-    return static_cast<unsigned>(r.bin) < nbins;
-}
-
-// Fixed-point in-bin offset of a pair: t = x - bin in [-1/2, 1/2] bin units is stored as
-// rint(t * 2^15 (1 - 2^-8)) + kResBias in [0, 2^16).  Sums of these are exact integers, so the
-// per-bin mean distance does not depend on summation order; the quantisation step is 2^-15 of a bin
-// (7.6e-6 A at the default 0.25 A bins), and rounding errors of many pairs average out.  The
-// distance is bin * c + t * c with c the bin width (the finalisation's scale is 2^15 (1 - 2^-8) / c).
-constexpr float kResScale = 32640.0f;  // 2^15 (1 - 2^-8)
-__device__ __forceinline__ uint32_t pair_residual(const PairBin& p) {
-    const float q = __fmaf_rn(p.t, kResScale, kMagic);
-    return static_cast<uint32_t>(__float_as_int(q) - kMagicBits + kResBias);
+// Fixed-point in-bin offset of a pair: the distance is d = bin*c + r with |r| <= c/2 (1 + 2^-10)
+// (c = 1/inv_w rounded to float), r is stored as rint(r * scale) + kResBias in [0, 2^16) with
+// scale = 2^15 / c * (1 - 2^-8).  Sums of these are exact integers, so the per-bin mean distance
+// does not depend on summation order; the quantisation step is about c * 2^-15 (7.6e-6 A at the
+// default 0.25 A bins, 3.1e-6 A at 0.1 A), and rounding errors of many pairs average out.
+__device__ __forceinline__ uint32_t pair_residual(const PairBin& p, float c, float scale) {
+    float r = __fmaf_rn(-p.xr, c, p.d);
+    float t = __fadd_rn(__fmul_rn(r, scale), kMagic);
+    return static_cast<uint32_t>(__float_as_int(t) - kMagicBits + kResBias);
 }
 
 // In the reference's j-loops (SimpleCalculator.h:117-141, HistogramManagerMTFFAvg.cpp:216-232)

@@ -128,7 +128,7 @@ __device__ __forceinline__ void flush_hist(const PairJob& J, const Onchip& S) {
 template <bool GENERAL, bool WEIGHTED, bool SINGLE>
 __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, const float4* s_pts, const float4 a, int i,
                                            int j0, int k0, int k1, bool diag, float wsc, unsigned long long& overflow) {
-    const float inv_w = J.inv_w;
+    const float inv_w = J.inv_w, c = J.c, scale = J.scale;
     const unsigned nbins = static_cast<unsigned>(J.nbins);
     const int rmode = J.row_mode, rlo = J.row_lo, rhi = J.row_hi;
     const int ts = tail_start(J.self ? i + 1 : 0, J.nb);
@@ -142,17 +142,10 @@ __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, co
 #pragma unroll 4
     for (int jj = k0; jj < k1; ++jj) {
         const float4 b = s_pts[jj];
-        PairBin p;
-        // Which evaluation a pair gets depends only on the reference's rule (scalar-tail partner or
-        // not), never on the tiling, so results do not depend on tile shapes or launch grouping.
-        if (GENERAL && (diag && j0 + jj <= i)) continue;
-        if (GENERAL && j0 + jj >= ts) {
-            p = pair_eval(a, b, inv_w, true);
-            if (static_cast<unsigned>(p.bin) >= nbins) {
-                ++overflow;
-                continue;
-            }
-        } else if (!pair_eval_fast(a, b, inv_w, nbins, p)) {
+        const int j = j0 + jj;
+        if (GENERAL && diag && j <= i) continue;
+        const PairBin p = pair_eval(a, b, inv_w, GENERAL && j >= ts);
+        if (static_cast<unsigned>(p.bin) >= nbins) {
             ++overflow;
             continue;
         }
@@ -162,7 +155,7 @@ __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, co
             const int row = pair_rows ? rowbase + __float_as_int(b.w) : rowbase;
             if (all_rows || (row >= rlo && row < rhi)) atomicAdd(&S.cnt[(row - rlo) * S.pad + p.bin], 1u);
         }
-        if (do_d) atomicAdd(&S.dacc[p.bin], pair_residual(p));
+        if (do_d) atomicAdd(&S.dacc[p.bin], pair_residual(p, c, scale));
         if (do_w) {
             const float wp = __fmul_rn(a.w, b.w);
             const int wq = __float2int_rn(__fmul_rn(wp, wsc));  // |wq| <= 2^30
