@@ -37,6 +37,9 @@ EXPORTED = [
     "ausaxs_gpu_structure_histogram", "ausaxs_gpu_histogram_mt_noalloc", "ausaxs_gpu_linear_lsq",
     "ausaxs_gpu_batch_create", "ausaxs_gpu_batch_destroy", "ausaxs_gpu_batch_autotune", "ausaxs_gpu_batch_candidate",
     "ausaxs_gpu_batch_profile_device", "ausaxs_gpu_batch_profile", "ausaxs_gpu_batch_histogram",
+    "ausaxs_gpu_server_create", "ausaxs_gpu_server_destroy", "ausaxs_gpu_server_admit", "ausaxs_gpu_server_release",
+    "ausaxs_gpu_server_usage", "ausaxs_gpu_server_submit", "ausaxs_gpu_server_poll", "ausaxs_gpu_server_wait",
+    "ausaxs_gpu_server_body_center", "ausaxs_gpu_server_coordinates", "ausaxs_gpu_server_histogram",
 ]
 
 
@@ -113,6 +116,18 @@ def load():
         L.ausaxs_gpu_batch_profile_device.argtypes = [vp, f64, C.c_int32, C.POINTER(DebyeParams), f64]
         L.ausaxs_gpu_batch_profile.argtypes = [vp, f64, C.c_int32, C.POINTER(DebyeParams), f64]
         L.ausaxs_gpu_batch_histogram.argtypes = [vp, C.c_int32, C.POINTER(HistResult)]
+        L.ausaxs_gpu_server_create.argtypes = [C.c_int32, C.c_int64, C.c_int32, C.c_int32, C.POINTER(vp)]
+        L.ausaxs_gpu_server_destroy.argtypes = [vp]
+        L.ausaxs_gpu_server_admit.argtypes = [vp, C.POINTER(HistConfig), C.c_int32, f32, i64, f32, i64, C.c_double,
+                                              f64, C.c_int32, C.POINTER(DebyeParams), f64, f64, i32, i64]
+        L.ausaxs_gpu_server_release.argtypes = [vp, C.c_int32]
+        L.ausaxs_gpu_server_usage.argtypes = [vp, i64, i64, i32]
+        L.ausaxs_gpu_server_submit.argtypes = [vp, C.c_int32, C.c_int32, f64, f64, i64]
+        L.ausaxs_gpu_server_poll.argtypes = [vp, C.c_int64, i32, f64, f64]
+        L.ausaxs_gpu_server_wait.argtypes = [vp, C.c_int64, C.c_int32, f64, f64]
+        L.ausaxs_gpu_server_body_center.argtypes = [vp, C.c_int32, C.c_int32, f64]
+        L.ausaxs_gpu_server_coordinates.argtypes = [vp, C.c_int32, f32, f32]
+        L.ausaxs_gpu_server_histogram.argtypes = [vp, C.c_int32, C.POINTER(HistResult)]
         _lib = L
         return L
 
@@ -316,3 +331,118 @@ class Batch:
             setattr(r, k, dptr(v))
         check(load().ausaxs_gpu_batch_histogram(self.h, index, C.byref(r)))
         return r, bufs
+
+
+ERR_CAPACITY = 5
+ERR_TIMEOUT = 6
+ERR_NOT_FOUND = 7
+
+
+class Server:
+    """Rigid-body serving (ausaxs_gpu_server_*): device-resident multi-body assemblies, one body moved
+    per request, I(q) and the linear fit against a target returned per request."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 8 << 30, max_inflight: int = 64, slots_per_assembly: int = 4):
+        h = C.c_void_p()
+        check(load().ausaxs_gpu_server_create(device, int(hbm_budget), max_inflight, slots_per_assembly, C.byref(h)))
+        self.h = h
+        self.nq = {}
+        self.n_atoms = {}
+        self.n_waters = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().ausaxs_gpu_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def admit(self, cfg: HistConfig, bodies_atoms: list, bodies_waters: list, q, params: DebyeParams,
+              target=None, target_err=None, margin: float = 20.0):
+        """bodies_atoms[k]: [n_k, 4] {x, y, z, ff}; bodies_waters[k]: [m_k, 4] {x, y, z, w}.  Returns (id, footprint)."""
+        def cat(parts):
+            parts = [np.ascontiguousarray(p, np.float32).reshape(-1, 4) for p in parts]
+            off = np.zeros(len(parts) + 1, np.int64)
+            off[1:] = np.cumsum([len(p) for p in parts])
+            return np.ascontiguousarray(np.concatenate(parts) if off[-1] else np.zeros((1, 4), np.float32)), off
+
+        a, ao = cat(bodies_atoms)
+        w, wo = cat(bodies_waters)
+        q = np.ascontiguousarray(q, np.float64)
+        tg = None if target is None else np.ascontiguousarray(target, np.float64)
+        te = None if target_err is None else np.ascontiguousarray(target_err, np.float64)
+        i = C.c_int32(-1)
+        fp = C.c_int64(0)
+        i64 = lambda x: x.ctypes.data_as(C.POINTER(C.c_int64))
+        rc = load().ausaxs_gpu_server_admit(self.h, C.byref(cfg), len(bodies_atoms), fptr(a), i64(ao), fptr(w), i64(wo),
+                                            float(margin), dptr(q), len(q), C.byref(params), dptr(tg), dptr(te),
+                                            C.byref(i), C.byref(fp))
+        check(rc)
+        self.nq[i.value] = len(q)
+        self.n_atoms[i.value] = int(ao[-1])
+        self.n_waters[i.value] = int(wo[-1])
+        return i.value, fp.value
+
+    def release(self, id: int):
+        check(load().ausaxs_gpu_server_release(self.h, id))
+
+    def usage(self):
+        u, b, n = C.c_int64(), C.c_int64(), C.c_int32()
+        check(load().ausaxs_gpu_server_usage(self.h, C.byref(u), C.byref(b), C.byref(n)))
+        return u.value, b.value, n.value
+
+    def submit(self, id: int, body: int = -1, R=None, t=None) -> int:
+        Rm = None if R is None else np.ascontiguousarray(R, np.float64).reshape(9)
+        tv = None if t is None else np.ascontiguousarray(t, np.float64).reshape(3)
+        tk = C.c_int64(-1)
+        check(load().ausaxs_gpu_server_submit(self.h, id, body, dptr(Rm), dptr(tv), C.byref(tk)))
+        return tk.value
+
+    def try_submit(self, id: int, body: int = -1, R=None, t=None):
+        """Ticket, or None when no slot is free."""
+        try:
+            return self.submit(id, body, R, t)
+        except AusaxsError as e:
+            if e.code == ERR_CAPACITY:
+                return None
+            raise
+
+    def poll(self, ticket: int, id: int):
+        I = np.zeros(self.nq[id])
+        fit = np.zeros(5)
+        done = C.c_int32(0)
+        check(load().ausaxs_gpu_server_poll(self.h, ticket, C.byref(done), dptr(I), dptr(fit)))
+        return (I, fit) if done.value else None
+
+    def wait(self, ticket: int, id: int, timeout_ms: int = 10000):
+        I = np.zeros(self.nq[id])
+        fit = np.zeros(5)
+        check(load().ausaxs_gpu_server_wait(self.h, ticket, timeout_ms, dptr(I), dptr(fit)))
+        return I, fit
+
+    def body_center(self, id: int, body: int) -> np.ndarray:
+        c = np.zeros(3)
+        check(load().ausaxs_gpu_server_body_center(self.h, id, body, dptr(c)))
+        return c
+
+    def coordinates(self, id: int):
+        a = np.zeros((max(1, self.n_atoms[id]), 4), np.float32)
+        w = np.zeros((max(1, self.n_waters[id]), 4), np.float32)
+        check(load().ausaxs_gpu_server_coordinates(self.h, id, fptr(a), fptr(w)))
+        return a[: self.n_atoms[id]], w[: self.n_waters[id]]
+
+    def histogram(self, id: int, bin_count: int):
+        bufs = {k: np.zeros(n) for k, n in [("aa", 225 * bin_count), ("aw", 15 * bin_count), ("ww", bin_count),
+                                             ("tot", bin_count), ("d_axis", bin_count), ("d_axis_ax", bin_count),
+                                             ("d_axis_xx", bin_count)]}
+        r = HistResult()
+        for k, v in bufs.items():
+            setattr(r, k, dptr(v))
+        check(load().ausaxs_gpu_server_histogram(self.h, id, C.byref(r)))
+        m = r.max_bin
+        return {"max_bin": m, "aa": bufs["aa"][: 225 * m].reshape(15, 15, m), "aw": bufs["aw"][: 15 * m].reshape(15, m),
+                "ww": bufs["ww"][:m], "d_axis": bufs["d_axis"][:m]}

@@ -21,18 +21,6 @@
 namespace ausaxs_b200 {
 namespace {
 
-struct ZeroRange {
-    unsigned long long* p;
-    long long words;
-};
-
-// y: range, x: chunk of the range
-__global__ void zero_ranges_kernel(const ZeroRange* ranges) {
-    const ZeroRange r = ranges[blockIdx.y];
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < r.words; k += (long long)gridDim.x * blockDim.x)
-        r.p[k] = 0;
-}
-
 // Pair-plan candidates of the autotuner: tile of small structures, tile of large ones, the point
 // count from which a structure is large, and whether jobs are split into row classes.
 struct Candidate {
@@ -208,7 +196,7 @@ struct Batch {
     // side streams so a class's tail overlaps the next class
     void enqueue_pairs(cudaStream_t s) {
         Ctx& C = *ctx;
-        zero_ranges_kernel<<<dim3(16, n_zero), 256, 0, s>>>(zero.as<ZeroRange>());
+        zero_ranges_launch(zero.as<ZeroRange>(), n_zero, s);
         C.check_launch("zero");
         const int n = (int)launches.size();
         if (n > 1) AUSAXS_CUDA(cudaEventRecord(fork, s));

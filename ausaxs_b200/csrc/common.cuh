@@ -63,9 +63,6 @@ __device__ __forceinline__ uint32_t pair_residual(const PairBin& p, float c, flo
     return static_cast<uint32_t>(__float_as_int(t) - kMagicBits + kResBias);
 }
 
-// In the reference's j-loops (SimpleCalculator.h:117-141, HistogramManagerMTFFAvg.cpp:216-232)
-// the last (len mod 4) partners of each outer point go through the scalar evaluator.
-__device__ __forceinline__ int32_t tail_start(int32_t j0, int32_t n) { return n - ((n - j0) & 3); }
 
 // ---------------------------------------------------------------------------------------------
 // Five-Gaussian atomic form factors f(q) = sum_i a_i exp(-b_i q^2) + c, with b tabulated in

@@ -33,7 +33,6 @@ void Ctx::check_launch(const char* what) {
     if (e != cudaSuccess) throw Error{AUSAXS_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
 }
 
-static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 void Ctx::time_begin(int cls, cudaEvent_t* ev) {
     *ev = nullptr;
@@ -139,6 +138,19 @@ void Structure::load(const float* atoms, int n_atoms, const float* waters, int n
 
 static long long tri(long long t) { return t * (t + 1) / 2; }
 
+namespace {
+// y: range, x: chunk of the range
+__global__ void zero_ranges_kernel(const ZeroRange* ranges) {
+    const ZeroRange r = ranges[blockIdx.y];
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < r.words; k += (long long)gridDim.x * blockDim.x)
+        r.p[k] = 0;
+}
+}  // namespace
+
+void zero_ranges_launch(const ZeroRange* ranges_dev, int n, cudaStream_t s) {
+    if (n > 0) zero_ranges_kernel<<<dim3(16, n), 256, 0, s>>>(ranges_dev);
+}
+
 void append_pair_jobs(const Plan& P, int tile, bool by_class, std::vector<PairJob> (&jobs)[3], long long (&tiles)[3],
                       int (&rows)[3], int max_rows) {
     auto nt = [tile](int n) { return (n + tile - 1) / tile; };
@@ -170,6 +182,10 @@ void append_pair_jobs(const Plan& P, int tile, bool by_class, std::vector<PairJo
             pj.dsum = r0 == 0 ? j.dsum : nullptr;
             pj.wsum = r0 == 0 ? j.wsum : nullptr;
             pj.wscale = 0;  // read from device memory by weighted launches
+            pj.a_base = j.a_base;
+            pj.b_base = j.b_base;
+            pj.tail_end = j.tail_end >= 0 ? j.tail_end : j.nbp;
+            pj.tail_from_outer = j.tail_from_outer >= 0 ? j.tail_from_outer : j.self;
             jobs[g].push_back(pj);
             tiles[g] += t;
             rows[g] = std::max(rows[g], r1 - r0);
@@ -188,7 +204,7 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
                                             : "the weighted manager needs weighted atoms"};
     const int weighted = cfg.weighted_bins ? 1 : 0;
     const float inv_w = (float)(1.0 / cfg.bin_width);
-    int nb = (int)std::ceil((double)dmax * inv_w) + 2;
+    int nb = (int)std::ceil((double)(dmax + dmax_extra) * inv_w) + 2;
     nb = std::max(nb, 11);
     nb = std::min(nb, cfg.bin_count);
     if (P.manager == cfg.manager && P.weighted == weighted && P.bin_count == cfg.bin_count &&

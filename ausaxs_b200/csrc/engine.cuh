@@ -26,6 +26,8 @@ struct Error {
         if (e_ != cudaSuccess) throw ::ausaxs_b200::Error{AUSAXS_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)}; \
     } while (0)
 
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
 // A growable device allocation (grows, never shrinks; freed with its owner).
 struct DevBuf {
     void* p = nullptr;
@@ -49,6 +51,8 @@ struct JobSpec {
     unsigned long long* counts;  // [rows][nb]
     unsigned long long* dsum;    // [nb] or null
     long long* wsum;             // [nb] or null
+    // scalar-tail geometry (PairJob): -1 = a plain job (tail_end = nbp, tail_from_outer = self)
+    int a_base = 0, b_base = 0, tail_end = -1, tail_from_outer = -1;
 };
 
 // Launch plan of one structure under one histogram configuration: job table, accumulator and
@@ -95,6 +99,7 @@ struct Structure {
     int ff_to_type[kNff] = {};
     float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
     float dmax = 0;
+    float dmax_extra = 0;  // distance range kept beyond the current bounding-box diagonal (moving bodies)
     Plan plan;
 
     // copy in (host or device pointers), census, validation and dense-type conversion (one sync)
@@ -145,6 +150,13 @@ struct Ctx {
 // hold at most max_rows rows (0: the plan's own limit).
 void append_pair_jobs(const Plan& P, int tile, bool by_class, std::vector<PairJob> (&jobs)[3], long long (&tiles)[3],
                       int (&rows)[3], int max_rows = 0);
+
+// Clears n device ranges of u64 words in one launch (table in device memory).
+struct ZeroRange {
+    unsigned long long* p;
+    long long words;
+};
+void zero_ranges_launch(const ZeroRange* ranges_dev, int n, cudaStream_t s);
 
 // Tensor-core contraction (precision 0) followed by the FP64 epilogue, or FP64 only (precision 1).
 void run_debye(Ctx& C, DebyeArgs& A, int groups_present, DevBuf& tc, int precision);

@@ -150,6 +150,10 @@ extern "C" int ausaxs_gpu_histogram_mt_noalloc(const float* atoms, int32_t n_ato
         J.counts = cnt(k);
         J.dsum = weighted_bins ? dsm(k) : nullptr;
         J.wsum = wsm(k);
+        J.a_base = 0;
+        J.b_base = 0;
+        J.tail_end = sp.nbp;
+        J.tail_from_outer = sp.self;
         tiles_total += tiles;
     }
     init.clear_words = (kMiscBytes + 3 * kSlotBytes) / 8;

@@ -131,7 +131,11 @@ __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, co
     const float inv_w = J.inv_w, c = J.c, scale = J.scale;
     const unsigned nbins = static_cast<unsigned>(J.nbins);
     const int rmode = J.row_mode, rlo = J.row_lo, rhi = J.row_hi;
-    const int ts = tail_start(J.self ? i + 1 : 0, J.nb);
+    // first inner index (local) whose pair goes through the scalar evaluator: in the reference's
+    // j-loops (SimpleCalculator.h:117-141, HistogramManagerMTFFAvg.cpp:216-232) the last
+    // (row length mod 4) partners of each outer point do
+    const int row_begin = J.tail_from_outer ? J.a_base + i + 1 : 0;
+    const int ts = J.tail_end - ((J.tail_end - row_begin) & 3) - J.b_base;
     const int ta = __float_as_int(a.w);
     const bool pair_rows = rmode == kRowPair;
     const int rowbase = pair_rows ? ta * J.types : (rmode == kRowOuter ? ta : 0);
@@ -225,7 +229,7 @@ __global__ void __launch_bounds__(TILE) pairhist_kernel(PairLaunch L) {
             __syncthreads();
             pairs_since_flush += static_cast<long long>(TILE) * TILE;
             const bool diag = J.self && ti == tj;
-            const bool has_tail = j0 + jn > J.nb - 3;  // scalar-tail partners are among the last 3 inner points
+            const bool has_tail = J.b_base + j0 + jn > J.tail_end - 3;  // scalar-tail partners: last 3 of a row
             const bool general = diag || has_tail;
             const bool single = J.row_mode == kRowSingle && J.row_lo == 0 && J.row_hi >= 1;
             for (int k0 = 0; k0 < jn; k0 += kSegment) {

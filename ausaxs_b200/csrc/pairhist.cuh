@@ -35,6 +35,12 @@ struct PairJob {
     long long* wsum;             // [nbins] biased fixed-point weight-product sums, or null (weighted jobs):
                                  //         per pair rint(w_i w_j * wscale) + 2^30
     float wscale;                // unused (the launch-wide scale lives in device memory)
+    // Where this job's pairs sit in the reference's loops, for its scalar-tail rule: outer point i's
+    // row runs over inner indices [row_begin, tail_end) of the full point set, row_begin =
+    // a_base + i + 1 when tail_from_outer (self loops) else 0, and the job's inner point j is point
+    // b_base + j of that set.  A plain job: a_base = b_base = 0, tail_end = nb, tail_from_outer =
+    // self.  A partial job (one body pair of a multi-body structure) keeps the full structure's rows.
+    int32_t a_base, b_base, tail_end, tail_from_outer;
 };
 
 struct PairLaunch {

@@ -237,6 +237,56 @@ AUSAXS_API int ausaxs_gpu_batch_profile(ausaxs_gpu_batch* b, const double* q, in
 AUSAXS_API int ausaxs_gpu_batch_histogram(ausaxs_gpu_batch* b, int32_t index, ausaxs_hist_result* out);
 
 /*
+ * Rigid-body serving.  The reference's incremental manager, PartialHistogramManagerMT
+ * (PartialHistogramManagerMT.cpp:42-170, 308-341), keeps per-body self partials and per-body-pair
+ * cross partials and rebuilds the master from them after a body moves (Simple model only).  A server
+ * keeps multi-body FFAVG assemblies on the device with the same decomposition; a request moves one
+ * body (x <- R x + t, Body::rotate then Body::translate, source/core/data/Body.cpp:135-156, applied to
+ * the body's current pose), recomputes the partials between that body and the others, and returns
+ * I(q) plus the linear fit {a, b, sigma_a, sigma_b, chi2} against the assembly's target profile
+ * (ausaxs_gpu_linear_lsq).  Each pair is evaluated with the full assembly's loop geometry, so the
+ * histograms equal a full HistogramManagerMTFFAvg::calculate_all() of the moved assembly exactly.
+ *
+ * ausaxs_gpu_server_create: hbm_budget_bytes bounds the summed footprint of admitted assemblies;
+ *   max_inflight bounds requests in flight; slots_per_assembly bounds one assembly's.
+ * ausaxs_gpu_server_admit: bodies are rows [off[k], off[k+1]) of the concatenated host arrays
+ *   (atoms {x,y,z,ff}, waters {x,y,z,w}; offsets have n_bodies + 1 entries); cfg->manager must be
+ *   AUSAXS_MANAGER_FFAVG (cfg->z_exv as ausaxs_gpu_histogram); margin (A) widens the distance range
+ *   beyond the initial bounding-box diagonal for later moves; q, params: the transform of every
+ *   response; target/target_err (may be null: no fit, zeros) the fitted profile.  AUSAXS_ERR_CAPACITY
+ *   when the footprint does not fit the free budget (footprint is returned either way).
+ * ausaxs_gpu_server_submit: body -1 recomputes the current state without a move.  R is row-major
+ *   3x3.  Returns a ticket, or AUSAXS_ERR_CAPACITY when no slot is free (retry after a completion).
+ * ausaxs_gpu_server_poll / _wait: copy I(q) [n_q] and fit5 [5] (either may be null) when done; wait
+ *   gives AUSAXS_ERR_TIMEOUT after timeout_ms.  A request whose pairs fell outside the distance range
+ *   yields NaN in I(q), and so do all later requests of that assembly.
+ * ausaxs_gpu_server_body_center: the body's current centroid (for moves about it).
+ * ausaxs_gpu_server_coordinates / _histogram: current coordinates (atoms with dense type indices
+ *   in w) and histograms (as ausaxs_gpu_structure_histogram) after the assembly's last request.
+ * One server per host thread.
+ */
+typedef struct ausaxs_gpu_server ausaxs_gpu_server;
+
+AUSAXS_API int ausaxs_gpu_server_create(int32_t device, int64_t hbm_budget_bytes, int32_t max_inflight,
+                                        int32_t slots_per_assembly, ausaxs_gpu_server** out);
+AUSAXS_API int ausaxs_gpu_server_destroy(ausaxs_gpu_server* s);
+AUSAXS_API int ausaxs_gpu_server_admit(ausaxs_gpu_server* s, const ausaxs_hist_config* cfg, int32_t n_bodies,
+                                       const float* atoms, const int64_t* atom_offsets, const float* waters,
+                                       const int64_t* water_offsets, double margin, const double* q, int32_t n_q,
+                                       const ausaxs_debye_params* params, const double* target,
+                                       const double* target_err, int32_t* id, int64_t* footprint);
+AUSAXS_API int ausaxs_gpu_server_release(ausaxs_gpu_server* s, int32_t id);
+AUSAXS_API int ausaxs_gpu_server_usage(ausaxs_gpu_server* s, int64_t* used, int64_t* budget, int32_t* inflight);
+AUSAXS_API int ausaxs_gpu_server_submit(ausaxs_gpu_server* s, int32_t id, int32_t body, const double* R,
+                                        const double* t, int64_t* ticket);
+AUSAXS_API int ausaxs_gpu_server_poll(ausaxs_gpu_server* s, int64_t ticket, int32_t* done, double* Iq, double* fit5);
+AUSAXS_API int ausaxs_gpu_server_wait(ausaxs_gpu_server* s, int64_t ticket, int32_t timeout_ms, double* Iq,
+                                      double* fit5);
+AUSAXS_API int ausaxs_gpu_server_body_center(ausaxs_gpu_server* s, int32_t id, int32_t body, double* center);
+AUSAXS_API int ausaxs_gpu_server_coordinates(ausaxs_gpu_server* s, int32_t id, float* atoms_xyzw, float* waters_xyzw);
+AUSAXS_API int ausaxs_gpu_server_histogram(ausaxs_gpu_server* s, int32_t id, ausaxs_hist_result* out);
+
+/*
  * Weighted linear least squares of a model against data plus chi-square, on the device:
  * fitter::detail::LinearLeastSquares::fit (source/core/fitter/detail/LinearLeastSquares.cpp:26-55),
  * fitting model ~ a * data + b with weights 1/err^2 as LinearFitter sets it up (the measured

@@ -1,0 +1,161 @@
+"""Rigid-body serving: incremental inter-body recompute against a full recompute of the moved
+assembly, results alone vs mixed with other requests, admission by footprint and slots.
+
+Bar: exact.  Every pair keeps the full assembly's loop geometry and all accumulation is integer, so
+the master histogram after any sequence of moves equals HistogramManagerMTFFAvg::calculate_all() of
+the moved coordinates bit for bit, and I(q) equals the single-structure transform of it."""
+import numpy as np
+import pytest
+
+from ausaxs_b200 import _capi, hist, synth
+from oracle import py as O
+
+pytestmark = pytest.mark.gpu
+
+RHO = 0.334
+
+
+def _bodies(seed, sizes, waters=0.15):
+    rng = np.random.default_rng(seed)
+    atoms, wats, ffs = [], [], []
+    for k, n in enumerate(sizes):
+        xyz, ff = synth.globule(seed * 10 + k, n)
+        xyz = xyz + rng.uniform(-25, 25, 3)
+        nw = int(round(waters * n))
+        w = synth.waters(seed * 10 + k + 5, xyz, ff, nw) if nw else np.zeros((0, 3))
+        atoms.append(hist.pack(xyz, ff, True))
+        wats.append(hist.pack(w, np.ones(len(w), np.int32), True))
+        ffs.append(ff)
+    return atoms, wats, ffs
+
+
+def _cfg(atoms, volume_per_atom=18.0):
+    n = sum(len(a) for a in atoms)
+    return _capi.HistConfig(_capi.MANAGER_FFAVG, 1, 0.25, 8000, volume_per_atom * n * RHO / n)
+
+
+def _random_move(rng, center, max_deg=5.0, max_t=2.0):
+    R = synth.random_rotation(rng, max_deg)
+    t = rng.uniform(-1, 1, 3)
+    t *= max_t * rng.uniform() / max(np.linalg.norm(t), 1e-12)
+    # rotation about the body's centroid: x <- R (x - c) + c + t
+    return R, center - R @ center + t
+
+
+def _full(server, sid, ffs, cfg, q, gpu_ctx):
+    a, w = server.coordinates(sid)
+    m = hist.Molecule(atoms=a[:, :3].astype(np.float64), ff_types=np.concatenate(ffs),
+                      waters=w[:, :3].astype(np.float64), volume=cfg.z_exv * len(a) / RHO)
+    mgr = hist.HistogramManagerMTFFAvg(m, True, 0.25, 8000, gpu_ctx)
+    return mgr.calculate_all(), hist.profile(mgr, q)
+
+
+def test_moves_equal_full_recompute(gpu_ctx):
+    atoms, wats, ffs = _bodies(3, [700, 1500, 400, 1100])
+    cfg = _cfg(atoms)
+    q = np.linspace(0.005, 0.5, 120)
+    p = _capi.DebyeParams(1.0, 1.0, 1.0, 0.0, 0.0, 1.0, 1, 1e-5)
+    S = _capi.Server(hbm_budget=2 << 30)
+    sid, fp = S.admit(cfg, atoms, wats, q, p, margin=30.0)
+    assert fp > 0
+    rng = np.random.default_rng(1)
+    for step in range(6):
+        body = int(rng.integers(0, 4)) if step else -1
+        if body >= 0:
+            R, t = _random_move(rng, S.body_center(sid, body), max_deg=20.0, max_t=4.0)
+            tk = S.submit(sid, body, R, t)
+        else:
+            tk = S.submit(sid)
+        I, fit = S.wait(tk, sid)
+        h, I_full = _full(S, sid, ffs, cfg, q, gpu_ctx)
+        g = S.histogram(sid, 8000)
+        assert g["max_bin"] == h.max_bin
+        np.testing.assert_array_equal(g["aa"], h.get_raw_aa_counts_by_ff())
+        np.testing.assert_array_equal(g["aw"], h.get_raw_aw_counts_by_ff())
+        np.testing.assert_array_equal(g["ww"], h.get_raw_ww_counts_by_ff())
+        np.testing.assert_array_equal(g["d_axis"], h.get_d_axis())
+        np.testing.assert_allclose(I, I_full, rtol=1e-13, atol=0)
+    S.close()
+
+
+def test_alone_equals_mixed(gpu_ctx):
+    atoms, wats, _ = _bodies(5, [900, 600, 1300])
+    others = [_bodies(s, [800, 1000, 500]) for s in (6, 7)]
+    q = np.linspace(0.005, 0.5, 100)
+    p = _capi.DebyeParams(1.0, 1.0, 1.0, 0.0, 0.0, 1.0, 1, 1e-5)
+    rng = np.random.default_rng(2)
+    moves = [(int(rng.integers(0, 3)), synth.random_rotation(rng, 5.0), rng.uniform(-2, 2, 3)) for _ in range(8)]
+
+    S1 = _capi.Server(hbm_budget=2 << 30)
+    a_id, _ = S1.admit(_cfg(atoms), atoms, wats, q, p)
+    alone = [S1.wait(S1.submit(a_id, b, R, t), a_id)[0] for b, R, t in moves]
+    S1.close()
+
+    # the same moves with two other assemblies' moves in flight around each of them, and every
+    # move of this assembly submitted before any of its results is read
+    mixed = []
+    S3 = _capi.Server(hbm_budget=2 << 30, slots_per_assembly=8)
+    ids = [S3.admit(_cfg(o[0]), o[0], o[1], q, p)[0] for o in others]
+    a3, _ = S3.admit(_cfg(atoms), atoms, wats, q, p)
+    rng = np.random.default_rng(9)
+    pending = []
+    for b, R, t in moves:
+        other_tk = [(oid, S3.submit(oid, int(rng.integers(0, 3)), synth.random_rotation(rng, 5.0),
+                                    rng.uniform(-2, 2, 3))) for oid in ids]
+        tk = S3.submit(a3, b, R, t)
+        pending.append(tk)
+        for oid, otk in other_tk:
+            S3.wait(otk, oid)
+    for tk in pending:
+        mixed.append(S3.wait(tk, a3)[0])
+    S3.close()
+    for x, y in zip(alone, mixed):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_fit_matches_oracle_lsq(gpu_ctx):
+    atoms, wats, _ = _bodies(11, [600, 800])
+    q = np.linspace(0.005, 0.5, 80)
+    p = _capi.DebyeParams(1.0, 1.0, 1.0, 0.0, 0.0, 1.0, 1, 1e-5)
+    S = _capi.Server(hbm_budget=1 << 30)
+    sid, _ = S.admit(_cfg(atoms), atoms, wats, q, p)
+    I0, _ = S.wait(S.submit(sid), sid)
+    rng = np.random.default_rng(3)
+    target = I0 * 1.7 + 5.0 + rng.normal(0, 0.01 * np.abs(I0))
+    err = 0.01 * np.abs(I0)
+    S.close()
+    S = _capi.Server(hbm_budget=1 << 30)
+    sid, _ = S.admit(_cfg(atoms), atoms, wats, q, p, target=target, target_err=err)
+    I1, fit = S.wait(S.submit(sid, 1, synth.random_rotation(rng, 5.0), np.array([0.5, -0.3, 1.0])), sid)
+    ref = O.linear_lsq(target, I1, err)
+    np.testing.assert_allclose(fit, ref, rtol=1e-9)
+    S.close()
+
+
+def test_admission_by_footprint_and_slots(gpu_ctx):
+    atoms, wats, _ = _bodies(13, [500, 700])
+    q = np.linspace(0.005, 0.5, 50)
+    p = _capi.DebyeParams(1.0, 1.0, 1.0, 0.0, 0.0, 1.0, 1, 1e-5)
+    probe = _capi.Server(hbm_budget=1 << 40)
+    _, fp = probe.admit(_cfg(atoms), atoms, wats, q, p)
+    probe.close()
+    S = _capi.Server(hbm_budget=int(fp * 1.5), max_inflight=64, slots_per_assembly=2)
+    a, _ = S.admit(_cfg(atoms), atoms, wats, q, p)
+    with pytest.raises(_capi.AusaxsError) as e:
+        S.admit(_cfg(atoms), atoms, wats, q, p)
+    assert e.value.code == _capi.ERR_CAPACITY
+    used, budget, _ = S.usage()
+    assert used == fp and budget == int(fp * 1.5)
+    t1, t2 = S.submit(a), S.submit(a)
+    assert S.try_submit(a) is None  # both slots in flight
+    S.wait(t1, a)
+    t3 = S.submit(a)
+    S.wait(t2, a)
+    S.wait(t3, a)
+    with pytest.raises(_capi.AusaxsError) as e:
+        S.wait(t3, a)
+    assert e.value.code == _capi.ERR_NOT_FOUND
+    S.release(a)
+    b, _ = S.admit(_cfg(atoms), atoms, wats, q, p)
+    assert S.usage()[0] == fp
+    S.close()
