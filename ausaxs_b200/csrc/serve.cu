@@ -6,7 +6,8 @@
 // and :308-341): per-body self partials, per-body-pair cross partials and master = sum of partials,
 // updated as master -= old + new; it exists for the Simple model only (the form-factor variants are
 // disabled in HistogramSettings.h:34-36).  Here the FFAvg histograms (aa by type pair, aw by atom
-// type, ww) are decomposed the same way.  Every pair job carries the full assembly's row geometry
+// type, ww) are decomposed the same way, and a move recomputes every partial with the moved body,
+// its self partials included.  Every pair job carries the full assembly's row geometry
 // (PairJob a_base/b_base/tail_end), so each pair is evaluated exactly as in a full
 // HistogramManagerMTFFAvg::calculate_all() of the moved assembly; all accumulation is integer, so
 // the master (the sum of the partials) equals the full recompute bit for bit, whether a request runs
@@ -254,7 +255,11 @@ struct Assembly {
             tmp.max_group_rows = P.max_group_rows;
             std::vector<ZeroRange> zr;
             for (const Part& pt : parts) {
-                const bool moved = k == B || ((pt.k == k) != (pt.l == k));  // self partials never change
+                // every partial with the moved body, its self partials included: the moved coordinates are
+                // rounded to float, so a few of its own pairs can change bins (the reference keeps them,
+                // PartialHistogramManagerMT.cpp:118-125; recomputing keeps the master equal to a full
+                // calculate_all() of the moved coordinates)
+                const bool moved = k == B || pt.k == k || pt.l == k;
                 if (!moved) continue;
                 JobSpec j = spec_of(pt);
                 if (j.na > 0 && j.nbp > 0 && !(j.self && j.na < 2)) tmp.specs.push_back(j);
