@@ -39,7 +39,7 @@ EXPORTED = [
     "ausaxs_gpu_batch_profile_device", "ausaxs_gpu_batch_profile", "ausaxs_gpu_batch_histogram",
     "ausaxs_gpu_server_create", "ausaxs_gpu_server_destroy", "ausaxs_gpu_server_admit", "ausaxs_gpu_server_release",
     "ausaxs_gpu_server_usage", "ausaxs_gpu_server_submit", "ausaxs_gpu_server_poll", "ausaxs_gpu_server_wait",
-    "ausaxs_gpu_server_body_center", "ausaxs_gpu_server_coordinates", "ausaxs_gpu_server_histogram",
+    "ausaxs_gpu_server_completed", "ausaxs_gpu_server_body_center", "ausaxs_gpu_server_coordinates", "ausaxs_gpu_server_histogram",
 ]
 
 
@@ -125,6 +125,7 @@ def load():
         L.ausaxs_gpu_server_submit.argtypes = [vp, C.c_int32, C.c_int32, f64, f64, i64]
         L.ausaxs_gpu_server_poll.argtypes = [vp, C.c_int64, i32, f64, f64]
         L.ausaxs_gpu_server_wait.argtypes = [vp, C.c_int64, C.c_int32, f64, f64]
+        L.ausaxs_gpu_server_completed.argtypes = [vp, i64, C.c_int32, i32]
         L.ausaxs_gpu_server_body_center.argtypes = [vp, C.c_int32, C.c_int32, f64]
         L.ausaxs_gpu_server_coordinates.argtypes = [vp, C.c_int32, f32, f32]
         L.ausaxs_gpu_server_histogram.argtypes = [vp, C.c_int32, C.POINTER(HistResult)]
@@ -423,6 +424,14 @@ class Server:
         fit = np.zeros(5)
         check(load().ausaxs_gpu_server_wait(self.h, ticket, timeout_ms, dptr(I), dptr(fit)))
         return I, fit
+
+    def completed(self, capacity: int = 256):
+        """Tickets whose results are ready (collect them with poll)."""
+        out = np.zeros(capacity, np.int64)
+        n = C.c_int32(0)
+        check(load().ausaxs_gpu_server_completed(self.h, out.ctypes.data_as(C.POINTER(C.c_int64)), capacity,
+                                                 C.byref(n)))
+        return out[: n.value].tolist()
 
     def body_center(self, id: int, body: int) -> np.ndarray:
         c = np.zeros(3)

@@ -575,6 +575,22 @@ int ausaxs_gpu_server_wait(ausaxs_gpu_server* s, int64_t ticket, int32_t timeout
     });
 }
 
+int ausaxs_gpu_server_completed(ausaxs_gpu_server* s, int64_t* tickets, int32_t capacity, int32_t* n) {
+    return guarded([&] {
+        if (!s || !n || (capacity > 0 && !tickets)) throw Error{AUSAXS_ERR_ARGUMENT, "null argument"};
+        Server& S = s->impl;
+        AUSAXS_CUDA(cudaSetDevice(S.device));
+        int k = 0;
+        for (auto& r : S.inflight) {
+            if (k >= capacity) break;
+            cudaError_t e = cudaEventQuery(r.second.ev);
+            if (e == cudaSuccess) tickets[k++] = r.first;
+            else if (e != cudaErrorNotReady) throw Error{AUSAXS_ERR_CUDA, std::string("request: ") + cudaGetErrorString(e)};
+        }
+        *n = k;
+    });
+}
+
 int ausaxs_gpu_server_body_center(ausaxs_gpu_server* s, int32_t id, int32_t body, double* c) {
     return guarded([&] {
         if (!s || !c) throw Error{AUSAXS_ERR_ARGUMENT, "null argument"};

@@ -260,6 +260,8 @@ AUSAXS_API int ausaxs_gpu_batch_histogram(ausaxs_gpu_batch* b, int32_t index, au
  * ausaxs_gpu_server_poll / _wait: copy I(q) [n_q] and fit5 [5] (either may be null) when done; wait
  *   gives AUSAXS_ERR_TIMEOUT after timeout_ms.  A request whose pairs fell outside the distance range
  *   yields NaN in I(q), and so do all later requests of that assembly.
+ * ausaxs_gpu_server_completed: up to `capacity` tickets whose results are ready (not consumed:
+ *   collect them with poll).
  * ausaxs_gpu_server_body_center: the body's current centroid (for moves about it).
  * ausaxs_gpu_server_coordinates / _histogram: current coordinates (atoms with dense type indices
  *   in w) and histograms (as ausaxs_gpu_structure_histogram) after the assembly's last request.
@@ -282,6 +284,7 @@ AUSAXS_API int ausaxs_gpu_server_submit(ausaxs_gpu_server* s, int32_t id, int32_
 AUSAXS_API int ausaxs_gpu_server_poll(ausaxs_gpu_server* s, int64_t ticket, int32_t* done, double* Iq, double* fit5);
 AUSAXS_API int ausaxs_gpu_server_wait(ausaxs_gpu_server* s, int64_t ticket, int32_t timeout_ms, double* Iq,
                                       double* fit5);
+AUSAXS_API int ausaxs_gpu_server_completed(ausaxs_gpu_server* s, int64_t* tickets, int32_t capacity, int32_t* n);
 AUSAXS_API int ausaxs_gpu_server_body_center(ausaxs_gpu_server* s, int32_t id, int32_t body, double* center);
 AUSAXS_API int ausaxs_gpu_server_coordinates(ausaxs_gpu_server* s, int32_t id, float* atoms_xyzw, float* waters_xyzw);
 AUSAXS_API int ausaxs_gpu_server_histogram(ausaxs_gpu_server* s, int32_t id, ausaxs_hist_result* out);
