@@ -36,6 +36,19 @@ METRIC = "I(q) profiles/s & p99 latency vs plain GPU path at ≤1e-4 rel. I(q) e
 UNIT = "profiles/s"
 
 
+def max_over_ranks(x: float, world: int) -> float:
+    """The largest value of x over all ranks (a time: the job is as slow as its slowest rank)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -251,10 +264,7 @@ def run_batch(args, rank, world, local_rank):
         launches = ctx.launches - launches0
         step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
     total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, world)
     value = world * n * args.steps / (total_ms / 1e3)
     I_batch = I_dev.cpu().numpy().reshape(n, nq)
 
@@ -426,6 +436,8 @@ def run_serving(args, rank, world, local_rank):
 
     run(4 * chains, None)  # warm-up
     sat = run(args.steps * chains, None)
+    # whole job: every rank serves its own chains; the job lasts as long as its slowest rank
+    sat_total = world * sat["requests"] / max_over_ranks(sat["requests"] / sat["moves_per_s"], world)
     sweep = []
     for frac in (0.25, 0.5, 0.75, 0.9):
         sweep.append(run(args.steps * chains, frac * sat["moves_per_s"]))
@@ -436,7 +448,7 @@ def run_serving(args, rank, world, local_rank):
         per_move.append(np.mean([n * (tot - n) + n * (n - 1) / 2 for n in sz]))
     pairs_per_move = float(np.mean(per_move))
     line = {
-        "metric": "rigid-body moves/s (I(q) + chi2 per move) with p50/p99 latency", "value": sat["moves_per_s"],
+        "metric": "rigid-body moves/s (I(q) + chi2 per move) with p50/p99 latency", "value": sat_total,
         "unit": "moves/s", "n_gpus": world, "steps": args.steps, "warmup": 4, "ms_per_step": 1e3 / sat["moves_per_s"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 distances, u64 integer partial histograms, f64 transform and fit",
@@ -446,7 +458,7 @@ def run_serving(args, rank, world, local_rank):
                    "atoms_total": int(sum(sum(s) for s in sizes)), "pairs_per_move_mean": pairs_per_move,
                    "footprint_bytes_total": int(sum(footprints)), "admit_s": t_admit, "generate_s": t_gen,
                    "saturation": sat, "poisson_sweep": sweep},
-        "e2e": {"value": sat["moves_per_s"], "unit": "moves/s", "h2d_bytes_per_step": 96,
+        "e2e": {"value": sat_total, "unit": "moves/s", "h2d_bytes_per_step": 96,
                 "d2h_bytes_per_step": (nq + 5) * 8, "p50_ms": sat["p50_ms"], "p99_ms": sat["p99_ms"],
                 "note": "every request crosses the host ABI: pose in, I(q) and fit out"},
         "roofline": {"bound": "issue", "kernel": "pairhist_kernel", "unit": "Gpair/s",
@@ -454,6 +466,10 @@ def run_serving(args, rank, world, local_rank):
                      "peak": None, "frac": None, "traffic": None},
     }
     S.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ref_args = argparse.Namespace(steps=1, warmup=0)
+        r = run_reference_serving(ref_args, 1)
+        line["cpu_baseline"] = r.get("cpu_baseline", {"unavailable": r.get("unavailable")})
     return line
 
 
@@ -511,10 +527,7 @@ def run_ours(args, rank, world, local_rank):
         k_ms, k_n = ctx.kernel_time(0)
         ctx.enable_timing(False)
     total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local_rank}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, world)
     value = world * args.steps / (total_ms / 1e3)
     I_gpu = I_dev.cpu().numpy()
     # the same structure through the FP64 transform: deviation of the timed result
@@ -550,10 +563,7 @@ def run_ours(args, rank, world, local_rank):
         e2e_step()
         lat.append(time.perf_counter() - t0)
     e2e_total = sum(lat)
-    if world > 1:
-        t = torch.tensor([e2e_total], dtype=torch.float64, device=f"cuda:{local_rank}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_total = float(t.item())
+    e2e_total = max_over_ranks(e2e_total, world)
     e2e = world * args.steps / e2e_total
     e2e_match = float(np.max(np.abs(pin_I.numpy() / I_gpu - 1)))
 
@@ -610,7 +620,46 @@ def atomic_peak_estimate(device):
     return {}
 
 
+def run_reference_serving(args, world):
+    """The reference's answer to a rigid move of an FFAvg assembly: a full calculate_all() of the
+    moved assembly plus its transform (its partial manager exists for the Simple model only), timed on
+    one assembly of the serving workload."""
+    from ausaxs_b200 import synth
+    from oracle import py as O
+
+    if not O.ref_available():
+        return {"impl": "reference", "unavailable": "reference build oracle/_ref/libausaxs_ref.so not present"}
+    threads = max(1, (os.cpu_count() or 2) - 1)
+    O.ref(threads)
+    O.ref_set_axes(0.25, 8000, 1e-4, 1.0)
+    O.ref_set_simple_exv(False)
+    A = synth.assembly(40)
+    xyz = np.concatenate(A.bodies)
+    ff = np.concatenate(A.ff)
+    w = np.concatenate(A.weights)
+    rm = O.RefMolecule(xyz, w, ff, np.zeros((0, 3)), np.zeros(0), volume=18.0 * len(xyz))
+    rm.set_manager("ffavg")
+    times = []
+    for it in range(args.warmup + args.steps):
+        h = rm.calculate()
+        _, _, _, t_debye = h.debye()
+        if it >= args.warmup:
+            times.append(h.seconds + t_debye * (400 / 200.0))
+    v = 1.0 / statistics.median(times)
+    det = {"cores": threads, "kind": "reference",
+           "sample": f"one {len(xyz)}-atom 8-body assembly: full FFAvg calculate_all() + debye_transform() per move"}
+    return {"impl": "reference", "metric": "rigid-body moves/s (I(q) + chi2 per move) with p50/p99 latency",
+            "value": v, "unit": "moves/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 distances, f64 bins and transform (reference CPU)", "data": "synthetic (seeded generator)",
+            "config": {"workload": "cfg4 (one assembly)", "manager": "ffavg"},
+            "cpu_baseline": {"value": v, "unit": "moves/s", **det},
+            "e2e": {"value": v, "unit": "moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def run_reference(args, rank, world):
+    if args.workload == "cfg4":
+        return run_reference_serving(args, world)
     wl = workload(args.workload)
     if args.workload == "cfg3":
         v, det = time_reference_batch(wl, steps=args.steps, warmup=args.warmup, target_pairs=1e9)
