@@ -43,6 +43,14 @@ constexpr int kChunk = 512;
 constexpr int kThreads = 256;
 constexpr int kMaxRows = 264;
 
+// Excluded volume (A^3) per form_factor_t for explicit excluded volume: the reference's default set
+// constants::exv::MinimumFluctuation_implicit_H (include/core/form_factor/ExvTable.h:67-81), in the
+// order of ExvFormFactorSet::get (ExvFormFactor.h:53-72); OTHER is the argon sphere 4 pi/3 1.88^3
+// (ExvTable.h:135, vdwTable.h:13).  Entry 0 (the excluded volume itself) is never used.
+__constant__ double c_exv_volume[kNff] = {0.0,    20.911, 0.0,    12.352, 11.640, 34.583, 41.851, 0.027,
+                                          2.181,  20.562, 20.722, 14.238, 15.413, 28.529,
+                                          4.0 * 3.14159265358979323846 / 3.0 * 1.88 * 1.88 * 1.88};
+
 __device__ double ff_raw(int t, double q) {
     const FormFactor5& f = c_ff[t];
     const double s_to_q = 1.0 / (4 * 4 * kPi * kPi);
@@ -65,25 +73,59 @@ __device__ __forceinline__ double sinc64(double x) {
 
 struct QFactors {
     double f[kNff];  // raw atomic form factors at q
-    double fx;       // excluded-volume form factor at q
+    double fx;       // excluded-volume form factor at q (FFAvg, FFGrid)
+    double xe[kNff]; // per-type excluded-volume form factors at q (FFExplicit)
+    double e;        // FFExplicit exv_factor(q) = cx^3 exp(-(r^2/4)(cx^2 - 1) q^2), r = 1.62 A
     double ba, bx;   // Debye-Waller factors
     double eq2;      // exp(-q^2)
 };
 
-__device__ double row_coef(const DebyeArgs& A, const RowDesc& r, const QFactors& F, int& profile) {
+// The profiles one histogram row contributes to and with which coefficient (<= 3 terms); profile
+// indices {aa, ax, aw, xx, wx, ww} = 0..5.  Simple rows carry the cw powers of I here (the profiles
+// themselves do not), so sum_terms sign(p) * cf is the row's coefficient in I.
+struct RowTerms {
+    int n;
+    int p[3];
+    double cf[3];
+    double in_I;  // coefficient of the row's sinc sum in I
+};
+
+__device__ RowTerms row_terms(const DebyeArgs& A, const RowDesc& r, const QFactors& F) {
+    RowTerms t{};
+    auto add = [&](int p, double c) {
+        t.p[t.n] = p;
+        t.cf[t.n] = c;
+        ++t.n;
+        t.in_I += (p == 1 || p == 4) ? -c : c;
+    };
     switch (r.kind) {
-        case kRowAA: profile = 0; return (F.f[r.ta] * F.f[r.tb]) * F.ba * F.ba;
-        case kRowAX: profile = 1; return 2 * A.crho * A.cx * (F.f[r.ta] * F.fx) * F.ba * F.bx;
-        case kRowXX: profile = 3; return (A.cx * A.crho) * (A.cx * A.crho) * (F.fx * F.fx) * F.bx * F.bx;
-        case kRowAW: profile = 2; return 2 * A.cw * (F.f[r.ta] * F.f[kWater]) * F.ba;
-        case kRowWX: profile = 4; return 2 * A.crho * A.cx * A.cw * (F.fx * F.f[kWater]) * F.bx;
-        case kRowWW: profile = 5; return A.cw * A.cw * (F.f[kWater] * F.f[kWater]);
-        case kRowSAA: profile = 0; return F.eq2;
-        case kRowSAW: profile = 2; return F.eq2;
-        case kRowSWW: profile = 5; return F.eq2;
+        case kRowAA: add(0, (F.f[r.ta] * F.f[r.tb]) * F.ba * F.ba); break;
+        case kRowAX: add(1, 2 * A.crho * A.cx * (F.f[r.ta] * F.fx) * F.ba * F.bx); break;
+        case kRowXX: add(3, (A.cx * A.crho) * (A.cx * A.crho) * (F.fx * F.fx) * F.bx * F.bx); break;
+        case kRowAW: add(2, 2 * A.cw * (F.f[r.ta] * F.f[kWater]) * F.ba); break;
+        case kRowWX: add(4, 2 * A.crho * A.cx * A.cw * (F.fx * F.f[kWater]) * F.bx); break;
+        case kRowWW: add(5, A.cw * A.cw * (F.f[kWater] * F.f[kWater])); break;
+        case kRowSAA: add(0, F.eq2); break;
+        case kRowSAW:
+            add(2, F.eq2);
+            t.in_I *= A.cw;
+            break;
+        case kRowSWW:
+            add(5, F.eq2);
+            t.in_I *= A.cw * A.cw;
+            break;
+        case kRowEAA:
+            add(0, (F.f[r.ta] * F.f[r.tb]) * F.ba * F.ba);
+            add(1, A.crho * F.e * (F.f[r.ta] * F.xe[r.tb] + F.f[r.tb] * F.xe[r.ta]) * F.ba * F.bx);
+            add(3, (F.e * A.crho) * (F.e * A.crho) * (F.xe[r.ta] * F.xe[r.tb]) * F.bx * F.bx);
+            break;
+        case kRowEAW:
+            add(2, 2 * A.cw * (F.f[r.ta] * F.f[kWater]) * F.ba);
+            add(4, A.crho * F.e * A.cw * (F.f[kWater] * F.xe[r.ta] + F.f[r.ta] * F.xe[kWater]) * F.bx);
+            break;
+        default: break;
     }
-    profile = 0;
-    return 0;
+    return t;
 }
 
 __device__ void debye_body(const DebyeArgs& A, const int k) {
@@ -98,6 +140,15 @@ __device__ void debye_body(const DebyeArgs& A, const int k) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = kThreads >> 5;
 
     if (threadIdx.x < kNff) s_F.f[threadIdx.x] = ff_raw(threadIdx.x, q);
+    if (threadIdx.x >= 64 && threadIdx.x < 64 + kNff) {
+        // ExvFormFactor(V).evaluate(q) = V rho_w exp(-V^(2/3)/(4 pi) q^2) (ExvFormFactor.h:20-33)
+        const double v = c_exv_volume[threadIdx.x - 64];
+        s_F.xe[threadIdx.x - 64] = v * kRhoWater * exp(-(pow(v, 2.0 / 3) / (4 * kPi)) * q * q);
+    }
+    if (threadIdx.x == 96) {
+        const double rm2 = kAvgRadius * kAvgRadius / 4;  // exv_factor (CompositeDistanceHistogramFFExplicitBase.cpp:54-57)
+        s_F.e = pow(A.cx, 3) * exp(-rm2 * (pow(A.cx, 2) - 1) * q * q);
+    }
     if (threadIdx.x == 32) {
         if (A.exv_model == 1) {
             double e = pow(A.grid_volume, 2.0 / 3) / (4 * kPi);  // ExvFormFactor (ExvFormFactor.h:20-33)
@@ -135,9 +186,7 @@ __device__ void debye_body(const DebyeArgs& A, const int k) {
         const size_t plane = static_cast<size_t>(R) * A.nq;
         double I = 0, err = 0;
         for (int r = lane; r < R; r += 32) {
-            int p;
-            double cf = row_coef(A, A.rows[r], s_F, p);
-            double sgn = (p == 1 || p == 4) ? -1.0 : 1.0;
+            const double cf = row_terms(A, A.rows[r], s_F).in_I;
             double v = 0, bnd = 0, ha = 0;
             for (int z = 0; z < A.tc_splits; ++z) {
                 v += A.sinqd_tc[z * plane + static_cast<size_t>(r) * A.nq + k];
@@ -145,9 +194,7 @@ __device__ void debye_body(const DebyeArgs& A, const int k) {
                 ha += A.habs_tc[static_cast<size_t>(z) * R + r];
             }
             s_acc[r] = v;
-            if (A.rows[r].kind == kRowSAW) cf *= A.cw;
-            if (A.rows[r].kind == kRowSWW) cf *= A.cw * A.cw;
-            I += sgn * cf * v;
+            I += cf * v;
             err += fabs(cf) * (c_rel * bnd + c_abs * ha);
         }
         for (int o = 16; o > 0; o >>= 1) {
@@ -191,15 +238,14 @@ __device__ void debye_body(const DebyeArgs& A, const int k) {
     if (warp == 0) {
         double prof[6] = {0, 0, 0, 0, 0, 0};
         for (int r = lane; r < R; r += 32) {
-            int p;
-            double cf = row_coef(A, A.rows[r], s_F, p);
-            prof[p] += cf * s_acc[r];
+            const RowTerms t = row_terms(A, A.rows[r], s_F);
+            for (int k2 = 0; k2 < t.n; ++k2) prof[t.p[k2]] += t.cf[k2] * s_acc[r];
         }
         for (int p = 0; p < 6; ++p)
             for (int o = 16; o > 0; o >>= 1) prof[p] += __shfl_xor_sync(0xffffffffu, prof[p], o);
         if (lane == 0) {
             double I;
-            if (A.rows[0].kind >= kRowSAA) {
+            if (A.rows[0].kind >= kRowSAA && A.rows[0].kind <= kRowSWW) {
                 I = prof[0] + A.cw * prof[2] + A.cw * A.cw * prof[5];
             } else {
                 I = 0;

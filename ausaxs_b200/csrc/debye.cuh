@@ -14,7 +14,12 @@ enum RowKind : int32_t {
     kRowWW = 5,   // cw^2 F(water, water)                          -> ww
     kRowSAA = 6,  // Simple: exp(-q^2)                             -> aa
     kRowSAW = 7,  // Simple: exp(-q^2) (I gets cw)                 -> aw
-    kRowSWW = 8   // Simple: exp(-q^2) (I gets cw^2)               -> ww
+    kRowSWW = 8,  // Simple: exp(-q^2) (I gets cw^2)               -> ww
+    // FFExplicit (CompositeDistanceHistogramFFExplicitBase.cpp:64-211): one aa row serves three
+    // profiles, one aw row two, with per-type excluded-volume form factors x_t and e(q)
+    kRowEAA = 9,  // F(ta,tb) -> aa;  crho e (f_ta x_tb + f_tb x_ta) -> ax;  (e crho)^2 x_ta x_tb -> xx
+    kRowEAW = 10, // 2 cw F(ta,w) -> aw;  crho e cw (f_w x_ta + f_ta x_w) -> wx
+    kRowZero = 11 // not used by this transform (FFExplicit's exv marginal rows)
 };
 
 struct RowDesc {
@@ -33,7 +38,8 @@ struct DebyeArgs {
     const int32_t* max_bin;     // device int: bins in use
     const RowDesc* rows;        // [R]
     const unsigned long long* overflow;  // non-zero: the histogram lost pairs, I(q) is set to NaN
-    int32_t exv_model;          // 0: average exv form factor (FFAvg), 1: grid dummies of volume V
+    int32_t exv_model;          // 0: average exv form factor (FFAvg), 1: grid dummies of volume V,
+                                // 2: per-type excluded volumes (FFExplicit)
     double cw, cx, crho, dw_atomic, dw_exv, grid_volume;
     const double* q;
     int32_t nq;

@@ -455,12 +455,14 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
         rd[2] = {0, kRowSWW, 0, 0};
     } else {
         int g_ax = grid ? 1 : 0, g_xx = grid ? 2 : 0;
+        // FFExplicit: the aa and aw rows also feed the exv profiles; the exv marginal rows are unused
+        const bool ex = cfg.manager == AUSAXS_MANAGER_FFEXPLICIT;
         for (int a = 0; a < T; ++a)
-            for (int b = 0; b < T; ++b) rd[a * T + b] = {0, kRowAA, type_ff[a], type_ff[b]};
-        for (int a = 0; a < T; ++a) rd[T * T + a] = {g_ax, kRowAX, type_ff[a], kExv};
-        rd[T * T + T] = {g_xx, kRowXX, kExv, kExv};
-        for (int a = 0; a < T; ++a) rd[T * T + T + 1 + a] = {0, kRowAW, type_ff[a], kWater};
-        rd[T * T + 2 * T + 1] = {g_ax, kRowWX, kExv, kWater};
+            for (int b = 0; b < T; ++b) rd[a * T + b] = {0, ex ? kRowEAA : kRowAA, type_ff[a], type_ff[b]};
+        for (int a = 0; a < T; ++a) rd[T * T + a] = {g_ax, ex ? kRowZero : kRowAX, type_ff[a], kExv};
+        rd[T * T + T] = {g_xx, ex ? kRowZero : kRowXX, kExv, kExv};
+        for (int a = 0; a < T; ++a) rd[T * T + T + 1 + a] = {0, ex ? kRowEAW : kRowAW, type_ff[a], kWater};
+        rd[T * T + 2 * T + 1] = {g_ax, ex ? kRowZero : kRowWX, kExv, kWater};
         rd[T * T + 2 * T + 2] = {0, kRowWW, kWater, kWater};
     }
     AUSAXS_CUDA(cudaMemcpy(base + P.off_rows, rd.data(), sizeof(RowDesc) * R, cudaMemcpyHostToDevice));
@@ -500,8 +502,6 @@ void Structure::enqueue_histogram(const ausaxs_hist_config& cfg) {
 DebyeArgs Structure::debye_args(const ausaxs_hist_config& cfg, const double* q_dev, int nq, const ausaxs_debye_params& p,
                                 double* Iq_dev, double* prof_dev) {
     Plan& P = plan;
-    if (cfg.manager == AUSAXS_MANAGER_FFEXPLICIT)
-        throw Error{AUSAXS_ERR_ARGUMENT, "the Debye transform of FFEXPLICIT histograms needs per-type excluded-volume tables, which this build does not carry"};
     char* base = P.dev.as<char>();
     DebyeArgs A{};
     A.R = P.R;
@@ -514,7 +514,7 @@ DebyeArgs Structure::debye_args(const ausaxs_hist_config& cfg, const double* q_d
     A.max_bin = reinterpret_cast<const int32_t*>(base + P.off_maxbin);
     A.rows = reinterpret_cast<const RowDesc*>(base + P.off_rows);
     A.overflow = reinterpret_cast<const unsigned long long*>(base + P.off_overflow);
-    A.exv_model = grid ? 1 : 0;
+    A.exv_model = grid ? 1 : (cfg.manager == AUSAXS_MANAGER_FFEXPLICIT ? 2 : 0);
     A.cw = p.cw;
     A.cx = p.cx;
     A.crho = p.crho;
@@ -642,8 +642,6 @@ void debye_of_host_histogram(Ctx& C, const ausaxs_hist_config& cfg, const ausaxs
                              int nq, const ausaxs_debye_params& p, double* Iq, double* profiles) {
     const int mb = h.max_bin;
     if (mb <= 0 || !h.d_axis || !h.aa || !h.aw || !h.ww) throw Error{AUSAXS_ERR_ARGUMENT, "incomplete histogram"};
-    if (cfg.manager == AUSAXS_MANAGER_FFEXPLICIT)
-        throw Error{AUSAXS_ERR_ARGUMENT, "the Debye transform of FFEXPLICIT histograms needs per-type excluded-volume tables, which this build does not carry"};
     const bool mt = cfg.manager == AUSAXS_MANAGER_MT;
     const bool grid = cfg.manager == AUSAXS_MANAGER_FFGRID;
     if (grid && (!h.d_axis_ax || !h.d_axis_xx)) throw Error{AUSAXS_ERR_ARGUMENT, "grid histogram without ax/xx axes"};
@@ -670,12 +668,18 @@ void debye_of_host_histogram(Ctx& C, const ausaxs_hist_config& cfg, const ausaxs
             if (used) types.push_back(f);
         }
         int g_ax = grid ? 1 : 0, g_xx = grid ? 2 : 0;
-        for (int a : types)
-            for (int b : types) row(h.aa + (size_t)(a * kNff + b) * mb, {0, kRowAA, a, b});
-        for (int a : types) row(h.aa + (size_t)(a * kNff + kExv) * mb, {g_ax, kRowAX, a, kExv});
-        row(h.aa, {g_xx, kRowXX, kExv, kExv});
-        for (int a : types) row(h.aw + (size_t)a * mb, {0, kRowAW, a, kWater});
-        row(h.aw, {g_ax, kRowWX, kExv, kWater});
+        if (cfg.manager == AUSAXS_MANAGER_FFEXPLICIT) {
+            for (int a : types)
+                for (int b : types) row(h.aa + (size_t)(a * kNff + b) * mb, {0, kRowEAA, a, b});
+            for (int a : types) row(h.aw + (size_t)a * mb, {0, kRowEAW, a, kWater});
+        } else {
+            for (int a : types)
+                for (int b : types) row(h.aa + (size_t)(a * kNff + b) * mb, {0, kRowAA, a, b});
+            for (int a : types) row(h.aa + (size_t)(a * kNff + kExv) * mb, {g_ax, kRowAX, a, kExv});
+            row(h.aa, {g_xx, kRowXX, kExv, kExv});
+            for (int a : types) row(h.aw + (size_t)a * mb, {0, kRowAW, a, kWater});
+            row(h.aw, {g_ax, kRowWX, kExv, kWater});
+        }
         row(h.ww, {0, kRowWW, kWater, kWater});
     }
     const int R = (int)rd.size();
@@ -709,7 +713,7 @@ void debye_of_host_histogram(Ctx& C, const ausaxs_hist_config& cfg, const ausaxs
     A.max_bin = reinterpret_cast<const int32_t*>(base + off_mb);
     A.rows = reinterpret_cast<const RowDesc*>(base + off_rows);
     A.overflow = nullptr;
-    A.exv_model = grid ? 1 : 0;
+    A.exv_model = grid ? 1 : (cfg.manager == AUSAXS_MANAGER_FFEXPLICIT ? 2 : 0);
     A.cw = p.cw;
     A.cx = p.cx;
     A.crho = p.crho;

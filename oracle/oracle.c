@@ -407,12 +407,29 @@ double oracle_ff_exv_volume(double volume, double q) {
     return volume * 0.334 * exp(-e * q * q);
 }
 
+/* Excluded volume per form_factor_t of the reference's default set for explicit excluded volume,
+ * constants::exv::MinimumFluctuation_implicit_H (include/core/form_factor/ExvTable.h:67-81; OTHER
+ * uses the argon sphere, 4 pi/3 * 1.88^3, ExvTable.h:135 and vdwTable.h:13), in the order of
+ * ExvFormFactorSet::get (include/core/form_factor/ExvFormFactor.h:53-72).  Entry 0 is unused. */
+double oracle_exv_volume(int type) {
+    static const double v[NFF] = {0.0,    20.911, 0.0,    12.352, 11.640, 34.583, 41.851, 0.027,
+                                  2.181,  20.562, 20.722, 14.238, 15.413, 28.529, 0.0};
+    if (type == NFF - 1) return 4 * PI_ / 3 * 1.88 * 1.88 * 1.88;
+    return (type >= 0 && type < NFF) ? v[type] : 0.0;
+}
+
 /*
- * FFAvg / FFGrid intensity (CompositeDistanceHistogramFFAvgBase.cpp:57-76, 333-374, 470-558;
+ * FFAvg / FFGrid / FFExplicit intensity (CompositeDistanceHistogramFFAvgBase.cpp:57-76, 333-374, 470-558;
  * CompositeDistanceHistogramFFGrid.cpp:37-119).
  *   kind 0 (FFAvg): products of raw form factors, F(ff, exv) uses the raw excluded_volume entry.
  *   kind 2 (FFGrid): F(ff, exv) = f_ff * ExvFormFactor(width^3), F(exv, exv) likewise, and ax/wx
  *                    use d_axis_ax, xx uses d_axis_xx.
+ *   kind 1 (FFExplicit, CompositeDistanceHistogramFFExplicitBase.cpp:54-57, 64-211): the atom-atom
+ *                    and atom-water sinc sums serve aa/ax/xx and aw/wx with per-type excluded-volume
+ *                    form factors x_t = ExvFormFactor(V_t); ax += crho e(q) s_aa[f1][f2]
+ *                    (f_f1 x_f2 + f_f2 x_f1), xx += (e(q) crho)^2 s_aa[f1][f2] x_f1 x_f2,
+ *                    wx += crho e(q) cw s_aw[f1] (f_w x_f1 + f_f1 x_w), with
+ *                    e(q) = cx^3 exp(-(1.62^2/4)(cx^2 - 1) q^2) in place of cx.
  * Inputs: the histograms as returned by oracle_hist_ff (mb bins).  Outputs profiles[6][nq]
  * = {aa, ax, aw, xx, wx, ww} and Iq = aa - ax + aw + xx - wx + ww.
  */
@@ -444,12 +461,31 @@ void oracle_debye_ff(int kind, const double* aa, const double* aw, const double*
         double paa = 0, pax = 0, paw = 0, pxx = 0, pwx = 0, pww = 0;
         for (int f1 = 1; f1 < NFF; ++f1)
             for (int f2 = 1; f2 < NFF; ++f2) paa += s_aa[(size_t)(f1 * NFF + f2) * nq + k] * (fa[f1] * fa[f2]);
-        double cxq = cx; /* exv_factor(q) = cx for FFAvg / FFGrid */
-        for (int f1 = 1; f1 < NFF; ++f1) pax += 2 * crho * cxq * s_aa[(size_t)(f1 * NFF + 0) * nq + k] * (fa[f1] * fx);
-        pxx = pow(cxq * crho, 2) * s_aa[k] * (fx * fx);
-        for (int f1 = 1; f1 < NFF; ++f1) paw += 2 * cw * s_aw[(size_t)f1 * nq + k] * (fa[f1] * fa[1]);
-        pww = cw * cw * s_ww[k] * (fa[1] * fa[1]);
-        pwx = 2 * crho * cxq * cw * s_aw[k] * (fx * fa[1]);
+        if (kind == 1) {
+            const double rm2 = 1.62 * 1.62 / 4;
+            double e = pow(cx, 3) * exp(-rm2 * (pow(cx, 2) - 1) * qq * qq);
+            double xe[NFF];
+            for (int t = 0; t < NFF; ++t) xe[t] = oracle_ff_exv_volume(oracle_exv_volume(t), qq);
+            for (int f1 = 1; f1 < NFF; ++f1)
+                for (int f2 = 1; f2 < NFF; ++f2) {
+                    double s = s_aa[(size_t)(f1 * NFF + f2) * nq + k];
+                    pax += crho * e * s * (fa[f1] * xe[f2] + fa[f2] * xe[f1]);
+                    pxx += pow(e * crho, 2) * s * (xe[f1] * xe[f2]);
+                }
+            for (int f1 = 1; f1 < NFF; ++f1) {
+                double s = s_aw[(size_t)f1 * nq + k];
+                paw += 2 * cw * s * (fa[f1] * fa[1]);
+                pwx += crho * e * cw * s * (fa[1] * xe[f1] + fa[f1] * xe[1]);
+            }
+            pww = cw * cw * s_ww[k] * (fa[1] * fa[1]);
+        } else {
+            double cxq = cx; /* exv_factor(q) = cx for FFAvg / FFGrid */
+            for (int f1 = 1; f1 < NFF; ++f1) pax += 2 * crho * cxq * s_aa[(size_t)(f1 * NFF + 0) * nq + k] * (fa[f1] * fx);
+            pxx = pow(cxq * crho, 2) * s_aa[k] * (fx * fx);
+            for (int f1 = 1; f1 < NFF; ++f1) paw += 2 * cw * s_aw[(size_t)f1 * nq + k] * (fa[f1] * fa[1]);
+            pww = cw * cw * s_ww[k] * (fa[1] * fa[1]);
+            pwx = 2 * crho * cxq * cw * s_aw[k] * (fx * fa[1]);
+        }
         if (dw_atomic != 0 || dw_exv != 0) {
             double ba = exp(-qq * qq * dw_atomic * dw_atomic * 0.5);
             double bx = exp(-qq * qq * dw_exv * dw_exv * 0.5);

@@ -48,9 +48,8 @@ def run_case(name, atoms, ff, w, waters, ww, exv, volume, bin_width, manager, cw
         if manager == "ffgrid":
             ax, xx = h.grid_axes()
             out["d_axis_ax"], out["d_axis_xx"] = ax[: len(d)], xx[: len(d)]
-    if manager != "ffexplicit":
-        q, I, prof, _ = h.debye(cw, cx, crho, dwa, dwx)
-        out["q"], out["Iq"], out["profiles"] = q, I, prof
+    q, I, prof, _ = h.debye(cw, cx, crho, dwa, dwx)
+    out["q"], out["Iq"], out["profiles"] = q, I, prof
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
     print(name, "bins", len(d), "I" if "Iq" in out else "")
 
@@ -82,7 +81,8 @@ def main():
         run_case(f"random{k}_mt", xyz, f, wt, wat, wwt, exv, vol, bw, "mt", cw=1.3)
         run_case(f"random{k}_ffavg", xyz, f, wt, wat, wwt, exv, vol, bw, "ffavg", cw=1.1, cx=0.97, crho=1.02,
                  dwa=0.4, dwx=0.2)
-        run_case(f"random{k}_ffexplicit", xyz, f, wt, wat, wwt, exv, vol, bw, "ffexplicit")
+        run_case(f"random{k}_ffexplicit", xyz, f, wt, wat, wwt, exv, vol, bw, "ffexplicit", cw=1.1, cx=0.97,
+                 crho=1.02, dwa=0.4, dwx=0.2)
         if nx:
             run_case(f"random{k}_ffgrid", xyz, f, wt, wat, wwt, exv, vol, bw, "ffgrid", cw=0.9, cx=1.05)
     # Simple excluded volume enabled (weights shifted by -rho_w V / N, SimpleExvModel.cpp:23-28)

@@ -66,7 +66,7 @@ def test_histograms_vs_reference_golden(name, gpu_ctx):
     np.testing.assert_allclose(h.get_d_axis(), g["d_axis"], atol=d_atol(float(g["bin_width"])), rtol=0)
 
 
-@pytest.mark.parametrize("name", [c for c in golden_cases() if "ffexplicit" not in c])
+@pytest.mark.parametrize("name", golden_cases())
 def test_intensity_vs_reference_golden(name, gpu_ctx):
     g = load_golden(name)
     h = manager_for(g, gpu_ctx).calculate_all()
@@ -125,6 +125,27 @@ def test_ffgrid_vs_oracle(gpu_ctx):
                            with_profiles=True)
     Io, po = O.debye_ff(2, o, q, 1.1, 0.9)
     np.testing.assert_allclose(I, Io, rtol=1e-6, atol=1e-9 * np.abs(Io).max())
+
+
+def test_ffexplicit_vs_oracle(gpu_ctx):
+    xyz, ff, wat, _ = _random_ff(21, 2200, 500)
+    ff[::37] = 14  # some OTHER atoms (argon excluded volume)
+    m = hist.Molecule(atoms=xyz, ff_types=ff, waters=wat, volume=1.0)
+    h = hist.HistogramManagerMTFFExplicit(m, True, 0.25, 8000, gpu_ctx).calculate_all()
+    o = O.hist_ff(1, O.pack_points(xyz, ff, True), O.pack_points(wat, np.ones(len(wat), np.int32), True), None,
+                  0.25, 8000, 0.0)
+    np.testing.assert_array_equal(h.get_raw_aa_counts_by_ff(), o.aa)
+    q = np.linspace(0.005, 0.8, 250)
+    h.apply_water_scaling_factor(1.07)
+    h.apply_excluded_volume_scaling_factor(1.04)
+    h.apply_solvent_density_scaling_factor(0.98)
+    h.apply_atomic_debye_waller_factor(0.3)
+    _, I = h.debye_transform(q)
+    Io, po = O.debye_ff(1, o, q, 1.07, 1.04, 0.98, 0.3, 0.0)
+    np.testing.assert_allclose(I, Io, rtol=1e-6, atol=1e-9 * np.abs(Io).max())
+    prof = h.profiles(q)
+    for k in range(6):
+        np.testing.assert_allclose(prof[k], po[k], rtol=1e-6, atol=1e-9 * max(np.abs(po[k]).max(), 1.0))
 
 
 def test_mt_vs_oracle(gpu_ctx):

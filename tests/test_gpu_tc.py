@@ -30,7 +30,7 @@ def _pair(h, q, ctx, tolerance):
 
 def _cases(ctx):
     out = []
-    for name in [c for c in golden_cases() if "ffexplicit" not in c]:
+    for name in golden_cases():
         g = load_golden(name)
         h = manager_for(g, ctx).calculate_all()
         cw, cx, crho, dwa, dwx = g["params"]

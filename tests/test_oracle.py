@@ -40,7 +40,7 @@ def test_oracle_histograms_match_reference(name):
     np.testing.assert_allclose(o.d_axis, g["d_axis"], rtol=0, atol=1e-9)
 
 
-@pytest.mark.parametrize("name", [c for c in CASES if "ffexplicit" not in c])
+@pytest.mark.parametrize("name", CASES)
 def test_oracle_intensity_matches_reference(name):
     g = load_golden(name)
     o = oracle_for(g)
@@ -50,7 +50,7 @@ def test_oracle_intensity_matches_reference(name):
         I = O.debye_simple(o, q, cw)
         np.testing.assert_allclose(I, g["Iq"], rtol=1e-10)
         return
-    kind = {"ffavg": 0, "ffgrid": 2}[str(g["manager"])]
+    kind = {"ffavg": 0, "ffexplicit": 1, "ffgrid": 2}[str(g["manager"])]
     I, prof = O.debye_ff(kind, o, q, cw, cx, crho, dwa, dwx)
     scale = np.abs(g["Iq"]).max()
     np.testing.assert_allclose(I, g["Iq"], rtol=1e-9, atol=1e-12 * scale)
