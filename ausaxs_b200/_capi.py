@@ -39,7 +39,7 @@ EXPORTED = [
     "ausaxs_gpu_batch_profile_device", "ausaxs_gpu_batch_profile", "ausaxs_gpu_batch_histogram",
     "ausaxs_gpu_server_create", "ausaxs_gpu_server_destroy", "ausaxs_gpu_server_admit", "ausaxs_gpu_server_release",
     "ausaxs_gpu_server_usage", "ausaxs_gpu_server_submit", "ausaxs_gpu_server_poll", "ausaxs_gpu_server_wait",
-    "ausaxs_gpu_server_completed", "ausaxs_gpu_server_body_center", "ausaxs_gpu_server_coordinates", "ausaxs_gpu_server_histogram",
+    "ausaxs_gpu_server_completed", "ausaxs_gpu_server_launch_count", "ausaxs_gpu_server_body_center", "ausaxs_gpu_server_coordinates", "ausaxs_gpu_server_histogram",
 ]
 
 
@@ -126,6 +126,7 @@ def load():
         L.ausaxs_gpu_server_poll.argtypes = [vp, C.c_int64, i32, f64, f64]
         L.ausaxs_gpu_server_wait.argtypes = [vp, C.c_int64, C.c_int32, f64, f64]
         L.ausaxs_gpu_server_completed.argtypes = [vp, i64, C.c_int32, i32]
+        L.ausaxs_gpu_server_launch_count.argtypes = [vp, i64]
         L.ausaxs_gpu_server_body_center.argtypes = [vp, C.c_int32, C.c_int32, f64]
         L.ausaxs_gpu_server_coordinates.argtypes = [vp, C.c_int32, f32, f32]
         L.ausaxs_gpu_server_histogram.argtypes = [vp, C.c_int32, C.POINTER(HistResult)]
@@ -432,6 +433,11 @@ class Server:
         check(load().ausaxs_gpu_server_completed(self.h, out.ctypes.data_as(C.POINTER(C.c_int64)), capacity,
                                                  C.byref(n)))
         return out[: n.value].tolist()
+
+    def launches(self) -> int:
+        n = C.c_int64(0)
+        check(load().ausaxs_gpu_server_launch_count(self.h, C.byref(n)))
+        return n.value
 
     def body_center(self, id: int, body: int) -> np.ndarray:
         c = np.zeros(3)

@@ -52,6 +52,25 @@ __device__ __forceinline__ PairBin pair_eval(float4 a, float4 b, float inv_w, bo
     return r;
 }
 
+// pair_eval without the scalar-tail rule (the SIMD evaluators), with the range check folded into the
+// magic-number rounding: xm = kMagic + rint(x) exactly while x < 2^22, so rint(x) < nbins is
+// xm < kMagic + nbins (bin_limit, exact in float); NaN, infinite and huge distances fail it too.
+__device__ __forceinline__ bool pair_eval_simd(float4 a, float4 b, float inv_w, float bin_limit, PairBin& r) {
+    const float dx = __fsub_rn(a.x, b.x);
+    const float dy = __fsub_rn(a.y, b.y);
+    const float dz = __fsub_rn(a.z, b.z);
+    const float s = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+    r.d = __fsqrt_rn(s);
+    const float xm = __fadd_rn(__fmul_rn(r.d, inv_w), kMagic);
+    if (!(xm < bin_limit)) return false;
+    r.bin = __float_as_int(xm) - kMagicBits;
+    r.xr = __fsub_rn(xm, kMagic);
+    return true;
+}
+__host__ __device__ inline float pair_bin_limit(int nbins) {
+    return kMagic + static_cast<float>(nbins < (1 << 22) ? nbins : (1 << 22));
+}
+
 // Fixed-point in-bin offset of a pair: the distance is d = bin*c + r with |r| <= c/2 (1 + 2^-10)
 // (c = 1/inv_w rounded to float), r is stored as rint(r * scale) + kResBias in [0, 2^16) with
 // scale = 2^15 / c * (1 - 2^-8).  Sums of these are exact integers, so the per-bin mean distance
@@ -59,7 +78,7 @@ __device__ __forceinline__ PairBin pair_eval(float4 a, float4 b, float inv_w, bo
 // default 0.25 A bins, 3.1e-6 A at 0.1 A), and rounding errors of many pairs average out.
 __device__ __forceinline__ uint32_t pair_residual(const PairBin& p, float c, float scale) {
     float r = __fmaf_rn(-p.xr, c, p.d);
-    float t = __fadd_rn(__fmul_rn(r, scale), kMagic);
+    float t = __fmaf_rn(r, scale, kMagic);  // rint(r * scale), one rounding
     return static_cast<uint32_t>(__float_as_int(t) - kMagicBits + kResBias);
 }
 

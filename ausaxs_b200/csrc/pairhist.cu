@@ -123,13 +123,18 @@ __device__ __forceinline__ void flush_hist(const PairJob& J, const Onchip& S) {
 }
 
 // Pairs of one outer point against inner points [k0, k1) of the staged tile.  GENERAL handles the
-// diagonal tiles of self jobs (j > i only) and the tiles that contain scalar-tail partners; SINGLE
-// is a one-row job whose count index is the bin itself.
-template <bool GENERAL, bool WEIGHTED, bool SINGLE>
+// diagonal tiles of self jobs (j > i only) and the tiles that contain scalar-tail partners.  ROWS
+// selects the count row: kRowsSingle, one row whose index is the bin; kRowsOffset, every row of the
+// job is on chip and the staged inner points carry their row offset (inner type * pitch for pair
+// rows, 0 for outer rows) in w; kRowsGeneric, a row group of a job whose rows do not all fit.
+enum { kRowsSingle = 0, kRowsOffset = 1, kRowsGeneric = 2 };
+
+template <bool GENERAL, bool WEIGHTED, int ROWS>
 __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, const float4* s_pts, const float4 a, int i,
                                            int j0, int k0, int k1, bool diag, float wsc, unsigned long long& overflow) {
     const float inv_w = J.inv_w, c = J.c, scale = J.scale;
     const unsigned nbins = static_cast<unsigned>(J.nbins);
+    const float bin_limit = pair_bin_limit(J.nbins);
     const int rmode = J.row_mode, rlo = J.row_lo, rhi = J.row_hi;
     // first inner index (local) whose pair goes through the scalar evaluator: in the reference's
     // j-loops (SimpleCalculator.h:117-141, HistogramManagerMTFFAvg.cpp:216-232) the last
@@ -139,25 +144,32 @@ __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, co
     const int ta = __float_as_int(a.w);
     const bool pair_rows = rmode == kRowPair;
     const int rowbase = pair_rows ? ta * J.types : (rmode == kRowOuter ? ta : 0);
-    const int full_rows = pair_rows ? J.types * J.types : (rmode == kRowOuter ? J.types : 1);
-    const bool all_rows = rlo == 0 && rhi >= full_rows;
+    const int cnt_base = (rowbase - rlo) * S.pad;  // kRowsOffset: + inner offset + bin
     const bool do_d = J.dsum != nullptr;
     const bool do_w = WEIGHTED && J.wsum != nullptr;
 #pragma unroll 4
     for (int jj = k0; jj < k1; ++jj) {
         const float4 b = s_pts[jj];
-        const int j = j0 + jj;
-        if (GENERAL && diag && j <= i) continue;
-        const PairBin p = pair_eval(a, b, inv_w, GENERAL && j >= ts);
-        if (static_cast<unsigned>(p.bin) >= nbins) {
+        PairBin p;
+        if (GENERAL) {
+            const int j = j0 + jj;
+            if (diag && j <= i) continue;
+            p = pair_eval(a, b, inv_w, j >= ts);
+            if (static_cast<unsigned>(p.bin) >= nbins) {
+                ++overflow;
+                continue;
+            }
+        } else if (!pair_eval_simd(a, b, inv_w, bin_limit, p)) {
             ++overflow;
             continue;
         }
-        if (SINGLE) {
+        if (ROWS == kRowsSingle) {
             atomicAdd(&S.cnt[p.bin], 1u);
+        } else if (ROWS == kRowsOffset) {
+            atomicAdd(&S.cnt[cnt_base + __float_as_int(b.w) + p.bin], 1u);
         } else {
             const int row = pair_rows ? rowbase + __float_as_int(b.w) : rowbase;
-            if (all_rows || (row >= rlo && row < rhi)) atomicAdd(&S.cnt[(row - rlo) * S.pad + p.bin], 1u);
+            if (row >= rlo && row < rhi) atomicAdd(&S.cnt[(row - rlo) * S.pad + p.bin], 1u);
         }
         if (do_d) atomicAdd(&S.dacc[p.bin], pair_residual(p, c, scale));
         if (do_w) {
@@ -169,7 +181,7 @@ __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, co
 }
 
 template <int TILE, bool WEIGHTED>
-__global__ void __launch_bounds__(TILE) pairhist_kernel(PairLaunch L) {
+__global__ void __launch_bounds__(TILE, 1024 / TILE) pairhist_kernel(PairLaunch L) {
     extern __shared__ __align__(16) unsigned char smem[];
     Onchip S;
     S.pad = L.smem_bins + 1;
@@ -221,8 +233,16 @@ __global__ void __launch_bounds__(TILE) pairhist_kernel(PairLaunch L) {
             tile_coords(J, g - J.tile_begin, ti, tj);
             const int j0 = tj * TILE;
             const int jn = min(TILE, J.nb - j0);
+            const bool single = J.row_mode == kRowSingle && J.row_lo == 0 && J.row_hi >= 1;
+            const int full_rows = J.row_mode == kRowPair ? J.types * J.types : (J.row_mode == kRowOuter ? J.types : 1);
+            const bool offset_rows = !single && J.row_lo == 0 && J.row_hi >= full_rows;
             __syncthreads();  // previous tile done with s_pts
-            if (threadIdx.x < jn) s_pts[threadIdx.x] = J.B[j0 + threadIdx.x];
+            if (threadIdx.x < jn) {
+                float4 v = J.B[j0 + threadIdx.x];
+                // row offset of the inner point for jobs with every row on chip
+                if (offset_rows) v.w = __int_as_float(J.row_mode == kRowPair ? __float_as_int(v.w) * S.pad : 0);
+                s_pts[threadIdx.x] = v;
+            }
             const int i = ti * TILE + threadIdx.x;
             const bool active = i < J.na;
             const float4 a = active ? J.A[i] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -231,16 +251,17 @@ __global__ void __launch_bounds__(TILE) pairhist_kernel(PairLaunch L) {
             const bool diag = J.self && ti == tj;
             const bool has_tail = J.b_base + j0 + jn > J.tail_end - 3;  // scalar-tail partners: last 3 of a row
             const bool general = diag || has_tail;
-            const bool single = J.row_mode == kRowSingle && J.row_lo == 0 && J.row_hi >= 1;
             for (int k0 = 0; k0 < jn; k0 += kSegment) {
                 const int k1 = min(jn, k0 + kSegment);
                 if (active) {
                     if (general) {
-                        if (single) tile_pairs<true, WEIGHTED, true>(J, S, s_pts, a, i, j0, k0, k1, diag, wsc, overflow);
-                        else tile_pairs<true, WEIGHTED, false>(J, S, s_pts, a, i, j0, k0, k1, diag, wsc, overflow);
+                        if (single) tile_pairs<true, WEIGHTED, kRowsSingle>(J, S, s_pts, a, i, j0, k0, k1, diag, wsc, overflow);
+                        else if (offset_rows) tile_pairs<true, WEIGHTED, kRowsOffset>(J, S, s_pts, a, i, j0, k0, k1, diag, wsc, overflow);
+                        else tile_pairs<true, WEIGHTED, kRowsGeneric>(J, S, s_pts, a, i, j0, k0, k1, diag, wsc, overflow);
                     } else {
-                        if (single) tile_pairs<false, WEIGHTED, true>(J, S, s_pts, a, i, j0, k0, k1, false, wsc, overflow);
-                        else tile_pairs<false, WEIGHTED, false>(J, S, s_pts, a, i, j0, k0, k1, false, wsc, overflow);
+                        if (single) tile_pairs<false, WEIGHTED, kRowsSingle>(J, S, s_pts, a, i, j0, k0, k1, false, wsc, overflow);
+                        else if (offset_rows) tile_pairs<false, WEIGHTED, kRowsOffset>(J, S, s_pts, a, i, j0, k0, k1, false, wsc, overflow);
+                        else tile_pairs<false, WEIGHTED, kRowsGeneric>(J, S, s_pts, a, i, j0, k0, k1, false, wsc, overflow);
                     }
                 }
                 if (J.dsum) {

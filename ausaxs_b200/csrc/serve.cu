@@ -575,6 +575,15 @@ int ausaxs_gpu_server_wait(ausaxs_gpu_server* s, int64_t ticket, int32_t timeout
     });
 }
 
+int ausaxs_gpu_server_launch_count(ausaxs_gpu_server* s, int64_t* launches) {
+    return guarded([&] {
+        if (!s || !launches) throw Error{AUSAXS_ERR_ARGUMENT, "null argument"};
+        long long n = 0;
+        for (auto& a : s->impl.asms) n += a.second->C.launches;
+        *launches = n;
+    });
+}
+
 int ausaxs_gpu_server_completed(ausaxs_gpu_server* s, int64_t* tickets, int32_t capacity, int32_t* n) {
     return guarded([&] {
         if (!s || !n || (capacity > 0 && !tickets)) throw Error{AUSAXS_ERR_ARGUMENT, "null argument"};

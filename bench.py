@@ -435,7 +435,10 @@ def run_serving(args, rank, world, local_rank):
                 "mean_ms": float(lat.mean())}
 
     run(4 * chains, None)  # warm-up
-    sat = run(args.steps * chains, None)
+    launches0 = S.launches()
+    with ClockSampler(local_rank) as clk:
+        sat = run(args.steps * chains, None)
+    sat_launches = S.launches() - launches0
     # whole job: every rank serves its own chains; the job lasts as long as its slowest rank
     sat_total = world * sat["requests"] / max_over_ranks(sat["requests"] / sat["moves_per_s"], world)
     sweep = []
@@ -461,10 +464,17 @@ def run_serving(args, rank, world, local_rank):
         "e2e": {"value": sat_total, "unit": "moves/s", "h2d_bytes_per_step": 96,
                 "d2h_bytes_per_step": (nq + 5) * 8, "p50_ms": sat["p50_ms"], "p99_ms": sat["p99_ms"],
                 "note": "every request crosses the host ABI: pose in, I(q) and fit out"},
-        "roofline": {"bound": "issue", "kernel": "pairhist_kernel", "unit": "Gpair/s",
-                     "achieved": pairs_per_move * sat["moves_per_s"] / 1e9,
-                     "peak": None, "frac": None, "traffic": None},
+        "gpu_launches": int(sat_launches),
+        "clocks": clk.summary(),
     }
+    peaks, _ = load_peaks()
+    sm_mhz = line["clocks"].get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+    sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
+    issue_peak = sms * 4 * sm_mhz * 1e6 * 32 / INSTR_PER_PAIR
+    achieved = pairs_per_move * sat["moves_per_s"]
+    line["roofline"] = {"bound": "issue", "kernel": "pairhist_kernel", "unit": "Gpair/s", "achieved": achieved / 1e9,
+                        "peak": issue_peak / 1e9, "frac": achieved / issue_peak, "traffic": None,
+                        "note": "pair evaluations of the saturated serving run (moved body x the rest + its own pairs)"}
     S.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ref_args = argparse.Namespace(steps=1, warmup=0)

@@ -284,6 +284,8 @@ AUSAXS_API int ausaxs_gpu_server_submit(ausaxs_gpu_server* s, int32_t id, int32_
 AUSAXS_API int ausaxs_gpu_server_poll(ausaxs_gpu_server* s, int64_t ticket, int32_t* done, double* Iq, double* fit5);
 AUSAXS_API int ausaxs_gpu_server_wait(ausaxs_gpu_server* s, int64_t ticket, int32_t timeout_ms, double* Iq,
                                       double* fit5);
+/* Kernels launched for the admitted assemblies so far (instrumentation, as ausaxs_gpu_ctx_launch_count). */
+AUSAXS_API int ausaxs_gpu_server_launch_count(ausaxs_gpu_server* s, int64_t* launches);
 AUSAXS_API int ausaxs_gpu_server_completed(ausaxs_gpu_server* s, int64_t* tickets, int32_t capacity, int32_t* n);
 AUSAXS_API int ausaxs_gpu_server_body_center(ausaxs_gpu_server* s, int32_t id, int32_t body, double* center);
 AUSAXS_API int ausaxs_gpu_server_coordinates(ausaxs_gpu_server* s, int32_t id, float* atoms_xyzw, float* waters_xyzw);
