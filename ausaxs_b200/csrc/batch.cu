@@ -55,6 +55,9 @@ struct Batch {
     std::vector<Launch> launches;
     int choice = -1;
     DevBuf jobs, misc, zero, fin, args;  // misc: tile counters [16], overflow at [16]
+    DevBuf d_stats;                      // census of every structure (creation only)
+    DevBuf arena;                        // every structure's point arrays
+    PrepStats* h_stats = nullptr;        // pinned slots owned by the context
     int n_zero = 0;
     cudaStream_t side[2] = {nullptr, nullptr};
     cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
@@ -70,6 +73,7 @@ struct Batch {
     } key;
 
     ~Batch() {
+        if (ctx && ctx->stream) cudaStreamSynchronize(ctx->stream);
         if (exec) cudaGraphExecDestroy(exec);
         for (auto& st : side)
             if (st) cudaStreamDestroy(st);
@@ -88,22 +92,51 @@ struct Batch {
         const bool grid = c.manager == AUSAXS_MANAGER_FFGRID;
         if (grid && !xoff) throw Error{AUSAXS_ERR_ARGUMENT, "FFGRID batches need excluded-volume offsets"};
         cfg = c;
+        // every structure's copies and census first, one synchronisation, then validation and plans
+        h_stats = ctx->stats_slots(n);
+        d_stats.ensure(sizeof(PrepStats) * n);
+        // one arena for every structure's point arrays (raw atoms, waters, dummies, dense atoms, type
+        // table) instead of five allocations per structure
+        auto pts = [](int64_t k) { return align_up((size_t)std::max<int64_t>(1, k) * 16, 256); };
+        size_t arena_bytes = 0;
         for (int i = 0; i < n; ++i) {
             const int64_t na = aoff[i + 1] - aoff[i], nw = woff[i + 1] - woff[i];
             const int64_t nx = grid ? xoff[i + 1] - xoff[i] : 0;
             if (na < 0 || nw < 0 || nx < 0 || na > INT32_MAX || nw > INT32_MAX || nx > INT32_MAX)
                 throw Error{AUSAXS_ERR_ARGUMENT, "bad offsets"};
+            arena_bytes += 2 * pts(na) + pts(nw) + pts(nx) + 256;
+        }
+        arena.ensure(arena_bytes);
+        size_t at = 0;
+        for (int i = 0; i < n; ++i) {
+            const int64_t na = aoff[i + 1] - aoff[i], nw = woff[i + 1] - woff[i];
+            const int64_t nx = grid ? xoff[i + 1] - xoff[i] : 0;
             auto S = std::make_unique<Structure>();
             S->ctx = ctx;
-            S->load(atoms ? atoms + 4 * aoff[i] : nullptr, (int)na, waters ? waters + 4 * woff[i] : nullptr, (int)nw,
-                    grid && exv ? exv + 4 * xoff[i] : nullptr, (int)nx, 1, host);
+            auto take = [&](DevBuf& b, size_t bytes) {
+                b.view(arena.as<char>(at), bytes);
+                at += bytes;
+            };
+            take(S->raw_a, pts(na));
+            take(S->dense_a, pts(na));
+            take(S->raw_w, pts(nw));
+            take(S->raw_x, pts(nx));
+            take(S->meta, 256);
+            S->load_begin(atoms ? atoms + 4 * aoff[i] : nullptr, (int)na, waters ? waters + 4 * woff[i] : nullptr,
+                          (int)nw, grid && exv ? exv + 4 * xoff[i] : nullptr, (int)nx, 1, host, h_stats + i,
+                          d_stats.as<PrepStats>() + i);
+            items.push_back(std::move(S));
+        }
+        AUSAXS_CUDA(cudaStreamSynchronize(ctx->stream));
+        for (int i = 0; i < n; ++i) {
+            Structure& S = *items[i];
+            S.load_end(h_stats[i]);
             ausaxs_hist_config ci = c;
             if (z_exv) ci.z_exv = z_exv[i];
-            S->plan_for(ci);
-            max_nb = std::max(max_nb, S->plan.nb);
-            pairs += S->plan.pairs;
+            S.plan_for(ci);
+            max_nb = std::max(max_nb, S.plan.nb);
+            pairs += S.plan.pairs;
             cfgs.push_back(ci);
-            items.push_back(std::move(S));
         }
         order.resize(n);
         std::iota(order.begin(), order.end(), 0);

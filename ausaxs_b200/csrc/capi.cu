@@ -81,6 +81,7 @@ int ausaxs_gpu_ctx_destroy(ausaxs_gpu_ctx* ctx) {
         cudaStreamSynchronize(C.stream);
         C.scratch.reset();
         if (C.h_stats) cudaFreeHost(C.h_stats);
+        if (C.h_stats_many) cudaFreeHost(C.h_stats_many);
         if (C.own_stream) cudaStreamDestroy(C.stream);
         delete ctx;
     });

@@ -81,8 +81,9 @@ struct TcArgs {
     int32_t* error_flag;
 };
 bool debye_tc_launch(const TcArgs& A, cudaStream_t s);
-// K splits for a contraction of up to `bins` bins, R rows and nq q values (fills the SMs once)
-int debye_tc_splits(int R, int bins, int nq, int sms);
+// K splits for a contraction of up to `bins` bins, R rows, nq q values and `groups` distance axes
+// (fills the SMs once)
+int debye_tc_splits(int R, int bins, int nq, int sms, int groups);
 // bins of one K split when max_bin bins are in use (multiple of the 64-bin staging chunk)
 __host__ __device__ inline int debye_tc_split_bins(int max_bin, int splits) {
     const int chunks = (max_bin + 63) / 64;

@@ -6,7 +6,7 @@
 // (CompositeDistanceHistogramFFAvgBase.cpp:427-467 computes it as R*Q inner products in FP64).
 // Each CTA owns a 128-row x 128-q tile of one K split (a contiguous bin range) for one distance
 // axis g; the partial sums of the splits are added in FP64 by the epilogue (debye.cu).
-//   * staging: thread m converts row m of H (FP64 -> FP32) for the chunk's 64 bins and splits it
+//   * staging: threads m and m + 128 convert row m of H (FP64 -> FP32) for the chunk's 64 bins and splits it
 //     into three BF16 terms hi + mid + lo (exact for an FP32 value); thread n generates the sinc
 //     values of q n on the fly from the distance axis (FP32) and splits them likewise; rounded-up
 //     BF16 magnitudes |H|, |S| go to two more tiles.  Tiles use the no-swizzle K-major core-matrix
@@ -29,7 +29,7 @@ namespace {
 constexpr int kM = 128;         // rows per CTA (UMMA M)
 constexpr int kN = 128;         // q values per CTA (UMMA N)
 constexpr int kKC = 64;         // bins per staged chunk (4 UMMA K-steps of 16)
-constexpr int kThreadsTC = 128;
+constexpr int kThreadsTC = 256;  // two threads per operand row / q column (halves of a K chunk)
 constexpr int kTileBytes = kM * kKC * 2;  // one BF16 operand tile, 16 KiB
 constexpr int kTmemCols = 512;            // main, correction, bound accumulators (128 columns each)
 constexpr int kColCorr = kN, kColBound = 2 * kN;
@@ -166,8 +166,10 @@ __global__ void __launch_bounds__(kThreadsTC, 1) debye_tc_kernel(TcParams P) {
     __shared__ uint32_t s_tmem;
     __shared__ int s_fail;
     __shared__ float s_ax[kKC];
+    __shared__ float s_habs[kM];
 
     const int tid = threadIdx.x, warp = tid >> 5;
+    const int m = tid & (kM - 1), half = tid >> 7;  // operand row / q column, half of the K chunk
     const int split = blockIdx.z / 3, g = blockIdx.z % 3;
     const int q0 = blockIdx.x * kN;
     const int r0 = blockIdx.y * kM;
@@ -176,15 +178,15 @@ __global__ void __launch_bounds__(kThreadsTC, 1) debye_tc_kernel(TcParams P) {
     const int kb = split * per, ke = min(mb, kb + per);
     const double* axis = P.axis[g];
 
-    // thread tid stages row r0 + tid of H and q value q0 + tid of S
-    const int r = r0 + tid;
+    // threads m and m + 128 stage row r0 + m of H and q value q0 + m of S (one half of a chunk each)
+    const int r = r0 + m;
     const bool row_on = r < P.R && P.rows[r].group == g;
     if (!__syncthreads_or(row_on)) return;  // no row of this tile uses distance axis g
     float* out_v = P.sinqd + static_cast<size_t>(split) * P.R * P.nq;
     float* out_b = P.bound + static_cast<size_t>(split) * P.R * P.nq;
     if (kb >= ke) {
         // this split holds no bins: its partial sums are zero
-        if (row_on) {
+        if (row_on && half == 0) {
             for (int j = 0; j < kN && q0 + j < P.nq; ++j) {
                 out_v[static_cast<size_t>(r) * P.nq + q0 + j] = 0.f;
                 out_b[static_cast<size_t>(r) * P.nq + q0 + j] = 0.f;
@@ -193,8 +195,8 @@ __global__ void __launch_bounds__(kThreadsTC, 1) debye_tc_kernel(TcParams P) {
         }
         return;
     }
-    const float qn = q0 + tid < P.nq ? static_cast<float>(P.q[q0 + tid]) : 0.f;
-    const bool q_on = q0 + tid < P.nq;
+    const float qn = q0 + m < P.nq ? static_cast<float>(P.q[q0 + m]) : 0.f;
+    const bool q_on = q0 + m < P.nq;
     const double* hrow = row_on ? P.H + static_cast<size_t>(r) * P.nb : nullptr;
 
     if (tid == 0) {
@@ -220,9 +222,9 @@ __global__ void __launch_bounds__(kThreadsTC, 1) debye_tc_kernel(TcParams P) {
     for (int k0 = kb; k0 < ke; k0 += kKC) {
         if (tid < kKC) s_ax[tid] = k0 + tid < ke ? static_cast<float>(axis[k0 + tid]) : 0.f;
         __syncthreads();
-        // ---- stage the operand tiles of this chunk: row tid of A, column tid of B ----
+        // ---- stage the operand tiles of this chunk: row m of A, column m of B, this thread's half ----
 #pragma unroll 1
-        for (int kg = 0; kg < kKC / 8; ++kg) {
+        for (int kg = half * (kKC / 16); kg < (half + 1) * (kKC / 16); ++kg) {
             float hv[8], sv[8];
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
@@ -237,7 +239,7 @@ __global__ void __launch_bounds__(kThreadsTC, 1) debye_tc_kernel(TcParams P) {
                 }
                 sv[j] = sc;
             }
-            const int off = tile_offset(tid, kg * 8);
+            const int off = tile_offset(m, kg * 8);
             const Split8 a = split8(hv);
             *reinterpret_cast<uint4*>(A_hi + off) = a.hi;
             *reinterpret_cast<uint4*>(A_mid + off) = a.mid;
@@ -285,9 +287,10 @@ __global__ void __launch_bounds__(kThreadsTC, 1) debye_tc_kernel(TcParams P) {
 
     if (!s_fail) {
         asm volatile("tcgen05.fence::after_thread_sync;");
-        const uint32_t lane_base = static_cast<uint32_t>(warp * 32) << 16;  // this warp's TMEM lanes
+        // warp w reads TMEM lanes 32 (w % 4) .. +31 (its rows), the two halves split the q columns
+        const uint32_t lane_base = static_cast<uint32_t>((warp & 3) * 32) << 16;
 #pragma unroll 1
-        for (int c0 = 0; c0 < kN; c0 += 32) {
+        for (int c0 = half * (kN / 2); c0 < (half + 1) * (kN / 2); c0 += 32) {
             float vm[32], vc[32], vb[32];
             tmem_ld32(tmem + lane_base + c0, vm);
             tmem_ld32(tmem + lane_base + kColCorr + c0, vc);
@@ -303,7 +306,9 @@ __global__ void __launch_bounds__(kThreadsTC, 1) debye_tc_kernel(TcParams P) {
                 }
             }
         }
-        if (row_on && blockIdx.x == 0) P.habs[static_cast<size_t>(split) * P.R + r] = habs;
+        if (half == 1) s_habs[m] = habs;
+        __syncthreads();
+        if (half == 0 && row_on && blockIdx.x == 0) P.habs[static_cast<size_t>(split) * P.R + r] = habs + s_habs[m];
     } else {
         // the MMAs of the timed-out chunk may still be running: wait for them (bounded) before
         // the tensor memory is released
@@ -319,8 +324,8 @@ __global__ void __launch_bounds__(kThreadsTC, 1) debye_tc_kernel(TcParams P) {
 
 size_t debye_tc_smem_bytes() { return 8 * static_cast<size_t>(kTileBytes) + 1024; }
 
-int debye_tc_splits(int R, int bins, int nq, int sms) {
-    const long long tiles = (long long)((nq + kN - 1) / kN) * ((R + kM - 1) / kM);
+int debye_tc_splits(int R, int bins, int nq, int sms, int groups) {
+    const long long tiles = (long long)((nq + kN - 1) / kN) * ((R + kM - 1) / kM) * std::max(1, groups);
     const int chunks = std::max(1, (bins + kKC - 1) / kKC);
     long long s = (sms + tiles - 1) / std::max(1ll, tiles);
     s = std::max(1ll, std::min<long long>(s, std::min(64, chunks)));

@@ -15,6 +15,7 @@ namespace ausaxs_b200 {
 
 void DevBuf::ensure(size_t bytes) {
     if (bytes <= n) return;
+    if (!owned) throw Error{AUSAXS_ERR_CAPACITY, "device buffer view too small"};
     if (p) cudaFree(p);
     p = nullptr;
     n = 0;
@@ -24,7 +25,21 @@ void DevBuf::ensure(size_t bytes) {
 }
 
 DevBuf::~DevBuf() {
-    if (p) cudaFree(p);
+    if (p && owned) cudaFree(p);
+}
+
+PrepStats* Ctx::stats_slots(size_t n) {
+    if (n > n_stats_many) {
+        if (h_stats_many) {
+            cudaStreamSynchronize(stream);  // earlier read-backs may still target the old slots
+            cudaFreeHost(h_stats_many);
+        }
+        h_stats_many = nullptr;
+        n_stats_many = 0;
+        AUSAXS_CUDA(cudaMallocHost(&h_stats_many, sizeof(PrepStats) * n));
+        n_stats_many = n;
+    }
+    return h_stats_many;
 }
 
 void Ctx::check_launch(const char* what) {
@@ -65,8 +80,8 @@ void Ctx::time_collect() {
     }
 }
 
-void Structure::load(const float* atoms, int n_atoms, const float* waters, int n_waters, const float* exv, int n_exv,
-                     int ff_typed_, bool host) {
+void Structure::load_begin(const float* atoms, int n_atoms, const float* waters, int n_waters, const float* exv,
+                           int n_exv, int ff_typed_, bool host, PrepStats* h_stats, PrepStats* d_stats) {
     if (n_atoms < 0 || n_waters < 0 || n_exv < 0) throw Error{AUSAXS_ERR_ARGUMENT, "negative point count"};
     if ((n_atoms && !atoms) || (n_waters && !waters) || (n_exv && !exv)) throw Error{AUSAXS_ERR_ARGUMENT, "null point array"};
     Ctx& C = *ctx;
@@ -85,16 +100,18 @@ void Structure::load(const float* atoms, int n_atoms, const float* waters, int n
 
     PrepStats init{};
     for (int k = 0; k < 3; ++k) init.lo[k] = 0xffffffffu, init.hi[k] = 0;
-    *C.h_stats = init;
-    C.stats.ensure(sizeof(PrepStats));
-    AUSAXS_CUDA(cudaMemcpyAsync(C.stats.p, C.h_stats, sizeof(PrepStats), cudaMemcpyHostToDevice, s));
-    census_launch(raw_a.as<float4>(), n_a, ff_typed, C.stats.as<PrepStats>(), C.sm_count, s);
-    census_launch(raw_w.as<float4>(), n_w, 0, C.stats.as<PrepStats>(), C.sm_count, s);
-    census_launch(raw_x.as<float4>(), n_x, 0, C.stats.as<PrepStats>(), C.sm_count, s);
+    *h_stats = init;  // pinned: the copy below reads it asynchronously, the census result overwrites it
+    AUSAXS_CUDA(cudaMemcpyAsync(d_stats, h_stats, sizeof(PrepStats), cudaMemcpyHostToDevice, s));
+    census_launch(raw_a.as<float4>(), n_a, ff_typed, d_stats, C.sm_count, s);
+    census_launch(raw_w.as<float4>(), n_w, 0, d_stats, C.sm_count, s);
+    census_launch(raw_x.as<float4>(), n_x, 0, d_stats, C.sm_count, s);
     C.check_launch("census");
-    AUSAXS_CUDA(cudaMemcpyAsync(C.h_stats, C.stats.p, sizeof(PrepStats), cudaMemcpyDeviceToHost, s));
-    AUSAXS_CUDA(cudaStreamSynchronize(s));
-    const PrepStats st = *C.h_stats;
+    AUSAXS_CUDA(cudaMemcpyAsync(h_stats, d_stats, sizeof(PrepStats), cudaMemcpyDeviceToHost, s));
+}
+
+void Structure::load_end(const PrepStats& st) {
+    Ctx& C = *ctx;
+    cudaStream_t s = C.stream;
     if (st.bad & 1u)
         throw Error{AUSAXS_ERR_FORM_FACTOR,
                     "an atom has a form-factor type outside [1, 15) (UNKNOWN or excluded volume); form factor "
@@ -125,15 +142,23 @@ void Structure::load(const float* atoms, int n_atoms, const float* waters, int n
     }
     T = T_new;
     meta.ensure(256);
-    int32_t hmeta[2 * kNff];
     for (int k = 0; k < kNff; ++k) hmeta[k] = k < T ? type_count[k] : 0, hmeta[kNff + k] = ff_to_type[k];
+    // pageable source: the call returns once the bytes are staged, so hmeta may change afterwards
     AUSAXS_CUDA(cudaMemcpyAsync(meta.p, hmeta, sizeof(hmeta), cudaMemcpyHostToDevice, s));
     if (ff_typed) {
         dense_a.ensure(align_up(std::max(1, n_a) * 16, 256));
         to_dense_launch(raw_a.as<float4>(), dense_a.as<float4>(), n_a, meta.as<int32_t>(kNff * 4), C.sm_count, s);
         C.check_launch("to_dense");
     }
-    AUSAXS_CUDA(cudaStreamSynchronize(s));  // hmeta lives on this stack frame
+}
+
+void Structure::load(const float* atoms, int n_atoms, const float* waters, int n_waters, const float* exv, int n_exv,
+                     int ff_typed_, bool host) {
+    Ctx& C = *ctx;
+    C.stats.ensure(sizeof(PrepStats));
+    load_begin(atoms, n_atoms, waters, n_waters, exv, n_exv, ff_typed_, host, C.h_stats, C.stats.as<PrepStats>());
+    AUSAXS_CUDA(cudaStreamSynchronize(C.stream));
+    load_end(*C.h_stats);
 }
 
 static long long tri(long long t) { return t * (t + 1) / 2; }
@@ -315,10 +340,8 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
     off += align_up((size_t)nb * 8, 256);
     P.off_rows = off;
     off += align_up(sizeof(RowDesc) * R, 256);
-    P.off_expand_aa = off;
-    off += align_up((size_t)kNff * kNff * nb * 8, 256);
-    P.off_expand_aw = off;
-    off += align_up((size_t)kNff * nb * 8, 256);
+    P.off_expand_aa = 0;  // host-layout expansion buffers: allocated on the first read-back
+    P.off_expand_aw = align_up((size_t)kNff * kNff * nb * 8, 256);
     P.dev.ensure(off);
     char* base = P.dev.as<char>();
 
@@ -380,8 +403,8 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
         L.overflow = reinterpret_cast<unsigned long long*>(base + P.off_overflow);
         L.weighted = w_launch;
         L.wscale = reinterpret_cast<const float*>(base + P.off_wscale);
-        AUSAXS_CUDA(cudaMemcpy(base + job_off, group_jobs[g].data(), sizeof(PairJob) * group_jobs[g].size(),
-                               cudaMemcpyHostToDevice));
+        AUSAXS_CUDA(cudaMemcpyAsync(base + job_off, group_jobs[g].data(), sizeof(PairJob) * group_jobs[g].size(),
+                                    cudaMemcpyHostToDevice, C.stream));  // pageable: staged on return
         job_off += sizeof(PairJob) * group_jobs[g].size();
         P.total_tiles += group_tiles[g];
     }
@@ -465,7 +488,7 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
         rd[T * T + 2 * T + 1] = {g_ax, ex ? kRowZero : kRowWX, kExv, kWater};
         rd[T * T + 2 * T + 2] = {0, kRowWW, kWater, kWater};
     }
-    AUSAXS_CUDA(cudaMemcpy(base + P.off_rows, rd.data(), sizeof(RowDesc) * R, cudaMemcpyHostToDevice));
+    AUSAXS_CUDA(cudaMemcpyAsync(base + P.off_rows, rd.data(), sizeof(RowDesc) * R, cudaMemcpyHostToDevice, C.stream));
     return P;
 }
 
@@ -545,7 +568,7 @@ void run_debye(Ctx& C, DebyeArgs& A, int groups_present, DevBuf& tc, int precisi
         // split-BF16 tensor-core contraction for every q, FP64 re-evaluation of the flagged ones
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, C.device);
-        const int splits = debye_tc_splits(A.R, A.nb, A.nq, sms);
+        const int splits = debye_tc_splits(A.R, A.nb, A.nq, sms, __builtin_popcount((unsigned)groups_present));
         const size_t plane = (size_t)A.R * A.nq;
         const size_t n = (size_t)splits * plane;
         const size_t bytes_v = align_up(n * 4, 256), bytes_h = align_up((size_t)splits * A.R * 4, 256);
@@ -619,8 +642,9 @@ void Structure::read_histogram(const ausaxs_hist_config& cfg, ausaxs_hist_result
         d2h(out->aw, H + nb, mb);
         d2h(out->ww, H + 2 * nb, mb);
     } else {
-        double* eaa = reinterpret_cast<double*>(base + P.off_expand_aa);
-        double* eaw = reinterpret_cast<double*>(base + P.off_expand_aw);
+        P.expand.ensure(P.off_expand_aw + align_up((size_t)kNff * nb * 8, 256));
+        double* eaa = P.expand.as<double>(P.off_expand_aa);
+        double* eaw = P.expand.as<double>(P.off_expand_aw);
         ff_expand_launch(P.fin_ff, eaa, eaw, mb, s);
         C.check_launch("expand");
         d2h(out->aa, eaa, (size_t)kNff * kNff * mb);

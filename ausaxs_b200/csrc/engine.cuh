@@ -32,7 +32,13 @@ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 struct DevBuf {
     void* p = nullptr;
     size_t n = 0;
+    bool owned = true;  // false: a view into memory owned elsewhere (never grown or freed here)
     void ensure(size_t bytes);
+    void view(void* ptr, size_t bytes) {
+        p = ptr;
+        n = bytes;
+        owned = false;
+    }
     ~DevBuf();
     template <typename T>
     T* as(size_t byte_offset = 0) const { return reinterpret_cast<T*>(static_cast<char*>(p) + byte_offset); }
@@ -78,7 +84,8 @@ struct Plan {
     DevBuf dev;
     size_t off_jobs = 0, off_acc = 0, acc_bytes = 0, off_counter = 0, off_overflow = 0, off_maxbin = 0, off_wscale = 0,
            off_self = 0, off_fp64cols = 0, off_H = 0, off_tot = 0, off_d = 0, off_dax = 0, off_dxx = 0, off_rows = 0,
-           off_expand_aa = 0, off_expand_aw = 0;
+           off_expand_aa = 0, off_expand_aw = 0;  // in `expand`, allocated by the first host read-back
+    DevBuf expand;
     FinalizeFF fin_ff{};
     FinalizeMT fin_mt{};
     std::vector<JobSpec> specs;  // the structure's passes (tiled by append_pair_jobs)
@@ -105,6 +112,13 @@ struct Structure {
     // copy in (host or device pointers), census, validation and dense-type conversion (one sync)
     void load(const float* atoms, int n_atoms, const float* waters, int n_waters, const float* exv, int n_exv,
               int ff_typed_, bool host);
+    // the same in two halves, so many structures share one synchronisation: load_begin enqueues the
+    // copies and the census into d_stats and its read-back into h_stats (pinned); after the stream has
+    // been synchronised, load_end validates and enqueues the dense-type conversion
+    void load_begin(const float* atoms, int n_atoms, const float* waters, int n_waters, const float* exv, int n_exv,
+                    int ff_typed_, bool host, PrepStats* h_stats, PrepStats* d_stats);
+    void load_end(const PrepStats& st);
+    int32_t hmeta[2 * kNff] = {};  // host copy of meta (type counts, ff -> dense type)
     const float4* atoms_for_pairs() const { return ff_typed ? dense_a.as<float4>() : raw_a.as<float4>(); }
     Plan& plan_for(const ausaxs_hist_config& cfg);
     void enqueue_histogram(const ausaxs_hist_config& cfg);
@@ -136,6 +150,9 @@ struct Ctx {
     void time_collect();
     DevBuf stats;
     PrepStats* h_stats = nullptr;  // pinned
+    PrepStats* h_stats_many = nullptr;  // pinned, census slots of batched loads (grows, freed with the context)
+    size_t n_stats_many = 0;
+    PrepStats* stats_slots(size_t n);
     std::unique_ptr<Structure> scratch;
     DevBuf io;                     // q / I(q) / profiles of one-shot host calls
     DevBuf tc;                     // tensor-core scratch of one-shot host calls
