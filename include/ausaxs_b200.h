@@ -7,7 +7,7 @@
  *        hist::IHistogramManager::calculate_all()
  *      returns (include/core/hist/histogram_manager/IHistogramManager.h:16-29) for the
  *      managers HistogramManagerMT, HistogramManagerMTFFAvg, HistogramManagerMTFFExplicit and
- *      HistogramManagerMTFFGrid (source/core/hist/histogram_manager/*.cpp);
+ *      HistogramManagerMTFFGrid (one .cpp per manager in source/core/hist/histogram_manager/);
  *   2. the Debye transform, i.e.
  *        ICompositeDistanceHistogram::debye_transform() and get_profile_*()
  *      (include/core/hist/intensity_calculator/ICompositeDistanceHistogram.h:24-71,
