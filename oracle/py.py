@@ -186,6 +186,24 @@ def ref_path() -> str:
     return os.path.join(HERE, "_ref", "libausaxs_ref.so")
 
 
+def ref_read_structure(path: str, implicit_h: int = -1, center: int = -1):
+    """A structure file read by the reference's own reader: (xyz [n,3], weights [n], ff [n] int,
+    waters [m,3], water weights [m])."""
+    L = ref()
+    f = L.ref_read_structure
+    f.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_void_p, C.c_int,
+                  C.POINTER(C.c_int)]
+    na, nw = C.c_int(), C.c_int()
+    if f(path.encode(), implicit_h, center, None, 0, C.byref(na), None, 0, C.byref(nw)):
+        raise RuntimeError(L.ref_last_error().decode())
+    a = np.zeros((max(1, na.value), 5))
+    w = np.zeros((max(1, nw.value), 4))
+    if f(path.encode(), implicit_h, center, a.ctypes.data, na.value, C.byref(na), w.ctypes.data, nw.value, C.byref(nw)):
+        raise RuntimeError(L.ref_last_error().decode())
+    a, w = a[: na.value], w[: nw.value]
+    return a[:, :3].copy(), a[:, 3].copy(), a[:, 4].astype(np.int32), w[:, :3].copy(), w[:, 3].copy()
+
+
 def ref_available() -> bool:
     return os.path.exists(ref_path())
 

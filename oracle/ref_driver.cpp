@@ -37,6 +37,8 @@
 #include <settings/Flags.h>
 #include <settings/GeneralSettings.h>
 #include <settings/HistogramSettings.h>
+#include <settings/MoleculeSettings.h>
+#include <io/File.h>
 
 #include <chrono>
 #include <cstring>
@@ -165,6 +167,42 @@ void* ref_molecule_new(const double* atoms, int n_a, const double* waters, int n
 }
 
 void ref_molecule_free(void* m) { delete static_cast<FixedVolumeMolecule*>(m); }
+
+// A structure file read by the reference's own reader (data::Molecule(io::File), which assigns the
+// united-atom form-factor types), returned as arrays: atoms n x {x, y, z, weight, ff}, waters
+// n x {x, y, z, weight}.  Call with capacities 0 to get the counts.  implicit_hydrogens and center
+// take the reference's defaults unless set to 0 / 1 explicitly (-1: default).
+int ref_read_structure(const char* path, int implicit_h, int center, double* atoms, int cap_a, int* n_a, double* waters,
+                       int cap_w, int* n_w) {
+    return guarded([&] {
+        if (implicit_h >= 0) settings::molecule::implicit_hydrogens = implicit_h != 0;
+        if (center >= 0) settings::molecule::center = center != 0;
+        data::Molecule m{io::File(std::string(path))};
+        auto a = m.get_atoms();
+        auto w = m.get_waters();
+        *n_a = static_cast<int>(a.size());
+        *n_w = static_cast<int>(w.size());
+        if (atoms && cap_a >= *n_a) {
+            for (size_t i = 0; i < a.size(); ++i) {
+                double* r = atoms + 5 * i;
+                r[0] = a[i].coordinates().x();
+                r[1] = a[i].coordinates().y();
+                r[2] = a[i].coordinates().z();
+                r[3] = a[i].weight();
+                r[4] = static_cast<int>(a[i].form_factor_type());
+            }
+        }
+        if (waters && cap_w >= *n_w) {
+            for (size_t i = 0; i < w.size(); ++i) {
+                double* r = waters + 4 * i;
+                r[0] = w[i].coordinates().x();
+                r[1] = w[i].coordinates().y();
+                r[2] = w[i].coordinates().z();
+                r[3] = w[i].weight();
+            }
+        }
+    });
+}
 
 // Rigid move of one body: x <- R x + t, through Body::rotate / Body::translate
 // (source/core/data/Body.cpp:135-156), which also signal the partial managers.

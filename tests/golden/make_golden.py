@@ -12,7 +12,9 @@ reference's default q axis.  Cases:
 
 * ``cube_*``  : the reference's SimpleCube known-answer structure (tests/feature/hist/hist_test_helper.h:87-162)
                 for every manager;
-* ``random_*``: seeded random molecules (ragged sizes, all four elements, non-default bin width).
+* ``random_*``: seeded random molecules (ragged sizes, all four elements, non-default bin width);
+* ``pdb_*``   : the proteins 2epe and 6lyz from the reference's own test files, read by the
+                reference's reader (united-atom form-factor types).
 """
 from __future__ import annotations
 
@@ -25,6 +27,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from oracle import py as O  # noqa: E402
+
+REF_ROOT = os.environ.get("AUSAXS_REFERENCE", "/root/reference")  # reference checkout (read-only)
 
 CUBE = np.array([[-1, -1, -1], [-1, 1, -1], [1, -1, -1], [1, 1, -1], [-1, -1, 1], [-1, 1, 1], [1, -1, 1], [1, 1, 1]], float)
 
@@ -85,6 +89,20 @@ def main():
                  crho=1.02, dwa=0.4, dwx=0.2)
         if nx:
             run_case(f"random{k}_ffgrid", xyz, f, wt, wat, wwt, exv, vol, bw, "ffgrid", cw=0.9, cx=1.05)
+    # Real proteins from the reference's own test files (tests/files in the reference), read by the
+    # reference's reader, so the atoms carry its united-atom form-factor types (CH, CH2, NH, OH, ...)
+    files = os.path.join(REF_ROOT, "tests", "files")
+    for pdb in ("2epe", "6lyz"):
+        path = os.path.join(files, pdb + ".pdb")
+        if not os.path.exists(path):
+            continue
+        xyz, wt, f, wat, wwt = O.ref_read_structure(path)
+        vol = 18.0 * len(xyz)
+        run_case(f"pdb_{pdb}_mt", xyz, f, wt, wat, wwt, np.zeros((0, 3)), vol, 0.25, "mt", cw=1.2)
+        run_case(f"pdb_{pdb}_ffavg", xyz, f, wt, wat, wwt, np.zeros((0, 3)), vol, 0.25, "ffavg", cw=1.05, cx=0.98,
+                 crho=1.01, dwa=0.3, dwx=0.1)
+        run_case(f"pdb_{pdb}_ffexplicit", xyz, f, wt, wat, wwt, np.zeros((0, 3)), vol, 0.1, "ffexplicit", cw=1.05,
+                 cx=1.02)
     # Simple excluded volume enabled (weights shifted by -rho_w V / N, SimpleExvModel.cpp:23-28)
     xyz = rng.normal(0, 6, (120, 3))
     f = rng.choice(elements, 120)
