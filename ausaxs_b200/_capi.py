@@ -34,7 +34,7 @@ EXPORTED = [
     "ausaxs_gpu_last_error", "ausaxs_gpu_ctx_enable_timing", "ausaxs_gpu_ctx_kernel_time",
     "ausaxs_gpu_ctx_fp64_columns", "ausaxs_gpu_ctx_tc_error_estimate", "ausaxs_gpu_histogram", "ausaxs_gpu_debye", "ausaxs_gpu_profile",
     "ausaxs_gpu_structure_create", "ausaxs_gpu_structure_destroy", "ausaxs_gpu_structure_profile",
-    "ausaxs_gpu_structure_histogram", "ausaxs_gpu_histogram_mt_noalloc", "ausaxs_gpu_linear_lsq",
+    "ausaxs_gpu_structure_histogram", "ausaxs_gpu_histogram_mt_noalloc", "ausaxs_gpu_linear_lsq", "ausaxs_gpu_grid_exv",
     "ausaxs_gpu_batch_create", "ausaxs_gpu_batch_destroy", "ausaxs_gpu_batch_autotune", "ausaxs_gpu_batch_candidate",
     "ausaxs_gpu_batch_profile_device", "ausaxs_gpu_batch_profile", "ausaxs_gpu_batch_histogram",
     "ausaxs_gpu_server_create", "ausaxs_gpu_server_destroy", "ausaxs_gpu_server_admit", "ausaxs_gpu_server_release",
@@ -106,6 +106,8 @@ def load():
                                                    C.POINTER(DebyeParams), f64, f64]
         L.ausaxs_gpu_structure_histogram.argtypes = [vp, vp, C.POINTER(HistConfig), C.POINTER(HistResult)]
         L.ausaxs_gpu_linear_lsq.argtypes = [vp, f64, f64, f64, C.c_int32, f64]
+        L.ausaxs_gpu_grid_exv.argtypes = [vp, f32, C.c_int32, f32, C.c_int32, f32, C.c_int64, C.POINTER(C.c_int64),
+                                          C.POINTER(C.c_double)]
         i64 = C.POINTER(C.c_int64)
         i32 = C.POINTER(C.c_int32)
         L.ausaxs_gpu_batch_create.argtypes = [vp, C.POINTER(HistConfig), C.c_int32, f32, i64, f32, i64, f32, i64, f64,
@@ -214,6 +216,22 @@ def linear_lsq(ctx: "Context", data, model, err) -> np.ndarray:
 
 
 _default = {}
+
+
+EXV_FROM_GRID = -1
+
+
+def grid_exv(ctx: "Context", atoms, waters):
+    """Excluded-volume dummies of the molecular grid (RawGridExv) and the grid volume: ([n, 4] records, volume)."""
+    a = np.ascontiguousarray(atoms, np.float32).reshape(-1, 4)
+    w = np.ascontiguousarray(waters, np.float32).reshape(-1, 4)
+    n = C.c_int64(0)
+    vol = C.c_double(0)
+    check(load().ausaxs_gpu_grid_exv(ctx.h, fptr(a), len(a), fptr(w), len(w), None, 0, C.byref(n), C.byref(vol)))
+    out = np.zeros((max(1, n.value), 4), np.float32)
+    check(load().ausaxs_gpu_grid_exv(ctx.h, fptr(a), len(a), fptr(w), len(w), fptr(out), n.value, C.byref(n),
+                                     C.byref(vol)))
+    return out[: n.value], vol.value
 
 
 def default_context(device: int = 0) -> Context:

@@ -4,6 +4,7 @@
 #include <string>
 
 #include "engine.cuh"
+#include "gridexv.cuh"
 #include "guard.cuh"
 #include "lsq.cuh"
 
@@ -24,6 +25,31 @@ bool ff_manager(int m) { return m == AUSAXS_MANAGER_FFAVG || m == AUSAXS_MANAGER
 
 void check_cfg(const ausaxs_hist_config* cfg) {
     if (!cfg) throw Error{AUSAXS_ERR_ARGUMENT, "null configuration"};
+}
+
+// The scratch structure of a one-shot host call, with the grid-derived inputs the configuration asks
+// for: FFGRID with n_exv = AUSAXS_EXV_FROM_GRID takes its dummies from the molecular grid (RawGridExv,
+// generated on the device), FFAVG with z_exv < 0 takes Z_exv = V_grid rho_w / N_atoms from the grid
+// volume (HistogramManagerMTFFAvg.cpp:351-364 with Molecule::get_volume_grid()).  Returns the effective
+// configuration.
+ausaxs_hist_config load_scratch(Ctx& C, const ausaxs_hist_config& cfg, const float* atoms, int32_t n_atoms,
+                                const float* waters, int32_t n_waters, const float* exv, int32_t n_exv) {
+    Structure& S = scratch(C);
+    ausaxs_hist_config c = cfg;
+    const bool grid = cfg.manager == AUSAXS_MANAGER_FFGRID;
+    const bool gen = grid && n_exv == AUSAXS_EXV_FROM_GRID;
+    const bool zgrid = cfg.manager == AUSAXS_MANAGER_FFAVG && cfg.z_exv < 0;
+    if (!gen && !zgrid) {
+        if (n_exv < 0 && grid) throw Error{AUSAXS_ERR_ARGUMENT, "negative exv count"};
+        S.load(atoms, n_atoms, waters, n_waters, grid ? exv : nullptr, grid ? n_exv : 0, ff_manager(cfg.manager), true);
+        return c;
+    }
+    S.load(atoms, n_atoms, waters, n_waters, nullptr, 0, 1, true);  // census: validation and bounding box
+    GridExv g;
+    g.run(C, S.raw_a.as<float4>(), n_atoms, S.raw_w.as<float4>(), n_waters, S.lo, S.hi, gen);
+    if (zgrid) c.z_exv = n_atoms ? g.volume * 0.334 / n_atoms : 0.0;  // rho_w (Constants.h:114)
+    if (gen) S.load(atoms, n_atoms, waters, n_waters, g.points.as<float>(), (int)g.count, 1, true, 0);
+    return c;
 }
 
 ausaxs_debye_params default_params(const ausaxs_debye_params* p) {
@@ -151,11 +177,10 @@ int ausaxs_gpu_histogram(ausaxs_gpu_ctx* ctx, const ausaxs_hist_config* cfg, con
         check_cfg(cfg);
         Ctx& C = ctx->impl;
         AUSAXS_CUDA(cudaSetDevice(C.device));
+        const ausaxs_hist_config c = load_scratch(C, *cfg, atoms, n_atoms, waters, n_waters, exv, n_exv);
         Structure& S = scratch(C);
-        const bool grid = cfg->manager == AUSAXS_MANAGER_FFGRID;
-        S.load(atoms, n_atoms, waters, n_waters, grid ? exv : nullptr, grid ? n_exv : 0, ff_manager(cfg->manager), true);
-        S.enqueue_histogram(*cfg);
-        S.read_histogram(*cfg, out);
+        S.enqueue_histogram(c);
+        S.read_histogram(c, out);
     });
 }
 
@@ -179,9 +204,8 @@ int ausaxs_gpu_profile(ausaxs_gpu_ctx* ctx, const ausaxs_hist_config* cfg, const
         check_cfg(cfg);
         Ctx& C = ctx->impl;
         AUSAXS_CUDA(cudaSetDevice(C.device));
+        const ausaxs_hist_config c = load_scratch(C, *cfg, atoms, n_atoms, waters, n_waters, exv, n_exv);
         Structure& S = scratch(C);
-        const bool grid = cfg->manager == AUSAXS_MANAGER_FFGRID;
-        S.load(atoms, n_atoms, waters, n_waters, grid ? exv : nullptr, grid ? n_exv : 0, ff_manager(cfg->manager), true);
         ausaxs_debye_params p = default_params(params);
         size_t need = (size_t)n_q * 8 * 8 + 256;
         C.io.ensure(need);
@@ -189,8 +213,8 @@ int ausaxs_gpu_profile(ausaxs_gpu_ctx* ctx, const ausaxs_hist_config* cfg, const
         double* dI = dq + n_q;
         double* dP = dI + n_q;
         AUSAXS_CUDA(cudaMemcpyAsync(dq, q, (size_t)n_q * 8, cudaMemcpyHostToDevice, C.stream));
-        S.enqueue_histogram(*cfg);
-        S.enqueue_debye(*cfg, dq, n_q, p, dI, profiles ? dP : nullptr);
+        S.enqueue_histogram(c);
+        S.enqueue_debye(c, dq, n_q, p, dI, profiles ? dP : nullptr);
         AUSAXS_CUDA(cudaMemcpyAsync(Iq, dI, (size_t)n_q * 8, cudaMemcpyDeviceToHost, C.stream));
         if (profiles) AUSAXS_CUDA(cudaMemcpyAsync(profiles, dP, (size_t)n_q * 6 * 8, cudaMemcpyDeviceToHost, C.stream));
         unsigned long long overflow = 0;

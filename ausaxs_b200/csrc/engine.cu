@@ -81,7 +81,7 @@ void Ctx::time_collect() {
 }
 
 void Structure::load_begin(const float* atoms, int n_atoms, const float* waters, int n_waters, const float* exv,
-                           int n_exv, int ff_typed_, bool host, PrepStats* h_stats, PrepStats* d_stats) {
+                           int n_exv, int ff_typed_, bool host, PrepStats* h_stats, PrepStats* d_stats, int exv_host) {
     if (n_atoms < 0 || n_waters < 0 || n_exv < 0) throw Error{AUSAXS_ERR_ARGUMENT, "negative point count"};
     if ((n_atoms && !atoms) || (n_waters && !waters) || (n_exv && !exv)) throw Error{AUSAXS_ERR_ARGUMENT, "null point array"};
     Ctx& C = *ctx;
@@ -96,7 +96,8 @@ void Structure::load_begin(const float* atoms, int n_atoms, const float* waters,
     cudaMemcpyKind kind = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
     if (n_a) AUSAXS_CUDA(cudaMemcpyAsync(raw_a.p, atoms, (size_t)n_a * 16, kind, s));
     if (n_w) AUSAXS_CUDA(cudaMemcpyAsync(raw_w.p, waters, (size_t)n_w * 16, kind, s));
-    if (n_x) AUSAXS_CUDA(cudaMemcpyAsync(raw_x.p, exv, (size_t)n_x * 16, kind, s));
+    const bool x_host = exv_host < 0 ? host : exv_host != 0;
+    if (n_x) AUSAXS_CUDA(cudaMemcpyAsync(raw_x.p, exv, (size_t)n_x * 16, x_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
 
     PrepStats init{};
     for (int k = 0; k < 3; ++k) init.lo[k] = 0xffffffffu, init.hi[k] = 0;
@@ -153,10 +154,10 @@ void Structure::load_end(const PrepStats& st) {
 }
 
 void Structure::load(const float* atoms, int n_atoms, const float* waters, int n_waters, const float* exv, int n_exv,
-                     int ff_typed_, bool host) {
+                     int ff_typed_, bool host, int exv_host) {
     Ctx& C = *ctx;
     C.stats.ensure(sizeof(PrepStats));
-    load_begin(atoms, n_atoms, waters, n_waters, exv, n_exv, ff_typed_, host, C.h_stats, C.stats.as<PrepStats>());
+    load_begin(atoms, n_atoms, waters, n_waters, exv, n_exv, ff_typed_, host, C.h_stats, C.stats.as<PrepStats>(), exv_host);
     AUSAXS_CUDA(cudaStreamSynchronize(C.stream));
     load_end(*C.h_stats);
 }

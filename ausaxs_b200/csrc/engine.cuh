@@ -111,12 +111,13 @@ struct Structure {
 
     // copy in (host or device pointers), census, validation and dense-type conversion (one sync)
     void load(const float* atoms, int n_atoms, const float* waters, int n_waters, const float* exv, int n_exv,
-              int ff_typed_, bool host);
+              int ff_typed_, bool host, int exv_host = -1);
+    // (exv_host: where exv lives when it differs from the other arrays; -1 = as `host`)
     // the same in two halves, so many structures share one synchronisation: load_begin enqueues the
     // copies and the census into d_stats and its read-back into h_stats (pinned); after the stream has
     // been synchronised, load_end validates and enqueues the dense-type conversion
     void load_begin(const float* atoms, int n_atoms, const float* waters, int n_waters, const float* exv, int n_exv,
-                    int ff_typed_, bool host, PrepStats* h_stats, PrepStats* d_stats);
+                    int ff_typed_, bool host, PrepStats* h_stats, PrepStats* d_stats, int exv_host = -1);
     void load_end(const PrepStats& st);
     int32_t hmeta[2 * kNff] = {};  // host copy of meta (type counts, ff -> dense type)
     const float4* atoms_for_pairs() const { return ff_typed ? dense_a.as<float4>() : raw_a.as<float4>(); }

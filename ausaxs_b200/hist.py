@@ -73,8 +73,8 @@ class Molecule:
     weights: Optional[np.ndarray] = None    # [n] effective charges
     waters: Optional[np.ndarray] = None     # [m, 3]
     water_weights: Optional[np.ndarray] = None
-    exv: Optional[np.ndarray] = None        # [k, 3] grid dummies (FFGrid)
-    volume: float = 0.0
+    exv: Optional[np.ndarray] = None        # [k, 3] grid dummies (FFGrid); None: from the molecular grid
+    volume: Optional[float] = None          # None: the molecular grid's volume (Molecule::get_volume_grid)
 
     def size_atom(self) -> int:
         return len(self.atoms)
@@ -83,7 +83,12 @@ class Molecule:
         return 0 if self.waters is None else len(self.waters)
 
     def get_volume_grid(self) -> float:
-        return float(self.volume)
+        """The given volume, or the volume of the molecular grid computed on the device
+        (Molecule::get_volume_grid, source/core/data/Molecule.cpp:147-150)."""
+        if self.volume is not None:
+            return float(self.volume)
+        a, w, _ = self.compact_ff()
+        return _capi.grid_exv(_capi.default_context(), a, w)[1]
 
     def compact_ff(self):
         a = pack(self.atoms, self.ff_types, True)
@@ -236,11 +241,17 @@ class _Manager:
     def config(self) -> HistConfig:
         z = 0.0
         if self.manager == _capi.MANAGER_FFAVG and self.protein.size_atom():
-            z = self.protein.get_volume_grid() * RHO_WATER / self.protein.size_atom()
+            # without a given volume the device takes Z_exv from the molecular grid (z_exv < 0)
+            z = -1.0 if self.protein.volume is None else self.protein.get_volume_grid() * RHO_WATER / self.protein.size_atom()
         return HistConfig(self.manager, int(self.weighted_bins), float(self.bin_width), int(self.bin_count), z)
 
     def _inputs(self):
         raise NotImplementedError
+
+    def _exv_count(self, x) -> int:
+        if x is not None:
+            return len(x)
+        return _capi.EXV_FROM_GRID if self.manager == _capi.MANAGER_FFGRID else 0
 
     def calculate_all(self):
         cfg = self.config()
@@ -260,7 +271,7 @@ class _Manager:
         for k, v in bufs.items():
             setattr(r, k, dptr(v))
         check(load().ausaxs_gpu_histogram(self.ctx.h, C.byref(cfg), fptr(a), len(a), fptr(w), len(w), fptr(x),
-                                          0 if x is None else len(x), C.byref(r)))
+                                          self._exv_count(x), C.byref(r)))
         m = r.max_bin
         res = {"max_bin": m, "pairs": r.pairs}
         if ff:
@@ -324,7 +335,8 @@ class HistogramManagerMTFFGrid(_Manager):
         super().__init__(protein, True, bin_width, bin_count, ctx)
 
     def _inputs(self):
-        return self.protein.compact_ff()
+        a, w, x = self.protein.compact_ff()
+        return a, w, (x if self.protein.exv is not None else None)  # None: dummies from the molecular grid
 
 
 def profile(manager: _Manager, q, cw=1.0, cx=1.0, crho=1.0, dw_atomic=0.0, dw_exv=0.0, grid_width=1.0,
@@ -337,7 +349,7 @@ def profile(manager: _Manager, q, cw=1.0, cx=1.0, crho=1.0, dw_atomic=0.0, dw_ex
     prof = np.zeros(6 * len(q)) if with_profiles else None
     p = DebyeParams(cw, cx, crho, dw_atomic, dw_exv, grid_width, precision, tolerance)
     check(load().ausaxs_gpu_profile(manager.ctx.h, C.byref(cfg), fptr(a), len(a), fptr(w), len(w), fptr(x),
-                                    0 if x is None else len(x), dptr(q), len(q), C.byref(p), dptr(I), dptr(prof)))
+                                    manager._exv_count(x), dptr(q), len(q), C.byref(p), dptr(I), dptr(prof)))
     return (I, prof.reshape(6, len(q))) if with_profiles else I
 
 

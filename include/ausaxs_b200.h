@@ -129,11 +129,18 @@ typedef struct {
     double* d_axis_xx;
 } ausaxs_hist_result;
 
+/* n_exv value asking ausaxs_gpu_histogram / ausaxs_gpu_profile (FFGRID) to take the excluded-volume
+ * dummies from the structure's molecular grid, as the reference does (see ausaxs_gpu_grid_exv). */
+#define AUSAXS_EXV_FROM_GRID (-1)
+
 /*
  * IHistogramManager::calculate_all() for one structure (host buffers).
  * atoms: n_atoms records, waters: n_waters records, exv: n_exv excluded-volume dummies (FFGRID only;
  * RawGridExv::create supplies these in the reference, source/core/grid/exv/RawGridExv.cpp:10-59).
  * FF managers read the int32 form-factor type from the 4th word, MT reads the float weight.
+ * FFGRID with n_exv = AUSAXS_EXV_FROM_GRID generates the dummies on the device (ausaxs_gpu_grid_exv);
+ * FFAVG with cfg->z_exv < 0 takes Z_exv = V_grid * rho_w / N_atoms from the grid volume, as
+ * HistogramManagerMTFFAvg does with Molecule::get_volume_grid().
  */
 AUSAXS_API int ausaxs_gpu_histogram(ausaxs_gpu_ctx* ctx, const ausaxs_hist_config* cfg, const float* atoms, int32_t n_atoms,
                          const float* waters, int32_t n_waters, const float* exv, int32_t n_exv,
@@ -235,6 +242,18 @@ AUSAXS_API int ausaxs_gpu_batch_profile_device(ausaxs_gpu_batch* b, const double
 AUSAXS_API int ausaxs_gpu_batch_profile(ausaxs_gpu_batch* b, const double* q, int32_t n_q,
                                         const ausaxs_debye_params* params, double* Iq);
 AUSAXS_API int ausaxs_gpu_batch_histogram(ausaxs_gpu_batch* b, int32_t index, ausaxs_hist_result* out);
+
+/*
+ * Excluded-volume dummies of a structure's molecular grid: grid::exv::RawGridExv::create
+ * (source/core/grid/exv/RawGridExv.cpp:10-59) on the expanded grid that
+ * HistogramManagerMTFFGrid::calculate_all() uses, with the reference's default grid settings (1 A
+ * cells, rvol 2.15 A, exv width 1 A, AtomicOnly expansion; Grid.cpp:34-102, SphericalExpander.h:27-76),
+ * and the grid volume Molecule::get_volume_grid() returns (A^3).  atoms {x,y,z,ff} and waters
+ * {x,y,z,w} are host records.  Dummies are written as {x, y, z, 0} records in the reference's order
+ * (x-major sweep) when capacity > 0 (AUSAXS_ERR_CAPACITY if it is too small); *n_exv is their count.
+ */
+AUSAXS_API int ausaxs_gpu_grid_exv(ausaxs_gpu_ctx* ctx, const float* atoms, int32_t n_atoms, const float* waters,
+                                   int32_t n_waters, float* exv_out, int64_t capacity, int64_t* n_exv, double* volume);
 
 /*
  * Rigid-body serving.  The reference's incremental manager, PartialHistogramManagerMT

@@ -554,3 +554,133 @@ void oracle_linear_lsq(const double* data, const double* model, const double* er
     out[3] = Sxx / delta;
     out[4] = chi2;
 }
+
+/*
+ * Grid excluded-volume dummies, RawGridExv::create on the expanded molecular grid
+ * (source/core/grid/exv/RawGridExv.cpp:10-59) as HistogramManagerMTFFGrid::calculate_all() sees it
+ * (Molecule::get_volume_grid() expands the grid first, Grid.cpp:428-431), with the reference's
+ * default settings: cell width 1 A, scaling 0.25 (1 for structures under 50 A in any direction),
+ * min_exv_radius (rvol) 2.15 A, exv width 1 A, AtomicOnly expansion, hydration shell correction
+ * -0.35 A (source/core/settings/GridSettings.cpp, MoleculeSettings.cpp:41).
+ *   axes (Grid.cpp:34-102): the bounding box of atoms, waters and the origin, widened per axis by
+ *     max(diff/2 * scaling, r_vdw(P) + r_vdw(O) + shell correction + 3 cells), floored/ceiled with
+ *     one more cell; bins = (max - min) / width;
+ *   members (Grid.cpp:332-375): each atom marks the cell round((x - min) / width) A_CENTER, each
+ *     water W_CENTER;
+ *   expansion (include/core/grid/expansion/SphericalExpander.h:27-76): for every atom, cells of the
+ *     box bin +- ceil(max(r_vdw, rvol) / width) whose centre lies within r_vdw get A_AREA when they hold
+ *     nothing but VOLUME, within (r_vdw, rvol] VOLUME when they hold nothing;
+ *   dummies: cells with A_CENTER, A_AREA or VOLUME, swept x-major over the atoms' bin box widened by
+ *     round(max(rvol, 2) / width) cells, at their centres min + i * width.
+ * atoms: n x {x, y, z, ff} (double), waters: n x {x, y, z}.  Writes up to cap dummies (n x 3) and
+ * returns their count; *volume = count * width^3 (Grid::get_volume).
+ */
+static double vdw_of_ff(int ff) {
+    /* constants::radius::get_vdw_radius(form_factor_t) (include/core/form_factor/FormFactorType.h:173-192)
+     * over include/core/constants/vdwTable.h: H 1.1, C 1.96, N 1.79, O 1.71, S 2.06, Ar 1.88 */
+    switch (ff) {
+        case 1: return 1.71;                                /* WATER = OH: oxygen */
+        case 2: return 1.1;                                 /* H */
+        case 3: case 4: case 5: case 6: return 1.96;        /* C, CH, CH2, CH3 */
+        case 7: case 8: case 9: case 10: return 1.79;       /* N, NH, NH2, NH3 */
+        case 11: return 1.71;                               /* O */
+        case 12: case 13: return 2.06;                      /* S, SH */
+        case 14: return 1.88;                               /* OTHER: argon */
+        default: return 0.0;
+    }
+}
+
+int64_t oracle_grid_exv(const double* atoms, int32_t na, const double* waters, int32_t nw, double* out, int64_t cap,
+                        double* volume) {
+    enum { A_CENTER = 1, W_CENTER = 2, A_AREA = 4, VOLUME = 8 };
+    const double width = 1.0, rvol = 2.15;
+    double mn[3] = {0, 0, 0}, mx[3] = {0, 0, 0};
+    for (int32_t i = 0; i < na; ++i)
+        for (int d = 0; d < 3; ++d) {
+            if (atoms[4 * (size_t)i + d] < mn[d]) mn[d] = atoms[4 * (size_t)i + d];
+            if (atoms[4 * (size_t)i + d] > mx[d]) mx[d] = atoms[4 * (size_t)i + d];
+        }
+    for (int32_t i = 0; i < nw; ++i)
+        for (int d = 0; d < 3; ++d) {
+            if (waters[3 * (size_t)i + d] < mn[d]) mn[d] = waters[3 * (size_t)i + d];
+            if (waters[3 * (size_t)i + d] > mx[d]) mx[d] = waters[3 * (size_t)i + d];
+        }
+    double diff[3] = {mx[0] - mn[0], mx[1] - mn[1], mx[2] - mn[2]};
+    double scaling = (diff[0] < 50 || diff[1] < 50 || diff[2] < 50) ? 1.0 : 0.25;
+    double margin = 2.14 + 1.71 + (-0.35) + 3 * width;
+    double gmin[3];
+    int bins[3];
+    for (int d = 0; d < 3; ++d) {
+        double e = fmax(0.5 * diff[d] * scaling, margin);
+        gmin[d] = floor(mn[d] - e - width);
+        double gmax = ceil(mx[d] + e + width);
+        bins[d] = (int)((gmax - gmin[d]) / width);
+    }
+    size_t cells = (size_t)bins[0] * bins[1] * bins[2];
+    unsigned char* g = calloc(cells, 1);
+    if (!g) return -1;
+#define CELL(i, j, k) g[((size_t)(i) * bins[1] + (j)) * bins[2] + (k)]
+    int lo[3] = {1 << 30, 1 << 30, 1 << 30}, hi[3] = {-(1 << 30), -(1 << 30), -(1 << 30)};
+    for (int32_t i = 0; i < na; ++i) {
+        int b[3];
+        for (int d = 0; d < 3; ++d) {
+            b[d] = (int)round((atoms[4 * (size_t)i + d] - gmin[d]) / width);
+            if (b[d] < lo[d]) lo[d] = b[d];
+            if (b[d] + 1 > hi[d]) hi[d] = b[d] + 1;
+        }
+        CELL(b[0], b[1], b[2]) |= A_CENTER;
+    }
+    for (int32_t i = 0; i < nw; ++i) {
+        int b[3];
+        for (int d = 0; d < 3; ++d) b[d] = (int)round((waters[3 * (size_t)i + d] - gmin[d]) / width);
+        CELL(b[0], b[1], b[2]) |= W_CENTER;
+    }
+    for (int32_t a = 0; a < na; ++a) {
+        const double* p = atoms + 4 * (size_t)a;
+        double rvdw = vdw_of_ff((int)p[3]), rvdw2 = rvdw * rvdw, rvol2 = rvol * rvol;
+        int br = (int)ceil(fmax(rvdw, rvol) / width);
+        int b[3], lo_[3], hi_[3];
+        for (int d = 0; d < 3; ++d) {
+            b[d] = (int)round((p[d] - gmin[d]) / width);
+            lo_[d] = b[d] - br > 0 ? b[d] - br : 0;
+            hi_[d] = b[d] + br + 1 < bins[d] ? b[d] + br + 1 : bins[d];
+        }
+        for (int i = lo_[0]; i < hi_[0]; ++i) {
+            double x2 = pow(gmin[0] + i * width - p[0], 2);
+            for (int j = lo_[1]; j < hi_[1]; ++j) {
+                double x2y2 = x2 + pow(gmin[1] + j * width - p[1], 2);
+                for (int k = lo_[2]; k < hi_[2]; ++k) {
+                    double dist = x2y2 + pow(gmin[2] + k * width - p[2], 2);
+                    unsigned char* c = &CELL(i, j, k);
+                    int fill = dist <= rvdw2;
+                    if (fill) {
+                        if (!(*c == 0 || *c == VOLUME)) continue;
+                        *c |= A_AREA;
+                    } else if (dist <= rvol2) {
+                        if (*c != 0) continue;
+                        *c |= VOLUME;
+                    }
+                }
+            }
+        }
+    }
+    int buffer = (int)fmax(1.0, round(fmax(rvol, 2.0) / width));
+    int64_t n = 0;
+    if (na > 0) {
+        for (int i = lo[0] - buffer > 0 ? lo[0] - buffer : 0; i < (hi[0] + buffer + 1 < bins[0] ? hi[0] + buffer + 1 : bins[0]); ++i)
+            for (int j = lo[1] - buffer > 0 ? lo[1] - buffer : 0; j < (hi[1] + buffer + 1 < bins[1] ? hi[1] + buffer + 1 : bins[1]); ++j)
+                for (int k = lo[2] - buffer > 0 ? lo[2] - buffer : 0; k < (hi[2] + buffer + 1 < bins[2] ? hi[2] + buffer + 1 : bins[2]); ++k) {
+                    if (!(CELL(i, j, k) & (A_CENTER | A_AREA | VOLUME))) continue;
+                    if (out && n < cap) {
+                        out[3 * n] = gmin[0] + i * width;
+                        out[3 * n + 1] = gmin[1] + j * width;
+                        out[3 * n + 2] = gmin[2] + k * width;
+                    }
+                    ++n;
+                }
+    }
+#undef CELL
+    free(g);
+    if (volume) *volume = (double)n * width * width * width;
+    return n;
+}

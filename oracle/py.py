@@ -171,6 +171,21 @@ def ff_raw(t, q):
     return np.array([lib().oracle_ff_raw(int(t), float(x)) for x in np.atleast_1d(q)])
 
 
+def grid_exv(xyz, ff, waters=None):
+    """Grid excluded-volume dummies of the expanded molecular grid (RawGridExv::create): [n, 3], volume."""
+    L = lib()
+    f = L.oracle_grid_exv
+    f.restype = C.c_int64
+    f.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, C.POINTER(C.c_double)]
+    a = np.ascontiguousarray(np.column_stack([np.asarray(xyz, float).reshape(-1, 3), np.asarray(ff, float)]))
+    w = np.ascontiguousarray(np.zeros((0, 3)) if waters is None else np.asarray(waters, float).reshape(-1, 3))
+    vol = C.c_double(0)
+    n = f(a.ctypes.data, len(a), w.ctypes.data, len(w), None, 0, C.byref(vol))
+    out = np.zeros((max(1, n), 3))
+    f(a.ctypes.data, len(a), w.ctypes.data, len(w), out.ctypes.data, n, C.byref(vol))
+    return out[:n], vol.value
+
+
 def linear_lsq(data, model, err):
     out = np.zeros(5)
     lib().oracle_linear_lsq(np.ascontiguousarray(data, np.float64), np.ascontiguousarray(model, np.float64),
@@ -202,6 +217,23 @@ def ref_read_structure(path: str, implicit_h: int = -1, center: int = -1):
         raise RuntimeError(L.ref_last_error().decode())
     a, w = a[: na.value], w[: nw.value]
     return a[:, :3].copy(), a[:, 3].copy(), a[:, 4].astype(np.int32), w[:, :3].copy(), w[:, 3].copy()
+
+
+def ref_grid_exv(xyz, ff, waters=None):
+    """RawGridExv::create of the reference on the expanded grid: dummies [n, 3], volume."""
+    L = ref()
+    f = L.ref_grid_exv
+    f.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int),
+                  C.POINTER(C.c_double)]
+    a = np.ascontiguousarray(np.column_stack([np.asarray(xyz, float).reshape(-1, 3), np.asarray(ff, float)]))
+    w = np.ascontiguousarray(np.zeros((0, 3)) if waters is None else np.asarray(waters, float).reshape(-1, 3))
+    n, vol = C.c_int(), C.c_double()
+    if f(a.ctypes.data, len(a), w.ctypes.data, len(w), None, 0, C.byref(n), C.byref(vol)):
+        raise RuntimeError(L.ref_last_error().decode())
+    out = np.zeros((max(1, n.value), 3))
+    if f(a.ctypes.data, len(a), w.ctypes.data, len(w), out.ctypes.data, n.value, C.byref(n), C.byref(vol)):
+        raise RuntimeError(L.ref_last_error().decode())
+    return out[: n.value], vol.value
 
 
 def ref_available() -> bool:

@@ -38,6 +38,9 @@
 #include <settings/GeneralSettings.h>
 #include <settings/HistogramSettings.h>
 #include <settings/MoleculeSettings.h>
+#include <settings/GridSettings.h>
+#include <grid/Grid.h>
+#include <grid/exv/RawGridExv.h>
 #include <io/File.h>
 
 #include <chrono>
@@ -167,6 +170,39 @@ void* ref_molecule_new(const double* atoms, int n_a, const double* waters, int n
 }
 
 void ref_molecule_free(void* m) { delete static_cast<FixedVolumeMolecule*>(m); }
+
+// RawGridExv::create on the molecule's expanded grid, as HistogramManagerMTFFGrid::calculate_all()
+// uses it (get_volume_grid() expands first): atoms n x {x, y, z, ff}, waters n x {x, y, z}; writes
+// up to cap dummies n x {x, y, z}.  settings::grid::scaling is reset to its default first: the
+// reference's Grid constructor sets it to 1 for small structures and leaves it so for later grids.
+int ref_grid_exv(const double* atoms, int n_a, const double* waters, int n_w, double* out, int cap, int* n_out,
+                 double* volume) {
+    return guarded([&] {
+        settings::grid::scaling = 0.25;
+        std::vector<data::AtomFF> a;
+        for (int i = 0; i < n_a; ++i) {
+            const double* r = atoms + 4 * static_cast<size_t>(i);
+            a.emplace_back(Vector3<double>(r[0], r[1], r[2]), static_cast<form_factor::form_factor_t>(static_cast<int>(r[3])));
+        }
+        std::vector<data::Water> w;
+        for (int i = 0; i < n_w; ++i) {
+            const double* r = waters + 3 * static_cast<size_t>(i);
+            w.emplace_back(Vector3<double>(r[0], r[1], r[2]));
+        }
+        std::vector<data::Body> bodies;
+        bodies.emplace_back(std::move(a), std::move(w));
+        data::Molecule m(std::move(bodies));
+        *volume = m.get_volume_grid();
+        auto exv = grid::exv::RawGridExv::create(m.get_grid()).interior;
+        *n_out = static_cast<int>(exv.size());
+        if (out && cap >= *n_out)
+            for (size_t i = 0; i < exv.size(); ++i) {
+                out[3 * i] = exv[i].x();
+                out[3 * i + 1] = exv[i].y();
+                out[3 * i + 2] = exv[i].z();
+            }
+    });
+}
 
 // A structure file read by the reference's own reader (data::Molecule(io::File), which assigns the
 // united-atom form-factor types), returned as arrays: atoms n x {x, y, z, weight, ff}, waters

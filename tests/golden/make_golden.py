@@ -58,6 +58,14 @@ def run_case(name, atoms, ff, w, waters, ww, exv, volume, bin_width, manager, cw
     print(name, "bins", len(d), "I" if "Iq" in out else "")
 
 
+def grid_case(name, atoms, ff, waters):
+    d, vol = O.ref_grid_exv(atoms, ff, waters)
+    assert np.all(d == np.round(d)), "dummies of a 1 A grid with integer bounds sit at integer coordinates"
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), atoms=atoms, ff=np.asarray(ff, np.int32), waters=waters,
+                        dummies=d.astype(np.int32), volume=vol, manager="gridexv")
+    print(name, "dummies", len(d), "volume", vol)
+
+
 def main():
     O.ref()
     # SimpleCube: 8 corners + centre as atoms (carbon), 8 corner waters
@@ -103,6 +111,17 @@ def main():
                  crho=1.01, dwa=0.3, dwx=0.1)
         run_case(f"pdb_{pdb}_ffexplicit", xyz, f, wt, wat, wwt, np.zeros((0, 3)), vol, 0.1, "ffexplicit", cw=1.05,
                  cx=1.02)
+    # Grid excluded-volume dummies (RawGridExv::create on the expanded grid) and the grid volume
+    grid_case("gridexv_cube", np.vstack([CUBE, [[0, 0, 0]]]), np.full(9, 3), CUBE.copy())
+    for k, (na, nw, spread) in enumerate([(300, 60, 8.0), (1500, 300, 14.0)]):
+        xyz = rng.normal(0, spread, (na, 3)).astype(np.float32).astype(np.float64)
+        f = rng.choice([1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14], na)
+        wat = rng.normal(0, spread * 1.2, (nw, 3)).astype(np.float32).astype(np.float64)
+        grid_case(f"gridexv_random{k}", xyz, f, wat)
+    path = os.path.join(files, "2epe.pdb")
+    if os.path.exists(path):
+        xyz, _, f, wat, _ = O.ref_read_structure(path)
+        grid_case("gridexv_2epe", xyz.astype(np.float32).astype(np.float64), f, wat.astype(np.float32).astype(np.float64))
     # Simple excluded volume enabled (weights shifted by -rho_w V / N, SimpleExvModel.cpp:23-28)
     xyz = rng.normal(0, 6, (120, 3))
     f = rng.choice(elements, 120)

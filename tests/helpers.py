@@ -11,7 +11,13 @@ RHO_W = 0.334
 
 
 def golden_cases(prefix=""):
-    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, prefix + "*.npz")))
+    """Histogram/intensity fixtures (the grid excluded-volume fixtures are listed by grid_cases)."""
+    return sorted(n for n in (os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, prefix + "*.npz")))
+                  if not n.startswith("gridexv_"))
+
+
+def grid_cases():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "gridexv_*.npz")))
 
 
 def load_golden(name):

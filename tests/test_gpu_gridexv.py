@@ -1,0 +1,79 @@
+"""Excluded-volume dummies of the molecular grid on the device (RawGridExv on the expanded grid)
+against the reference's fixtures and the oracle, and the FFGrid / FFAvg paths that take their
+excluded volume from that grid.  Bar: the same cells in the same order, the same volume, and
+histograms bit-identical to those built from the oracle's dummies."""
+import numpy as np
+import pytest
+
+from ausaxs_b200 import _capi, hist
+from oracle import py as O
+from tests.helpers import grid_cases, load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _records(xyz, ff):
+    return hist.pack(xyz, ff, True)
+
+
+@pytest.mark.parametrize("name", grid_cases())
+def test_grid_dummies_vs_reference(name, gpu_ctx):
+    g = load_golden(name)
+    a = _records(g["atoms"], g["ff"])
+    w = _records(g["waters"], np.ones(len(g["waters"]), np.int32))
+    d, vol = _capi.grid_exv(gpu_ctx, a, w)
+    np.testing.assert_array_equal(d[:, :3], g["dummies"].astype(np.float32))
+    assert np.all(d[:, 3].view(np.int32) == 0)  # form_factor_t EXCLUDED_VOLUME
+    assert vol == float(g["volume"])
+
+
+@pytest.mark.parametrize("seed,na,nw,spread", [(1, 1, 0, 5.0), (2, 40, 0, 3.0), (3, 2000, 400, 12.0), (4, 6000, 0, 30.0)])
+def test_grid_dummies_vs_oracle(seed, na, nw, spread, gpu_ctx):
+    rng = np.random.default_rng(seed)
+    xyz = rng.normal(0, spread, (na, 3)).astype(np.float32).astype(np.float64)
+    ff = rng.choice(np.arange(1, 15), na).astype(np.int32)
+    wat = rng.normal(0, spread * 1.2, (nw, 3)).astype(np.float32).astype(np.float64)
+    d, vol = _capi.grid_exv(gpu_ctx, _records(xyz, ff), _records(wat, np.ones(nw, np.int32)))
+    do, vo = O.grid_exv(xyz, ff, wat)
+    np.testing.assert_array_equal(d[:, :3].astype(np.float64), do)
+    assert vol == vo
+
+
+def test_ffgrid_from_grid_equals_given_dummies(gpu_ctx):
+    rng = np.random.default_rng(5)
+    xyz = rng.normal(0, 10, (1800, 3)).astype(np.float32).astype(np.float64)
+    ff = rng.choice([3, 4, 5, 7, 8, 11, 12], 1800).astype(np.int32)
+    wat = rng.normal(0, 12, (300, 3)).astype(np.float32).astype(np.float64)
+    dummies, _ = O.grid_exv(xyz, ff, wat)
+    m_grid = hist.Molecule(atoms=xyz, ff_types=ff, waters=wat, volume=1.0)           # dummies from the grid
+    m_given = hist.Molecule(atoms=xyz, ff_types=ff, waters=wat, exv=dummies, volume=1.0)
+    h1 = hist.HistogramManagerMTFFGrid(m_grid, 0.1, 8000, gpu_ctx).calculate_all()
+    h2 = hist.HistogramManagerMTFFGrid(m_given, 0.1, 8000, gpu_ctx).calculate_all()
+    np.testing.assert_array_equal(h1.get_raw_aa_counts_by_ff(), h2.get_raw_aa_counts_by_ff())
+    np.testing.assert_array_equal(h1.get_raw_aw_counts_by_ff(), h2.get_raw_aw_counts_by_ff())
+    np.testing.assert_array_equal(h1.get_d_axis_xx(), h2.get_d_axis_xx())
+    o = O.hist_ff(2, O.pack_points(xyz, ff, True), O.pack_points(wat, np.ones(len(wat), np.int32), True),
+                  O.pack_points(dummies, np.zeros(len(dummies), np.int32), True), 0.1, 8000, 0.0)
+    np.testing.assert_array_equal(h1.get_raw_aa_counts_by_ff(), o.aa)
+    q = np.linspace(0.01, 0.8, 120)
+    I = hist.profile(hist.HistogramManagerMTFFGrid(m_grid, 0.1, 8000, gpu_ctx), q)
+    Io, _ = O.debye_ff(2, o, q)
+    np.testing.assert_allclose(I, Io, rtol=1e-6, atol=1e-9 * np.abs(Io).max())
+
+
+def test_ffavg_z_from_grid_volume(gpu_ctx):
+    rng = np.random.default_rng(6)
+    xyz = rng.normal(0, 9, (1200, 3)).astype(np.float32).astype(np.float64)
+    ff = rng.choice([3, 7, 11, 12], 1200).astype(np.int32)
+    wat = rng.normal(0, 11, (200, 3)).astype(np.float32).astype(np.float64)
+    _, vol = O.grid_exv(xyz, ff, wat)
+    m = hist.Molecule(atoms=xyz, ff_types=ff, waters=wat)  # no volume: Molecule::get_volume_grid()
+    assert m.get_volume_grid() == vol
+    h = hist.HistogramManagerMTFFAvg(m, True, 0.25, 8000, gpu_ctx).calculate_all()
+    o = O.hist_ff(0, O.pack_points(xyz, ff, True), O.pack_points(wat, np.ones(len(wat), np.int32), True), None,
+                  0.25, 8000, vol * 0.334 / len(xyz))
+    np.testing.assert_array_equal(h.get_raw_aa_counts_by_ff(), o.aa)
+    q = np.linspace(0.005, 0.5, 100)
+    _, I = h.debye_transform(q)
+    Io, _ = O.debye_ff(0, o, q)
+    np.testing.assert_allclose(I, Io, rtol=1e-6)

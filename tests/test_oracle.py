@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from oracle import py as O
-from tests.helpers import golden_cases, load_golden, oracle_for
+from tests.helpers import grid_cases, golden_cases, load_golden, oracle_for
 
 CASES = golden_cases()
 
@@ -109,3 +109,11 @@ def test_linear_lsq_matches_reference():
     r = O.ref_linear_lsq(x, y, e)
     o = O.linear_lsq(x, y, e)
     np.testing.assert_allclose(o[[0, 1, 4]], r[[0, 1, 4]], rtol=1e-10)
+
+
+@pytest.mark.parametrize("name", grid_cases())
+def test_oracle_grid_exv_matches_reference(name):
+    g = load_golden(name)
+    d, vol = O.grid_exv(g["atoms"], g["ff"], g["waters"])
+    np.testing.assert_array_equal(d, g["dummies"])  # same cells, same (x-major) order
+    assert vol == float(g["volume"]) == len(d)
