@@ -106,8 +106,8 @@ def load():
                                                    C.POINTER(DebyeParams), f64, f64]
         L.ausaxs_gpu_structure_histogram.argtypes = [vp, vp, C.POINTER(HistConfig), C.POINTER(HistResult)]
         L.ausaxs_gpu_linear_lsq.argtypes = [vp, f64, f64, f64, C.c_int32, f64]
-        L.ausaxs_gpu_grid_exv.argtypes = [vp, f32, C.c_int32, f32, C.c_int32, f32, C.c_int64, C.POINTER(C.c_int64),
-                                          C.POINTER(C.c_double)]
+        L.ausaxs_gpu_grid_exv.argtypes = [vp, f32, C.c_int32, f32, C.c_int32, C.c_int32, f32, C.c_int64,
+                                          C.POINTER(C.c_int64), C.POINTER(C.c_double)]
         i64 = C.POINTER(C.c_int64)
         i32 = C.POINTER(C.c_int32)
         L.ausaxs_gpu_batch_create.argtypes = [vp, C.POINTER(HistConfig), C.c_int32, f32, i64, f32, i64, f32, i64, f64,
@@ -222,16 +222,31 @@ EXV_FROM_GRID = -1
 
 
 def grid_exv(ctx: "Context", atoms, waters):
-    """Excluded-volume dummies of the molecular grid (RawGridExv) and the grid volume: ([n, 4] records, volume)."""
+    """Excluded-volume dummies of the molecular grid (RawGridExv) and the grid volume: ([n, 4] records, volume).
+    One device pass when the first guess of the dummy count (40 per atom) suffices, else a second."""
     a = np.ascontiguousarray(atoms, np.float32).reshape(-1, 4)
     w = np.ascontiguousarray(waters, np.float32).reshape(-1, 4)
     n = C.c_int64(0)
     vol = C.c_double(0)
-    check(load().ausaxs_gpu_grid_exv(ctx.h, fptr(a), len(a), fptr(w), len(w), None, 0, C.byref(n), C.byref(vol)))
-    out = np.zeros((max(1, n.value), 4), np.float32)
-    check(load().ausaxs_gpu_grid_exv(ctx.h, fptr(a), len(a), fptr(w), len(w), fptr(out), n.value, C.byref(n),
-                                     C.byref(vol)))
-    return out[: n.value], vol.value
+    cap = 40 * len(a) + 1024
+    while True:
+        out = np.zeros((cap, 4), np.float32)
+        rc = load().ausaxs_gpu_grid_exv(ctx.h, fptr(a), len(a), fptr(w), len(w), 1, fptr(out), cap, C.byref(n),
+                                        C.byref(vol))
+        if rc == ERR_CAPACITY and n.value > cap:
+            cap = n.value
+            continue
+        check(rc)
+        return out[: n.value], vol.value
+
+
+def grid_exv_device(ctx: "Context", atoms_dev, n_atoms: int, waters_dev, n_waters: int, out_dev, capacity: int):
+    """The same on device records (device addresses); writes the dummies to out_dev.  Returns (count, volume)."""
+    n = C.c_int64(0)
+    vol = C.c_double(0)
+    check(load().ausaxs_gpu_grid_exv(ctx.h, devptr(atoms_dev, C.c_float), n_atoms, devptr(waters_dev, C.c_float),
+                                     n_waters, 0, devptr(out_dev, C.c_float), capacity, C.byref(n), C.byref(vol)))
+    return n.value, vol.value
 
 
 def default_context(device: int = 0) -> Context:
@@ -243,15 +258,16 @@ def default_context(device: int = 0) -> Context:
 class Structure:
     """A device-resident structure (ausaxs_gpu_structure_*): upload once, profile many times."""
 
-    def __init__(self, ctx: Context, atoms, waters, exv=None, ff_typed: bool = True):
+    def __init__(self, ctx: Context, atoms, waters, exv=None, ff_typed: bool = True, exv_from_grid: bool = False):
+        """exv: excluded-volume dummy records, or exv_from_grid: the dummies of the molecular grid."""
         self.ctx = ctx
         self._a = np.ascontiguousarray(atoms, np.float32)
         self._w = np.ascontiguousarray(waters, np.float32)
         self._x = None if exv is None else np.ascontiguousarray(exv, np.float32)
+        nx = EXV_FROM_GRID if exv_from_grid else (0 if self._x is None else len(self._x))
         h = C.c_void_p()
         check(load().ausaxs_gpu_structure_create(ctx.h, int(ff_typed), fptr(self._a), len(self._a), fptr(self._w),
-                                                 len(self._w), fptr(self._x), 0 if self._x is None else len(self._x),
-                                                 1, C.byref(h)))
+                                                 len(self._w), fptr(self._x), nx, 1, C.byref(h)))
         self.h = h
 
     def close(self):
@@ -352,10 +368,6 @@ class Batch:
         check(load().ausaxs_gpu_batch_histogram(self.h, index, C.byref(r)))
         return r, bufs
 
-
-ERR_CAPACITY = 5
-ERR_TIMEOUT = 6
-ERR_NOT_FOUND = 7
 
 
 class Server:

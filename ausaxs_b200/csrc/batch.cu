@@ -175,11 +175,9 @@ struct Batch {
         int rows[2][3] = {{1, 1, 1}, {1, 1, 1}};
         const bool grid = cfg.manager == AUSAXS_MANAGER_FFGRID;
         // on-chip rows that fit next to the batch-wide bin count
-        const size_t cap = 232448 - 1024;
-        if (pairhist_smem_bytes(1, max_nb, false, 512) > cap)
+        if (pairhist_launch_smem(1, max_nb, false, 512) > kPairSmemCap)
             throw Error{AUSAXS_ERR_CAPACITY, "too many distance bins for a batched launch"};
-        int max_rows = 1;
-        while (max_rows < 4096 && pairhist_smem_bytes(max_rows + 1, max_nb, false, 512) <= cap) ++max_rows;
+        const int max_rows = pairhist_max_rows(max_nb, false);
         for (int i : order) {
             const Structure& S = *items[i];
             const int biggest = std::max({S.n_a, S.n_w, grid ? S.n_x : 0});
@@ -202,9 +200,10 @@ struct Batch {
                 if (js[b][g].empty()) continue;
                 Launch La;
                 La.tile = b ? c.tile_large : c.tile_small;
-                La.smem = pairhist_smem_bytes(rows[b][g], max_nb, false, La.tile);
-                if (La.smem > 232448 - 1024) throw Error{AUSAXS_ERR_CAPACITY, "too many distance bins for a batched launch"};
-                const int per_sm = std::max(1, std::min((int)(233472 / (La.smem + 1024)), 2048 / La.tile));
+                La.smem = pairhist_launch_smem(rows[b][g], max_nb, false, La.tile);
+                if (La.smem > kPairSmemCap) throw Error{AUSAXS_ERR_CAPACITY, "too many distance bins for a batched launch"};
+                const int per_sm =
+                    pairhist_ctas_per_sm(La.smem, La.tile, pairhist_dreg(rows[b][g], max_nb, false, La.tile));
                 La.grid = (int)std::min<long long>((long long)ctx->sm_count * per_sm, std::max<long long>(1, tiles[b][g]));
                 PairLaunch& L = La.L;
                 L.jobs = jobs.as<PairJob>() + at;
@@ -216,6 +215,7 @@ struct Batch {
                 L.tile_counter = misc.as<unsigned long long>() + counter++;
                 L.overflow = overflow();
                 L.weighted = 0;
+                L.dreg = pairhist_dreg(rows[b][g], max_nb, false, La.tile) ? 1 : 0;
                 L.wscale = nullptr;
                 AUSAXS_CUDA(cudaMemcpy(jobs.as<PairJob>() + at, js[b][g].data(), sizeof(PairJob) * js[b][g].size(),
                                        cudaMemcpyHostToDevice));

@@ -21,10 +21,28 @@ Structure& scratch(Ctx& C) {
     return *C.scratch;
 }
 
+GridExv& grid_workspace(Ctx& C) {
+    if (!C.grid) C.grid = std::make_shared<GridExv>();
+    return *C.grid;
+}
+
 bool ff_manager(int m) { return m == AUSAXS_MANAGER_FFAVG || m == AUSAXS_MANAGER_FFEXPLICIT || m == AUSAXS_MANAGER_FFGRID; }
 
 void check_cfg(const ausaxs_hist_config* cfg) {
     if (!cfg) throw Error{AUSAXS_ERR_ARGUMENT, "null configuration"};
+}
+
+// Loads an FF-typed structure and runs its molecular grid (RawGridExv on the expanded grid); with
+// with_dummies the structure is reloaded with the grid's dummies as its excluded-volume points.
+// Returns the grid volume (Molecule::get_volume_grid()).
+double load_with_grid(Structure& S, const float* atoms, int32_t n_atoms, const float* waters, int32_t n_waters,
+                      bool host, bool with_dummies) {
+    Ctx& C = *S.ctx;
+    S.load(atoms, n_atoms, waters, n_waters, nullptr, 0, 1, host);  // census: validation and bounding box
+    GridExv& g = grid_workspace(C);
+    g.run(C, S.raw_a.as<float4>(), n_atoms, S.raw_w.as<float4>(), n_waters, S.lo, S.hi, with_dummies);
+    if (with_dummies) S.load(atoms, n_atoms, waters, n_waters, g.points.as<float>(), (int)g.count, 1, host, 0);
+    return g.volume;
 }
 
 // The scratch structure of a one-shot host call, with the grid-derived inputs the configuration asks
@@ -44,11 +62,8 @@ ausaxs_hist_config load_scratch(Ctx& C, const ausaxs_hist_config& cfg, const flo
         S.load(atoms, n_atoms, waters, n_waters, grid ? exv : nullptr, grid ? n_exv : 0, ff_manager(cfg.manager), true);
         return c;
     }
-    S.load(atoms, n_atoms, waters, n_waters, nullptr, 0, 1, true);  // census: validation and bounding box
-    GridExv g;
-    g.run(C, S.raw_a.as<float4>(), n_atoms, S.raw_w.as<float4>(), n_waters, S.lo, S.hi, gen);
-    if (zgrid) c.z_exv = n_atoms ? g.volume * 0.334 / n_atoms : 0.0;  // rho_w (Constants.h:114)
-    if (gen) S.load(atoms, n_atoms, waters, n_waters, g.points.as<float>(), (int)g.count, 1, true, 0);
+    const double volume = load_with_grid(S, atoms, n_atoms, waters, n_waters, true, gen);
+    if (zgrid) c.z_exv = n_atoms ? volume * 0.334 / n_atoms : 0.0;  // rho_w (Constants.h:114)
     return c;
 }
 
@@ -145,7 +160,7 @@ int ausaxs_gpu_ctx_enable_timing(ausaxs_gpu_ctx* ctx, int32_t enable) {
 
 int ausaxs_gpu_ctx_kernel_time(ausaxs_gpu_ctx* ctx, int32_t kernel_class, double* ms, int64_t* launches) {
     return guarded([&] {
-        if (!ctx || kernel_class < 0 || kernel_class > 3) throw Error{AUSAXS_ERR_ARGUMENT, "bad argument"};
+        if (!ctx || kernel_class < 0 || kernel_class > 4) throw Error{AUSAXS_ERR_ARGUMENT, "bad argument"};
         Ctx& C = ctx->impl;
         C.time_collect();
         if (ms) *ms = C.timed[kernel_class].ms;
@@ -254,7 +269,12 @@ int ausaxs_gpu_structure_create(ausaxs_gpu_ctx* ctx, int32_t ff_typed, const flo
         auto* h = new ausaxs_gpu_structure();
         h->impl.ctx = &C;
         try {
-            h->impl.load(atoms, n_atoms, waters, n_waters, exv, n_exv, ff_typed ? 1 : 0, host_pointers != 0);
+            if (n_exv == AUSAXS_EXV_FROM_GRID) {
+                if (!ff_typed) throw Error{AUSAXS_ERR_ARGUMENT, "grid excluded volume needs form-factor typed atoms"};
+                load_with_grid(h->impl, atoms, n_atoms, waters, n_waters, host_pointers != 0, true);
+            } else {
+                h->impl.load(atoms, n_atoms, waters, n_waters, exv, n_exv, ff_typed ? 1 : 0, host_pointers != 0);
+            }
         } catch (...) {
             delete h;
             throw;
@@ -291,6 +311,43 @@ int ausaxs_gpu_structure_histogram(ausaxs_gpu_ctx* ctx, ausaxs_gpu_structure* s,
         check_cfg(cfg);
         s->impl.enqueue_histogram(*cfg);
         s->impl.read_histogram(*cfg, out);
+    });
+}
+
+// Excluded-volume dummies of the molecular grid (RawGridExv::create on the expanded grid) and the grid
+// volume; the scratch structure takes the census, the context's grid workspace is reused.
+int ausaxs_gpu_grid_exv(ausaxs_gpu_ctx* ctx, const float* atoms, int32_t n_atoms, const float* waters,
+                        int32_t n_waters, int32_t host_pointers, float* exv_out, int64_t capacity, int64_t* n_exv,
+                        double* volume) {
+    return guarded([&] {
+        if (!ctx || !n_exv || n_atoms < 0 || n_waters < 0 || (n_atoms && !atoms) || (n_waters && !waters) ||
+            (capacity > 0 && !exv_out))
+            throw Error{AUSAXS_ERR_ARGUMENT, "invalid argument"};
+        Ctx& C = ctx->impl;
+        AUSAXS_CUDA(cudaSetDevice(C.device));
+        const bool host = host_pointers != 0;
+        *n_exv = 0;
+        if (volume) *volume = 0;
+        Structure& S = scratch(C);  // census and validation of the points (form-factor types, finite coordinates)
+        S.load(atoms, n_atoms, waters, n_waters, nullptr, 0, 1, host);
+        GridExv& g = grid_workspace(C);
+        // device output: the dummies go straight to exv_out; a short buffer fails once the count is known
+        float4* direct = (!host && capacity > 0) ? reinterpret_cast<float4*>(exv_out) : nullptr;
+        try {
+            g.run(C, S.raw_a.as<float4>(), n_atoms, S.raw_w.as<float4>(), n_waters, S.lo, S.hi, capacity > 0, direct,
+                  capacity);
+        } catch (const Error&) {
+            *n_exv = g.count;
+            if (volume) *volume = g.volume;
+            throw;
+        }
+        *n_exv = g.count;
+        if (volume) *volume = g.volume;
+        if (host && capacity > 0 && g.count > 0) {
+            if (capacity < g.count) throw Error{AUSAXS_ERR_CAPACITY, "exv_out holds fewer records than the grid has dummies"};
+            AUSAXS_CUDA(cudaMemcpyAsync(exv_out, g.points.p, (size_t)g.count * 16, cudaMemcpyDeviceToHost, C.stream));
+        }
+        AUSAXS_CUDA(cudaStreamSynchronize(C.stream));
     });
 }
 

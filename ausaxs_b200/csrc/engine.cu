@@ -106,6 +106,7 @@ void Structure::load_begin(const float* atoms, int n_atoms, const float* waters,
     census_launch(raw_a.as<float4>(), n_a, ff_typed, d_stats, C.sm_count, s);
     census_launch(raw_w.as<float4>(), n_w, 0, d_stats, C.sm_count, s);
     census_launch(raw_x.as<float4>(), n_x, 0, d_stats, C.sm_count, s);
+    radius_launch(raw_a.as<float4>(), n_a, raw_w.as<float4>(), n_w, raw_x.as<float4>(), n_x, d_stats, C.sm_count, s);
     C.check_launch("census");
     AUSAXS_CUDA(cudaMemcpyAsync(h_stats, d_stats, sizeof(PrepStats), cudaMemcpyDeviceToHost, s));
 }
@@ -126,7 +127,12 @@ void Structure::load_end(const PrepStats& st) {
             double e = (double)hi[k] - (double)lo[k];
             d2 += e * e;
         }
-        dmax = (float)(std::sqrt(d2) * (1 + 1e-6) + 1e-3);
+        // every pair distance is at most the box diagonal and at most twice the radius about the box
+        // centre (tight for globules and shells, where the diagonal is sqrt(3) times the diameter)
+        double r2;
+        std::memcpy(&r2, &st.r2, sizeof r2);
+        const double bound = std::min(std::sqrt(d2), 2.0 * std::sqrt(r2));
+        dmax = (float)(bound * (1 + 1e-6) + 1e-3);
     } else {
         dmax = 0;
     }
@@ -293,10 +299,8 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
     for (auto& j : js) slot_rows[j.slot] = std::max(slot_rows[j.slot], j.rows);
 
     // on-chip budget: split rows of a job into groups when its [rows][nb] counts do not fit
-    const size_t smem_cap = 232448 - 1024;
-    int max_group_rows = 1;
-    while (max_group_rows < 4096 && pairhist_smem_bytes(max_group_rows + 1, nb, weighted && mt, 512) <= smem_cap) ++max_group_rows;
-    if (pairhist_smem_bytes(1, nb, weighted && mt, 512) > smem_cap)
+    const int max_group_rows = pairhist_max_rows(nb, weighted && mt);
+    if (pairhist_launch_smem(1, nb, weighted && mt, 512) > kPairSmemCap)
         throw Error{AUSAXS_ERR_CAPACITY, "too many distance bins for the on-chip histogram"};
 
     // layout
@@ -390,8 +394,8 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
         if (group_jobs[g].empty()) continue;
         Plan::Group& G = P.group[P.n_launch++];
         G.tile = tile;
-        G.smem = pairhist_smem_bytes(group_rows[g], nb, w_launch, tile);
-        int per_sm = std::max(1, std::min((int)(233472 / (G.smem + 1024)), 2048 / tile));
+        G.smem = pairhist_launch_smem(group_rows[g], nb, w_launch, tile);
+        const int per_sm = pairhist_ctas_per_sm(G.smem, tile, pairhist_dreg(group_rows[g], nb, w_launch, tile));
         G.grid = (int)std::min<long long>((long long)C.sm_count * per_sm, std::max<long long>(1, group_tiles[g]));
         PairLaunch& L = G.launch;
         L.jobs = reinterpret_cast<const PairJob*>(base + job_off);
@@ -403,6 +407,7 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
         L.tile_counter = reinterpret_cast<unsigned long long*>(base + P.off_counter) + g;
         L.overflow = reinterpret_cast<unsigned long long*>(base + P.off_overflow);
         L.weighted = w_launch;
+        L.dreg = pairhist_dreg(group_rows[g], nb, w_launch, tile) ? 1 : 0;
         L.wscale = reinterpret_cast<const float*>(base + P.off_wscale);
         AUSAXS_CUDA(cudaMemcpyAsync(base + job_off, group_jobs[g].data(), sizeof(PairJob) * group_jobs[g].size(),
                                     cudaMemcpyHostToDevice, C.stream));  // pageable: staged on return

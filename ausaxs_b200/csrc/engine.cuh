@@ -132,6 +132,8 @@ struct Structure {
     void read_histogram(const ausaxs_hist_config& cfg, ausaxs_hist_result* out);
 };
 
+struct GridExv;
+
 struct Ctx {
     int device = 0;
     int sm_count = 148;
@@ -139,13 +141,14 @@ struct Ctx {
     bool own_stream = false;
     long long launches = 0;
     // optional per-kernel-class timing with CUDA events on the context's stream
-    // (class 0: pair histograms, 1: finalisation, 2: Debye transform)
+    // (class 0: pair histograms, 1: finalisation, 2: FP64 Debye transform, 3: tensor-core Debye transform,
+    // 4: grid excluded volume)
     bool timing = false;
     struct Timed {
         std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
         double ms = 0;
         long long count = 0;
-    } timed[4];
+    } timed[5];
     void time_begin(int cls, cudaEvent_t* ev);
     void time_end(int cls, cudaEvent_t ev);
     void time_collect();
@@ -155,6 +158,7 @@ struct Ctx {
     size_t n_stats_many = 0;
     PrepStats* stats_slots(size_t n);
     std::unique_ptr<Structure> scratch;
+    std::shared_ptr<GridExv> grid;  // molecular-grid workspace of one-shot calls (gridexv.cuh)
     DevBuf io;                     // q / I(q) / profiles of one-shot host calls
     DevBuf tc;                     // tensor-core scratch of one-shot host calls
     int last_fp64_columns = 0;     // q values the last host transform evaluated in FP64

@@ -172,11 +172,12 @@ extern "C" int ausaxs_gpu_histogram_mt_noalloc(const float* atoms, int32_t n_ato
         L.tile_counter = counters;
         L.overflow = overflow;
         L.weighted = 1;
+        L.dreg = 0;
         L.wscale = wscale;
         const size_t smem = pairhist_smem_bytes(1, nb, true, kNoAllocTile);
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const int per_sm = std::max(1, std::min((int)(233472 / (smem + 1024)), 2048 / kNoAllocTile));
+        const int per_sm = pairhist_ctas_per_sm(smem, kNoAllocTile, false);
         const int grid = (int)std::min<long long>((long long)sms * per_sm, std::max<long long>(1, tiles_total));
         L.chunk = (int)std::max<long long>(1, std::min<long long>(8, tiles_total / ((long long)grid * 8)));
         pairhist_launch(L, kNoAllocTile, grid, smem, s);

@@ -77,9 +77,31 @@ __device__ __forceinline__ void add_carry(uint32_t* lo, uint32_t* hi, int b, uin
     if (old + v < old) atomicAdd(&hi[b], 1u);
 }
 
-// dacc -> d64 for the bins of a job; callers synchronise before (atomics done) and after.
-template <int TILE>
-__device__ __forceinline__ void drain_offsets(const Onchip& S, int nb) {
+// u64 offset sums held in registers (launches with DREG): thread t owns bins t + k * TILE
+template <int TILE, bool DREG>
+struct OffsetRegs {
+    static constexpr int kSlots = DREG ? kDregBins / TILE : 1;
+    unsigned long long v[kSlots];
+};
+
+// dacc -> d64 (shared memory, or the thread's registers) for the bins of a job; callers synchronise
+// before (atomics done) and after.
+template <int TILE, bool DREG>
+__device__ __forceinline__ void drain_offsets(const Onchip& S, int nb, OffsetRegs<TILE, DREG>& R) {
+    if (DREG) {
+#pragma unroll
+        for (int k = 0; k < OffsetRegs<TILE, DREG>::kSlots; ++k) {
+            const int b = threadIdx.x + k * TILE;
+            if (b < nb) {
+                const uint32_t v = S.dacc[b];
+                if (v) {
+                    R.v[k] += v;
+                    S.dacc[b] = 0;
+                }
+            }
+        }
+        return;
+    }
     for (int b = threadIdx.x; b < nb; b += TILE) {
         uint32_t v = S.dacc[b];
         if (v) {
@@ -89,8 +111,8 @@ __device__ __forceinline__ void drain_offsets(const Onchip& S, int nb) {
     }
 }
 
-template <int TILE, bool WEIGHTED>
-__device__ __forceinline__ void flush_hist(const PairJob& J, const Onchip& S) {
+template <int TILE, bool WEIGHTED, bool DREG>
+__device__ __forceinline__ void flush_hist(const PairJob& J, const Onchip& S, OffsetRegs<TILE, DREG>& R) {
     __syncthreads();
     const int rows = J.row_hi - J.row_lo;
     const int nb = J.nbins;
@@ -103,8 +125,16 @@ __device__ __forceinline__ void flush_hist(const PairJob& J, const Onchip& S) {
             S.cnt[r * S.pad + b] = 0;
         }
     }
+    if (DREG && J.dsum) {
+#pragma unroll
+        for (int k = 0; k < OffsetRegs<TILE, DREG>::kSlots; ++k) {
+            const int b = threadIdx.x + k * TILE;
+            if (b < nb && R.v[k]) atomicAdd(&J.dsum[b], R.v[k]);
+            R.v[k] = 0;
+        }
+    }
     for (int b = threadIdx.x; b < nb; b += TILE) {
-        if (J.dsum) {
+        if (!DREG && J.dsum) {
             unsigned long long v = S.d64[b];
             if (v) {
                 atomicAdd(&J.dsum[b], v);
@@ -180,8 +210,9 @@ __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, co
     }
 }
 
-template <int TILE, bool WEIGHTED>
-__global__ void __launch_bounds__(TILE, 1024 / TILE) pairhist_kernel(PairLaunch L) {
+// DREG: the u64 offset sums live in registers (one CTA per SM; pairhist_dreg decides)
+template <int TILE, bool WEIGHTED, bool DREG>
+__global__ void __launch_bounds__(TILE, DREG ? 1 : 1024 / TILE) pairhist_kernel(PairLaunch L) {
     extern __shared__ __align__(16) unsigned char smem[];
     Onchip S;
     S.pad = L.smem_bins + 1;
@@ -191,7 +222,7 @@ __global__ void __launch_bounds__(TILE, 1024 / TILE) pairhist_kernel(PairLaunch 
     S.cnt = reinterpret_cast<uint32_t*>(smem);
     off += (static_cast<size_t>(L.smem_rows) * S.pad * 4 + 15) & ~static_cast<size_t>(15);
     S.d64 = reinterpret_cast<unsigned long long*>(smem + off);
-    off += w64;
+    if (!DREG) off += w64;
     S.dacc = reinterpret_cast<uint32_t*>(smem + off);
     off += w32;
     S.wlo = reinterpret_cast<uint32_t*>(smem + off);
@@ -209,6 +240,9 @@ __global__ void __launch_bounds__(TILE, 1024 / TILE) pairhist_kernel(PairLaunch 
     }
     __syncthreads();
 
+    OffsetRegs<TILE, DREG> R;
+#pragma unroll
+    for (int k = 0; k < OffsetRegs<TILE, DREG>::kSlots; ++k) R.v[k] = 0;
     const float wsc = WEIGHTED ? *L.wscale : 0.f;
     int cur = -1;
     long long pairs_since_flush = 0;
@@ -224,7 +258,7 @@ __global__ void __launch_bounds__(TILE, 1024 / TILE) pairhist_kernel(PairLaunch 
             const int jb = find_job(L.jobs, L.n_jobs, g);
             // u32 counts stay exact below 2^32 pairs per bin between flushes
             if (jb != cur || pairs_since_flush > (1ll << 31)) {
-                if (cur >= 0) flush_hist<TILE, WEIGHTED>(L.jobs[cur], S);
+                if (cur >= 0) flush_hist<TILE, WEIGHTED, DREG>(L.jobs[cur], S, R);
                 cur = jb;
                 pairs_since_flush = 0;
             }
@@ -266,13 +300,13 @@ __global__ void __launch_bounds__(TILE, 1024 / TILE) pairhist_kernel(PairLaunch 
                 }
                 if (J.dsum) {
                     __syncthreads();
-                    drain_offsets<TILE>(S, J.nbins);
+                    drain_offsets<TILE, DREG>(S, J.nbins, R);
                     __syncthreads();
                 }
             }
         }
     }
-    if (cur >= 0) flush_hist<TILE, WEIGHTED>(L.jobs[cur], S);
+    if (cur >= 0) flush_hist<TILE, WEIGHTED, DREG>(L.jobs[cur], S, R);
     // warp-aggregated overflow report
     for (int o = 16; o > 0; o >>= 1) overflow += __shfl_xor_sync(0xffffffffu, overflow, o);
     if ((threadIdx.x & 31) == 0 && overflow) atomicAdd(L.overflow, overflow);
@@ -280,23 +314,24 @@ __global__ void __launch_bounds__(TILE, 1024 / TILE) pairhist_kernel(PairLaunch 
 
 }  // namespace
 
+namespace {
+template <int TILE, bool WEIGHTED, bool DREG>
+void launch_one(const PairLaunch& L, int grid, size_t smem, cudaStream_t s) {
+    cudaFuncSetAttribute(pairhist_kernel<TILE, WEIGHTED, DREG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    pairhist_kernel<TILE, WEIGHTED, DREG><<<grid, TILE, smem, s>>>(L);
+}
+}  // namespace
+
 void pairhist_launch(const PairLaunch& L, int tile, int grid, size_t smem, cudaStream_t s) {
+    // register-held offset sums exist for unweighted launches only (pairhist_dreg)
     if (tile == 256) {
-        if (L.weighted) {
-            cudaFuncSetAttribute(pairhist_kernel<256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            pairhist_kernel<256, true><<<grid, 256, smem, s>>>(L);
-        } else {
-            cudaFuncSetAttribute(pairhist_kernel<256, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            pairhist_kernel<256, false><<<grid, 256, smem, s>>>(L);
-        }
+        if (L.weighted) launch_one<256, true, false>(L, grid, smem, s);
+        else if (L.dreg) launch_one<256, false, true>(L, grid, smem, s);
+        else launch_one<256, false, false>(L, grid, smem, s);
     } else {
-        if (L.weighted) {
-            cudaFuncSetAttribute(pairhist_kernel<512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            pairhist_kernel<512, true><<<grid, 512, smem, s>>>(L);
-        } else {
-            cudaFuncSetAttribute(pairhist_kernel<512, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            pairhist_kernel<512, false><<<grid, 512, smem, s>>>(L);
-        }
+        if (L.weighted) launch_one<512, true, false>(L, grid, smem, s);
+        else if (L.dreg) launch_one<512, false, true>(L, grid, smem, s);
+        else launch_one<512, false, false>(L, grid, smem, s);
     }
 }
 

@@ -54,17 +54,52 @@ struct PairLaunch {
     unsigned long long* overflow;   // pairs whose bin fell outside the job's nbins
     int32_t weighted;
     const float* wscale;            // device: 2^k with max|w_i w_j| * 2^k < 2^30 (weighted launches)
+    int32_t dreg;                   // u64 offset sums in registers instead of shared memory (pairhist_dreg)
 };
 
-// Bytes of dynamic shared memory a launch needs (layout of pairhist_kernel).
-inline size_t pairhist_smem_bytes(int rows, int bins, bool weighted, int tile) {
+// Shared-memory budget of one CTA (opt-in maximum less the static allocations) and the footprint above
+// which only one CTA fits on an SM.
+constexpr size_t kPairSmemCap = 232448 - 1024;
+constexpr size_t kPairSmemTwoPerSm = 233472 / 2 - 1024;
+// Register-held offset sums cover bins [0, kDregBins): thread t holds bins t + k * TILE.
+constexpr int kDregBins = 4096;
+
+// Bytes of dynamic shared memory a launch needs (layout of pairhist_kernel); dreg: the u64 offset sums
+// live in registers.
+inline size_t pairhist_smem_bytes(int rows, int bins, bool weighted, int tile, bool dreg = false) {
     size_t pad = (size_t)bins + 1;
     size_t row = (pad * 4 + 15) & ~(size_t)15;
     size_t b = ((size_t)rows * pad * 4 + 15) & ~(size_t)15;  // u32 counts
-    b += ((pad * 8 + 15) & ~(size_t)15) + row;               // offset sums: u64 + u32 accumulator
+    if (!dreg) b += (pad * 8 + 15) & ~(size_t)15;            // offset sums: u64
+    b += row;                                                // u32 offset accumulator
     if (weighted) b += 2 * row;                              // weight sums (lo, hi)
     b += (size_t)tile * 16;                                  // inner tile of points (16-byte aligned)
     return b + 64;
+}
+
+// Whether a launch keeps its u64 offset sums in registers: unweighted launches of at most kDregBins bins
+// whose shared-memory layout holds the CTA to one per SM anyway (the register variant is compiled for
+// one CTA per SM); the freed pad * 8 bytes let more count rows stay on chip.
+inline bool pairhist_dreg(int rows, int bins, bool weighted, int tile) {
+    return !weighted && bins <= kDregBins && pairhist_smem_bytes(rows, bins, weighted, tile) > kPairSmemTwoPerSm;
+}
+
+inline size_t pairhist_launch_smem(int rows, int bins, bool weighted, int tile) {
+    return pairhist_smem_bytes(rows, bins, weighted, tile, pairhist_dreg(rows, bins, weighted, tile));
+}
+
+// Resident CTAs per SM of a launch (register-sum launches are compiled for one).
+inline int pairhist_ctas_per_sm(size_t smem, int tile, bool dreg) {
+    if (dreg) return 1;
+    const int by_smem = (int)(233472 / (smem + 1024));
+    return by_smem < 1 ? 1 : (by_smem < 2048 / tile ? by_smem : 2048 / tile);
+}
+
+// Rows of [rows][bins] counts that fit on chip for 512-point tiles (256-point tiles need less).
+inline int pairhist_max_rows(int bins, bool weighted) {
+    int r = 1;
+    while (r < 4096 && pairhist_launch_smem(r + 1, bins, weighted, 512) <= kPairSmemCap) ++r;
+    return r;
 }
 
 void pairhist_launch(const PairLaunch& L, int tile, int grid, size_t smem, cudaStream_t s);

@@ -60,6 +60,25 @@ __global__ void census_kernel(const float4* p, int n, int ff_typed, PrepStats* s
     }
 }
 
+__device__ __forceinline__ float o2f(unsigned int o) {
+    return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
+}
+
+// max |p - c|^2 in double over the three point sets; non-negative doubles order like their bits
+__global__ void radius_kernel(const float4* a, int na, const float4* w, int nw, const float4* x, int nx, PrepStats* st) {
+    double c[3];
+    for (int k = 0; k < 3; ++k) c[k] = 0.5 * ((double)o2f(st->lo[k]) + (double)o2f(st->hi[k]));
+    double r2 = 0;
+    const int n = na + nw + nx;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 v = i < na ? a[i] : (i < na + nw ? w[i - na] : x[i - na - nw]);
+        const double dx = v.x - c[0], dy = v.y - c[1], dz = v.z - c[2];
+        r2 = fmax(r2, dx * dx + dy * dy + dz * dz);
+    }
+    for (int o = 16; o > 0; o >>= 1) r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
+    if ((threadIdx.x & 31) == 0 && r2 > 0) atomicMax(&st->r2, static_cast<unsigned long long>(__double_as_longlong(r2)));
+}
+
 __global__ void to_dense_kernel(const float4* in, float4* out, int n, const int32_t* ff_to_type) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 v = in[i];
@@ -81,6 +100,15 @@ void census_launch(const float4* p, int n, int ff_typed, PrepStats* st, int sm_c
     int blocks = (n + 255) / 256;
     if (blocks > sm_count * 2) blocks = sm_count * 2;
     census_kernel<<<blocks, 256, 0, s>>>(p, n, ff_typed, st);
+}
+
+void radius_launch(const float4* a, int na, const float4* w, int nw, const float4* x, int nx, PrepStats* st,
+                   int sm_count, cudaStream_t s) {
+    const long long n = (long long)na + nw + nx;
+    if (n <= 0) return;
+    long long blocks = (n + 255) / 256;
+    if (blocks > sm_count * 2) blocks = sm_count * 2;
+    radius_kernel<<<(int)blocks, 256, 0, s>>>(a, na, w, nw, x, nx, st);
 }
 
 void to_dense_launch(const float4* in, float4* out, int n, const int32_t* ff_to_type, int sm_count, cudaStream_t s) {

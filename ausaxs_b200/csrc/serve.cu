@@ -286,8 +286,9 @@ struct Assembly {
             all_jobs.insert(all_jobs.end(), js[0].begin(), js[0].end());
             max_rows = std::max(max_rows, rows[0]);
         }
-        smem = pairhist_smem_bytes(max_rows, nb, false, tile);
-        const int per_sm = std::max(1, std::min((int)(233472 / (smem + 1024)), 2048 / tile));
+        smem = pairhist_launch_smem(max_rows, nb, false, tile);
+        for (Work& Wk : work) Wk.L.dreg = pairhist_dreg(max_rows, nb, false, tile) ? 1 : 0;
+        const int per_sm = pairhist_ctas_per_sm(smem, tile, pairhist_dreg(max_rows, nb, false, tile));
         // device tables: jobs, zero ranges, partial pointers of the master sum
         std::vector<const unsigned long long*> ptrs[3];
         for (const Part& pt : parts) ptrs[pt.kind].push_back(part.as<unsigned long long>(pt.off));

@@ -627,8 +627,6 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clocks,
         "peaks_source": peak_kind,
     }
-    if args.atomic_peak:
-        line["roofline"].update(atomic_peak_estimate(local_rank))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, det = time_reference(m, wl, steps=1, warmup=0)
         if v is not None:
@@ -638,10 +636,6 @@ def run_ours(args, rank, world, local_rank):
     st.close()
     ctx.close()
     return line
-
-
-def atomic_peak_estimate(device):
-    return {}
 
 
 def run_reference_serving(args, world):
@@ -681,9 +675,159 @@ def run_reference_serving(args, world):
             "e2e": {"value": v, "unit": "moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+GRID_METRIC = "excluded-volume grids/s (RawGridExv dummies + grid volume of one structure)"
+GRID_UNIT = "grids/s"
+
+
+def grid_workload():
+    """The 50k-atom + 10k-water structure of the WAXS configuration; its 1 A molecular grid."""
+    from ausaxs_b200 import synth
+
+    m = synth.cfg1().molecules[0]
+    return m, "gridexv: molecular grid of the 50k-atom + 10k-water structure (1 A cells, rvol 2.15 A)"
+
+
+def grid_shape(m):
+    """Cells of the expanded grid (the same axes rule as the device code) for the traffic model."""
+    lo = np.minimum(0.0, np.minimum(m.atoms.min(0), m.waters.min(0)))
+    hi = np.maximum(0.0, np.maximum(m.atoms.max(0), m.waters.max(0)))
+    diff = hi - lo
+    scaling = 1.0 if np.any(diff < 50) else 0.25
+    e = np.maximum(0.5 * diff * scaling, 2.14 + 1.71 - 0.35 + 3.0)
+    bins = np.ceil(hi + e + 1.0) - np.floor(lo - e - 1.0)
+    return int(np.prod(bins))
+
+
+def run_gridexv(args, rank, world, local_rank):
+    import ctypes as C
+
+    import torch
+
+    from ausaxs_b200 import _capi
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device(f"cuda:{local_rank}")
+    stream = torch.cuda.Stream(local_rank)
+    ctx = _capi.Context(local_rank)
+    ctx.set_stream(stream.cuda_stream)
+    m, name = grid_workload()
+    A, W, _ = m.compact_ff()
+    cells = grid_shape(m)
+    a_d, w_d = torch.from_numpy(A).to(dev), torch.from_numpy(W).to(dev)
+    n0 = len(_capi.grid_exv(ctx, A, W)[0])
+    out = torch.zeros((n0, 4), dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+
+    def step():
+        return _capi.grid_exv_device(ctx, a_d, len(A), w_d, len(W), out, n0)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        ctx.enable_timing(True)
+        launches0 = ctx.launches
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        with ClockSampler(local_rank) as clk:
+            torch.cuda.synchronize()
+            for k in range(args.steps):
+                starts[k].record(stream)
+                n, vol = step()
+                ends[k].record(stream)
+            torch.cuda.synchronize()
+        launches = ctx.launches - launches0
+        k_ms, k_n = ctx.kernel_time(4)
+        ctx.enable_timing(False)
+    total_ms = max_over_ranks(sum(s.elapsed_time(e) for s, e in zip(starts, ends)), world)
+    value = world * args.steps / (total_ms / 1e3)
+
+    # end to end through the host C ABI: pinned records in, pinned dummies out
+    pin_a = torch.from_numpy(A).pin_memory()
+    pin_w = torch.from_numpy(W).pin_memory()
+    pin_o = torch.zeros((n0, 4), dtype=torch.float32).pin_memory()
+    L = _capi.load()
+    nn, vv = C.c_int64(0), C.c_double(0)
+
+    def e2e_step():
+        _capi.check(L.ausaxs_gpu_grid_exv(ctx.h, _capi.devptr(pin_a, C.c_float), len(A), _capi.devptr(pin_w, C.c_float),
+                                          len(W), 1, _capi.devptr(pin_o, C.c_float), n0, C.byref(nn), C.byref(vv)))
+
+    for _ in range(max(1, args.warmup // 2)):
+        e2e_step()
+    lat = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        e2e_step()
+        lat.append(time.perf_counter() - t0)
+    e2e = world * args.steps / max_over_ranks(sum(lat), world)
+    same = bool(np.array_equal(pin_o.numpy(), out.cpu().numpy())) and nn.value == n and vv.value == vol
+
+    peaks, peak_kind = load_peaks()
+    kernel_ms = k_ms / args.steps
+    # algorithmic bytes of one grid: clear the cell words, two sweeps over them (count, write), the
+    # points read by the three point kernels, the dummies written
+    alg = cells * 4 * 3 + (len(A) + len(W)) * 16 + len(A) * 16 * 2 + n * 16
+    achieved = alg / (kernel_ms / 1e3) / 1e9
+    line = {
+        "metric": GRID_METRIC, "value": value, "unit": GRID_UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 cell distances, u32 cell flags", "data": "synthetic (seeded generator)",
+        "config": {"workload": name, "atoms": m.size_atom(), "waters": m.size_water(), "cells": cells,
+                   "dummies": int(n), "volume_A3": vol, "l2": f"grid of {cells * 4 / 1e6:.0f} MB stays in L2 (no flush: "
+                   "the step is bound by launch and synchronisation latency, not DRAM)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e, "unit": GRID_UNIT, "h2d_bytes_per_step": int(A.nbytes + W.nbytes),
+                "d2h_bytes_per_step": int(n * 16 + 16), "p50_ms": 1e3 * float(np.percentile(lat, 50)),
+                "p99_ms": 1e3 * float(np.percentile(lat, 99)), "same_as_resident": same},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "grid excluded-volume kernels (class 4)", "achieved": achieved,
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "algorithmic_bytes": int(alg), "kernel_ms_per_step": kernel_ms,
+                     "kernel_intervals_per_step": k_n / args.steps,
+                     "note": "two event intervals per step (before and after the count read-back)"},
+        "clocks": clk.summary(),
+        "peaks_source": peak_kind,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = reference_grid(m)
+    ctx.close()
+    return line
+
+
+def reference_grid(m, steps: int = 1, warmup: int = 0):
+    from oracle import py as O
+
+    if not O.ref_available():
+        return {"unavailable": "reference build oracle/_ref/libausaxs_ref.so not present"}
+    O.ref(1)
+    ts = []
+    for it in range(warmup + steps):
+        t, n, vol = O.ref_grid_exv_seconds(m.atoms, m.ff_types, m.waters)
+        if it >= warmup:
+            ts.append(t)
+    v = 1.0 / statistics.median(ts)
+    return {"value": v, "unit": GRID_UNIT, "cores": 1, "kind": "reference", "dummies": n, "volume_A3": vol,
+            "sample": "the whole structure: Molecule construction, grid creation and expansion, RawGridExv sweep "
+                      "(single-threaded in the reference)"}
+
+
 def run_reference(args, rank, world):
     if args.workload == "cfg4":
         return run_reference_serving(args, world)
+    if args.workload == "gridexv":
+        m, name = grid_workload()
+        det = reference_grid(m, steps=args.steps, warmup=args.warmup)
+        if "unavailable" in det:
+            return {"impl": "reference", **det}
+        v = det["value"]
+        return {"impl": "reference", "metric": GRID_METRIC, "value": v, "unit": GRID_UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64 (reference CPU)",
+                "data": "synthetic (seeded generator)", "config": {"workload": name}, "cpu_baseline": det,
+                "e2e": {"value": v, "unit": GRID_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     wl = workload(args.workload)
     if args.workload == "cfg3":
         v, det = time_reference_batch(wl, steps=args.steps, warmup=args.warmup, target_pairs=1e9)
@@ -705,11 +849,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4"])
+    ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4", "gridexv"])
     ap.add_argument("--chains", type=int, default=64)
     ap.add_argument("--hbm-budget-gb", type=float, default=40.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--atomic-peak", action="store_true")
     ap.add_argument("--precision", type=int, default=0, choices=[0, 1])
     ap.add_argument("--tolerance", type=float, default=1e-4)
     args = ap.parse_args()
@@ -728,7 +871,8 @@ def main():
 
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    line = {"cfg3": run_batch, "cfg4": run_serving}.get(args.workload, run_ours)(args, rank, world, local_rank)
+    line = {"cfg3": run_batch, "cfg4": run_serving, "gridexv": run_gridexv}.get(args.workload, run_ours)(
+        args, rank, world, local_rank)
     if world > 1:
         import torch
 

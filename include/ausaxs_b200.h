@@ -78,7 +78,7 @@ AUSAXS_API const char* ausaxs_gpu_last_error(void);
  * every later launch of a kernel class is bracketed by CUDA events on the context's stream.
  * ausaxs_gpu_ctx_kernel_time synchronises the stream and returns the accumulated device time (ms)
  * and number of launches of one class: 0 = pair histograms, 1 = finalisation, 2 = FP64 Debye
- * epilogue, 3 = tensor-core Debye contraction.
+ * epilogue, 3 = tensor-core Debye contraction, 4 = grid excluded-volume kernels.
  * ausaxs_gpu_ctx_fp64_columns: how many q values the last ausaxs_gpu_debye call evaluated in FP64
  * (all of them with precision 1; those whose tensor-core error estimate exceeded the tolerance with
  * precision 0).
@@ -188,7 +188,10 @@ AUSAXS_API int ausaxs_gpu_profile(ausaxs_gpu_ctx* ctx, const ausaxs_hist_config*
  * ausaxs_gpu_structure_create: points as in ausaxs_gpu_histogram; host_pointers != 0 means the
  *   arrays are host memory, otherwise device memory of the context's device.  ff_typed != 0: the
  *   4th word is the int32 form-factor type (FF managers), else the float weight (MT).  One
- *   synchronisation (point census: bounding box, type counts, validation).
+ *   synchronisation (point census: bounding box, type counts, validation).  With ff_typed and
+ *   n_exv = AUSAXS_EXV_FROM_GRID the structure's dummies are those of its molecular grid, generated
+ *   on the device once (the reference's Molecule caches its grid the same way, Molecule.cpp:246-248);
+ *   three synchronisations.
  * ausaxs_gpu_structure_profile: q, Iq and profiles are device pointers.  A histogram that lost
  *   pairs to bin overflow yields NaN in Iq.
  * ausaxs_gpu_structure_histogram: host result as ausaxs_gpu_histogram (synchronises).
@@ -249,11 +252,14 @@ AUSAXS_API int ausaxs_gpu_batch_histogram(ausaxs_gpu_batch* b, int32_t index, au
  * HistogramManagerMTFFGrid::calculate_all() uses, with the reference's default grid settings (1 A
  * cells, rvol 2.15 A, exv width 1 A, AtomicOnly expansion; Grid.cpp:34-102, SphericalExpander.h:27-76),
  * and the grid volume Molecule::get_volume_grid() returns (A^3).  atoms {x,y,z,ff} and waters
- * {x,y,z,w} are host records.  Dummies are written as {x, y, z, 0} records in the reference's order
- * (x-major sweep) when capacity > 0 (AUSAXS_ERR_CAPACITY if it is too small); *n_exv is their count.
+ * {x,y,z,w} are records in host memory (host_pointers != 0) or in device memory of the context's
+ * device, as is exv_out.  Dummies are written as {x, y, z, 0} records in the reference's order
+ * (x-major sweep) when capacity > 0; *n_exv is their count, set also when the call fails with
+ * AUSAXS_ERR_CAPACITY because capacity is too small.  Synchronises the context's stream.
  */
 AUSAXS_API int ausaxs_gpu_grid_exv(ausaxs_gpu_ctx* ctx, const float* atoms, int32_t n_atoms, const float* waters,
-                                   int32_t n_waters, float* exv_out, int64_t capacity, int64_t* n_exv, double* volume);
+                                   int32_t n_waters, int32_t host_pointers, float* exv_out, int64_t capacity,
+                                   int64_t* n_exv, double* volume);
 
 /*
  * Rigid-body serving.  The reference's incremental manager, PartialHistogramManagerMT

@@ -236,6 +236,26 @@ def ref_grid_exv(xyz, ff, waters=None):
     return out[: n.value], vol.value
 
 
+def ref_grid_exv_seconds(xyz, ff, waters=None) -> tuple:
+    """Wall time of one reference RawGridExv::create on a fresh molecule (grid creation, expansion and
+    sweep; the dummies are counted, not copied out): (seconds, dummy count, volume)."""
+    import time
+
+    L = ref()
+    f = L.ref_grid_exv
+    f.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int),
+                  C.POINTER(C.c_double)]
+    a = np.ascontiguousarray(np.column_stack([np.asarray(xyz, float).reshape(-1, 3), np.asarray(ff, float)]))
+    w = np.ascontiguousarray(np.zeros((0, 3)) if waters is None else np.asarray(waters, float).reshape(-1, 3))
+    n, vol = C.c_int(), C.c_double()
+    t0 = time.perf_counter()
+    rc = f(a.ctypes.data, len(a), w.ctypes.data, len(w), None, 0, C.byref(n), C.byref(vol))
+    t = time.perf_counter() - t0
+    if rc:
+        raise RuntimeError(L.ref_last_error().decode())
+    return t, n.value, vol.value
+
+
 def ref_available() -> bool:
     return os.path.exists(ref_path())
 

@@ -83,3 +83,51 @@ def test_ffavg_z_from_grid_volume(gpu_ctx):
     _, I = h.debye_transform(q)
     Io, _ = O.debye_ff(0, o, q)
     np.testing.assert_allclose(I, Io, rtol=1e-5)
+
+
+def test_grid_dummies_device_pointers_and_capacity(gpu_ctx):
+    import torch
+
+    g = load_golden("gridexv_random1")
+    a = _records(g["atoms"], g["ff"])
+    w = _records(g["waters"], np.ones(len(g["waters"]), np.int32))
+    dev = torch.device("cuda:0")
+    a_d, w_d = torch.from_numpy(a).to(dev), torch.from_numpy(w).to(dev)
+    n_ref = len(g["dummies"])
+    small = torch.zeros((n_ref - 1, 4), dtype=torch.float32, device=dev)
+    out = torch.zeros((n_ref, 4), dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()  # the library runs on its context's stream
+    with pytest.raises(_capi.AusaxsError) as e:
+        _capi.grid_exv_device(gpu_ctx, a_d, len(a), w_d, len(w), small, n_ref - 1)
+    assert e.value.code == _capi.ERR_CAPACITY
+    n, vol = _capi.grid_exv_device(gpu_ctx, a_d, len(a), w_d, len(w), out, n_ref)
+    assert n == n_ref and vol == float(g["volume"])
+    np.testing.assert_array_equal(out.cpu().numpy()[:, :3], g["dummies"].astype(np.float32))
+    # no atoms: an empty grid, volume 0
+    n0, v0 = _capi.grid_exv_device(gpu_ctx, a_d, 0, w_d, len(w), out, n_ref)
+    assert n0 == 0 and v0 == 0.0
+
+
+def test_structure_from_grid_equals_given_dummies(gpu_ctx):
+    import torch
+
+    rng = np.random.default_rng(7)
+    xyz = rng.normal(0, 11, (2500, 3)).astype(np.float32).astype(np.float64)
+    ff = rng.choice([3, 4, 5, 7, 8, 11, 12], 2500).astype(np.int32)
+    wat = rng.normal(0, 13, (400, 3)).astype(np.float32).astype(np.float64)
+    a, w = _records(xyz, ff), _records(wat, np.ones(len(wat), np.int32))
+    d, _ = _capi.grid_exv(gpu_ctx, a, w)
+    cfg = _capi.HistConfig(_capi.MANAGER_FFGRID, 1, 0.1, 8000, 0.0)
+    params = _capi.DebyeParams(1.0, 1.0, 1.0, 0.0, 0.0, 1.0, 1, 1e-5)
+    q = torch.linspace(0.01, 0.6, 90, dtype=torch.float64, device="cuda:0")
+    out = []
+    for st in (_capi.Structure(gpu_ctx, a, w, exv_from_grid=True), _capi.Structure(gpu_ctx, a, w, exv=d)):
+        I = torch.zeros(90, dtype=torch.float64, device="cuda:0")
+        torch.cuda.synchronize()
+        st.profile_device(cfg, q, 90, params, I)
+        torch.cuda.synchronize()
+        out.append(I.cpu().numpy())
+        st.close()
+    np.testing.assert_array_equal(out[0], out[1])
+    with pytest.raises(_capi.AusaxsError):  # grid dummies need form-factor types
+        _capi.Structure(gpu_ctx, a, w, ff_typed=False, exv_from_grid=True)

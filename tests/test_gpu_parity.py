@@ -127,6 +127,32 @@ def test_ffgrid_vs_oracle(gpu_ctx):
     np.testing.assert_allclose(I, Io, rtol=1e-6, atol=1e-9 * np.abs(Io).max())
 
 
+@pytest.mark.parametrize("manager,na,nw,nx", [("ffavg", 3000, 600, 0), ("ffgrid", 2000, 400, 16500)])
+def test_wide_histograms_vs_oracle(manager, na, nw, nx, gpu_ctx):
+    """About 3,000 bins of 0.1 A with 16 type-pair rows: the u64 offset sums move to registers so every
+    row stays on chip (256-point tiles for the FFAvg case, 512-point tiles for the FFGrid case, which
+    has more than 16,384 dummies)."""
+    xyz, ff, wat, exv = _random_ff(17 + na, na, nw, nx, spread=30.0)
+    kind = {"ffavg": 0, "ffgrid": 2}[manager]
+    if kind == 2:
+        m = hist.Molecule(atoms=xyz, ff_types=ff, waters=wat, exv=exv, volume=1.0)
+        h = hist.HistogramManagerMTFFGrid(m, 0.1, 8000, gpu_ctx).calculate_all()
+    else:
+        m = hist.Molecule(atoms=xyz, ff_types=ff, waters=wat, volume=20.0 * na)
+        h = hist.HistogramManagerMTFFAvg(m, True, 0.1, 8000, gpu_ctx).calculate_all()
+    o = O.hist_ff(kind, O.pack_points(xyz, ff, True), O.pack_points(wat, np.ones(nw, np.int32), True),
+                  O.pack_points(exv, np.zeros(nx, np.int32), True) if nx else None, 0.1, 8000,
+                  0.0 if kind == 2 else 20.0 * na * 0.334 / na)
+    assert h.max_bin == len(o.d_axis) and 1500 < h.max_bin < 3300  # 16 rows fit on chip only with register sums
+    np.testing.assert_array_equal(h.get_raw_aa_counts_by_ff(), o.aa)
+    np.testing.assert_array_equal(h.get_raw_aw_counts_by_ff(), o.aw)
+    np.testing.assert_array_equal(h.get_raw_ww_counts_by_ff(), o.ww)
+    np.testing.assert_allclose(h.get_d_axis(), o.d_axis, atol=d_atol(0.1), rtol=0)
+    if kind == 2:
+        np.testing.assert_allclose(h.get_d_axis_ax(), o.d_axis_ax, atol=d_atol(0.1), rtol=0)
+        np.testing.assert_allclose(h.get_d_axis_xx(), o.d_axis_xx, atol=d_atol(0.1), rtol=0)
+
+
 def test_ffexplicit_vs_oracle(gpu_ctx):
     xyz, ff, wat, _ = _random_ff(21, 2200, 500)
     ff[::37] = 14  # some OTHER atoms (argon excluded volume)
