@@ -23,7 +23,9 @@ namespace {
 
 constexpr uint32_t kACenter = 1, kWCenter = 2, kSphere = 4;
 constexpr double kRvol = 2.15;   // settings::grid::min_exv_radius (GridSettings.cpp:14)
-constexpr int kScanBlock = 1024;  // cells per compaction block
+constexpr int kScanThreads = 1024;                     // threads of a compaction block
+constexpr int kCellsPerThread = 4;                     // consecutive cells per thread (one 16-byte load)
+constexpr int kScanBlock = kScanThreads * kCellsPerThread;  // cells per compaction block
 
 // constants::radius::get_vdw_radius(form_factor_t) (include/core/form_factor/FormFactorType.h:173-192):
 // H 1.1, C-family 1.96, N-family 1.79, O / OH 1.71, S / SH 2.06, OTHER (Ar) 1.88 A
@@ -45,39 +47,37 @@ __device__ __forceinline__ size_t cell_index(const GridShape& G, int i, int j, i
 
 __device__ __forceinline__ int to_bin(double v, double lo) { return static_cast<int>(round(v - lo)); }
 
-// A_CENTER / W_CENTER for the cells holding atom / water centres, and the atoms' bin box (reduced per
-// warp first; the loop runs warp-uniformly so every lane takes part in the reductions)
+// A_CENTER / W_CENTER for the cells holding atom / water centres, and the atoms' bin box (reduced in
+// registers, then per warp, then per block: one atomic per block and box word)
 __global__ void mark_centres(const float4* __restrict__ atoms, int na, const float4* __restrict__ waters, int nw,
                              GridShape G, uint32_t* grid, int* box) {
-    const int lane = threadIdx.x & 31;
-    const int stride = gridDim.x * blockDim.x;
-    for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < na + nw; base += stride) {
-        const int t = base + lane;
-        const bool live = t < na + nw;
-        const float4 p = !live ? make_float4(0.f, 0.f, 0.f, 0.f) : (t < na ? atoms[t] : waters[t - na]);
+    __shared__ int s_box[6];
+    if (threadIdx.x < 6) s_box[threadIdx.x] = INT_MIN;
+    __syncthreads();
+    int r[6] = {INT_MIN, INT_MIN, INT_MIN, INT_MIN, INT_MIN, INT_MIN};  // -min bin, max bin + 1
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < na + nw; t += gridDim.x * blockDim.x) {
+        const float4 p = t < na ? atoms[t] : waters[t - na];
         const int i = to_bin(p.x, G.gmin[0]), j = to_bin(p.y, G.gmin[1]), k = to_bin(p.z, G.gmin[2]);
-        if (base < na) {  // warp-uniform: this warp holds atoms
-            const bool atom = t < na;
-            const int lo[3] = {atom ? -i : INT_MIN, atom ? -j : INT_MIN, atom ? -k : INT_MIN};
-            const int hi[3] = {atom ? i + 1 : INT_MIN, atom ? j + 1 : INT_MIN, atom ? k + 1 : INT_MIN};
-            for (int d = 0; d < 3; ++d) {
-                const int l = __reduce_max_sync(0xffffffffu, lo[d]);
-                const int h = __reduce_max_sync(0xffffffffu, hi[d]);
-                if (lane == 0) {
-                    atomicMax(&box[d], l);
-                    atomicMax(&box[3 + d], h);
-                }
-            }
+        if (t < na) {
+            r[0] = max(r[0], -i), r[1] = max(r[1], -j), r[2] = max(r[2], -k);
+            r[3] = max(r[3], i + 1), r[4] = max(r[4], j + 1), r[5] = max(r[5], k + 1);
         }
-        if (!live || i < 0 || j < 0 || k < 0 || i >= G.bins[0] || j >= G.bins[1] || k >= G.bins[2]) continue;
+        if (i < 0 || j < 0 || k < 0 || i >= G.bins[0] || j >= G.bins[1] || k >= G.bins[2]) continue;
         atomicOr(&grid[cell_index(G, i, j, k)], t < na ? kACenter : kWCenter);
     }
+#pragma unroll
+    for (int d = 0; d < 6; ++d) {
+        const int v = __reduce_max_sync(0xffffffffu, r[d]);
+        if ((threadIdx.x & 31) == 0 && v != INT_MIN) atomicMax(&s_box[d], v);
+    }
+    __syncthreads();
+    if (threadIdx.x < 6 && s_box[threadIdx.x] != INT_MIN) atomicMax(&box[threadIdx.x], s_box[threadIdx.x]);
 }
 
 // One thread per (atom, x column, y column) of the atom's box bin +- ceil(r): the cells of that column
 // within r = max(r_vdw, rvol) of the atom get kSphere (distances as the reference forms them:
 // ((x - ax)^2 + (y - ay)^2) + (z - az)^2 in double).  Cells holding a water centre are masked when the
-// grid is swept (kept()), so the OR needs no read of the cell first.
+// grid is swept (kept_bits), so the OR needs no read of the cell first.
 constexpr int kSpan = 7;  // 2 * ceil(max r) + 1 cells: r <= 2.15 A for every form-factor type
 
 __global__ void mark_spheres(const float4* __restrict__ atoms, int na, GridShape G, uint32_t* grid) {
@@ -133,22 +133,43 @@ __device__ __forceinline__ void cell_of(const GridShape& G, uint32_t L, int& i, 
     j = static_cast<int>(row - static_cast<uint32_t>(i) * static_cast<uint32_t>(G.bins[1]));
 }
 
-__device__ __forceinline__ bool kept(const GridShape& G, const Window& W, const uint32_t* grid, size_t L) {
+// The kept flags of the kCellsPerThread consecutive cells starting at L (bit c: cell L + c), in sweep
+// order; cells at or beyond `cells` are not kept.  One index decomposition per thread, the following
+// cells step k with carries into j and i.
+__device__ __forceinline__ uint32_t kept_bits(const GridShape& G, const Window& W, const uint32_t* grid, uint32_t L,
+                                              uint32_t cells) {
+    if (L >= cells) return 0u;
+    uint32_t v[kCellsPerThread];
+    if (L + kCellsPerThread <= cells) {
+        const uint4 q = *reinterpret_cast<const uint4*>(grid + L);  // L is a multiple of 4: 16-byte aligned
+        v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+    } else {
+#pragma unroll
+        for (int c = 0; c < kCellsPerThread; ++c) v[c] = L + c < cells ? grid[L + c] : 0u;
+    }
     int i, j, k;
-    cell_of(G, static_cast<uint32_t>(L), i, j, k);
-    if (i < W.lo[0] || i >= W.hi[0] || j < W.lo[1] || j >= W.hi[1] || k < W.lo[2] || k >= W.hi[2]) return false;
-    const uint32_t v = grid[L];
-    return (v & kACenter) || ((v & kSphere) && !(v & kWCenter));
+    cell_of(G, L, i, j, k);
+    uint32_t bits = 0;
+#pragma unroll
+    for (int c = 0; c < kCellsPerThread; ++c) {
+        const bool in = i >= W.lo[0] && i < W.hi[0] && j >= W.lo[1] && j < W.hi[1] && k >= W.lo[2] && k < W.hi[2];
+        const bool keep = (v[c] & kACenter) || ((v[c] & kSphere) && !(v[c] & kWCenter));
+        if (in && keep && L + c < cells) bits |= 1u << c;
+        if (++k == G.bins[2]) {
+            k = 0;
+            if (++j == G.bins[1]) j = 0, ++i;
+        }
+    }
+    return bits;
 }
 
-__global__ void count_kept(GridShape G, const int* box, const uint32_t* grid, size_t cells, unsigned int* block_counts) {
+__global__ void count_kept(GridShape G, const int* box, const uint32_t* grid, uint32_t cells, unsigned int* block_counts) {
     __shared__ unsigned int s;
     if (threadIdx.x == 0) s = 0;
     __syncthreads();
     const Window W = window(G, box);
-    const size_t L = static_cast<size_t>(blockIdx.x) * kScanBlock + threadIdx.x;
-    const bool k = L < cells && kept(G, W, grid, L);
-    const unsigned int warp_n = __popc(__ballot_sync(0xffffffffu, k));
+    const uint32_t L = blockIdx.x * kScanBlock + threadIdx.x * kCellsPerThread;
+    const unsigned int warp_n = __reduce_add_sync(0xffffffffu, __popc(kept_bits(G, W, grid, L, cells)));
     if ((threadIdx.x & 31) == 0 && warp_n) atomicAdd(&s, warp_n);
     __syncthreads();
     if (threadIdx.x == 0) block_counts[blockIdx.x] = s;
@@ -192,32 +213,50 @@ __global__ void scan_counts(unsigned int* counts, int n, unsigned long long* tot
     if (threadIdx.x == 0) *total = carry;
 }
 
-__global__ void write_kept(GridShape G, const int* box, const uint32_t* grid, size_t cells, const unsigned int* offsets,
+__global__ void write_kept(GridShape G, const int* box, const uint32_t* grid, uint32_t cells, const unsigned int* offsets,
                            float4* out, long long cap) {
-    __shared__ unsigned int warp_base[kScanBlock / 32];
+    constexpr int kWarps = kScanThreads / 32;
+    __shared__ unsigned int warp_base[kWarps];
     const Window W = window(G, box);
-    const size_t L = static_cast<size_t>(blockIdx.x) * kScanBlock + threadIdx.x;
-    const bool k = L < cells && kept(G, W, grid, L);
-    const unsigned int mask = __ballot_sync(0xffffffffu, k);
-    if ((threadIdx.x & 31) == 0) warp_base[threadIdx.x >> 5] = __popc(mask);
+    const uint32_t L = blockIdx.x * kScanBlock + threadIdx.x * kCellsPerThread;
+    const uint32_t bits = kept_bits(G, W, grid, L, cells);
+    const int lane = threadIdx.x & 31;
+    // inclusive scan of the per-thread counts within the warp, then the warps' bases in order
+    const unsigned int n = __popc(bits);
+    unsigned int x = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_base[threadIdx.x >> 5] = x;
     __syncthreads();
-    if (threadIdx.x == 0) {  // exclusive prefix over the block's warps, in order
+    if (threadIdx.x == 0) {
         unsigned int acc = 0;
-        for (int w = 0; w < kScanBlock / 32; ++w) {
+        for (int w = 0; w < kWarps; ++w) {
             const unsigned int c = warp_base[w];
             warp_base[w] = acc;
             acc += c;
         }
     }
     __syncthreads();
-    if (!k) return;
-    const unsigned int lane_rank = __popc(mask & ((1u << (threadIdx.x & 31)) - 1u));
-    const long long pos = static_cast<long long>(offsets[blockIdx.x]) + warp_base[threadIdx.x >> 5] + lane_rank;
-    if (pos >= cap) return;
-    int ii, jj, kk;
-    cell_of(G, static_cast<uint32_t>(L), ii, jj, kk);
-    out[pos] = make_float4(static_cast<float>(G.gmin[0] + ii), static_cast<float>(G.gmin[1] + jj),
-                           static_cast<float>(G.gmin[2] + kk), __int_as_float(0));  // form_factor_t EXCLUDED_VOLUME
+    if (!bits) return;
+    long long pos = static_cast<long long>(offsets[blockIdx.x]) + warp_base[threadIdx.x >> 5] + (x - n);
+    int i, j, k;
+    cell_of(G, L, i, j, k);
+#pragma unroll
+    for (int c = 0; c < kCellsPerThread; ++c) {
+        if (bits & (1u << c)) {
+            if (pos < cap)
+                out[pos] = make_float4(static_cast<float>(G.gmin[0] + i), static_cast<float>(G.gmin[1] + j),
+                                       static_cast<float>(G.gmin[2] + k), __int_as_float(0));  // EXCLUDED_VOLUME
+            ++pos;
+        }
+        if (++k == G.bins[2]) {
+            k = 0;
+            if (++j == G.bins[1]) j = 0, ++i;
+        }
+    }
 }
 
 }  // namespace
@@ -245,7 +284,8 @@ void GridExv::run(Ctx& C, const float4* atoms, int na, const float4* waters, int
         G.bins[d] = (int)(gmax - G.gmin[d]);
         cells *= (size_t)G.bins[d];
     }
-    if (cells >= (size_t)1 << 32) throw Error{AUSAXS_ERR_CAPACITY, "excluded-volume grid of 2^32 cells or more"};
+    // 32-bit cell indices, with room for the last compaction block's overhang
+    if (cells >= ((size_t)1 << 32) - kScanBlock) throw Error{AUSAXS_ERR_CAPACITY, "excluded-volume grid of 2^32 cells or more"};
     G.buffer = (int)std::max(1.0, std::round(std::max(kRvol, 2.0)));  // round(max(rvol, 2)) cells
     const size_t nblocks = (cells + kScanBlock - 1) / kScanBlock;
     const size_t grid_bytes = align_up(cells * 4, 256), cnt_bytes = align_up(nblocks * 4, 256);
@@ -268,7 +308,7 @@ void GridExv::run(Ctx& C, const float4* atoms, int na, const float4* waters, int
         mark_spheres<<<blocks_s, threads, 0, s>>>(atoms, na, G, grid);
         C.check_launch("grid spheres");
     }
-    count_kept<<<(unsigned)nblocks, kScanBlock, 0, s>>>(G, box, grid, cells, counts);
+    count_kept<<<(unsigned)nblocks, kScanThreads, 0, s>>>(G, box, grid, (uint32_t)cells, counts);
     C.check_launch("grid count");
     scan_counts<<<1, 1024, 0, s>>>(counts, (int)nblocks, total);
     C.check_launch("grid scan");
@@ -287,7 +327,7 @@ void GridExv::run(Ctx& C, const float4* atoms, int na, const float4* waters, int
         throw Error{AUSAXS_ERR_CAPACITY, "exv_out holds fewer records than the grid has dummies"};
     }
     C.time_begin(4, &ev);
-    write_kept<<<(unsigned)nblocks, kScanBlock, 0, s>>>(G, box, grid, cells, counts, dst, (long long)n);
+    write_kept<<<(unsigned)nblocks, kScanThreads, 0, s>>>(G, box, grid, (uint32_t)cells, counts, dst, (long long)n);
     C.check_launch("grid write");
     C.time_end(4, ev);
 }

@@ -168,8 +168,8 @@ def cfg2(seed: int = 21, subunit: int = 8333) -> Workload:
     w = waters(seed + 1, xyz, ffs, 60000)
     m = Molecule(atoms=xyz, ff_types=ffs, weights=ff_charge(ffs), waters=w,
                  water_weights=np.full(len(w), ff_charge([FF_WATER])[0]), volume=float(len(xyz)) * 11.0)
-    return Workload("cfg2: 500k-atom icosahedral shell + 60k waters, FFAvg, 0.1 A bins, 2000 q", [m], 0.1,
-                    np.linspace(0.005, 1.0, 2000), "ffavg")
+    name = "cfg2: 500k-atom icosahedral shell" if subunit == 8333 else f"cfg2 shape: {len(xyz)}-atom icosahedral shell"
+    return Workload(name + " + 60k waters, FFAvg, 0.1 A bins, 2000 q", [m], 0.1, np.linspace(0.005, 1.0, 2000), "ffavg")
 
 
 def _molecule_args(args):

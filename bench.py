@@ -57,9 +57,13 @@ def load_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
-def workload(name: str):
+def workload(name: str, subunit: int = 0):
+    """subunit (cfg2 only): atoms per icosahedral subunit; smaller shells keep the radius and bin count
+    of the full shell (profiling cases)."""
     from ausaxs_b200 import synth
 
+    if name == "cfg2" and subunit:
+        return synth.cfg2(subunit=subunit)
     return {"cfg0": synth.cfg0, "cfg1": synth.cfg1, "cfg2": synth.cfg2, "cfg3": synth.cfg3}[name]()
 
 
@@ -507,7 +511,7 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.Stream(local_rank)
     ctx = _capi.Context(local_rank)
     ctx.set_stream(stream.cuda_stream)
-    wl = workload(args.workload)
+    wl = workload(args.workload, args.subunit)
     m = wl.molecules[0]
     grid = wl.manager == "ffgrid"
     mgr = (HistogramManagerMTFFGrid(m, wl.bin_width, wl.bin_count, ctx) if grid
@@ -853,6 +857,7 @@ def main():
     ap.add_argument("--chains", type=int, default=64)
     ap.add_argument("--hbm-budget-gb", type=float, default=40.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--subunit", type=int, default=0, help="cfg2: atoms per subunit (default 8333; smaller for profiling)")
     ap.add_argument("--precision", type=int, default=0, choices=[0, 1])
     ap.add_argument("--tolerance", type=float, default=1e-4)
     args = ap.parse_args()
