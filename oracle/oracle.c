@@ -433,25 +433,45 @@ double oracle_exv_volume(int type) {
  * Inputs: the histograms as returned by oracle_hist_ff (mb bins).  Outputs profiles[6][nq]
  * = {aa, ax, aw, xx, wx, ww} and Iq = aa - ax + aw + xx - wx + ww.
  */
-void oracle_debye_ff(int kind, const double* aa, const double* aw, const double* ww, int32_t mb, const double* d_axis,
-                     const double* d_axis_ax, const double* d_axis_xx, const double* q, int32_t nq, double cw,
-                     double cx, double crho, double dw_atomic, double dw_exv, double grid_width, double* profiles,
-                     double* Iq) {
-    double* s_aa = malloc(sizeof(double) * (size_t)NFF * NFF * nq);
-    double* s_aw = malloc(sizeof(double) * (size_t)NFF * nq);
-    double* s_ww = malloc(sizeof(double) * (size_t)nq);
+/* The sinc sums of every raw histogram row (they do not depend on cw, cx, crho or the Debye-Waller
+ * factors; the reference caches them the same way, CompositeDistanceHistogramFFAvgBase.cpp:377-397). */
+typedef struct {
+    double* s_aa; /* [15][15][nq] */
+    double* s_aw; /* [15][nq] */
+    double* s_ww; /* [nq] */
+} ff_sums;
+
+static void ff_sums_compute(int kind, const double* aa, const double* aw, const double* ww, int32_t mb,
+                            const double* d_axis, const double* d_axis_ax, const double* d_axis_xx, const double* q,
+                            int32_t nq, ff_sums* S) {
+    S->s_aa = malloc(sizeof(double) * (size_t)NFF * NFF * nq);
+    S->s_aw = malloc(sizeof(double) * (size_t)NFF * nq);
+    S->s_ww = malloc(sizeof(double) * (size_t)nq);
     const double* dax = kind == 2 ? d_axis_ax : d_axis;
     const double* dxx = kind == 2 ? d_axis_xx : d_axis;
     /* aa rows: ff1 >= 1 and ff2 >= 1 with the aa axis; [ff][exv] with the ax axis; [exv][exv] with xx */
     for (int f1 = 0; f1 < NFF; ++f1) {
         for (int f2 = 0; f2 < NFF; ++f2) {
             const double* ax = (f1 == 0 && f2 == 0) ? dxx : (f2 == 0 ? dax : d_axis);
-            oracle_sinqd(aa + (size_t)(f1 * NFF + f2) * mb, 1, mb, ax, q, nq, s_aa + (size_t)(f1 * NFF + f2) * nq);
+            oracle_sinqd(aa + (size_t)(f1 * NFF + f2) * mb, 1, mb, ax, q, nq, S->s_aa + (size_t)(f1 * NFF + f2) * nq);
         }
-        oracle_sinqd(aw + (size_t)f1 * mb, 1, mb, f1 == 0 ? dax : d_axis, q, nq, s_aw + (size_t)f1 * nq);
+        oracle_sinqd(aw + (size_t)f1 * mb, 1, mb, f1 == 0 ? dax : d_axis, q, nq, S->s_aw + (size_t)f1 * nq);
     }
-    oracle_sinqd(ww, 1, mb, d_axis, q, nq, s_ww);
+    oracle_sinqd(ww, 1, mb, d_axis, q, nq, S->s_ww);
+}
 
+static void ff_sums_free(ff_sums* S) {
+    free(S->s_aa);
+    free(S->s_aw);
+    free(S->s_ww);
+}
+
+/* The profiles and I(q) from the sinc sums and the free parameters. */
+static void ff_combine(int kind, const ff_sums* S, const double* q, int32_t nq, double cw, double cx, double crho,
+                       double dw_atomic, double dw_exv, double grid_width, double* profiles, double* Iq) {
+    const double* s_aa = S->s_aa;
+    const double* s_aw = S->s_aw;
+    const double* s_ww = S->s_ww;
     double Vg = grid_width * grid_width * grid_width;
     for (int32_t k = 0; k < nq; ++k) {
         double qq = q[k];
@@ -495,12 +515,14 @@ void oracle_debye_ff(int kind, const double* aa, const double* aw, const double*
             paw *= ba;
             pwx *= bx;
         }
-        profiles[0 * nq + k] = paa;
-        profiles[1 * nq + k] = pax;
-        profiles[2 * nq + k] = paw;
-        profiles[3 * nq + k] = pxx;
-        profiles[4 * nq + k] = pwx;
-        profiles[5 * nq + k] = pww;
+        if (profiles) {
+            profiles[0 * nq + k] = paa;
+            profiles[1 * nq + k] = pax;
+            profiles[2 * nq + k] = paw;
+            profiles[3 * nq + k] = pxx;
+            profiles[4 * nq + k] = pwx;
+            profiles[5 * nq + k] = pww;
+        }
         double I = 0;
         I += paa;
         I -= pax;
@@ -510,9 +532,16 @@ void oracle_debye_ff(int kind, const double* aa, const double* aw, const double*
         I += pww;
         Iq[k] = I;
     }
-    free(s_aa);
-    free(s_aw);
-    free(s_ww);
+}
+
+void oracle_debye_ff(int kind, const double* aa, const double* aw, const double* ww, int32_t mb, const double* d_axis,
+                     const double* d_axis_ax, const double* d_axis_xx, const double* q, int32_t nq, double cw,
+                     double cx, double crho, double dw_atomic, double dw_exv, double grid_width, double* profiles,
+                     double* Iq) {
+    ff_sums S;
+    ff_sums_compute(kind, aa, aw, ww, mb, d_axis, d_axis_ax, d_axis_xx, q, nq, &S);
+    ff_combine(kind, &S, q, nq, cw, cx, crho, dw_atomic, dw_exv, grid_width, profiles, Iq);
+    ff_sums_free(&S);
 }
 
 /* Simple composite intensity: exp(-q^2) * sum_b (aa + k aw + k^2 ww) sinc(q d)
@@ -545,7 +574,7 @@ void oracle_linear_lsq(const double* data, const double* model, const double* er
     double b = (Sxx * Sy - Sx * Sxy) / delta;
     double chi2 = 0;
     for (int32_t i = 0; i < n; ++i) {
-        double r = (model[i] - (a * data[i] + b)) / err[i];
+        double r = (model[i] - (a * data[i] + b)) * (1. / err[i]);
         chi2 += r * r;
     }
     out[0] = a;
@@ -553,6 +582,100 @@ void oracle_linear_lsq(const double* data, const double* model, const double* er
     out[2] = S / delta;
     out[3] = Sxx / delta;
     out[4] = chi2;
+}
+
+/*
+ * fitter::SmartFitter::fit() with one enabled parameter and the minimiser of a build without dlib,
+ * mini::Golden (source/core/fitter/SmartFitter.cpp:147-176, source/core/mini/Golden.cpp:26-74), for
+ * data on the model's own q axis (SmartFitter::splice then returns the model values).
+ *   kind: 0 FFAvg, 1 FFExplicit, 2 FFGrid (histograms as oracle_debye_ff), 3 Simple (aa, aw, ww
+ *         weighted counts, only param 0 applies);
+ *   param: 0 cw, 1 cx, 2 crho, 3 dw_atomic, 4 dw_exv searched in [lo, hi] to an interval of width
+ *         tol (mini::Minimizer::tol); base[5]: the other parameters' values;
+ *   out = {value (centre of the final interval), a, b, chi2 at value, function evaluations as the
+ *         reference reports them (without the final evaluation at value)}.
+ * Each evaluation is the reference's: the transform at the trial parameters, then the linear fit
+ * data ~ a * model + b with weights 1/sigma^2 and chi2 = sum ((data - (a model + b)) / sigma)^2.
+ */
+typedef struct {
+    int kind;
+    const ff_sums* S;
+    const double *aa, *aw, *ww, *d_axis, *q, *y, *sigma;
+    int32_t mb, nq;
+    int param;
+    double par[5], grid_width;
+    double *I, lsq[5];
+    int fevals;
+} fit_ctx;
+
+static double fit_chi2(fit_ctx* F, double v) {
+    F->par[F->param] = v;
+    if (F->kind == 3)
+        oracle_debye_simple(F->aa, F->aw, F->ww, F->mb, F->d_axis, F->q, F->nq, F->par[0], F->I);
+    else
+        ff_combine(F->kind, F->S, F->q, F->nq, F->par[0], F->par[1], F->par[2], F->par[3], F->par[4], F->grid_width,
+                   NULL, F->I);
+    oracle_linear_lsq(F->I, F->y, F->sigma, F->nq, F->lsq);
+    F->fevals += 1;
+    return F->lsq[4];
+}
+
+void oracle_fit(int kind, const double* aa, const double* aw, const double* ww, int32_t mb, const double* d_axis,
+                const double* d_axis_ax, const double* d_axis_xx, const double* q, const double* y,
+                const double* sigma, int32_t nq, int param, double lo, double hi, double tol, const double* base,
+                double grid_width, double* out) {
+    ff_sums S = {0, 0, 0};
+    if (kind != 3) ff_sums_compute(kind, aa, aw, ww, mb, d_axis, d_axis_ax, d_axis_xx, q, nq, &S);
+    fit_ctx F;
+    memset(&F, 0, sizeof F);
+    F.kind = kind;
+    F.S = &S;
+    F.aa = aa, F.aw = aw, F.ww = ww, F.d_axis = d_axis, F.q = q, F.y = y, F.sigma = sigma;
+    F.mb = mb, F.nq = nq, F.param = param, F.grid_width = grid_width;
+    for (int k = 0; k < 5; ++k) F.par[k] = base[k];
+    F.I = malloc(sizeof(double) * (size_t)(nq > 0 ? nq : 1));
+
+    /* Golden::search (Golden.cpp:26-67) */
+    const double phi = (1 + sqrt(5)) / 2, invphi = 1 / phi, invphi2 = invphi * invphi;
+    double a = lo, b = hi, temp = a + b;
+    a = fmin(a, b);
+    b = temp - a;
+    double diff = b - a, ilo = a, ihi = b;
+    if (!(diff < tol)) {
+        unsigned int n = (unsigned int)ceil(log(tol / diff) / log(invphi));
+        double c = a + invphi2 * diff, d = a + invphi * diff;
+        double fc = fit_chi2(&F, c), fd = fit_chi2(&F, d);
+        for (unsigned int k = 0; k < n - 1; k++) {
+            if (fc < fd) {
+                b = d;
+                d = c;
+                fd = fc;
+                diff = invphi * diff;
+                c = a + invphi2 * diff;
+                fc = fit_chi2(&F, c);
+            } else {
+                a = c;
+                c = d;
+                fc = fd;
+                diff = invphi * diff;
+                d = a + invphi * diff;
+                fd = fit_chi2(&F, d);
+            }
+        }
+        if (fc < fd) ilo = a, ihi = d;
+        else ilo = c, ihi = b;
+    }
+    /* Golden::minimize_override: the interval's centre (Limit::center = min + span / 2) and its chi2 */
+    const double value = ilo + (ihi - ilo) / 2;
+    /* the reference reports the count taken before this last evaluation: in
+       Result(p, function({p.value}), fevals) GCC reads fevals before making the call */
+    out[4] = F.fevals;
+    out[3] = fit_chi2(&F, value);
+    out[0] = value;
+    out[1] = F.lsq[0];
+    out[2] = F.lsq[1];
+    free(F.I);
+    if (kind != 3) ff_sums_free(&S);
 }
 
 /*

@@ -67,6 +67,9 @@ def lib():
         L.oracle_ff_exv_volume.argtypes = [C.c_double, C.c_double]
         L.oracle_linear_lsq.restype = None
         L.oracle_linear_lsq.argtypes = [_f64p, _f64p, _f64p, C.c_int32, _f64p]
+        L.oracle_fit.restype = None
+        L.oracle_fit.argtypes = [C.c_int, _f64p, _f64p, _f64p, C.c_int32, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p,
+                                 C.c_int32, C.c_int, C.c_double, C.c_double, C.c_double, _f64p, C.c_double, _f64p]
         _lib = L
     return _lib
 
@@ -148,6 +151,33 @@ def debye_ff(kind, h: FFHist, q, cw=1.0, cx=1.0, crho=1.0, dw_atomic=0.0, dw_exv
                       np.ascontiguousarray(h.ww), mb, np.ascontiguousarray(h.d_axis), np.ascontiguousarray(dax),
                       np.ascontiguousarray(dxx), q, nq, cw, cx, crho, dw_atomic, dw_exv, grid_width, prof, I)
     return I, prof.reshape(6, nq)
+
+
+# The reference's search limits per parameter (ICompositeDistanceHistogram.h:70,
+# ICompositeDistanceHistogramExv.cpp:8-12): cw, cx, crho, atomic and exv Debye-Waller.
+FIT_LIMITS = {0: (0.0, 10.0), 1: (0.92, 1.08), 2: (0.5, 2.0), 3: (0.0, 5.0), 4: (0.0, 5.0)}
+
+
+def fit(kind, h, q, y, sigma, param=0, lo=None, hi=None, tol=1e-4, base=(1.0, 1.0, 1.0, 0.0, 0.0), grid_width=1.0):
+    """SmartFitter::fit with the Golden minimiser over one parameter (kind 3: Simple histogram).
+    Returns (value, a, b, chi2, evaluations)."""
+    L = lib()
+    f = L.oracle_fit
+    lo = FIT_LIMITS[param][0] if lo is None else lo
+    hi = FIT_LIMITS[param][1] if hi is None else hi
+    q, y, sigma = (np.ascontiguousarray(x, np.float64) for x in (q, y, sigma))
+    out = np.zeros(5)
+    base = np.ascontiguousarray(base, np.float64)
+    if kind == 3:
+        aa, aw, ww = (np.ascontiguousarray(x) for x in (h.aa, h.aw, h.ww))
+        dax = dxx = np.ascontiguousarray(h.d_axis)
+    else:
+        aa, aw, ww = np.ascontiguousarray(h.aa.reshape(-1)), np.ascontiguousarray(h.aw.reshape(-1)), np.ascontiguousarray(h.ww)
+        dax = np.ascontiguousarray(h.d_axis_ax if h.d_axis_ax is not None else h.d_axis)
+        dxx = np.ascontiguousarray(h.d_axis_xx if h.d_axis_xx is not None else h.d_axis)
+    f(int(kind), aa, aw, ww, len(h.d_axis), np.ascontiguousarray(h.d_axis), dax, dxx, q, y, sigma, len(q), int(param),
+      float(lo), float(hi), float(tol), base, float(grid_width), out)
+    return out[0], out[1], out[2], out[3], int(out[4])
 
 
 def debye_simple(h: SimpleHist, q, cw=1.0):
@@ -288,6 +318,7 @@ def ref(threads: int = 0):
                                 C.POINTER(C.c_int), C.POINTER(C.c_double)]
         R.ref_exact_debye.argtypes = [vp, _f64p, C.c_int, _f64p]
         R.ref_linear_lsq.argtypes = [_f64p, _f64p, _f64p, C.c_int, _f64p]
+        R.ref_fit.argtypes = [vp, C.c_int, _f64p, _f64p, _f64p, C.c_int, _f64p]
         n = threads if threads > 0 else max(1, (os.cpu_count() or 2) - 1)
         _check(R, R.ref_init(n))
         _ref = R
@@ -393,6 +424,15 @@ class RefHist:
         a, x = np.zeros(na.value), np.zeros(nx.value)
         _check(ref(), ref().ref_hist_grid_axes(self.h, a, x))
         return a, x
+
+    def fit(self, param: int, q, I, sigma):
+        """fitter::SmartFitter(data, histogram).fit() with one enabled parameter (consumes the
+        histogram): (value, a, b, chi2, evaluations)."""
+        R = ref()
+        out = np.zeros(5)
+        q, I, sigma = (np.ascontiguousarray(x, np.float64) for x in (q, I, sigma))
+        _check(R, R.ref_fit(self.h, int(param), q, I, sigma, len(q), out))
+        return out[0], out[1], out[2], out[3], int(out[4])
 
     def debye(self, cw=1.0, cx=1.0, crho=1.0, dw_atomic=0.0, dw_exv=0.0):
         R = ref()

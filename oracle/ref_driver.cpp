@@ -16,6 +16,9 @@
 #include <data/atoms/Water.h>
 #include <dataset/SimpleDataset.h>
 #include <fitter/detail/LinearLeastSquares.h>
+#include <fitter/FitResult.h>
+#include <fitter/SmartFitter.h>
+#include <settings/FitSettings.h>
 #include <grid/detail/GridExcludedVolume.h>
 #include <hist/detail/SimpleExvModel.h>
 #include <hist/distribution/Distribution1D.h>
@@ -406,6 +409,35 @@ int ref_debye(void* r, double cw, double cx, double crho, double dw_atomic, doub
                 put(4, x->get_profile_wx());
             }
         }
+    });
+}
+
+// fitter::SmartFitter::fit() (source/core/fitter/SmartFitter.cpp:147-176) with one enabled parameter
+// (param 0 water scaling, 1 excluded-volume scaling, 2 solvent density, 3 atomic Debye-Waller, 4 exv
+// Debye-Waller) and the default minimiser of a build without dlib (mini::Golden), on the data
+// (q, I, sigma).  Consumes the histogram.  out = {value, a, b, chi2, fevals}.
+int ref_fit(void* r, int param, const double* q, const double* I, const double* sigma, int n, double* out) {
+    return guarded([&] {
+        using sf = settings::fit;
+        sf::fit_hydration = param == 0;
+        sf::fit_excluded_volume = param == 1;
+        sf::fit_solvent_density = param == 2;
+        sf::fit_atomic_debye_waller = param == 3;
+        sf::fit_exv_debye_waller = param == 4;
+        SimpleDataset data(std::vector<double>(q, q + n), std::vector<double>(I, I + n),
+                           std::vector<double>(sigma, sigma + n));
+        std::unique_ptr<hist::DistanceHistogram> h = std::move(static_cast<Result*>(r)->h);
+        fitter::SmartFitter f(data, std::move(h));
+        auto res = f.fit();
+        // the inner linear fit's a and b are added in front of the fitted parameter
+        const auto v = res->get_parameter_values();
+        out[0] = v.back();
+        out[1] = double(res->get_parameter("a"));
+        out[2] = double(res->get_parameter("b"));
+        out[3] = res->fval;
+        out[4] = res->fevals;
+        sf::fit_hydration = true;  // the defaults (FitSettings.cpp:12-16)
+        sf::fit_excluded_volume = sf::fit_solvent_density = sf::fit_atomic_debye_waller = sf::fit_exv_debye_waller = false;
     });
 }
 

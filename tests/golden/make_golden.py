@@ -14,7 +14,10 @@ reference's default q axis.  Cases:
                 for every manager;
 * ``random_*``: seeded random molecules (ragged sizes, all four elements, non-default bin width);
 * ``pdb_*``   : the proteins 2epe and 6lyz from the reference's own test files, read by the
-                reference's reader (united-atom form-factor types).
+                reference's reader (united-atom form-factor types);
+* ``gridexv_*``: RawGridExv dummies and grid volumes;
+* ``fit_*``   : SmartFitter::fit with the Golden minimiser over one parameter, on synthetic data on
+                the model's own q axis.
 """
 from __future__ import annotations
 
@@ -64,6 +67,34 @@ def grid_case(name, atoms, ff, waters):
     np.savez_compressed(os.path.join(HERE, name + ".npz"), atoms=atoms, ff=np.asarray(ff, np.int32), waters=waters,
                         dummies=d.astype(np.int32), volume=vol, manager="gridexv")
     print(name, "dummies", len(d), "volume", vol)
+
+
+FIT_PARAMS = ("cw", "cx", "crho", "dw_atomic", "dw_exv")
+
+
+def fit_case(name, atoms, ff, w, waters, ww, exv, volume, bin_width, manager, param, truth, seed):
+    """SmartFitter::fit (Golden over one parameter) on synthetic data: the model on its own q axis at
+    the true parameter value, scaled, offset and with 1 % Gaussian noise (a separate seeded stream)."""
+    O.ref_set_axes(bin_width, 8000, 1e-4, 0.5)
+    O.ref_set_simple_exv(False)
+    m = O.RefMolecule(atoms, w, ff, waters, ww, volume=volume)
+    m.set_manager(manager, exv_xyz=exv if manager == "ffgrid" else None)
+    h = m.calculate()
+    base = [1.0, 1.0, 1.0, 0.0, 0.0]
+    true = list(base)
+    true[param] = truth
+    q, I, _, _ = h.debye(*true)
+    r = np.random.default_rng(seed)
+    y0 = 2.5 * I + 0.002 * np.abs(I).max()
+    sigma = 0.01 * np.abs(y0) + 1e-6 * np.abs(y0).max()
+    y = y0 + sigma * r.standard_normal(len(q))
+    h.debye(*base)  # the histogram's free parameters back at their defaults before fitting
+    fit = h.fit(param, q, y, sigma)
+    out = dict(atoms=atoms, ff=ff.astype(np.int32), w=w, waters=waters, ww=ww, exv=exv, volume=volume,
+               bin_width=bin_width, manager=manager, simple_exv=False, fit_param=param, fit_truth=truth,
+               fit_base=np.array(base), q=q, y=y, sigma=sigma, fit_out=np.array(fit[:4] + (float(fit[4]),)))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, FIT_PARAMS[param], "truth", truth, "fit", fit)
 
 
 def main():
@@ -122,6 +153,25 @@ def main():
     if os.path.exists(path):
         xyz, _, f, wat, _ = O.ref_read_structure(path)
         grid_case("gridexv_2epe", xyz.astype(np.float32).astype(np.float64), f, wat.astype(np.float32).astype(np.float64))
+    # SmartFitter fits with the Golden minimiser, one parameter each (seeded noise streams of their own)
+    frng = np.random.default_rng(7)
+    xyz = frng.normal(0, 9, (400, 3))
+    f = frng.choice(elements, 400, p=[0.63, 0.17, 0.19, 0.01])
+    wt = np.array([charge[t] for t in f])
+    wat = frng.normal(0, 11, (90, 3))
+    wwt = np.full(90, 8.999659)
+    exv = np.round(frng.uniform(-9, 9, (300, 3)))
+    fit_case("fit_random_mt_cw", xyz, f, wt, wat, wwt, np.zeros((0, 3)), 18.0 * 400, 0.25, "mt", 0, 1.4, 101)
+    fit_case("fit_random_ffavg_cw", xyz, f, wt, wat, wwt, np.zeros((0, 3)), 18.0 * 400, 0.25, "ffavg", 0, 1.6, 102)
+    fit_case("fit_random_ffavg_dwa", xyz, f, wt, wat, wwt, np.zeros((0, 3)), 18.0 * 400, 0.25, "ffavg", 3, 0.7, 103)
+    fit_case("fit_random_ffgrid_cx", xyz, f, wt, wat, wwt, exv, 18.0 * 400, 0.1, "ffgrid", 1, 1.03, 104)
+    fit_case("fit_random_ffexplicit_crho", xyz, f, wt, wat, wwt, np.zeros((0, 3)), 18.0 * 400, 0.1, "ffexplicit", 2,
+             1.15, 105)
+    path = os.path.join(files, "2epe.pdb")
+    if os.path.exists(path):
+        xyz, wt, f, wat, wwt = O.ref_read_structure(path)
+        fit_case("fit_pdb_2epe_ffavg_cw", xyz, f, wt, wat, wwt, np.zeros((0, 3)), 18.0 * len(xyz), 0.25, "ffavg", 0,
+                 2.2, 106)
     # Simple excluded volume enabled (weights shifted by -rho_w V / N, SimpleExvModel.cpp:23-28)
     xyz = rng.normal(0, 6, (120, 3))
     f = rng.choice(elements, 120)

@@ -11,13 +11,21 @@ RHO_W = 0.334
 
 
 def golden_cases(prefix=""):
-    """Histogram/intensity fixtures (the grid excluded-volume fixtures are listed by grid_cases)."""
+    """Histogram/intensity fixtures (grid excluded-volume and fit fixtures are listed by grid_cases and
+    fit_cases)."""
     return sorted(n for n in (os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, prefix + "*.npz")))
-                  if not n.startswith("gridexv_"))
+                  if not n.startswith(("gridexv_", "fit_")))
 
 
 def grid_cases():
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "gridexv_*.npz")))
+
+
+def fit_cases():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "fit_*.npz")))
+
+
+FIT_KIND = {"ffavg": 0, "ffexplicit": 1, "ffgrid": 2, "mt": 3}
 
 
 def load_golden(name):

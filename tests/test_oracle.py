@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from oracle import py as O
-from tests.helpers import grid_cases, golden_cases, load_golden, oracle_for
+from tests.helpers import FIT_KIND, fit_cases, grid_cases, golden_cases, load_golden, oracle_for
 
 CASES = golden_cases()
 
@@ -117,3 +117,15 @@ def test_oracle_grid_exv_matches_reference(name):
     d, vol = O.grid_exv(g["atoms"], g["ff"], g["waters"])
     np.testing.assert_array_equal(d, g["dummies"])  # same cells, same (x-major) order
     assert vol == float(g["volume"]) == len(d)
+
+
+@pytest.mark.parametrize("name", fit_cases())
+def test_oracle_fit_matches_reference(name):
+    """SmartFitter::fit (Golden over one parameter): the same search path, so the same parameter value
+    and evaluation count; a, b and chi2 to rounding."""
+    g = load_golden(name)
+    kind = FIT_KIND[str(g["manager"])]
+    v, a, b, chi2, n = O.fit(kind, oracle_for(g), g["q"], g["y"], g["sigma"], int(g["fit_param"]), base=g["fit_base"])
+    r = g["fit_out"]
+    assert v == r[0] and n == int(r[4])
+    np.testing.assert_allclose([a, b, chi2], r[1:4], rtol=1e-10)
