@@ -35,6 +35,7 @@ EXPORTED = [
     "ausaxs_gpu_ctx_fp64_columns", "ausaxs_gpu_ctx_tc_error_estimate", "ausaxs_gpu_histogram", "ausaxs_gpu_debye", "ausaxs_gpu_profile",
     "ausaxs_gpu_structure_create", "ausaxs_gpu_structure_destroy", "ausaxs_gpu_structure_profile",
     "ausaxs_gpu_structure_histogram", "ausaxs_gpu_histogram_mt_noalloc", "ausaxs_gpu_linear_lsq", "ausaxs_gpu_grid_exv",
+    "ausaxs_gpu_fit", "ausaxs_gpu_structure_fit",
     "ausaxs_gpu_batch_create", "ausaxs_gpu_batch_destroy", "ausaxs_gpu_batch_autotune", "ausaxs_gpu_batch_candidate",
     "ausaxs_gpu_batch_profile_device", "ausaxs_gpu_batch_profile", "ausaxs_gpu_batch_histogram",
     "ausaxs_gpu_server_create", "ausaxs_gpu_server_destroy", "ausaxs_gpu_server_admit", "ausaxs_gpu_server_release",
@@ -66,6 +67,18 @@ class DebyeParams(C.Structure):
                 ("dw_exv", C.c_double), ("grid_width", C.c_double), ("precision", C.c_int32),
                 ("tolerance", C.c_double)]
 
+
+class FitOptions(C.Structure):
+    _fields_ = [("parameter", C.c_int32), ("lo", C.c_double), ("hi", C.c_double), ("tolerance", C.c_double)]
+
+
+class FitResult(C.Structure):
+    _fields_ = [("value", C.c_double), ("a", C.c_double), ("b", C.c_double), ("a_err", C.c_double),
+                ("b_err", C.c_double), ("chi2", C.c_double), ("evaluations", C.c_int32)]
+
+
+# fitted-parameter indices of ausaxs_fit_options (SmartFitter's EnabledFitParameters order)
+FIT_PARAMETERS = {"cw": 0, "cx": 1, "crho": 2, "dw_atomic": 3, "dw_exv": 4}
 
 _lib = None
 _lock = threading.Lock()
@@ -106,6 +119,10 @@ def load():
                                                    C.POINTER(DebyeParams), f64, f64]
         L.ausaxs_gpu_structure_histogram.argtypes = [vp, vp, C.POINTER(HistConfig), C.POINTER(HistResult)]
         L.ausaxs_gpu_linear_lsq.argtypes = [vp, f64, f64, f64, C.c_int32, f64]
+        L.ausaxs_gpu_fit.argtypes = [vp, C.POINTER(HistConfig), C.POINTER(HistResult), f64, f64, f64, C.c_int32,
+                                     C.POINTER(DebyeParams), C.POINTER(FitOptions), C.POINTER(FitResult), f64]
+        L.ausaxs_gpu_structure_fit.argtypes = [vp, vp, C.POINTER(HistConfig), f64, f64, f64, C.c_int32,
+                                               C.POINTER(DebyeParams), C.POINTER(FitOptions), C.POINTER(FitResult), f64]
         L.ausaxs_gpu_grid_exv.argtypes = [vp, f32, C.c_int32, f32, C.c_int32, C.c_int32, f32, C.c_int64,
                                           C.POINTER(C.c_int64), C.POINTER(C.c_double)]
         i64 = C.POINTER(C.c_int64)
@@ -286,6 +303,15 @@ class Structure:
         check(load().ausaxs_gpu_structure_profile(self.ctx.h, self.h, C.byref(cfg), devptr(q_dev), nq,
                                                   C.byref(params), devptr(I_dev),
                                                   devptr(prof_dev) if prof_dev is not None else C.cast(0, C.POINTER(C.c_double))))
+
+    def fit_device(self, cfg: HistConfig, q_dev, y_dev, sigma_dev, n: int, base: DebyeParams, options: FitOptions,
+                   I_fit_dev=None) -> FitResult:
+        """ausaxs_gpu_structure_fit: q, data, errors (and the fitted curve) are device addresses."""
+        out = FitResult()
+        check(load().ausaxs_gpu_structure_fit(self.ctx.h, self.h, C.byref(cfg), devptr(q_dev), devptr(y_dev),
+                                              devptr(sigma_dev), n, C.byref(base), C.byref(options), C.byref(out),
+                                              devptr(I_fit_dev) if I_fit_dev is not None else C.cast(0, C.POINTER(C.c_double))))
+        return out
 
     def histogram(self, cfg: HistConfig, bin_count: int):
         ff = cfg.manager != MANAGER_MT

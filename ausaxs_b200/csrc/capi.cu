@@ -1,9 +1,11 @@
 // The C ABI (include/ausaxs_b200.h): status codes and last-error text instead of exceptions, the
 // convention of the reference's own C API (include/api/api/api_helper.h:15-45).
+#include <cmath>
 #include <cstring>
 #include <string>
 
 #include "engine.cuh"
+#include "fit.cuh"
 #include "gridexv.cuh"
 #include "guard.cuh"
 #include "lsq.cuh"
@@ -75,6 +77,59 @@ ausaxs_debye_params default_params(const ausaxs_debye_params* p) {
     d.precision = 0;
     d.tolerance = 1e-5;
     return d;
+}
+// The search of a fit: interval, Golden constants and iteration count as mini::Golden forms them
+// (Golden.h:36-37, Golden.cpp:26-46); limits per parameter from ICompositeDistanceHistogram.h:70 and
+// ICompositeDistanceHistogramExv.cpp:8-12.
+FitArgs fit_search(const ausaxs_hist_config& cfg, const ausaxs_fit_options* o, const ausaxs_debye_params& base) {
+    if (!o || o->parameter < 0 || o->parameter > 4) throw Error{AUSAXS_ERR_ARGUMENT, "fit parameter must be 0..4"};
+    const bool mt = cfg.manager == AUSAXS_MANAGER_MT;
+    if (mt && o->parameter != 0) throw Error{AUSAXS_ERR_ARGUMENT, "the Simple histogram has the water scaling only"};
+    static const double limits[5][2] = {{0.0, 10.0}, {0.92, 1.08}, {0.5, 2.0}, {0.0, 5.0}, {0.0, 5.0}};
+    FitArgs F{};
+    F.model = mt ? kFitSimple : (cfg.manager == AUSAXS_MANAGER_FFEXPLICIT ? kFitExplicitExv : kFitAverageExv);
+    F.param = o->parameter;
+    F.lo = o->lo == o->hi ? limits[o->parameter][0] : o->lo;
+    F.hi = o->lo == o->hi ? limits[o->parameter][1] : o->hi;
+    if (!(std::isfinite(F.lo) && std::isfinite(F.hi))) throw Error{AUSAXS_ERR_ARGUMENT, "non-finite search interval"};
+    const double tol = o->tolerance > 0 ? o->tolerance : 1e-4;
+    const double phi = (1 + std::sqrt(5.0)) / 2;
+    F.invphi = 1 / phi;
+    F.invphi2 = F.invphi * F.invphi;
+    double a = F.lo, b = F.hi;
+    const double temp = a + b;
+    a = std::min(a, b);
+    b = temp - a;
+    const double diff = b - a;
+    F.steps = diff < tol ? -1 : (int)std::ceil(std::log(tol / diff) / std::log(F.invphi));
+    F.base[0] = base.cw;
+    F.base[1] = base.cx;
+    F.base[2] = base.crho;
+    F.base[3] = base.dw_atomic;
+    F.base[4] = base.dw_exv;
+    return F;
+}
+
+// The transform parameters of the unit profiles: cw = cx = crho = 1, no Debye-Waller factors, FP64.
+ausaxs_debye_params unit_params(const ausaxs_debye_params& base) {
+    ausaxs_debye_params u = base;
+    u.cw = u.cx = u.crho = 1.0;
+    u.dw_atomic = u.dw_exv = 0.0;
+    u.precision = 1;
+    return u;
+}
+
+void read_fit(Ctx& C, const double* out_dev, ausaxs_fit_result* out) {
+    double o[7];
+    AUSAXS_CUDA(cudaMemcpyAsync(o, out_dev, sizeof o, cudaMemcpyDeviceToHost, C.stream));
+    AUSAXS_CUDA(cudaStreamSynchronize(C.stream));
+    out->value = o[0];
+    out->a = o[1];
+    out->b = o[2];
+    out->chi2 = o[3];
+    out->evaluations = (int32_t)o[4];
+    out->a_err = o[5];
+    out->b_err = o[6];
 }
 }  // namespace
 
@@ -311,6 +366,76 @@ int ausaxs_gpu_structure_histogram(ausaxs_gpu_ctx* ctx, ausaxs_gpu_structure* s,
         check_cfg(cfg);
         s->impl.enqueue_histogram(*cfg);
         s->impl.read_histogram(*cfg, out);
+    });
+}
+
+int ausaxs_gpu_fit(ausaxs_gpu_ctx* ctx, const ausaxs_hist_config* cfg, const ausaxs_hist_result* hist, const double* q,
+                   const double* I, const double* sigma, int32_t n, const ausaxs_debye_params* base,
+                   const ausaxs_fit_options* options, ausaxs_fit_result* out, double* I_fit) {
+    return guarded([&] {
+        if (!ctx || !hist || !q || !I || !sigma || !out || n < 2) throw Error{AUSAXS_ERR_ARGUMENT, "invalid argument"};
+        check_cfg(cfg);
+        Ctx& C = ctx->impl;
+        AUSAXS_CUDA(cudaSetDevice(C.device));
+        const ausaxs_debye_params b = default_params(base);
+        FitArgs F = fit_search(*cfg, options, b);
+        const size_t vec = align_up((size_t)n * 8, 256);
+        HostDebye D = upload_host_histogram(C, *cfg, *hist, q, n, unit_params(b), 4 * vec + 256);
+        double* y = reinterpret_cast<double*>(D.extra);
+        double* sg = reinterpret_cast<double*>(D.extra + vec);
+        F.Iw = reinterpret_cast<double*>(D.extra + 2 * vec);
+        F.I_fit = I_fit ? reinterpret_cast<double*>(D.extra + 3 * vec) : nullptr;
+        F.out = reinterpret_cast<double*>(D.extra + 4 * vec);
+        AUSAXS_CUDA(cudaMemcpyAsync(y, I, (size_t)n * 8, cudaMemcpyHostToDevice, C.stream));
+        AUSAXS_CUDA(cudaMemcpyAsync(sg, sigma, (size_t)n * 8, cudaMemcpyHostToDevice, C.stream));
+        run_debye(C, D.A, D.groups, C.tc, 1);
+        F.nq = n;
+        F.q = D.A.q;
+        F.P = D.A.profiles;
+        F.y = y;
+        F.sigma = sg;
+        fit_launch(F, C.stream);
+        C.check_launch("fit");
+        if (I_fit) AUSAXS_CUDA(cudaMemcpyAsync(I_fit, F.I_fit, (size_t)n * 8, cudaMemcpyDeviceToHost, C.stream));
+        read_fit(C, F.out, out);
+    });
+}
+
+int ausaxs_gpu_structure_fit(ausaxs_gpu_ctx* ctx, ausaxs_gpu_structure* s, const ausaxs_hist_config* cfg,
+                             const double* q, const double* I, const double* sigma, int32_t n,
+                             const ausaxs_debye_params* base, const ausaxs_fit_options* options, ausaxs_fit_result* out,
+                             double* I_fit) {
+    return guarded([&] {
+        if (!ctx || !s || !q || !I || !sigma || !out || n < 2) throw Error{AUSAXS_ERR_ARGUMENT, "invalid argument"};
+        check_cfg(cfg);
+        if (s->impl.ctx != &ctx->impl) throw Error{AUSAXS_ERR_ARGUMENT, "structure belongs to another context"};
+        Ctx& C = ctx->impl;
+        AUSAXS_CUDA(cudaSetDevice(C.device));
+        const ausaxs_debye_params b = default_params(base);
+        FitArgs F = fit_search(*cfg, options, b);
+        const size_t vec = align_up((size_t)n * 8, 256);
+        C.io.ensure(8 * vec + 256);
+        char* io = C.io.as<char>();
+        double* prof = reinterpret_cast<double*>(io);
+        double* Iu = reinterpret_cast<double*>(io + 6 * vec);
+        F.Iw = reinterpret_cast<double*>(io + 7 * vec);
+        F.out = reinterpret_cast<double*>(io + 8 * vec);
+        s->impl.enqueue_histogram(*cfg);
+        DebyeArgs A = s->impl.debye_args(*cfg, q, n, unit_params(b), Iu, prof);
+        run_debye(C, A, cfg->manager == AUSAXS_MANAGER_FFGRID ? 7 : 1, s->impl.plan.tc, 1);
+        F.nq = n;
+        F.q = q;
+        F.P = prof;
+        F.y = I;
+        F.sigma = sigma;
+        F.I_fit = I_fit;
+        fit_launch(F, C.stream);
+        C.check_launch("fit");
+        unsigned long long overflow = 0;
+        AUSAXS_CUDA(cudaMemcpyAsync(&overflow, A.overflow, 8, cudaMemcpyDeviceToHost, C.stream));
+        read_fit(C, F.out, out);
+        if (overflow)
+            throw Error{AUSAXS_ERR_BIN_OVERFLOW, "pair distances beyond bin_count * bin_width; increase settings::axes::bin_count"};
     });
 }
 

@@ -668,8 +668,8 @@ void Structure::read_histogram(const ausaxs_hist_config& cfg, ausaxs_hist_result
         throw Error{AUSAXS_ERR_BIN_OVERFLOW, "pair distances beyond bin_count * bin_width; increase settings::axes::bin_count"};
 }
 
-void debye_of_host_histogram(Ctx& C, const ausaxs_hist_config& cfg, const ausaxs_hist_result& h, const double* q,
-                             int nq, const ausaxs_debye_params& p, double* Iq, double* profiles) {
+HostDebye upload_host_histogram(Ctx& C, const ausaxs_hist_config& cfg, const ausaxs_hist_result& h, const double* q,
+                                int nq, const ausaxs_debye_params& p, size_t extra_bytes) {
     const int mb = h.max_bin;
     if (mb <= 0 || !h.d_axis || !h.aa || !h.aw || !h.ww) throw Error{AUSAXS_ERR_ARGUMENT, "incomplete histogram"};
     const bool mt = cfg.manager == AUSAXS_MANAGER_MT;
@@ -719,7 +719,8 @@ void debye_of_host_histogram(Ctx& C, const ausaxs_hist_config& cfg, const ausaxs
     size_t off_rows = off_ax2 + align_up((size_t)mb * 8, 256), off_mb = off_rows + align_up(sizeof(RowDesc) * R, 256);
     size_t off_q = off_mb + 256, off_I = off_q + align_up((size_t)nq * 8, 256), off_P = off_I + align_up((size_t)nq * 8, 256);
     size_t off_E = off_P + align_up((size_t)nq * 6 * 8, 256);
-    size_t total = off_E + align_up((size_t)nq * 8, 256);
+    size_t off_X = off_E + align_up((size_t)nq * 8, 256);
+    size_t total = off_X + align_up(extra_bytes, 256);
     C.io.ensure(total);
     char* base = C.io.as<char>();
     cudaStream_t s = C.stream;
@@ -733,7 +734,9 @@ void debye_of_host_histogram(Ctx& C, const ausaxs_hist_config& cfg, const ausaxs
     int32_t mbv = mb;
     AUSAXS_CUDA(cudaMemcpyAsync(base + off_mb, &mbv, 4, cudaMemcpyHostToDevice, s));
     AUSAXS_CUDA(cudaMemcpyAsync(base + off_q, q, (size_t)nq * 8, cudaMemcpyHostToDevice, s));
-    DebyeArgs A{};
+    HostDebye out;
+    DebyeArgs& A = out.A;
+    A = DebyeArgs{};
     A.R = R;
     A.nb = mb;
     A.H = reinterpret_cast<const double*>(base + off_H);
@@ -754,20 +757,32 @@ void debye_of_host_histogram(Ctx& C, const ausaxs_hist_config& cfg, const ausaxs
     A.nq = nq;
     A.tolerance = p.tolerance > 0 ? p.tolerance : 1e-5;
     A.Iq = reinterpret_cast<double*>(base + off_I);
-    A.profiles = profiles ? reinterpret_cast<double*>(base + off_P) : nullptr;
+    A.profiles = reinterpret_cast<double*>(base + off_P);
     int32_t* cols = reinterpret_cast<int32_t*>(base + off_mb) + 1;
     AUSAXS_CUDA(cudaMemsetAsync(cols, 0, 4, s));
     A.fp64_columns = cols;
     A.tc_err_est = p.precision == 0 ? reinterpret_cast<double*>(base + off_E) : nullptr;
+    out.extra = base + off_X;
+    out.groups = grid ? 7 : 1;
+    return out;
+}
+
+void debye_of_host_histogram(Ctx& C, const ausaxs_hist_config& cfg, const ausaxs_hist_result& h, const double* q,
+                             int nq, const ausaxs_debye_params& p, double* Iq, double* profiles) {
+    HostDebye D = upload_host_histogram(C, cfg, h, q, nq, p, 0);
+    DebyeArgs& A = D.A;
+    double* prof_dev = A.profiles;
+    if (!profiles) A.profiles = nullptr;
+    cudaStream_t s = C.stream;
     C.last_tc_err.assign(p.precision == 0 ? nq : 0, INFINITY);
     if (nq > 0) {
-        run_debye(C, A, grid ? 7 : 1, C.tc, p.precision);
+        run_debye(C, A, D.groups, C.tc, p.precision);
         int32_t ncols = 0;
-        AUSAXS_CUDA(cudaMemcpyAsync(&ncols, cols, 4, cudaMemcpyDeviceToHost, s));
-        AUSAXS_CUDA(cudaMemcpyAsync(Iq, base + off_I, (size_t)nq * 8, cudaMemcpyDeviceToHost, s));
-        if (profiles) AUSAXS_CUDA(cudaMemcpyAsync(profiles, base + off_P, (size_t)nq * 6 * 8, cudaMemcpyDeviceToHost, s));
+        AUSAXS_CUDA(cudaMemcpyAsync(&ncols, A.fp64_columns, 4, cudaMemcpyDeviceToHost, s));
+        AUSAXS_CUDA(cudaMemcpyAsync(Iq, A.Iq, (size_t)nq * 8, cudaMemcpyDeviceToHost, s));
+        if (profiles) AUSAXS_CUDA(cudaMemcpyAsync(profiles, prof_dev, (size_t)nq * 6 * 8, cudaMemcpyDeviceToHost, s));
         if (p.precision == 0)
-            AUSAXS_CUDA(cudaMemcpyAsync(C.last_tc_err.data(), base + off_E, (size_t)nq * 8, cudaMemcpyDeviceToHost, s));
+            AUSAXS_CUDA(cudaMemcpyAsync(C.last_tc_err.data(), A.tc_err_est, (size_t)nq * 8, cudaMemcpyDeviceToHost, s));
         AUSAXS_CUDA(cudaStreamSynchronize(s));
         C.last_fp64_columns = p.precision == 0 ? ncols : nq;
     }

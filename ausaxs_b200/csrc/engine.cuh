@@ -183,9 +183,18 @@ void zero_ranges_launch(const ZeroRange* ranges_dev, int n, cudaStream_t s);
 // Tensor-core contraction (precision 0) followed by the FP64 epilogue, or FP64 only (precision 1).
 void run_debye(Ctx& C, DebyeArgs& A, int groups_present, DevBuf& tc, int precision);
 
-// CompositeDistanceHistogram*::debye_transform() of a histogram given in the reference's host
-// layouts (ausaxs_hist_result): compacts the rows of the form-factor types present, uploads them
-// and runs the transform (synchronises).
+// A histogram given in the reference's host layouts (ausaxs_hist_result), compacted to the rows of
+// the form-factor types present and uploaded into the context's io buffer with q: the transform's
+// arguments (I(q) and profiles [6][nq] in the io buffer too) and extra_bytes of scratch after them.
+struct HostDebye {
+    DebyeArgs A;
+    char* extra = nullptr;
+    int groups = 1;  // distance-axis groups present (run_debye)
+};
+HostDebye upload_host_histogram(Ctx& C, const ausaxs_hist_config& cfg, const ausaxs_hist_result& h, const double* q,
+                                int nq, const ausaxs_debye_params& p, size_t extra_bytes);
+
+// CompositeDistanceHistogram*::debye_transform() of a host histogram (synchronises).
 void debye_of_host_histogram(Ctx& C, const ausaxs_hist_config& cfg, const ausaxs_hist_result& h, const double* q,
                              int nq, const ausaxs_debye_params& p, double* Iq, double* profiles);
 

@@ -818,7 +818,174 @@ def reference_grid(m, steps: int = 1, warmup: int = 0):
                       "(single-threaded in the reference)"}
 
 
+FIT_METRIC = "fits/s (coordinates -> histogram -> SmartFitter fit of cw by golden-section search)"
+FIT_UNIT = "fits/s"
+# the reference's q axis (constants::axes::q_axis: 200 bins on [1e-4, 1]) below qmax = 0.5: 99 points
+FIT_Q = 1e-4 + 0.0049995 * np.arange(99)
+
+
+def fit_data(I, seed=17):
+    """Synthetic measurement from a model curve: scaled, offset, 1 % Gaussian noise."""
+    r = np.random.default_rng(seed)
+    y0 = 2.5 * I + 0.002 * np.abs(I).max()
+    sigma = 0.01 * np.abs(y0) + 1e-6 * np.abs(y0).max()
+    return y0 + sigma * r.standard_normal(len(I)), sigma
+
+
+def run_fit(args, rank, world, local_rank):
+    import ctypes as C
+
+    import torch
+
+    from ausaxs_b200 import _capi
+    from ausaxs_b200._capi import HistResult
+    from ausaxs_b200.hist import NFF, HistogramManagerMTFFAvg
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device(f"cuda:{local_rank}")
+    stream = torch.cuda.Stream(local_rank)
+    ctx = _capi.Context(local_rank)
+    ctx.set_stream(stream.cuda_stream)
+    wl = workload("cfg0")
+    m = wl.molecules[0]
+    mgr = HistogramManagerMTFFAvg(m, True, wl.bin_width, wl.bin_count, ctx)
+    cfg = mgr.config()
+    A, W, _ = mgr._inputs()
+    h = mgr.calculate_all()
+    h.apply_water_scaling_factor(1.3)
+    q = np.ascontiguousarray(FIT_Q)
+    _, I_true = h.debye_transform(q)
+    y, sigma = fit_data(I_true)
+    base = _capi.DebyeParams(1.0, 1.0, 1.0, 0.0, 0.0, 1.0, 1, 0.0)
+    opt = _capi.FitOptions(0, 0.0, 0.0, 1e-4)
+    st = _capi.Structure(ctx, A, W, None, ff_typed=True)
+    q_d, y_d, s_d = (torch.from_numpy(np.ascontiguousarray(v)).to(dev) for v in (q, y, sigma))
+    torch.cuda.synchronize()
+
+    def step():
+        return st.fit_device(cfg, q_d, y_d, s_d, len(q), base, opt)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        ctx.enable_timing(True)
+        launches0 = ctx.launches
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        with ClockSampler(local_rank) as clk:
+            torch.cuda.synchronize()
+            for k in range(args.steps):
+                starts[k].record(stream)
+                r = step()
+                ends[k].record(stream)
+            torch.cuda.synchronize()
+        launches = ctx.launches - launches0
+        k_ms, k_n = ctx.kernel_time(0)
+        ctx.enable_timing(False)
+    total_ms = max_over_ranks(sum(s_.elapsed_time(e) for s_, e in zip(starts, ends)), world)
+    value = world * args.steps / (total_ms / 1e3)
+
+    # end to end through the host C ABI: coordinates -> ausaxs_gpu_histogram -> ausaxs_gpu_fit
+    L = _capi.load()
+    nb = wl.bin_count
+    bufs = {k: np.zeros(n) for k, n in [("aa", NFF * NFF * nb), ("aw", NFF * nb), ("ww", nb), ("tot", nb), ("d_axis", nb),
+                                         ("d_axis_ax", nb), ("d_axis_xx", nb)]}
+    res = HistResult()
+    for k, v in bufs.items():
+        setattr(res, k, _capi.dptr(v))
+    out = _capi.FitResult()
+
+    def e2e_step():
+        _capi.check(L.ausaxs_gpu_histogram(ctx.h, C.byref(cfg), _capi.fptr(A), len(A), _capi.fptr(W), len(W),
+                                           _capi.fptr(None), 0, C.byref(res)))
+        _capi.check(L.ausaxs_gpu_fit(ctx.h, C.byref(cfg), C.byref(res), _capi.dptr(q), _capi.dptr(y), _capi.dptr(sigma),
+                                     len(q), C.byref(base), C.byref(opt), C.byref(out), _capi.dptr(None)))
+
+    for _ in range(max(1, args.warmup // 2)):
+        e2e_step()
+    lat = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        e2e_step()
+        lat.append(time.perf_counter() - t0)
+    e2e = world * args.steps / max_over_ranks(sum(lat), world)
+    pairs = pair_count(m, False)
+    peaks, peak_kind = load_peaks()
+    clocks = clk.summary()
+    sm_mhz = clocks.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
+    sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
+    issue_peak = sms * 4 * sm_mhz * 1e6 * 32 / INSTR_PER_PAIR
+    pair_rate = pairs / (k_ms / args.steps / 1e3)
+    line = {
+        "metric": FIT_METRIC, "value": value, "unit": FIT_UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 distances, integer bins, f64 transform and fit", "data": "synthetic (seeded generator)",
+        "config": {"workload": "fit: cfg0 structure (5k atoms + 1k waters, FFAvg, 0.25 A bins), 99 q on the "
+                               "reference's axis, cw fitted in [0, 10] to 1e-4",
+                   "fitted": {"cw": r.value, "a": r.a, "b": r.b, "chi2": r.chi2, "evaluations": r.evaluations},
+                   "same_e2e": bool(out.value == r.value and out.evaluations == r.evaluations),
+                   "l2": "inputs of 0.1 MB stay in L2 (the step is bound by launch latency)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e, "unit": FIT_UNIT, "h2d_bytes_per_step": int(A.nbytes + W.nbytes + 3 * q.nbytes),
+                "d2h_bytes_per_step": int(8 * (NFF * NFF + NFF + 3) * h.max_bin + 56),
+                "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99))},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "issue", "kernel": "pairhist_kernel", "achieved": pair_rate / 1e9, "peak": issue_peak / 1e9,
+                     "unit": "Gpair/s", "frac": pair_rate / issue_peak, "traffic": None,
+                     "note": "a 5k-atom histogram is launch-latency bound; the fit kernel itself is one CTA"},
+        "clocks": clocks,
+        "peaks_source": peak_kind,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = reference_fit(steps=1, warmup=0)
+    st.close()
+    ctx.close()
+    return line
+
+
+def reference_fit(steps: int, warmup: int):
+    """The reference: calculate_all() of the cfg0 structure, then SmartFitter::fit() of cw."""
+    from oracle import py as O
+
+    if not O.ref_available():
+        return {"unavailable": "reference build oracle/_ref/libausaxs_ref.so not present"}
+    threads = max(1, (os.cpu_count() or 2) - 1)
+    O.ref(threads)
+    wl = workload("cfg0")
+    m = wl.molecules[0]
+    O.ref_set_axes(wl.bin_width, 8000, 1e-4, 0.5)
+    O.ref_set_simple_exv(False)
+    rm = O.RefMolecule(m.atoms, m.weights, m.ff_types, m.waters, m.water_weights, volume=m.volume)
+    rm.set_manager("ffavg")
+    ts = []
+    for it in range(warmup + steps):
+        h = rm.calculate()
+        q, I, _, _ = h.debye(1.3, 1.0, 1.0, 0.0, 0.0)
+        y, sigma = fit_data(I)
+        h.debye(1.0, 1.0, 1.0, 0.0, 0.0)
+        h.fit(0, q, y, sigma)
+        if it >= warmup:
+            ts.append(h.seconds + h.fit_seconds)
+    v = 1.0 / statistics.median(ts)
+    return {"value": v, "unit": FIT_UNIT, "cores": threads, "kind": "reference",
+            "sample": "the whole workload: calculate_all() of the 5k-atom structure (thread pool) and "
+                      "SmartFitter::fit() of cw (Golden, single-threaded)"}
+
+
 def run_reference(args, rank, world):
+    if args.workload == "fit":
+        det = reference_fit(steps=args.steps, warmup=args.warmup)
+        if "unavailable" in det:
+            return {"impl": "reference", **det}
+        v = det["value"]
+        return {"impl": "reference", "metric": FIT_METRIC, "value": v, "unit": FIT_UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64 (reference CPU)",
+                "data": "synthetic (seeded generator)", "config": {"workload": "fit (cfg0 structure, cw)"},
+                "cpu_baseline": det, "e2e": {"value": v, "unit": FIT_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if args.workload == "cfg4":
         return run_reference_serving(args, world)
     if args.workload == "gridexv":
@@ -853,7 +1020,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4", "gridexv"])
+    ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4", "gridexv", "fit"])
     ap.add_argument("--chains", type=int, default=64)
     ap.add_argument("--hbm-budget-gb", type=float, default=40.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -876,7 +1043,7 @@ def main():
 
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    line = {"cfg3": run_batch, "cfg4": run_serving, "gridexv": run_gridexv}.get(args.workload, run_ours)(
+    line = {"cfg3": run_batch, "cfg4": run_serving, "gridexv": run_gridexv, "fit": run_fit}.get(args.workload, run_ours)(
         args, rank, world, local_rank)
     if world > 1:
         import torch

@@ -247,6 +247,51 @@ AUSAXS_API int ausaxs_gpu_batch_profile(ausaxs_gpu_batch* b, const double* q, in
 AUSAXS_API int ausaxs_gpu_batch_histogram(ausaxs_gpu_batch* b, int32_t index, ausaxs_hist_result* out);
 
 /*
+ * Fit of one free parameter of a composite histogram to measured data: fitter::SmartFitter::fit()
+ * (source/core/fitter/SmartFitter.cpp:147-176) with the minimiser of a build without dlib, the
+ * golden-section search mini::Golden (source/core/mini/Golden.cpp:26-74).  Every trial value is scored
+ * by the linear fit I ~ a I_model + b with weights 1/sigma^2 and its chi2
+ * (fitter::detail::LinearLeastSquares, LinearLeastSquares.cpp:26-78); the model is evaluated at the
+ * data's own q values (the reference splines its fixed q axis onto them, which is the identity when
+ * the data lie on that axis).  One FP64 transform gives the six unit profiles, the whole search then
+ * runs in one kernel.
+ *
+ * parameter: 0 water scaling cw, 1 excluded-volume scaling cx, 2 solvent density crho, 3 atomic and
+ *   4 excluded-volume Debye-Waller sigma (SmartFitter's enabled parameter; the others keep their
+ *   values from `base`, whose precision and tolerance fields are not used).  lo == hi selects the
+ *   reference's limits for the parameter (cw [0, 10], cx [0.92, 1.08], crho [0.5, 2], Debye-Waller
+ *   [0, 5]); tolerance <= 0 selects 1e-4 (mini::Minimizer::tol).  The Simple (MT) histogram has cw
+ *   only.
+ * evaluations counts the trials as the reference reports them (the final evaluation at value
+ * excluded).  I_fit (optional, n values) receives a I_model + b at the fitted value.
+ */
+typedef struct {
+    int32_t parameter;
+    double lo, hi;
+    double tolerance;
+} ausaxs_fit_options;
+
+typedef struct {
+    double value;        /* the fitted parameter: centre of the final interval */
+    double a, b;         /* I ~ a I_model + b at value */
+    double a_err, b_err; /* sqrt of the diagonal of the normal equations' inverse */
+    double chi2;
+    int32_t evaluations;
+} ausaxs_fit_result;
+
+/* A histogram previously returned by ausaxs_gpu_histogram (host buffers); q, I, sigma: host, n values. */
+AUSAXS_API int ausaxs_gpu_fit(ausaxs_gpu_ctx* ctx, const ausaxs_hist_config* cfg, const ausaxs_hist_result* hist,
+                              const double* q, const double* I, const double* sigma, int32_t n,
+                              const ausaxs_debye_params* base, const ausaxs_fit_options* options,
+                              ausaxs_fit_result* out, double* I_fit);
+/* A device-resident structure (its histogram is computed on the device); q, I, sigma and I_fit are
+ * device arrays; out is host memory (synchronises). */
+AUSAXS_API int ausaxs_gpu_structure_fit(ausaxs_gpu_ctx* ctx, ausaxs_gpu_structure* s, const ausaxs_hist_config* cfg,
+                                        const double* q, const double* I, const double* sigma, int32_t n,
+                                        const ausaxs_debye_params* base, const ausaxs_fit_options* options,
+                                        ausaxs_fit_result* out, double* I_fit);
+
+/*
  * Excluded-volume dummies of a structure's molecular grid: grid::exv::RawGridExv::create
  * (source/core/grid/exv/RawGridExv.cpp:10-59) on the expanded grid that
  * HistogramManagerMTFFGrid::calculate_all() uses, with the reference's default grid settings (1 A

@@ -429,9 +429,10 @@ class RefHist:
         """fitter::SmartFitter(data, histogram).fit() with one enabled parameter (consumes the
         histogram): (value, a, b, chi2, evaluations)."""
         R = ref()
-        out = np.zeros(5)
+        out = np.zeros(6)
         q, I, sigma = (np.ascontiguousarray(x, np.float64) for x in (q, I, sigma))
         _check(R, R.ref_fit(self.h, int(param), q, I, sigma, len(q), out))
+        self.fit_seconds = out[5]
         return out[0], out[1], out[2], out[3], int(out[4])
 
     def debye(self, cw=1.0, cx=1.0, crho=1.0, dw_atomic=0.0, dw_exv=0.0):

@@ -415,7 +415,7 @@ int ref_debye(void* r, double cw, double cx, double crho, double dw_atomic, doub
 // fitter::SmartFitter::fit() (source/core/fitter/SmartFitter.cpp:147-176) with one enabled parameter
 // (param 0 water scaling, 1 excluded-volume scaling, 2 solvent density, 3 atomic Debye-Waller, 4 exv
 // Debye-Waller) and the default minimiser of a build without dlib (mini::Golden), on the data
-// (q, I, sigma).  Consumes the histogram.  out = {value, a, b, chi2, fevals}.
+// (q, I, sigma).  Consumes the histogram.  out = {value, a, b, chi2, fevals, seconds of fit()}.
 int ref_fit(void* r, int param, const double* q, const double* I, const double* sigma, int n, double* out) {
     return guarded([&] {
         using sf = settings::fit;
@@ -428,7 +428,9 @@ int ref_fit(void* r, int param, const double* q, const double* I, const double* 
                            std::vector<double>(sigma, sigma + n));
         std::unique_ptr<hist::DistanceHistogram> h = std::move(static_cast<Result*>(r)->h);
         fitter::SmartFitter f(data, std::move(h));
+        const auto t0 = std::chrono::steady_clock::now();
         auto res = f.fit();
+        out[5] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         // the inner linear fit's a and b are added in front of the fitted parameter
         const auto v = res->get_parameter_values();
         out[0] = v.back();
