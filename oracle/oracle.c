@@ -207,6 +207,34 @@ int64_t oracle_hist_simple(const opoint* atoms, int32_t na, const opoint* waters
 }
 
 /*
+ * One job of hist::distance_calculator::SimpleCalculator<weighted_bins = true>
+ * (include/core/hist/distance_calculator/SimpleCalculator.h:94-215) with a scaling factor:
+ *   self (b == NULL): the pairs i < j of a with factor 2*scaling, plus the diagonal
+ *        scaling * sum(float(w*w)) in bin 0 (its count: that value truncated to unsigned);
+ *   cross: enqueue_calculate_cross(a, b): b outer, a inner, factor 2*scaling.
+ * Accumulates value (weights), count and dsum (bin-centre sums) into the caller's arrays (nbins
+ * each).  Returns the pairs whose bin fell outside [0, nbins).
+ */
+int64_t oracle_calc_job(const opoint* a, int32_t na, const opoint* b, int32_t nb, int32_t scaling, double bin_width,
+                        int32_t nbins, double* value, double* count, double* dsum) {
+    float inv_w = (float)(1.0 / bin_width);
+    double* cnt = calloc(nbins, 8);
+    job_out o = {cnt, dsum, count, value, 0};
+    if (b == NULL) {
+        pair_job(a, na, a, na, 1, ROW_SINGLE, 0, 2.0 * scaling, inv_w, nbins, &o);
+        double tw = 0;
+        for (int32_t i = 0; i < na; ++i) tw += a[i].v.w * a[i].v.w;
+        tw *= scaling;
+        value[0] += tw;
+        count[0] += (double)(uint32_t)tw;
+    } else {
+        pair_job(b, nb, a, na, 0, ROW_SINGLE, 0, 2.0 * scaling, inv_w, nbins, &o);
+    }
+    free(cnt);
+    return o.overflow;
+}
+
+/*
  * Form-factor managers.
  *   kind 0: HistogramManagerMTFFAvg     (source/core/hist/histogram_manager/HistogramManagerMTFFAvg.cpp:194-372)
  *   kind 1: HistogramManagerMTFFExplicit (HistogramManagerMTFFExplicit.cpp:216-437)

@@ -67,6 +67,9 @@ def lib():
         L.oracle_ff_exv_volume.argtypes = [C.c_double, C.c_double]
         L.oracle_linear_lsq.restype = None
         L.oracle_linear_lsq.argtypes = [_f64p, _f64p, _f64p, C.c_int32, _f64p]
+        L.oracle_calc_job.restype = C.c_int64
+        L.oracle_calc_job.argtypes = [_f32p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_int32,
+                                      _f64p, _f64p, _f64p]
         L.oracle_fit.restype = None
         L.oracle_fit.argtypes = [C.c_int, _f64p, _f64p, _f64p, C.c_int32, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p,
                                  C.c_int32, C.c_int, C.c_double, C.c_double, C.c_double, _f64p, C.c_double, _f64p]
@@ -319,6 +322,8 @@ def ref(threads: int = 0):
         R.ref_exact_debye.argtypes = [vp, _f64p, C.c_int, _f64p]
         R.ref_linear_lsq.argtypes = [_f64p, _f64p, _f64p, C.c_int, _f64p]
         R.ref_fit.argtypes = [vp, C.c_int, _f64p, _f64p, _f64p, C.c_int, _f64p]
+        R.ref_calculator.argtypes = [_f64p, _i32p, C.c_int, C.c_int, _i32p, _i32p, _i32p, _i32p,
+                                     C.POINTER(C.c_int), _i32p, _f64p]
         n = threads if threads > 0 else max(1, (os.cpu_count() or 2) - 1)
         _check(R, R.ref_init(n))
         _ref = R
@@ -443,6 +448,50 @@ class RefHist:
         _check(R, R.ref_debye(self.h, cw, cx, crho, dw_atomic, dw_exv, q, I, prof, C.byref(nq), C.byref(secs)))
         n = nq.value
         return q[:n].copy(), I[:n].copy(), prof[: 6 * n].reshape(6, n).copy(), secs.value
+
+
+def calculator(sets, jobs, bin_width, nbins):
+    """SimpleCalculator<true, false> restated: sets = list of [n, 4] float32 {x, y, z, w} records;
+    jobs = [(a, b or None, scaling, merge_id)].  Returns {(is_cross, merge_id): (value, count, dsum)}."""
+    L = lib()
+    out = {}
+    n_results = [0, 0]  # results of each kind so far
+    for a, b, scaling, merge in jobs:
+        kind = 0 if b is None else 1
+        if merge == -1:  # a result of its own, with id = the number of results of this kind (SimpleCalculator.h:100-109)
+            merge = n_results[kind]
+        key = (kind, merge)
+        if key not in out:
+            n_results[kind] += 1
+            out[key] = tuple(np.zeros(nbins) for _ in range(3))
+        v, c, d = out[key]
+        A = np.ascontiguousarray(sets[a], np.float32)
+        B = None if b is None else np.ascontiguousarray(sets[b], np.float32)
+        L.oracle_calc_job(A, len(A), None if B is None else B.ctypes.data, 0 if B is None else len(B), int(scaling),
+                          float(bin_width), int(nbins), v, c, d)
+    return out
+
+
+def ref_calculator(sets, jobs):
+    """The reference's SimpleCalculator<true, false> on the same jobs (bins: settings::axes)."""
+    R = ref()
+    pts = np.ascontiguousarray(np.concatenate([np.asarray(s, np.float64).reshape(-1, 4) for s in sets]))
+    off = np.zeros(len(sets) + 1, np.int32)
+    off[1:] = np.cumsum([len(s) for s in sets])
+    ja = np.array([j[0] for j in jobs], np.int32)
+    jb = np.array([-1 if j[1] is None else j[1] for j in jobs], np.int32)
+    sc = np.array([j[2] for j in jobs], np.int32)
+    mg = np.array([j[3] for j in jobs], np.int32)
+    nbins = R.ref_hist_bins_setting() if hasattr(R, "ref_hist_bins_setting") else 8000
+    n = C.c_int(0)
+    keys = np.zeros(2 * len(jobs), np.int32)
+    out = np.zeros(3 * len(jobs) * nbins)
+    _check(R, R.ref_calculator(pts, off, len(sets), len(jobs), ja, jb, sc, mg, C.byref(n), keys, out))
+    res = {}
+    for r in range(n.value):
+        v = out[3 * r * nbins:(3 * r + 3) * nbins].reshape(3, nbins)
+        res[(int(keys[2 * r]), int(keys[2 * r + 1]))] = (v[0].copy(), v[1].copy(), v[2].copy())
+    return res
 
 
 def ref_set_axes(bin_width=0.25, bin_count=8000, qmin=1e-4, qmax=0.5):

@@ -10,6 +10,8 @@
 // molecule; histogram_manager.cpp:74-190 for the managers).  Arrays are
 // row-major FP64, sizes are explicit, errors come back as a non-zero int with
 // the message in ref_last_error().
+#include <map>
+
 #include <data/Body.h>
 #include <data/Molecule.h>
 #include <data/atoms/AtomFF.h>
@@ -21,7 +23,9 @@
 #include <settings/FitSettings.h>
 #include <grid/detail/GridExcludedVolume.h>
 #include <hist/detail/SimpleExvModel.h>
+#include <hist/distance_calculator/SimpleCalculator.h>
 #include <hist/distribution/Distribution1D.h>
+#include <hist/distribution/WeightedDistribution1D.h>
 #include <hist/distribution/Distribution2D.h>
 #include <hist/distribution/Distribution3D.h>
 #include <hist/histogram_manager/HistogramManager.h>
@@ -440,6 +444,57 @@ int ref_fit(void* r, int param, const double* q, const double* I, const double* 
         out[4] = res->fevals;
         sf::fit_hydration = true;  // the defaults (FitSettings.cpp:12-16)
         sf::fit_excluded_volume = sf::fit_solvent_density = sf::fit_atomic_debye_waller = sf::fit_exv_debye_waller = false;
+    });
+}
+
+// hist::distance_calculator::SimpleCalculator<true, false> on a job list over point sets {x, y, z, w}
+// (set s is rows [set_off[s], set_off[s+1]) of pts): job k is enqueue_calculate_self(set ja[k],
+// scaling[k], merge[k]) when jb[k] < 0, else enqueue_calculate_cross(set ja[k], set jb[k], ...).
+// Results: the self merge ids, then the cross merge ids, each ascending; keys[2 r] = is_cross,
+// keys[2 r + 1] = merge id; out[(3 r + {0, 1, 2}) * bin_count + i] = value, count, bin-centre sum.
+int ref_calculator(const double* pts, const int* set_off, int n_sets, int n_jobs, const int* ja, const int* jb,
+                   const int* scaling, const int* merge, int* n_results, int* keys, double* out) {
+    return guarded([&] {
+        std::vector<hist::detail::CompactCoordinates<false>> sets;
+        sets.reserve(n_sets);
+        for (int s = 0; s < n_sets; ++s) {
+            std::vector<data::Water> w;
+            for (int i = set_off[s]; i < set_off[s + 1]; ++i) w.emplace_back(Vector3<double>(pts[4 * i], pts[4 * i + 1], pts[4 * i + 2]));
+            sets.emplace_back(w);
+            auto& d = sets.back().get_data();
+            for (int i = set_off[s]; i < set_off[s + 1]; ++i) {
+                auto& e = d[i - set_off[s]];
+                e.value.pos = Vector3<float>(pts[4 * i], pts[4 * i + 1], pts[4 * i + 2]);
+                e.value.w = static_cast<float>(pts[4 * i + 3]);
+            }
+        }
+        hist::distance_calculator::SimpleCalculator<true, false> calc;
+        for (int k = 0; k < n_jobs; ++k) {
+            if (jb[k] < 0) calc.enqueue_calculate_self(sets[ja[k]], scaling[k], merge[k]);
+            else calc.enqueue_calculate_cross(sets[ja[k]], sets[jb[k]], scaling[k], merge[k]);
+        }
+        auto res = calc.run();
+        const size_t nb = settings::axes::bin_count;
+        int r = 0;
+        auto put = [&](int cross, std::map<int, const hist::WeightedDistribution1D*>& m) {
+            for (auto& [id, dist] : m) {
+                keys[2 * r] = cross;
+                keys[2 * r + 1] = id;
+                for (size_t i = 0; i < nb && i < dist->size(); ++i) {
+                    const auto& e = dist->index(i);
+                    out[(3 * r + 0) * nb + i] = e.value;
+                    out[(3 * r + 1) * nb + i] = e.count;
+                    out[(3 * r + 2) * nb + i] = e.bin_center;
+                }
+                ++r;
+            }
+        };
+        std::map<int, const hist::WeightedDistribution1D*> self, cross;
+        for (auto& [id, d] : res.self) self[id] = &d;
+        for (auto& [id, d] : res.cross) cross[id] = &d;
+        put(0, self);
+        put(1, cross);
+        *n_results = r;
     });
 }
 

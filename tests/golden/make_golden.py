@@ -97,6 +97,21 @@ def fit_case(name, atoms, ff, w, waters, ww, exv, volume, bin_width, manager, pa
     print(name, FIT_PARAMS[param], "truth", truth, "fit", fit)
 
 
+def calc_case(name, sets, jobs, bin_width):
+    """hist::distance_calculator::SimpleCalculator<true, false> on a job list (self and cross jobs with
+    scaling factors and merge ids, as SymmetryManagerMT issues them)."""
+    O.ref_set_axes(bin_width, 8000, 1e-4, 0.5)
+    res = O.ref_calculator(sets, jobs)
+    keys = sorted(res)
+    last = max(int(np.max(np.nonzero(np.any(np.stack(res[k]) != 0, axis=0))[0])) for k in keys) + 1
+    out = dict(points=np.concatenate(sets).astype(np.float32), offsets=np.cumsum([0] + [len(x) for x in sets]),
+               jobs=np.array([(a, -1 if b is None else b, sc, m) for a, b, sc, m in jobs], np.int32),
+               bin_width=bin_width, manager="calculator", keys=np.array(keys, np.int32),
+               results=np.stack([np.stack(res[k])[:, :last] for k in keys]))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, "results", len(keys), "bins", last)
+
+
 def main():
     O.ref()
     # SimpleCube: 8 corners + centre as atoms (carbon), 8 corner waters
@@ -153,6 +168,24 @@ def main():
     if os.path.exists(path):
         xyz, _, f, wat, _ = O.ref_read_structure(path)
         grid_case("gridexv_2epe", xyz.astype(np.float32).astype(np.float64), f, wat.astype(np.float32).astype(np.float64))
+    # SimpleCalculator job lists (seeded stream of their own)
+    crng = np.random.default_rng(11)
+
+    def pts(n, spread):
+        return np.column_stack([crng.normal(0, spread, (n, 3)), crng.uniform(0.5, 8.0, n)]).astype(np.float32)
+
+    sets = [pts(n, 7.0) for n in (257, 64, 131, 33)]
+    calc_case("calc_random_merge", sets, [(0, None, 4, 0), (1, None, 1, 0), (0, 1, 3, 0), (2, 0, 1, 0), (0, 2, 2, 1),
+                                          (3, None, 60, 1), (3, 1, 7, -1), (2, None, 1, -1), (1, 2, 5, 2)], 0.25)
+    # a body with a 5-fold cyclic copy chain: self x 5, the chain's distinct pairs with their multiplicities
+    body = pts(300, 5.0)
+    ang = 2 * np.pi / 5
+    rot = lambda k: np.array([[np.cos(k * ang), -np.sin(k * ang), 0], [np.sin(k * ang), np.cos(k * ang), 0], [0, 0, 1]])
+    copies = [np.column_stack([(body[:, :3].astype(np.float64) + [14.0, 0, 0]) @ rot(k).T, body[:, 3]]).astype(np.float32)
+              for k in range(5)]
+    waters = pts(80, 16.0)
+    calc_case("calc_cyclic5", copies + [waters], [(0, None, 5, 0), (0, 1, 5, 0), (0, 2, 5, 0)] +
+              [(5, k, 1, 1) for k in range(5)] + [(5, None, 1, 2)], 0.1)
     # SmartFitter fits with the Golden minimiser, one parameter each (seeded noise streams of their own)
     frng = np.random.default_rng(7)
     xyz = frng.normal(0, 9, (400, 3))

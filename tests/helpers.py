@@ -11,10 +11,10 @@ RHO_W = 0.334
 
 
 def golden_cases(prefix=""):
-    """Histogram/intensity fixtures (grid excluded-volume and fit fixtures are listed by grid_cases and
-    fit_cases)."""
+    """Histogram/intensity fixtures (grid excluded-volume, fit and calculator fixtures are listed by
+    grid_cases, fit_cases and calc_cases)."""
     return sorted(n for n in (os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, prefix + "*.npz")))
-                  if not n.startswith(("gridexv_", "fit_")))
+                  if not n.startswith(("gridexv_", "fit_", "calc_")))
 
 
 def grid_cases():
@@ -26,6 +26,18 @@ def fit_cases():
 
 
 FIT_KIND = {"ffavg": 0, "ffexplicit": 1, "ffgrid": 2, "mt": 3}
+
+
+def calc_cases():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "calc_*.npz")))
+
+
+def calc_inputs(g):
+    """Point sets and the job list [(a, b or None, scaling, merge_id)] of a calculator fixture."""
+    off = g["offsets"]
+    sets = [g["points"][off[k]:off[k + 1]] for k in range(len(off) - 1)]
+    jobs = [(int(a), None if b < 0 else int(b), int(sc), int(m)) for a, b, sc, m in g["jobs"]]
+    return sets, jobs
 
 
 def load_golden(name):

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from oracle import py as O
-from tests.helpers import FIT_KIND, fit_cases, grid_cases, golden_cases, load_golden, oracle_for
+from tests.helpers import FIT_KIND, calc_cases, calc_inputs, fit_cases, grid_cases, golden_cases, load_golden, oracle_for
 
 CASES = golden_cases()
 
@@ -129,3 +129,17 @@ def test_oracle_fit_matches_reference(name):
     r = g["fit_out"]
     assert v == r[0] and n == int(r[4])
     np.testing.assert_allclose([a, b, chi2], r[1:4], rtol=1e-10)
+
+
+@pytest.mark.parametrize("name", calc_cases())
+def test_oracle_calculator_matches_reference(name):
+    """SimpleCalculator jobs with scaling factors and merge ids: values, counts and bin-centre sums exact."""
+    g = load_golden(name)
+    sets, jobs = calc_inputs(g)
+    o = O.calculator(sets, jobs, float(g["bin_width"]), 8000)
+    assert sorted(o) == [tuple(k) for k in g["keys"]]
+    for r, k in enumerate(g["keys"]):
+        n = g["results"].shape[2]
+        for i in range(3):
+            np.testing.assert_array_equal(o[tuple(k)][i][:n], g["results"][r][i])
+            assert not np.any(o[tuple(k)][i][n:])
