@@ -36,6 +36,9 @@ EXPORTED = [
     "ausaxs_gpu_structure_create", "ausaxs_gpu_structure_destroy", "ausaxs_gpu_structure_profile",
     "ausaxs_gpu_structure_histogram", "ausaxs_gpu_histogram_mt_noalloc", "ausaxs_gpu_linear_lsq", "ausaxs_gpu_grid_exv",
     "ausaxs_gpu_fit", "ausaxs_gpu_structure_fit",
+    "ausaxs_gpu_calculator_create", "ausaxs_gpu_calculator_destroy", "ausaxs_gpu_calculator_enqueue_self",
+    "ausaxs_gpu_calculator_enqueue_cross", "ausaxs_gpu_calculator_run", "ausaxs_gpu_calculator_result_ids",
+    "ausaxs_gpu_calculator_result",
     "ausaxs_gpu_batch_create", "ausaxs_gpu_batch_destroy", "ausaxs_gpu_batch_autotune", "ausaxs_gpu_batch_candidate",
     "ausaxs_gpu_batch_profile_device", "ausaxs_gpu_batch_profile", "ausaxs_gpu_batch_histogram",
     "ausaxs_gpu_server_create", "ausaxs_gpu_server_destroy", "ausaxs_gpu_server_admit", "ausaxs_gpu_server_release",
@@ -123,6 +126,14 @@ def load():
                                      C.POINTER(DebyeParams), C.POINTER(FitOptions), C.POINTER(FitResult), f64]
         L.ausaxs_gpu_structure_fit.argtypes = [vp, vp, C.POINTER(HistConfig), f64, f64, f64, C.c_int32,
                                                C.POINTER(DebyeParams), C.POINTER(FitOptions), C.POINTER(FitResult), f64]
+        i32p = C.POINTER(C.c_int32)
+        L.ausaxs_gpu_calculator_create.argtypes = [vp, C.c_double, C.c_int32, C.POINTER(vp)]
+        L.ausaxs_gpu_calculator_destroy.argtypes = [vp]
+        L.ausaxs_gpu_calculator_enqueue_self.argtypes = [vp, f32, C.c_int32, C.c_int32, C.c_int32, i32p]
+        L.ausaxs_gpu_calculator_enqueue_cross.argtypes = [vp, f32, C.c_int32, f32, C.c_int32, C.c_int32, C.c_int32, i32p]
+        L.ausaxs_gpu_calculator_run.argtypes = [vp, i32p, i32p]
+        L.ausaxs_gpu_calculator_result_ids.argtypes = [vp, C.c_int32, i32p, C.c_int32, i32p]
+        L.ausaxs_gpu_calculator_result.argtypes = [vp, C.c_int32, C.c_int32, f64, f64, f64]
         L.ausaxs_gpu_grid_exv.argtypes = [vp, f32, C.c_int32, f32, C.c_int32, C.c_int32, f32, C.c_int64,
                                           C.POINTER(C.c_int64), C.POINTER(C.c_double)]
         i64 = C.POINTER(C.c_int64)
@@ -264,6 +275,66 @@ def grid_exv_device(ctx: "Context", atoms_dev, n_atoms: int, waters_dev, n_water
     check(load().ausaxs_gpu_grid_exv(ctx.h, devptr(atoms_dev, C.c_float), n_atoms, devptr(waters_dev, C.c_float),
                                      n_waters, 0, devptr(out_dev, C.c_float), capacity, C.byref(n), C.byref(vol)))
     return n.value, vol.value
+
+
+class Calculator:
+    """hist::distance_calculator::SimpleCalculator<true, vbw> on the device (ausaxs_gpu_calculator_*):
+    enqueue_calculate_self / enqueue_calculate_cross with scaling factors and merge ids, then run()
+    -> {"self": {id: (value, count, distance_sum)}, "cross": {...}}, each bin_count long."""
+
+    def __init__(self, ctx: Context, bin_width: float = 0.25, bin_count: int = 8000):
+        self.ctx = ctx
+        self.bin_count = bin_count
+        self._keep = []  # the arrays must stay valid until run()
+        h = C.c_void_p()
+        check(load().ausaxs_gpu_calculator_create(ctx.h, float(bin_width), int(bin_count), C.byref(h)))
+        self.h = h
+
+    def _pts(self, p):
+        a = np.ascontiguousarray(p, np.float32).reshape(-1, 4)
+        self._keep.append(a)
+        return a
+
+    def enqueue_calculate_self(self, points, scaling: int = 1, merge_id: int = -1) -> int:
+        a = self._pts(points)
+        r = C.c_int32(0)
+        check(load().ausaxs_gpu_calculator_enqueue_self(self.h, fptr(a), len(a), int(scaling), int(merge_id), C.byref(r)))
+        return r.value
+
+    def enqueue_calculate_cross(self, points_1, points_2, scaling: int = 1, merge_id: int = -1) -> int:
+        a, b = self._pts(points_1), self._pts(points_2)
+        r = C.c_int32(0)
+        check(load().ausaxs_gpu_calculator_enqueue_cross(self.h, fptr(a), len(a), fptr(b), len(b), int(scaling),
+                                                        int(merge_id), C.byref(r)))
+        return r.value
+
+    def run(self) -> dict:
+        L = load()
+        ns, nc = C.c_int32(0), C.c_int32(0)
+        check(L.ausaxs_gpu_calculator_run(self.h, C.byref(ns), C.byref(nc)))
+        self._keep = []
+        out = {"self": {}, "cross": {}}
+        for cross, key, n in ((0, "self", ns.value), (1, "cross", nc.value)):
+            ids = np.zeros(max(1, n), np.int32)
+            m = C.c_int32(0)
+            check(L.ausaxs_gpu_calculator_result_ids(self.h, cross, ids.ctypes.data_as(C.POINTER(C.c_int32)), n,
+                                                     C.byref(m)))
+            for i in ids[:m.value]:
+                v, c, d = (np.zeros(self.bin_count) for _ in range(3))
+                check(L.ausaxs_gpu_calculator_result(self.h, cross, int(i), dptr(v), dptr(c), dptr(d)))
+                out[key][int(i)] = (v, c, d)
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().ausaxs_gpu_calculator_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def default_context(device: int = 0) -> Context:

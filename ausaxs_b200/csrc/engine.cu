@@ -214,6 +214,7 @@ void append_pair_jobs(const Plan& P, int tile, bool by_class, std::vector<PairJo
             pj.dsum = r0 == 0 ? j.dsum : nullptr;
             pj.wsum = r0 == 0 ? j.wsum : nullptr;
             pj.wscale = 0;  // read from device memory by weighted launches
+            pj.mult = j.mult;
             pj.a_base = j.a_base;
             pj.b_base = j.b_base;
             pj.tail_end = j.tail_end >= 0 ? j.tail_end : j.nbp;

@@ -59,6 +59,7 @@ struct JobSpec {
     long long* wsum;             // [nb] or null
     // scalar-tail geometry (PairJob): -1 = a plain job (tail_end = nbp, tail_from_outer = self)
     int a_base = 0, b_base = 0, tail_end = -1, tail_from_outer = -1;
+    int mult = 1;  // multiplicity of every pair (PairJob::mult)
 };
 
 // Launch plan of one structure under one histogram configuration: job table, accumulator and

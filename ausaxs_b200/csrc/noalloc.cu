@@ -136,6 +136,7 @@ extern "C" int ausaxs_gpu_histogram_mt_noalloc(const float* atoms, int32_t n_ato
         J.nb = sp.nbp;
         J.self = sp.self;
         J.row_mode = kRowSingle;
+        J.mult = 1;
         J.types = 0;
         J.row_lo = 0;
         J.row_hi = 1;

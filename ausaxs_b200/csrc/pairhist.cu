@@ -121,7 +121,7 @@ __device__ __forceinline__ void flush_hist(const PairJob& J, const Onchip& S, Of
         int r = idx / nb, b = idx - r * nb;
         uint32_t v = S.cnt[r * S.pad + b];
         if (v) {
-            atomicAdd(&J.counts[static_cast<size_t>(r) * nb + b], static_cast<unsigned long long>(v));
+            atomicAdd(&J.counts[static_cast<size_t>(r) * nb + b], static_cast<unsigned long long>(v) * J.mult);
             S.cnt[r * S.pad + b] = 0;
         }
     }
@@ -129,7 +129,7 @@ __device__ __forceinline__ void flush_hist(const PairJob& J, const Onchip& S, Of
 #pragma unroll
         for (int k = 0; k < OffsetRegs<TILE, DREG>::kSlots; ++k) {
             const int b = threadIdx.x + k * TILE;
-            if (b < nb && R.v[k]) atomicAdd(&J.dsum[b], R.v[k]);
+            if (b < nb && R.v[k]) atomicAdd(&J.dsum[b], R.v[k] * J.mult);
             R.v[k] = 0;
         }
     }
@@ -137,14 +137,14 @@ __device__ __forceinline__ void flush_hist(const PairJob& J, const Onchip& S, Of
         if (!DREG && J.dsum) {
             unsigned long long v = S.d64[b];
             if (v) {
-                atomicAdd(&J.dsum[b], v);
+                atomicAdd(&J.dsum[b], v * J.mult);
                 S.d64[b] = 0;
             }
         }
         if (WEIGHTED && J.wsum) {
             unsigned long long v = (static_cast<unsigned long long>(S.whi[b]) << 32) | S.wlo[b];
             if (v) {
-                atomicAdd(reinterpret_cast<unsigned long long*>(&J.wsum[b]), v);
+                atomicAdd(reinterpret_cast<unsigned long long*>(&J.wsum[b]), v * J.mult);
                 S.wlo[b] = S.whi[b] = 0;
             }
         }

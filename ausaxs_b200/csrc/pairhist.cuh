@@ -41,6 +41,9 @@ struct PairJob {
     // b_base + j of that set.  A plain job: a_base = b_base = 0, tail_end = nb, tail_from_outer =
     // self.  A partial job (one body pair of a multi-body structure) keeps the full structure's rows.
     int32_t a_base, b_base, tail_end, tail_from_outer;
+    // Multiplicity of every pair of the job (>= 1): its count, offset and weight contributions are
+    // added mult times, as SimpleCalculator's scaling factor does (SimpleCalculator.h:291-330).
+    int32_t mult;
 };
 
 struct PairLaunch {

@@ -292,6 +292,41 @@ AUSAXS_API int ausaxs_gpu_structure_fit(ausaxs_gpu_ctx* ctx, ausaxs_gpu_structur
                                         ausaxs_fit_result* out, double* I_fit);
 
 /*
+ * hist::distance_calculator::SimpleCalculator<weighted_bins = true> (include/core/hist/
+ * distance_calculator/SimpleCalculator.h:37-92) on the device: the distance calculator that
+ * HistogramManagerMT, SymmetryManagerMT and PartialSymmetryManagerMT issue their work to.
+ *   enqueue_self(points, n, scaling, merge_id): the pairs i < j of one weighted point set
+ *     ({x, y, z, w} records, host memory), each with factor 2 * scaling, plus the diagonal
+ *     scaling * sum(w*w) in bin 0;
+ *   enqueue_cross(points_1, n_1, points_2, n_2, scaling, merge_id): every pair of the two sets, factor
+ *     2 * scaling (points_2 outer, points_1 inner, as the reference loops);
+ *   merge_id: jobs with the same id accumulate into one result (self and cross ids are separate);
+ *     -1 makes a result of its own whose id is its index; *result_index is the reference's return
+ *     value (the result's position among those of its kind).
+ * The arrays must stay valid and unchanged until run(), as in the reference; a set passed several
+ * times (same pointer and size) is copied once.  run() executes every job in shared persistent
+ * launches (synchronises) and clears the jobs; the results of the last run stay available:
+ *   result_ids lists the merge ids of one kind (ascending);
+ *   result(cross, merge_id, ...) gives, for each of the bin_count bins, the WeightedDistribution1D
+ *     entry: value (weighted count), count and the sum of the pair distances (bin-centre sum).
+ */
+typedef struct ausaxs_gpu_calculator ausaxs_gpu_calculator;
+
+AUSAXS_API int ausaxs_gpu_calculator_create(ausaxs_gpu_ctx* ctx, double bin_width, int32_t bin_count,
+                                            ausaxs_gpu_calculator** out);
+AUSAXS_API int ausaxs_gpu_calculator_destroy(ausaxs_gpu_calculator* c);
+AUSAXS_API int ausaxs_gpu_calculator_enqueue_self(ausaxs_gpu_calculator* c, const float* points, int32_t n,
+                                                  int32_t scaling, int32_t merge_id, int32_t* result_index);
+AUSAXS_API int ausaxs_gpu_calculator_enqueue_cross(ausaxs_gpu_calculator* c, const float* points_1, int32_t n_1,
+                                                   const float* points_2, int32_t n_2, int32_t scaling,
+                                                   int32_t merge_id, int32_t* result_index);
+AUSAXS_API int ausaxs_gpu_calculator_run(ausaxs_gpu_calculator* c, int32_t* n_self, int32_t* n_cross);
+AUSAXS_API int ausaxs_gpu_calculator_result_ids(ausaxs_gpu_calculator* c, int32_t cross, int32_t* ids,
+                                                int32_t capacity, int32_t* n);
+AUSAXS_API int ausaxs_gpu_calculator_result(ausaxs_gpu_calculator* c, int32_t cross, int32_t merge_id, double* value,
+                                            double* count, double* distance_sum);
+
+/*
  * Excluded-volume dummies of a structure's molecular grid: grid::exv::RawGridExv::create
  * (source/core/grid/exv/RawGridExv.cpp:10-59) on the expanded grid that
  * HistogramManagerMTFFGrid::calculate_all() uses, with the reference's default grid settings (1 A

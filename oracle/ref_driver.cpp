@@ -106,6 +106,52 @@ struct Result {
 };
 
 bool custom_width() { return settings::flags::custom_bin_width; }
+
+// The calculator on the width instantiation the managers would pick (custom bin width: variable).
+template <bool vbw>
+void run_calculator(const double* pts, const int* set_off, int n_sets, int n_jobs, const int* ja, const int* jb,
+                    const int* scaling, const int* merge, int* n_results, int* keys, double* out) {
+    std::vector<hist::detail::CompactCoordinates<vbw>> sets;
+    sets.reserve(n_sets);
+    for (int s = 0; s < n_sets; ++s) {
+        std::vector<data::Water> w;
+        for (int i = set_off[s]; i < set_off[s + 1]; ++i) w.emplace_back(Vector3<double>(pts[4 * i], pts[4 * i + 1], pts[4 * i + 2]));
+        sets.emplace_back(w);
+        auto& d = sets.back().get_data();
+        for (int i = set_off[s]; i < set_off[s + 1]; ++i) {
+            auto& e = d[i - set_off[s]];
+            e.value.pos = Vector3<float>(pts[4 * i], pts[4 * i + 1], pts[4 * i + 2]);
+            e.value.w = static_cast<float>(pts[4 * i + 3]);
+        }
+    }
+    hist::distance_calculator::SimpleCalculator<true, vbw> calc;
+    for (int k = 0; k < n_jobs; ++k) {
+        if (jb[k] < 0) calc.enqueue_calculate_self(sets[ja[k]], scaling[k], merge[k]);
+        else calc.enqueue_calculate_cross(sets[ja[k]], sets[jb[k]], scaling[k], merge[k]);
+    }
+    auto res = calc.run();
+    const size_t nb = settings::axes::bin_count;
+    int r = 0;
+    auto put = [&](int cross, std::map<int, const hist::WeightedDistribution1D*>& m) {
+        for (auto& [id, dist] : m) {
+            keys[2 * r] = cross;
+            keys[2 * r + 1] = id;
+            for (size_t i = 0; i < nb && i < dist->size(); ++i) {
+                const auto& e = dist->index(i);
+                out[(3 * r + 0) * nb + i] = e.value;
+                out[(3 * r + 1) * nb + i] = e.count;
+                out[(3 * r + 2) * nb + i] = e.bin_center;
+            }
+            ++r;
+        }
+    };
+    std::map<int, const hist::WeightedDistribution1D*> self, cross;
+    for (auto& [id, d] : res.self) self[id] = &d;
+    for (auto& [id, d] : res.cross) cross[id] = &d;
+    put(0, self);
+    put(1, cross);
+    *n_results = r;
+}
 }  // namespace
 
 extern "C" {
@@ -455,46 +501,8 @@ int ref_fit(void* r, int param, const double* q, const double* I, const double* 
 int ref_calculator(const double* pts, const int* set_off, int n_sets, int n_jobs, const int* ja, const int* jb,
                    const int* scaling, const int* merge, int* n_results, int* keys, double* out) {
     return guarded([&] {
-        std::vector<hist::detail::CompactCoordinates<false>> sets;
-        sets.reserve(n_sets);
-        for (int s = 0; s < n_sets; ++s) {
-            std::vector<data::Water> w;
-            for (int i = set_off[s]; i < set_off[s + 1]; ++i) w.emplace_back(Vector3<double>(pts[4 * i], pts[4 * i + 1], pts[4 * i + 2]));
-            sets.emplace_back(w);
-            auto& d = sets.back().get_data();
-            for (int i = set_off[s]; i < set_off[s + 1]; ++i) {
-                auto& e = d[i - set_off[s]];
-                e.value.pos = Vector3<float>(pts[4 * i], pts[4 * i + 1], pts[4 * i + 2]);
-                e.value.w = static_cast<float>(pts[4 * i + 3]);
-            }
-        }
-        hist::distance_calculator::SimpleCalculator<true, false> calc;
-        for (int k = 0; k < n_jobs; ++k) {
-            if (jb[k] < 0) calc.enqueue_calculate_self(sets[ja[k]], scaling[k], merge[k]);
-            else calc.enqueue_calculate_cross(sets[ja[k]], sets[jb[k]], scaling[k], merge[k]);
-        }
-        auto res = calc.run();
-        const size_t nb = settings::axes::bin_count;
-        int r = 0;
-        auto put = [&](int cross, std::map<int, const hist::WeightedDistribution1D*>& m) {
-            for (auto& [id, dist] : m) {
-                keys[2 * r] = cross;
-                keys[2 * r + 1] = id;
-                for (size_t i = 0; i < nb && i < dist->size(); ++i) {
-                    const auto& e = dist->index(i);
-                    out[(3 * r + 0) * nb + i] = e.value;
-                    out[(3 * r + 1) * nb + i] = e.count;
-                    out[(3 * r + 2) * nb + i] = e.bin_center;
-                }
-                ++r;
-            }
-        };
-        std::map<int, const hist::WeightedDistribution1D*> self, cross;
-        for (auto& [id, d] : res.self) self[id] = &d;
-        for (auto& [id, d] : res.cross) cross[id] = &d;
-        put(0, self);
-        put(1, cross);
-        *n_results = r;
+        if (custom_width()) run_calculator<true>(pts, set_off, n_sets, n_jobs, ja, jb, scaling, merge, n_results, keys, out);
+        else run_calculator<false>(pts, set_off, n_sets, n_jobs, ja, jb, scaling, merge, n_results, keys, out);
     });
 }
 
