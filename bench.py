@@ -975,7 +975,151 @@ def reference_fit(steps: int, warmup: int):
                       "SmartFitter::fit() of cw (Golden, single-threaded)"}
 
 
+SYM_METRIC = "symmetric histograms/s (icosahedral 60-mer through SimpleCalculator jobs, Simple model)"
+SYM_UNIT = "histograms/s"
+
+
+def symmetry_setup(seed: int = 21, subunit: int = 8333):
+    """cfg2's shell as one body with 60-fold icosahedral symmetry: the job list SymmetryManagerMT issues
+    (SymmetryManagerMT.cpp:37-136) for it, and the expanded structure.  Point sets are float32
+    {x, y, z, w} records; jobs are (a, b or None, scaling, merge id) over them."""
+    from ausaxs_b200 import synth
+
+    cos_half = 1.0 - 1.0 / 36.0
+    sub, ff = synth.globule(seed, subunit, r_in=120.0, r_out=150.0, cone_cos=cos_half)
+    R = synth.icosahedral_rotations()
+    w = synth.ff_charge(ff)
+    copies = [np.column_stack([sub @ r.T, w]).astype(np.float32) for r in R]
+    xyz = np.concatenate([c[:, :3] for c in copies]).astype(np.float64)
+    wat = synth.waters(seed + 1, xyz, np.tile(ff, len(R)), 60000)
+    waters = np.column_stack([wat, np.full(len(wat), synth.ff_charge([synth.FF_WATER])[0])]).astype(np.float32)
+    sets = copies + [waters]
+    W = len(copies)
+    # classes of copy pairs with the same relative rotation up to inversion (PairScheduleUtil.cpp:33-58):
+    # representative (0, k) for the first k of each class, scaling = the class size
+    key = lambda M: tuple(np.round(M.ravel() * 1e4).astype(np.int64))
+    classes = {}
+    for i in range(W):
+        for j in range(i + 1, W):
+            D = R[j].T @ R[i]
+            kk = min(key(D), key(D.T))
+            if kk not in classes:
+                classes[kk] = [i, j, 0]
+            classes[kk][2] += 1
+    jobs = [(0, None, W, 0), (W, 0, 1, 1)]  # the body once with scaling 1 + copies; waters x body
+    jobs += [(i, j, n, 0) for i, j, n in classes.values()]
+    jobs += [(W, k, 1, 1) for k in range(1, W)]  # waters x every copy
+    jobs += [(W, None, 1, 1)]  # waters
+    return sets, jobs, np.concatenate(copies), waters
+
+
+def symmetry_pairs(sets, jobs):
+    n = [len(x) for x in sets]
+    return sum(n[a] * (n[a] - 1) // 2 if b is None else n[a] * n[b] for a, b, _, _ in jobs)
+
+
+def run_symmetry(args, rank, world, local_rank):
+    import torch
+
+    from ausaxs_b200 import _capi, hist
+
+    torch.cuda.set_device(local_rank)
+    ctx = _capi.Context(local_rank)
+    sets, jobs, atoms, waters = symmetry_setup()
+    bw = 0.1
+
+    def step():
+        calc = _capi.Calculator(ctx, bw, 8000)
+        for a, b, sc, m in jobs:
+            if b is None:
+                calc.enqueue_calculate_self(sets[a], sc, m)
+            else:
+                calc.enqueue_calculate_cross(sets[a], sets[b], sc, m)
+        out = calc.run()
+        calc.close()
+        return out
+
+    for _ in range(args.warmup):
+        out = step()
+    launches0 = ctx.launches
+    with ClockSampler(local_rank) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            out = step()
+        t = time.perf_counter() - t0
+    launches = ctx.launches - launches0
+    t = max_over_ranks(t, world)
+    value = world * args.steps / t
+    # the plain Simple histogram of the expanded structure (HistogramManagerMT), timed the same way
+    m = hist.Molecule(atoms=atoms[:, :3].astype(np.float64), weights=atoms[:, 3], waters=waters[:, :3].astype(np.float64),
+                      water_weights=waters[:, 3])
+    mgr = hist.HistogramManagerMT(m, True, bw, 8000, ctx)
+    h = mgr.calculate_all()
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.steps // 2)):
+        h = mgr.calculate_all()
+    t_plain = (time.perf_counter() - t0) / max(1, args.steps // 2)
+    aa = out["self"][0][0] + out["cross"][0][0]
+    n = min(len(aa), len(h.get_aa_counts()))
+    plain_aa = np.zeros(len(aa))
+    plain_aa[:len(h.get_aa_counts())] = h.get_aa_counts()
+    dev = float(np.abs(aa - plain_aa).sum() / np.abs(plain_aa).sum())
+    pairs = symmetry_pairs(sets, jobs)
+    line = {
+        "metric": SYM_METRIC, "value": value, "unit": SYM_UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 distances, integer bins, f64 results", "data": "synthetic (seeded generator)",
+        "config": {"workload": "symmetry: cfg2 shell as one 8333-atom body with icosahedral symmetry (60 copies) + "
+                               "60k waters, Simple weights, 0.1 A bins",
+                   "jobs": len(jobs), "pair_classes": len(jobs) - 62, "pairs_per_step": int(pairs),
+                   "pairs_plain": int(len(atoms) * (len(atoms) - 1) // 2 + len(atoms) * len(waters) +
+                                      len(waters) * (len(waters) - 1) // 2),
+                   "plain_ms": 1e3 * t_plain, "speedup_vs_plain": t_plain / (t / args.steps),
+                   "aa_l1_rel_diff_vs_plain": dev,
+                   "timing": "wall clock around the host-pointer calls (points uploaded, results read back every step)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": value, "unit": SYM_UNIT, "h2d_bytes_per_step": int(sum(x.nbytes for x in sets)),
+                "d2h_bytes_per_step": int(4 * 3 * 8000 * 8)},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = reference_symmetry(sets, jobs, bw)
+    ctx.close()
+    return line
+
+
+def reference_symmetry(sets, jobs, bw):
+    """The reference's SimpleCalculator on the body's jobs (self and the pair classes, no waters),
+    scaled by the pairs of the whole job list."""
+    from oracle import py as O
+
+    if not O.ref_available():
+        return {"unavailable": "reference build oracle/_ref/libausaxs_ref.so not present"}
+    threads = max(1, (os.cpu_count() or 2) - 1)
+    O.ref(threads)
+    O.ref_set_axes(bw, 8000, 1e-4, 0.5)
+    sample = [j for j in jobs if j[0] < len(sets) - 1 and (j[1] is None or j[1] < len(sets) - 1)]
+    t0 = time.perf_counter()
+    O.ref_calculator(sets, sample)
+    t = time.perf_counter() - t0
+    frac = symmetry_pairs(sets, sample) / symmetry_pairs(sets, jobs)
+    return {"value": frac / t, "unit": SYM_UNIT, "cores": threads, "kind": "reference",
+            "sample": f"the body's self and pair-class jobs ({frac:.3f} of the pairs), time scaled by pairs"}
+
+
 def run_reference(args, rank, world):
+    if args.workload == "symmetry":
+        sets, jobs, _, _ = symmetry_setup()
+        det = reference_symmetry(sets, jobs, 0.1)
+        if "unavailable" in det:
+            return {"impl": "reference", **det}
+        v = det["value"]
+        return {"impl": "reference", "metric": SYM_METRIC, "value": v, "unit": SYM_UNIT, "n_gpus": world,
+                "steps": 1, "warmup": 0, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32 distances, f64 bins (reference CPU)",
+                "data": "synthetic (seeded generator)", "config": {"workload": "symmetry (icosahedral 60-mer)"},
+                "cpu_baseline": det, "e2e": {"value": v, "unit": SYM_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if args.workload == "fit":
         det = reference_fit(steps=args.steps, warmup=args.warmup)
         if "unavailable" in det:
@@ -1020,7 +1164,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4", "gridexv", "fit"])
+    ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4", "gridexv", "fit", "symmetry"])
     ap.add_argument("--chains", type=int, default=64)
     ap.add_argument("--hbm-budget-gb", type=float, default=40.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -1043,7 +1187,8 @@ def main():
 
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    line = {"cfg3": run_batch, "cfg4": run_serving, "gridexv": run_gridexv, "fit": run_fit}.get(args.workload, run_ours)(
+    line = {"cfg3": run_batch, "cfg4": run_serving, "gridexv": run_gridexv, "fit": run_fit,
+            "symmetry": run_symmetry}.get(args.workload, run_ours)(
         args, rank, world, local_rank)
     if world > 1:
         import torch
