@@ -2,7 +2,9 @@
  * A plain C caller of the C ABI (include/ausaxs_b200.h), the way a reference-side binding would use it:
  * the reference's SimpleCube known-answer structure (tests/feature/hist/hist_test_helper.h:87-162 in
  * the reference: 8 carbon atoms on the corners of a 2 A cube plus one in its centre, 8 waters on the
- * corners), HistogramManagerMTFFAvg's calculate_all() and debye_transform(), and one error path.
+ * corners), HistogramManagerMTFFAvg's calculate_all() and debye_transform(), the grid excluded volume
+ * of the cube (149 dummies of 1 A^3 in the reference's RawGridExv), a SimpleCalculator self job with
+ * a scaling factor, a noise-free SmartFitter fit of the water scaling, and one error path.
  * Exit status 0 and "ok" when every check holds.
  */
 #include <math.h>
@@ -72,6 +74,53 @@ int main(void) {
     }
     for (int i = 0; i < 3; ++i)
         if (!isfinite(I[i])) return 7;
+    /* grid excluded volume of the cube (the reference's RawGridExv gives 149 dummies, 149 A^3) */
+    int64_t n_exv = 0;
+    double vol = 0;
+    if (ausaxs_gpu_grid_exv(ctx, &atoms[0][0], 9, &waters[0][0], 8, 1, NULL, 0, &n_exv, &vol) != AUSAXS_OK ||
+        n_exv != 149 || vol != 149.0) {
+        fprintf(stderr, "grid exv: %lld dummies, %.1f A^3 (%s)\n", (long long)n_exv, vol, ausaxs_gpu_last_error());
+        return 9;
+    }
+    /* SimpleCalculator: the cube's atoms with weight 1, scaling 3: factor 6 per pair, 3 * 9 on the diagonal */
+    float unit[9][4];
+    for (int i = 0; i < 9; ++i) {
+        memcpy(unit[i], atoms[i], 3 * sizeof(float));
+        unit[i][3] = 1.0f;
+    }
+    ausaxs_gpu_calculator* calc = NULL;
+    int32_t idx = -1, ns = 0, nc = 0;
+    double* cv = calloc(NB, sizeof(double));
+    double* cn = calloc(NB, sizeof(double));
+    if (ausaxs_gpu_calculator_create(ctx, 0.25, NB, &calc) != AUSAXS_OK ||
+        ausaxs_gpu_calculator_enqueue_self(calc, &unit[0][0], 9, 3, -1, &idx) != AUSAXS_OK || idx != 0 ||
+        ausaxs_gpu_calculator_run(calc, &ns, &nc) != AUSAXS_OK || ns != 1 || nc != 0 ||
+        ausaxs_gpu_calculator_result(calc, 0, 0, cv, cn, NULL) != AUSAXS_OK) {
+        fprintf(stderr, "calculator: %s\n", ausaxs_gpu_last_error());
+        return 10;
+    }
+    if (cv[0] != 27 || cn[0] != 27 || cv[7] != 48 || cv[8] != 72 || cv[11] != 72 || cv[14] != 24) {
+        fprintf(stderr, "calculator values %g %g %g %g %g\n", cv[0], cv[7], cv[8], cv[11], cv[14]);
+        return 11;
+    }
+    ausaxs_gpu_calculator_destroy(calc);
+    /* SmartFitter: data = 3 * I(cw = 2) + 5 on 20 q values; the water scaling comes back as 2 */
+    double fq[20], fI[20], fs[20];
+    for (int i = 0; i < 20; ++i) fq[i] = 0.01 + 0.02 * i;
+    ausaxs_debye_params p2 = p;
+    p2.cw = 2.0;
+    if (ausaxs_gpu_debye(ctx, &cfg, &r, fq, 20, &p2, fI, NULL) != AUSAXS_OK) return 12;
+    for (int i = 0; i < 20; ++i) {
+        fI[i] = 3 * fI[i] + 5;
+        fs[i] = 0.01 * fI[i];
+    }
+    ausaxs_fit_options opt = {0, 0.0, 0.0, 1e-4};
+    ausaxs_fit_result fit;
+    if (ausaxs_gpu_fit(ctx, &cfg, &r, fq, fI, fs, 20, &p, &opt, &fit, NULL) != AUSAXS_OK ||
+        fabs(fit.value - 2.0) > 1e-4 || fabs(fit.a - 3.0) > 1e-3 || fit.chi2 > 1e-2) {
+        fprintf(stderr, "fit: cw %.6f a %.6f chi2 %.3g (%s)\n", fit.value, fit.a, fit.chi2, ausaxs_gpu_last_error());
+        return 13;
+    }
     /* errors come back as status codes plus text, never as a crash */
     if (ausaxs_gpu_histogram(ctx, &cfg, &atoms[0][0], -1, NULL, 0, NULL, 0, &r) != AUSAXS_ERR_ARGUMENT ||
         strlen(ausaxs_gpu_last_error()) == 0)
@@ -82,6 +131,8 @@ int main(void) {
     free(ww);
     free(tot);
     free(d);
+    free(cv);
+    free(cn);
     printf("ok I(0.01)=%.6e I(0.1)=%.6e I(0.5)=%.6e\n", I[0], I[1], I[2]);
     return 0;
 }
