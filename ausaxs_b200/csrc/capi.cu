@@ -380,12 +380,13 @@ int ausaxs_gpu_fit(ausaxs_gpu_ctx* ctx, const ausaxs_hist_config* cfg, const aus
         const ausaxs_debye_params b = default_params(base);
         FitArgs F = fit_search(*cfg, options, b);
         const size_t vec = align_up((size_t)n * 8, 256);
-        HostDebye D = upload_host_histogram(C, *cfg, *hist, q, n, unit_params(b), 4 * vec + 256);
+        HostDebye D = upload_host_histogram(C, *cfg, *hist, q, n, unit_params(b), 5 * vec + 256);
         double* y = reinterpret_cast<double*>(D.extra);
         double* sg = reinterpret_cast<double*>(D.extra + vec);
         F.Iw = reinterpret_cast<double*>(D.extra + 2 * vec);
         F.I_fit = I_fit ? reinterpret_cast<double*>(D.extra + 3 * vec) : nullptr;
-        F.out = reinterpret_cast<double*>(D.extra + 4 * vec);
+        F.W = reinterpret_cast<double*>(D.extra + 4 * vec);
+        F.out = reinterpret_cast<double*>(D.extra + 5 * vec);
         AUSAXS_CUDA(cudaMemcpyAsync(y, I, (size_t)n * 8, cudaMemcpyHostToDevice, C.stream));
         AUSAXS_CUDA(cudaMemcpyAsync(sg, sigma, (size_t)n * 8, cudaMemcpyHostToDevice, C.stream));
         run_debye(C, D.A, D.groups, C.tc, 1);
@@ -414,12 +415,13 @@ int ausaxs_gpu_structure_fit(ausaxs_gpu_ctx* ctx, ausaxs_gpu_structure* s, const
         const ausaxs_debye_params b = default_params(base);
         FitArgs F = fit_search(*cfg, options, b);
         const size_t vec = align_up((size_t)n * 8, 256);
-        C.io.ensure(8 * vec + 256);
+        C.io.ensure(9 * vec + 256);
         char* io = C.io.as<char>();
         double* prof = reinterpret_cast<double*>(io);
         double* Iu = reinterpret_cast<double*>(io + 6 * vec);
         F.Iw = reinterpret_cast<double*>(io + 7 * vec);
-        F.out = reinterpret_cast<double*>(io + 8 * vec);
+        F.W = reinterpret_cast<double*>(io + 8 * vec);
+        F.out = reinterpret_cast<double*>(io + 9 * vec);
         s->impl.enqueue_histogram(*cfg);
         DebyeArgs A = s->impl.debye_args(*cfg, q, n, unit_params(b), Iu, prof);
         run_debye(C, A, cfg->manager == AUSAXS_MANAGER_FFGRID ? 7 : 1, s->impl.plan.tc, 1);

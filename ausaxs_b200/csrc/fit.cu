@@ -17,8 +17,13 @@
 // (fitter::detail::LinearLeastSquares, LinearLeastSquares.cpp:26-78).
 //
 // One CTA runs the whole search: every thread executes the same Golden control flow on the
-// block-wide chi2 values, so no state is broadcast.  The interval arithmetic is written with
-// explicit round-to-nearest operations (no contraction), as the host evaluates it.
+// block-wide chi2 values, so no state is broadcast.  The sums that do not depend on the trial
+// (S = sum w, Sy = sum w y, Syy = sum w y^2, w = 1/sigma^2) are formed once; a trial needs Sx, Sxx and
+// Sxy only, one block reduction, and its chi2 follows from the sums,
+//     chi2 = Syy - 2 a Sxy - 2 b Sy + a^2 Sxx + 2 a b Sx + b^2 S,
+// which at the fitted value is recomputed as the reference forms it (explicit residuals).  The
+// interval arithmetic is written with explicit round-to-nearest operations (no contraction), as the
+// host evaluates it.
 #include <cmath>
 
 #include "common.cuh"
@@ -27,7 +32,7 @@
 namespace ausaxs_b200 {
 namespace {
 
-constexpr int kFitThreads = 512;
+constexpr int kFitThreads = 256;
 constexpr int kFitWarps = kFitThreads / 32;
 
 // block-wide sum of N values; every thread gets the totals
@@ -76,34 +81,52 @@ __device__ double model_intensity(const FitArgs& F, const double (&p)[5], int k)
 }
 
 __global__ void __launch_bounds__(kFitThreads) fit_kernel(FitArgs F) {
-    __shared__ double s_red[5][kFitWarps];
+    __shared__ double s_red[3][kFitWarps];
     const int n = F.nq;
-    double fit_a = 0, fit_b = 0, delta = 0, S = 0, Sxx = 0;
-    // chi2 of one trial value, identical in every thread
+    // trial-independent sums; w = 1/sigma^2 kept in the scratch array W
+    double fixed[3] = {0, 0, 0};  // S, Sy, Syy
+    for (int k = threadIdx.x; k < n; k += kFitThreads) {
+        const double is = 1. / F.sigma[k];
+        const double w = is * is;
+        F.W[k] = w;
+        fixed[0] += w;
+        fixed[1] += F.y[k] * w;
+        fixed[2] += F.y[k] * F.y[k] * w;
+    }
+    block_sum<3>(fixed, s_red);
+    const double S = fixed[0], Sy = fixed[1], Syy = fixed[2];
+    double fit_a = 0, fit_b = 0, Sx = 0, Sxx = 0, delta = 1;
+    // chi2 of one trial value from the sums, identical in every thread
     auto evaluate = [&](double v) -> double {
         double p[5] = {F.base[0], F.base[1], F.base[2], F.base[3], F.base[4]};
         p[F.param] = v;
-        double sums[5] = {0, 0, 0, 0, 0};  // S, Sx, Sy, Sxx, Sxy
+        double t[3] = {0, 0, 0};  // Sx, Sxx, Sxy
+        for (int k = threadIdx.x; k < n; k += kFitThreads) {
+            const double x = model_intensity(F, p, k);
+            const double w = F.W[k];
+            t[0] += x * w;
+            t[1] += x * x * w;
+            t[2] += x * F.y[k] * w;
+        }
+        block_sum<3>(t, s_red);
+        Sx = t[0];
+        Sxx = t[1];
+        delta = S * Sxx - Sx * Sx;
+        fit_a = (S * t[2] - Sx * Sy) / delta;
+        fit_b = (Sxx * Sy - Sx * t[2]) / delta;
+        return Syy - 2 * fit_a * t[2] - 2 * fit_b * Sy + fit_a * fit_a * Sxx + 2 * fit_a * fit_b * Sx +
+               fit_b * fit_b * S;
+    };
+    // the final evaluation as the reference forms it: the sums, then the explicit residuals
+    auto evaluate_residuals = [&](double v) -> double {
+        evaluate(v);
+        double p[5] = {F.base[0], F.base[1], F.base[2], F.base[3], F.base[4]};
+        p[F.param] = v;
+        double c2[1] = {0};
         for (int k = threadIdx.x; k < n; k += kFitThreads) {
             const double x = model_intensity(F, p, k);
             F.Iw[k] = x;
-            const double is = 1. / F.sigma[k];
-            const double w = is * is;
-            sums[0] += w;
-            sums[1] += x * w;
-            sums[2] += F.y[k] * w;
-            sums[3] += x * x * w;
-            sums[4] += x * F.y[k] * w;
-        }
-        block_sum<5>(sums, s_red);
-        S = sums[0];
-        Sxx = sums[3];
-        delta = sums[0] * sums[3] - sums[1] * sums[1];
-        fit_a = (sums[0] * sums[4] - sums[1] * sums[2]) / delta;
-        fit_b = (sums[3] * sums[2] - sums[1] * sums[4]) / delta;
-        double c2[1] = {0};
-        for (int k = threadIdx.x; k < n; k += kFitThreads) {
-            const double r = (F.y[k] - (fit_a * F.Iw[k] + fit_b)) * (1. / F.sigma[k]);
+            const double r = (F.y[k] - (fit_a * x + fit_b)) * (1. / F.sigma[k]);
             c2[0] += r * r;
         }
         block_sum<1>(c2, s_red);
@@ -144,7 +167,7 @@ __global__ void __launch_bounds__(kFitThreads) fit_kernel(FitArgs F) {
     }
     // Golden::minimize_override: the centre of the final interval (Limit::center = min + span / 2)
     const double value = __dadd_rn(ilo, __dsub_rn(ihi, ilo) / 2);
-    const double chi2 = evaluate(value);
+    const double chi2 = evaluate_residuals(value);
     if (F.I_fit)
         for (int k = threadIdx.x; k < n; k += kFitThreads) F.I_fit[k] = fit_a * F.Iw[k] + fit_b;
     if (threadIdx.x == 0) {

@@ -28,7 +28,8 @@ struct FitArgs {
     double lo, hi;         // search interval
     int32_t steps;         // Golden iterations n = ceil(log(tol / (hi - lo)) / log(1 / phi)); < 0: no search
     double invphi, invphi2;
-    double* Iw;            // [nq] scratch: model intensities of the current trial
+    double* Iw;            // [nq] scratch: model intensities at the fitted value
+    double* W;             // [nq] scratch: 1 / sigma^2
     double* out;           // [7]: value, a, b, chi2, evaluations, a_err, b_err
     double* I_fit;         // [nq] or null: a I_model + b at the fitted value
 };
