@@ -102,3 +102,22 @@ def test_calculator_errors(gpu_ctx):
         _capi.check(_capi.load().ausaxs_gpu_calculator_result(calc.h, 1, 3, _capi.dptr(v), _capi.dptr(v), _capi.dptr(v)))
     assert e.value.code == _capi.ERR_NOT_FOUND
     calc.close()
+
+
+def test_calculator_empty_sets_and_repeated_runs(gpu_ctx):
+    rng = np.random.default_rng(6)
+    a = np.column_stack([rng.normal(0, 4, (50, 3)), rng.uniform(1, 2, 50)]).astype(np.float32)
+    empty = np.zeros((0, 4), np.float32)
+    calc = _capi.Calculator(gpu_ctx, 0.25, 8000)
+    assert calc.run() == {"self": {}, "cross": {}}  # nothing enqueued
+    calc.enqueue_calculate_self(empty, 2, 0)
+    calc.enqueue_calculate_cross(a, empty, 1, 0)
+    out = calc.run()
+    assert not np.any(out["self"][0][0]) and not np.any(out["cross"][0][0])
+    for _ in range(2):  # the same jobs twice give the same results (run clears the jobs)
+        calc.enqueue_calculate_self(a, 3, 7)
+        r = calc.run()
+        assert list(r["self"]) == [7]
+    o = O.calculator([a], [(0, None, 3, 7)], 0.25, 8000)
+    check_result(r["self"][7], o[(0, 7)], [a], 0.25, 8000)
+    calc.close()

@@ -84,3 +84,24 @@ def test_fit_argument_errors(gpu_ctx):
         SmartFitter((g["q"], g["y"], g["sigma"]), h).fit("cx")
     with pytest.raises(ValueError):
         SmartFitter((g["q"], g["y"][:-1], g["sigma"]), h)
+
+
+def test_fit_minimum_outside_the_interval(gpu_ctx):
+    """The Golden search converges to the interval's edge when the minimum lies beyond it, as the
+    reference does; the oracle takes the same path."""
+    g = load_golden("fit_random_ffavg_cw")  # truth cw = 1.6
+    h = manager_for(g, gpu_ctx).calculate_all()
+    r = SmartFitter((g["q"], g["y"], g["sigma"]), h).fit("cw", (2.0, 4.0))
+    o = O.fit(FIT_KIND["ffavg"], oracle_for(g), g["q"], g["y"], g["sigma"], 0, 2.0, 4.0)
+    assert abs(r.value - 2.0) < 1e-4 and abs(r.value - o[0]) <= 1e-4
+
+
+@pytest.mark.parametrize("param", ["dw_atomic", "dw_exv"])
+def test_fit_debye_waller_vs_oracle(param, gpu_ctx):
+    g = load_golden("fit_random_ffavg_dwa")
+    h = manager_for(g, gpu_ctx).calculate_all()
+    k = PARAMS.index(param)
+    r = SmartFitter((g["q"], g["y"], g["sigma"]), h).fit(param)
+    o = O.fit(FIT_KIND["ffavg"], oracle_for(g), g["q"], g["y"], g["sigma"], k)
+    assert abs(r.value - o[0]) <= 1e-4
+    np.testing.assert_allclose(r.chi2, o[3], rtol=1e-6)

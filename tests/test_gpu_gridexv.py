@@ -131,3 +131,16 @@ def test_structure_from_grid_equals_given_dummies(gpu_ctx):
     np.testing.assert_array_equal(out[0], out[1])
     with pytest.raises(_capi.AusaxsError):  # grid dummies need form-factor types
         _capi.Structure(gpu_ctx, a, w, ff_typed=False, exv_from_grid=True)
+
+
+def test_grid_dummies_edge_cases(gpu_ctx):
+    """Waters only (no atoms: nothing is kept) and a single atom of each van der Waals radius class."""
+    w = _records(np.array([[0.0, 0.0, 0.0], [5.0, 1.0, -2.0]]), np.ones(2, np.int32))
+    d, vol = _capi.grid_exv(gpu_ctx, np.zeros((0, 4), np.float32), w)
+    assert len(d) == 0 and vol == 0.0
+    for ff in (2, 3, 7, 11, 12, 14):
+        xyz = np.array([[0.3, -0.2, 0.7]])
+        d, vol = _capi.grid_exv(gpu_ctx, _records(xyz, np.array([ff], np.int32)), np.zeros((0, 4), np.float32))
+        do, vo = O.grid_exv(xyz.astype(np.float32).astype(np.float64), np.array([ff]), None)
+        np.testing.assert_array_equal(d[:, :3].astype(np.float64), do)
+        assert vol == vo
