@@ -13,7 +13,10 @@ constexpr float kMagic = 12582912.0f;      // 1.5 * 2^23: x + kMagic rounds x to
 constexpr int32_t kMagicBits = 0x4B400000; // bit pattern of kMagic
 constexpr int kResBits = 16;              // bits of the fixed-point in-bin offset (see pair_residual)
 constexpr int32_t kResBias = 1 << (kResBits - 1);  // bias making the offset non-negative
-constexpr int kSegment = 128;             // inner points between drains: 512 x 128 pairs x 2^16 < 2^32
+// inner points between drains of the 32-bit offset accumulators: TILE x segment <= 2^16 pairs per bin,
+// each adding < 2^16, so a drained word stays below 2^32
+template <int TILE>
+__host__ __device__ constexpr int drain_segment() { return 65536 / TILE; }
 
 // ---------------------------------------------------------------------------------------------
 // Pair evaluation with the reference's rounding sequence.

@@ -265,6 +265,15 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
 
     long long biggest = std::max<long long>({(long long)n_a, (long long)n_w, (long long)n_x_eff});
     P.tile = biggest >= 16384 ? 512 : 256;
+    // Type-pair rows whose 512-point layout holds the CTA to one per SM (register-held offset sums)
+    // and that still fit with 1024-point tiles run 1024 threads per CTA: the same shared memory
+    // then serves 32 warps per SM instead of 16 (every launch of the plan uses the tile size).
+    if (P.tile == 512 && !mt) {
+        const int rows_aa = T * T;
+        if (pairhist_dreg(rows_aa, nb, false, 512) && pairhist_dreg(rows_aa, nb, false, 1024) &&
+            pairhist_launch_smem(rows_aa, nb, false, 1024) <= kPairSmemCap)
+            P.tile = 1024;
+    }
     const int tile = P.tile;
     auto nt = [tile](int n) { return (n + tile - 1) / tile; };
 
@@ -300,7 +309,7 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
     for (auto& j : js) slot_rows[j.slot] = std::max(slot_rows[j.slot], j.rows);
 
     // on-chip budget: split rows of a job into groups when its [rows][nb] counts do not fit
-    const int max_group_rows = pairhist_max_rows(nb, weighted && mt);
+    const int max_group_rows = pairhist_max_rows(nb, weighted && mt, tile == 1024 ? 1024 : 512);
     if (pairhist_launch_smem(1, nb, weighted && mt, 512) > kPairSmemCap)
         throw Error{AUSAXS_ERR_CAPACITY, "too many distance bins for the on-chip histogram"};
 

@@ -57,7 +57,7 @@ __device__ __forceinline__ void tile_coords(const PairJob& J, long long t, int& 
 // On-chip privatised histograms of one CTA.
 //   counts   : u32 per (row, bin), one atomic per pair.
 //   offsets  : the in-bin distance offset of a pair is quantised to 16 bits (kResBits) and added
-//              with a 32-bit atomic to dacc; every kSegment inner points (at most 2^16 pairs per
+//              with a 32-bit atomic to dacc; every drain_segment<TILE>() inner points (at most 2^16 pairs per
 //              bin, so dacc cannot wrap) the threads drain dacc into the u64 sums d64 without
 //              atomics.  (A 64-bit shared-memory atomic costs about three times as much per pair on
 //              sm_100a; this keeps one cheap 32-bit atomic per pair and an exact integer sum.)
@@ -285,8 +285,8 @@ __global__ void __launch_bounds__(TILE, DREG ? 1 : 1024 / TILE) pairhist_kernel(
             const bool diag = J.self && ti == tj;
             const bool has_tail = J.b_base + j0 + jn > J.tail_end - 3;  // scalar-tail partners: last 3 of a row
             const bool general = diag || has_tail;
-            for (int k0 = 0; k0 < jn; k0 += kSegment) {
-                const int k1 = min(jn, k0 + kSegment);
+            for (int k0 = 0; k0 < jn; k0 += drain_segment<TILE>()) {
+                const int k1 = min(jn, k0 + drain_segment<TILE>());
                 if (active) {
                     if (general) {
                         if (single) tile_pairs<true, WEIGHTED, kRowsSingle>(J, S, s_pts, a, i, j0, k0, k1, diag, wsc, overflow);
@@ -324,7 +324,11 @@ void launch_one(const PairLaunch& L, int grid, size_t smem, cudaStream_t s) {
 
 void pairhist_launch(const PairLaunch& L, int tile, int grid, size_t smem, cudaStream_t s) {
     // register-held offset sums exist for unweighted launches only (pairhist_dreg)
-    if (tile == 256) {
+    if (tile == 1024) {
+        if (L.weighted) launch_one<1024, true, false>(L, grid, smem, s);
+        else if (L.dreg) launch_one<1024, false, true>(L, grid, smem, s);
+        else launch_one<1024, false, false>(L, grid, smem, s);
+    } else if (tile == 256) {
         if (L.weighted) launch_one<256, true, false>(L, grid, smem, s);
         else if (L.dreg) launch_one<256, false, true>(L, grid, smem, s);
         else launch_one<256, false, false>(L, grid, smem, s);

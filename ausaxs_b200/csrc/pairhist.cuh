@@ -91,17 +91,17 @@ inline size_t pairhist_launch_smem(int rows, int bins, bool weighted, int tile) 
     return pairhist_smem_bytes(rows, bins, weighted, tile, pairhist_dreg(rows, bins, weighted, tile));
 }
 
-// Resident CTAs per SM of a launch (register-sum launches are compiled for one).
+// Resident CTAs per SM of a launch (register-sum launches and 1024-point tiles are compiled for one).
 inline int pairhist_ctas_per_sm(size_t smem, int tile, bool dreg) {
-    if (dreg) return 1;
+    if (dreg || tile >= 1024) return 1;
     const int by_smem = (int)(233472 / (smem + 1024));
     return by_smem < 1 ? 1 : (by_smem < 2048 / tile ? by_smem : 2048 / tile);
 }
 
-// Rows of [rows][bins] counts that fit on chip for 512-point tiles (256-point tiles need less).
-inline int pairhist_max_rows(int bins, bool weighted) {
+// Rows of [rows][bins] counts that fit on chip for `tile`-point tiles (512 covers 256 as well).
+inline int pairhist_max_rows(int bins, bool weighted, int tile = 512) {
     int r = 1;
-    while (r < 4096 && pairhist_launch_smem(r + 1, bins, weighted, 512) <= kPairSmemCap) ++r;
+    while (r < 4096 && pairhist_launch_smem(r + 1, bins, weighted, tile) <= kPairSmemCap) ++r;
     return r;
 }
 
