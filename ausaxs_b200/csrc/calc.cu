@@ -30,7 +30,7 @@ struct CalcSlot {
     long long* ws;
     double diag_value;  // sum over the slot's self jobs of scaling * sum(float(w*w))
     double diag_count;  // sum over them of that value truncated to unsigned
-    double* out;        // [3][bin_count]: value, count, distance sum
+    double* out;        // [3][nb]: value, count, distance sum
 };
 
 __device__ __forceinline__ double unbiased_weights(const long long* w, const unsigned long long* n, int b, double inv) {
@@ -38,31 +38,28 @@ __device__ __forceinline__ double unbiased_weights(const long long* w, const uns
     return static_cast<double>(static_cast<long long>(raw)) * inv;
 }
 
-// grid.y = slot; every bin of bin_count (zero beyond the accumulated range)
-__global__ void calc_finalize_kernel(const CalcSlot* slots, int nb, int bin_count, const float* wscale, float c,
-                                     float scale) {
+// grid.y = slot; the nb accumulated bins (every later bin is zero)
+__global__ void calc_finalize_kernel(const CalcSlot* slots, int nb, const float* wscale, float c, float scale) {
     const CalcSlot S = slots[blockIdx.y];
     const double inv = 1.0 / static_cast<double>(*wscale);
-    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < bin_count; b += gridDim.x * blockDim.x) {
-        double v = 0, n = 0, d = 0;
-        if (b < nb) {
-            const unsigned long long cnt = S.cnt[b];
-            v = 2.0 * unbiased_weights(S.ws, S.cnt, b, inv);
-            n = 2.0 * static_cast<double>(cnt);
-            if (cnt) {
-                // sum of the pairs' float distances: cnt * b * c + sum of the fixed-point offsets
-                const long long resid = static_cast<long long>(S.ds[b]) - static_cast<long long>(cnt) * kResBias;
-                d = 2.0 * (static_cast<double>(cnt) * b * static_cast<double>(c) +
-                           static_cast<double>(resid) / static_cast<double>(scale));
-            }
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+        const unsigned long long cnt = S.cnt[b];
+        double v = 2.0 * unbiased_weights(S.ws, S.cnt, b, inv);
+        double n = 2.0 * static_cast<double>(cnt);
+        double d = 0;
+        if (cnt) {
+            // sum of the pairs' float distances: cnt * b * c + sum of the fixed-point offsets
+            const long long resid = static_cast<long long>(S.ds[b]) - static_cast<long long>(cnt) * kResBias;
+            d = 2.0 * (static_cast<double>(cnt) * b * static_cast<double>(c) +
+                       static_cast<double>(resid) / static_cast<double>(scale));
         }
         if (b == 0) {
             v += S.diag_value;
             n += S.diag_count;
         }
         S.out[b] = v;
-        S.out[static_cast<size_t>(bin_count) + b] = n;
-        S.out[2 * static_cast<size_t>(bin_count) + b] = d;
+        S.out[static_cast<size_t>(nb) + b] = n;
+        S.out[2 * static_cast<size_t>(nb) + b] = d;
     }
 }
 
@@ -176,7 +173,7 @@ struct Calculator {
         unsigned long long* counter = reinterpret_cast<unsigned long long*>(ab + (size_t)n_slots * 3 * row);
         unsigned long long* overflow = counter + 4;
         float* wscale = reinterpret_cast<float*>(counter + 8);
-        out.ensure((size_t)n_slots * 3 * bin_count * 8);
+        out.ensure((size_t)n_slots * 3 * nb * 8);
         const float4* P = points.as<float4>();
         weight_scale_launch(P, (int)staged.size(), P, 0, wscale, s);
         C.check_launch("calculator weight scale");
@@ -194,7 +191,7 @@ struct Calculator {
             table_h[k].ds = reinterpret_cast<unsigned long long*>(ab + (size_t)(3 * k + 1) * row);
             table_h[k].ws = reinterpret_cast<long long*>(ab + (size_t)(3 * k + 2) * row);
             table_h[k].diag_value = table_h[k].diag_count = 0;
-            table_h[k].out = out.as<double>() + (size_t)k * 3 * bin_count;
+            table_h[k].out = out.as<double>() + (size_t)k * 3 * nb;
         }
         long long pairs = 0;
         int biggest = 0;
@@ -278,13 +275,16 @@ struct Calculator {
             C.time_end(0, ev);
         }
         const int threads = 256;
-        calc_finalize_kernel<<<dim3((unsigned)((bin_count + threads - 1) / threads), (unsigned)n_slots), threads, 0, s>>>(
-            reinterpret_cast<const CalcSlot*>(table.p), nb, bin_count, wscale, plan.c, plan.scale);
+        calc_finalize_kernel<<<dim3((unsigned)((nb + threads - 1) / threads), (unsigned)n_slots), threads, 0, s>>>(
+            reinterpret_cast<const CalcSlot*>(table.p), nb, wscale, plan.c, plan.scale);
         C.check_launch("calculator finalize");
         unsigned long long of = 0;
         AUSAXS_CUDA(cudaMemcpyAsync(&of, overflow, 8, cudaMemcpyDeviceToHost, s));
-        AUSAXS_CUDA(cudaMemcpyAsync(results.data(), out.p, results.size() * 8, cudaMemcpyDeviceToHost, s));
+        std::vector<double> packed((size_t)n_slots * 3 * nb);
+        AUSAXS_CUDA(cudaMemcpyAsync(packed.data(), out.p, packed.size() * 8, cudaMemcpyDeviceToHost, s));
         AUSAXS_CUDA(cudaStreamSynchronize(s));
+        for (size_t r = 0; r < (size_t)n_slots * 3; ++r)  // [slot][3][nb] -> [slot][3][bin_count]
+            std::memcpy(results.data() + r * bin_count, packed.data() + r * nb, (size_t)nb * 8);
         pairs_last = pairs;
         clear();
         if (of)
