@@ -577,8 +577,9 @@ void Structure::enqueue_debye(const ausaxs_hist_config& cfg, const double* q_dev
     run_debye(*ctx, A, cfg.manager == AUSAXS_MANAGER_FFGRID ? 7 : 1, plan.tc, p.precision);
 }
 
-void run_debye(Ctx& C, DebyeArgs& A, int groups_present, DevBuf& tc, int precision) {
-    if (A.nq <= 0) return;
+int run_debye(Ctx& C, DebyeArgs& A, int groups_present, DevBuf& tc, int precision) {
+    precision = debye_precision(precision, A.R, A.nb, A.nq);
+    if (A.nq <= 0) return precision;
     cudaStream_t s = C.stream;
     if (precision == 0) {
         // split-BF16 tensor-core contraction for every q, FP64 re-evaluation of the flagged ones
@@ -629,6 +630,7 @@ void run_debye(Ctx& C, DebyeArgs& A, int groups_present, DevBuf& tc, int precisi
     debye_fp64_launch(A, s);
     C.check_launch("debye");
     C.time_end(2, ev);
+    return precision;
 }
 
 void Structure::read_histogram(const ausaxs_hist_config& cfg, ausaxs_hist_result* out) {
@@ -771,7 +773,7 @@ HostDebye upload_host_histogram(Ctx& C, const ausaxs_hist_config& cfg, const aus
     int32_t* cols = reinterpret_cast<int32_t*>(base + off_mb) + 1;
     AUSAXS_CUDA(cudaMemsetAsync(cols, 0, 4, s));
     A.fp64_columns = cols;
-    A.tc_err_est = p.precision == 0 ? reinterpret_cast<double*>(base + off_E) : nullptr;
+    A.tc_err_est = p.precision != 1 ? reinterpret_cast<double*>(base + off_E) : nullptr;
     out.extra = base + off_X;
     out.groups = grid ? 7 : 1;
     return out;
@@ -784,17 +786,17 @@ void debye_of_host_histogram(Ctx& C, const ausaxs_hist_config& cfg, const ausaxs
     double* prof_dev = A.profiles;
     if (!profiles) A.profiles = nullptr;
     cudaStream_t s = C.stream;
-    C.last_tc_err.assign(p.precision == 0 ? nq : 0, INFINITY);
+    C.last_tc_err.assign(p.precision != 1 ? nq : 0, INFINITY);
     if (nq > 0) {
-        run_debye(C, A, D.groups, C.tc, p.precision);
+        const int used = run_debye(C, A, D.groups, C.tc, p.precision);
         int32_t ncols = 0;
         AUSAXS_CUDA(cudaMemcpyAsync(&ncols, A.fp64_columns, 4, cudaMemcpyDeviceToHost, s));
         AUSAXS_CUDA(cudaMemcpyAsync(Iq, A.Iq, (size_t)nq * 8, cudaMemcpyDeviceToHost, s));
         if (profiles) AUSAXS_CUDA(cudaMemcpyAsync(profiles, prof_dev, (size_t)nq * 6 * 8, cudaMemcpyDeviceToHost, s));
-        if (p.precision == 0)
+        if (p.precision != 1)
             AUSAXS_CUDA(cudaMemcpyAsync(C.last_tc_err.data(), A.tc_err_est, (size_t)nq * 8, cudaMemcpyDeviceToHost, s));
         AUSAXS_CUDA(cudaStreamSynchronize(s));
-        C.last_fp64_columns = p.precision == 0 ? ncols : nq;
+        C.last_fp64_columns = used == 0 ? ncols : nq;
     }
     AUSAXS_CUDA(cudaStreamSynchronize(s));
 }

@@ -181,8 +181,18 @@ struct ZeroRange {
 };
 void zero_ranges_launch(const ZeroRange* ranges_dev, int n, cudaStream_t s);
 
-// Tensor-core contraction (precision 0) followed by the FP64 epilogue, or FP64 only (precision 1).
-void run_debye(Ctx& C, DebyeArgs& A, int groups_present, DevBuf& tc, int precision);
+// Tensor-core contraction (precision 0) followed by the FP64 epilogue, or FP64 only (precision 1);
+// precision 2 picks 0 when the contraction pays off (debye_precision).  Returns the precision used.
+int run_debye(Ctx& C, DebyeArgs& A, int groups_present, DevBuf& tc, int precision);
+
+// The contraction's fixed cost (operand staging in a few CTAs, ~50 us) exceeds the FP64 transform's
+// below about 5e6 row x bin x q products (measured: 48 us against 25 us at 2.4e6, 92 + ~50 us
+// against ~400 us at 5.4e7); precision 2 uses the tensor cores from 8e6 on.
+constexpr double kTcMinWork = 8e6;
+inline int debye_precision(int precision, int rows, int bins, int nq) {
+    if (precision != 2) return precision;
+    return (double)rows * bins * nq >= kTcMinWork ? 0 : 1;
+}
 
 // A histogram given in the reference's host layouts (ausaxs_hist_result), compacted to the rows of
 // the form-factor types present and uploaded into the context's io buffer with q: the transform's

@@ -519,8 +519,9 @@ def run_ours(args, rank, world, local_rank):
     cfg = mgr.config()
     A, W, X = mgr._inputs()
     pairs = pair_count(m, grid)
-    # precision 0: split-BF16 tensor-core transform, FP64 for every q whose rigorous error bound
-    # exceeds the tolerance (the path's I(q) bar, 1e-4 relative to the FP64 transform)
+    # precision 2 (default): the split-BF16 tensor-core transform where it pays off (FP64 for every q
+    # whose rigorous error bound exceeds the tolerance, the path's I(q) bar of 1e-4 relative to the
+    # FP64 transform), the FP64 transform for small ones
     params = _capi.DebyeParams(1.0, 1.0, 1.0, 0.0, 0.0, 1.0, args.precision, args.tolerance)
     nq = len(wl.q)
     q_dev = torch.tensor(wl.q, dtype=torch.float64, device=f"cuda:{local_rank}")
@@ -1169,7 +1170,8 @@ def main():
     ap.add_argument("--hbm-budget-gb", type=float, default=40.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--subunit", type=int, default=0, help="cfg2: atoms per subunit (default 8333; smaller for profiling)")
-    ap.add_argument("--precision", type=int, default=0, choices=[0, 1])
+    ap.add_argument("--precision", type=int, default=2, choices=[0, 1, 2],
+                    help="Debye transform: 0 tensor cores, 1 FP64, 2 automatic (tensor cores from 8e6 row x bin x q)")
     ap.add_argument("--tolerance", type=float, default=1e-4)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

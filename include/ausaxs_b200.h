@@ -152,7 +152,9 @@ AUSAXS_API int ausaxs_gpu_histogram(ausaxs_gpu_ctx* ctx, const ausaxs_hist_confi
  * scaling, crho = solvent density scaling, Debye-Waller sigmas for atoms and exv).
  * grid_width: settings::grid::exv::width, the FFGRID dummy volume is grid_width^3.
  * precision: 0 = split-BF16 tensor-core contraction with FP64 recomputation of every q whose
- *            estimated error exceeds tolerance; 1 = FP64 on CUDA cores for every q.
+ *            estimated error exceeds tolerance; 1 = FP64 on CUDA cores for every q; 2 = automatic:
+ *            0 when the transform has at least 8e6 row x bin x q products (below that the
+ *            contraction's fixed cost exceeds the FP64 transform's), else 1.
  */
 typedef struct {
     double cw, cx, crho, dw_atomic, dw_exv;

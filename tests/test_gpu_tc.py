@@ -100,3 +100,28 @@ def test_tc_large_counts_and_many_bins(gpu_ctx):
     I64, _, Itc = _pair(h, q, gpu_ctx, 1e30)
     est = gpu_ctx.tc_error_estimate(len(q))
     assert np.all(np.abs(Itc - I64) <= est * np.abs(Itc))
+
+
+def test_automatic_precision_picks_by_size(gpu_ctx):
+    """precision 2: FP64 for a small transform (every q counted as FP64), tensor cores for a large one."""
+    g = load_golden("random0_ffavg")
+    h = manager_for(g, gpu_ctx).calculate_all()
+    h.precision, h.tolerance = 2, TOL
+    q = np.asarray(g["q"])
+    _, I2 = h.debye_transform(q)
+    assert gpu_ctx.fp64_columns() == len(q)
+    h.precision = 1
+    _, I1 = h.debye_transform(q)
+    np.testing.assert_array_equal(I2, I1)
+    rng = np.random.default_rng(8)
+    xyz = rng.normal(0, 25, (20000, 3))
+    m = hist.Molecule(atoms=xyz, ff_types=rng.choice([3, 7, 11], 20000).astype(np.int32),
+                      waters=rng.normal(0, 28, (2000, 3)), volume=20000 * 18.0)
+    h = hist.HistogramManagerMTFFAvg(m, True, 0.1, 8000, gpu_ctx).calculate_all()
+    h.precision, h.tolerance = 2, TOL
+    q = np.linspace(1e-4, 1.0, 1000)
+    _, I2 = h.debye_transform(q)
+    assert gpu_ctx.fp64_columns() < len(q)  # tensor cores kept most q
+    h.precision = 1
+    _, I1 = h.debye_transform(q)
+    np.testing.assert_allclose(I2, I1, rtol=TOL)
