@@ -153,10 +153,14 @@ def cfg0(seed: int = 1) -> Workload:
                     np.linspace(0.005, 0.5, 200), "ffavg")
 
 
-def cfg1(seed: int = 11) -> Workload:
-    m = _molecule(seed, 50000, 10000, rg=40.0, exv_width=1.0)
-    return Workload("cfg1: 50k atoms + 10k waters + 1 A grid exv, FFGrid, 0.1 A bins, 1000 q", [m], 0.1,
-                    np.linspace(0.005, 1.0, 1000), "ffgrid")
+def cfg1(seed: int = 11, atoms: int = 50000) -> Workload:
+    """atoms != 50000: the same composition and density (Rg ~ atoms^(1/3), waters atoms/5), for
+    profiling cases of the same kernels."""
+    rg = 40.0 * (atoms / 50000) ** (1.0 / 3.0)
+    m = _molecule(seed, atoms, atoms // 5, rg=rg, exv_width=1.0)
+    name = "cfg1: 50k atoms + 10k waters" if atoms == 50000 else f"cfg1 shape: {atoms} atoms + {atoms // 5} waters"
+    return Workload(name + " + 1 A grid exv, FFGrid, 0.1 A bins, 1000 q", [m], 0.1, np.linspace(0.005, 1.0, 1000),
+                    "ffgrid")
 
 
 def cfg2(seed: int = 21, subunit: int = 8333) -> Workload:

@@ -57,13 +57,16 @@ def load_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
-def workload(name: str, subunit: int = 0):
+def workload(name: str, subunit: int = 0, atoms: int = 0):
     """subunit (cfg2 only): atoms per icosahedral subunit; smaller shells keep the radius and bin count
-    of the full shell (profiling cases)."""
+    of the full shell.  atoms (cfg1 only): a globule of the same composition and density.  Both are
+    profiling cases."""
     from ausaxs_b200 import synth
 
     if name == "cfg2" and subunit:
         return synth.cfg2(subunit=subunit)
+    if name == "cfg1" and atoms:
+        return synth.cfg1(atoms=atoms)
     return {"cfg0": synth.cfg0, "cfg1": synth.cfg1, "cfg2": synth.cfg2, "cfg3": synth.cfg3}[name]()
 
 
@@ -511,7 +514,7 @@ def run_ours(args, rank, world, local_rank):
     stream = torch.cuda.Stream(local_rank)
     ctx = _capi.Context(local_rank)
     ctx.set_stream(stream.cuda_stream)
-    wl = workload(args.workload, args.subunit)
+    wl = workload(args.workload, args.subunit, args.atoms)
     m = wl.molecules[0]
     grid = wl.manager == "ffgrid"
     mgr = (HistogramManagerMTFFGrid(m, wl.bin_width, wl.bin_count, ctx) if grid
@@ -1170,6 +1173,7 @@ def main():
     ap.add_argument("--hbm-budget-gb", type=float, default=40.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--subunit", type=int, default=0, help="cfg2: atoms per subunit (default 8333; smaller for profiling)")
+    ap.add_argument("--atoms", type=int, default=0, help="cfg1: atoms of the globule (default 50000; smaller for profiling)")
     ap.add_argument("--precision", type=int, default=2, choices=[0, 1, 2],
                     help="Debye transform: 0 tensor cores, 1 FP64, 2 automatic (tensor cores from 8e6 row x bin x q)")
     ap.add_argument("--tolerance", type=float, default=1e-4)
