@@ -31,7 +31,9 @@ import numpy as np  # noqa: E402
 # thread instructions per pair of the pair kernel and its DRAM bytes per profile, from an ncu capture
 # (--set full) of the three pair launches of the 50k-atom FFGrid profile
 INSTR_PER_PAIR = 39.8
-PAIR_TRAFFIC_BYTES = 7.3e6
+# DRAM bytes (read + write) of the three pair launches of one 50k-atom FFGrid profile: 3.12 MB measured
+# by ncu on the cfg1-shaped 10k-atom case (85,967 points), scaled by points to cfg1's 436,380
+PAIR_TRAFFIC_BYTES = 1.58e7
 METRIC = "I(q) profiles/s & p99 latency vs plain GPU path at ≤1e-4 rel. I(q) error"
 UNIT = "profiles/s"
 
@@ -606,9 +608,10 @@ def run_ours(args, rank, world, local_rank):
     sm_mhz = clocks.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
     sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
     # The pair kernel is bound by instruction issue (its inputs live in shared memory; DRAM traffic is
-    # ~7 MB per profile).  Issue peak: every SM sub-partition issues one warp instruction per cycle;
+    # ~16 MB per profile).  Issue peak: every SM sub-partition issues one warp instruction per cycle;
     # INSTR_PER_PAIR thread instructions per pair evaluation were counted by ncu
-    # (smsp__inst_executed.sum x 32 / pairs, one-row launch of the 50k-atom FFGrid profile).
+    # (smsp__inst_executed.sum x 32 / pairs, one-row launch of the FFGrid histograms; 39.9 on the
+    # cfg1-shaped 10k-atom case).
     issue_peak = sms * 4 * sm_mhz * 1e6 * 32 / INSTR_PER_PAIR
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -627,7 +630,7 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": int(launches),
         "roofline": {"bound": "issue", "kernel": "pairhist_kernel", "achieved": pair_rate / 1e9,
                      "peak": issue_peak / 1e9, "unit": "Gpair/s", "frac": pair_rate / issue_peak,
-                     "traffic": PAIR_TRAFFIC_BYTES if wl.name.startswith("cfg1") else None,
+                     "traffic": PAIR_TRAFFIC_BYTES if wl.name.startswith("cfg1:") else None,
                      "peak_source": f"issue model: {sms} SMs x 4 x {sm_mhz:.0f} MHz x 32 / {INSTR_PER_PAIR} instr per pair",
                      "kernel_ms_per_step": kernel_ms, "kernel_launches_per_step": k_n / args.steps,
                      "hbm_frac": (PAIR_TRAFFIC_BYTES / (kernel_ms / 1e3)) / (peaks["hbm_gbs"] * 1e9),
