@@ -353,6 +353,132 @@ def profile(manager: _Manager, q, cw=1.0, cx=1.0, crho=1.0, dw_atomic=0.0, dw_ex
     return (I, prof.reshape(6, len(q))) if with_profiles else I
 
 
+def combine_partials(self_aa, cross_aa, aw, ww, bin_width: float) -> dict:
+    """PartialHistogramManagerMT::calculate / calculate_all (PartialHistogramManagerMT.cpp:152-252): the
+    master is the sum of every partial (its base is zero), p_tot = master truncated to max_bin (last
+    non-zero value, at least 10), aa = self + cross partials, aw = water partials, ww, and the weighted
+    axis of the master (WeightedDistribution1D.cpp:51-58, bin 0 pinned to 0).  Each partial is a
+    (value, count, distance sum) triple of equal-length arrays."""
+    parts = list(self_aa) + list(cross_aa) + list(aw) + ([ww] if ww is not None else [])
+    n = len(parts[0][0])
+    value, count, dsum = (np.zeros(n) for _ in range(3))
+    for v, c, d in parts:
+        value += v
+        count += c
+        dsum += d
+    nz = np.nonzero(value[10:])[0]
+    mb = int(nz[-1]) + 11 if len(nz) else 10
+    aa = sum(v for v, _, _ in list(self_aa) + list(cross_aa))
+    aw_v = sum((v for v, _, _ in aw), np.zeros(n))
+    ww_v = ww[0] if ww is not None else np.zeros(n)
+    width = (mb * bin_width) / mb  # Axis(0, mb * width, mb).width()
+    cnt = count[:mb].astype(np.uint64).astype(np.uint32).astype(np.float64)
+    bc = dsum[:mb]
+    d_axis = ((bc == 0) * (np.arange(mb) * width) + bc) / ((cnt == 0) + cnt)
+    d_axis[0] = 0.0
+    return {"aa": aa[:mb].copy(), "aw": aw_v[:mb].copy(), "ww": ww_v[:mb].copy(), "tot": value[:mb].copy(),
+            "d_axis": d_axis, "max_bin": mb}
+
+
+class PartialHistogramManagerMT:
+    """PartialHistogramManagerMT (source/core/hist/histogram_manager/PartialHistogramManagerMT.cpp:42-252)
+    over the device SimpleCalculator: the partial histograms of every body (self), every pair of bodies
+    (cross) and every body with the waters are kept; calculate_all() recomputes only those of bodies
+    whose coordinates changed since the last call (a rigid move leaves a body's self partial as it was,
+    as the reference does) and returns the composite of their sum.  The waters are the hydration of
+    body `water_owner` and move with it (Body::rotate / Body::translate, Body.cpp:135-156, which then
+    signal a modified hydration: the water self partial and every body-water partial are recomputed).
+    bodies: [(xyz [n, 3], weights [n])]; waters: (xyz [m, 3], weights [m]) or None."""
+
+    def __init__(self, bodies, waters=None, bin_width: float = 0.25, bin_count: int = 8000,
+                 ctx: Optional[_capi.Context] = None, water_owner: int = 0):
+        self.ctx = ctx or _capi.default_context()
+        self.bin_width, self.bin_count = bin_width, bin_count
+        self.xyz = [np.array(x, np.float64).reshape(-1, 3) for x, _ in bodies]
+        self.records = [pack(x, w, False) for x, w in bodies]
+        self.water_owner = water_owner
+        self.water_xyz = None
+        self.waters = None
+        if waters is not None and len(waters[0]):
+            self.water_xyz = np.array(waters[0], np.float64).reshape(-1, 3)
+            self.waters = pack(self.water_xyz, waters[1], False)
+        B = len(self.records)
+        self.moved = [True] * B          # externally modified (initially every partial is computed)
+        self.internal = [True] * B       # internally modified: the self partial is recomputed
+        self.water_changed = self.waters is not None
+        self.self_p, self.aw_p = [None] * B, [None] * B
+        self.cross_p = {}
+        self.ww_p = None
+
+    def set_body_coordinates(self, k: int, xyz, internal: bool = False):
+        """New coordinates of body k (a rigid move unless `internal`, which also recomputes its self partial)."""
+        self.xyz[k] = np.array(xyz, np.float64).reshape(-1, 3)
+        self.records[k] = pack(self.xyz[k], self.records[k][:, 3].copy(), False)
+        self.moved[k] = True
+        self.internal[k] = self.internal[k] or internal
+
+    def set_water_coordinates(self, xyz):
+        """New coordinates of the waters (a modified hydration)."""
+        self.water_xyz = np.array(xyz, np.float64).reshape(-1, 3)
+        self.waters = pack(self.water_xyz, self.waters[:, 3].copy(), False)
+        self.water_changed = True
+
+    @staticmethod
+    def _rigid(xyz, R, t):
+        # Body::rotate then Body::translate: x <- R x (row sums left to right, Vector3.h:169-181), then x + t
+        R = np.asarray(R, np.float64).reshape(3, 3)
+        t = np.asarray(t, np.float64).reshape(3)
+        x, y, z = xyz[:, 0], xyz[:, 1], xyz[:, 2]
+        rot = np.column_stack([R[i, 0] * x + R[i, 1] * y + R[i, 2] * z for i in range(3)])
+        return rot + t
+
+    def move_body(self, k: int, R, t):
+        """Rigid move x <- R x + t of body k, and of the waters when body k holds them."""
+        self.set_body_coordinates(k, self._rigid(self.xyz[k], R, t))
+        if self.waters is not None and k == self.water_owner:
+            self.set_water_coordinates(self._rigid(self.water_xyz, R, t))
+
+    def calculate_all(self) -> "CompositeDistanceHistogram":
+        B = len(self.records)
+        calc = _capi.Calculator(self.ctx, self.bin_width, self.bin_count)
+        jobs = []  # (kind, key) in enqueue order; merge ids: self k, cross i*B+j, water B*B+k, ww B*B+B
+        for k in range(B):
+            if self.internal[k]:
+                calc.enqueue_calculate_self(self.records[k], 1, k)
+                jobs.append(("self", k))
+        if self.waters is not None and self.water_changed:
+            calc.enqueue_calculate_self(self.waters, 1, B * B + B)
+            jobs.append(("ww", None))
+        for i in range(B):
+            for j in range(i):
+                if self.moved[i] or self.moved[j]:
+                    calc.enqueue_calculate_cross(self.records[i], self.records[j], 1, i * B + j)
+                    jobs.append(("cross", (i, j)))
+            if self.waters is not None and (self.moved[i] or self.water_changed):
+                calc.enqueue_calculate_cross(self.records[i], self.waters, 1, B * B + i)
+                jobs.append(("aw", i))
+        res = calc.run()
+        calc.close()
+        for kind, key in jobs:
+            if kind == "self":
+                self.self_p[key] = res["self"][key]
+            elif kind == "ww":
+                self.ww_p = res["self"][B * B + B]
+            elif kind == "cross":
+                self.cross_p[key] = res["cross"][key[0] * B + key[1]]
+            else:
+                self.aw_p[key] = res["cross"][B * B + key]
+        self.moved = [False] * B
+        self.internal = [False] * B
+        self.water_changed = False
+        r = combine_partials(self.self_p, list(self.cross_p.values()), [p for p in self.aw_p if p is not None],
+                             self.ww_p, self.bin_width)
+        cfg = HistConfig(_capi.MANAGER_MT, 1, float(self.bin_width), int(self.bin_count), 0.0)
+        n = r["max_bin"]
+        res = {"max_bin": n, "pairs": 0, "aa": r["aa"], "aw": r["aw"], "ww": r["ww"], "tot": r["tot"], "d_axis": r["d_axis"]}
+        return CompositeDistanceHistogram(cfg, res, self.ctx)
+
+
 class BatchedProfiles:
     """Profiles of many independent molecules at once (ausaxs_gpu_batch_*): for every molecule the
     result of ``HistogramManagerMTFFAvg(m).calculate_all()->debye_transform()`` (or FFGrid), from

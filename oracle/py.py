@@ -307,6 +307,7 @@ def ref(threads: int = 0):
         R.ref_molecule_new.argtypes = [_f64p, C.c_int, _f64p, C.c_int, _i32p, C.c_int, C.c_double]
         R.ref_molecule_free.argtypes = [vp]
         R.ref_body_move.argtypes = [vp, C.c_int, _f64p, _f64p]
+        R.ref_body_coords.argtypes = [vp, C.c_int, C.c_void_p, C.POINTER(C.c_int)]
         R.ref_manager_set.argtypes = [vp, C.c_int, C.c_int, _f64p, C.c_int]
         R.ref_manager_calculate.restype = vp
         R.ref_manager_calculate.argtypes = [vp, C.POINTER(C.c_double)]
@@ -369,6 +370,16 @@ class RefMolecule:
         x = np.zeros(3) if exv_xyz is None or len(exv_xyz) == 0 else np.ascontiguousarray(np.asarray(exv_xyz, np.float64).reshape(-1))
         nx = 0 if exv_xyz is None else len(exv_xyz)
         _check(R, R.ref_manager_set(self.h, MANAGERS[name], int(weighted_bins), x, nx))
+
+    def body_coords(self, body):
+        """The body's current atom coordinates (after any moves), [n, 3] float64; body = -1: the
+        molecule's waters, which their owning body carries along when it moves."""
+        R = ref()
+        n = C.c_int(0)
+        _check(R, R.ref_body_coords(self.h, body, None, C.byref(n)))
+        out = np.zeros((max(1, n.value), 3))
+        _check(R, R.ref_body_coords(self.h, body, out.ctypes.data, C.byref(n)))
+        return out[:n.value]
 
     def move_body(self, body, Rm, t):
         R = ref()

@@ -305,6 +305,26 @@ int ref_body_move(void* m, int body, const double* R, const double* t) {
     });
 }
 
+// The current coordinates of a body's atoms, or with body = -1 of the molecule's waters (which the
+// bodies own and move with them, Body.cpp:135-156): n x 3 doubles; out may be null to query n.
+int ref_body_coords(void* m, int body, double* out, int* n) {
+    return guarded([&] {
+        auto* mol = static_cast<FixedVolumeMolecule*>(m);
+        auto put = [&](const auto& items) {
+            *n = static_cast<int>(items.size());
+            if (!out) return;
+            for (size_t i = 0; i < items.size(); ++i) {
+                const auto& c = items[i].coordinates();
+                out[3 * i] = c.x();
+                out[3 * i + 1] = c.y();
+                out[3 * i + 2] = c.z();
+            }
+        };
+        if (body < 0) put(mol->get_waters());
+        else put(mol->get_body(body).get_atoms());
+    });
+}
+
 // manager: 0 HistogramManager (1 thread), 1 HistogramManagerMT, 2 MTFFAvg,
 // 3 MTFFExplicit, 4 MTFFGrid (exv dummies given), 5 PartialHistogramManagerMT.
 // The manager is installed in the molecule (Molecule::set_histogram_manager,

@@ -17,7 +17,9 @@ reference's default q axis.  Cases:
                 reference's reader (united-atom form-factor types);
 * ``gridexv_*``: RawGridExv dummies and grid volumes;
 * ``fit_*``   : SmartFitter::fit with the Golden minimiser over one parameter, on synthetic data on
-                the model's own q axis.
+                the model's own q axis;
+* ``calc_*``  : SimpleCalculator job lists (scaling factors, merge ids);
+* ``partial_*``: PartialHistogramManagerMT over a multi-body molecule, initially and after rigid moves.
 """
 from __future__ import annotations
 
@@ -112,6 +114,41 @@ def calc_case(name, sets, jobs, bin_width):
     print(name, "results", len(keys), "bins", last)
 
 
+def rotation(axis, angle):
+    axis = np.asarray(axis, float) / np.linalg.norm(axis)
+    K = np.array([[0, -axis[2], axis[1]], [axis[2], 0, -axis[0]], [-axis[1], axis[0], 0]])
+    return np.eye(3) + np.sin(angle) * K + (1 - np.cos(angle)) * K @ K
+
+
+def partial_case(name, bodies, ws, waters, ww, moves, bin_width):
+    """PartialHistogramManagerMT over a multi-body molecule: calculate_all() initially and after each
+    rigid move (body, R, t); per step the bodies' and the waters' coordinates (the waters belong to a
+    body and move with it) and the composite histogram."""
+    O.ref_set_axes(bin_width, 8000, 1e-4, 0.5)
+    O.ref_set_simple_exv(False)
+    xyz = np.concatenate(bodies)
+    m = O.RefMolecule(xyz, np.concatenate(ws), np.full(len(xyz), 3), waters, ww, body_sizes=[len(b) for b in bodies],
+                      volume=18.0 * len(xyz))
+    m.set_manager("partial")
+    out = dict(weights=np.concatenate(ws), body_sizes=np.array([len(b) for b in bodies], np.int32), waters=waters, ww=ww,
+               bin_width=bin_width, manager="partial", moves=np.array([k for k, _, _ in moves], np.int32),
+               move_R=np.array([R for _, R, _ in moves]), move_t=np.array([t for _, _, t in moves]))
+    for step in range(len(moves) + 1):
+        if step:
+            k, Rm, t = moves[step - 1]
+            m.move_body(k, Rm, t)
+        h = m.calculate()
+        coords = np.concatenate([m.body_coords(b) for b in range(len(bodies))])
+        aa, aw, ww_h = h.simple()
+        tot, d = h.total()
+        out[f"coords{step}"] = coords
+        out[f"waters{step}"] = m.body_coords(-1)
+        for key, v in (("aa", aa), ("aw", aw), ("ww", ww_h), ("tot", tot), ("d_axis", d)):
+            out[f"{key}{step}"] = v
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, "steps", len(moves) + 1, "bins", len(out["d_axis0"]))
+
+
 def main():
     O.ref()
     # SimpleCube: 8 corners + centre as atoms (carbon), 8 corner waters
@@ -186,6 +223,16 @@ def main():
     waters = pts(80, 16.0)
     calc_case("calc_cyclic5", copies + [waters], [(0, None, 5, 0), (0, 1, 5, 0), (0, 2, 5, 0)] +
               [(5, k, 1, 1) for k in range(5)] + [(5, None, 1, 2)], 0.1)
+    # PartialHistogramManagerMT: four bodies, waters, two rigid moves (seeded stream of its own)
+    prng = np.random.default_rng(13)
+    bodies = [prng.normal(c, 4.0, (n, 3)) for c, n in (((0, 0, 0), 180), ((12, 0, 0), 120), ((0, 13, 2), 150),
+                                                         ((-9, -8, 5), 90))]
+    ws = [prng.uniform(4.0, 9.0, len(b)) for b in bodies]
+    waters = prng.normal(0, 12, (70, 3))
+    ww = np.full(70, 8.999659)
+    moves = [(2, rotation((1, 2, 0.5), 0.07), np.array([0.8, -1.1, 0.4])),
+             (0, rotation((0.2, -1, 1), 0.05), np.array([-0.5, 0.3, 1.2]))]
+    partial_case("partial_random_4bodies", bodies, ws, waters, ww, moves, 0.25)
     # SmartFitter fits with the Golden minimiser, one parameter each (seeded noise streams of their own)
     frng = np.random.default_rng(7)
     xyz = frng.normal(0, 9, (400, 3))
