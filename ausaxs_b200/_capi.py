@@ -35,7 +35,10 @@ EXPORTED = [
     "ausaxs_gpu_ctx_fp64_columns", "ausaxs_gpu_ctx_tc_error_estimate", "ausaxs_gpu_histogram", "ausaxs_gpu_debye", "ausaxs_gpu_profile",
     "ausaxs_gpu_structure_create", "ausaxs_gpu_structure_destroy", "ausaxs_gpu_structure_profile",
     "ausaxs_gpu_structure_histogram", "ausaxs_gpu_histogram_mt_noalloc", "ausaxs_gpu_linear_lsq", "ausaxs_gpu_grid_exv",
-    "ausaxs_gpu_fit", "ausaxs_gpu_structure_fit",
+    "ausaxs_gpu_fit", "ausaxs_gpu_structure_fit", "ausaxs_gpu_hydrate", "ausaxs_gpu_hydrate_device", "ausaxs_hydrate_axes",
+    "ausaxs_gpu_ctx_hydration_stats",
+    "ausaxs_gpu_hydration_grid_create", "ausaxs_gpu_hydration_grid_destroy", "ausaxs_gpu_hydration_grid_add",
+    "ausaxs_gpu_hydration_grid_remove", "ausaxs_gpu_hydration_grid_hydrate",
     "ausaxs_gpu_calculator_create", "ausaxs_gpu_calculator_destroy", "ausaxs_gpu_calculator_enqueue_self",
     "ausaxs_gpu_calculator_enqueue_cross", "ausaxs_gpu_calculator_run", "ausaxs_gpu_calculator_result_ids",
     "ausaxs_gpu_calculator_result",
@@ -160,6 +163,17 @@ def load():
         L.ausaxs_gpu_server_body_center.argtypes = [vp, C.c_int32, C.c_int32, f64]
         L.ausaxs_gpu_server_coordinates.argtypes = [vp, C.c_int32, f32, f32]
         L.ausaxs_gpu_server_histogram.argtypes = [vp, C.c_int32, C.POINTER(HistResult)]
+        L.ausaxs_gpu_hydrate.argtypes = [vp, f64, i32, C.c_int64, f64, f64, C.c_uint64, f64, C.c_int64, i64, i64, i32]
+        L.ausaxs_hydrate_axes.argtypes = [f64, C.c_int64, f64]
+        L.ausaxs_gpu_ctx_hydration_stats.argtypes = [vp, i64, i32]
+        L.ausaxs_gpu_hydrate_device.argtypes = [vp, f64, i32, C.c_int64, f64, f64, C.c_uint64, f64, C.c_int64, i64, i64,
+                                                i32]
+        L.ausaxs_gpu_hydration_grid_create.argtypes = [vp, f64, C.POINTER(vp)]
+        L.ausaxs_gpu_hydration_grid_destroy.argtypes = [vp]
+        L.ausaxs_gpu_hydration_grid_add.argtypes = [vp, f64, i32, C.c_int64]
+        L.ausaxs_gpu_hydration_grid_remove.argtypes = [vp, f64, i32, C.c_int64]
+        L.ausaxs_gpu_hydration_grid_hydrate.argtypes = [vp, f64, i32, C.c_int64, f64, C.c_uint64, f64, C.c_int64, i64,
+                                                        i64, i32]
         _lib = L
         return L
 
@@ -275,6 +289,118 @@ def grid_exv_device(ctx: "Context", atoms_dev, n_atoms: int, waters_dev, n_water
     check(load().ausaxs_gpu_grid_exv(ctx.h, devptr(atoms_dev, C.c_float), n_atoms, devptr(waters_dev, C.c_float),
                                      n_waters, 0, devptr(out_dev, C.c_float), capacity, C.byref(n), C.byref(vol)))
     return n.value, vol.value
+
+
+HYDRATE_DIRECTIONS = 26
+
+
+def hydrate_axes(atoms) -> np.ndarray:
+    """The axes Grid(bodies) builds around the atoms for the hydration: {min x, y, z, bins x, y, z}."""
+    a = np.ascontiguousarray(np.asarray(atoms, np.float64).reshape(-1, 3))
+    out = np.zeros(6)
+    check(load().ausaxs_hydrate_axes(fptr(a, C.c_double), len(a), fptr(out, C.c_double)))
+    return out
+
+
+def _hydrate_inputs(atoms, ff_types, noise):
+    a = np.ascontiguousarray(np.asarray(atoms, np.float64).reshape(-1, 3))
+    f = np.ascontiguousarray(np.asarray(ff_types, np.int32).reshape(-1))
+    nz = None
+    if noise is not None:
+        nz = np.zeros((HYDRATE_DIRECTIONS * len(a), 3))
+        src = np.asarray(noise, np.float64).reshape(-1, 3)[: len(nz)]
+        nz[: len(src)] = src
+    return a, f, nz
+
+
+def _hydrate_call(fn, a, nz):
+    """Runs fn(out, cap, n, cand, rounds) with a growing capacity; returns (waters, candidates, rounds)."""
+    n = C.c_int64(0)
+    rounds = C.c_int32(0)
+    cap = max(1024, 2 * len(a))
+    while True:
+        out = np.zeros((cap, 3))
+        cand = np.zeros(cap, np.int64)
+        rc = fn(fptr(out, C.c_double), cap, C.byref(n), fptr(cand, C.c_int64), C.byref(rounds))
+        if rc == ERR_CAPACITY and n.value > cap:
+            cap = n.value
+            continue
+        check(rc)
+        return out[: n.value], cand[: n.value], rounds.value
+
+
+def hydration_stats(ctx: "Context"):
+    """(candidates that passed the static tests, rounds) of the context's last hydration."""
+    s, r = C.c_int64(0), C.c_int32(0)
+    check(load().ausaxs_gpu_ctx_hydration_stats(ctx.h, C.byref(s), C.byref(r)))
+    return s.value, r.value
+
+
+def hydrate_device(ctx: "Context", atoms_dev, ff_dev, n_atoms: int, axes, out_dev, capacity: int, cand_dev=None,
+                   noise_dev=None, seed: int = 0):
+    """ausaxs_gpu_hydrate_device: device atoms (n x 3 double), types (int32), optional noise table;
+    writes the waters (and candidate indices) into device buffers.  Returns (count, rounds)."""
+    ax = np.ascontiguousarray(np.asarray(axes, np.float64)[:6])
+    n = C.c_int64(0)
+    rounds = C.c_int32(0)
+    check(load().ausaxs_gpu_hydrate_device(
+        ctx.h, devptr(atoms_dev, C.c_double), devptr(ff_dev, C.c_int32), n_atoms, fptr(ax, C.c_double),
+        None if noise_dev is None else devptr(noise_dev, C.c_double), int(seed), devptr(out_dev, C.c_double), capacity,
+        C.byref(n), None if cand_dev is None else devptr(cand_dev, C.c_int64), C.byref(rounds)))
+    return n.value, rounds.value
+
+
+class HydrationGrid:
+    """A hydration grid kept on the device across calls (ausaxs_gpu_hydration_grid_*), as the reference
+    keeps a molecule's grid::Grid between rigid-body steps: add(atoms, ff) = Grid::add with the volume
+    expansion, remove(atoms, ff) = Grid::remove of atoms at those (current) coordinates, hydrate(atoms,
+    ff, noise, seed) = RadialHydration over the grid's members in the order given."""
+
+    def __init__(self, ctx: "Context", axes):
+        self.ctx = ctx
+        self.axes = np.ascontiguousarray(np.asarray(axes, np.float64)[:6])
+        h = C.c_void_p()
+        check(load().ausaxs_gpu_hydration_grid_create(ctx.h, fptr(self.axes, C.c_double), C.byref(h)))
+        self.h = h
+
+    def add(self, atoms, ff_types):
+        a, f, _ = _hydrate_inputs(atoms, ff_types, None)
+        check(load().ausaxs_gpu_hydration_grid_add(self.h, fptr(a, C.c_double), fptr(f, C.c_int32), len(a)))
+
+    def remove(self, atoms, ff_types):
+        a, f, _ = _hydrate_inputs(atoms, ff_types, None)
+        check(load().ausaxs_gpu_hydration_grid_remove(self.h, fptr(a, C.c_double), fptr(f, C.c_int32), len(a)))
+
+    def hydrate(self, atoms, ff_types, noise=None, seed: int = 0):
+        a, f, nz = _hydrate_inputs(atoms, ff_types, noise)
+        L = load()
+        return _hydrate_call(lambda out, cap, n, cand, rounds: L.ausaxs_gpu_hydration_grid_hydrate(
+            self.h, fptr(a, C.c_double), fptr(f, C.c_int32), len(a), fptr(nz, C.c_double), int(seed), out, cap, n,
+            cand, rounds), a, nz)
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().ausaxs_gpu_hydration_grid_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def hydrate(ctx: "Context", atoms, ff_types, axes=None, noise=None, seed: int = 0):
+    """RadialHydration on a fresh grid on the device (ausaxs_gpu_hydrate): waters [m, 3] (double) in the
+    reference's order, their candidate indices (atom * 26 + direction) and the rounds the device
+    took.  atoms in the order the generator visits them; noise: [n * 26, 3] displacements or None
+    (then seed != 0 draws Gaussian ones of sigma 0.75 A on the device)."""
+    a, f, nz = _hydrate_inputs(atoms, ff_types, noise)
+    ax = None if axes is None else np.ascontiguousarray(np.asarray(axes, np.float64)[:6])
+    L = load()
+    return _hydrate_call(lambda out, cap, n, cand, rounds: L.ausaxs_gpu_hydrate(
+        ctx.h, fptr(a, C.c_double), fptr(f, C.c_int32), len(a), fptr(ax, C.c_double), fptr(nz, C.c_double),
+        int(seed), out, cap, n, cand, rounds), a, nz)
 
 
 class Calculator:

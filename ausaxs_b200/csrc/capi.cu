@@ -7,6 +7,7 @@
 #include "engine.cuh"
 #include "fit.cuh"
 #include "gridexv.cuh"
+#include "hydrate.cuh"
 #include "guard.cuh"
 #include "lsq.cuh"
 
@@ -138,6 +139,105 @@ namespace ausaxs_b200 {
 void set_last_error(const char* msg) { g_last_error = msg; }
 }  // namespace ausaxs_b200
 
+struct ausaxs_gpu_hydration_grid {
+    ausaxs_gpu_ctx* ctx = nullptr;
+    double gmin[3] = {0, 0, 0};
+    int bins[3] = {0, 0, 0};
+    DevBuf cells;  // cell states, then an error word
+    DevBuf stage;  // atoms and types of add / remove calls
+    size_t cell_bytes = 0;
+};
+
+namespace {
+// form-factor types with a radius (get_vdw_radius(form_factor_t) throws for EXCLUDED_VOLUME, COUNT and
+// unknown values), finite coordinates, and (axes given) every atom's cell inside the grid
+void check_hydration_atoms(const double* atoms, const int32_t* ff, int64_t n, const double* gmin, const int* bins) {
+    for (int64_t a = 0; a < n; ++a) {
+        const int32_t f = ff[a];
+        if (f < 1 || f > 16 || f == 15) throw Error{AUSAXS_ERR_FORM_FACTOR, "form-factor type without a radius"};
+        for (int d = 0; d < 3; ++d) {
+            if (!std::isfinite(atoms[3 * a + d])) throw Error{AUSAXS_ERR_ARGUMENT, "non-finite atom coordinate"};
+            if (gmin) {
+                const double b = std::round(atoms[3 * a + d] - gmin[d]);
+                if (!(b >= 0 && b < bins[d])) throw Error{AUSAXS_ERR_ARGUMENT, "an atom lies outside the hydration grid"};
+            }
+        }
+    }
+}
+
+void read_axes(const double* axes, double gmin[3], int bins[3]) {
+    for (int d = 0; d < 3; ++d) {
+        gmin[d] = axes[d];
+        bins[d] = (int)axes[3 + d];
+        if (!std::isfinite(axes[d]) || !(axes[3 + d] >= 1 && axes[3 + d] < 2147483647.0) || axes[3 + d] != (double)bins[d])
+            throw Error{AUSAXS_ERR_ARGUMENT, "invalid hydration grid axes"};
+    }
+    hydration_cells_check(gmin, bins);
+}
+
+Hydrator& hydrator(Ctx& C) {
+    if (!C.hyd) C.hyd = std::make_shared<Hydrator>();
+    return *C.hyd;
+}
+
+// atoms, types and noise into the hydrator's input buffer
+void stage_hydration_inputs(Ctx& C, Hydrator& H, const double* atoms, const int32_t* ff, int64_t n, const double* noise,
+                            double** d_atoms, int32_t** d_ff, double** d_noise) {
+    const size_t a_bytes = align_up((size_t)n * 24, 256), f_bytes = align_up((size_t)n * 4, 256);
+    const size_t n_bytes = noise ? (size_t)n * AUSAXS_HYDRATE_DIRECTIONS * 24 : 0;
+    H.in.ensure(a_bytes + f_bytes + n_bytes + 256);
+    *d_atoms = H.in.as<double>();
+    *d_ff = H.in.as<int32_t>(a_bytes);
+    *d_noise = noise ? H.in.as<double>(a_bytes + f_bytes) : nullptr;
+    if (n) {
+        AUSAXS_CUDA(cudaMemcpyAsync(*d_atoms, atoms, (size_t)n * 24, cudaMemcpyHostToDevice, C.stream));
+        AUSAXS_CUDA(cudaMemcpyAsync(*d_ff, ff, (size_t)n * 4, cudaMemcpyHostToDevice, C.stream));
+        if (noise) AUSAXS_CUDA(cudaMemcpyAsync(*d_noise, noise, n_bytes, cudaMemcpyHostToDevice, C.stream));
+    }
+}
+
+void read_waters(Ctx& C, Hydrator& H, double* waters_out, int64_t capacity, int64_t* n_waters, int64_t* candidates_out,
+                 int32_t* rounds) {
+    *n_waters = H.count;
+    if (rounds) *rounds = H.rounds;
+    if (capacity > 0 && H.count > 0) {
+        if (capacity < H.count) throw Error{AUSAXS_ERR_CAPACITY, "waters_out holds fewer waters than were placed"};
+        AUSAXS_CUDA(cudaMemcpyAsync(waters_out, H.waters(), (size_t)H.count * 24, cudaMemcpyDeviceToHost, C.stream));
+        if (candidates_out)
+            AUSAXS_CUDA(cudaMemcpyAsync(candidates_out, H.candidates(), (size_t)H.count * 8, cudaMemcpyDeviceToHost, C.stream));
+    }
+    AUSAXS_CUDA(cudaStreamSynchronize(C.stream));
+}
+
+bool bad_hydrate_args(const double* atoms, const int32_t* ff, int64_t n, double* waters_out, int64_t capacity,
+                      int64_t* n_waters) {
+    return !n_waters || n < 0 || (n && (!atoms || !ff)) || capacity < 0 || (capacity > 0 && !waters_out);
+}
+}  // namespace
+
+namespace {
+int hydration_grid_edit(ausaxs_gpu_hydration_grid* g, const double* atoms, const int32_t* ff, int64_t n, bool add) {
+    return guarded([&] {
+        if (!g || n < 0 || (n && (!atoms || !ff))) throw Error{AUSAXS_ERR_ARGUMENT, "invalid argument"};
+        check_hydration_atoms(atoms, ff, n, g->gmin, g->bins);
+        if (!n) return;
+        Ctx& C = g->ctx->impl;
+        AUSAXS_CUDA(cudaSetDevice(C.device));
+        const size_t a_bytes = align_up((size_t)n * 24, 256);
+        g->stage.ensure(a_bytes + align_up((size_t)n * 4, 256));
+        double* d_atoms = g->stage.as<double>();
+        int32_t* d_ff = g->stage.as<int32_t>(a_bytes);
+        AUSAXS_CUDA(cudaMemcpyAsync(d_atoms, atoms, (size_t)n * 24, cudaMemcpyHostToDevice, C.stream));
+        AUSAXS_CUDA(cudaMemcpyAsync(d_ff, ff, (size_t)n * 4, cudaMemcpyHostToDevice, C.stream));
+        int* err = g->cells.as<int>(g->cell_bytes);
+        if (add) hydration_add(C, g->cells.as<uint8_t>(), g->gmin, g->bins, d_atoms, d_ff, n, err);
+        else hydration_remove(C, g->cells.as<uint8_t>(), g->gmin, g->bins, d_atoms, d_ff, n, err);
+        // the staging buffer is reused by the next call: let this one finish with it
+        AUSAXS_CUDA(cudaStreamSynchronize(C.stream));
+    });
+}
+}  // namespace
+
 extern "C" {
 
 const char* ausaxs_gpu_last_error(void) { return g_last_error.c_str(); }
@@ -215,7 +315,7 @@ int ausaxs_gpu_ctx_enable_timing(ausaxs_gpu_ctx* ctx, int32_t enable) {
 
 int ausaxs_gpu_ctx_kernel_time(ausaxs_gpu_ctx* ctx, int32_t kernel_class, double* ms, int64_t* launches) {
     return guarded([&] {
-        if (!ctx || kernel_class < 0 || kernel_class > 4) throw Error{AUSAXS_ERR_ARGUMENT, "bad argument"};
+        if (!ctx || kernel_class < 0 || kernel_class > 5) throw Error{AUSAXS_ERR_ARGUMENT, "bad argument"};
         Ctx& C = ctx->impl;
         C.time_collect();
         if (ms) *ms = C.timed[kernel_class].ms;
@@ -475,6 +575,140 @@ int ausaxs_gpu_grid_exv(ausaxs_gpu_ctx* ctx, const float* atoms, int32_t n_atoms
             AUSAXS_CUDA(cudaMemcpyAsync(exv_out, g.points.p, (size_t)g.count * 16, cudaMemcpyDeviceToHost, C.stream));
         }
         AUSAXS_CUDA(cudaStreamSynchronize(C.stream));
+    });
+}
+
+
+int ausaxs_hydrate_axes(const double* atoms, int64_t n_atoms, double* axes) {
+    return guarded([&] {
+        if (!axes || n_atoms < 0 || (n_atoms && !atoms)) throw Error{AUSAXS_ERR_ARGUMENT, "invalid argument"};
+        double gmin[3];
+        int bins[3];
+        hydrate_axes(atoms, n_atoms, gmin, bins);
+        for (int d = 0; d < 3; ++d) axes[d] = gmin[d], axes[3 + d] = bins[d];
+    });
+}
+
+
+// Hydration shell (RadialHydration) on a fresh grid: the atoms, types and noise table go to the
+// context's hydration workspace, the waters and their candidate indices come back.
+int ausaxs_gpu_hydrate(ausaxs_gpu_ctx* ctx, const double* atoms, const int32_t* ff_types, int64_t n_atoms,
+                       const double* axes, const double* noise, uint64_t noise_seed, double* waters_out,
+                       int64_t capacity, int64_t* n_waters, int64_t* candidates_out, int32_t* rounds) {
+    return guarded([&] {
+        if (!ctx || bad_hydrate_args(atoms, ff_types, n_atoms, waters_out, capacity, n_waters))
+            throw Error{AUSAXS_ERR_ARGUMENT, "invalid argument"};
+        *n_waters = 0;
+        if (rounds) *rounds = 0;
+        double gmin[3];
+        int bins[3];
+        if (axes) read_axes(axes, gmin, bins);
+        else hydrate_axes(atoms, n_atoms, gmin, bins);
+        check_hydration_atoms(atoms, ff_types, n_atoms, gmin, bins);
+        Ctx& C = ctx->impl;
+        AUSAXS_CUDA(cudaSetDevice(C.device));
+        Hydrator& H = hydrator(C);
+        double *d_atoms, *d_noise;
+        int32_t* d_ff;
+        stage_hydration_inputs(C, H, atoms, ff_types, n_atoms, noise, &d_atoms, &d_ff, &d_noise);
+        H.run(C, d_atoms, d_ff, n_atoms, gmin, bins, d_noise, noise ? 0ull : (unsigned long long)noise_seed);
+        read_waters(C, H, waters_out, capacity, n_waters, candidates_out, rounds);
+    });
+}
+
+// The same on device-resident atoms, types and noise, writing device buffers (no host staging).
+int ausaxs_gpu_hydrate_device(ausaxs_gpu_ctx* ctx, const double* atoms, const int32_t* ff_types, int64_t n_atoms,
+                              const double* axes, const double* noise, uint64_t noise_seed, double* waters_out,
+                              int64_t capacity, int64_t* n_waters, int64_t* candidates_out, int32_t* rounds) {
+    return guarded([&] {
+        if (!ctx || !axes || bad_hydrate_args(atoms, ff_types, n_atoms, waters_out, capacity, n_waters))
+            throw Error{AUSAXS_ERR_ARGUMENT, "invalid argument"};
+        *n_waters = 0;
+        if (rounds) *rounds = 0;
+        double gmin[3];
+        int bins[3];
+        read_axes(axes, gmin, bins);
+        Ctx& C = ctx->impl;
+        AUSAXS_CUDA(cudaSetDevice(C.device));
+        Hydrator& H = hydrator(C);
+        H.run(C, atoms, ff_types, n_atoms, gmin, bins, noise, noise ? 0ull : (unsigned long long)noise_seed);
+        *n_waters = H.count;
+        if (rounds) *rounds = H.rounds;
+        if (capacity > 0 && H.count > 0) {
+            if (capacity < H.count) throw Error{AUSAXS_ERR_CAPACITY, "waters_out holds fewer waters than were placed"};
+            AUSAXS_CUDA(cudaMemcpyAsync(waters_out, H.waters(), (size_t)H.count * 24, cudaMemcpyDeviceToDevice, C.stream));
+            if (candidates_out)
+                AUSAXS_CUDA(cudaMemcpyAsync(candidates_out, H.candidates(), (size_t)H.count * 8, cudaMemcpyDeviceToDevice,
+                                            C.stream));
+        }
+        AUSAXS_CUDA(cudaStreamSynchronize(C.stream));
+    });
+}
+
+int ausaxs_gpu_ctx_hydration_stats(ausaxs_gpu_ctx* ctx, int64_t* survivors, int32_t* rounds) {
+    return guarded([&] {
+        if (!ctx) throw Error{AUSAXS_ERR_ARGUMENT, "invalid argument"};
+        const Ctx& C = ctx->impl;
+        if (survivors) *survivors = C.hyd ? C.hyd->survivors : 0;
+        if (rounds) *rounds = C.hyd ? C.hyd->rounds : 0;
+    });
+}
+
+int ausaxs_gpu_hydration_grid_create(ausaxs_gpu_ctx* ctx, const double* axes, ausaxs_gpu_hydration_grid** out) {
+    return guarded([&] {
+        if (!ctx || !axes || !out) throw Error{AUSAXS_ERR_ARGUMENT, "invalid argument"};
+        *out = nullptr;
+        auto g = std::make_unique<ausaxs_gpu_hydration_grid>();
+        g->ctx = ctx;
+        read_axes(axes, g->gmin, g->bins);
+        Ctx& C = ctx->impl;
+        AUSAXS_CUDA(cudaSetDevice(C.device));
+        g->cell_bytes = align_up((size_t)g->bins[0] * g->bins[1] * g->bins[2], 256);
+        g->cells.ensure(g->cell_bytes + 256);
+        AUSAXS_CUDA(cudaMemsetAsync(g->cells.p, 0, g->cell_bytes + 8, C.stream));
+        AUSAXS_CUDA(cudaStreamSynchronize(C.stream));
+        *out = g.release();
+    });
+}
+
+int ausaxs_gpu_hydration_grid_destroy(ausaxs_gpu_hydration_grid* g) {
+    return guarded([&] {
+        if (!g) return;
+        AUSAXS_CUDA(cudaSetDevice(g->ctx->impl.device));
+        AUSAXS_CUDA(cudaStreamSynchronize(g->ctx->impl.stream));
+        delete g;
+    });
+}
+
+
+int ausaxs_gpu_hydration_grid_add(ausaxs_gpu_hydration_grid* g, const double* atoms, const int32_t* ff_types,
+                                  int64_t n_atoms) {
+    return hydration_grid_edit(g, atoms, ff_types, n_atoms, true);
+}
+
+int ausaxs_gpu_hydration_grid_remove(ausaxs_gpu_hydration_grid* g, const double* atoms, const int32_t* ff_types,
+                                     int64_t n_atoms) {
+    return hydration_grid_edit(g, atoms, ff_types, n_atoms, false);
+}
+
+int ausaxs_gpu_hydration_grid_hydrate(ausaxs_gpu_hydration_grid* g, const double* atoms, const int32_t* ff_types,
+                                      int64_t n_atoms, const double* noise, uint64_t noise_seed, double* waters_out,
+                                      int64_t capacity, int64_t* n_waters, int64_t* candidates_out, int32_t* rounds) {
+    return guarded([&] {
+        if (!g || bad_hydrate_args(atoms, ff_types, n_atoms, waters_out, capacity, n_waters))
+            throw Error{AUSAXS_ERR_ARGUMENT, "invalid argument"};
+        *n_waters = 0;
+        if (rounds) *rounds = 0;
+        check_hydration_atoms(atoms, ff_types, n_atoms, g->gmin, g->bins);
+        Ctx& C = g->ctx->impl;
+        AUSAXS_CUDA(cudaSetDevice(C.device));
+        Hydrator& H = hydrator(C);
+        double *d_atoms, *d_noise;
+        int32_t* d_ff;
+        stage_hydration_inputs(C, H, atoms, ff_types, n_atoms, noise, &d_atoms, &d_ff, &d_noise);
+        H.generate(C, g->cells.as<uint8_t>(), g->gmin, g->bins, d_atoms, d_ff, n_atoms, d_noise,
+                   noise ? 0ull : (unsigned long long)noise_seed);
+        read_waters(C, H, waters_out, capacity, n_waters, candidates_out, rounds);
     });
 }
 

@@ -134,6 +134,7 @@ struct Structure {
 };
 
 struct GridExv;
+struct Hydrator;
 
 struct Ctx {
     int device = 0;
@@ -143,13 +144,13 @@ struct Ctx {
     long long launches = 0;
     // optional per-kernel-class timing with CUDA events on the context's stream
     // (class 0: pair histograms, 1: finalisation, 2: FP64 Debye transform, 3: tensor-core Debye transform,
-    // 4: grid excluded volume)
+    // 4: grid excluded volume, 5: hydration)
     bool timing = false;
     struct Timed {
         std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
         double ms = 0;
         long long count = 0;
-    } timed[5];
+    } timed[6];
     void time_begin(int cls, cudaEvent_t* ev);
     void time_end(int cls, cudaEvent_t ev);
     void time_collect();
@@ -160,6 +161,7 @@ struct Ctx {
     PrepStats* stats_slots(size_t n);
     std::unique_ptr<Structure> scratch;
     std::shared_ptr<GridExv> grid;  // molecular-grid workspace of one-shot calls (gridexv.cuh)
+    std::shared_ptr<Hydrator> hyd;  // hydration workspace (hydrate.cuh)
     DevBuf io;                     // q / I(q) / profiles of one-shot host calls
     DevBuf tc;                     // tensor-core scratch of one-shot host calls
     int last_fp64_columns = 0;     // q values the last host transform evaluated in FP64

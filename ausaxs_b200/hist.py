@@ -62,6 +62,10 @@ def pack(xyz, fourth, as_int: bool) -> np.ndarray:
     return np.ascontiguousarray(out)
 
 
+# constants::charge::get_ff_charge(WATER): the weight data::Water carries (Water.h:15-18)
+WATER_CHARGE = 8.999659
+
+
 @dataclass
 class Molecule:
     """The inputs of the hot path a data::Molecule provides: atoms with form-factor type and
@@ -89,6 +93,17 @@ class Molecule:
             return float(self.volume)
         a, w, _ = self.compact_ff()
         return _capi.grid_exv(_capi.default_context(), a, w)[1]
+
+    def generate_new_hydration(self, noise=None, seed: int = 0, ctx: Optional[_capi.Context] = None) -> int:
+        """Molecule::generate_new_hydration() (source/core/data/Molecule.cpp:219-226) with the reference's
+        default RadialHydration and no culling, on the device: replaces the waters (weighted by the
+        water form factor's charge, as data::Water is) and returns their count.  noise: one
+        displacement per candidate ([n * 26, 3]), else seed != 0 draws Gaussian ones (sigma 0.75 A)
+        on the device, else none."""
+        w, _, _ = _capi.hydrate(ctx or _capi.default_context(), self.atoms, self.ff_types, None, noise, seed)
+        self.waters = w
+        self.water_weights = np.full(len(w), WATER_CHARGE)
+        return len(w)
 
     def compact_ff(self):
         a = pack(self.atoms, self.ff_types, True)

@@ -825,6 +825,150 @@ def reference_grid(m, steps: int = 1, warmup: int = 0):
                       "(single-threaded in the reference)"}
 
 
+HYD_METRIC = "hydration shells/s (Molecule::generate_new_hydration, RadialHydration, fresh grid, one structure)"
+HYD_UNIT = "shells/s"
+
+
+def hydrate_workload():
+    """The 50k-atom globule of the WAXS configuration, hydrated from scratch (its atoms only)."""
+    from ausaxs_b200 import synth
+
+    m = synth.cfg1().molecules[0]
+    xyz = np.ascontiguousarray(np.asarray(m.atoms, np.float64))
+    ff = np.ascontiguousarray(np.asarray(m.ff_types, np.int32))
+    return xyz, ff, "hydrate: RadialHydration of the 50k-atom globule (1 A grid, 26 directions, no noise)"
+
+
+def run_hydrate(args, rank, world, local_rank):
+    import ctypes as C
+
+    import torch
+
+    from ausaxs_b200 import _capi
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device(f"cuda:{local_rank}")
+    stream = torch.cuda.Stream(local_rank)
+    ctx = _capi.Context(local_rank)
+    ctx.set_stream(stream.cuda_stream)
+    xyz, ff, name = hydrate_workload()
+    axes = _capi.hydrate_axes(xyz)
+    cells = int(np.prod(axes[3:]))
+    w0, c0, _ = _capi.hydrate(ctx, xyz, ff)
+    cap = len(w0) + 1024
+    a_d, f_d = torch.from_numpy(xyz).to(dev), torch.from_numpy(ff).to(dev)
+    out = torch.zeros((cap, 3), dtype=torch.float64, device=dev)
+    cand = torch.zeros(cap, dtype=torch.int64, device=dev)
+    torch.cuda.synchronize()
+
+    def step():
+        return _capi.hydrate_device(ctx, a_d, f_d, len(xyz), axes, out, cap, cand)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        ctx.enable_timing(True)
+        launches0 = ctx.launches
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        with ClockSampler(local_rank) as clk:
+            torch.cuda.synchronize()
+            for k in range(args.steps):
+                starts[k].record(stream)
+                n, rounds = step()
+                ends[k].record(stream)
+            torch.cuda.synchronize()
+        launches = ctx.launches - launches0
+        k_ms, k_n = ctx.kernel_time(5)
+        ctx.enable_timing(False)
+    total_ms = max_over_ranks(sum(s_.elapsed_time(e) for s_, e in zip(starts, ends)), world)
+    value = world * args.steps / (total_ms / 1e3)
+    same = n == len(w0) and bool(np.array_equal(out[:n].cpu().numpy(), w0))
+
+    # end to end through the host C ABI: pinned atoms and types in, pinned waters out
+    pin_a = torch.from_numpy(xyz).pin_memory()
+    pin_f = torch.from_numpy(ff).pin_memory()
+    pin_o = torch.zeros((cap, 3), dtype=torch.float64).pin_memory()
+    pin_c = torch.zeros(cap, dtype=torch.int64).pin_memory()
+    L = _capi.load()
+    nn, rr = C.c_int64(0), C.c_int32(0)
+
+    def e2e_step():
+        _capi.check(L.ausaxs_gpu_hydrate(ctx.h, _capi.devptr(pin_a, C.c_double), _capi.devptr(pin_f, C.c_int32),
+                                         len(xyz), None, None, 0, _capi.devptr(pin_o, C.c_double), cap, C.byref(nn),
+                                         _capi.devptr(pin_c, C.c_int64), C.byref(rr)))
+
+    for _ in range(max(1, args.warmup // 2)):
+        e2e_step()
+    lat = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        e2e_step()
+        lat.append(time.perf_counter() - t0)
+    e2e = world * args.steps / max_over_ranks(sum(lat), world)
+    same = same and nn.value == n and bool(np.array_equal(pin_o.numpy()[:n], w0))
+
+    peaks, peak_kind = load_peaks()
+    kernel_ms = k_ms / args.steps
+    surv, _ = _capi.hydration_stats(ctx)
+    # algorithmic bytes of one shell, as a one-round resolution would touch them: atoms and types read,
+    # the cell grid written once, one cell read and one atom read per candidate, the 79 probe cells
+    # (state byte and two key words) of every candidate that survives the static tests, the waters
+    # and their indices written
+    alg = len(xyz) * 28 + cells + 26 * len(xyz) * 25 + surv * 79 * 17 + n * 32
+    achieved = alg / (kernel_ms / 1e3) / 1e9
+    line = {
+        "metric": HYD_METRIC, "value": value, "unit": HYD_UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 positions and distances, u8 cell states, u64 candidate keys",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": name, "atoms": len(xyz), "cells": cells, "waters": int(n), "rounds": int(rounds),
+                   "candidates_surviving_static_tests": surv,
+                   "l2": f"grid of {cells / 1e6:.1f} MB and keys of {cells * 16 / 1e6:.0f} MB stay in L2 (no flush: the "
+                         "step is bound by the rounds' launch and read-back latency, not DRAM)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e, "unit": HYD_UNIT, "h2d_bytes_per_step": int(xyz.nbytes + ff.nbytes),
+                "d2h_bytes_per_step": int(n * 32 + 16), "p50_ms": 1e3 * float(np.percentile(lat, 50)),
+                "p99_ms": 1e3 * float(np.percentile(lat, 99)), "same_as_resident": same},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "hydration kernels (class 5)", "achieved": achieved,
+                     "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                     "algorithmic_bytes": int(alg), "kernel_ms_per_step": kernel_ms,
+                     "kernel_intervals_per_step": k_n / args.steps,
+                     "note": "latency-bound: the rounds (scatter + evaluate each) run in batches of 8 between "
+                             "read-backs; the intervals exclude the host gaps at the read-backs"},
+        "clocks": clk.summary(),
+        "peaks_source": peak_kind,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = reference_hydrate(xyz, ff)
+    ctx.close()
+    return line
+
+
+def reference_hydrate(xyz, ff, steps: int = 1, warmup: int = 0):
+    from oracle import py as O
+
+    if not O.ref_available():
+        return {"unavailable": "reference build oracle/_ref/libausaxs_ref.so not present"}
+    O.ref(1)
+    ts = []
+    n = 0
+    for it in range(warmup + steps):
+        m = O.RefMolecule(xyz, np.ones(len(xyz)), ff, np.zeros((0, 3)), np.zeros(0))
+        _, w, _, _, t = m.hydrate(None, True, 1)
+        n = len(w)
+        if it >= warmup:
+            ts.append(t)
+    v = 1.0 / statistics.median(ts)
+    return {"value": v, "unit": HYD_UNIT, "cores": 1, "kind": "reference", "waters": n,
+            "sample": "the whole structure: grid creation and expansion, RadialHydration over every atom "
+                      "(single-threaded in the reference)"}
+
+
 FIT_METRIC = "fits/s (coordinates -> histogram -> SmartFitter fit of cw by golden-section search)"
 FIT_UNIT = "fits/s"
 # the reference's q axis (constants::axes::q_axis: 200 bins on [1e-4, 1]) below qmax = 0.5: 99 points
@@ -1139,6 +1283,17 @@ def run_reference(args, rank, world):
                 "cpu_baseline": det, "e2e": {"value": v, "unit": FIT_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if args.workload == "cfg4":
         return run_reference_serving(args, world)
+    if args.workload == "hydrate":
+        xyz, ff, name = hydrate_workload()
+        det = reference_hydrate(xyz, ff, steps=args.steps, warmup=args.warmup)
+        if "unavailable" in det:
+            return {"impl": "reference", **det}
+        v = det["value"]
+        return {"impl": "reference", "metric": HYD_METRIC, "value": v, "unit": HYD_UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64 (reference CPU)",
+                "data": "synthetic (seeded generator)", "config": {"workload": name}, "cpu_baseline": det,
+                "e2e": {"value": v, "unit": HYD_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if args.workload == "gridexv":
         m, name = grid_workload()
         det = reference_grid(m, steps=args.steps, warmup=args.warmup)
@@ -1171,7 +1326,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4", "gridexv", "fit", "symmetry"])
+    ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4", "gridexv", "fit", "symmetry",
+                                                              "hydrate"])
     ap.add_argument("--chains", type=int, default=64)
     ap.add_argument("--hbm-budget-gb", type=float, default=40.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -1197,7 +1353,7 @@ def main():
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     line = {"cfg3": run_batch, "cfg4": run_serving, "gridexv": run_gridexv, "fit": run_fit,
-            "symmetry": run_symmetry}.get(args.workload, run_ours)(
+            "symmetry": run_symmetry, "hydrate": run_hydrate}.get(args.workload, run_ours)(
         args, rank, world, local_rank)
     if world > 1:
         import torch

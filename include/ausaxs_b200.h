@@ -78,7 +78,7 @@ AUSAXS_API const char* ausaxs_gpu_last_error(void);
  * every later launch of a kernel class is bracketed by CUDA events on the context's stream.
  * ausaxs_gpu_ctx_kernel_time synchronises the stream and returns the accumulated device time (ms)
  * and number of launches of one class: 0 = pair histograms, 1 = finalisation, 2 = FP64 Debye
- * epilogue, 3 = tensor-core Debye contraction, 4 = grid excluded-volume kernels.
+ * epilogue, 3 = tensor-core Debye contraction, 4 = grid excluded-volume kernels, 5 = hydration kernels.
  * ausaxs_gpu_ctx_fp64_columns: how many q values the last ausaxs_gpu_debye call evaluated in FP64
  * (all of them with precision 1; those whose tensor-core error estimate exceeded the tolerance with
  * precision 0).
@@ -342,6 +342,66 @@ AUSAXS_API int ausaxs_gpu_calculator_result(ausaxs_gpu_calculator* c, int32_t cr
 AUSAXS_API int ausaxs_gpu_grid_exv(ausaxs_gpu_ctx* ctx, const float* atoms, int32_t n_atoms, const float* waters,
                                    int32_t n_waters, int32_t host_pointers, float* exv_out, int64_t capacity,
                                    int64_t* n_exv, double* volume);
+
+/*
+ * Hydration shell: the waters data::Molecule::generate_new_hydration() places with the reference's
+ * default strategy, hydrate::RadialHydration without culling
+ * (source/core/hydrate/generation/RadialHydration.cpp:43-206, GridBasedHydration.cpp:34-79), as
+ * the rigid-body loop calls it after every move (source/rigidbody/controller/SimpleController.cpp:76).
+ *   atoms: n_atoms x {x, y, z} (double, host memory) in the order the generator visits them (the
+ *     grid's member order: bodies in order, a body that was moved appended after the others);
+ *     ff_types: their form-factor types (1-14 or 16, FormFactorType.h:14-33).
+ *   axes: {min x, y, z, bins x, y, z} of the grid (1 A cells), or null for the axes Grid(bodies)
+ *     builds around these atoms (ausaxs_hydrate_axes); every atom must lie inside.
+ *   noise: n_atoms x 26 x 3 displacements, one row per candidate in candidate order (the reference
+ *     draws one from its noise generator per candidate), or null: then noise_seed != 0 draws
+ *     Gaussian displacements of sigma 0.75 A on the device (a stream of its own, not the
+ *     reference's), and noise_seed == 0 means none.
+ *   Writes the waters (x, y, z, double) in the reference's order into waters_out and, when not null,
+ *   their candidate indices (atom * 26 + direction, so the waters of each body can be told apart)
+ *   into candidates_out, when capacity suffices; *n_waters is their count, set also when the call
+ *   fails with AUSAXS_ERR_CAPACITY.  *rounds (may be null): the resolution rounds the device took.
+ *   Synchronises the context's stream.
+ */
+#define AUSAXS_HYDRATE_DIRECTIONS 26
+AUSAXS_API int ausaxs_gpu_hydrate(ausaxs_gpu_ctx* ctx, const double* atoms, const int32_t* ff_types, int64_t n_atoms,
+                                  const double* axes, const double* noise, uint64_t noise_seed, double* waters_out,
+                                  int64_t capacity, int64_t* n_waters, int64_t* candidates_out, int32_t* rounds);
+/* ausaxs_gpu_hydrate on device memory of the context's device: atoms, ff_types, noise, waters_out and
+ * candidates_out are device pointers; axes (host, 6 doubles) must be given.  The form-factor types are
+ * not checked (a type without a radius counts as radius 0); an atom outside the axes fails the call. */
+AUSAXS_API int ausaxs_gpu_hydrate_device(ausaxs_gpu_ctx* ctx, const double* atoms, const int32_t* ff_types,
+                                         int64_t n_atoms, const double* axes, const double* noise, uint64_t noise_seed,
+                                         double* waters_out, int64_t capacity, int64_t* n_waters,
+                                         int64_t* candidates_out, int32_t* rounds);
+/* Of the context's last hydration: the candidates that passed the static tests (their cell inside the
+ * grid and not an atom's) and the resolution rounds. */
+AUSAXS_API int ausaxs_gpu_ctx_hydration_stats(ausaxs_gpu_ctx* ctx, int64_t* survivors, int32_t* rounds);
+/* The axes Grid(bodies) builds around n_atoms atoms (x, y, z doubles) for the hydration: {min x, y, z,
+ * bins x, y, z} (Grid.cpp:34-102).  Host only. */
+AUSAXS_API int ausaxs_hydrate_axes(const double* atoms, int64_t n_atoms, double* axes);
+
+/*
+ * A hydration grid kept across calls, as the reference keeps a molecule's grid::Grid between
+ * rigid-body steps: create it with the axes, add every body's atoms (Grid::add with the volume
+ * expansion), and per step remove the moved body at its old coordinates (Grid::remove: its atoms'
+ * spheres of max(r_vdw, 2.15 A) lose their A_AREA / VOLUME marks, whatever other atoms cover them, and
+ * its centre cells their A_CENTER mark; SingleTransform.cpp:20-69), add it at the new ones, and
+ * hydrate.  hydrate takes the grid's member atoms in the grid's order (a re-added body comes last)
+ * and otherwise behaves as ausaxs_gpu_hydrate.  Atoms must lie inside the axes.  The grid belongs to
+ * the context it was made with; calls on it synchronise that context's stream.
+ */
+typedef struct ausaxs_gpu_hydration_grid ausaxs_gpu_hydration_grid;
+AUSAXS_API int ausaxs_gpu_hydration_grid_create(ausaxs_gpu_ctx* ctx, const double* axes, ausaxs_gpu_hydration_grid** out);
+AUSAXS_API int ausaxs_gpu_hydration_grid_destroy(ausaxs_gpu_hydration_grid* grid);
+AUSAXS_API int ausaxs_gpu_hydration_grid_add(ausaxs_gpu_hydration_grid* grid, const double* atoms,
+                                             const int32_t* ff_types, int64_t n_atoms);
+AUSAXS_API int ausaxs_gpu_hydration_grid_remove(ausaxs_gpu_hydration_grid* grid, const double* atoms,
+                                                const int32_t* ff_types, int64_t n_atoms);
+AUSAXS_API int ausaxs_gpu_hydration_grid_hydrate(ausaxs_gpu_hydration_grid* grid, const double* atoms,
+                                                 const int32_t* ff_types, int64_t n_atoms, const double* noise,
+                                                 uint64_t noise_seed, double* waters_out, int64_t capacity,
+                                                 int64_t* n_waters, int64_t* candidates_out, int32_t* rounds);
 
 /*
  * Rigid-body serving.  The reference's incremental manager, PartialHistogramManagerMT

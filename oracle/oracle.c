@@ -835,3 +835,295 @@ int64_t oracle_grid_exv(const double* atoms, int32_t na, const double* waters, i
     if (volume) *volume = (double)n * width * width * width;
     return n;
 }
+
+/*
+ * Hydration shell, Molecule::generate_new_hydration() with the reference's default strategy:
+ * RadialHydration (source/core/hydrate/generation/RadialHydration.cpp:43-206) on the grid of
+ * GridBasedHydration::hydrate (GridBasedHydration.cpp:34-79), no culling (NoCulling.cpp).
+ *   axes: as Grid(bodies) builds them (Grid.cpp:34-102), from the atoms alone (the hydration is
+ *     cleared before the grid is made), with the box extents truncated to int: oracle_hydrate_axes;
+ *   grid: each atom marks its cell A_CENTER; expand_volume() then marks, per atom, the cells within
+ *     r_vdw A_AREA and those within (r_vdw, rvol] VOLUME (SphericalExpander.h:27-76);
+ *   directions: prepare_rotations(8): one octant of the sphere at theta, phi in {0, pi/4, pi/2},
+ *     reflected into all eight octants, components below 1e-5 zeroed and duplicates (distance
+ *     < 1e-5) dropped, in first-seen order: 26 unit vectors; probe offsets round(k rh u) / width
+ *     for k = 1, 3, 5, with rh = r_vdw(O) + shell correction = 1.71 - 0.35;
+ *   candidates, atom by atom in grid order and direction by direction: x = atom + u (r_vdw + rh) +
+ *     noise (formed as fma(u, r_vdw + rh, atom + noise), as the reference build contracts it); accepted when its cell lies in the grid and holds nothing but VOLUME, and
+ *     collision_check passes (RadialHydration.cpp:143-205): over the directions, a 1rh probe
+ *     (clamped to the grid) that holds more than VOLUME counts as inside (a third one rejects) and
+ *     skips the direction; else a 3rh probe outside the grid scores +2 and ends the direction, one
+ *     holding more than VOLUME scores -2 and ends it, a free one +2; then a 5rh probe outside scores
+ *     +1, one holding more than VOLUME -1; the candidate passes when score > min_score (0.25) x 3 x 26;
+ *   an accepted water marks its cell W_CENTER and the EMPTY cells within r_vdw(O) of x (box
+ *     bin +- ceil(r_vdw(O))) W_AREA (SphericalExpander.h:78-115, AtomicOnly: no water VOLUME),
+ *     before the next candidate is tried.
+ * xyz: n x 3 atom coordinates (double) in the order the generator visits them, ff: their form-factor
+ * types; axes: {min x, y, z, bins x, y, z}; noise: n x 26 x 3 (one row per candidate, in candidate
+ * order) or NULL for none.  Writes up to cap waters (n x 3) and their candidate indices
+ * (atom * 26 + direction) and returns the count.
+ */
+#define HYD_DIRS 26
+
+static int hyd_directions(double u[HYD_DIRS][3]) {
+    const double pi = 3.14159265358979323846;
+    const double ang = 2 * pi / 8;
+    int n = 0;
+    for (double theta = 0; theta <= pi * 0.5; theta += ang)
+        for (double phi = 0; phi <= pi * 0.5; phi += ang) {
+            double x = cos(phi) * sin(theta), y = sin(phi) * sin(theta), z = cos(theta);
+            double s[8][3] = {{x, y, z}, {-x, y, z}, {x, -y, z}, {-x, -y, z},
+                              {x, y, -z}, {-x, y, -z}, {x, -y, -z}, {-x, -y, -z}};
+            for (int r = 0; r < 8; ++r) {
+                double p[3] = {s[r][0], s[r][1], s[r][2]};
+                for (int d = 0; d < 3; ++d)
+                    if (fabs(p[d]) < 1e-5) p[d] = 0;
+                int present = 0;
+                for (int k = 0; k < n && !present; ++k) {
+                    double dx = u[k][0] - p[0], dy = u[k][1] - p[1], dz = u[k][2] - p[2];
+                    present = sqrt(dx * dx + dy * dy + dz * dz) < 1e-5;
+                }
+                if (!present) {
+                    if (n == HYD_DIRS) return -1;
+                    u[n][0] = p[0], u[n][1] = p[1], u[n][2] = p[2];
+                    ++n;
+                }
+            }
+        }
+    return n;
+}
+
+void oracle_hydrate_axes(const double* xyz, int64_t n, double* axes) {
+    /* Grid(bodies) keeps the running box in a Vector3 deduced from {0, 0, 0}, i.e. of int
+     * (Grid.cpp:36): every extent that widens it is truncated toward zero, and diff is an int */
+    const double width = 1.0;
+    int mn[3] = {0, 0, 0}, mx[3] = {0, 0, 0};
+    for (int64_t i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) {
+            if (xyz[3 * i + d] < mn[d]) mn[d] = (int)xyz[3 * i + d];
+            if (xyz[3 * i + d] > mx[d]) mx[d] = (int)xyz[3 * i + d];
+        }
+    int diff[3] = {mx[0] - mn[0], mx[1] - mn[1], mx[2] - mn[2]};
+    double scaling = (diff[0] < 50 || diff[1] < 50 || diff[2] < 50) ? 1.0 : 0.25;
+    double margin = 2.14 + 1.71 + (-0.35) + 3 * width;
+    for (int d = 0; d < 3; ++d) {
+        double e = fmax(0.5 * diff[d] * scaling, margin);
+        double lo = floor(mn[d] - e - width), hi = ceil(mx[d] + e + width);
+        axes[d] = lo;
+        axes[3 + d] = (double)(int)((hi - lo) / width);
+    }
+}
+
+/* The grid's atom state (one byte per cell, the reference's State bits) is kept by the caller between
+ * calls, as the reference keeps a molecule's grid across rigid-body steps:
+ *   oracle_hgrid_add: Grid::add(body) marks the atoms' cells A_CENTER (Grid.cpp:293-330), and the
+ *     volume expansion that hydrate() then runs treats the atoms in order: cells within r_vdw that hold
+ *     nothing or VOLUME get A_AREA, cells within (r_vdw, rvol] that hold nothing get VOLUME
+ *     (SphericalExpander.h:27-76);
+ *   oracle_hgrid_remove: Grid::remove(body) deflates each atom, clearing A_AREA and VOLUME within
+ *     max(r_vdw, rvol) whatever else covers those cells, and clears A_CENTER of its cell
+ *     (Grid.cpp:372-400, SphericalExpander.h:117-150);
+ *   oracle_hgrid_hydrate: the generation on a copy of the state (waters never touch the caller's
+ *     state: the reference clears them before each generation, and their removal only clears W_AREA,
+ *     SphericalExpander.h:152-186). */
+enum { HG_VOLUME = 1, HG_A_CENTER = 4, HG_A_AREA = 8, HG_W_CENTER = 16, HG_W_AREA = 32 };
+
+static void hg_shape(const double* axes, double gmin[3], int bins[3]) {
+    for (int d = 0; d < 3; ++d) gmin[d] = axes[d], bins[d] = (int)axes[3 + d];
+}
+
+void oracle_hgrid_add(unsigned char* g, const double* axes, const double* xyz, const int32_t* ff, int64_t n) {
+    const double width = 1.0, rvol = 2.15;
+    double gmin[3];
+    int bins[3];
+    hg_shape(axes, gmin, bins);
+#define CELL(i, j, k) g[((size_t)(i) * bins[1] + (j)) * bins[2] + (k)]
+    for (int64_t a = 0; a < n; ++a) {
+        int b[3], in = 1;
+        for (int d = 0; d < 3; ++d) {
+            b[d] = (int)round((xyz[3 * a + d] - gmin[d]) / width);
+            in = in && b[d] >= 0 && b[d] < bins[d];
+        }
+        if (in) CELL(b[0], b[1], b[2]) |= HG_A_CENTER; /* outside: the caller's error (the C ABI rejects it) */
+    }
+    for (int64_t a = 0; a < n; ++a) {
+        const double* p = xyz + 3 * a;
+        double rvdw = vdw_of_ff(ff[a]), rvdw2 = rvdw * rvdw, rvol2 = rvol * rvol;
+        int br = (int)ceil(fmax(rvdw, rvol) / width);
+        int b[3], lo_[3], hi_[3];
+        for (int d = 0; d < 3; ++d) {
+            b[d] = (int)round((p[d] - gmin[d]) / width);
+            lo_[d] = b[d] - br > 0 ? b[d] - br : 0;
+            hi_[d] = b[d] + br + 1 < bins[d] ? b[d] + br + 1 : bins[d];
+        }
+        for (int i = lo_[0]; i < hi_[0]; ++i) {
+            double x2 = pow(gmin[0] + i * width - p[0], 2);
+            for (int j = lo_[1]; j < hi_[1]; ++j) {
+                double x2y2 = x2 + pow(gmin[1] + j * width - p[1], 2);
+                for (int k = lo_[2]; k < hi_[2]; ++k) {
+                    double dist = x2y2 + pow(gmin[2] + k * width - p[2], 2);
+                    unsigned char* c = &CELL(i, j, k);
+                    if (dist <= rvdw2) {
+                        if (!(*c == 0 || (*c & HG_VOLUME))) continue;
+                        *c |= HG_A_AREA;
+                    } else if (dist <= rvol2) {
+                        if (*c != 0) continue;
+                        *c |= HG_VOLUME;
+                    }
+                }
+            }
+        }
+    }
+#undef CELL
+}
+
+void oracle_hgrid_remove(unsigned char* g, const double* axes, const double* xyz, const int32_t* ff, int64_t n) {
+    const double width = 1.0, rvol = 2.15;
+    double gmin[3];
+    int bins[3];
+    hg_shape(axes, gmin, bins);
+#define CELL(i, j, k) g[((size_t)(i) * bins[1] + (j)) * bins[2] + (k)]
+    for (int64_t a = 0; a < n; ++a) {
+        const double* p = xyz + 3 * a;
+        double rmax = fmax(vdw_of_ff(ff[a]), rvol), rmax2 = pow(rmax, 2);
+        int br = (int)ceil(rmax / width);
+        int b[3], lo_[3], hi_[3];
+        for (int d = 0; d < 3; ++d) {
+            b[d] = (int)round((p[d] - gmin[d]) / width);
+            lo_[d] = b[d] - br > 0 ? b[d] - br : 0;
+            hi_[d] = b[d] + br + 1 < bins[d] ? b[d] + br + 1 : bins[d];
+        }
+        for (int i = lo_[0]; i < hi_[0]; ++i) {
+            double x2 = pow(gmin[0] + i * width - p[0], 2);
+            for (int j = lo_[1]; j < hi_[1]; ++j) {
+                double x2y2 = x2 + pow(gmin[1] + j * width - p[1], 2);
+                for (int k = lo_[2]; k < hi_[2]; ++k) {
+                    double dist = x2y2 + pow(gmin[2] + k * width - p[2], 2);
+                    if (dist <= rmax2) CELL(i, j, k) &= (unsigned char)~(HG_A_AREA | HG_VOLUME);
+                }
+            }
+        }
+        if (b[0] >= 0 && b[0] < bins[0] && b[1] >= 0 && b[1] < bins[1] && b[2] >= 0 && b[2] < bins[2])
+            CELL(b[0], b[1], b[2]) &= (unsigned char)~HG_A_CENTER;
+    }
+#undef CELL
+}
+
+int64_t oracle_hgrid_hydrate(const unsigned char* state, const double* axes, const double* xyz, const int32_t* ff,
+                             int64_t n, const double* noise, double* out, int64_t cap, int64_t* cand_out) {
+    const double width = 1.0, rw = 1.71, rh = 1.71 + (-0.35);
+    double gmin[3];
+    int bins[3];
+    hg_shape(axes, gmin, bins);
+    double u[HYD_DIRS][3];
+    if (hyd_directions(u) != HYD_DIRS) return -2;
+    int p1[HYD_DIRS][3], p3[HYD_DIRS][3], p5[HYD_DIRS][3];
+    for (int i = 0; i < HYD_DIRS; ++i)
+        for (int d = 0; d < 3; ++d) {
+            p1[i][d] = (int)(round(rh * u[i][d]) / width);
+            p3[i][d] = (int)(round(3 * rh * u[i][d]) / width);
+            p5[i][d] = (int)(round(5 * rh * u[i][d]) / width);
+        }
+    size_t cells = (size_t)bins[0] * bins[1] * bins[2];
+    unsigned char* g = malloc(cells ? cells : 1);
+    if (!g) return -1;
+    memcpy(g, state, cells);
+#define CELL(i, j, k) g[((size_t)(i) * bins[1] + (j)) * bins[2] + (k)]
+#define FREE_(c) (((c) & ~HG_VOLUME) == 0)
+    const double min_points = 0.25 * 3 * HYD_DIRS;
+    int64_t m = 0;
+    for (int64_t a = 0; a < n; ++a) {
+        const double* p = xyz + 3 * a;
+        const double reff = vdw_of_ff(ff[a]) + rh;
+        for (int r = 0; r < HYD_DIRS; ++r) {
+            const double* nz = noise ? noise + 3 * (a * HYD_DIRS + r) : NULL;
+            double x[3];
+            int b[3], valid = 1;
+            for (int d = 0; d < 3; ++d) {
+                /* the reference build evaluates atom + u reff + noise as fma(u, reff, atom + noise) */
+                x[d] = fma(u[r][d], reff, p[d] + (nz ? nz[d] : 0.0));
+                b[d] = (int)round((x[d] - gmin[d]) / width);
+                valid = valid && b[d] >= 0 && b[d] < bins[d];
+            }
+            if (!valid || !FREE_(CELL(b[0], b[1], b[2]))) continue;
+            /* collision_check */
+            int inside = 0, score = 0, ok = 1;
+            for (int i = 0; i < HYD_DIRS && ok; ++i) {
+                int q[3];
+                for (int d = 0; d < 3; ++d) {
+                    q[d] = b[d] + p1[i][d];
+                    q[d] = q[d] < 0 ? 0 : (q[d] > bins[d] - 1 ? bins[d] - 1 : q[d]);
+                }
+                if (!FREE_(CELL(q[0], q[1], q[2]))) {
+                    if (2 < ++inside) ok = 0;
+                    continue;
+                }
+                int oob = 0;
+                for (int d = 0; d < 3; ++d) {
+                    q[d] = b[d] + p3[i][d];
+                    oob = oob || q[d] < 0 || q[d] >= bins[d];
+                }
+                if (oob) {
+                    score += 2;
+                    continue;
+                }
+                if (!FREE_(CELL(q[0], q[1], q[2]))) {
+                    score -= 2;
+                    continue;
+                }
+                score += 2;
+                oob = 0;
+                for (int d = 0; d < 3; ++d) {
+                    q[d] = b[d] + p5[i][d];
+                    oob = oob || q[d] < 0 || q[d] >= bins[d];
+                }
+                if (oob) {
+                    score += 1;
+                    continue;
+                }
+                if (!FREE_(CELL(q[0], q[1], q[2]))) score -= 1;
+            }
+            if (!ok || score <= min_points) continue;
+            /* Grid::add(water, expand = true) */
+            CELL(b[0], b[1], b[2]) |= HG_W_CENTER;
+            const double rw2 = rw * rw;
+            const int br = (int)ceil(rw / width);
+            int lo_[3], hi_[3];
+            for (int d = 0; d < 3; ++d) {
+                lo_[d] = b[d] - br > 0 ? b[d] - br : 0;
+                hi_[d] = b[d] + br + 1 < bins[d] ? b[d] + br + 1 : bins[d];
+            }
+            for (int i = lo_[0]; i < hi_[0]; ++i) {
+                double x2 = pow(gmin[0] + i * width - x[0], 2);
+                for (int j = lo_[1]; j < hi_[1]; ++j) {
+                    double x2y2 = x2 + pow(gmin[1] + j * width - x[1], 2);
+                    for (int k = lo_[2]; k < hi_[2]; ++k) {
+                        double dist = x2y2 + pow(gmin[2] + k * width - x[2], 2);
+                        if (dist <= rw2 && CELL(i, j, k) == 0) CELL(i, j, k) |= HG_W_AREA;
+                    }
+                }
+            }
+            if (out && m < cap) {
+                out[3 * m] = x[0], out[3 * m + 1] = x[1], out[3 * m + 2] = x[2];
+                if (cand_out) cand_out[m] = a * HYD_DIRS + r;
+            }
+            ++m;
+        }
+    }
+#undef FREE_
+#undef CELL
+    free(g);
+    return m;
+}
+
+/* A fresh grid of these atoms (Grid(bodies) with the given axes), then the generation. */
+int64_t oracle_hydrate(const double* xyz, const int32_t* ff, int64_t n, const double* axes, const double* noise,
+                       double* out, int64_t cap, int64_t* cand_out) {
+    size_t cells = (size_t)axes[3] * (size_t)axes[4] * (size_t)axes[5];
+    unsigned char* g = calloc(cells ? cells : 1, 1);
+    if (!g) return -1;
+    oracle_hgrid_add(g, axes, xyz, ff, n);
+    int64_t m = oracle_hgrid_hydrate(g, axes, xyz, ff, n, noise, out, cap, cand_out);
+    free(g);
+    return m;
+}

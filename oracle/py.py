@@ -70,6 +70,17 @@ def lib():
         L.oracle_calc_job.restype = C.c_int64
         L.oracle_calc_job.argtypes = [_f32p, C.c_int32, C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_int32,
                                       _f64p, _f64p, _f64p]
+        L.oracle_hydrate_axes.restype = None
+        L.oracle_hydrate_axes.argtypes = [_f64p, C.c_int64, _f64p]
+        L.oracle_hydrate.restype = C.c_int64
+        L.oracle_hydrate.argtypes = [_f64p, _i32p, C.c_int64, _f64p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+        _u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+        for name in ("oracle_hgrid_add", "oracle_hgrid_remove"):
+            getattr(L, name).restype = None
+            getattr(L, name).argtypes = [_u8p, _f64p, _f64p, _i32p, C.c_int64]
+        L.oracle_hgrid_hydrate.restype = C.c_int64
+        L.oracle_hgrid_hydrate.argtypes = [_u8p, _f64p, _f64p, _i32p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64,
+                                           C.c_void_p]
         L.oracle_fit.restype = None
         L.oracle_fit.argtypes = [C.c_int, _f64p, _f64p, _f64p, C.c_int32, _f64p, _f64p, _f64p, _f64p, _f64p, _f64p,
                                  C.c_int32, C.c_int, C.c_double, C.c_double, C.c_double, _f64p, C.c_double, _f64p]
@@ -308,6 +319,9 @@ def ref(threads: int = 0):
         R.ref_molecule_free.argtypes = [vp]
         R.ref_body_move.argtypes = [vp, C.c_int, _f64p, _f64p]
         R.ref_body_coords.argtypes = [vp, C.c_int, C.c_void_p, C.POINTER(C.c_int)]
+        R.ref_body_move_in_grid.argtypes = [vp, C.c_int, _f64p, _f64p]
+        R.ref_hydrate.argtypes = [vp, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_void_p,
+                                  C.c_int, C.POINTER(C.c_int), C.c_void_p, C.c_void_p]
         R.ref_manager_set.argtypes = [vp, C.c_int, C.c_int, _f64p, C.c_int]
         R.ref_manager_calculate.restype = vp
         R.ref_manager_calculate.argtypes = [vp, C.POINTER(C.c_double)]
@@ -380,6 +394,37 @@ class RefMolecule:
         out = np.zeros((max(1, n.value), 3))
         _check(R, R.ref_body_coords(self.h, body, out.ctypes.data, C.byref(n)))
         return out[:n.value]
+
+    def hydrate(self, noise=None, fresh_grid=True, n_bodies=1):
+        """Molecule::generate_new_hydration() (RadialHydration, no culling) with the noise generator
+        reading the rows of `noise` ([n, 3], zero when None).  Returns (grid member atoms in visiting
+        order [n, 4] {x, y, z, ff}, waters [m, 3] in body order, waters per body, grid axes [9]
+        {min xyz, max xyz, bins xyz}, seconds)."""
+        import time
+
+        R = ref()
+        nz = None if noise is None else np.ascontiguousarray(np.asarray(noise, np.float64).reshape(-1, 3))
+        na, nw = C.c_int(0), C.c_int(0)
+        per_body = np.zeros(max(1, n_bodies), np.int32)
+        axes = np.zeros(9)
+        t0 = time.perf_counter()
+        _check(R, R.ref_hydrate(self.h, None if nz is None else nz.ctypes.data, 0 if nz is None else len(nz),
+                                int(fresh_grid), None, 0, C.byref(na), None, 0, C.byref(nw), per_body.ctypes.data,
+                                axes.ctypes.data))
+        secs = time.perf_counter() - t0
+        atoms = np.zeros((max(1, na.value), 4))
+        waters = np.zeros((max(1, nw.value), 3))
+        # the second call regenerates with the same noise rows; the result is the same hydration
+        _check(R, R.ref_hydrate(self.h, None if nz is None else nz.ctypes.data, 0 if nz is None else len(nz), 0,
+                                atoms.ctypes.data, len(atoms), C.byref(na), waters.ctypes.data, len(waters),
+                                C.byref(nw), per_body.ctypes.data, axes.ctypes.data))
+        return atoms[:na.value], waters[:nw.value], per_body[:n_bodies].copy(), axes, secs
+
+    def move_body_in_grid(self, body, Rm, t):
+        """The rigid-body transforms' move: the body leaves the grid, moves and is appended back."""
+        R = ref()
+        _check(R, R.ref_body_move_in_grid(self.h, body, np.ascontiguousarray(np.asarray(Rm, np.float64).reshape(9)),
+                                          np.ascontiguousarray(np.asarray(t, np.float64).reshape(3))))
 
     def move_body(self, body, Rm, t):
         R = ref()
@@ -481,6 +526,81 @@ def calculator(sets, jobs, bin_width, nbins):
         L.oracle_calc_job(A, len(A), None if B is None else B.ctypes.data, 0 if B is None else len(B), int(scaling),
                           float(bin_width), int(nbins), v, c, d)
     return out
+
+
+HYDRATE_DIRECTIONS = 26
+
+
+def hydrate_noise(n_candidates: int, seed: int) -> np.ndarray:
+    """A reproducible noise table for the hydration tests, [n, 3] in (-0.75, 0.75): a multiplicative
+    integer hash of (seed, row, component) scaled to the range, exact in double on every platform."""
+    k = np.arange(3 * n_candidates, dtype=np.uint64) + np.uint64(seed) * np.uint64(0x9E3779B1)
+    h = (k * np.uint64(2654435761) + np.uint64(seed)) % np.uint64(1 << 32)
+    h = (h ^ (h >> np.uint64(15))) * np.uint64(2246822519) % np.uint64(1 << 32)
+    return ((h.astype(np.float64) / 4294967296.0) - 0.5).reshape(-1, 3) * 1.5
+
+
+def hydrate_axes(xyz):
+    """Grid axes {min x, y, z, bins x, y, z} of Grid(bodies) over the atoms alone."""
+    a = np.ascontiguousarray(np.asarray(xyz, np.float64).reshape(-1, 3))
+    out = np.zeros(6)
+    lib().oracle_hydrate_axes(a, len(a), out)
+    return out
+
+
+def hydrate(xyz, ff, axes=None, noise=None):
+    """RadialHydration restated (oracle_hydrate): waters [m, 3] and their candidate indices
+    (atom * 26 + direction), atoms in the order the generator visits them."""
+    a = np.ascontiguousarray(np.asarray(xyz, np.float64).reshape(-1, 3))
+    f = np.ascontiguousarray(np.asarray(ff, np.int32).reshape(-1))
+    ax = hydrate_axes(a) if axes is None else np.ascontiguousarray(np.asarray(axes, np.float64)[:6])
+    nz = None if noise is None else np.ascontiguousarray(np.asarray(noise, np.float64).reshape(-1, 3))
+    if nz is not None and len(nz) < HYDRATE_DIRECTIONS * len(a):
+        nz = np.vstack([nz, np.zeros((HYDRATE_DIRECTIONS * len(a) - len(nz), 3))])
+    cap = HYDRATE_DIRECTIONS * len(a) + 1
+    out = np.zeros((cap, 3))
+    cand = np.zeros(cap, np.int64)
+    m = lib().oracle_hydrate(a, f, len(a), ax, None if nz is None else nz.ctypes.data, out.ctypes.data, cap,
+                             cand.ctypes.data)
+    if m < 0:
+        raise RuntimeError(f"oracle_hydrate failed ({m})")
+    return out[:m], cand[:m]
+
+
+class HydrationGrid:
+    """The oracle's hydration grid kept across calls, as the reference keeps a molecule's grid::Grid:
+    add(xyz, ff) = Grid::add with the volume expansion, remove(xyz, ff) = Grid::remove of atoms at
+    those (current) coordinates, hydrate(xyz, ff, noise) = the generation over the grid's members in
+    the order given (oracle_hgrid_*)."""
+
+    def __init__(self, axes):
+        self.axes = np.ascontiguousarray(np.asarray(axes, np.float64)[:6])
+        self.state = np.zeros(int(np.prod(self.axes[3:].astype(np.int64))), np.uint8)
+
+    @staticmethod
+    def _in(xyz, ff):
+        return (np.ascontiguousarray(np.asarray(xyz, np.float64).reshape(-1, 3)),
+                np.ascontiguousarray(np.asarray(ff, np.int32).reshape(-1)))
+
+    def add(self, xyz, ff):
+        a, f = self._in(xyz, ff)
+        lib().oracle_hgrid_add(self.state, self.axes, a, f, len(a))
+
+    def remove(self, xyz, ff):
+        a, f = self._in(xyz, ff)
+        lib().oracle_hgrid_remove(self.state, self.axes, a, f, len(a))
+
+    def hydrate(self, xyz, ff, noise=None):
+        a, f = self._in(xyz, ff)
+        nz = None if noise is None else np.ascontiguousarray(np.asarray(noise, np.float64).reshape(-1, 3))
+        cap = HYDRATE_DIRECTIONS * len(a) + 1
+        out = np.zeros((cap, 3))
+        cand = np.zeros(cap, np.int64)
+        m = lib().oracle_hgrid_hydrate(self.state, self.axes, a, f, len(a), None if nz is None else nz.ctypes.data,
+                                       out.ctypes.data, cap, cand.ctypes.data)
+        if m < 0:
+            raise RuntimeError(f"oracle_hgrid_hydrate failed ({m})")
+        return out[:m], cand[:m]
 
 
 def ref_calculator(sets, jobs):

@@ -48,6 +48,9 @@
 #include <settings/GridSettings.h>
 #include <grid/Grid.h>
 #include <grid/exv/RawGridExv.h>
+#include <grid/detail/GridMember.h>
+#include <hydrate/generation/RadialHydration.h>
+#include <hydrate/generation/HydrationStrategy.h>
 #include <io/File.h>
 
 #include <chrono>
@@ -302,6 +305,91 @@ int ref_body_move(void* m, int body, const double* R, const double* t) {
         Matrix<double> M{{R[0], R[1], R[2]}, {R[3], R[4], R[5]}, {R[6], R[7], R[8]}};
         b.rotate(M);
         b.translate(Vector3<double>(t[0], t[1], t[2]));
+    });
+}
+
+// Hydration: Molecule::generate_new_hydration() with the default strategy (RadialHydration, no
+// culling), its noise generator reading successive rows of `noise` (n x 3; zero once exhausted or
+// when noise is null).  fresh_grid = 1 drops the molecule's grid and generator first, so the grid
+// is rebuilt from the current atoms (Grid(bodies), with settings::grid::scaling back at its default);
+// 0 keeps both, as the rigid-body loop does between steps.  Writes the grid's member atoms in the
+// order the generator visits them (n_a x {x, y, z, ff}), the waters of every body in body order
+// (n_w x 3), the waters per body, and the grid axes {min x, y, z, max x, y, z, bins x, y, z}.
+namespace {
+std::vector<double> g_noise;
+size_t g_noise_at = 0;
+}  // namespace
+
+int ref_hydrate(void* m, const double* noise, int n_noise, int fresh_grid, double* atoms_out, int cap_a, int* n_a,
+                double* waters_out, int cap_w, int* n_w, int* per_body, double* axes_out) {
+    return guarded([&] {
+        auto* mol = static_cast<FixedVolumeMolecule*>(m);
+        settings::hydrate::hydration_strategy = settings::hydrate::HydrationStrategy::RadialStrategy;
+        settings::hydrate::culling_strategy = settings::hydrate::CullingStrategy::NoStrategy;
+        g_noise.assign(noise ? noise : nullptr, noise ? noise + 3 * static_cast<size_t>(n_noise) : nullptr);
+        g_noise_at = 0;
+        hydrate::RadialHydration::set_noise_generator([] {
+            if (3 * g_noise_at + 2 >= g_noise.size()) return Vector3<double>(0, 0, 0);
+            const double* r = g_noise.data() + 3 * g_noise_at++;
+            return Vector3<double>(r[0], r[1], r[2]);
+        });
+        if (fresh_grid) {
+            settings::grid::scaling = 0.25;
+            mol->clear_hydration();
+            mol->clear_grid();
+            mol->set_hydration_generator(nullptr);
+        }
+        mol->generate_new_hydration();
+        auto* grid = mol->get_grid();
+        *n_a = static_cast<int>(grid->a_members.size());
+        if (atoms_out && cap_a >= *n_a) {
+            for (size_t i = 0; i < grid->a_members.size(); ++i) {
+                const auto& a = grid->a_members[i].get_atom();
+                double* r = atoms_out + 4 * i;
+                r[0] = a.coordinates().x();
+                r[1] = a.coordinates().y();
+                r[2] = a.coordinates().z();
+                r[3] = static_cast<int>(a.form_factor_type());
+            }
+        }
+        auto w = mol->get_waters();
+        *n_w = static_cast<int>(w.size());
+        if (waters_out && cap_w >= *n_w) {
+            for (size_t i = 0; i < w.size(); ++i) {
+                waters_out[3 * i] = w[i].coordinates().x();
+                waters_out[3 * i + 1] = w[i].coordinates().y();
+                waters_out[3 * i + 2] = w[i].coordinates().z();
+            }
+        }
+        if (per_body)
+            for (size_t b = 0; b < mol->size_body(); ++b) {
+                auto h = mol->get_body(b).get_waters();
+                per_body[b] = h.has_value() ? static_cast<int>(h.value().get().size()) : 0;
+            }
+        if (axes_out) {
+            const auto& ax = grid->get_axes();
+            const Axis* a3[3] = {&ax.x, &ax.y, &ax.z};
+            for (int d = 0; d < 3; ++d) {
+                axes_out[d] = a3[d]->min;
+                axes_out[3 + d] = a3[d]->max;
+                axes_out[6 + d] = a3[d]->bins;
+            }
+        }
+    });
+}
+
+// A rigid move of one body as the rigid-body transforms make it (SingleTransform.cpp:20-69): the body
+// leaves the grid, moves (x <- R x + t) and is added back, which appends its atoms to the grid's
+// member list; the grid's axes are kept.
+int ref_body_move_in_grid(void* m, int body, const double* R, const double* t) {
+    return guarded([&] {
+        auto* mol = static_cast<FixedVolumeMolecule*>(m);
+        auto& b = mol->get_body(body);
+        mol->get_grid()->remove(b);
+        Matrix<double> M{{R[0], R[1], R[2]}, {R[3], R[4], R[5]}, {R[6], R[7], R[8]}};
+        b.rotate(M);
+        b.translate(Vector3<double>(t[0], t[1], t[2]));
+        mol->get_grid()->add(b);
     });
 }
 

@@ -19,7 +19,9 @@ reference's default q axis.  Cases:
 * ``fit_*``   : SmartFitter::fit with the Golden minimiser over one parameter, on synthetic data on
                 the model's own q axis;
 * ``calc_*``  : SimpleCalculator job lists (scaling factors, merge ids);
-* ``partial_*``: PartialHistogramManagerMT over a multi-body molecule, initially and after rigid moves.
+* ``partial_*``: PartialHistogramManagerMT over a multi-body molecule, initially and after rigid moves;
+* ``hydrate_*``: Molecule::generate_new_hydration() (RadialHydration) with seeded noise tables, on a
+                fresh grid and after rigid moves.
 """
 from __future__ import annotations
 
@@ -149,6 +151,32 @@ def partial_case(name, bodies, ws, waters, ww, moves, bin_width):
     print(name, "steps", len(moves) + 1, "bins", len(out["d_axis0"]))
 
 
+def hydrate_case(name, xyz, ff, body_sizes, noise_seed, moves=()):
+    """Molecule::generate_new_hydration() (RadialHydration, no culling) with the noise table
+    O.hydrate_noise(26 n, noise_seed + step) (one row per candidate; none when noise_seed is None), on
+    a fresh grid; then after each rigid move (body, R, t) made as the rigid-body transforms make it
+    (the body leaves the grid and is appended back, the axes are kept), again.  Per step: the grid's
+    atoms in visiting order, the waters in body order, the waters per body and the grid axes."""
+    O.ref_set_axes(0.25, 8000, 1e-4, 0.5)
+    O.ref_set_simple_exv(False)
+    m = O.RefMolecule(xyz, np.ones(len(xyz)), ff, np.zeros((0, 3)), np.zeros(0), body_sizes=list(body_sizes))
+    out = dict(body_sizes=np.asarray(body_sizes, np.int32), manager="hydrate", steps=len(moves) + 1,
+               moves=np.array([k for k, _, _ in moves], np.int32), noise_seed=-1 if noise_seed is None else noise_seed)
+    for step in range(len(moves) + 1):
+        if step:
+            k, Rm, t = moves[step - 1]
+            m.move_body_in_grid(k, Rm, t)
+        noise = None if noise_seed is None else O.hydrate_noise(26 * len(xyz), noise_seed + step)
+        a, w, per_body, axes, _ = m.hydrate(noise, fresh_grid=(step == 0), n_bodies=len(body_sizes))
+        out[f"atoms{step}"] = a[:, :3].copy()
+        out[f"ff{step}"] = a[:, 3].astype(np.int32)
+        out[f"waters{step}"] = w
+        out[f"per_body{step}"] = per_body
+        out[f"axes{step}"] = np.concatenate([axes[:3], axes[6:]])
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print(name, "waters", [len(out[f"waters{s}"]) for s in range(len(moves) + 1)])
+
+
 def main():
     O.ref()
     # SimpleCube: 8 corners + centre as atoms (carbon), 8 corner waters
@@ -233,6 +261,23 @@ def main():
     moves = [(2, rotation((1, 2, 0.5), 0.07), np.array([0.8, -1.1, 0.4])),
              (0, rotation((0.2, -1, 1), 0.05), np.array([-0.5, 0.3, 1.2]))]
     partial_case("partial_random_4bodies", bodies, ws, waters, ww, moves, 0.25)
+    # hydration shells (RadialHydration), seeded streams of their own
+    hrng = np.random.default_rng(17)
+    xyz = hrng.normal(0, 6, (300, 3))
+    f = hrng.choice([2, 3, 4, 7, 8, 11, 12, 14], 300)
+    hydrate_case("hydrate_random_2bodies", xyz, f, [180, 120], 171)
+    xyz = hrng.normal(0, 10, (1500, 3))
+    f = hrng.choice(elements, 1500)
+    hydrate_case("hydrate_random_nonoise", xyz, f, [1500], None)
+    xyz = np.concatenate([hrng.normal(c, 4.0, (n, 3)) for c, n in (((0, 0, 0), 200), ((14, 0, 0), 150), ((0, 15, 3), 120))])
+    f = hrng.choice(elements, len(xyz))
+    hydrate_case("hydrate_moves_3bodies", xyz, f, [200, 150, 120], 173,
+                 moves=[(0, rotation((1, 0.3, -0.4), 0.3), np.array([-6.0, 2.0, 1.0])),
+                        (2, rotation((0, 1, 0), -0.2), np.array([3.0, 9.0, -2.0]))])
+    path = os.path.join(files, "2epe.pdb")
+    if os.path.exists(path):
+        xyz, _, f, _, _ = O.ref_read_structure(path)
+        hydrate_case("hydrate_pdb_2epe", xyz, f, [len(xyz)], 175)
     # SmartFitter fits with the Golden minimiser, one parameter each (seeded noise streams of their own)
     frng = np.random.default_rng(7)
     xyz = frng.normal(0, 9, (400, 3))

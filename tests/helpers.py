@@ -12,9 +12,9 @@ RHO_W = 0.334
 
 def golden_cases(prefix=""):
     """Histogram/intensity fixtures (grid excluded-volume, fit and calculator fixtures are listed by
-    grid_cases, fit_cases and calc_cases; the multi-step partial-manager fixtures belong to their own test)."""
+    grid_cases, fit_cases and calc_cases; the multi-step partial-manager and hydration fixtures belong to their own tests)."""
     return sorted(n for n in (os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, prefix + "*.npz")))
-                  if not n.startswith(("gridexv_", "fit_", "calc_", "partial_")))
+                  if not n.startswith(("gridexv_", "fit_", "calc_", "partial_", "hydrate_")))
 
 
 def grid_cases():
