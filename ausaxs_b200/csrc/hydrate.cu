@@ -52,7 +52,7 @@ constexpr double kNoiseSigma = 0.75;      // RadialHydration's default noise (Ra
 constexpr uint8_t kVolume = 1, kACenter = 4, kAArea = 8, kBlock = kACenter | kAArea;
 constexpr int kListThreads = 1024;        // one candidate per thread in the list passes
 constexpr int kMaxRounds = 1 << 16;
-constexpr int kBatch = 8;                 // rounds between read-backs of the round counters
+constexpr int kBatch = 16;                // rounds between read-backs of the round counters
 
 // constants::radius::get_vdw_radius(form_factor_t) (FormFactorType.h:173-192): H 1.1, C-family 1.96,
 // N-family 1.79, O / OH 1.71, S / SH 2.06, OTHER (Ar) 1.88, UNKNOWN 0 A
@@ -243,10 +243,49 @@ __device__ __forceinline__ Cand candidate(long long c, const double* __restrict_
     return K;
 }
 
+// The collision check against the atoms alone, every other cell counted as possibly blocked: true when
+// the candidate fails whatever the waters before it do (three or more 1rh probes on atoms, or a score
+// that cannot exceed min_score * 3 * 26).  Reads the cell bytes only.
+__device__ __forceinline__ bool fails_on_atoms(const int b[3], const HGrid& G, const uint8_t* __restrict__ cells) {
+    int inside = 0, smax = 0;
+#pragma unroll 2
+    for (int i = 0; i < kHydDirections; ++i) {
+        int q1[3], q3[3], q5[3];
+        bool oob3 = false, oob5 = false;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            q1[d] = min(max(b[d] + c_dirs.p1[i][d], 0), G.bins[d] - 1);
+            q3[d] = b[d] + c_dirs.p3[i][d];
+            q5[d] = b[d] + c_dirs.p5[i][d];
+            oob3 = oob3 || q3[d] < 0 || q3[d] >= G.bins[d];
+            oob5 = oob5 || q5[d] < 0 || q5[d] >= G.bins[d];
+        }
+        const uint8_t s1 = cells[cell_at(G, q1[0], q1[1], q1[2])];
+        const uint8_t s3 = oob3 ? 0 : cells[cell_at(G, q3[0], q3[1], q3[2])];
+        const uint8_t s5 = oob5 ? 0 : cells[cell_at(G, q5[0], q5[1], q5[2])];
+        if (s1 & kBlock) {
+            ++inside;
+            continue;
+        }
+        int ghi;
+        if (oob3) ghi = 2;
+        else if (s3 & kBlock) ghi = -2;
+        else ghi = 2 + (oob5 ? 1 : ((s5 & kBlock) ? -1 : 0));
+        smax += max(ghi, 0);
+    }
+    return inside >= 3 || smax <= kMinScore * 3 * kHydDirections;
+}
+
 __global__ void hyd_count(long long n_cand, const double* xyz, const int32_t* ff, const double* noise,
-                          unsigned long long seed, HGrid G, const uint8_t* cells, unsigned int* block_counts) {
+                          unsigned long long seed, HGrid G, const uint8_t* cells, uint8_t* flags,
+                          unsigned int* block_counts) {
     const long long c = blockIdx.x * (long long)kListThreads + threadIdx.x;
-    const bool keep = c < n_cand && candidate(c, xyz, ff, noise, seed, G, cells).keep;
+    bool keep = false;
+    if (c < n_cand) {
+        const Cand K = candidate(c, xyz, ff, noise, seed, G, cells);
+        keep = K.keep && !fails_on_atoms(K.b, G, cells);
+        flags[c] = keep;
+    }
     const int n = __syncthreads_count(keep);
     if (threadIdx.x == 0) block_counts[blockIdx.x] = (unsigned int)n;
 }
@@ -315,15 +354,13 @@ struct List {
 };
 
 __global__ void hyd_write(long long n_cand, const double* xyz, const int32_t* ff, const double* noise,
-                          unsigned long long seed, HGrid G, const uint8_t* cells, const unsigned int* offsets, List L) {
+                          unsigned long long seed, HGrid G, const uint8_t* cells, const uint8_t* flags,
+                          const unsigned int* offsets, List L) {
     __shared__ unsigned int warp_base[kListThreads / 32];
     const long long c = blockIdx.x * (long long)kListThreads + threadIdx.x;
     Cand K{};
-    bool keep = false;
-    if (c < n_cand) {
-        K = candidate(c, xyz, ff, noise, seed, G, cells);
-        keep = K.keep;
-    }
+    const bool keep = c < n_cand && flags[c];
+    if (keep) K = candidate(c, xyz, ff, noise, seed, G, cells);
     const unsigned int rank = block_rank(keep, warp_base);
     if (!keep) return;
     const long long e = (long long)offsets[blockIdx.x] + rank;
@@ -394,14 +431,16 @@ __device__ __forceinline__ int probe_value(const ProbeData& p, int c, uint32_t a
 // (RadialHydration.cpp:143-205) over three-valued cells, giving bounds of its 1rh count and score
 // terms; lane 26 reads the candidate's own cell.  The warp sums the bounds; c is accepted when
 // every outcome passes (own cell free, at most 2 blocked 1rh probes, score > min_score * 3 * 26),
-// rejected when every outcome fails, and otherwise goes to the next round's list.  An accepted
-// candidate's marks are written by 25 lanes, one box column each.
+// rejected when every outcome fails, and otherwise goes to the next round's list.  The marks of an
+// accepted candidate (into the accepted keys) or of one that stays undecided (into the other array of
+// undecided keys, read by the next round) are written by 25 lanes, one box column each.
 __global__ void __launch_bounds__(256) hyd_evaluate(List L, const unsigned int* __restrict__ active,
                                                    const unsigned long long* __restrict__ n_active, unsigned int* next,
                                                    unsigned long long* n_next, HGrid G, const uint8_t* __restrict__ cells,
                                                    unsigned long long* keys_acc,
-                                                   const unsigned long long* __restrict__ keys_und, uint32_t acc_hi,
-                                                   uint32_t und_hi) {
+                                                   const unsigned long long* __restrict__ keys_und,
+                                                   unsigned long long* keys_und_next, uint32_t acc_hi, uint32_t und_hi,
+                                                   uint32_t und_hi_next) {
     const long long n = (long long)*n_active;
     const int lane = threadIdx.x & 31;
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
@@ -475,14 +514,16 @@ __global__ void __launch_bounds__(256) hyd_evaluate(List L, const unsigned int* 
         }
         if (verdict == 0) {
             if (lane == 0) next[atomicAdd(n_next, 1ull)] = e;
-            continue;
+        } else if (lane == 0) {
+            L.state[e] = (int8_t)verdict;
         }
-        if (lane == 0) L.state[e] = (int8_t)verdict;
-        if (verdict == 1 && lane < kWBox * kWBox) {
+        if (verdict != -1 && lane < kWBox * kWBox) {
+            // accepted: its marks for every later reader; still undecided: its marks for the next round
             const double x[3] = {L.x[e], L.x[L.cap + e], L.x[2 * L.cap + e]};
-            const unsigned long long key = key_of(acc_hi, c);
+            unsigned long long* keys = verdict == 1 ? keys_acc : keys_und_next;
+            const unsigned long long key = key_of(verdict == 1 ? acc_hi : und_hi_next, c);
             water_marks_column(G, cells, x, b, lane / kWBox - 2, lane % kWBox - 2,
-                               [&](size_t q) { atomicMin(keys_acc + q, key); });
+                               [&](size_t q) { atomicMin(keys + q, key); });
         }
     }
 }
@@ -587,18 +628,19 @@ void Hydrator::generate(Ctx& C, const uint8_t* cells, const double gmin[3], cons
         dirs_device = C.device;
     }
     const HGrid G = to_grid(gmin, bins);
+    // key grids: accepted, and two of undecided (round r reads one, writes the next round's into the other)
     if (key_cells < ncells) {
-        keys.ensure(align_up(2 * ncells * 8, 256));
-        AUSAXS_CUDA(cudaMemsetAsync(keys.p, 0xff, 2 * ncells * 8, s));
+        keys.ensure(align_up(3 * ncells * 8, 256));
+        AUSAXS_CUDA(cudaMemsetAsync(keys.p, 0xff, 3 * ncells * 8, s));
         key_cells = ncells;
         call_epoch = round_epoch = 0;
     }
-    if (call_epoch > 0xfffff000u || round_epoch > 0xfffff000u) {
-        AUSAXS_CUDA(cudaMemsetAsync(keys.p, 0xff, 2 * key_cells * 8, s));
+    if (call_epoch > 0xfff00000u || round_epoch > 0xfff00000u) {
+        AUSAXS_CUDA(cudaMemsetAsync(keys.p, 0xff, 3 * key_cells * 8, s));
         call_epoch = round_epoch = 0;
     }
     unsigned long long* keys_acc = keys.as<unsigned long long>();
-    unsigned long long* keys_und = keys_acc + key_cells;
+    unsigned long long* keys_und[2] = {keys_acc + key_cells, keys_acc + 2 * key_cells};
     const uint32_t acc_hi = 0xffffffffu - (++call_epoch);
     const long long cap = std::max(1LL, n_cand);
     size_t off = 0;
@@ -615,7 +657,7 @@ void Hydrator::generate(Ctx& C, const uint8_t* cells, const double gmin[3], cons
     const long long nblocks = std::max(1LL, (n_cand + kListThreads - 1) / kListThreads);
     off = 0;
     const size_t o_counts = take(nblocks * 4), o_total = take(8), o_rounds = take((kMaxRounds + 1) * 8),
-                 o_acc_total = take(8);
+                 o_acc_total = take(8), o_flags = take(cap);
     off_waters = take(3 * cap * 8);
     off_cands = take(cap * 8);
     work.ensure(off);
@@ -623,21 +665,28 @@ void Hydrator::generate(Ctx& C, const uint8_t* cells, const double gmin[3], cons
     unsigned long long* total = work.as<unsigned long long>(o_total);
     unsigned long long* round_n = work.as<unsigned long long>(o_rounds);
     unsigned long long* acc_total = work.as<unsigned long long>(o_acc_total);
+    uint8_t* flags = work.as<uint8_t>(o_flags);
 
     cudaEvent_t ev;
     C.time_begin(5, &ev);
     AUSAXS_CUDA(cudaMemsetAsync(total, 0, 8, s));
-    const int threads = 256;
     if (n > 0) {
-        hyd_count<<<(unsigned)nblocks, kListThreads, 0, s>>>(n_cand, atoms, ff, noise, seed, G, cells, counts);
+        hyd_count<<<(unsigned)nblocks, kListThreads, 0, s>>>(n_cand, atoms, ff, noise, seed, G, cells, flags, counts);
         C.check_launch("hydration candidates");
         hyd_scan<<<1, 1024, 0, s>>>(counts, (int)nblocks, total);
         C.check_launch("hydration scan");
-        hyd_write<<<(unsigned)nblocks, kListThreads, 0, s>>>(n_cand, atoms, ff, noise, seed, G, cells, counts, L);
+        hyd_write<<<(unsigned)nblocks, kListThreads, 0, s>>>(n_cand, atoms, ff, noise, seed, G, cells, flags, counts, L);
         C.check_launch("hydration list");
     }
-    // rounds, in batches between read-backs of the counters of undecided candidates
+    // the first round's undecided keys: every listed candidate
     const int grid_rounds = C.sm_count * 8;
+    const int threads = 256;
+    uint32_t epoch = ++round_epoch;
+    if (n > 0) {
+        hyd_scatter<<<grid_rounds, threads, 0, s>>>(L, L.active[0], total, G, cells, keys_und[0], 0xffffffffu - epoch);
+        C.check_launch("hydration scatter");
+    }
+    // rounds, in batches between read-backs of the counters of undecided candidates
     std::vector<unsigned long long> h(kBatch);
     unsigned long long left = 0;
     C.time_end(5, ev);
@@ -651,12 +700,12 @@ void Hydrator::generate(Ctx& C, const uint8_t* cells, const double gmin[3], cons
         AUSAXS_CUDA(cudaMemsetAsync(round_n + r + 1, 0, kBatch * 8, s));
         for (int k = 0; k < kBatch; ++k, ++r) {
             const unsigned long long* n_in = r == 0 ? total : round_n + r;
-            const uint32_t und_hi = 0xffffffffu - (++round_epoch);
-            hyd_scatter<<<grid_rounds, threads, 0, s>>>(L, L.active[r & 1], n_in, G, cells, keys_und, und_hi);
-            C.check_launch("hydration scatter");
+            const uint32_t next_epoch = ++round_epoch;
             hyd_evaluate<<<grid_rounds, threads, 0, s>>>(L, L.active[r & 1], n_in, L.active[(r + 1) & 1], round_n + r + 1, G,
-                                                      cells, keys_acc, keys_und, acc_hi, und_hi);
-            C.check_launch("hydration evaluate");
+                                                      cells, keys_acc, keys_und[r & 1], keys_und[(r + 1) & 1], acc_hi,
+                                                      0xffffffffu - epoch, 0xffffffffu - next_epoch);
+            C.check_launch("hydration round");
+            epoch = next_epoch;
         }
         C.time_end(5, ev);
         AUSAXS_CUDA(cudaMemcpyAsync(h.data(), round_n + r - kBatch + 1, kBatch * 8, cudaMemcpyDeviceToHost, s));
