@@ -72,7 +72,9 @@ struct Dirs {
     double u[kHydDirections][3];
     int p1[kHydDirections][3], p3[kHydDirections][3], p5[kHydDirections][3];
 };
-__constant__ Dirs c_dirs;
+__constant__ Dirs c_dirs;  // read with one index across the warp (a broadcast)
+__device__ Dirs g_dirs;    // the same, read with a different index per lane: through the L1, since the
+                           // constant cache serialises a warp's distinct addresses
 
 // RadialHydration::prepare_rotations(8) (RadialHydration.cpp:73-141): theta, phi over one octant in
 // steps of 2 pi / 8, reflected into the eight octants, components under 1e-5 zeroed, duplicates
@@ -235,7 +237,7 @@ __device__ __forceinline__ Cand candidate(long long c, const double* __restrict_
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         const double nz = noise ? noise[3 * c + d] : (seed ? gauss(seed, c, d) : 0.0);
-        K.x[d] = fma(c_dirs.u[r][d], reff, __dadd_rn(xyz[3 * a + d], nz));
+        K.x[d] = fma(__ldg(&g_dirs.u[r][d]), reff, __dadd_rn(xyz[3 * a + d], nz));
         K.b[d] = (int)round(K.x[d] - G.gmin[d]);
         valid = valid && K.b[d] >= 0 && K.b[d] < G.bins[d];
     }
@@ -457,9 +459,9 @@ __global__ void __launch_bounds__(256) hyd_evaluate(List L, const unsigned int* 
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
                 const int bd = d == 0 ? b.x : (d == 1 ? b.y : b.z);
-                q1[d] = min(max(bd + c_dirs.p1[lane][d], 0), G.bins[d] - 1);
-                q3[d] = bd + c_dirs.p3[lane][d];
-                q5[d] = bd + c_dirs.p5[lane][d];
+                q1[d] = min(max(bd + __ldg(&g_dirs.p1[lane][d]), 0), G.bins[d] - 1);
+                q3[d] = bd + __ldg(&g_dirs.p3[lane][d]);
+                q5[d] = bd + __ldg(&g_dirs.p5[lane][d]);
                 oob3 = oob3 || q3[d] < 0 || q3[d] >= G.bins[d];
                 oob5 = oob5 || q5[d] < 0 || q5[d] >= G.bins[d];
             }
@@ -625,6 +627,7 @@ void Hydrator::generate(Ctx& C, const uint8_t* cells, const double gmin[3], cons
     if (dirs_device != C.device) {
         const Dirs D = make_dirs();
         AUSAXS_CUDA(cudaMemcpyToSymbol(c_dirs, &D, sizeof(D)));
+        AUSAXS_CUDA(cudaMemcpyToSymbol(g_dirs, &D, sizeof(D)));
         dirs_device = C.device;
     }
     const HGrid G = to_grid(gmin, bins);

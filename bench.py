@@ -938,7 +938,7 @@ def run_hydrate(args, rank, world, local_rank):
                      "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": None,
                      "algorithmic_bytes": int(alg), "kernel_ms_per_step": kernel_ms,
                      "kernel_intervals_per_step": k_n / args.steps,
-                     "note": "latency-bound: the rounds (scatter + evaluate each) run in batches of 8 between "
+                     "note": "latency-bound: the rounds (one kernel each) run in batches of 16 between "
                              "read-backs; the intervals exclude the host gaps at the read-backs"},
         "clocks": clk.summary(),
         "peaks_source": peak_kind,
