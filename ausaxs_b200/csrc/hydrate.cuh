@@ -21,7 +21,7 @@ void hydration_remove(Ctx& C, uint8_t* cells, const double gmin[3], const int bi
 struct Hydrator {
     DevBuf in;      // atoms (double, n x 3), form-factor types, noise table
     DevBuf cells;   // cell states of one-shot calls
-    DevBuf keys;    // [2][key_cells] epoch-tagged minimum candidate indices (accepted, undecided)
+    DevBuf keys;    // [3][key_cells] epoch-tagged minimum candidate indices (accepted, two undecided)
     size_t key_cells = 0;
     DevBuf list;    // candidates that survive the static tests, in candidate order, and their state
     DevBuf work;    // block counts, round counters, output staging
