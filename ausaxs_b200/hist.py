@@ -438,6 +438,20 @@ class PartialHistogramManagerMT:
         self.waters = pack(self.water_xyz, self.waters[:, 3].copy(), False)
         self.water_changed = True
 
+    def set_waters(self, xyz, weights):
+        """A new hydration of any size (Molecule::generate_new_hydration after a move, SimpleController.cpp:76):
+        the hydration counts as modified, so the water self partial and every body-water partial are
+        recomputed (PartialHistogramManagerMT.cpp:82-108)."""
+        xyz = np.array(xyz, np.float64).reshape(-1, 3)
+        B = len(self.records)
+        if len(xyz) == 0:
+            self.water_xyz = self.waters = None
+            self.ww_p, self.aw_p = None, [None] * B
+        else:
+            self.water_xyz = xyz
+            self.waters = pack(xyz, np.asarray(weights, np.float64).reshape(-1), False)
+        self.water_changed = True
+
     @staticmethod
     def _rigid(xyz, R, t):
         # Body::rotate then Body::translate: x <- R x (row sums left to right, Vector3.h:169-181), then x + t

@@ -96,3 +96,70 @@ def test_device_manager_matches_reference():
                    f"{key} step {step}")
         d_bound = bw * 2.0 ** -15 + (np.arange(len(r["d_axis"])) + 1) * bw * 2.0 ** -24 + 1e-9
         within(r["d_axis"], g[f"d_axis{step}"], d_bound, f"d_axis step {step}")
+
+
+@pytest.mark.gpu
+def test_rigid_body_step_with_regenerated_hydration():
+    """One step of the reference's rigid-body loop on device entry points only: a body moves (the kept
+    hydration grid loses it at its old coordinates and gets it back at the new ones), the hydration is
+    regenerated, and the partial manager recomputes the moved body's cross partials and every water
+    partial.  Checked against the oracle: the kept-grid hydration restatement for the waters, and its
+    SimpleCalculator partials combined as the reference combines them for the histograms."""
+    from ausaxs_b200 import _capi, synth
+    from tests.test_gpu_calc import within
+
+    rng = np.random.default_rng(5)
+    sizes = [400, 300, 250]
+    xyz = [rng.normal(c, 5.0, (n, 3)) for c, n in zip(((0, 0, 0), (16, 0, 0), (0, 17, 0)), sizes)]
+    ff = [rng.choice([3, 7, 11, 12], n).astype(np.int32) for n in sizes]
+    wts = [synth.ff_charge(f) for f in ff]
+    allx, allf = np.concatenate(xyz), np.concatenate(ff)
+    axes = O.hydrate_axes(allx)
+    ctx = _capi.default_context()
+    grid, ora = _capi.HydrationGrid(ctx, axes), O.HydrationGrid(axes)
+    try:
+        for gr in (grid, ora):
+            gr.add(allx, allf)
+        waters, _, _ = grid.hydrate(allx, allf)
+        np.testing.assert_array_equal(waters, ora.hydrate(allx, allf)[0])
+        bw = 0.25
+        m = hist.PartialHistogramManagerMT(list(zip(xyz, wts)), (waters, np.full(len(waters), hist.WATER_CHARGE)), bw,
+                                           8000, ctx)
+        m.calculate_all()
+        first = [np.column_stack([x, w]).astype(np.float32) for x, w in zip(xyz, wts)]
+        # move body 1 about its centre, as the rigid-body transforms do
+        k, ang = 1, 0.3
+        R = np.array([[np.cos(ang), -np.sin(ang), 0], [np.sin(ang), np.cos(ang), 0], [0, 0, 1]])
+        c = xyz[k].mean(0)
+        new = (xyz[k] - c) @ R.T + c + np.array([1.5, -2.0, 0.7])
+        for gr in (grid, ora):
+            gr.remove(xyz[k], ff[k])
+            gr.add(new, ff[k])
+        xyz[k] = new
+        order = [0, 2, 1]  # the re-added body comes last in the grid's member list
+        members, types = np.concatenate([xyz[b] for b in order]), np.concatenate([ff[b] for b in order])
+        waters2, _, _ = grid.hydrate(members, types)
+        np.testing.assert_array_equal(waters2, ora.hydrate(members, types)[0])
+        m.set_body_coordinates(k, new)
+        m.set_waters(waters2, np.full(len(waters2), hist.WATER_CHARGE))
+        h = m.calculate_all()
+    finally:
+        grid.close()
+    B = len(sizes)
+    cur = [np.column_stack([x, w]).astype(np.float32) for x, w in zip(xyz, wts)]
+    wrec = np.column_stack([waters2, np.full(len(waters2), hist.WATER_CHARGE)]).astype(np.float32)
+    jobs = [(b, None, 1, b) for b in range(B)] + [(2 * B, None, 1, B)]
+    jobs += [(B + i, B + j, 1, i * B + j) for i in range(B) for j in range(i)]
+    jobs += [(B + i, 2 * B, 1, B * B + i) for i in range(B)]
+    o = O.calculator(first + cur + [wrec], jobs, bw, 8000)
+    ref = hist.combine_partials([o[(0, b)] for b in range(B)], [o[(1, i * B + j)] for i in range(B) for j in range(i)],
+                                [o[(1, B * B + i)] for i in range(B)], o[(0, B)], bw)
+    got = {"aa": h.get_aa_counts(), "aw": h.get_aw_counts(), "ww": h.get_ww_counts(), "tot": h.get_counts(),
+           "d_axis": h.get_d_axis()}
+    assert len(got["tot"]) == ref["max_bin"]
+    wmax2 = max(float(np.max(np.concatenate(wts))), hist.WATER_CHARGE) ** 2
+    n_pairs = np.abs(ref["tot"]) / min(float(np.min(np.concatenate(wts))), hist.WATER_CHARGE) ** 2 + 1
+    for key in ("aa", "aw", "ww", "tot"):
+        within(got[key], ref[key], 4 * n_pairs * wmax2 * 2.0 ** -30 + 1e-12 * np.abs(ref[key]).max(), key)
+    within(got["d_axis"], ref["d_axis"], bw * 2.0 ** -15 + (np.arange(len(ref["d_axis"])) + 1) * bw * 2.0 ** -24 + 1e-9,
+           "d_axis")
