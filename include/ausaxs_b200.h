@@ -389,7 +389,8 @@ AUSAXS_API int ausaxs_hydrate_axes(const double* atoms, int64_t n_atoms, double*
  * its centre cells their A_CENTER mark; SingleTransform.cpp:20-69), add it at the new ones, and
  * hydrate.  hydrate takes the grid's member atoms in the grid's order (a re-added body comes last)
  * and otherwise behaves as ausaxs_gpu_hydrate.  Atoms must lie inside the axes.  The grid belongs to
- * the context it was made with; calls on it synchronise that context's stream.
+ * the context it was made with (destroy the grid before the context); calls on it synchronise that
+ * context's stream.
  */
 typedef struct ausaxs_gpu_hydration_grid ausaxs_gpu_hydration_grid;
 AUSAXS_API int ausaxs_gpu_hydration_grid_create(ausaxs_gpu_ctx* ctx, const double* axes, ausaxs_gpu_hydration_grid** out);
