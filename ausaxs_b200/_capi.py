@@ -28,7 +28,7 @@ MANAGER_FFAVG = 2
 MANAGER_FFEXPLICIT = 3
 MANAGER_FFGRID = 4
 
-# every symbol include/ausaxs_b200.h declares
+# every symbol include/ausaxs_b200.h and include/ausaxs_b200_diag.h declare
 EXPORTED = [
     "ausaxs_gpu_ctx_create", "ausaxs_gpu_ctx_destroy", "ausaxs_gpu_ctx_set_stream", "ausaxs_gpu_ctx_launch_count",
     "ausaxs_gpu_last_error", "ausaxs_gpu_ctx_enable_timing", "ausaxs_gpu_ctx_kernel_time",
@@ -43,7 +43,8 @@ EXPORTED = [
     "ausaxs_gpu_calculator_enqueue_cross", "ausaxs_gpu_calculator_run", "ausaxs_gpu_calculator_result_ids",
     "ausaxs_gpu_calculator_result",
     "ausaxs_gpu_batch_create", "ausaxs_gpu_batch_destroy", "ausaxs_gpu_batch_autotune", "ausaxs_gpu_batch_candidate",
-    "ausaxs_gpu_batch_profile_device", "ausaxs_gpu_batch_profile", "ausaxs_gpu_batch_histogram",
+    "ausaxs_gpu_batch_profile_device", "ausaxs_gpu_batch_profile", "ausaxs_gpu_batch_pair_time",
+    "ausaxs_gpu_batch_histogram", "ausaxs_gpu_smem_atomic_rate",
     "ausaxs_gpu_server_create", "ausaxs_gpu_server_destroy", "ausaxs_gpu_server_admit", "ausaxs_gpu_server_release",
     "ausaxs_gpu_server_usage", "ausaxs_gpu_server_submit", "ausaxs_gpu_server_poll", "ausaxs_gpu_server_wait",
     "ausaxs_gpu_server_completed", "ausaxs_gpu_server_launch_count", "ausaxs_gpu_server_body_center", "ausaxs_gpu_server_coordinates", "ausaxs_gpu_server_histogram",
@@ -148,7 +149,9 @@ def load():
         L.ausaxs_gpu_batch_candidate.argtypes = [C.c_int32, i32, i32, i32, i32]
         L.ausaxs_gpu_batch_profile_device.argtypes = [vp, f64, C.c_int32, C.POINTER(DebyeParams), f64]
         L.ausaxs_gpu_batch_profile.argtypes = [vp, f64, C.c_int32, C.POINTER(DebyeParams), f64]
+        L.ausaxs_gpu_batch_pair_time.argtypes = [vp, f64]
         L.ausaxs_gpu_batch_histogram.argtypes = [vp, C.c_int32, C.POINTER(HistResult)]
+        L.ausaxs_gpu_smem_atomic_rate.argtypes = [C.c_int32, C.c_int32, f64, f64]
         L.ausaxs_gpu_server_create.argtypes = [C.c_int32, C.c_int64, C.c_int32, C.c_int32, C.POINTER(vp)]
         L.ausaxs_gpu_server_destroy.argtypes = [vp]
         L.ausaxs_gpu_server_admit.argtypes = [vp, C.POINTER(HistConfig), C.c_int32, f32, i64, f32, i64, C.c_double,
@@ -176,6 +179,13 @@ def load():
                                                         i64, i32]
         _lib = L
         return L
+
+
+def smem_atomic_rate(device: int = 0, conflict_free: bool = True):
+    """(shared-memory atomics per second over the device, kernel milliseconds)."""
+    r, ms = C.c_double(0.0), C.c_double(0.0)
+    check(load().ausaxs_gpu_smem_atomic_rate(device, int(conflict_free), C.byref(r), C.byref(ms)))
+    return r.value, ms.value
 
 
 def check(rc: int):
@@ -580,6 +590,12 @@ class Batch:
 
     def profile_device(self, q_dev, nq: int, params: DebyeParams, I_dev):
         check(load().ausaxs_gpu_batch_profile_device(self.h, devptr(q_dev), nq, C.byref(params), devptr(I_dev)))
+
+    def pair_time(self) -> float:
+        """Device milliseconds of the last profile's pair stage (waits for it)."""
+        ms = C.c_double(0.0)
+        check(load().ausaxs_gpu_batch_pair_time(self.h, C.byref(ms)))
+        return ms.value
 
     def histogram(self, index: int, bin_count: int):
         bufs = {k: np.zeros(n) for k, n in [("aa", 225 * bin_count), ("aw", 15 * bin_count), ("ww", bin_count),

@@ -61,6 +61,9 @@ struct Batch {
     int n_zero = 0;
     cudaStream_t side[2] = {nullptr, nullptr};
     cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
+    // recorded around the pair stage inside the captured profile: the pair launches' device time of
+    // the last replay (ausaxs_gpu_batch_pair_time)
+    cudaEvent_t pair_t0 = nullptr, pair_t1 = nullptr;
     // captured profile
     cudaGraphExec_t exec = nullptr;
     struct Key {
@@ -80,6 +83,8 @@ struct Batch {
         if (fork) cudaEventDestroy(fork);
         for (auto& e : join)
             if (e) cudaEventDestroy(e);
+        if (pair_t0) cudaEventDestroy(pair_t0);
+        if (pair_t1) cudaEventDestroy(pair_t1);
     }
 
     unsigned long long* overflow() const { return misc.as<unsigned long long>() + 16; }
@@ -160,6 +165,8 @@ struct Batch {
         for (auto& st : side) AUSAXS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
         AUSAXS_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
         for (auto& e : join) AUSAXS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        AUSAXS_CUDA(cudaEventCreate(&pair_t0));
+        AUSAXS_CUDA(cudaEventCreate(&pair_t1));
         std::lock_guard<std::mutex> lk(g_tune_mutex);
         auto it = g_tuned.find(shape());
         build(it != g_tuned.end() ? it->second : kDefaultCandidate);
@@ -247,7 +254,9 @@ struct Batch {
     }
 
     void enqueue_all(int nq, cudaStream_t s) {
+        AUSAXS_CUDA(cudaEventRecord(pair_t0, s));
         enqueue_pairs(s);
+        AUSAXS_CUDA(cudaEventRecord(pair_t1, s));
         ff_finalize_batch_launch(fin.as<FinalizeFF>(), (int)items.size(), max_nb, s);
         ctx->check_launch("finalize");
         debye_fp64_batch_launch(args.as<DebyeArgs>(), (int)items.size(), nq, s);
@@ -429,6 +438,19 @@ int ausaxs_gpu_batch_profile(ausaxs_gpu_batch* b, const double* q, int32_t n_q, 
         AUSAXS_CUDA(cudaMemcpyAsync(&overflow, B.overflow(), 8, cudaMemcpyDeviceToHost, C.stream));
         AUSAXS_CUDA(cudaStreamSynchronize(C.stream));
         if (overflow) throw Error{AUSAXS_ERR_BIN_OVERFLOW, "pair distances beyond bin_count * bin_width; increase settings::axes::bin_count"};
+    });
+}
+
+int ausaxs_gpu_batch_pair_time(ausaxs_gpu_batch* b, double* ms) {
+    return guarded([&] {
+        if (!b || !ms) throw Error{AUSAXS_ERR_ARGUMENT, "null argument"};
+        Batch& B = b->impl;
+        AUSAXS_CUDA(cudaSetDevice(B.ctx->device));
+        if (!B.exec) throw Error{AUSAXS_ERR_ARGUMENT, "the batch has not been profiled"};
+        AUSAXS_CUDA(cudaEventSynchronize(B.pair_t1));
+        float t = 0;
+        AUSAXS_CUDA(cudaEventElapsedTime(&t, B.pair_t0, B.pair_t1));
+        *ms = t;
     });
 }
 

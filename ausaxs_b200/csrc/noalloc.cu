@@ -8,16 +8,22 @@
 // and get the histogram with no cudaMalloc, cudaFree or allocating library call.
 //
 // Limits and sharing rules:
-//   * at most kNoAllocMaxBins bins (the scratch array is sized for it: about 640 KiB, held on every
-//     device that loads this library until the process exits);
+//   * at most kNoAllocMaxBins bins (the scratch array is sized for it: 591,104 bytes, about 577 KiB,
+//     held on every device that loads this library until the process exits);
 //   * all calls share the one array and it keeps the last call's contents (everything that must
 //     start at zero is cleared by the call itself); calls that overlap on the GPU -- on different
-//     streams, or from different host threads -- race on it and give wrong results;
-//   * the first call on a device looks up the array's device address (cudaGetSymbolAddress) and
-//     caches it; make that first call before any stream capture.
+//     streams, or from different host threads -- race on it and give wrong results, so serialise
+//     the calls on one stream or order them with events;
+//   * the array's device address belongs to the CUDA context that loaded this module.  The first
+//     call in a context (per device, per context: a context created again after cudaDeviceReset
+//     counts as new) looks the address up with cudaGetSymbolAddress and caches it under the
+//     context's unique id; make that first call before any stream capture.
+#include <cuda.h>  // CUcontext and the driver entry point types only; libcuda is not linked
+
 #include <algorithm>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/ausaxs_b200.h"
 #include "finalize.cuh"
@@ -35,13 +41,51 @@ constexpr size_t kMiscBytes = 256;  // tile counters, overflow, weight scale, se
 constexpr size_t kSlotBytes = 3ull * kNoAllocMaxBins * 8;  // counts, offset sums, weight sums of one job
 constexpr size_t kScratchBytes = kJobBytes + kMiscBytes + 3 * kSlotBytes;
 
+static_assert(kScratchBytes == 591104, "the documented scratch size");
+
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
+// Device addresses of the scratch array, one per (device, context).  The context is identified by
+// cuCtxGetId, which is unique for the life of the process (a context created again at the same
+// handle gets a new id), reached through cudaGetDriverEntryPoint so that the library needs no link
+// against the driver library.  Where the driver does not provide it, the device alone is the key.
 struct ScratchAddr {
+    struct Entry {
+        int dev;
+        unsigned long long ctx_id;
+        void* ptr;
+    };
     std::mutex m;
-    void* ptr[64] = {};
+    std::vector<Entry> entries;
+    bool resolved = false;
+    CUresult (*ctx_get_current)(CUcontext*) = nullptr;
+    CUresult (*ctx_get_id)(CUcontext, unsigned long long*) = nullptr;
 };
 ScratchAddr g_addr;
+
+// The current context's id (0 when it cannot be determined).  Called with g_addr.m held.
+unsigned long long current_context_id() {
+    if (!g_addr.resolved) {
+        g_addr.resolved = true;
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        cudaDriverEntryPointQueryResult q1{}, q2{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+            q1 == cudaDriverEntryPointSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) == cudaSuccess &&
+            q2 == cudaDriverEntryPointSuccess) {
+            g_addr.ctx_get_current = reinterpret_cast<CUresult (*)(CUcontext*)>(f1);
+            g_addr.ctx_get_id = reinterpret_cast<CUresult (*)(CUcontext, unsigned long long*)>(f2);
+        }
+        cudaGetLastError();  // a failed lookup leaves nothing behind for the caller
+    }
+    if (!g_addr.ctx_get_current || !g_addr.ctx_get_id) return 0;
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (g_addr.ctx_get_current(&c) != CUDA_SUCCESS || !c) return 0;
+    if (g_addr.ctx_get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
 
 // Clears the scratch accumulators and writes the job table (passed by value, so no host copy).
 struct NoAllocInit {
@@ -81,18 +125,26 @@ extern "C" int ausaxs_gpu_histogram_mt_noalloc(const float* atoms, int32_t n_ato
         return fail(AUSAXS_ERR_ARGUMENT, "bin_width must be positive and bin_count at least 11");
     if (bin_count > kNoAllocMaxBins)
         return fail(AUSAXS_ERR_CAPACITY, "bin_count exceeds the allocation-free limit of 8192 bins");
+    // an error left behind by an earlier, unrelated call must not be reported as this call's
+    cudaGetLastError();
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return fail(AUSAXS_ERR_CUDA, "no current CUDA device");
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) return fail(AUSAXS_ERR_CUDA, "no current CUDA device");
+    // make the device's primary context current (initialised if it was not; a no-op when it already
+    // is) so that the context id below is the one the launches use
+    if (cudaSetDevice(dev) != cudaSuccess) return fail(AUSAXS_ERR_CUDA, "cannot initialise the CUDA context");
     void* base_ptr = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_addr.m);
-        if (!g_addr.ptr[dev]) {
+        const unsigned long long ctx_id = current_context_id();
+        for (const auto& e : g_addr.entries)
+            if (e.dev == dev && e.ctx_id == ctx_id) base_ptr = e.ptr;
+        if (!base_ptr) {
             void* p = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
             if (e != cudaSuccess || !p) return fail(AUSAXS_ERR_CUDA, cudaGetErrorString(e));
-            g_addr.ptr[dev] = p;
+            g_addr.entries.push_back({dev, ctx_id, p});
+            base_ptr = p;
         }
-        base_ptr = g_addr.ptr[dev];
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     char* base = static_cast<char*>(base_ptr);
@@ -158,11 +210,15 @@ extern "C" int ausaxs_gpu_histogram_mt_noalloc(const float* atoms, int32_t n_ato
         tiles_total += tiles;
     }
     init.clear_words = (kMiscBytes + 3 * kSlotBytes) / 8;
+    cudaError_t e = cudaSuccess;
     noalloc_init_kernel<<<64, 256, 0, s>>>(init);
-    cudaMemsetAsync(dmaxbin, 0, sizeof(int32_t), s);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(AUSAXS_ERR_CUDA, cudaGetErrorString(e));
+    if ((e = cudaMemsetAsync(dmaxbin, 0, sizeof(int32_t), s)) != cudaSuccess)
+        return fail(AUSAXS_ERR_CUDA, cudaGetErrorString(e));
     weight_scale_launch(A, n_atoms, W, n_waters, wscale, s);
     weight_square_sum_launch(A, n_atoms, self, s);
     weight_square_sum_launch(W, n_waters, self + 1, s);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(AUSAXS_ERR_CUDA, cudaGetErrorString(e));
     if (init.n_jobs > 0) {
         PairLaunch L{};
         L.jobs = reinterpret_cast<const PairJob*>(base);
@@ -176,12 +232,14 @@ extern "C" int ausaxs_gpu_histogram_mt_noalloc(const float* atoms, int32_t n_ato
         L.dreg = 0;
         L.wscale = wscale;
         const size_t smem = pairhist_smem_bytes(1, nb, true, kNoAllocTile);
-        int sms = 148;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        int sms = 0;
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess || sms <= 0)
+            return fail(AUSAXS_ERR_CUDA, "cannot query the multiprocessor count");
         const int per_sm = pairhist_ctas_per_sm(smem, kNoAllocTile, false);
         const int grid = (int)std::min<long long>((long long)sms * per_sm, std::max<long long>(1, tiles_total));
         L.chunk = (int)std::max<long long>(1, std::min<long long>(8, tiles_total / ((long long)grid * 8)));
         pairhist_launch(L, kNoAllocTile, grid, smem, s);
+        if ((e = cudaGetLastError()) != cudaSuccess) return fail(AUSAXS_ERR_CUDA, cudaGetErrorString(e));
     }
     FinalizeMT F{};
     F.nb = nb;
@@ -207,7 +265,6 @@ extern "C" int ausaxs_gpu_histogram_mt_noalloc(const float* atoms, int32_t n_ato
     F.d_axis = hist_out + 4 * (size_t)nb;  // row 4
     mt_finalize_launch(F, s);
     if (overflow_out) noalloc_copy_u64<<<1, 1, 0, s>>>(overflow, overflow_out);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return fail(AUSAXS_ERR_CUDA, cudaGetErrorString(e));
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(AUSAXS_ERR_CUDA, cudaGetErrorString(e));
     return AUSAXS_OK;
 }

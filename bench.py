@@ -1,17 +1,24 @@
 """Benchmark of the Debye hot path: I(q) profiles per second on a B200.
 
-One step = coordinates of one structure -> pair histograms -> FP64/tensor-core Debye transform ->
-I(q).  Default workload (single GPU): the WAXS configuration -- a 50,000-atom globule with 10,000
-shell waters and excluded-volume dummies on a 1 A grid filling the molecular volume, 0.1 A bins,
-1,000 q in [0.005, 1.0], HistogramManagerMTFFGrid semantics -- generated from a seed (no dataset).
+Default workload (single GPU): the batched configuration -- 256 independent globules, atom counts
+log-uniform in [500, 50,000], waters 20 % of the atoms, 0.25 A bins, 400 q in [0.005, 0.8],
+HistogramManagerMTFFAvg semantics, generated from a seed (no dataset).  One step = every
+structure's coordinates -> pair histograms -> FP64 Debye transform -> I(q), one CUDA-graph replay.
 
-  value : profiles/s with the structure resident in HBM (ausaxs_gpu_structure_profile)
-  e2e   : profiles/s through ausaxs_gpu_profile with pinned host buffers (H2D of the points and
-          D2H of I(q) inside every step)
+  value            : batched profiles/s, structures resident in HBM
+  plain_sequential : the same 256 profiles as 256 plain single-structure calls, and the ratio
+  e2e              : profiles/s through the C ABI from pinned host buffers (the batch created,
+                     profiled and destroyed every step: H2D of all points, D2H of every I(q))
+  roofline         : the pair kernel against min(FP32 bound, measured shared-atomic bound)
+  serving          : the rigid-body serving configuration (64 chains of 8-body assemblies): moves/s
+                     at saturation, p50/p99 latency at 25/50/75 % of it, lone-request latencies
 
+Other workloads (--workload): cfg0, cfg1 (50k-atom FFGrid, 1,000 q), cfg2 (500k-atom shell), cfg4
+(serving alone), gridexv, hydrate, fit, symmetry, atomics-peak.
 Under torchrun (N > 1) every rank runs its own replica (weak scaling).
 ``--impl reference`` times the reference implementation compiled from its sources (oracle/_ref)
-on the host cores, on a bounded sample of the same workload, scaled to profiles/s.
+on the host cores: for the default workload, whole structures of the batch in size-stratified
+chunks, one chunk per step, so the timed steps cover the batch once (no extrapolation).
 """
 from __future__ import annotations
 
@@ -34,6 +41,9 @@ INSTR_PER_PAIR = 39.8
 # DRAM bytes (read + write) of the three pair launches of one 50k-atom FFGrid profile: 3.12 MB measured
 # by ncu on the cfg1-shaped 10k-atom case (85,967 points), scaled by points to cfg1's 436,380
 PAIR_TRAFFIC_BYTES = 1.58e7
+# DRAM bytes (read + write) of the pair launches of one step of the 256-structure batch (ncu); None until
+# captured
+BATCH_PAIR_TRAFFIC_BYTES = None
 METRIC = "I(q) profiles/s & p99 latency vs plain GPU path at ≤1e-4 rel. I(q) error"
 UNIT = "profiles/s"
 
@@ -88,11 +98,12 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+        import tempfile
+
+        self.path = os.path.join(tempfile.gettempdir(), f"ausaxs_b200_clocks_{os.getpid()}_{id(self)}.csv")
 
     def __enter__(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
@@ -109,13 +120,19 @@ class ClockSampler:
             except Exception:
                 self.proc.kill()
             self.f.close()
+            self.text = open(self.path).read() if os.path.exists(self.path) else ""
+            try:
+                os.remove(self.path)
+            except OSError:
+                pass
 
     def summary(self):
-        if not self.proc or not os.path.exists(self.path):
+        text = getattr(self, "text", "")
+        if not self.proc or not text:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        for line in text.splitlines():
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -185,9 +202,34 @@ def time_reference(m, wl, steps: int, warmup: int, target_pairs: float = 4e9):
     return 1.0 / per, detail
 
 
-def time_reference_batch(wl, steps: int, warmup: int, target_pairs: float = 4e9):
-    """The reference on whole structures drawn at random from the batch until about target_pairs
-    pairs; the batch time is scaled by total pairs / sampled pairs.  Returns (profiles/s, details)."""
+def batch_chunks(wl, n_chunks: int):
+    """Size-stratified partition of a batch's structures into n_chunks chunks (structures ranked by
+    pair count, dealt round-robin), so that every chunk has the batch's size mix and the chunks
+    together are the whole batch."""
+    ranked = sorted(range(len(wl.molecules)), key=lambda i: -pair_count(wl.molecules[i], False))
+    n_chunks = max(1, min(n_chunks, len(ranked)))
+    return [ranked[c::n_chunks] for c in range(n_chunks)]
+
+
+def time_reference_structures(wl, picked, O):
+    """Seconds of the reference for the structures `picked`: calculate_all() + debye_transform() each.
+    The reference's FF-typed transform runs on its fixed 200-point q axis; its time is scaled to the
+    workload's q count (the transform is < 2 % of a structure's time)."""
+    t = 0.0
+    for i in picked:
+        m = wl.molecules[i]
+        rm = O.RefMolecule(m.atoms, m.weights, m.ff_types, m.waters, m.water_weights, volume=m.volume)
+        rm.set_manager(wl.manager)
+        h = rm.calculate()
+        _, _, _, t_debye = h.debye()
+        t += h.seconds + t_debye * (len(wl.q) / 200.0)
+    return t
+
+
+def time_reference_batch(wl, steps: int, warmup: int, n_chunks: int = 0):
+    """The reference over the batch in size-stratified chunks of whole structures: step k runs chunk
+    k mod n_chunks (n_chunks = steps by default, so the timed steps cover every structure once).
+    Returns (profiles/s = structures timed / seconds, details); nothing is extrapolated."""
     from oracle import py as O
 
     if not O.ref_available():
@@ -196,31 +238,51 @@ def time_reference_batch(wl, steps: int, warmup: int, target_pairs: float = 4e9)
     O.ref(threads)
     O.ref_set_axes(wl.bin_width, 8000, 1e-4, 1.0)
     O.ref_set_simple_exv(False)
-    total = sum(pair_count(m, False) for m in wl.molecules)
-    rng = np.random.default_rng(5)
-    picked, got = [], 0
-    for i in rng.permutation(len(wl.molecules)):
-        if got >= target_pairs:
-            break
-        picked.append(int(i))
-        got += pair_count(wl.molecules[i], False)
-    times = []
+    chunks = batch_chunks(wl, n_chunks or steps)
+    done, secs = 0, 0.0
     for it in range(warmup + steps):
-        t = 0.0
-        for i in picked:
-            m = wl.molecules[i]
-            rm = O.RefMolecule(m.atoms, m.weights, m.ff_types, m.waters, m.water_weights, volume=m.volume)
-            rm.set_manager(wl.manager)
-            h = rm.calculate()
-            _, _, _, t_debye = h.debye()
-            t += h.seconds + t_debye * (len(wl.q) / 200.0)
+        c = chunks[(it - warmup) % len(chunks)] if it >= warmup else chunks[(len(chunks) - 1 - it) % len(chunks)]
+        t = time_reference_structures(wl, c, O)
         if it >= warmup:
-            times.append(t * total / got)
-    per_batch = statistics.median(times)
+            done += len(c)
+            secs += t
+    covered = min(steps, len(chunks)) / len(chunks)
     detail = {"cores": threads, "kind": "reference",
-              "sample": (f"{len(picked)} whole structures of the {len(wl.molecules)} ({got / total:.4f} of the pairs); "
-                         f"batch time scaled by pairs, debye_transform() time by q count")}
-    return len(wl.molecules) / per_batch, detail
+              "sample": (f"{done} structures of the {len(wl.molecules)} in {steps} size-stratified chunks "
+                         f"({covered:.3f} of the batch; each structure: calculate_all() + debye_transform(), the "
+                         f"transform's 200-q time scaled to {len(wl.q)} q); no pair-count extrapolation"),
+              "seconds": secs}
+    return done / secs, detail
+
+
+def batch_config(wl):
+    """The workload's identity, printed unchanged by both arms."""
+    mols = wl.molecules
+    return {"workload": wl.name, "structures": len(mols), "atoms_total": int(sum(m.size_atom() for m in mols)),
+            "waters_total": int(sum(m.size_water() for m in mols)),
+            "pairs_per_step": int(sum(pair_count(m, False) for m in mols)), "bin_width": wl.bin_width,
+            "q_points": len(wl.q), "q_range": [float(wl.q[0]), float(wl.q[-1])], "manager": wl.manager,
+            "seed": 31}
+
+
+def pair_roofline(pairs_per_launch: float, kernel_ms: float, sm_mhz: float, sms: int, atomic_rate: float,
+                  atomics_per_pair: int, instr_per_pair: float):
+    """Roofline of the pair kernel as pair evaluations per second: the lower of the FP32 bound
+    (sms x 128 lanes x f_SM / 9 FP32 operations per pair) and the shared-atomic bound (measured
+    conflict-free atomics/s / atomics per pair).  A secondary figure compares against the issue rate
+    at the kernel's own instruction count (ncu)."""
+    achieved = pairs_per_launch / (kernel_ms / 1e3)
+    fp32 = sms * 128 * sm_mhz * 1e6 / 9.0
+    atom = atomic_rate / atomics_per_pair
+    peak = min(fp32, atom)
+    issue = sms * 4 * sm_mhz * 1e6 * 32 / instr_per_pair
+    return {"bound": "fp32" if fp32 <= atom else "smem_atomic", "kernel": "pairhist_kernel",
+            "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "Gpair/s", "frac": achieved / peak,
+            "fp32_bound": fp32 / 1e9, "smem_atomic_bound": atom / 1e9, "smem_atomics_per_s": atomic_rate,
+            "atomics_per_pair": atomics_per_pair, "sm_mhz": sm_mhz, "issue_frac": achieved / issue,
+            "instr_per_pair": instr_per_pair, "kernel_ms_per_step": kernel_ms,
+            "peak_source": (f"min({sms} SMs x 128 x {sm_mhz:.0f} MHz / 9 FP32 ops per pair, measured conflict-free "
+                            f"shared atomics / {atomics_per_pair} per pair)")}
 
 
 def run_batch(args, rank, world, local_rank):
@@ -248,6 +310,8 @@ def run_batch(args, rank, world, local_rank):
     q_dev = torch.tensor(wl.q, dtype=torch.float64, device=dev)
     I_dev = torch.zeros(n * nq, dtype=torch.float64, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    atomic_rate, _ = _capi.smem_atomic_rate(local_rank, True)
+    atomic_rate_random, _ = _capi.smem_atomic_rate(local_rank, False)
 
     def step():
         B._b.profile_device(q_dev, nq, params, I_dev)
@@ -262,6 +326,7 @@ def run_batch(args, rank, world, local_rank):
         launches0 = ctx.launches
         starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
         ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        pair_ms = []
         with ClockSampler(local_rank) as clk:
             torch.cuda.synchronize()
             for k in range(args.steps):
@@ -269,6 +334,7 @@ def run_batch(args, rank, world, local_rank):
                 step()
                 ends[k].record(stream)
                 flush.fill_(float(k))
+                pair_ms.append(B._b.pair_time())  # events inside the graph, read after the step ends
             torch.cuda.synchronize()
         launches = ctx.launches - launches0
         step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
@@ -311,8 +377,6 @@ def run_batch(args, rank, world, local_rank):
     # end to end through the C ABI from pinned host buffers (the compact records the caller holds):
     # every step creates the batch (H2D of all coordinates, census, plans), profiles it and reads
     # every I(q) back, then destroys it
-    import ctypes as C
-
     L = _capi.load()
     pin_a = torch.from_numpy(B._b._a).pin_memory()
     pin_w = torch.from_numpy(B._b._w).pin_memory()
@@ -333,52 +397,62 @@ def run_batch(args, rank, world, local_rank):
         if k >= args.warmup // 2:
             lat.append(time.perf_counter() - t0)
     Ie = pin_I.numpy().reshape(n, nq)
-    e2e = world * n * len(lat) / sum(lat)
+    e2e = world * n * len(lat) / max_over_ranks(sum(lat), world)
     e2e_diff = float(np.max(np.abs(Ie / I_batch - 1)))
 
     peaks, peak_kind = load_peaks()
-    pair_ms = cand_ms[choice]
     clocks = clk.summary()
     sm_mhz = clocks.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
     sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
-    issue_peak = sms * 4 * sm_mhz * 1e6 * 32 / INSTR_PER_PAIR
-    pair_rate = pairs / (pair_ms / 1e3)
+    kernel_ms = statistics.mean(pair_ms)
+    roof = pair_roofline(pairs, kernel_ms, sm_mhz, sms, atomic_rate, 2, INSTR_PER_PAIR)
+    roof["traffic"] = BATCH_PAIR_TRAFFIC_BYTES
+    roof["smem_atomics_per_s_random_bins"] = atomic_rate_random
+    roof["note"] = ("kernel_ms = device time of the pair stage (accumulator clearing + every pair launch of the "
+                    "graph), events inside the graph, mean over the timed steps; FFAvg pairs add two shared "
+                    "atomics (count, distance offset)")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 distances, u32/u64 integer bins, f64 transform", "data": "synthetic (seeded generator)",
-        "config": {"workload": wl.name, "structures": n, "atoms_total": int(sum(m.size_atom() for m in mols)),
-                   "pairs_per_step": pairs, "bin_width": wl.bin_width, "q_points": nq, "manager": wl.manager,
-                   "autotune": {"choice": choice, "candidate": _capi.Batch.candidate(choice),
-                                "pair_ms_per_candidate": [round(float(x), 3) for x in cand_ms[:7]]},
-                   "plain_sequential": {"value": plain_value, "unit": UNIT, "speedup": value / plain_value,
-                                        "max_rel_diff": plain_diff},
-                   "l2": "256 MiB buffer written between timed steps (outside the events)",
-                   "parallelism": f"replicas x{world}"},
+        "config": batch_config(wl),
+        "plain_sequential": {"value": plain_value, "unit": UNIT, "speedup_batched_vs_plain": value / plain_value,
+                             "max_rel_diff_vs_batched": plain_diff,
+                             "note": f"{n} resident structures, one ausaxs_gpu_structure_profile call each, in sequence"},
+        "autotune": {"choice": choice, "candidate": _capi.Batch.candidate(choice),
+                     "pair_ms_per_candidate": [round(float(x), 3) for x in cand_ms[:7]]},
+        "l2": "256 MiB buffer written between timed steps (outside the events)",
+        "parallelism": f"replicas x{world}",
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(n * nq * 8 + 8),
                 "p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
                 "max_rel_diff_vs_resident": e2e_diff,
                 "note": "C ABI from pinned host records: batch created every step (upload, census, plans), profiled, every I(q) read back, destroyed"},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "issue", "kernel": "pairhist_kernel", "achieved": pair_rate / 1e9,
-                     "peak": issue_peak / 1e9, "unit": "Gpair/s", "frac": pair_rate / issue_peak, "traffic": None,
-                     "peak_source": f"issue model: {sms} SMs x 4 x {sm_mhz:.0f} MHz x 32 / {INSTR_PER_PAIR} instr per pair",
-                     "pair_ms_per_step": pair_ms},
+        "roofline": roof,
         "clocks": clocks,
         "peaks_source": peak_kind,
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, det = time_reference_batch(wl, steps=1, warmup=0)
-        line["cpu_baseline"] = {"value": v, "unit": UNIT, **det} if v is not None else det
     B.close()
     ctx.close()
+    del flush
+    if args.workload == "cfg3" and not args.no_serving:
+        line["serving"] = serving_measure(args, rank, world, local_rank, compact=True)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, det = time_reference_batch(wl, steps=1, warmup=0, n_chunks=16)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, **det} if v is not None else det
     return line
 
 
 def run_serving(args, rank, world, local_rank):
+    return serving_measure(args, rank, world, local_rank, compact=False)
+
+
+def serving_measure(args, rank, world, local_rank, compact=False):
     """Rigid-body serving: 64 device-resident 8-body assemblies, one random rigid move per request,
     Poisson arrivals at several rates and a closed-loop saturation run; latency from the scheduled
-    arrival to the observed completion (host clock)."""
+    arrival to the observed completion (host clock).  Also the latency of a move submitted alone (no
+    other request in flight), for the largest body of every assembly and for random bodies.
+    compact: the figures as a sub-object of another workload's line."""
     import collections
 
     import torch
@@ -457,22 +531,42 @@ def run_serving(args, rank, world, local_rank):
                 "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                 "mean_ms": float(lat.mean())}
 
+    n_req = args.serve_requests or 5 * chains
     run(4 * chains, None)  # warm-up
     launches0 = S.launches()
     with ClockSampler(local_rank) as clk:
-        sat = run(args.steps * chains, None)
+        sat = run(n_req, None)
     sat_launches = S.launches() - launches0
     # whole job: every rank serves its own chains; the job lasts as long as its slowest rank
     sat_total = world * sat["requests"] / max_over_ranks(sat["requests"] / sat["moves_per_s"], world)
     sweep = []
-    for frac in (0.25, 0.5, 0.75, 0.9):
-        sweep.append(run(args.steps * chains, frac * sat["moves_per_s"]))
+    for frac in (0.25, 0.5, 0.75):
+        sweep.append(run(n_req, frac * sat["moves_per_s"]))
+
+    def lone(k, body):
+        R, tv = move(ids[k], body)
+        t0 = time.perf_counter()
+        S.wait(S.submit(ids[k], body, R, tv), ids[k])
+        return 1e3 * (time.perf_counter() - t0)
+
+    lone_largest = [lone(k, int(np.argmax(sizes[k]))) for k in range(chains)]
+    lone_random = [lone(k, int(rng.integers(0, 8))) for k in range(chains)]
     # pair evaluations of an average move: the moved body against every other body plus its own pairs
     per_move = []
     for sz in sizes:
         tot = sum(sz)
         per_move.append(np.mean([n * (tot - n) + n * (n - 1) / 2 for n in sz]))
     pairs_per_move = float(np.mean(per_move))
+    lone_stats = {"largest_body_p50_ms": float(np.percentile(lone_largest, 50)),
+                  "largest_body_max_ms": float(np.max(lone_largest)),
+                  "random_body_p50_ms": float(np.percentile(lone_random, 50)),
+                  "note": "one move submitted with nothing else in flight, submit to result on the host"}
+    if compact:
+        S.close()
+        return {"workload": f"cfg4: {chains} chains x 8-body assemblies, bodies 3k-20k atoms, 400 q, moves <= 5 deg + <= 2 A",
+                "moves_per_s_saturated": sat_total, "saturation": sat, "poisson_sweep": sweep, "lone": lone_stats,
+                "pairs_per_move_mean": pairs_per_move, "gpu_launches_saturated": int(sat_launches),
+                "clocks": clk.summary()}
     line = {
         "metric": "rigid-body moves/s (I(q) + chi2 per move) with p50/p99 latency", "value": sat_total,
         "unit": "moves/s", "n_gpus": world, "steps": args.steps, "warmup": 4, "ms_per_step": 1e3 / sat["moves_per_s"],
@@ -483,7 +577,7 @@ def run_serving(args, rank, world, local_rank):
                                f"moves <= 5 deg about the body centroid + <= 2 A",
                    "atoms_total": int(sum(sum(s) for s in sizes)), "pairs_per_move_mean": pairs_per_move,
                    "footprint_bytes_total": int(sum(footprints)), "admit_s": t_admit, "generate_s": t_gen,
-                   "saturation": sat, "poisson_sweep": sweep},
+                   "saturation": sat, "poisson_sweep": sweep, "lone": lone_stats},
         "e2e": {"value": sat_total, "unit": "moves/s", "h2d_bytes_per_step": 96,
                 "d2h_bytes_per_step": (nq + 5) * 8, "p50_ms": sat["p50_ms"], "p99_ms": sat["p99_ms"],
                 "note": "every request crosses the host ABI: pose in, I(q) and fit out"},
@@ -493,11 +587,12 @@ def run_serving(args, rank, world, local_rank):
     peaks, _ = load_peaks()
     sm_mhz = line["clocks"].get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
     sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
-    issue_peak = sms * 4 * sm_mhz * 1e6 * 32 / INSTR_PER_PAIR
-    achieved = pairs_per_move * sat["moves_per_s"]
-    line["roofline"] = {"bound": "issue", "kernel": "pairhist_kernel", "unit": "Gpair/s", "achieved": achieved / 1e9,
-                        "peak": issue_peak / 1e9, "frac": achieved / issue_peak, "traffic": None,
-                        "note": "pair evaluations of the saturated serving run (moved body x the rest + its own pairs)"}
+    atomic_rate, _ = _capi.smem_atomic_rate(local_rank, True)
+    # pair evaluations of the saturated run per second of it (every other stage of a request included)
+    line["roofline"] = pair_roofline(pairs_per_move, 1e3 / sat["moves_per_s"], sm_mhz, sms, atomic_rate, 2,
+                                     INSTR_PER_PAIR)
+    line["roofline"]["traffic"] = None
+    line["roofline"]["note"] = "pair evaluations of the saturated serving run (moved body x the rest + its own pairs)"
     S.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ref_args = argparse.Namespace(steps=1, warmup=0)
@@ -1259,7 +1354,37 @@ def reference_symmetry(sets, jobs, bw):
             "sample": f"the body's self and pair-class jobs ({frac:.3f} of the pairs), time scaled by pairs"}
 
 
+def run_atomics_peak(args, rank, world, local_rank):
+    """Shared-memory atomic throughput of the device (the second bound of the pair kernel's roofline)."""
+    import torch
+
+    from ausaxs_b200 import _capi
+
+    torch.cuda.set_device(local_rank)
+    runs = {True: [], False: []}
+    with ClockSampler(local_rank) as clk:
+        for _ in range(args.warmup + args.steps):
+            for cf in (True, False):
+                runs[cf].append(_capi.smem_atomic_rate(local_rank, cf))
+    cf = [r for r, _ in runs[True][args.warmup:]]
+    rnd = [r for r, _ in runs[False][args.warmup:]]
+    clocks = clk.summary()
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
+    v = statistics.median(cf)
+    return {"metric": "shared-memory 32-bit atomics/s (conflict-free lanes)", "value": v, "unit": "atomics/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": statistics.median([m for _, m in runs[True][args.warmup:]]), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (generated bins)",
+            "config": {"workload": "atomics-peak: every SM full of 512-thread CTAs, 4,096-word shared arrays"},
+            "random_bins": statistics.median(rnd),
+            "per_sm_per_clock": v / (sms * sm_mhz * 1e6), "random_bins_per_sm_per_clock": statistics.median(rnd) / (sms * sm_mhz * 1e6),
+            "clocks": clocks, "gpu_launches": 2 * 2 * (args.warmup + args.steps)}
+
+
 def run_reference(args, rank, world):
+    if args.workload == "atomics-peak":
+        return {"impl": "reference", "unavailable": "a device measurement: the reference has no GPU code"}
     if args.workload == "symmetry":
         sets, jobs, _, _ = symmetry_setup()
         det = reference_symmetry(sets, jobs, 0.1)
@@ -1307,9 +1432,21 @@ def run_reference(args, rank, world):
                 "e2e": {"value": v, "unit": GRID_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     wl = workload(args.workload)
     if args.workload == "cfg3":
-        v, det = time_reference_batch(wl, steps=args.steps, warmup=args.warmup, target_pairs=1e9)
-    else:
-        v, det = time_reference(wl.molecules[0], wl, steps=args.steps, warmup=args.warmup, target_pairs=2e9)
+        v, det = time_reference_batch(wl, steps=args.steps, warmup=args.warmup)
+        if v is None:
+            return {"impl": "reference", **det}
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * det["seconds"] / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32 distances, f64 bins and transform (reference CPU)",
+                "data": "synthetic (seeded generator)", "config": batch_config(wl),
+                "cpu_baseline": {"value": v, "unit": UNIT, **det},
+                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        if not args.no_serving:
+            r = run_reference_serving(argparse.Namespace(steps=2, warmup=0), world)
+            line["serving"] = {k: r.get(k) for k in ("value", "unit", "cpu_baseline", "unavailable") if k in r}
+        return line
+    v, det = time_reference(wl.molecules[0], wl, steps=args.steps, warmup=args.warmup, target_pairs=2e9)
     if v is None:
         return {"impl": "reference", **det}
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -1326,11 +1463,13 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4", "gridexv", "fit", "symmetry",
-                                                              "hydrate"])
+    ap.add_argument("--workload", default="cfg3", choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4", "gridexv", "fit", "symmetry",
+                                                              "hydrate", "atomics-peak"])
     ap.add_argument("--chains", type=int, default=64)
     ap.add_argument("--hbm-budget-gb", type=float, default=40.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true", help="cfg3: skip the serving sub-object")
+    ap.add_argument("--serve-requests", type=int, default=0, help="serving: requests per load point (default 5 x chains)")
     ap.add_argument("--subunit", type=int, default=0, help="cfg2: atoms per subunit (default 8333; smaller for profiling)")
     ap.add_argument("--atoms", type=int, default=0, help="cfg1: atoms of the globule (default 50000; smaller for profiling)")
     ap.add_argument("--precision", type=int, default=2, choices=[0, 1, 2],
@@ -1353,7 +1492,7 @@ def main():
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     line = {"cfg3": run_batch, "cfg4": run_serving, "gridexv": run_gridexv, "fit": run_fit,
-            "symmetry": run_symmetry, "hydrate": run_hydrate}.get(args.workload, run_ours)(
+            "symmetry": run_symmetry, "hydrate": run_hydrate, "atomics-peak": run_atomics_peak}.get(args.workload, run_ours)(
         args, rank, world, local_rank)
     if world > 1:
         import torch

@@ -229,6 +229,8 @@ AUSAXS_API int ausaxs_gpu_structure_histogram(ausaxs_gpu_ctx* ctx, ausaxs_gpu_st
  *   q, Iq, n_q or the parameters change).  The transform is FP64 for every q; params->precision is
  *   not used.  Any bin overflow in the batch makes every Iq NaN.
  * ausaxs_gpu_batch_profile: host q and Iq (synchronises; bin overflow is an error).
+ * ausaxs_gpu_batch_pair_time: device milliseconds of the pair stage (accumulator clearing and every
+ *   pair launch) of the last profile, from events recorded inside the captured graph (waits for it).
  * ausaxs_gpu_batch_histogram: structure `index`'s histograms from the last profile, as
  *   ausaxs_gpu_structure_histogram.
  */
@@ -246,6 +248,7 @@ AUSAXS_API int ausaxs_gpu_batch_profile_device(ausaxs_gpu_batch* b, const double
                                                const ausaxs_debye_params* params, double* Iq);
 AUSAXS_API int ausaxs_gpu_batch_profile(ausaxs_gpu_batch* b, const double* q, int32_t n_q,
                                         const ausaxs_debye_params* params, double* Iq);
+AUSAXS_API int ausaxs_gpu_batch_pair_time(ausaxs_gpu_batch* b, double* ms);
 AUSAXS_API int ausaxs_gpu_batch_histogram(ausaxs_gpu_batch* b, int32_t index, ausaxs_hist_result* out);
 
 /*
@@ -475,19 +478,24 @@ AUSAXS_API int ausaxs_gpu_linear_lsq(ausaxs_gpu_ctx* ctx, const double* data, co
  * section, or an embedding application that forbids cudaMalloc after start-up, since allocation can
  * synchronise the device).  It computes what ausaxs_gpu_histogram returns for AUSAXS_MANAGER_MT, but
  * from device inputs into device outputs, and calls no cudaMalloc, cudaFree or allocating library
- * routine: its temporaries live in one file-scope device array (about 640 KiB per device, held
- * until the process exits).
+ * routine: its temporaries live in one file-scope device array (591,104 bytes, about 577 KiB, per
+ * device, held until the process exits).
  *   atoms, waters   : device arrays of n x {float x, y, z, w} (weights in the 4th word)
  *   bin_count       : at most 8192 (AUSAXS_ERR_CAPACITY above that); every pair distance must fall
- *                     below bin_count * bin_width
+ *                     below bin_count * bin_width.  The pair kernel keeps bin_count bins on chip, so
+ *                     pass the smallest bin_count that covers the structure's largest distance: at
+ *                     8,000 bins one CTA fits per SM and the call runs slower than ausaxs_gpu_histogram,
+ *                     which trims its bins to the structure
  *   hist_out        : device, 5 * bin_count doubles: rows {aa, aw, ww, tot, d_axis}, each with stride
  *                     bin_count, zero beyond *max_bin_out
  *   max_bin_out     : device int32
  *   overflow_out    : device u64 (may be NULL): pairs that fell beyond bin_count
  *   stream          : cudaStream_t as void* (NULL = legacy default stream); the call only enqueues.
  * All calls share the one scratch array, which keeps the last call's contents (each call clears
- * what must start at zero); calls that overlap on the GPU race and give wrong results.  The first
- * call on a device looks up the array's address and caches it: make it before any stream capture.
+ * what must start at zero); calls that overlap on the GPU race and give wrong results: issue them on
+ * one stream, or order them with events.  The array's address belongs to the CUDA context: the first
+ * call in each context of a device (a context created again after cudaDeviceReset is a new one)
+ * looks it up and caches it, so make that first call before any stream capture.
  */
 AUSAXS_API int ausaxs_gpu_histogram_mt_noalloc(const float* atoms, int32_t n_atoms, const float* waters,
                                                int32_t n_waters, double bin_width, int32_t bin_count,
