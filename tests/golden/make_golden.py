@@ -22,6 +22,18 @@ reference's default q axis.  Cases:
 * ``partial_*``: PartialHistogramManagerMT over a multi-body molecule, initially and after rigid moves;
 * ``hydrate_*``: Molecule::generate_new_hydration() (RadialHydration) with seeded noise tables, on a
                 fresh grid and after rigid moves.
+
+Full-size fixtures (``python tests/golden/make_golden.py fullsize``; minutes of reference CPU time):
+
+* ``fullsize_cfg1``: the 50,000-atom globule with 10,000 waters and its 1 A grid dummies
+                (HistogramManagerMTFFGrid, 0.1 A bins) and ``fullsize_cfg2``: the 500,000-atom icosahedral
+                shell with 60,000 waters (HistogramManagerMTFFAvg, 0.1 A bins);
+* ``fullsize_cfg3``: 8 structures of the seeded 256-structure batch, spread over its size range
+                (HistogramManagerMTFFAvg, 0.25 A bins).
+Their inputs are not stored: ausaxs_b200.synth regenerates them from the seed, and a SHA-256 digest of
+the float64 inputs is stored to prove the regeneration identical.  Stored: the reference's raw
+counts by form-factor type, its distance axes, and I(q) at the workload's q grid from the oracle's
+generalised-q transform applied to the reference's histograms.
 """
 from __future__ import annotations
 
@@ -34,6 +46,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 from oracle import py as O  # noqa: E402
+from tests.helpers import input_digest  # noqa: E402
 
 REF_ROOT = os.environ.get("AUSAXS_REFERENCE", "/root/reference")  # reference checkout (read-only)
 
@@ -305,5 +318,66 @@ def main():
              simple_exv=True)
 
 
+def reference_hist(m, manager, bin_width, q):
+    """The reference's histograms of a molecule and the oracle's I(q) of them at q."""
+    import time
+
+    O.ref_set_axes(bin_width, 8000, 1e-4, 1.0)
+    O.ref_set_simple_exv(False)
+    rm = O.RefMolecule(m.atoms, m.weights, m.ff_types, m.waters, m.water_weights, volume=m.volume)
+    rm.set_manager(manager, exv_xyz=m.exv if manager == "ffgrid" else None)
+    t0 = time.perf_counter()
+    h = rm.calculate()
+    secs = time.perf_counter() - t0
+    aa, aw, ww = h.ff()
+    tot, d = h.total()
+    # raw doubles: pair counts, and for FFAvg the excluded-volume rows scaled by Z_exv
+    out = dict(aa=aa, aw=aw, ww_h=ww, tot=tot, d_axis=d)
+    kind = {"ffavg": 0, "ffgrid": 2}[manager]
+    ax = xx = None
+    if manager == "ffgrid":
+        ax, xx = h.grid_axes()
+        ax, xx = ax[: len(d)], xx[: len(d)]
+        out["d_axis_ax"], out["d_axis_xx"] = ax, xx
+    fh = O.FFHist(aa, aw, ww, tot, d, ax, xx)
+    out["q"] = np.asarray(q, np.float64)
+    out["Iq"], _ = O.debye_ff(kind, fh, out["q"])
+    return out, secs
+
+
+def fullsize():
+    from ausaxs_b200 import synth
+
+    O.ref()
+    which = sys.argv[2:] or ["cfg1", "cfg2", "cfg3"]
+    for name, wl in (("fullsize_cfg1", synth.cfg1() if "cfg1" in which else None),
+                     ("fullsize_cfg2", synth.cfg2() if "cfg2" in which else None)):
+        if wl is None:
+            continue
+        m = wl.molecules[0]
+        out, secs = reference_hist(m, wl.manager, wl.bin_width, wl.q)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), digest=input_digest(m), workload=wl.name,
+                            manager=wl.manager, bin_width=wl.bin_width, **out)
+        print(name, "bins", len(out["d_axis"]), f"{secs:.1f} s")
+    if "cfg3" not in which:
+        return
+    wl = synth.cfg3()
+    ranked = sorted(range(len(wl.molecules)), key=lambda i: -wl.molecules[i].size_atom())
+    picks = [ranked[int(round(k * (len(ranked) - 1) / 7))] for k in range(8)]
+    store = {"indices": np.array(picks, np.int64), "workload": wl.name, "manager": wl.manager,
+             "bin_width": wl.bin_width}
+    for k, i in enumerate(picks):
+        m = wl.molecules[i]
+        out, secs = reference_hist(m, wl.manager, wl.bin_width, wl.q)
+        store[f"digest{k}"] = input_digest(m)
+        for key, v in out.items():
+            store[f"{key}{k}"] = v
+        print("cfg3 structure", i, m.size_atom(), "atoms", f"{secs:.1f} s")
+    np.savez_compressed(os.path.join(HERE, "fullsize_cfg3.npz"), **store)
+
+
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "fullsize":
+        fullsize()
+    else:
+        main()

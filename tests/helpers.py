@@ -14,7 +14,7 @@ def golden_cases(prefix=""):
     """Histogram/intensity fixtures (grid excluded-volume, fit and calculator fixtures are listed by
     grid_cases, fit_cases and calc_cases; the multi-step partial-manager and hydration fixtures belong to their own tests)."""
     return sorted(n for n in (os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, prefix + "*.npz")))
-                  if not n.startswith(("gridexv_", "fit_", "calc_", "partial_", "hydrate_")))
+                  if not n.startswith(("gridexv_", "fit_", "calc_", "partial_", "hydrate_", "fullsize_")))
 
 
 def grid_cases():
@@ -68,3 +68,15 @@ def oracle_for(g):
     X = O.pack_points(g["exv"], np.zeros(len(g["exv"]), np.int32), True)
     z = float(g["volume"]) * RHO_W / len(atoms)
     return O.hist_ff(kind, A, W, X if kind == 2 else None, bw, 8000, z)
+
+
+def input_digest(m) -> str:
+    """SHA-256 over a molecule's float64 inputs (atoms, form-factor types, waters, dummies, volume): the
+    full-size fixtures store it so that regenerating their inputs from the seed is checked to be exact."""
+    import hashlib
+
+    h = hashlib.sha256()
+    for a in (m.atoms, m.ff_types.astype(np.int64), m.waters, m.exv if m.exv is not None else np.zeros((0, 3))):
+        h.update(np.ascontiguousarray(a).tobytes())
+    h.update(np.float64(m.volume).tobytes())
+    return h.hexdigest()

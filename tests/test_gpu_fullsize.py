@@ -1,56 +1,100 @@
-"""Full-size configurations, checked through properties that do not need the oracle (which cannot
-finish these sizes in seconds): pair-count conservation per histogram block, distance-axis
-consistency (every weighted bin mean lies inside its bin), and the tensor-core transform against
-the FP64 transform within the path's I(q) bar (1e-4 relative)."""
+"""The benchmark configurations at full size against the reference's own output.
+
+Fixtures (tests/golden/make_golden.py fullsize) hold what the reference, compiled from its sources,
+computes for the seeded inputs: raw pair counts by form-factor type and distance axes of
+HistogramManagerMTFFGrid (the 50,000-atom globule with 10,000 waters and 376,380 grid dummies,
+0.1 A bins), of HistogramManagerMTFFAvg (the 500,000-atom icosahedral shell with 60,000 waters,
+0.1 A bins) and of 8 structures of the seeded 256-structure batch (0.25 A bins), plus I(q) at each
+workload's q grid from the oracle's FP64 transform of the reference's histograms.  The inputs are
+regenerated from their seeds; a digest proves them identical to the fixtures'.
+
+Bars: pair counts bit-exact; distance axes within bin_width * 2^-15 (the fixed-point offset sums);
+I(q) of the path bench.py times (split-BF16 tensor-core transform where it pays, FP64 for every q
+whose error bound exceeds the tolerance) within 1e-4 relative, the FP64 transform within 1e-6."""
 import numpy as np
 import pytest
 
 from ausaxs_b200 import hist, synth
+from tests.helpers import input_digest, load_golden
 
 pytestmark = pytest.mark.gpu
 
-
-def _check_axis(d, width):
-    b = np.arange(len(d))
-    # bin b holds distances d with rint(d / width) = b: its mean is within half a bin of b * width
-    # (float rounding of d / width allows 1e-6 relative more); bin 0 is pinned to 0
-    assert d[0] == 0
-    assert np.all(np.abs(d[1:] - b[1:] * width) <= 0.5 * width * (1 + 1e-6) + 1e-6 * d[1:])
+IQ_RTOL = 1e-4     # the path's I(q) bar against the FP64 oracle
+IQ_RTOL_FP64 = 1e-6  # FP64 transform: the d-axis quantisation (<= 3e-6 A) times q <= 1
 
 
-def _tc_vs_fp64(h, q):
+def d_atol(bin_width):
+    return bin_width * 2.0 ** -15
+
+
+def _check_hist(h, g, bw, grid):
+    mb = len(g["d_axis"])
+    assert h.max_bin == mb
+    np.testing.assert_array_equal(h.get_raw_aa_counts_by_ff(), g["aa"])
+    np.testing.assert_array_equal(h.get_raw_aw_counts_by_ff(), g["aw"])
+    np.testing.assert_array_equal(h.get_raw_ww_counts_by_ff(), g["ww_h"])
+    np.testing.assert_allclose(h.get_d_axis(), g["d_axis"], atol=d_atol(bw), rtol=0)
+    if grid:
+        np.testing.assert_allclose(h.get_d_axis_ax(), g["d_axis_ax"], atol=d_atol(bw), rtol=0)
+        np.testing.assert_allclose(h.get_d_axis_xx(), g["d_axis_xx"], atol=d_atol(bw), rtol=0)
+
+
+def _check_iq(h, g):
+    q = g["q"]
     h.precision, h.tolerance = 1, 1e-5
     _, I64 = h.debye_transform(q)
-    h.precision, h.tolerance = 0, 1e-4
+    np.testing.assert_allclose(I64, g["Iq"], rtol=IQ_RTOL_FP64, atol=0)
+    h.precision, h.tolerance = 2, 1e-4  # bench.py's transform
+    _, I = h.debye_transform(q)
+    np.testing.assert_allclose(I, g["Iq"], rtol=IQ_RTOL, atol=0)
+    h.precision, h.tolerance = 0, 1e-4  # tensor cores for every q (FP64 for the flagged ones)
     _, Itc = h.debye_transform(q)
-    np.testing.assert_allclose(Itc, I64, rtol=1e-4, atol=0)
+    np.testing.assert_allclose(Itc, g["Iq"], rtol=IQ_RTOL, atol=0)
 
 
-def test_cfg1_grid_counts_and_transform(gpu_ctx):
+def test_cfg1_ffgrid_vs_reference(gpu_ctx):
+    g = load_golden("fullsize_cfg1")
     w = synth.cfg1()
     m = w.molecules[0]
-    na, nw, nx = m.size_atom(), m.size_water(), len(m.exv)
+    assert input_digest(m) == str(g["digest"]), "the seeded inputs changed"
     h = hist.HistogramManagerMTFFGrid(m, w.bin_width, w.bin_count, gpu_ctx).calculate_all()
-    aa, aw, ww = h.get_raw_aa_counts_by_ff(), h.get_raw_aw_counts_by_ff(), h.get_raw_ww_counts_by_ff()
-    assert aa[1:, 1:].sum() == na * na          # 2 x pairs + self terms
-    assert aa[1:, 0].sum() == na * nx           # atom-dummy cross (factor 1)
-    assert aa[0, 0].sum() == nx * nx            # dummy-dummy
-    assert aw[1:].sum() == na * nw and aw[0].sum() == nw * nx
-    assert ww.sum() == nw * nw
-    _check_axis(h.get_d_axis(), w.bin_width)
-    _tc_vs_fp64(h, w.q)
+    na, nw, nx = m.size_atom(), m.size_water(), len(m.exv)
+    aa = h.get_raw_aa_counts_by_ff()
+    assert aa[1:, 1:].sum() == na * na and aa[1:, 0].sum() == na * nx and aa[0, 0].sum() == nx * nx
+    _check_hist(h, g, w.bin_width, True)
+    assert len(g["q"]) == 1000
+    _check_iq(h, g)
 
 
-def test_cfg2_icosahedral_shell(gpu_ctx):
+def test_cfg2_ffavg_vs_reference(gpu_ctx):
+    g = load_golden("fullsize_cfg2")
     w = synth.cfg2()
     m = w.molecules[0]
-    na, nw = m.size_atom(), m.size_water()
+    assert input_digest(m) == str(g["digest"]), "the seeded inputs changed"
     h = hist.HistogramManagerMTFFAvg(m, True, w.bin_width, w.bin_count, gpu_ctx).calculate_all()
-    aa, aw, ww = h.get_raw_aa_counts_by_ff(), h.get_raw_aw_counts_by_ff(), h.get_raw_ww_counts_by_ff()
-    assert aa[1:, 1:].sum() == na * na
-    assert aw[1:].sum() == na * nw
-    assert ww.sum() == nw * nw
-    assert h.get_counts().sum() == na * na + na * nw + nw * nw
     assert h.max_bin > 2500  # the 150 A shell spans about 3,000 bins of 0.1 A
-    _check_axis(h.get_d_axis(), w.bin_width)
-    _tc_vs_fp64(h, w.q)
+    _check_hist(h, g, w.bin_width, False)
+    assert len(g["q"]) == 2000
+    _check_iq(h, g)
+
+
+def test_cfg3_batch_structures_vs_reference(gpu_ctx):
+    """The whole seeded 256-structure batch through the batched path (one graph replay); 8 of its
+    structures, spread over its size range, against the reference."""
+    g = load_golden("fullsize_cfg3")
+    w = synth.cfg3()
+    picks = [int(i) for i in g["indices"]]
+    B = hist.BatchedProfiles(w.molecules, bin_width=w.bin_width, bin_count=w.bin_count, ctx=gpu_ctx)
+    I = B.debye_transform(w.q)
+    for k, i in enumerate(picks):
+        m = w.molecules[i]
+        assert input_digest(m) == str(g[f"digest{k}"]), f"the seeded inputs of structure {i} changed"
+        hb = B.histogram(i)
+        mb = len(g[f"d_axis{k}"])
+        assert hb["max_bin"] == mb, (i, hb["max_bin"], mb)
+        np.testing.assert_array_equal(hb["aa"], g[f"aa{k}"])
+        np.testing.assert_array_equal(hb["aw"], g[f"aw{k}"])
+        np.testing.assert_array_equal(hb["ww"], g[f"ww_h{k}"])
+        np.testing.assert_allclose(hb["d_axis"], g[f"d_axis{k}"], atol=d_atol(w.bin_width), rtol=0)
+        np.testing.assert_allclose(I[i], g[f"Iq{k}"], rtol=IQ_RTOL_FP64, atol=0)
+    B.close()
