@@ -210,7 +210,7 @@ struct Batch {
                 La.smem = pairhist_launch_smem(rows[b][g], max_nb, false, La.tile);
                 if (La.smem > kPairSmemCap) throw Error{AUSAXS_ERR_CAPACITY, "too many distance bins for a batched launch"};
                 const int per_sm =
-                    pairhist_ctas_per_sm(La.smem, La.tile, pairhist_dreg(rows[b][g], max_nb, false, La.tile));
+                    pairhist_ctas_per_sm(La.smem, La.tile, pairhist_dreg(rows[b][g], max_nb, false, La.tile), false);
                 La.grid = (int)std::min<long long>((long long)ctx->sm_count * per_sm, std::max<long long>(1, tiles[b][g]));
                 PairLaunch& L = La.L;
                 L.jobs = jobs.as<PairJob>() + at;

@@ -265,7 +265,7 @@ struct Calculator {
             L.wscale = wscale;
             L.dreg = 0;
             const size_t smem = pairhist_launch_smem(1, nb, true, tile);
-            const int per_sm = pairhist_ctas_per_sm(smem, tile, false);
+            const int per_sm = pairhist_ctas_per_sm(smem, tile, false, true);
             const int grid = (int)std::min<long long>((long long)C.sm_count * per_sm, std::max<long long>(1, tiles[0]));
             L.chunk = (int)std::max<long long>(1, std::min<long long>(8, tiles[0] / ((long long)grid * 8)));
             cudaEvent_t ev;

@@ -315,7 +315,7 @@ int ausaxs_gpu_ctx_enable_timing(ausaxs_gpu_ctx* ctx, int32_t enable) {
 
 int ausaxs_gpu_ctx_kernel_time(ausaxs_gpu_ctx* ctx, int32_t kernel_class, double* ms, int64_t* launches) {
     return guarded([&] {
-        if (!ctx || kernel_class < 0 || kernel_class > 5) throw Error{AUSAXS_ERR_ARGUMENT, "bad argument"};
+        if (!ctx || kernel_class < 0 || kernel_class > 6) throw Error{AUSAXS_ERR_ARGUMENT, "bad argument"};
         Ctx& C = ctx->impl;
         C.time_collect();
         if (ms) *ms = C.timed[kernel_class].ms;

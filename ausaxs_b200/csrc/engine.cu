@@ -184,10 +184,11 @@ void zero_ranges_launch(const ZeroRange* ranges_dev, int n, cudaStream_t s) {
 }
 
 void append_pair_jobs(const Plan& P, int tile, bool by_class, std::vector<PairJob> (&jobs)[3], long long (&tiles)[3],
-                      int (&rows)[3], int max_rows) {
+                      int (&rows)[3], int max_rows, bool skip_lattice) {
     auto nt = [tile](int n) { return (n + tile - 1) / tile; };
     const int group_rows = max_rows > 0 ? max_rows : P.max_group_rows;
     for (const JobSpec& j : P.specs) {
+        if (skip_lattice && j.lattice) continue;
         const long long t = j.self ? tri(nt(j.na)) : (long long)nt(j.na) * nt(j.nbp);
         for (int r0 = 0; r0 < j.rows; r0 += group_rows) {
             const int r1 = std::min(j.rows, r0 + group_rows);
@@ -224,6 +225,52 @@ void append_pair_jobs(const Plan& P, int tile, bool by_class, std::vector<PairJo
             rows[g] = std::max(rows[g], r1 - r0);
         }
     }
+}
+
+bool Structure::lattice_ready() {
+    if (lat.tried) return lat.usable;
+    lat.tried = true;
+    lat.usable = false;
+    if (n_x < kLatticeMinPoints) return false;
+    Ctx& C = *ctx;
+    cudaStream_t s = C.stream;
+    lat.scratch.ensure(256);
+    int* st = lat.scratch.as<int>();
+    lattice_scan_launch(raw_x.as<float4>(), n_x, st, C.sm_count, s);
+    C.check_launch("lattice scan");
+    int h[8] = {};
+    AUSAXS_CUDA(cudaMemcpyAsync(h, st, 7 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    AUSAXS_CUDA(cudaStreamSynchronize(s));
+    if (h[6]) return false;  // not every coordinate is a (modest) integer
+    LatticeGrid G;
+    for (int k = 0; k < 3; ++k) G.lo[k] = h[k];
+    G.lx = h[3] - h[0] + 1;
+    G.ly = h[4] - h[1] + 1;
+    G.lz = h[5] - h[2] + 1;
+    G.words = (G.lx + 31) / 32;
+    if (G.words > kLatticeMaxWords || (long long)G.ly * G.lz > (1ll << 20)) return false;
+    lat.s2_max = (long long)(G.lx - 1) * (G.lx - 1) + (long long)(G.ly - 1) * (G.ly - 1) + (long long)(G.lz - 1) * (G.lz - 1);
+    if (lat.s2_max >= (1ll << 24)) return false;  // the reference's float evaluation is exact below 2^24
+    const size_t n_lines_all = (size_t)G.ly * G.lz;
+    DevBuf bits;
+    bits.ensure(n_lines_all * G.words * 4);
+    AUSAXS_CUDA(cudaMemsetAsync(bits.p, 0, n_lines_all * G.words * 4, s));
+    lat.lines.ensure(n_lines_all * G.words * 4);
+    lat.table.ensure(n_lines_all * 4);
+    int* info = st + 8;
+    AUSAXS_CUDA(cudaMemsetAsync(info, 0, 2 * sizeof(int), s));
+    lattice_build_launch(raw_x.as<float4>(), n_x, G.lo, G.lx, G.ly, G.lz, G.words, bits.as<uint32_t>(),
+                         lat.lines.as<uint32_t>(), lat.table.as<int32_t>(), info, C.sm_count, s);
+    C.check_launch("lattice build");
+    AUSAXS_CUDA(cudaMemcpyAsync(h, info, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    AUSAXS_CUDA(cudaStreamSynchronize(s));  // also keeps `bits` alive until the build is done
+    if (h[1]) return false;  // two dummies in one cell (or outside the scanned box)
+    G.n_lines = h[0];
+    G.lines = lat.lines.as<uint32_t>();
+    G.table = lat.table.as<int32_t>();
+    lat.G = G;
+    lat.usable = true;
+    return true;
 }
 
 Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
@@ -360,6 +407,19 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
     P.dev.ensure(off);
     char* base = P.dev.as<char>();
 
+    // the dummies' self pairs (slot 5) by the lattice kernel when the dummies sit on the integer
+    // lattice and the reference's two rounding rules agree on every squared offset (lattice.cu)
+    P.lattice_grid = 0;
+    bool use_lattice = false;
+    if (grid && n_x >= kLatticeMinPoints && lattice_ready() && lattice_rules_agree(lat.s2_max, inv_w)) {
+        const size_t lsm = lattice_smem_bytes(lat.G.n_lines, lattice_kernel_words(lat.G.words), lat.G.ly, lat.G.lz, nb);
+        if (lsm <= kPairSmemCap) {
+            use_lattice = true;
+            P.lattice_smem = lsm;
+            const int per_sm = std::max(1, std::min(2048 / kLatticeThreads, (int)(233472 / (lsm + 1024))));
+            P.lattice_grid = C.sm_count * per_sm;
+        }
+    }
     // passes of this structure with their accumulators
     P.specs.clear();
     P.pairs = 0;
@@ -380,9 +440,23 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
         // offset sums only feed the weighted d-axis; weight sums are the Simple histogram's values
         sp.dsum = weighted ? reinterpret_cast<unsigned long long*>(base + slot_ds[j.slot]) : nullptr;
         sp.wsum = mt ? reinterpret_cast<long long*>(base + slot_ws[j.slot]) : nullptr;
+        sp.lattice = use_lattice && j.slot == 5;
         P.specs.push_back(sp);
     }
     P.max_group_rows = max_group_rows;
+    if (use_lattice) {
+        LatticeLaunch& LL = P.lattice;
+        LL.G = lat.G;
+        LL.nbins = nb;
+        LL.inv_w = P.inv_w;
+        LL.c = P.c;
+        LL.scale = P.scale;
+        LL.counts = reinterpret_cast<unsigned long long*>(base + slot_cnt[5]);
+        LL.dsum = weighted ? reinterpret_cast<unsigned long long*>(base + slot_ds[5]) : nullptr;
+        LL.overflow = reinterpret_cast<unsigned long long*>(base + P.off_overflow);
+        LL.counter = reinterpret_cast<unsigned long long*>(base + P.off_counter) + 8;  // cleared with the accumulators
+        LL.n_items = lat.G.lz * (2 * lat.G.ly - 1);
+    }
 
     // Jobs split into launch groups by the rows they keep on chip: one-row jobs (ww, xx, wx and all
     // Simple jobs) run with a small footprint and high occupancy, multi-row jobs (aa, aw, ax) get the
@@ -393,7 +467,7 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
     std::vector<PairJob> group_jobs[3];
     long long group_tiles[3] = {0, 0, 0};
     int group_rows[3] = {1, 1, 1};
-    append_pair_jobs(P, tile, split, group_jobs, group_tiles, group_rows);
+    append_pair_jobs(P, tile, split, group_jobs, group_tiles, group_rows, 0, true);
     if (group_jobs[0].size() + group_jobs[1].size() + group_jobs[2].size() > 64)
         throw Error{AUSAXS_ERR_CAPACITY, "too many row groups"};
     const bool w_launch = mt;  // Simple histograms always carry weight sums (values)
@@ -405,7 +479,7 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
         Plan::Group& G = P.group[P.n_launch++];
         G.tile = tile;
         G.smem = pairhist_launch_smem(group_rows[g], nb, w_launch, tile);
-        const int per_sm = pairhist_ctas_per_sm(G.smem, tile, pairhist_dreg(group_rows[g], nb, w_launch, tile));
+        const int per_sm = pairhist_ctas_per_sm(G.smem, tile, pairhist_dreg(group_rows[g], nb, w_launch, tile), w_launch);
         G.grid = (int)std::min<long long>((long long)C.sm_count * per_sm, std::max<long long>(1, group_tiles[g]));
         PairLaunch& L = G.launch;
         L.jobs = reinterpret_cast<const PairJob*>(base + job_off);
@@ -528,6 +602,13 @@ void Structure::enqueue_histogram(const ausaxs_hist_config& cfg) {
         pairhist_launch(G.launch, G.tile, G.grid, G.smem, s);
         C.check_launch("pairhist");
         C.time_end(0, ev);
+    }
+    if (P.lattice_grid > 0) {
+        cudaEvent_t ev;
+        C.time_begin(6, &ev);
+        lattice_launch(P.lattice, P.lattice_grid, P.lattice_smem, s);
+        C.check_launch("lattice");
+        C.time_end(6, ev);
     }
     cudaEvent_t evf;
     C.time_begin(1, &evf);

@@ -9,6 +9,7 @@
 #include "../../include/ausaxs_b200.h"
 #include "debye.cuh"
 #include "finalize.cuh"
+#include "lattice.cuh"
 #include "pairhist.cuh"
 #include "prep.cuh"
 
@@ -60,6 +61,7 @@ struct JobSpec {
     // scalar-tail geometry (PairJob): -1 = a plain job (tail_end = nbp, tail_from_outer = self)
     int a_base = 0, b_base = 0, tail_end = -1, tail_from_outer = -1;
     int mult = 1;  // multiplicity of every pair (PairJob::mult)
+    bool lattice = false;  // the plan bins this pass with the lattice kernel (the structure's own launches)
 };
 
 // Launch plan of one structure under one histogram configuration: job table, accumulator and
@@ -94,6 +96,19 @@ struct Plan {
     // tensor-core scratch
     DevBuf tc;
     int tc_nq = 0;
+    // the dummies' self pairs by the lattice kernel (lattice.cuh): launch shape, or grid == 0
+    LatticeLaunch lattice{};
+    int lattice_grid = 0;
+    size_t lattice_smem = 0;
+};
+
+// Lattice form of a structure's excluded-volume dummies, built on the first plan that asks for it.
+struct StructureLattice {
+    bool tried = false;   // built (or found unusable) already
+    bool usable = false;  // integer coordinates, no shared cells, lines short enough
+    LatticeGrid G;
+    long long s2_max = 0;  // largest squared offset between two dummies
+    DevBuf lines, table, scratch;
 };
 
 struct Structure {
@@ -109,6 +124,9 @@ struct Structure {
     float dmax = 0;
     float dmax_extra = 0;  // distance range kept beyond the current bounding-box diagonal (moving bodies)
     Plan plan;
+    StructureLattice lat;
+    // the dummies on the integer lattice (synchronises once per structure); true when usable
+    bool lattice_ready();
 
     // copy in (host or device pointers), census, validation and dense-type conversion (one sync)
     void load(const float* atoms, int n_atoms, const float* waters, int n_waters, const float* exv, int n_exv,
@@ -144,13 +162,13 @@ struct Ctx {
     long long launches = 0;
     // optional per-kernel-class timing with CUDA events on the context's stream
     // (class 0: pair histograms, 1: finalisation, 2: FP64 Debye transform, 3: tensor-core Debye transform,
-    // 4: grid excluded volume, 5: hydration)
+    // 4: grid excluded volume, 5: hydration, 6: lattice pairs of grid dummies)
     bool timing = false;
     struct Timed {
         std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
         double ms = 0;
         long long count = 0;
-    } timed[6];
+    } timed[7];
     void time_begin(int cls, cudaEvent_t* ev);
     void time_end(int cls, cudaEvent_t ev);
     void time_collect();
@@ -173,8 +191,9 @@ struct Ctx {
 // classes: 0 (one on-chip row), 1 (up to T rows), 2 (more), or all to class 0 when !by_class.
 // Tile ids continue from tiles[g]; rows[g] grows to the largest row group of class g.  Row groups
 // hold at most max_rows rows (0: the plan's own limit).
+// skip_lattice: leave out the passes the plan bins with the lattice kernel.
 void append_pair_jobs(const Plan& P, int tile, bool by_class, std::vector<PairJob> (&jobs)[3], long long (&tiles)[3],
-                      int (&rows)[3], int max_rows = 0);
+                      int (&rows)[3], int max_rows = 0, bool skip_lattice = false);
 
 // Clears n device ranges of u64 words in one launch (table in device memory).
 struct ZeroRange {

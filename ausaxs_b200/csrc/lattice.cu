@@ -1,0 +1,276 @@
+// Pair-distance histogram of points on the integer lattice by the autocorrelation of their occupancy.
+//
+// The grid model's excluded-volume dummies sit on the integer lattice (RawGridExv places one at the
+// centre of every volume cell of the 1 A molecular grid, source/core/grid/exv/RawGridExv.cpp:10-59),
+// and the reference bins their self pairs one by one (the exv-exv loop of
+// HistogramManagerMTFFGrid.cpp:66-84).  For integer coordinates every pair's squared distance is an
+// integer s2 that the reference's float evaluation forms exactly (s2 < 2^24), so its bin and in-bin
+// offset depend on s2 alone: the histogram is the sum over offsets (dx, dy, dz) of the number of
+// point pairs with that offset, each offset binned once.
+//
+// Counting the pairs per offset: the occupancy is stored as bit lines along x (one u32 word per 32
+// cells).  For a line offset (dy, dz) a warp walks every pair of non-empty lines (y, z), (y + dy,
+// z + dz) and lane l accumulates, for every x-shift s = 32 g + l, popc(P & (Q >> s)) (pairs with
+// x2 - x1 = s) and popc(Q & (P >> s)) (x1 - x2 = s), with funnel shifts across words.  Every
+// unordered pair appears once: each line offset is visited with dz > 0, or dz = 0 and dy > 0, or
+// within a line (dy = dz = 0, s > 0 only).  Per line pair and lane this is words * (words + 1)
+// AND + POPC terms against (points per line)^2 pair evaluations of the pair kernel, and the lines,
+// the line table and a per-CTA histogram stay in shared memory.
+//
+// The counts and the fixed-point offset sums it produces are the integers the pair kernel adds for the
+// same points, so the finalisation and everything after it see identical accumulators.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+
+#include "lattice.cuh"
+
+namespace ausaxs_b200 {
+
+namespace {
+
+__global__ void lattice_scan_init(int* st) {
+    if (threadIdx.x == 0) {
+        st[0] = st[1] = st[2] = INT_MAX;
+        st[3] = st[4] = st[5] = INT_MIN;
+        st[6] = 0;
+    }
+}
+
+__global__ void lattice_scan_kernel(const float4* p, int n, int* st) {
+    int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+    int bad = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 v = p[i];
+        const float c[3] = {v.x, v.y, v.z};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            // integers of magnitude below 2^20 (NaN fails the comparison)
+            if (!(c[k] == rintf(c[k]) && fabsf(c[k]) < 1048576.0f)) {
+                bad = 1;
+                continue;
+            }
+            const int iv = static_cast<int>(c[k]);
+            lo[k] = min(lo[k], iv);
+            hi[k] = max(hi[k], iv);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[k] = min(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+            hi[k] = max(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+        }
+    }
+    bad = __any_sync(0xffffffffu, bad);
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            if (lo[k] != INT_MAX) atomicMin(&st[k], lo[k]);
+            if (hi[k] != INT_MIN) atomicMax(&st[3 + k], hi[k]);
+        }
+        if (bad) atomicOr(&st[6], 1);
+    }
+}
+
+struct BuildArgs {
+    const float4* p;
+    int n;
+    int lo[3];
+    int lx, ly, lz, words;
+    uint32_t* grid;
+    int* info;
+};
+
+__global__ void lattice_set_kernel(BuildArgs A) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
+        const float4 v = A.p[i];
+        const int x = static_cast<int>(v.x) - A.lo[0];
+        const int y = static_cast<int>(v.y) - A.lo[1];
+        const int z = static_cast<int>(v.z) - A.lo[2];
+        // every coordinate lies in [lo, hi] by the scan; checked once more before the write
+        if (x < 0 || x >= A.lx || y < 0 || y >= A.ly || z < 0 || z >= A.lz) {
+            atomicOr(&A.info[1], 2);
+            continue;
+        }
+        const size_t w = (static_cast<size_t>(z) * A.ly + y) * A.words + (x >> 5);
+        const uint32_t bit = 1u << (x & 31);
+        if (atomicOr(&A.grid[w], bit) & bit) atomicOr(&A.info[1], 1);  // two points share a cell
+    }
+}
+
+// one CTA of 1024 threads: non-empty lines in (z, y) order into the compact store, the table, the count
+__global__ void __launch_bounds__(1024) lattice_compact_kernel(const uint32_t* grid, int n_lines_all, int words,
+                                                               uint32_t* lines, int32_t* table, int* info) {
+    __shared__ int warp_sum[32];
+    __shared__ int s_base;
+    if (threadIdx.x == 0) s_base = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int base = 0; base < n_lines_all; base += 1024) {
+        const int l = base + threadIdx.x;
+        bool ne = false;
+        if (l < n_lines_all)
+            for (int w = 0; w < words; ++w) ne |= grid[static_cast<size_t>(l) * words + w] != 0u;
+        const unsigned m = __ballot_sync(0xffffffffu, ne);
+        if (lane == 0) warp_sum[warp] = __popc(m);
+        __syncthreads();
+        int before = 0;
+        for (int k = 0; k < warp; ++k) before += warp_sum[k];
+        const int pos = s_base + before + __popc(m & ((1u << lane) - 1u));
+        if (l < n_lines_all) {
+            table[l] = ne ? pos : -1;
+            if (ne)
+                for (int w = 0; w < words; ++w)
+                    lines[static_cast<size_t>(pos) * words + w] = grid[static_cast<size_t>(l) * words + w];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int tot = 0;
+            for (int k = 0; k < 32; ++k) tot += warp_sum[k];
+            s_base += tot;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) info[0] = s_base;
+}
+
+template <int W>
+__global__ void __launch_bounds__(kLatticeThreads, 1) lattice_kernel(LatticeLaunch L) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int ly = L.G.ly, lz = L.G.lz, nb = L.nbins;
+    uint32_t* s_lines = reinterpret_cast<uint32_t*>(smem);
+    size_t off = (static_cast<size_t>(L.G.n_lines) * W * 4 + 15) & ~static_cast<size_t>(15);
+    int32_t* s_table = reinterpret_cast<int32_t*>(smem + off);
+    off += (static_cast<size_t>(ly) * lz * 4 + 15) & ~static_cast<size_t>(15);
+    unsigned long long* h_cnt = reinterpret_cast<unsigned long long*>(smem + off);  // [nb + 1]: last = overflow
+    unsigned long long* h_ds = h_cnt + (nb + 1);                                     // [nb + 1]
+    // the grid's line store has exactly `words` words per line; W may round it up (3 -> 4)
+    const int gw = L.G.words;
+    for (int k = threadIdx.x; k < L.G.n_lines * W; k += kLatticeThreads) {
+        const int line = k / W, w = k - line * W;
+        s_lines[k] = w < gw ? L.G.lines[static_cast<size_t>(line) * gw + w] : 0u;
+    }
+    for (int k = threadIdx.x; k < ly * lz; k += kLatticeThreads) s_table[k] = L.G.table[k];
+    for (int k = threadIdx.x; k < 2 * (nb + 1); k += kLatticeThreads) h_cnt[k] = 0ull;
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31;
+    const int span = 2 * ly - 1;
+    const float bin_limit = pair_bin_limit(nb);
+    for (;;) {
+        int item = 0;
+        if (lane == 0) item = static_cast<int>(atomicAdd(L.counter, 1ull));
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= L.n_items) break;
+        const int dz = item / span;
+        const int dy = item - dz * span - (ly - 1);
+        if (dz == 0 && dy < 0) continue;  // the mirror image of an item with dy > 0
+        const bool same = dz == 0 && dy == 0;
+        uint32_t C[W];
+#pragma unroll
+        for (int g = 0; g < W; ++g) C[g] = 0u;
+        const int y_lo = max(0, -dy), y_hi = min(ly, ly - dy);
+        for (int z1 = 0; z1 + dz < lz; ++z1) {
+            const int32_t* t1 = s_table + z1 * ly;
+            const int32_t* t2 = s_table + (z1 + dz) * ly + dy;
+            for (int y1 = y_lo; y1 < y_hi; ++y1) {
+                const int i1 = t1[y1];
+                if (i1 < 0) continue;
+                const int i2 = t2[y1];
+                if (i2 < 0) continue;
+                uint32_t P[W], Q[W];
+#pragma unroll
+                for (int w = 0; w < W; ++w) {
+                    P[w] = s_lines[i1 * W + w];
+                    Q[w] = s_lines[i2 * W + w];
+                }
+#pragma unroll
+                for (int g = 0; g < W; ++g) {
+#pragma unroll
+                    for (int w = 0; w + g < W; ++w) {
+                        const uint32_t qn = (w + g + 1 < W) ? Q[w + g + 1] : 0u;
+                        C[g] += __popc(P[w] & __funnelshift_r(Q[w + g], qn, lane));
+                        if (!same) {
+                            const uint32_t pn = (w + g + 1 < W) ? P[w + g + 1] : 0u;
+                            const uint32_t v = __popc(Q[w] & __funnelshift_r(P[w + g], pn, lane));
+                            C[g] += (g == 0 && lane == 0) ? 0u : v;  // x-shift 0 is counted once
+                        }
+                    }
+                }
+            }
+        }
+        if (same && lane == 0) C[0] = 0u;  // x-shift 0 within a line: a point with itself
+#pragma unroll
+        for (int g = 0; g < W; ++g) {
+            if (!C[g]) continue;
+            const int s = 32 * g + lane;
+            const int s2 = s * s + dy * dy + dz * dz;  // < 2^24: exact as a float
+            // the reference's bin rule and the pair kernel's fixed-point in-bin offset (common.cuh)
+            const float d = __fsqrt_rn(static_cast<float>(s2));
+            const float xm = __fadd_rn(__fmul_rn(d, L.inv_w), kMagic);
+            if (!(xm < bin_limit)) {
+                atomicAdd(&h_cnt[nb], static_cast<unsigned long long>(C[g]));
+                continue;
+            }
+            const int bin = __float_as_int(xm) - kMagicBits;
+            atomicAdd(&h_cnt[bin], static_cast<unsigned long long>(C[g]));
+            if (L.dsum) {
+                const float r = __fmaf_rn(-__fsub_rn(xm, kMagic), L.c, d);
+                const float t = __fmaf_rn(r, L.scale, kMagic);
+                const unsigned long long res = static_cast<uint32_t>(__float_as_int(t) - kMagicBits + kResBias);
+                atomicAdd(&h_ds[bin], res * C[g]);
+            }
+        }
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < nb; b += kLatticeThreads) {
+        if (h_cnt[b]) atomicAdd(&L.counts[b], h_cnt[b]);
+        if (L.dsum && h_ds[b]) atomicAdd(&L.dsum[b], h_ds[b]);
+    }
+    if (threadIdx.x == 0 && h_cnt[nb]) atomicAdd(L.overflow, h_cnt[nb]);
+}
+
+template <int W>
+void launch_w(const LatticeLaunch& L, int grid, size_t smem, cudaStream_t s) {
+    cudaFuncSetAttribute(lattice_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    lattice_kernel<W><<<grid, kLatticeThreads, smem, s>>>(L);
+}
+
+}  // namespace
+
+void lattice_scan_launch(const float4* p, int n, int* stats, int sm_count, cudaStream_t s) {
+    lattice_scan_init<<<1, 32, 0, s>>>(stats);
+    const int grid = std::max(1, std::min(sm_count * 4, (n + 255) / 256));
+    lattice_scan_kernel<<<grid, 256, 0, s>>>(p, n, stats);
+}
+
+void lattice_build_launch(const float4* p, int n, const int lo[3], int lx, int ly, int lz, int words, uint32_t* grid,
+                          uint32_t* lines, int32_t* table, int* info, int sm_count, cudaStream_t s) {
+    BuildArgs A{p, n, {lo[0], lo[1], lo[2]}, lx, ly, lz, words, grid, info};
+    const int g = std::max(1, std::min(sm_count * 4, (n + 255) / 256));
+    lattice_set_kernel<<<g, 256, 0, s>>>(A);
+    lattice_compact_kernel<<<1, 1024, 0, s>>>(grid, ly * lz, words, lines, table, info);
+}
+
+bool lattice_rules_agree(long long s2_max, float inv_w) {
+    // x = fl(fl(sqrt(s2)) * inv_w) exactly as the device and the reference's evaluators form it (IEEE
+    // single precision, correctly rounded square root); the rules differ only when x is a half-integer
+    for (long long s2 = 1; s2 <= s2_max; ++s2) {
+        const float d = std::sqrt(static_cast<float>(s2));
+        const float x = d * inv_w;
+        if (x - std::floor(x) == 0.5f) return false;
+    }
+    return true;
+}
+
+void lattice_launch(const LatticeLaunch& L, int grid, size_t smem, cudaStream_t s) {
+    switch (lattice_kernel_words(L.G.words)) {
+        case 1: launch_w<1>(L, grid, smem, s); break;
+        case 2: launch_w<2>(L, grid, smem, s); break;
+        case 4: launch_w<4>(L, grid, smem, s); break;
+        default: launch_w<8>(L, grid, smem, s); break;
+    }
+}
+
+}  // namespace ausaxs_b200

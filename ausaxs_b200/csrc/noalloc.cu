@@ -235,7 +235,7 @@ extern "C" int ausaxs_gpu_histogram_mt_noalloc(const float* atoms, int32_t n_ato
         int sms = 0;
         if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess || sms <= 0)
             return fail(AUSAXS_ERR_CUDA, "cannot query the multiprocessor count");
-        const int per_sm = pairhist_ctas_per_sm(smem, kNoAllocTile, false);
+        const int per_sm = pairhist_ctas_per_sm(smem, kNoAllocTile, false, true);
         const int grid = (int)std::min<long long>((long long)sms * per_sm, std::max<long long>(1, tiles_total));
         L.chunk = (int)std::max<long long>(1, std::min<long long>(8, tiles_total / ((long long)grid * 8)));
         pairhist_launch(L, kNoAllocTile, grid, smem, s);

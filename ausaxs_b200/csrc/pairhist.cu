@@ -7,14 +7,18 @@
 // the end (include/core/container/ThreadLocalWrapper.h:45-105).
 //
 // Design (B200):
-//   * one persistent grid; CTAs take chunks of square tiles (kTile outer x kTile inner points)
-//     from a global counter, over all jobs of the launch (aa, aw, ww, and ax, wx, xx for the grid
-//     model, or every job of a batch of structures);
-//   * each thread owns one outer point in registers; the inner tile is staged in shared memory
-//     and read as a broadcast float4 per pair;
+//   * one persistent grid; CTAs take chunks of square tiles (TILE outer x TILE inner points) from a
+//     global counter, over all jobs of the launch (aa, aw, ww, and ax, wx, xx for the grid model,
+//     or every job of a batch of structures);
+//   * each thread owns kOuter outer points in registers (lanes of a warp spread over the tile, so
+//     that neighbouring points of a chain -- similar distances, same bins -- sit in different warps);
+//     the inner tile is staged in shared memory by a 1D bulk copy (cp.async.bulk, mbarrier
+//     completion; double-buffered when the layout allows, so the next tile's copy overlaps this
+//     tile's pairs) and read as a broadcast float4 per inner point;
 //   * every CTA keeps privatised histograms in shared memory: u32 counts per (row, bin), one u64
 //     fixed-point sum of in-bin distance offsets per bin (the weighted bin centre), and for
-//     weighted jobs one i64 fixed-point sum of weight products per bin;
+//     weighted jobs one i64 fixed-point sum of weight products per bin; pairs beyond the last bin
+//     land in one extra column per row and are counted as overflow when the CTA flushes;
 //   * a CTA flushes its histograms to the global u64 accumulators when it moves to another job
 //     (or before a 32-bit count could wrap), so the global traffic is one atomic per non-empty
 //     on-chip bin per flush instead of one per pair.
@@ -54,13 +58,63 @@ __device__ __forceinline__ void tile_coords(const PairJob& J, long long t, int& 
     tj = static_cast<int>(r + (t - start(r)));
 }
 
+// ---------------------------------------------------------------------------------------------
+// Bulk-copy staging (cp.async.bulk global -> shared with mbarrier transaction counts).  Every wait
+// is bounded: after kWaitLimit polls the CTA records kWaitTimedOut in the launch's overflow word
+// (the host then reports an error), waits (bounded) for its other copy in flight and stops.
+// ---------------------------------------------------------------------------------------------
+constexpr unsigned kWaitLimit = 1u << 24;
+constexpr unsigned long long kWaitTimedOut = 1ull << 62;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_inval(unsigned long long* bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// thread 0: expect `bytes` on bar, then copy them (16-byte aligned, multiple of 16) into dst
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// orders this thread's generic-proxy accesses to shared memory before a later bulk copy into it
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// waits for phase `parity` of bar; false when the bound ran out
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+    const uint32_t a = smem_addr(bar);
+    for (unsigned it = 0; it < kWaitLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
 // On-chip privatised histograms of one CTA.
-//   counts   : u32 per (row, bin), one atomic per pair.
+//   counts   : u32 per (row, bin), one atomic per pair; column nbins of each row collects the pairs
+//              beyond the last bin (overflow), counted at the flush.
 //   offsets  : the in-bin distance offset of a pair is quantised to 16 bits (kResBits) and added
-//              with a 32-bit atomic to dacc; every drain_segment<TILE>() inner points (at most 2^16 pairs per
-//              bin, so dacc cannot wrap) the threads drain dacc into the u64 sums d64 without
-//              atomics.  (A 64-bit shared-memory atomic costs about three times as much per pair on
-//              sm_100a; this keeps one cheap 32-bit atomic per pair and an exact integer sum.)
+//              with a 32-bit atomic to dacc; every drain_segment<TILE>() inner points (at most 2^16
+//              pairs per bin, so dacc cannot wrap) the threads drain dacc into the u64 sums d64
+//              without atomics.  (A 64-bit shared-memory atomic costs about three times as much per
+//              pair on sm_100a; this keeps one cheap 32-bit atomic per pair and an exact integer sum.)
 //   weights  : weighted (Simple) jobs add rint(w_i w_j wscale) + 2^30 to wlo with exact carry
 //              propagation into whi (the old value returned by the atomic detects the wrap).
 struct Onchip {
@@ -77,21 +131,21 @@ __device__ __forceinline__ void add_carry(uint32_t* lo, uint32_t* hi, int b, uin
     if (old + v < old) atomicAdd(&hi[b], 1u);
 }
 
-// u64 offset sums held in registers (launches with DREG): thread t owns bins t + k * TILE
-template <int TILE, bool DREG>
+// u64 offset sums held in registers (launches with DREG): thread t owns bins t + k * NT
+template <int NT, bool DREG>
 struct OffsetRegs {
-    static constexpr int kSlots = DREG ? kDregBins / TILE : 1;
+    static constexpr int kSlots = DREG ? kDregBins / NT : 1;
     unsigned long long v[kSlots];
 };
 
 // dacc -> d64 (shared memory, or the thread's registers) for the bins of a job; callers synchronise
 // before (atomics done) and after.
-template <int TILE, bool DREG>
-__device__ __forceinline__ void drain_offsets(const Onchip& S, int nb, OffsetRegs<TILE, DREG>& R) {
+template <int NT, bool DREG>
+__device__ __forceinline__ void drain_offsets(const Onchip& S, int nb, OffsetRegs<NT, DREG>& R) {
     if (DREG) {
 #pragma unroll
-        for (int k = 0; k < OffsetRegs<TILE, DREG>::kSlots; ++k) {
-            const int b = threadIdx.x + k * TILE;
+        for (int k = 0; k < OffsetRegs<NT, DREG>::kSlots; ++k) {
+            const int b = threadIdx.x + k * NT;
             if (b < nb) {
                 const uint32_t v = S.dacc[b];
                 if (v) {
@@ -102,7 +156,7 @@ __device__ __forceinline__ void drain_offsets(const Onchip& S, int nb, OffsetReg
         }
         return;
     }
-    for (int b = threadIdx.x; b < nb; b += TILE) {
+    for (int b = threadIdx.x; b < nb; b += NT) {
         uint32_t v = S.dacc[b];
         if (v) {
             S.d64[b] += v;
@@ -111,13 +165,14 @@ __device__ __forceinline__ void drain_offsets(const Onchip& S, int nb, OffsetReg
     }
 }
 
-template <int TILE, bool WEIGHTED, bool DREG>
-__device__ __forceinline__ void flush_hist(const PairJob& J, const Onchip& S, OffsetRegs<TILE, DREG>& R) {
+template <int NT, bool WEIGHTED, bool DREG>
+__device__ __forceinline__ void flush_hist(const PairJob& J, const Onchip& S, OffsetRegs<NT, DREG>& R,
+                                           unsigned long long* overflow) {
     __syncthreads();
     const int rows = J.row_hi - J.row_lo;
     const int nb = J.nbins;
     const int n = rows * nb;
-    for (int idx = threadIdx.x; idx < n; idx += TILE) {
+    for (int idx = threadIdx.x; idx < n; idx += NT) {
         int r = idx / nb, b = idx - r * nb;
         uint32_t v = S.cnt[r * S.pad + b];
         if (v) {
@@ -125,15 +180,23 @@ __device__ __forceinline__ void flush_hist(const PairJob& J, const Onchip& S, Of
             S.cnt[r * S.pad + b] = 0;
         }
     }
+    // overflow column (bin nbins) of every row
+    for (int r = threadIdx.x; r < rows; r += NT) {
+        const uint32_t v = S.cnt[r * S.pad + nb];
+        if (v) {
+            atomicAdd(overflow, static_cast<unsigned long long>(v));
+            S.cnt[r * S.pad + nb] = 0;
+        }
+    }
     if (DREG && J.dsum) {
 #pragma unroll
-        for (int k = 0; k < OffsetRegs<TILE, DREG>::kSlots; ++k) {
-            const int b = threadIdx.x + k * TILE;
+        for (int k = 0; k < OffsetRegs<NT, DREG>::kSlots; ++k) {
+            const int b = threadIdx.x + k * NT;
             if (b < nb && R.v[k]) atomicAdd(&J.dsum[b], R.v[k] * J.mult);
             R.v[k] = 0;
         }
     }
-    for (int b = threadIdx.x; b < nb; b += TILE) {
+    for (int b = threadIdx.x; b < nb; b += NT) {
         if (!DREG && J.dsum) {
             unsigned long long v = S.d64[b];
             if (v) {
@@ -152,68 +215,116 @@ __device__ __forceinline__ void flush_hist(const PairJob& J, const Onchip& S, Of
     __syncthreads();
 }
 
-// Pairs of one outer point against inner points [k0, k1) of the staged tile.  GENERAL handles the
-// diagonal tiles of self jobs (j > i only) and the tiles that contain scalar-tail partners.  ROWS
-// selects the count row: kRowsSingle, one row whose index is the bin; kRowsOffset, every row of the
-// job is on chip and the staged inner points carry their row offset (inner type * pitch for pair
-// rows, 0 for outer rows) in w; kRowsGeneric, a row group of a job whose rows do not all fit.
+// Pairs of the thread's outer points against inner points [k0, k1) of the staged tile.  GENERAL
+// handles the diagonal tiles of self jobs (j > i only), the tiles that contain scalar-tail
+// partners and the last row of tiles (outer points beyond the set).  ROWS selects the count row:
+// kRowsSingle, one row whose index is the bin; kRowsOffset, every row of the job is on chip and
+// the staged inner points carry their row offset (inner type * pitch for pair rows, 0 for outer
+// rows) in w; kRowsGeneric, a row group of a job whose rows do not all fit.
 enum { kRowsSingle = 0, kRowsOffset = 1, kRowsGeneric = 2 };
 
-template <bool GENERAL, bool WEIGHTED, int ROWS>
-__device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, const float4* s_pts, const float4 a, int i,
-                                           int j0, int k0, int k1, bool diag, float wsc, unsigned long long& overflow) {
+struct Outer {
+    float4 a;
+    int i;        // index in the job's outer set
+    int cbase;    // count index of bin 0 in its row (kRowsSingle / kRowsOffset), or its row base (generic)
+    int ts;       // first inner index (local) that goes through the scalar evaluator
+    bool active;
+};
+
+// The count and offset arrays are indexed with the bit pattern of the magic-rounded distance
+// (kMagic + bin), their base pointers shifted by -kMagicBits.
+template <bool GENERAL, bool WEIGHTED, int ROWS, int R>
+__device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, const float4* s_pts, const Outer (&o)[R],
+                                           int j0, int k0, int k1, bool diag, float wsc) {
     const float inv_w = J.inv_w, c = J.c, scale = J.scale;
-    const unsigned nbins = static_cast<unsigned>(J.nbins);
-    const float bin_limit = pair_bin_limit(J.nbins);
-    const int rmode = J.row_mode, rlo = J.row_lo, rhi = J.row_hi;
-    // first inner index (local) whose pair goes through the scalar evaluator: in the reference's
-    // j-loops (SimpleCalculator.h:117-141, HistogramManagerMTFFAvg.cpp:216-232) the last
-    // (row length mod 4) partners of each outer point do
-    const int row_begin = J.tail_from_outer ? J.a_base + i + 1 : 0;
-    const int ts = J.tail_end - ((J.tail_end - row_begin) & 3) - J.b_base;
-    const int ta = __float_as_int(a.w);
-    const bool pair_rows = rmode == kRowPair;
-    const int rowbase = pair_rows ? ta * J.types : (rmode == kRowOuter ? ta : 0);
-    const int cnt_base = (rowbase - rlo) * S.pad;  // kRowsOffset: + inner offset + bin
+    const float bin_limit = pair_bin_limit(J.nbins);  // kMagic + nbins: the overflow column
+    const int rlo = J.row_lo, rhi = J.row_hi;
+    const bool pair_rows = J.row_mode == kRowPair;
     const bool do_d = J.dsum != nullptr;
     const bool do_w = WEIGHTED && J.wsum != nullptr;
-#pragma unroll 4
+    uint32_t* const cnt = S.cnt - kMagicBits;
+    uint32_t* const dacc = S.dacc - kMagicBits;
+#pragma unroll 2
     for (int jj = k0; jj < k1; ++jj) {
         const float4 b = s_pts[jj];
-        PairBin p;
-        if (GENERAL) {
-            const int j = j0 + jj;
-            if (diag && j <= i) continue;
-            p = pair_eval(a, b, inv_w, j >= ts);
-            if (static_cast<unsigned>(p.bin) >= nbins) {
-                ++overflow;
-                continue;
+        const int j = j0 + jj;
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            if (GENERAL && (!o[k].active || (diag && j <= o[k].i))) continue;
+            const float dx = __fsub_rn(o[k].a.x, b.x);
+            const float dy = __fsub_rn(o[k].a.y, b.y);
+            const float dz = __fsub_rn(o[k].a.z, b.z);
+            float s = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+            bool tail = false;
+            if (GENERAL) {
+                tail = j >= o[k].ts;
+                if (tail) s = __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
             }
-        } else if (!pair_eval_simd(a, b, inv_w, bin_limit, p)) {
-            ++overflow;
-            continue;
+            const float d = __fsqrt_rn(s);
+            const float x = __fmul_rn(d, inv_w);
+            // rint(x) by the magic number, ties to even; distances past the last bin (also NaN, inf
+            // and x >= 2^22) are clamped to the overflow column
+            float xm = fminf(__fadd_rn(x, kMagic), bin_limit);
+            if (GENERAL && tail && __fsub_rn(x, __fsub_rn(xm, kMagic)) == 0.5f)
+                xm = fminf(__fadd_rn(xm, 1.0f), bin_limit);  // std::round: ties away from zero
+            const int xb = __float_as_int(xm);
+            if (ROWS == kRowsSingle) {
+                atomicAdd(&cnt[xb], 1u);
+            } else if (ROWS == kRowsOffset) {
+                atomicAdd(&cnt[o[k].cbase + __float_as_int(b.w) + xb], 1u);
+            } else {
+                // a row group: count the rows it keeps; the group with row 0 also carries the offset sums
+                const int row = pair_rows ? o[k].cbase + __float_as_int(b.w) : o[k].cbase;
+                if (row >= rlo && row < rhi) atomicAdd(&cnt[(row - rlo) * S.pad + xb], 1u);
+            }
+            if (do_d) {
+                const float r = __fmaf_rn(-__fsub_rn(xm, kMagic), c, d);
+                const float t = __fmaf_rn(r, scale, kMagic);  // rint(r * scale), one rounding
+                atomicAdd(&dacc[xb], static_cast<uint32_t>(__float_as_int(t) - kMagicBits + kResBias));
+            }
+            if (do_w) {
+                const float wp = __fmul_rn(o[k].a.w, b.w);
+                const int wq = __float2int_rn(__fmul_rn(wp, wsc));  // |wq| <= 2^30
+                add_carry(S.wlo, S.whi, xb - kMagicBits, static_cast<uint32_t>(wq + (1 << 30)));
+            }
         }
-        if (ROWS == kRowsSingle) {
-            atomicAdd(&S.cnt[p.bin], 1u);
-        } else if (ROWS == kRowsOffset) {
-            atomicAdd(&S.cnt[cnt_base + __float_as_int(b.w) + p.bin], 1u);
+    }
+}
+
+template <int NT, int R, bool WEIGHTED, bool DREG>
+__device__ __forceinline__ void run_segments(const PairJob& J, const Onchip& S, const float4* s_pts, const Outer (&o)[R],
+                                             int j0, int jn, bool general, bool diag, float wsc,
+                                             OffsetRegs<NT, DREG>& Rg) {
+    constexpr int TILE = NT * R;
+    const bool single = J.row_mode == kRowSingle && J.row_lo == 0 && J.row_hi >= 1;
+    const int full_rows = J.row_mode == kRowPair ? J.types * J.types : (J.row_mode == kRowOuter ? J.types : 1);
+    const bool offset_rows = !single && J.row_lo == 0 && J.row_hi >= full_rows;
+    for (int k0 = 0; k0 < jn; k0 += drain_segment<TILE>()) {
+        const int k1 = min(jn, k0 + drain_segment<TILE>());
+        if (general) {
+            if (single) tile_pairs<true, WEIGHTED, kRowsSingle, R>(J, S, s_pts, o, j0, k0, k1, diag, wsc);
+            else if (offset_rows) tile_pairs<true, WEIGHTED, kRowsOffset, R>(J, S, s_pts, o, j0, k0, k1, diag, wsc);
+            else tile_pairs<true, WEIGHTED, kRowsGeneric, R>(J, S, s_pts, o, j0, k0, k1, diag, wsc);
         } else {
-            const int row = pair_rows ? rowbase + __float_as_int(b.w) : rowbase;
-            if (row >= rlo && row < rhi) atomicAdd(&S.cnt[(row - rlo) * S.pad + p.bin], 1u);
+            if (single) tile_pairs<false, WEIGHTED, kRowsSingle, R>(J, S, s_pts, o, j0, k0, k1, false, wsc);
+            else if (offset_rows) tile_pairs<false, WEIGHTED, kRowsOffset, R>(J, S, s_pts, o, j0, k0, k1, false, wsc);
+            else tile_pairs<false, WEIGHTED, kRowsGeneric, R>(J, S, s_pts, o, j0, k0, k1, false, wsc);
         }
-        if (do_d) atomicAdd(&S.dacc[p.bin], pair_residual(p, c, scale));
-        if (do_w) {
-            const float wp = __fmul_rn(a.w, b.w);
-            const int wq = __float2int_rn(__fmul_rn(wp, wsc));  // |wq| <= 2^30
-            add_carry(S.wlo, S.whi, p.bin, static_cast<uint32_t>(wq + (1 << 30)));
+        if (J.dsum) {
+            __syncthreads();
+            drain_offsets<NT, DREG>(S, J.nbins, Rg);
+            __syncthreads();
         }
     }
 }
 
 // DREG: the u64 offset sums live in registers (one CTA per SM; pairhist_dreg decides)
-template <int TILE, bool WEIGHTED, bool DREG>
-__global__ void __launch_bounds__(TILE, DREG ? 1 : 1024 / TILE) pairhist_kernel(PairLaunch L) {
+template <int NT, int R, bool WEIGHTED, bool DREG>
+__global__ void __launch_bounds__(NT, DREG ? 1 : (512 / NT > 1 ? 512 / NT : 1)) pairhist_kernel(PairLaunch L) {
+    constexpr int TILE = NT * R;
     extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ unsigned long long s_bar[2];
+    __shared__ long long s_grab;
     Onchip S;
     S.pad = L.smem_bins + 1;
     const size_t w32 = (static_cast<size_t>(S.pad) * 4 + 15) & ~static_cast<size_t>(15);
@@ -229,114 +340,190 @@ __global__ void __launch_bounds__(TILE, DREG ? 1 : 1024 / TILE) pairhist_kernel(
     if (WEIGHTED) off += w32;
     S.whi = reinterpret_cast<uint32_t*>(smem + off);
     if (WEIGHTED) off += w32;
-    float4* s_pts = reinterpret_cast<float4*>(smem + off);  // 16-byte aligned: every offset above is
-    __shared__ long long s_grab;
+    // staging buffer b at stage0 + b * stage_pitch (one buffer: both indices name it)
+    float4* const stage0 = reinterpret_cast<float4*>(smem + off);  // 16-byte aligned: every offset above is
+    const int stage_pitch = L.stages > 1 ? TILE : 0;
 
     // zero the on-chip histograms once; drains and flushes keep them zero afterwards
     {
         uint32_t* z = reinterpret_cast<uint32_t*>(smem);
-        size_t words = off / 4;
-        for (size_t k = threadIdx.x; k < words; k += TILE) z[k] = 0;
+        const size_t words = off / 4;
+        for (size_t k = threadIdx.x; k < words; k += NT) z[k] = 0;
+    }
+    if (threadIdx.x == 0) {
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
 
-    OffsetRegs<TILE, DREG> R;
+    OffsetRegs<NT, DREG> Rg;
 #pragma unroll
-    for (int k = 0; k < OffsetRegs<TILE, DREG>::kSlots; ++k) R.v[k] = 0;
+    for (int k = 0; k < OffsetRegs<NT, DREG>::kSlots; ++k) Rg.v[k] = 0;
     const float wsc = WEIGHTED ? *L.wscale : 0.f;
+    // lanes of a warp take outer points NT/32 apart; the warps interleave
+    const int spread = (threadIdx.x & 31) * (NT / 32) + (threadIdx.x >> 5);
     int cur = -1;
     long long pairs_since_flush = 0;
-    unsigned long long overflow = 0;
+    unsigned phases = 0u;  // bit b: the parity of staging barrier b's next phase
+    bool failed = false;
 
-    for (;;) {
+    // tile ids come in chunks from the global counter; the next tile id is known one tile ahead so
+    // that its copy can be issued before the current tile is processed
+    auto grab = [&]() -> long long {
         if (threadIdx.x == 0) s_grab = static_cast<long long>(atomicAdd(L.tile_counter, static_cast<unsigned long long>(L.chunk)));
         __syncthreads();
-        const long long g0 = s_grab;
-        if (g0 >= L.total_tiles) break;
-        const long long g1 = min(g0 + static_cast<long long>(L.chunk), static_cast<long long>(L.total_tiles));
-        for (long long g = g0; g < g1; ++g) {
-            const int jb = find_job(L.jobs, L.n_jobs, g);
-            // u32 counts stay exact below 2^32 pairs per bin between flushes
-            if (jb != cur || pairs_since_flush > (1ll << 31)) {
-                if (cur >= 0) flush_hist<TILE, WEIGHTED, DREG>(L.jobs[cur], S, R);
-                cur = jb;
-                pairs_since_flush = 0;
-            }
-            const PairJob& J = L.jobs[jb];
-            int ti, tj;
-            tile_coords(J, g - J.tile_begin, ti, tj);
-            const int j0 = tj * TILE;
-            const int jn = min(TILE, J.nb - j0);
-            const bool single = J.row_mode == kRowSingle && J.row_lo == 0 && J.row_hi >= 1;
-            const int full_rows = J.row_mode == kRowPair ? J.types * J.types : (J.row_mode == kRowOuter ? J.types : 1);
-            const bool offset_rows = !single && J.row_lo == 0 && J.row_hi >= full_rows;
-            __syncthreads();  // previous tile done with s_pts
-            if (threadIdx.x < jn) {
-                float4 v = J.B[j0 + threadIdx.x];
-                // row offset of the inner point for jobs with every row on chip
-                if (offset_rows) v.w = __int_as_float(J.row_mode == kRowPair ? __float_as_int(v.w) * S.pad : 0);
-                s_pts[threadIdx.x] = v;
-            }
-            const int i = ti * TILE + threadIdx.x;
-            const bool active = i < J.na;
-            const float4 a = active ? J.A[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-            __syncthreads();
-            pairs_since_flush += static_cast<long long>(TILE) * TILE;
-            const bool diag = J.self && ti == tj;
-            const bool has_tail = J.b_base + j0 + jn > J.tail_end - 3;  // scalar-tail partners: last 3 of a row
-            const bool general = diag || has_tail;
-            for (int k0 = 0; k0 < jn; k0 += drain_segment<TILE>()) {
-                const int k1 = min(jn, k0 + drain_segment<TILE>());
-                if (active) {
-                    if (general) {
-                        if (single) tile_pairs<true, WEIGHTED, kRowsSingle>(J, S, s_pts, a, i, j0, k0, k1, diag, wsc, overflow);
-                        else if (offset_rows) tile_pairs<true, WEIGHTED, kRowsOffset>(J, S, s_pts, a, i, j0, k0, k1, diag, wsc, overflow);
-                        else tile_pairs<true, WEIGHTED, kRowsGeneric>(J, S, s_pts, a, i, j0, k0, k1, diag, wsc, overflow);
-                    } else {
-                        if (single) tile_pairs<false, WEIGHTED, kRowsSingle>(J, S, s_pts, a, i, j0, k0, k1, false, wsc, overflow);
-                        else if (offset_rows) tile_pairs<false, WEIGHTED, kRowsOffset>(J, S, s_pts, a, i, j0, k0, k1, false, wsc, overflow);
-                        else tile_pairs<false, WEIGHTED, kRowsGeneric>(J, S, s_pts, a, i, j0, k0, k1, false, wsc, overflow);
-                    }
-                }
-                if (J.dsum) {
-                    __syncthreads();
-                    drain_offsets<TILE, DREG>(S, J.nbins, R);
-                    __syncthreads();
-                }
-            }
+        const long long v = s_grab;
+        __syncthreads();
+        return v;
+    };
+    // inner points of tile g into staging buffer buf (thread 0 issues the copy)
+    auto issue = [&](long long g, int buf) {
+        if (threadIdx.x != 0) return;
+        const int jb = find_job(L.jobs, L.n_jobs, g);
+        const PairJob& J = L.jobs[jb];
+        int ti, tj;
+        tile_coords(J, g - J.tile_begin, ti, tj);
+        const int j0 = tj * TILE;
+        const int jn = min(TILE, J.nb - j0);
+        bulk_load(stage0 + buf * stage_pitch, J.B + j0, static_cast<unsigned>(jn) * 16u, &s_bar[buf]);
+    };
+
+    long long g = grab();
+    long long g_end = min(g + static_cast<long long>(L.chunk), static_cast<long long>(L.total_tiles));
+    int buf = 0;
+    if (g < L.total_tiles) issue(g, buf);
+    while (g < L.total_tiles) {
+        // the next tile: the rest of this chunk, else a new chunk
+        long long gn = g + 1;
+        if (gn >= g_end) {
+            gn = grab();
+            g_end = min(gn + static_cast<long long>(L.chunk), static_cast<long long>(L.total_tiles));
         }
+        const bool prefetch = L.stages > 1 && gn < L.total_tiles;
+        if (prefetch) issue(gn, buf ^ 1);  // buffer buf ^ 1 was released by the previous tile's final barrier
+
+        const int jb = find_job(L.jobs, L.n_jobs, g);
+        // u32 counts stay exact below 2^32 pairs per bin between flushes
+        if (jb != cur || pairs_since_flush > (1ll << 31)) {
+            if (cur >= 0) flush_hist<NT, WEIGHTED, DREG>(L.jobs[cur], S, Rg, L.overflow);
+            cur = jb;
+            pairs_since_flush = 0;
+        }
+        const PairJob& J = L.jobs[jb];
+        int ti, tj;
+        tile_coords(J, g - J.tile_begin, ti, tj);
+        const int j0 = tj * TILE;
+        const int jn = min(TILE, J.nb - j0);
+        const bool single = J.row_mode == kRowSingle && J.row_lo == 0 && J.row_hi >= 1;
+        const int full_rows = J.row_mode == kRowPair ? J.types * J.types : (J.row_mode == kRowOuter ? J.types : 1);
+        const bool offset_rows = !single && J.row_lo == 0 && J.row_hi >= full_rows;
+
+        // outer points and their row bases (overlaps the copy in flight)
+        Outer o[R];
+        const int row_begin_base = J.tail_from_outer ? J.a_base + 1 : 0;
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            o[k].i = ti * TILE + spread + k * NT;
+            o[k].active = o[k].i < J.na;
+            o[k].a = o[k].active ? J.A[o[k].i] : make_float4(0.f, 0.f, 0.f, 0.f);
+            const int ta = __float_as_int(o[k].a.w);
+            const int rowbase = J.row_mode == kRowPair ? ta * J.types : (J.row_mode == kRowOuter ? ta : 0);
+            o[k].cbase = single ? 0 : (offset_rows ? (rowbase - J.row_lo) * S.pad : rowbase);
+            const int row_begin = J.tail_from_outer ? row_begin_base + o[k].i : 0;
+            o[k].ts = J.tail_end - ((J.tail_end - row_begin) & 3) - J.b_base;
+        }
+
+        const bool timed_out = !mbar_wait(&s_bar[buf], (phases >> buf) & 1u);
+        phases ^= 1u << buf;
+        if (__syncthreads_or(timed_out)) {  // block-uniform: every thread leaves together
+            failed = true;
+            if (threadIdx.x == 0) atomicOr(L.overflow, kWaitTimedOut);
+            // the other buffer's copy, if one was issued, is waited for (bounded) before leaving
+            if (prefetch) mbar_wait(&s_bar[buf ^ 1], (phases >> (buf ^ 1)) & 1u);
+            break;
+        }
+        float4* s_pts = stage0 + buf * stage_pitch;
+        if (offset_rows && J.row_mode == kRowPair) {
+            // row offset of the inner point for jobs with every row on chip
+            for (int k = threadIdx.x; k < jn; k += NT) s_pts[k].w = __int_as_float(__float_as_int(s_pts[k].w) * S.pad);
+            __syncthreads();
+        } else if (offset_rows) {
+            for (int k = threadIdx.x; k < jn; k += NT) s_pts[k].w = __int_as_float(0);
+            __syncthreads();
+        }
+        pairs_since_flush += static_cast<long long>(TILE) * TILE;
+        const bool diag = J.self && ti == tj;
+        const bool has_tail = J.b_base + j0 + jn > J.tail_end - 3;  // scalar-tail partners: last 3 of a row
+        const bool full = (ti + 1) * TILE <= J.na;
+        const bool general = diag || has_tail || !full;
+        run_segments<NT, R, WEIGHTED, DREG>(J, S, s_pts, o, j0, jn, general, diag, wsc, Rg);
+        fence_proxy_async();  // this thread's accesses to the buffer before the next bulk copy into it
+        __syncthreads();      // every thread is done with the buffer
+        if (!prefetch && gn < L.total_tiles) issue(gn, buf);
+        else buf ^= 1;
+        g = gn;
     }
-    if (cur >= 0) flush_hist<TILE, WEIGHTED, DREG>(L.jobs[cur], S, R);
-    // warp-aggregated overflow report
-    for (int o = 16; o > 0; o >>= 1) overflow += __shfl_xor_sync(0xffffffffu, overflow, o);
-    if ((threadIdx.x & 31) == 0 && overflow) atomicAdd(L.overflow, overflow);
+    if (cur >= 0 && !failed) flush_hist<NT, WEIGHTED, DREG>(L.jobs[cur], S, Rg, L.overflow);
+    if (!failed && threadIdx.x == 0) {
+        mbar_inval(&s_bar[0]);
+        mbar_inval(&s_bar[1]);
+    }
 }
 
-}  // namespace
-
-namespace {
-template <int TILE, bool WEIGHTED, bool DREG>
+template <int NT, int R, bool WEIGHTED, bool DREG>
 void launch_one(const PairLaunch& L, int grid, size_t smem, cudaStream_t s) {
-    cudaFuncSetAttribute(pairhist_kernel<TILE, WEIGHTED, DREG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    pairhist_kernel<TILE, WEIGHTED, DREG><<<grid, TILE, smem, s>>>(L);
+    cudaFuncSetAttribute(pairhist_kernel<NT, R, WEIGHTED, DREG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    pairhist_kernel<NT, R, WEIGHTED, DREG><<<grid, NT, smem, s>>>(L);
 }
+
+template <int TILE>
+void launch_tile(const PairLaunch& L, int grid, size_t smem, cudaStream_t s) {
+    constexpr int NT = TILE / kOuter;
+    // register-held offset sums exist for unweighted launches only (pairhist_dreg)
+    if (L.weighted) launch_one<NT, kOuter, true, false>(L, grid, smem, s);
+    else if (L.dreg) launch_one<NT, kOuter, false, true>(L, grid, smem, s);
+    else launch_one<NT, kOuter, false, false>(L, grid, smem, s);
+}
+
+template <int NT, int R, bool WEIGHTED, bool DREG>
+int occupancy_one(size_t smem) {
+    auto k = pairhist_kernel<NT, R, WEIGHTED, DREG>;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, NT, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    return n > 0 ? n : 1;
+}
+
+template <int TILE>
+int occupancy_tile(size_t smem, bool weighted, bool dreg) {
+    constexpr int NT = TILE / kOuter;
+    if (weighted) return occupancy_one<NT, kOuter, true, false>(smem);
+    if (dreg) return occupancy_one<NT, kOuter, false, true>(smem);
+    return occupancy_one<NT, kOuter, false, false>(smem);
+}
+
 }  // namespace
 
-void pairhist_launch(const PairLaunch& L, int tile, int grid, size_t smem, cudaStream_t s) {
-    // register-held offset sums exist for unweighted launches only (pairhist_dreg)
-    if (tile == 1024) {
-        if (L.weighted) launch_one<1024, true, false>(L, grid, smem, s);
-        else if (L.dreg) launch_one<1024, false, true>(L, grid, smem, s);
-        else launch_one<1024, false, false>(L, grid, smem, s);
-    } else if (tile == 256) {
-        if (L.weighted) launch_one<256, true, false>(L, grid, smem, s);
-        else if (L.dreg) launch_one<256, false, true>(L, grid, smem, s);
-        else launch_one<256, false, false>(L, grid, smem, s);
-    } else {
-        if (L.weighted) launch_one<512, true, false>(L, grid, smem, s);
-        else if (L.dreg) launch_one<512, false, true>(L, grid, smem, s);
-        else launch_one<512, false, false>(L, grid, smem, s);
-    }
+int pairhist_ctas_per_sm(size_t smem, int tile, bool dreg, bool weighted) {
+    if (tile == 1024) return occupancy_tile<1024>(smem, weighted, dreg);
+    if (tile == 256) return occupancy_tile<256>(smem, weighted, dreg);
+    return occupancy_tile<512>(smem, weighted, dreg);
+}
+
+void pairhist_launch(const PairLaunch& L0, int tile, int grid, size_t smem, cudaStream_t s) {
+    PairLaunch L = L0;
+    // double-buffered staging when the launch was given the room for it
+    L.stages = smem >= pairhist_layout_bytes(L.smem_rows, L.smem_bins, L.weighted != 0, tile, L.dreg != 0, 2) ? 2 : 1;
+    if (tile == 1024) launch_tile<1024>(L, grid, smem, s);
+    else if (tile == 256) launch_tile<256>(L, grid, smem, s);
+    else launch_tile<512>(L, grid, smem, s);
 }
 
 }  // namespace ausaxs_b200

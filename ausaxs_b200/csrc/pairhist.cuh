@@ -54,30 +54,51 @@ struct PairLaunch {
     int32_t smem_rows;              // rows of the on-chip count array
     int32_t smem_bins;              // bins of the on-chip arrays (>= every job's nbins)
     unsigned long long* tile_counter;
-    unsigned long long* overflow;   // pairs whose bin fell outside the job's nbins
+    unsigned long long* overflow;   // pairs whose bin fell outside the job's nbins (bit 62: a bounded
+                                    // wait of the kernel ran out)
     int32_t weighted;
     const float* wscale;            // device: 2^k with max|w_i w_j| * 2^k < 2^30 (weighted launches)
     int32_t dreg;                   // u64 offset sums in registers instead of shared memory (pairhist_dreg)
+    int32_t stages;                 // staging buffers of inner tiles (set by pairhist_launch from the
+                                    // shared memory it is given: 2 = the next tile's copy overlaps)
 };
+
+// Outer points per thread: a tile of `tile` points per side runs tile / kOuter threads.
+constexpr int kOuter = 2;
+inline int pairhist_threads(int tile) { return tile / kOuter; }
 
 // Shared-memory budget of one CTA (opt-in maximum less the static allocations) and the footprint above
 // which only one CTA fits on an SM.
 constexpr size_t kPairSmemCap = 232448 - 1024;
 constexpr size_t kPairSmemTwoPerSm = 233472 / 2 - 1024;
-// Register-held offset sums cover bins [0, kDregBins): thread t holds bins t + k * TILE.
+// Register-held offset sums cover bins [0, kDregBins): thread t holds bins t + k * threads.
 constexpr int kDregBins = 4096;
 
-// Bytes of dynamic shared memory a launch needs (layout of pairhist_kernel); dreg: the u64 offset sums
-// live in registers.
-inline size_t pairhist_smem_bytes(int rows, int bins, bool weighted, int tile, bool dreg = false) {
+// Bytes of dynamic shared memory of a launch's layout (pairhist_kernel): counts [rows][bins + 1]
+// (the last column collects overflow), u64 offset sums (unless dreg: in registers), the u32 offset
+// accumulator, weight sums (weighted), and `stages` buffers of `tile` inner points.
+inline size_t pairhist_layout_bytes(int rows, int bins, bool weighted, int tile, bool dreg, int stages) {
     size_t pad = (size_t)bins + 1;
     size_t row = (pad * 4 + 15) & ~(size_t)15;
     size_t b = ((size_t)rows * pad * 4 + 15) & ~(size_t)15;  // u32 counts
     if (!dreg) b += (pad * 8 + 15) & ~(size_t)15;            // offset sums: u64
     b += row;                                                // u32 offset accumulator
     if (weighted) b += 2 * row;                              // weight sums (lo, hi)
-    b += (size_t)tile * 16;                                  // inner tile of points (16-byte aligned)
+    b += (size_t)stages * tile * 16;                         // inner tiles of points (16-byte aligned)
     return b + 64;
+}
+
+// The launch's footprint: double-buffered staging when it fits and costs no CTA per SM, else one buffer.
+inline size_t pairhist_smem_bytes(int rows, int bins, bool weighted, int tile, bool dreg = false) {
+    const size_t one = pairhist_layout_bytes(rows, bins, weighted, tile, dreg, 1);
+    const size_t two = pairhist_layout_bytes(rows, bins, weighted, tile, dreg, 2);
+    if (two > kPairSmemCap) return one;
+    const int threads_cap = 2048 / pairhist_threads(tile);
+    auto ctas = [threads_cap](size_t b) {
+        const int by_smem = (int)(233472 / (b + 1024));
+        return by_smem < threads_cap ? by_smem : threads_cap;
+    };
+    return ctas(two) >= ctas(one) ? two : one;
 }
 
 // Whether a launch keeps its u64 offset sums in registers: unweighted launches of at most kDregBins bins
@@ -91,12 +112,8 @@ inline size_t pairhist_launch_smem(int rows, int bins, bool weighted, int tile) 
     return pairhist_smem_bytes(rows, bins, weighted, tile, pairhist_dreg(rows, bins, weighted, tile));
 }
 
-// Resident CTAs per SM of a launch (register-sum launches and 1024-point tiles are compiled for one).
-inline int pairhist_ctas_per_sm(size_t smem, int tile, bool dreg) {
-    if (dreg || tile >= 1024) return 1;
-    const int by_smem = (int)(233472 / (smem + 1024));
-    return by_smem < 1 ? 1 : (by_smem < 2048 / tile ? by_smem : 2048 / tile);
-}
+// Resident CTAs per SM of a launch with this footprint (the runtime's occupancy of the instantiation).
+int pairhist_ctas_per_sm(size_t smem, int tile, bool dreg, bool weighted);
 
 // Rows of [rows][bins] counts that fit on chip for `tile`-point tiles (512 covers 256 as well).
 inline int pairhist_max_rows(int bins, bool weighted, int tile = 512) {

@@ -288,7 +288,7 @@ struct Assembly {
         }
         smem = pairhist_launch_smem(max_rows, nb, false, tile);
         for (Work& Wk : work) Wk.L.dreg = pairhist_dreg(max_rows, nb, false, tile) ? 1 : 0;
-        const int per_sm = pairhist_ctas_per_sm(smem, tile, pairhist_dreg(max_rows, nb, false, tile));
+        const int per_sm = pairhist_ctas_per_sm(smem, tile, pairhist_dreg(max_rows, nb, false, tile), false);
         // device tables: jobs, zero ranges, partial pointers of the master sum
         std::vector<const unsigned long long*> ptrs[3];
         for (const Part& pt : parts) ptrs[pt.kind].push_back(part.as<unsigned long long>(pt.off));
