@@ -370,7 +370,10 @@ __global__ void __launch_bounds__(NT, DREG ? 1 : (512 / NT > 1 ? 512 / NT : 1)) 
 
     // tile ids come in chunks from the global counter; the next tile id is known one tile ahead so
     // that its copy can be issued before the current tile is processed
+    int grabs = 0;
     auto grab = [&]() -> long long {
+        if (L.max_grabs > 0 && grabs >= L.max_grabs) return static_cast<long long>(L.total_tiles);  // block-uniform
+        ++grabs;
         if (threadIdx.x == 0) s_grab = static_cast<long long>(atomicAdd(L.tile_counter, static_cast<unsigned long long>(L.chunk)));
         __syncthreads();
         const long long v = s_grab;

@@ -61,6 +61,9 @@ struct PairLaunch {
     int32_t dreg;                   // u64 offset sums in registers instead of shared memory (pairhist_dreg)
     int32_t stages;                 // staging buffers of inner tiles (set by pairhist_launch from the
                                     // shared memory it is given: 2 = the next tile's copy overlaps)
+    int32_t max_grabs;              // > 0: a CTA takes at most this many chunks and exits (the grid
+                                    // must then cover the tiles: grid * max_grabs * chunk >= total);
+                                    // bounded CTAs let the block scheduler interleave other launches
 };
 
 // Outer points per thread: a tile of `tile` points per side runs tile / kOuter threads.

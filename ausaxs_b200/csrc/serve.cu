@@ -13,10 +13,15 @@
 // the master (the sum of the partials) equals the full recompute bit for bit, whether a request runs
 // alone or overlaps others.
 //
-// Requests of one assembly run in order on its own stream; requests of different assemblies overlap
-// on the device.  A server admits assemblies while their device footprint fits its memory budget and
-// requests while an output slot is free (continuous batching: a request is admitted as soon as a
-// slot frees, without waiting for the others in flight).
+// Requests of one assembly run in order; requests of different assemblies overlap on the device.  A
+// server admits assemblies while their device footprint fits its memory budget and requests while an
+// output slot is free (continuous batching: a request is admitted as soon as a slot frees, without
+// waiting for the others in flight).  Scheduling on the device: every assembly has a high- and a
+// low-priority stream; a move whose pair count is at most the median over the server's bodies goes to
+// the high-priority one (an event keeps each assembly's requests in order across its two streams), and
+// the pair launches of requests are made of short-lived CTAs (a few tiles each) instead of one
+// persistent grid, so the block scheduler hands SMs to a small move as soon as running CTAs finish
+// instead of after a large move's whole launch.
 #include <algorithm>
 #include <array>
 #include <chrono>
@@ -89,8 +94,15 @@ void compose(Pose& P, const double* R, const double* t) {
 
 }  // namespace
 
+// tiles of a serving pair launch's CTA: a CTA lives for a few hundred microseconds at most
+constexpr int kServeTilesPerCta = 2;
+
 struct Assembly {
-    Ctx C;  // own stream
+    Ctx C;  // C.stream: the stream of the request being enqueued (one of `streams`)
+    cudaStream_t streams[2] = {nullptr, nullptr};  // [0] high priority, [1] low priority
+    cudaEvent_t last = nullptr;                    // end of the last enqueued request
+    bool has_last = false;
+    std::vector<long long> move_pairs;             // pair evaluations of a move of each body
     ausaxs_hist_config cfg{};
     Structure S;  // the whole assembly: current coordinates; its plan's accumulators are the master
     int B = 0, N = 0, W = 0;
@@ -124,11 +136,26 @@ struct Assembly {
 
     ~Assembly() {
         cudaSetDevice(C.device);
-        if (C.stream) cudaStreamSynchronize(C.stream);
+        sync();
         for (double* p : all_slots) cudaFreeHost(p);
         if (C.h_stats) cudaFreeHost(C.h_stats);
         C.h_stats = nullptr;
-        if (C.stream && C.own_stream) cudaStreamDestroy(C.stream);
+        for (auto& st : streams)
+            if (st) cudaStreamDestroy(st);
+        if (last) cudaEventDestroy(last);
+        C.stream = nullptr;
+    }
+
+    void sync() {
+        for (auto& st : streams)
+            if (st) cudaStreamSynchronize(st);
+    }
+
+    // the stream of a request with this priority, ordered after the assembly's previous request
+    void select_stream(bool high) {
+        cudaStream_t st = streams[high ? 0 : 1];
+        if (has_last && st != C.stream) AUSAXS_CUDA(cudaStreamWaitEvent(st, last, 0));
+        C.stream = st;
     }
 
     size_t block_bytes(int rows) const { return align_up((size_t)(rows + 1) * S.plan.nb * 8, 256); }
@@ -141,8 +168,13 @@ struct Assembly {
             throw Error{AUSAXS_ERR_ARGUMENT, "bad assembly arguments"};
         C.device = device;
         C.sm_count = sms;
-        AUSAXS_CUDA(cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking));
-        C.own_stream = true;
+        int least = 0, greatest = 0;
+        AUSAXS_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        AUSAXS_CUDA(cudaStreamCreateWithPriority(&streams[0], cudaStreamNonBlocking, greatest));
+        AUSAXS_CUDA(cudaStreamCreateWithPriority(&streams[1], cudaStreamNonBlocking, least));
+        AUSAXS_CUDA(cudaEventCreateWithFlags(&last, cudaEventDisableTiming));
+        C.stream = streams[1];
+        C.own_stream = false;  // the streams belong to the assembly
         AUSAXS_CUDA(cudaMallocHost(&C.h_stats, sizeof(PrepStats)));
         cfg = c;
         B = n_bodies;
@@ -309,8 +341,18 @@ struct Assembly {
         for (Work& Wk : work) {
             Wk.L.jobs = tables.as<PairJob>() + reinterpret_cast<size_t>(Wk.L.jobs);
             Wk.zero_off = jobs_bytes + Wk.zero_off * sizeof(ZeroRange);
-            Wk.grid = (int)std::min<long long>((long long)sms * per_sm, std::max<long long>(1, Wk.L.total_tiles));
-            Wk.L.chunk = (int)std::max<long long>(1, std::min<long long>(8, Wk.L.total_tiles / ((long long)Wk.grid * 8)));
+            // short-lived CTAs of kServeTilesPerCta tiles each (one tile per grab), at least one wave
+            Wk.L.chunk = 1;
+            Wk.L.max_grabs = kServeTilesPerCta;
+            const long long need = (Wk.L.total_tiles + kServeTilesPerCta - 1) / kServeTilesPerCta;
+            Wk.grid = (int)std::max<long long>(1, std::min<long long>(need, (long long)INT32_MAX));
+            (void)per_sm;
+        }
+        // pair evaluations of a move of each body (the body against the rest, and its own pairs)
+        const long long NW = (long long)N + W;
+        for (int k = 0; k < B; ++k) {
+            const long long nk = (long long)(a_off[k + 1] - a_off[k]) + (w_off[k + 1] - w_off[k]);
+            move_pairs.push_back(nk * (NW - nk) + nk * (nk - 1) / 2);
         }
         const FinalizeFF& F = P.fin_ff;
         msum.nb = nb;
@@ -416,6 +458,19 @@ struct Server {
     std::map<long long, Req> inflight;
     long long next_ticket = 1;
     std::vector<cudaEvent_t> events;
+    long long high_priority_pairs = 0;  // moves of at most this many pairs run on high-priority streams
+
+    // the median move size over the bodies of every admitted assembly
+    void update_priority_threshold() {
+        std::vector<long long> all;
+        for (auto& a : asms) all.insert(all.end(), a.second->move_pairs.begin(), a.second->move_pairs.end());
+        if (all.empty()) {
+            high_priority_pairs = 0;
+            return;
+        }
+        std::nth_element(all.begin(), all.begin() + all.size() / 2, all.end());
+        high_priority_pairs = all[all.size() / 2];
+    }
 
     ~Server() {
         cudaSetDevice(device);
@@ -499,6 +554,7 @@ int ausaxs_gpu_server_admit(ausaxs_gpu_server* s, const ausaxs_hist_config* cfg,
         S.used += (long long)A->footprint;
         *id = S.next_id++;
         S.asms[*id] = std::move(A);
+        S.update_priority_threshold();
     });
 }
 
@@ -512,6 +568,7 @@ int ausaxs_gpu_server_release(ausaxs_gpu_server* s, int32_t id) {
             if (r.second.asm_id == id) throw Error{AUSAXS_ERR_CAPACITY, "the assembly has requests in flight"};
         S.used -= (long long)A.footprint;
         S.asms.erase(id);
+        S.update_priority_threshold();
     });
 }
 
@@ -544,7 +601,10 @@ int ausaxs_gpu_server_submit(ausaxs_gpu_server* s, int32_t id, int32_t body, con
             AUSAXS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         }
         try {
+            A.select_stream(body >= 0 && A.move_pairs[body] <= S.high_priority_pairs);
             A.enqueue_request(body, R, t, slot);
+            AUSAXS_CUDA(cudaEventRecord(A.last, A.C.stream));
+            A.has_last = true;
             AUSAXS_CUDA(cudaEventRecord(ev, A.C.stream));
         } catch (...) {
             S.events.push_back(ev);
@@ -618,7 +678,7 @@ int ausaxs_gpu_server_coordinates(ausaxs_gpu_server* s, int32_t id, float* atoms
         Server& S = s->impl;
         AUSAXS_CUDA(cudaSetDevice(S.device));
         Assembly& A = S.get(id);
-        AUSAXS_CUDA(cudaStreamSynchronize(A.C.stream));
+        A.sync();
         if (atoms_xyzw && A.N)
             AUSAXS_CUDA(cudaMemcpy(atoms_xyzw, A.S.atoms_for_pairs(), (size_t)A.N * 16, cudaMemcpyDeviceToHost));
         if (waters_xyzw && A.W) AUSAXS_CUDA(cudaMemcpy(waters_xyzw, A.S.raw_w.p, (size_t)A.W * 16, cudaMemcpyDeviceToHost));
@@ -631,7 +691,7 @@ int ausaxs_gpu_server_histogram(ausaxs_gpu_server* s, int32_t id, ausaxs_hist_re
         Server& S = s->impl;
         AUSAXS_CUDA(cudaSetDevice(S.device));
         Assembly& A = S.get(id);
-        AUSAXS_CUDA(cudaStreamSynchronize(A.C.stream));
+        A.sync();
         A.S.read_histogram(A.cfg, out);
     });
 }
