@@ -254,9 +254,11 @@ struct Batch {
     }
 
     void enqueue_all(int nq, cudaStream_t s) {
-        AUSAXS_CUDA(cudaEventRecord(pair_t0, s));
+        // external records: event-record nodes of the captured graph (a plain record in a capture only
+        // orders streams), so every replay timestamps the pair stage
+        AUSAXS_CUDA(cudaEventRecordWithFlags(pair_t0, s, cudaEventRecordExternal));
         enqueue_pairs(s);
-        AUSAXS_CUDA(cudaEventRecord(pair_t1, s));
+        AUSAXS_CUDA(cudaEventRecordWithFlags(pair_t1, s, cudaEventRecordExternal));
         ff_finalize_batch_launch(fin.as<FinalizeFF>(), (int)items.size(), max_nb, s);
         ctx->check_launch("finalize");
         debye_fp64_batch_launch(args.as<DebyeArgs>(), (int)items.size(), nq, s);

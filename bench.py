@@ -334,7 +334,10 @@ def run_batch(args, rank, world, local_rank):
                 step()
                 ends[k].record(stream)
                 flush.fill_(float(k))
-                pair_ms.append(B._b.pair_time())  # events inside the graph, read after the step ends
+                try:
+                    pair_ms.append(B._b.pair_time())  # events inside the graph, read after the step ends
+                except _capi.AusaxsError:
+                    pair_ms.append(None)
             torch.cuda.synchronize()
         launches = ctx.launches - launches0
         step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
@@ -404,8 +407,11 @@ def run_batch(args, rank, world, local_rank):
     clocks = clk.summary()
     sm_mhz = clocks.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
     sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
-    kernel_ms = statistics.mean(pair_ms)
+    timed_pairs = [x for x in pair_ms if x is not None]
+    kernel_ms = statistics.mean(timed_pairs) if timed_pairs else float(cand_ms[choice])
     roof = pair_roofline(pairs, kernel_ms, sm_mhz, sms, atomic_rate, 2, INSTR_PER_PAIR)
+    if not timed_pairs:
+        roof["kernel_ms_source"] = "autotuner's timing of the chosen pair plan (graph events unavailable)"
     roof["traffic"] = BATCH_PAIR_TRAFFIC_BYTES
     roof["smem_atomics_per_s_random_bins"] = atomic_rate_random
     roof["note"] = ("kernel_ms = device time of the pair stage (accumulator clearing + every pair launch of the "
