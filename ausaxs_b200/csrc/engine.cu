@@ -239,9 +239,11 @@ bool Structure::lattice_ready() {
     lattice_scan_launch(raw_x.as<float4>(), n_x, st, C.sm_count, s);
     C.check_launch("lattice scan");
     int h[8] = {};
-    AUSAXS_CUDA(cudaMemcpyAsync(h, st, 7 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    AUSAXS_CUDA(cudaMemcpyAsync(h, st, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));
     AUSAXS_CUDA(cudaStreamSynchronize(s));
-    if (h[6]) return false;  // not every coordinate is a (modest) integer
+    if (h[6]) return false;  // not every coordinate is a (modest) integer or integer + 1/2
+    for (int k = 0; k < 3; ++k)
+        if (((h[7] >> (2 * k)) & 3) == 3) return false;  // integers and half-integers on one axis
     LatticeGrid G;
     for (int k = 0; k < 3; ++k) G.lo[k] = h[k];
     G.lx = h[3] - h[0] + 1;
@@ -411,7 +413,7 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
     // lattice and the reference's two rounding rules agree on every squared offset (lattice.cu)
     P.lattice_grid = 0;
     bool use_lattice = false;
-    if (grid && n_x >= kLatticeMinPoints && lattice_ready() && lattice_rules_agree(lat.s2_max, inv_w)) {
+    if (grid && n_x >= kLatticeMinPoints && lattice_ready()) {
         const size_t lsm = lattice_smem_bytes(lat.G.n_lines, lattice_kernel_words(lat.G.words), lat.G.ly, lat.G.lz, nb);
         if (lsm <= kPairSmemCap) {
             use_lattice = true;
@@ -456,6 +458,9 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
         LL.overflow = reinterpret_cast<unsigned long long*>(base + P.off_overflow);
         LL.counter = reinterpret_cast<unsigned long long*>(base + P.off_counter) + 8;  // cleared with the accumulators
         LL.n_items = lat.G.lz * (2 * lat.G.ly - 1);
+        LL.pts = raw_x.as<float4>();
+        LL.n_pts = n_x;
+        LL.tail_fix = lattice_rules_agree(lat.s2_max, inv_w) ? 0 : 1;
     }
 
     // Jobs split into launch groups by the rows they keep on chip: one-row jobs (ww, xx, wx and all

@@ -1,12 +1,14 @@
 // Pair-distance histogram of points on the integer lattice by the autocorrelation of their occupancy.
 //
-// The grid model's excluded-volume dummies sit on the integer lattice (RawGridExv places one at the
-// centre of every volume cell of the 1 A molecular grid, source/core/grid/exv/RawGridExv.cpp:10-59),
-// and the reference bins their self pairs one by one (the exv-exv loop of
-// HistogramManagerMTFFGrid.cpp:66-84).  For integer coordinates every pair's squared distance is an
-// integer s2 that the reference's float evaluation forms exactly (s2 < 2^24), so its bin and in-bin
-// offset depend on s2 alone: the histogram is the sum over offsets (dx, dy, dz) of the number of
-// point pairs with that offset, each offset binned once.
+// The grid model's excluded-volume dummies sit on a lattice of 1 A cells (RawGridExv places one per
+// volume cell of the molecular grid, source/core/grid/exv/RawGridExv.cpp:10-59; at integer or at
+// half-integer coordinates, depending on the grid's origin), and the reference bins their self pairs
+// one by one (the exv-exv loop of HistogramManagerMTFFGrid.cpp:66-84).  Every pair's coordinate
+// differences are then exact integers and its squared distance an integer s2 that the reference's
+// float evaluation forms exactly (s2 < 2^24), so its bin and in-bin offset depend on s2 alone: the
+// histogram is the sum over offsets (dx, dy, dz) of the number of point pairs with that offset, each
+// offset binned once -- by the SIMD evaluators' rule; the few pairs of the scalar tail whose distance
+// is an exact rounding tie are moved afterwards (lattice_tail_kernel).
 //
 // Counting the pairs per offset: the occupancy is stored as bit lines along x (one u32 word per 32
 // cells).  For a line offset (dy, dz) a warp walks every pair of non-empty lines (y, z), (y + dy,
@@ -34,23 +36,31 @@ __global__ void lattice_scan_init(int* st) {
         st[0] = st[1] = st[2] = INT_MAX;
         st[3] = st[4] = st[5] = INT_MIN;
         st[6] = 0;
+        st[7] = 0;
     }
 }
 
+// Cell index of a lattice coordinate: floor(v) (v an integer or an integer + 1/2)
+__device__ __forceinline__ int lattice_cell(float v) { return static_cast<int>(floorf(v)); }
+
+// Every coordinate must be an integer, or an integer + 1/2, of magnitude below 2^20, with one kind
+// per axis (st[7]: bit 2k integers seen on axis k, bit 2k + 1 half-integers): the difference of two
+// such floats is then an exact integer.
 __global__ void lattice_scan_kernel(const float4* p, int n, int* st) {
     int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
-    int bad = 0;
+    int bad = 0, kinds = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const float4 v = p[i];
         const float c[3] = {v.x, v.y, v.z};
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            // integers of magnitude below 2^20 (NaN fails the comparison)
-            if (!(c[k] == rintf(c[k]) && fabsf(c[k]) < 1048576.0f)) {
+            const float t = 2.0f * c[k];  // exact below 2^20
+            if (!(t == rintf(t) && fabsf(c[k]) < 1048576.0f)) {  // NaN fails the comparison
                 bad = 1;
                 continue;
             }
-            const int iv = static_cast<int>(c[k]);
+            kinds |= (c[k] == rintf(c[k]) ? 1 : 2) << (2 * k);
+            const int iv = lattice_cell(c[k]);
             lo[k] = min(lo[k], iv);
             hi[k] = max(hi[k], iv);
         }
@@ -62,6 +72,7 @@ __global__ void lattice_scan_kernel(const float4* p, int n, int* st) {
             hi[k] = max(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
         }
     }
+    for (int o = 16; o > 0; o >>= 1) kinds |= __shfl_xor_sync(0xffffffffu, kinds, o);
     bad = __any_sync(0xffffffffu, bad);
     if ((threadIdx.x & 31) == 0) {
 #pragma unroll
@@ -70,6 +81,7 @@ __global__ void lattice_scan_kernel(const float4* p, int n, int* st) {
             if (hi[k] != INT_MIN) atomicMax(&st[3 + k], hi[k]);
         }
         if (bad) atomicOr(&st[6], 1);
+        if (kinds) atomicOr(&st[7], kinds);
     }
 }
 
@@ -85,9 +97,9 @@ struct BuildArgs {
 __global__ void lattice_set_kernel(BuildArgs A) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
         const float4 v = A.p[i];
-        const int x = static_cast<int>(v.x) - A.lo[0];
-        const int y = static_cast<int>(v.y) - A.lo[1];
-        const int z = static_cast<int>(v.z) - A.lo[2];
+        const int x = lattice_cell(v.x) - A.lo[0];
+        const int y = lattice_cell(v.y) - A.lo[1];
+        const int z = lattice_cell(v.z) - A.lo[2];
         // every coordinate lies in [lo, hi] by the scan; checked once more before the write
         if (x < 0 || x >= A.lx || y < 0 || y >= A.ly || z < 0 || z >= A.lz) {
             atomicOr(&A.info[1], 2);
@@ -231,6 +243,42 @@ __global__ void __launch_bounds__(kLatticeThreads, 1) lattice_kernel(LatticeLaun
     if (threadIdx.x == 0 && h_cnt[nb]) atomicAdd(L.overflow, h_cnt[nb]);
 }
 
+// The reference bins the last (row length mod 4) partners of every row with its scalar evaluator,
+// which rounds ties away from zero (common.cuh::pair_eval); the lattice kernel used the SIMD rule (ties
+// to even) for every pair.  For the self pairs i < j of n points, row i's scalar partners are
+// j >= n - ((n - i - 1) & 3): at most 3 per row.  Where the two rules give different bins (an exact
+// half-integer distance in bin units) the pair's count and offset move to the scalar rule's bin.
+__global__ void lattice_tail_kernel(LatticeLaunch L) {
+    const int n = L.n_pts;
+    const float bin_limit = pair_bin_limit(L.nbins);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 a = L.pts[i];
+        const int ts = n - ((n - i - 1) & 3);
+        for (int j = ts > i + 1 ? ts : i + 1; j < n; ++j) {
+            const float4 b = L.pts[j];
+            const PairBin simd = pair_eval(a, b, L.inv_w, false);
+            const PairBin tail = pair_eval(a, b, L.inv_w, true);
+            if (simd.bin == tail.bin) continue;
+            // the pair leaves the SIMD rule's bin (or the overflow count) for the scalar rule's
+            const bool in0 = static_cast<unsigned>(simd.bin) < static_cast<unsigned>(L.nbins) &&
+                             __fadd_rn(simd.xr, kMagic) < bin_limit;
+            const bool in1 = static_cast<unsigned>(tail.bin) < static_cast<unsigned>(L.nbins);
+            if (in0) {
+                atomicAdd(&L.counts[simd.bin], ~0ull);  // -1 (two's complement: the total stays exact)
+                if (L.dsum) atomicAdd(&L.dsum[simd.bin], 0ull - pair_residual(simd, L.c, L.scale));
+            } else {
+                atomicAdd(L.overflow, ~0ull);
+            }
+            if (in1) {
+                atomicAdd(&L.counts[tail.bin], 1ull);
+                if (L.dsum) atomicAdd(&L.dsum[tail.bin], static_cast<unsigned long long>(pair_residual(tail, L.c, L.scale)));
+            } else {
+                atomicAdd(L.overflow, 1ull);
+            }
+        }
+    }
+}
+
 template <int W>
 void launch_w(const LatticeLaunch& L, int grid, size_t smem, cudaStream_t s) {
     cudaFuncSetAttribute(lattice_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -270,6 +318,10 @@ void lattice_launch(const LatticeLaunch& L, int grid, size_t smem, cudaStream_t 
         case 2: launch_w<2>(L, grid, smem, s); break;
         case 4: launch_w<4>(L, grid, smem, s); break;
         default: launch_w<8>(L, grid, smem, s); break;
+    }
+    if (L.tail_fix) {
+        const int g = std::max(1, std::min(grid * 2, (L.n_pts + 255) / 256));
+        lattice_tail_kernel<<<g, 256, 0, s>>>(L);
     }
 }
 

@@ -29,6 +29,10 @@ struct LatticeLaunch {
     unsigned long long* overflow;  // pairs beyond the last bin
     unsigned long long* counter;   // work-item counter (zeroed before the launch)
     int n_items;                   // lz * (2 ly - 1) line offsets (dz >= 0)
+    const float4* pts;             // the points themselves, in the reference's loop order
+    int n_pts;
+    int tail_fix;                  // the two rounding rules differ at some squared offset: correct the
+                                   // scalar-tail pairs (lattice_tail_kernel)
 };
 
 // Points per set below which the pair kernel is used for lattice points as well.
@@ -48,8 +52,9 @@ inline size_t lattice_smem_bytes(int n_lines, int words, int ly, int lz, int nbi
     return b + 64;
 }
 
-// Device scan of a point set (stats[0..2] integer minimum, [3..5] maximum, [6] non-zero when a
-// coordinate is not an integer of magnitude < 2^20); stats must hold 8 ints.
+// Device scan of a point set (stats[0..2] minimum cell floor(v), [3..5] maximum, [6] non-zero when a
+// coordinate is neither an integer nor an integer + 1/2 of magnitude < 2^20, [7] bit 2k: integers on
+// axis k, bit 2k + 1: half-integers); stats must hold 8 ints.
 void lattice_scan_launch(const float4* p, int n, int* stats, int sm_count, cudaStream_t s);
 // Bit lines of the points (grid zeroed by the caller: ly * lz * words words), then the compact line
 // store and the table; info[0] = lines, info[1] = non-zero when two points share a cell.
@@ -57,8 +62,9 @@ void lattice_build_launch(const float4* p, int n, const int lo[3], int lx, int l
                           uint32_t* lines, int32_t* table, int* info, int sm_count, cudaStream_t s);
 // Whether the reference's two rounding rules (ties to even in its SIMD evaluators, ties away from
 // zero in the scalar tail) bin every integer squared distance in [1, s2_max] alike at this inverse
-// bin width; the lattice path needs no per-pair loop position only then.
+// bin width; when they do not, lattice_launch also corrects the scalar-tail pairs.
 bool lattice_rules_agree(long long s2_max, float inv_w);
+// The lattice kernel, then (L.tail_fix) the scalar-tail correction.
 void lattice_launch(const LatticeLaunch& L, int grid, size_t smem, cudaStream_t s);
 
 }  // namespace ausaxs_b200
