@@ -87,6 +87,10 @@ void Structure::load_begin(const float* atoms, int n_atoms, const float* waters,
     Ctx& C = *ctx;
     cudaStream_t s = C.stream;
     ff_typed = ff_typed_;
+    // new points: the lattice form of the dummies (and a plan that bins them with it) is rebuilt
+    lat.tried = false;
+    lat.usable = false;
+    if (plan.lattice_grid > 0) plan.manager = 0;
     n_a = n_atoms;
     n_w = n_waters;
     n_x = n_exv;
@@ -291,7 +295,7 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
     nb = std::min(nb, cfg.bin_count);
     if (P.manager == cfg.manager && P.weighted == weighted && P.bin_count == cfg.bin_count &&
         P.bin_width == cfg.bin_width && P.n_a == n_a && P.n_w == n_w && P.n_x == n_x && P.T == T && P.nb >= nb &&
-        P.nb <= nb + 64)
+        P.nb <= nb + 64 && (cfg.manager != AUSAXS_MANAGER_FFGRID || n_x < kLatticeMinPoints || lat.tried))
         return P;
 
     Ctx& C = *ctx;

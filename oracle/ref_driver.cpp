@@ -34,6 +34,9 @@
 #include <hist/histogram_manager/HistogramManagerMTFFExplicit.h>
 #include <hist/histogram_manager/HistogramManagerMTFFGrid.h>
 #include <hist/histogram_manager/PartialHistogramManagerMT.h>
+#include <hist/histogram_manager/SymmetryManagerMT.h>
+#include <data/symmetry/PredefinedSymmetries.h>
+#include <data/symmetry/CompositeSymmetry.h>
 #include <hist/intensity_calculator/CompositeDistanceHistogramFFGrid.h>
 #include <hist/intensity_calculator/DistanceHistogram.h>
 #include <hist/intensity_calculator/ExactDebyeCalculator.h>
@@ -52,6 +55,10 @@
 #include <hydrate/generation/RadialHydration.h>
 #include <hydrate/generation/HydrationStrategy.h>
 #include <io/File.h>
+
+#ifdef AUSAXS_ADAPTER
+#include "adapter/gpu_adapter.h"
+#endif
 
 #include <chrono>
 #include <cstring>
@@ -298,6 +305,33 @@ int ref_read_structure(const char* path, int implicit_h, int center, double* ato
 
 // Rigid move of one body: x <- R x + t, through Body::rotate / Body::translate
 // (source/core/data/Body.cpp:135-156), which also signal the partial managers.
+// A predefined symmetry (symmetry::create: "c3", "d2", "tetrahedral", "icosahedral", "p2", ...) on a body,
+// its leaves' first translation and rotation parameters set as the reference's own tests set them
+// (tests/feature/hist/symmetries/symmetry_body_frame.cpp:99-109).
+int ref_body_add_symmetry(void* m, int body, const char* name, double translation, double rotation) {
+    return guarded([&] {
+        auto* mol = static_cast<FixedVolumeMolecule*>(m);
+        if (body < 0 || body >= (int)mol->size_body()) throw std::runtime_error("no such body");
+        auto sym = symmetry::create(name);
+        symmetry::for_each_leaf(*sym, [translation, rotation](symmetry::ISymmetry& leaf) {
+            auto t = leaf.span_translation();
+            auto r = leaf.span_rotation();
+            if (!t.empty()) t[0] = translation;
+            if (!r.empty()) r[0] = rotation;
+        });
+        mol->get_body(body).symmetry().add(std::move(sym));
+    });
+}
+
+// Whether this build runs the symmetry, Simple and partial managers' pair work on the device.
+int ref_adapter_build() {
+#ifdef AUSAXS_ADAPTER
+    return 1;
+#else
+    return 0;
+#endif
+}
+
 int ref_body_move(void* m, int body, const double* R, const double* t) {
     return guarded([&] {
         auto* mol = static_cast<FixedVolumeMolecule*>(m);
@@ -441,6 +475,13 @@ int ref_manager_set(void* m, int manager, int weighted_bins, const double* exv, 
                           : (hist::IHistogramManager*)new GivenExvGridManager<false>(mol, std::move(x));
                 break;
             case 5: PICK(hist::PartialHistogramManagerMT); break;
+            case 6: PICK(hist::SymmetryManagerMT); break;
+#ifdef AUSAXS_ADAPTER
+            case 7:  // the device FFAvg manager of the adapter (weighted bins)
+                out = vbw ? (hist::IHistogramManager*)new hist::GpuHistogramManagerMTFFAvg<true>(mol)
+                          : (hist::IHistogramManager*)new hist::GpuHistogramManagerMTFFAvg<false>(mol);
+                break;
+#endif
             default: throw std::runtime_error("unknown manager");
         }
 #undef PICK

@@ -119,3 +119,26 @@ def test_off_lattice_dummies_use_the_pair_kernel(gpu_ctx):
                   O.pack_points(exv, np.zeros(len(exv), np.int32), True), 0.1, 8000, 0.0)
     np.testing.assert_array_equal(h.get_raw_aa_counts_by_ff(), o.aa)
     ctx.close()
+
+
+def test_reloaded_dummies_are_not_binned_with_a_stale_lattice(gpu_ctx):
+    """One-shot calls reuse the context's scratch structure: after a lattice-eligible set of dummies,
+    a set of the same size with two dummies in one cell (not eligible) and then an eligible set with
+    other positions must each match the oracle (the lattice and the plan built for the previous
+    points are discarded on reload)."""
+    rng = np.random.default_rng(29)
+    xyz = rng.normal(0, 6, (400, 3))
+    ff = np.full(len(xyz), 3, np.int32)
+    n = 3000
+    base = _ball_lattice(31, 10.0, 0.0)[:n]
+    dup = base.copy()
+    dup[-1] = dup[0]                              # shared cell
+    moved = _ball_lattice(37, 10.0, 0.5)[:n]      # other positions, half-integer
+    for exv in (base, dup, moved, base):
+        m = hist.Molecule(atoms=xyz, ff_types=ff, waters=np.zeros((0, 3)), exv=exv, volume=1.0)
+        h = hist.HistogramManagerMTFFGrid(m, 0.1, 8000, gpu_ctx).calculate_all()
+        o = O.hist_ff(2, O.pack_points(xyz, ff, True), O.pack_points(np.zeros((0, 3)), np.zeros(0, np.int32), True),
+                      O.pack_points(exv, np.zeros(len(exv), np.int32), True), 0.1, 8000, 0.0)
+        assert h.max_bin == len(o.d_axis)
+        np.testing.assert_array_equal(h.get_raw_aa_counts_by_ff(), o.aa)
+        np.testing.assert_allclose(h.get_d_axis_xx(), o.d_axis_xx, atol=d_atol(0.1), rtol=0)
