@@ -242,7 +242,10 @@ def linear_lsq(data, model, err):
 # ---------------------------------------------------------------------------
 
 def ref_path() -> str:
-    return os.path.join(HERE, "_ref", "libausaxs_ref.so")
+    """The compiled reference; AUSAXS_REF_LIB=libausaxs_ref_gpu.so selects its adapter build (the
+    reference's Simple, partial and symmetry managers over the device calculator, and the device FFAvg
+    manager: oracle/Makefile target `adapter`)."""
+    return os.path.join(HERE, "_ref", os.environ.get("AUSAXS_REF_LIB", "libausaxs_ref.so"))
 
 
 def ref_read_structure(path: str, implicit_h: int = -1, center: int = -1):
@@ -318,6 +321,8 @@ def ref(threads: int = 0):
         R.ref_molecule_new.argtypes = [_f64p, C.c_int, _f64p, C.c_int, _i32p, C.c_int, C.c_double]
         R.ref_molecule_free.argtypes = [vp]
         R.ref_body_move.argtypes = [vp, C.c_int, _f64p, _f64p]
+        R.ref_body_add_symmetry.argtypes = [vp, C.c_int, C.c_char_p, C.c_double, C.c_double]
+        R.ref_adapter_build.restype = C.c_int
         R.ref_body_coords.argtypes = [vp, C.c_int, C.c_void_p, C.POINTER(C.c_int)]
         R.ref_body_move_in_grid.argtypes = [vp, C.c_int, _f64p, _f64p]
         R.ref_hydrate.argtypes = [vp, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_void_p,
@@ -350,7 +355,8 @@ def _check(R, rc):
         raise RuntimeError("reference: " + R.ref_last_error().decode())
 
 
-MANAGERS = {"single": 0, "mt": 1, "ffavg": 2, "ffexplicit": 3, "ffgrid": 4, "partial": 5}
+MANAGERS = {"single": 0, "mt": 1, "ffavg": 2, "ffexplicit": 3, "ffgrid": 4, "partial": 5, "symmetry": 6,
+            "gpu_ffavg": 7}
 
 
 class RefMolecule:
@@ -425,6 +431,10 @@ class RefMolecule:
         R = ref()
         _check(R, R.ref_body_move_in_grid(self.h, body, np.ascontiguousarray(np.asarray(Rm, np.float64).reshape(9)),
                                           np.ascontiguousarray(np.asarray(t, np.float64).reshape(3))))
+
+    def add_symmetry(self, body, name, translation, rotation=0.0):
+        """A predefined symmetry of the reference (symmetry::create(name)) on a body."""
+        _check(ref(), ref().ref_body_add_symmetry(self.h, body, name.encode(), float(translation), float(rotation)))
 
     def move_body(self, body, Rm, t):
         R = ref()
