@@ -224,6 +224,7 @@ struct Batch {
                 L.weighted = 0;
                 L.dreg = pairhist_dreg(rows[b][g], max_nb, false, La.tile) ? 1 : 0;
                 L.wscale = nullptr;
+                L.inv_w = items.empty() ? 0.f : items[order[0]]->plan.inv_w;
                 AUSAXS_CUDA(cudaMemcpy(jobs.as<PairJob>() + at, js[b][g].data(), sizeof(PairJob) * js[b][g].size(),
                                        cudaMemcpyHostToDevice));
                 at += js[b][g].size();

@@ -264,6 +264,8 @@ struct Calculator {
             L.weighted = 1;
             L.wscale = wscale;
             L.dreg = 0;
+            L.inv_w = plan.inv_w;
+            pair_sqrt_prepare(plan.inv_w, nb);
             const size_t smem = pairhist_launch_smem(1, nb, true, tile);
             const int per_sm = pairhist_ctas_per_sm(smem, tile, false, true);
             const int grid = (int)std::min<long long>((long long)C.sm_count * per_sm, std::max<long long>(1, tiles[0]));

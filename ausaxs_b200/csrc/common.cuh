@@ -74,6 +74,20 @@ __host__ __device__ inline float pair_bin_limit(int nbins) {
     return kMagic + static_cast<float>(nbins < (1 << 22) ? nbins : (1 << 22));
 }
 
+// Square root by one Newton-Raphson correction of the hardware reciprocal-square-root approximation
+// (Markstein's formulation: d0 = s y, r = s - d0^2 exactly by an FMA, d = d0 + r y / 2).  It differs
+// from the correctly rounded root by at most one unit in the last place on a small fraction of
+// inputs; the pair kernel uses it only for bin widths at which an exhaustive device check
+// (pair_sqrt_prepare) found that no float input lands in another bin under either rounding rule of
+// the reference, so bins stay exact and the distance sums move by at most one ulp of a distance.
+__device__ __forceinline__ float pair_sqrt_nr(float s) {
+    float y;
+    asm("rsqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(fmaxf(s, 1.17549435e-38f)));  // finite at s = 0
+    const float d0 = __fmul_rn(s, y);
+    const float h = __fmul_rn(0.5f, y);
+    return __fmaf_rn(__fmaf_rn(-d0, d0, s), h, d0);
+}
+
 // Fixed-point in-bin offset of a pair: the distance is d = bin*c + r with |r| <= c/2 (1 + 2^-10)
 // (c = 1/inv_w rounded to float), r is stored as rint(r * scale) + kResBias in [0, 2^16) with
 // scale = 2^15 / c * (1 - 2^-8).  Sums of these are exact integers, so the per-bin mean distance

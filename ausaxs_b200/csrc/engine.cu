@@ -472,6 +472,7 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
     // shared memory they need.  Large structures: one launch per row class (1, T, T*T rows) so each
     // gets the occupancy its footprint allows; small ones: everything in one launch (launch latency
     // dominates).  Tiles are numbered per group.
+    pair_sqrt_prepare(P.inv_w, nb);  // once per width and process: the Newton-Raphson root where it bins exactly
     const bool split = P.pairs >= 2000000000LL;
     std::vector<PairJob> group_jobs[3];
     long long group_tiles[3] = {0, 0, 0};
@@ -502,6 +503,7 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
         L.weighted = w_launch;
         L.dreg = pairhist_dreg(group_rows[g], nb, w_launch, tile) ? 1 : 0;
         L.wscale = reinterpret_cast<const float*>(base + P.off_wscale);
+        L.inv_w = P.inv_w;
         AUSAXS_CUDA(cudaMemcpyAsync(base + job_off, group_jobs[g].data(), sizeof(PairJob) * group_jobs[g].size(),
                                     cudaMemcpyHostToDevice, C.stream));  // pageable: staged on return
         job_off += sizeof(PairJob) * group_jobs[g].size();

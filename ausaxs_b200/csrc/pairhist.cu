@@ -23,6 +23,10 @@
 //     (or before a 32-bit count could wrap), so the global traffic is one atomic per non-empty
 //     on-chip bin per flush instead of one per pair.
 // All accumulations are integer, so results do not depend on scheduling.
+#include <cstring>
+#include <map>
+#include <mutex>
+
 #include "pairhist.cuh"
 
 namespace ausaxs_b200 {
@@ -233,7 +237,7 @@ struct Outer {
 
 // The count and offset arrays are indexed with the bit pattern of the magic-rounded distance
 // (kMagic + bin), their base pointers shifted by -kMagicBits.
-template <bool GENERAL, bool WEIGHTED, int ROWS, int R>
+template <bool GENERAL, bool WEIGHTED, int ROWS, int R, bool NR>
 __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, const float4* s_pts, const Outer (&o)[R],
                                            int j0, int k0, int k1, bool diag, float wsc) {
     const float inv_w = J.inv_w, c = J.c, scale = J.scale;
@@ -260,7 +264,7 @@ __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, co
                 tail = j >= o[k].ts;
                 if (tail) s = __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
             }
-            const float d = __fsqrt_rn(s);
+            const float d = NR ? pair_sqrt_nr(s) : __fsqrt_rn(s);
             const float x = __fmul_rn(d, inv_w);
             // rint(x) by the magic number, ties to even; distances past the last bin (also NaN, inf
             // and x >= 2^22) are clamped to the overflow column
@@ -291,7 +295,7 @@ __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, co
     }
 }
 
-template <int NT, int R, bool WEIGHTED, bool DREG>
+template <int NT, int R, bool WEIGHTED, bool DREG, bool NR>
 __device__ __forceinline__ void run_segments(const PairJob& J, const Onchip& S, const float4* s_pts, const Outer (&o)[R],
                                              int j0, int jn, bool general, bool diag, float wsc,
                                              OffsetRegs<NT, DREG>& Rg) {
@@ -302,13 +306,13 @@ __device__ __forceinline__ void run_segments(const PairJob& J, const Onchip& S, 
     for (int k0 = 0; k0 < jn; k0 += drain_segment<TILE>()) {
         const int k1 = min(jn, k0 + drain_segment<TILE>());
         if (general) {
-            if (single) tile_pairs<true, WEIGHTED, kRowsSingle, R>(J, S, s_pts, o, j0, k0, k1, diag, wsc);
-            else if (offset_rows) tile_pairs<true, WEIGHTED, kRowsOffset, R>(J, S, s_pts, o, j0, k0, k1, diag, wsc);
-            else tile_pairs<true, WEIGHTED, kRowsGeneric, R>(J, S, s_pts, o, j0, k0, k1, diag, wsc);
+            if (single) tile_pairs<true, WEIGHTED, kRowsSingle, R, NR>(J, S, s_pts, o, j0, k0, k1, diag, wsc);
+            else if (offset_rows) tile_pairs<true, WEIGHTED, kRowsOffset, R, NR>(J, S, s_pts, o, j0, k0, k1, diag, wsc);
+            else tile_pairs<true, WEIGHTED, kRowsGeneric, R, NR>(J, S, s_pts, o, j0, k0, k1, diag, wsc);
         } else {
-            if (single) tile_pairs<false, WEIGHTED, kRowsSingle, R>(J, S, s_pts, o, j0, k0, k1, false, wsc);
-            else if (offset_rows) tile_pairs<false, WEIGHTED, kRowsOffset, R>(J, S, s_pts, o, j0, k0, k1, false, wsc);
-            else tile_pairs<false, WEIGHTED, kRowsGeneric, R>(J, S, s_pts, o, j0, k0, k1, false, wsc);
+            if (single) tile_pairs<false, WEIGHTED, kRowsSingle, R, NR>(J, S, s_pts, o, j0, k0, k1, false, wsc);
+            else if (offset_rows) tile_pairs<false, WEIGHTED, kRowsOffset, R, NR>(J, S, s_pts, o, j0, k0, k1, false, wsc);
+            else tile_pairs<false, WEIGHTED, kRowsGeneric, R, NR>(J, S, s_pts, o, j0, k0, k1, false, wsc);
         }
         if (J.dsum) {
             __syncthreads();
@@ -319,7 +323,7 @@ __device__ __forceinline__ void run_segments(const PairJob& J, const Onchip& S, 
 }
 
 // DREG: the u64 offset sums live in registers (one CTA per SM; pairhist_dreg decides)
-template <int NT, int R, bool WEIGHTED, bool DREG>
+template <int NT, int R, bool WEIGHTED, bool DREG, bool NR>
 __global__ void __launch_bounds__(NT, DREG ? 1 : (512 / NT > 1 ? 512 / NT : 1)) pairhist_kernel(PairLaunch L) {
     constexpr int TILE = NT * R;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -460,7 +464,7 @@ __global__ void __launch_bounds__(NT, DREG ? 1 : (512 / NT > 1 ? 512 / NT : 1)) 
         const bool has_tail = J.b_base + j0 + jn > J.tail_end - 3;  // scalar-tail partners: last 3 of a row
         const bool full = (ti + 1) * TILE <= J.na;
         const bool general = diag || has_tail || !full;
-        run_segments<NT, R, WEIGHTED, DREG>(J, S, s_pts, o, j0, jn, general, diag, wsc, Rg);
+        run_segments<NT, R, WEIGHTED, DREG, NR>(J, S, s_pts, o, j0, jn, general, diag, wsc, Rg);
         fence_proxy_async();  // this thread's accesses to the buffer before the next bulk copy into it
         __syncthreads();      // every thread is done with the buffer
         if (!prefetch && gn < L.total_tiles) issue(gn, buf);
@@ -474,24 +478,31 @@ __global__ void __launch_bounds__(NT, DREG ? 1 : (512 / NT > 1 ? 512 / NT : 1)) 
     }
 }
 
-template <int NT, int R, bool WEIGHTED, bool DREG>
+template <int NT, int R, bool WEIGHTED, bool DREG, bool NR>
 void launch_one(const PairLaunch& L, int grid, size_t smem, cudaStream_t s) {
-    cudaFuncSetAttribute(pairhist_kernel<NT, R, WEIGHTED, DREG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    pairhist_kernel<NT, R, WEIGHTED, DREG><<<grid, NT, smem, s>>>(L);
+    cudaFuncSetAttribute(pairhist_kernel<NT, R, WEIGHTED, DREG, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    pairhist_kernel<NT, R, WEIGHTED, DREG, NR><<<grid, NT, smem, s>>>(L);
+}
+
+template <int NT, bool WEIGHTED, bool DREG>
+void launch_nr(const PairLaunch& L, int grid, size_t smem, cudaStream_t s) {
+    if (L.nr_sqrt) launch_one<NT, kOuter, WEIGHTED, DREG, true>(L, grid, smem, s);
+    else launch_one<NT, kOuter, WEIGHTED, DREG, false>(L, grid, smem, s);
 }
 
 template <int TILE>
 void launch_tile(const PairLaunch& L, int grid, size_t smem, cudaStream_t s) {
     constexpr int NT = TILE / kOuter;
     // register-held offset sums exist for unweighted launches only (pairhist_dreg)
-    if (L.weighted) launch_one<NT, kOuter, true, false>(L, grid, smem, s);
-    else if (L.dreg) launch_one<NT, kOuter, false, true>(L, grid, smem, s);
-    else launch_one<NT, kOuter, false, false>(L, grid, smem, s);
+    if (L.weighted) launch_nr<NT, true, false>(L, grid, smem, s);
+    else if (L.dreg) launch_nr<NT, false, true>(L, grid, smem, s);
+    else launch_nr<NT, false, false>(L, grid, smem, s);
 }
 
 template <int NT, int R, bool WEIGHTED, bool DREG>
 int occupancy_one(size_t smem) {
-    auto k = pairhist_kernel<NT, R, WEIGHTED, DREG>;
+    // both root variants share the launch shape; the exact one bounds the registers
+    auto k = pairhist_kernel<NT, R, WEIGHTED, DREG, false>;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
         return 1;
@@ -501,6 +512,12 @@ int occupancy_one(size_t smem) {
         cudaGetLastError();
         return 1;
     }
+    auto k2 = pairhist_kernel<NT, R, WEIGHTED, DREG, true>;
+    int n2 = 0;
+    if (cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n2, k2, NT, smem) == cudaSuccess && n2 < n)
+        n = n2;
+    cudaGetLastError();
     return n > 0 ? n : 1;
 }
 
@@ -512,6 +529,27 @@ int occupancy_tile(size_t smem, bool weighted, bool dreg) {
     return occupancy_one<NT, kOuter, false, false>(smem);
 }
 
+// ---------------------------------------------------------------------------------------------
+// Verification of the Newton-Raphson root per inverse bin width (pair_sqrt_prepare)
+// ---------------------------------------------------------------------------------------------
+__global__ void sqrt_check_kernel(uint32_t hi_bits, float inv_w, unsigned long long* mismatches) {
+    unsigned long long bad = 0;
+    for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < hi_bits; b += (uint64_t)gridDim.x * blockDim.x) {
+        const float s = __uint_as_float(static_cast<uint32_t>(b));
+        const float xa = __fmul_rn(__fsqrt_rn(s), inv_w), xb = __fmul_rn(pair_sqrt_nr(s), inv_w);
+        // ties to even (the SIMD evaluators) and ties away from zero (the scalar tail)
+        if (rintf(xa) != rintf(xb) || roundf(xa) != roundf(xb)) ++bad;
+    }
+    for (int o = 16; o > 0; o >>= 1) bad += __shfl_xor_sync(0xffffffffu, bad, o);
+    if ((threadIdx.x & 31) == 0 && bad) atomicAdd(mismatches, bad);
+}
+
+struct SqrtVerified {
+    std::mutex m;
+    std::map<uint32_t, int> bins;  // inverse bin width (bits) -> bins verified (0: failed)
+};
+SqrtVerified g_sqrt;
+
 }  // namespace
 
 int pairhist_ctas_per_sm(size_t smem, int tile, bool dreg, bool weighted) {
@@ -520,8 +558,49 @@ int pairhist_ctas_per_sm(size_t smem, int tile, bool dreg, bool weighted) {
     return occupancy_tile<512>(smem, weighted, dreg);
 }
 
+bool pair_sqrt_prepare(float inv_w, int bins) {
+    if (!(inv_w > 0) || bins <= 0) return false;
+    const int want = bins < 8192 ? 8192 : bins;
+    uint32_t key;
+    std::memcpy(&key, &inv_w, 4);
+    {
+        std::lock_guard<std::mutex> lk(g_sqrt.m);
+        auto it = g_sqrt.bins.find(key);
+        if (it != g_sqrt.bins.end() && (it->second == 0 || it->second >= want)) return it->second >= bins;
+    }
+    // every float below the squared distance of bin want + 2 (the overflow clamp lies below it)
+    const double dmax = (want + 2.0) / inv_w;
+    const float s_max = static_cast<float>(dmax * dmax);
+    uint32_t hi;
+    std::memcpy(&hi, &s_max, 4);
+    unsigned long long* d = nullptr;
+    unsigned long long h = 1;
+    bool ok = false;
+    if (hi < 0x7f800000u && cudaMalloc(&d, sizeof(unsigned long long)) == cudaSuccess) {
+        if (cudaMemset(d, 0, sizeof(unsigned long long)) == cudaSuccess) {
+            sqrt_check_kernel<<<148 * 8, 256>>>(hi + 1, inv_w, d);
+            ok = cudaMemcpy(&h, d, sizeof(unsigned long long), cudaMemcpyDeviceToHost) == cudaSuccess && h == 0;
+        }
+        cudaFree(d);
+    }
+    cudaGetLastError();
+    std::lock_guard<std::mutex> lk(g_sqrt.m);
+    g_sqrt.bins[key] = ok ? want : 0;
+    return ok && want >= bins;
+}
+
 void pairhist_launch(const PairLaunch& L0, int tile, int grid, size_t smem, cudaStream_t s) {
     PairLaunch L = L0;
+    // the Newton-Raphson root where every job's width was verified for its bins (pair_sqrt_prepare)
+    L.nr_sqrt = 0;
+    {
+        // the jobs live in device memory; the launch's bins and the width recorded with them decide
+        std::lock_guard<std::mutex> lk(g_sqrt.m);
+        uint32_t key;
+        std::memcpy(&key, &L.inv_w, 4);
+        auto it = g_sqrt.bins.find(key);
+        L.nr_sqrt = (L.inv_w > 0 && it != g_sqrt.bins.end() && it->second >= L.smem_bins) ? 1 : 0;
+    }
     // double-buffered staging when the launch was given the room for it
     L.stages = smem >= pairhist_layout_bytes(L.smem_rows, L.smem_bins, L.weighted != 0, tile, L.dreg != 0, 2) ? 2 : 1;
     if (tile == 1024) launch_tile<1024>(L, grid, smem, s);

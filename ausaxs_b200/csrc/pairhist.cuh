@@ -61,6 +61,9 @@ struct PairLaunch {
     int32_t dreg;                   // u64 offset sums in registers instead of shared memory (pairhist_dreg)
     int32_t stages;                 // staging buffers of inner tiles (set by pairhist_launch from the
                                     // shared memory it is given: 2 = the next tile's copy overlaps)
+    float inv_w;                    // the inverse bin width every job of the launch shares (0: unknown)
+    int32_t nr_sqrt;                // 1: the Newton-Raphson root (pair_sqrt_nr), set by pairhist_launch for
+                                    // a width pair_sqrt_prepare verified (else the correctly rounded root)
     int32_t max_grabs;              // > 0: a CTA takes at most this many chunks and exits (the grid
                                     // must then cover the tiles: grid * max_grabs * chunk >= total);
                                     // bounded CTAs let the block scheduler interleave other launches
@@ -126,5 +129,12 @@ inline int pairhist_max_rows(int bins, bool weighted, int tile = 512) {
 }
 
 void pairhist_launch(const PairLaunch& L, int tile, int grid, size_t smem, cudaStream_t s);
+
+// Exhaustive device check, once per process and inverse bin width, that pair_sqrt_nr bins every float
+// squared distance below ((bins + 2) / inv_w)^2 exactly as the correctly rounded root does, under the
+// reference's ties-to-even rule and its scalar tail's ties-away rule (synchronises the device; call it
+// when planning, outside stream capture).  Launches over at most `bins` bins of a verified width then
+// take the Newton-Raphson root.  Returns whether the width is verified.
+bool pair_sqrt_prepare(float inv_w, int bins);
 
 }  // namespace ausaxs_b200

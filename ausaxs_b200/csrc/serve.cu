@@ -314,6 +314,7 @@ struct Assembly {
             Wk.L.overflow = P.dev.as<unsigned long long>(P.off_overflow);
             Wk.L.weighted = 0;
             Wk.L.wscale = nullptr;
+            Wk.L.inv_w = P.inv_w;
             Wk.L.jobs = reinterpret_cast<const PairJob*>(all_jobs.size());  // index, rebased below
             all_jobs.insert(all_jobs.end(), js[0].begin(), js[0].end());
             max_rows = std::max(max_rows, rows[0]);

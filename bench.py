@@ -69,16 +69,18 @@ def load_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
 
 
-def workload(name: str, subunit: int = 0, atoms: int = 0):
+def workload(name: str, subunit: int = 0, atoms: int = 0, structures: int = 0):
     """subunit (cfg2 only): atoms per icosahedral subunit; smaller shells keep the radius and bin count
-    of the full shell.  atoms (cfg1 only): a globule of the same composition and density.  Both are
-    profiling cases."""
+    of the full shell.  atoms (cfg1 only): a globule of the same composition and density.  structures
+    (cfg3 only): the first structures of the seeded batch.  All three are profiling cases."""
     from ausaxs_b200 import synth
 
     if name == "cfg2" and subunit:
         return synth.cfg2(subunit=subunit)
     if name == "cfg1" and atoms:
         return synth.cfg1(atoms=atoms)
+    if name == "cfg3" and structures:
+        return synth.cfg3(count=structures)
     return {"cfg0": synth.cfg0, "cfg1": synth.cfg1, "cfg2": synth.cfg2, "cfg3": synth.cfg3}[name]()
 
 
@@ -299,7 +301,7 @@ def run_batch(args, rank, world, local_rank):
     stream = torch.cuda.Stream(local_rank)
     ctx = _capi.Context(local_rank)
     ctx.set_stream(stream.cuda_stream)
-    wl = workload(args.workload)
+    wl = workload(args.workload, structures=args.structures)
     mols = wl.molecules
     n = len(mols)
     nq = len(wl.q)
@@ -660,6 +662,7 @@ def run_ours(args, rank, world, local_rank):
         launches = ctx.launches - launches0
         step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
         k_ms, k_n = ctx.kernel_time(0)
+        lat_ms, lat_n = ctx.kernel_time(6)
         ctx.enable_timing(False)
     total_ms = sum(step_ms)
     total_ms = max_over_ranks(total_ms, world)
@@ -704,16 +707,14 @@ def run_ours(args, rank, world, local_rank):
 
     peaks, peak_kind = load_peaks()
     kernel_ms = k_ms / args.steps  # all pair-kernel launches of one profile
-    pair_rate = pairs / (kernel_ms / 1e3)
+    # the grid dummies' self pairs go to the lattice kernel when it launched (class 6)
+    nx = len(m.exv) if (grid and m.exv is not None) else 0
+    lattice_pairs = nx * (nx - 1) // 2 if lat_n else 0
+    pair_rate = (pairs - lattice_pairs) / (kernel_ms / 1e3)
     clocks = clk.summary()
     sm_mhz = clocks.get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
     sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
-    # The pair kernel is bound by instruction issue (its inputs live in shared memory; DRAM traffic is
-    # ~16 MB per profile).  Issue peak: every SM sub-partition issues one warp instruction per cycle;
-    # INSTR_PER_PAIR thread instructions per pair evaluation were counted by ncu
-    # (smsp__inst_executed.sum x 32 / pairs, one-row launch of the FFGrid histograms; 39.9 on the
-    # cfg1-shaped 10k-atom case).
-    issue_peak = sms * 4 * sm_mhz * 1e6 * 32 / INSTR_PER_PAIR
+    atomic_rate, _ = _capi.smem_atomic_rate(local_rank, True)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -729,13 +730,14 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": int(nq * 8 + 8), "p50_ms": 1e3 * float(np.percentile(lat, 50)),
                 "p99_ms": 1e3 * float(np.percentile(lat, 99)), "max_rel_diff_vs_resident": e2e_match},
         "gpu_launches": int(launches),
-        "roofline": {"bound": "issue", "kernel": "pairhist_kernel", "achieved": pair_rate / 1e9,
-                     "peak": issue_peak / 1e9, "unit": "Gpair/s", "frac": pair_rate / issue_peak,
-                     "traffic": PAIR_TRAFFIC_BYTES if wl.name.startswith("cfg1:") else None,
-                     "peak_source": f"issue model: {sms} SMs x 4 x {sm_mhz:.0f} MHz x 32 / {INSTR_PER_PAIR} instr per pair",
-                     "kernel_ms_per_step": kernel_ms, "kernel_launches_per_step": k_n / args.steps,
-                     "hbm_frac": (PAIR_TRAFFIC_BYTES / (kernel_ms / 1e3)) / (peaks["hbm_gbs"] * 1e9),
-                     "note": "pair binning is bound by FP32 issue and shared-memory atomics, not HBM or tensor pipes"},
+        "roofline": dict(pair_roofline(pairs - lattice_pairs, kernel_ms, sm_mhz, sms, atomic_rate, 2, INSTR_PER_PAIR),
+                         traffic=None, kernel_launches_per_step=k_n / args.steps,
+                         note="pair evaluations of the pair kernel per second of its launches (the grid dummies' "
+                              "self pairs, when the lattice kernel takes them, are not counted)"),
+        "lattice": ({"kernel": "lattice_kernel", "ms_per_step": lat_ms / args.steps, "dummy_pairs": lattice_pairs,
+                     "pair_equivalent_per_s": lattice_pairs / (lat_ms / args.steps / 1e3) if lat_ms else None,
+                     "note": "the dummies' self pairs by the occupancy autocorrelation (integer popcounts); the "
+                             "accumulators equal the pair kernel's"} if lat_n else None),
         "clocks": clocks,
         "peaks_source": peak_kind,
     }
@@ -1478,6 +1480,8 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=0, help="serving: requests per load point (default 5 x chains)")
     ap.add_argument("--subunit", type=int, default=0, help="cfg2: atoms per subunit (default 8333; smaller for profiling)")
     ap.add_argument("--atoms", type=int, default=0, help="cfg1: atoms of the globule (default 50000; smaller for profiling)")
+    ap.add_argument("--structures", type=int, default=0,
+                    help="cfg3: the first structures of the seeded batch (default all 256; fewer for profiling)")
     ap.add_argument("--precision", type=int, default=2, choices=[0, 1, 2],
                     help="Debye transform: 0 tensor cores, 1 FP64, 2 automatic (tensor cores from 8e6 row x bin x q)")
     ap.add_argument("--tolerance", type=float, default=1e-4)
