@@ -111,6 +111,11 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
     return false;
 }
 
+// 32-bit add to a shared-memory word given by its shared-window byte address (no return value)
+__device__ __forceinline__ void shared_red_add(uint32_t addr, uint32_t v) {
+    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"(addr), "r"(v));
+}
+
 // On-chip privatised histograms of one CTA.
 //   counts   : u32 per (row, bin), one atomic per pair; column nbins of each row collects the pairs
 //              beyond the last bin (overflow), counted at the flush.
@@ -229,9 +234,11 @@ enum { kRowsSingle = 0, kRowsOffset = 1, kRowsGeneric = 2 };
 
 struct Outer {
     float4 a;
-    int i;        // index in the job's outer set
-    int cbase;    // count index of bin 0 in its row (kRowsSingle / kRowsOffset), or its row base (generic)
-    int ts;       // first inner index (local) that goes through the scalar evaluator
+    int i;           // index in the job's outer set
+    int cbase;       // count index of bin 0 in its row (kRowsSingle / kRowsOffset), or its row base (generic)
+    uint32_t caddr;  // kRowsSingle / kRowsOffset: shared byte address of its row's count of bin 0, less
+                     // 4 * kMagicBits (so that 4 * (bits of the magic-rounded distance) lands on the bin)
+    int ts;          // first inner index (local) that goes through the scalar evaluator
     bool active;
 };
 
@@ -247,7 +254,8 @@ __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, co
     const bool do_d = J.dsum != nullptr;
     const bool do_w = WEIGHTED && J.wsum != nullptr;
     uint32_t* const cnt = S.cnt - kMagicBits;
-    uint32_t* const dacc = S.dacc - kMagicBits;
+    // shared byte address of dacc[0] less 4 * kMagicBits (wrapping u32 arithmetic)
+    const uint32_t dacc_addr = smem_addr(S.dacc) - 4u * static_cast<uint32_t>(kMagicBits);
 #pragma unroll 2
     for (int jj = k0; jj < k1; ++jj) {
         const float4 b = s_pts[jj];
@@ -273,9 +281,10 @@ __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, co
                 xm = fminf(__fadd_rn(xm, 1.0f), bin_limit);  // std::round: ties away from zero
             const int xb = __float_as_int(xm);
             if (ROWS == kRowsSingle) {
-                atomicAdd(&cnt[xb], 1u);
+                shared_red_add(o[k].caddr + (static_cast<uint32_t>(xb) << 2), 1u);
             } else if (ROWS == kRowsOffset) {
-                atomicAdd(&cnt[o[k].cbase + __float_as_int(b.w) + xb], 1u);
+                // staged w: the inner point's row offset in bytes
+                shared_red_add(o[k].caddr + static_cast<uint32_t>(__float_as_int(b.w)) + (static_cast<uint32_t>(xb) << 2), 1u);
             } else {
                 // a row group: count the rows it keeps; the group with row 0 also carries the offset sums
                 const int row = pair_rows ? o[k].cbase + __float_as_int(b.w) : o[k].cbase;
@@ -284,7 +293,8 @@ __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, co
             if (do_d) {
                 const float r = __fmaf_rn(-__fsub_rn(xm, kMagic), c, d);
                 const float t = __fmaf_rn(r, scale, kMagic);  // rint(r * scale), one rounding
-                atomicAdd(&dacc[xb], static_cast<uint32_t>(__float_as_int(t) - kMagicBits + kResBias));
+                shared_red_add(dacc_addr + (static_cast<uint32_t>(xb) << 2),
+                               static_cast<uint32_t>(__float_as_int(t) - kMagicBits + kResBias));
             }
             if (do_w) {
                 const float wp = __fmul_rn(o[k].a.w, b.w);
@@ -437,6 +447,7 @@ __global__ void __launch_bounds__(NT, DREG ? 1 : (512 / NT > 1 ? 512 / NT : 1)) 
             const int ta = __float_as_int(o[k].a.w);
             const int rowbase = J.row_mode == kRowPair ? ta * J.types : (J.row_mode == kRowOuter ? ta : 0);
             o[k].cbase = single ? 0 : (offset_rows ? (rowbase - J.row_lo) * S.pad : rowbase);
+            o[k].caddr = smem_addr(S.cnt) + 4u * static_cast<uint32_t>(o[k].cbase) - 4u * static_cast<uint32_t>(kMagicBits);
             const int row_begin = J.tail_from_outer ? row_begin_base + o[k].i : 0;
             o[k].ts = J.tail_end - ((J.tail_end - row_begin) & 3) - J.b_base;
         }
@@ -453,7 +464,7 @@ __global__ void __launch_bounds__(NT, DREG ? 1 : (512 / NT > 1 ? 512 / NT : 1)) 
         float4* s_pts = stage0 + buf * stage_pitch;
         if (offset_rows && J.row_mode == kRowPair) {
             // row offset of the inner point for jobs with every row on chip
-            for (int k = threadIdx.x; k < jn; k += NT) s_pts[k].w = __int_as_float(__float_as_int(s_pts[k].w) * S.pad);
+            for (int k = threadIdx.x; k < jn; k += NT) s_pts[k].w = __int_as_float(__float_as_int(s_pts[k].w) * S.pad * 4);
             __syncthreads();
         } else if (offset_rows) {
             for (int k = threadIdx.x; k < jn; k += NT) s_pts[k].w = __int_as_float(0);
