@@ -41,9 +41,9 @@ INSTR_PER_PAIR = 39.8
 # DRAM bytes (read + write) of the three pair launches of one 50k-atom FFGrid profile: 3.12 MB measured
 # by ncu on the cfg1-shaped 10k-atom case (85,967 points), scaled by points to cfg1's 436,380
 PAIR_TRAFFIC_BYTES = 1.58e7
-# DRAM bytes (read + write) of the pair launches of one step of the 256-structure batch (ncu); None until
-# captured
-BATCH_PAIR_TRAFFIC_BYTES = None
+# DRAM bytes (read + write) of the pair launches of one step of the 256-structure batch: 16.6 MB per pass
+# measured by ncu on its first 64 structures (0.86M points), scaled by points to the batch's 3.66M
+BATCH_PAIR_TRAFFIC_BYTES = 7.0e7
 METRIC = "I(q) profiles/s & p99 latency vs plain GPU path at ≤1e-4 rel. I(q) error"
 UNIT = "profiles/s"
 
@@ -673,6 +673,12 @@ def run_ours(args, rank, world, local_rank):
     st.profile_device(cfg, q_dev, nq, _capi.DebyeParams(1.0, 1.0, 1.0, 0.0, 0.0, 1.0, 1, 1e-5), I_64)
     torch.cuda.synchronize()
     iq_dev_fp64 = float(np.max(np.abs(I_gpu / I_64.cpu().numpy() - 1)))
+    # the q values the timed transform evaluated in FP64 (the tensor-core path re-evaluates every q whose
+    # error bound exceeds the tolerance; the automatic choice takes FP64 for small transforms)
+    h_chk = mgr.calculate_all()
+    h_chk.precision, h_chk.tolerance = args.precision, args.tolerance
+    h_chk.debye_transform(wl.q)
+    fp64_q = ctx.fp64_columns()
 
     # end to end through the host C ABI with pinned buffers
     pin_a = torch.from_numpy(A).pin_memory()
@@ -723,7 +729,8 @@ def run_ours(args, rank, world, local_rank):
                    "exv": 0 if m.exv is None or not grid else len(m.exv), "pairs_per_profile": pairs,
                    "bin_width": wl.bin_width, "q_points": nq, "manager": wl.manager,
                    "transform": {"precision": args.precision, "tolerance": args.tolerance,
-                                 "max_rel_diff_vs_fp64_transform": iq_dev_fp64},
+                                 "max_rel_diff_vs_fp64_transform": iq_dev_fp64,
+                                 "fp64_q_fraction": fp64_q / nq},
                    "l2": "256 MiB buffer written between timed steps (outside the events)",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(A.nbytes + W.nbytes + (X.nbytes if grid else 0) + pin_q.numel() * 8),
