@@ -422,7 +422,8 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
         if (lsm <= kPairSmemCap) {
             use_lattice = true;
             P.lattice_smem = lsm;
-            const int per_sm = std::max(1, std::min(2048 / kLatticeThreads, (int)(233472 / (lsm + 1024))));
+            const int per_sm = std::max(1, std::min(2048 / (lattice_kernel_words(lat.G.words) <= 4 ? 1024 : kLatticeThreads),
+                                                    (int)(233472 / (lsm + 1024))));
             P.lattice_grid = C.sm_count * per_sm;
         }
     }

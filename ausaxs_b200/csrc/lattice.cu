@@ -147,8 +147,13 @@ __global__ void __launch_bounds__(1024) lattice_compact_kernel(const uint32_t* g
     if (threadIdx.x == 0) info[0] = s_base;
 }
 
+// threads per CTA: one CTA per SM holds the whole line store, so its warps are all the SM has
 template <int W>
-__global__ void __launch_bounds__(kLatticeThreads, 1) lattice_kernel(LatticeLaunch L) {
+constexpr int lattice_threads() { return W <= 4 ? 1024 : kLatticeThreads; }
+
+template <int W>
+__global__ void __launch_bounds__(lattice_threads<W>(), 1) lattice_kernel(LatticeLaunch L) {
+    constexpr int NTH = lattice_threads<W>();
     extern __shared__ __align__(16) unsigned char smem[];
     const int ly = L.G.ly, lz = L.G.lz, nb = L.nbins;
     uint32_t* s_lines = reinterpret_cast<uint32_t*>(smem);
@@ -159,12 +164,12 @@ __global__ void __launch_bounds__(kLatticeThreads, 1) lattice_kernel(LatticeLaun
     unsigned long long* h_ds = h_cnt + (nb + 1);                                     // [nb + 1]
     // the grid's line store has exactly `words` words per line; W may round it up (3 -> 4)
     const int gw = L.G.words;
-    for (int k = threadIdx.x; k < L.G.n_lines * W; k += kLatticeThreads) {
+    for (int k = threadIdx.x; k < L.G.n_lines * W; k += NTH) {
         const int line = k / W, w = k - line * W;
         s_lines[k] = w < gw ? L.G.lines[static_cast<size_t>(line) * gw + w] : 0u;
     }
-    for (int k = threadIdx.x; k < ly * lz; k += kLatticeThreads) s_table[k] = L.G.table[k];
-    for (int k = threadIdx.x; k < 2 * (nb + 1); k += kLatticeThreads) h_cnt[k] = 0ull;
+    for (int k = threadIdx.x; k < ly * lz; k += NTH) s_table[k] = L.G.table[k];
+    for (int k = threadIdx.x; k < 2 * (nb + 1); k += NTH) h_cnt[k] = 0ull;
     __syncthreads();
 
     const int lane = threadIdx.x & 31;
@@ -236,7 +241,7 @@ __global__ void __launch_bounds__(kLatticeThreads, 1) lattice_kernel(LatticeLaun
         }
     }
     __syncthreads();
-    for (int b = threadIdx.x; b < nb; b += kLatticeThreads) {
+    for (int b = threadIdx.x; b < nb; b += NTH) {
         if (h_cnt[b]) atomicAdd(&L.counts[b], h_cnt[b]);
         if (L.dsum && h_ds[b]) atomicAdd(&L.dsum[b], h_ds[b]);
     }
@@ -282,7 +287,7 @@ __global__ void lattice_tail_kernel(LatticeLaunch L) {
 template <int W>
 void launch_w(const LatticeLaunch& L, int grid, size_t smem, cudaStream_t s) {
     cudaFuncSetAttribute(lattice_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    lattice_kernel<W><<<grid, kLatticeThreads, smem, s>>>(L);
+    lattice_kernel<W><<<grid, lattice_threads<W>(), smem, s>>>(L);
 }
 
 }  // namespace

@@ -38,7 +38,7 @@ struct LatticeLaunch {
 // Points per set below which the pair kernel is used for lattice points as well.
 constexpr int kLatticeMinPoints = 1024;
 constexpr int kLatticeMaxWords = 8;   // lines of up to 256 lattice cells along x
-constexpr int kLatticeThreads = 512;
+constexpr int kLatticeThreads = 512;  // lines of more than 128 cells; up to 128: 1024 threads
 
 // Words per line of the kernel instantiation that serves a grid of `words` words (1, 2, 4 or 8).
 inline int lattice_kernel_words(int words) { return words <= 2 ? words : (words <= 4 ? 4 : 8); }

@@ -35,12 +35,9 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-# thread instructions per pair of the pair kernel and its DRAM bytes per profile, from an ncu capture
-# (--set full) of the three pair launches of the 50k-atom FFGrid profile
-INSTR_PER_PAIR = 39.8
-# DRAM bytes (read + write) of the three pair launches of one 50k-atom FFGrid profile: 3.12 MB measured
-# by ncu on the cfg1-shaped 10k-atom case (85,967 points), scaled by points to cfg1's 436,380
-PAIR_TRAFFIC_BYTES = 1.58e7
+# warp instructions per 32 pair evaluations of the pair kernel, counted by ncu on the batch's pair launches
+# (smsp__inst_executed / (shared atomics / 2), profiles/pairhist_kernel_batch_64_structures.md)
+INSTR_PER_PAIR = 34.5
 # DRAM bytes (read + write) of the pair launches of one step of the 256-structure batch: 16.6 MB per pass
 # measured by ncu on its first 64 structures (0.86M points), scaled by points to the batch's 3.66M
 BATCH_PAIR_TRAFFIC_BYTES = 7.0e7
