@@ -44,7 +44,7 @@ EXPORTED = [
     "ausaxs_gpu_calculator_result",
     "ausaxs_gpu_batch_create", "ausaxs_gpu_batch_destroy", "ausaxs_gpu_batch_autotune", "ausaxs_gpu_batch_candidate",
     "ausaxs_gpu_batch_profile_device", "ausaxs_gpu_batch_profile", "ausaxs_gpu_batch_pair_time",
-    "ausaxs_gpu_batch_histogram", "ausaxs_gpu_smem_atomic_rate",
+    "ausaxs_gpu_batch_histogram", "ausaxs_gpu_batch_set_points", "ausaxs_gpu_smem_atomic_rate",
     "ausaxs_gpu_server_create", "ausaxs_gpu_server_destroy", "ausaxs_gpu_server_admit", "ausaxs_gpu_server_release",
     "ausaxs_gpu_server_usage", "ausaxs_gpu_server_submit", "ausaxs_gpu_server_poll", "ausaxs_gpu_server_wait",
     "ausaxs_gpu_server_completed", "ausaxs_gpu_server_launch_count", "ausaxs_gpu_server_body_center", "ausaxs_gpu_server_coordinates", "ausaxs_gpu_server_histogram",
@@ -151,6 +151,7 @@ def load():
         L.ausaxs_gpu_batch_profile.argtypes = [vp, f64, C.c_int32, C.POINTER(DebyeParams), f64]
         L.ausaxs_gpu_batch_pair_time.argtypes = [vp, f64]
         L.ausaxs_gpu_batch_histogram.argtypes = [vp, C.c_int32, C.POINTER(HistResult)]
+        L.ausaxs_gpu_batch_set_points.argtypes = [vp, f32, f32, f64, C.c_int32]
         L.ausaxs_gpu_smem_atomic_rate.argtypes = [C.c_int32, C.c_int32, f64, f64]
         L.ausaxs_gpu_server_create.argtypes = [C.c_int32, C.c_int64, C.c_int32, C.c_int32, C.POINTER(vp)]
         L.ausaxs_gpu_server_destroy.argtypes = [vp]
@@ -596,6 +597,26 @@ class Batch:
         ms = C.c_double(0.0)
         check(load().ausaxs_gpu_batch_pair_time(self.h, C.byref(ms)))
         return ms.value
+
+    def set_points(self, atoms: list, waters: list, z_exv=None):
+        """New coordinates for every structure (same shapes and atom types as at creation) and, when
+        given, new excluded-volume charges; the next profile replays the captured graph on them."""
+        a = np.ascontiguousarray(np.concatenate([np.asarray(p, np.float32).reshape(-1, 4) for p in atoms])
+                                 if self._ao[-1] else np.zeros((1, 4), np.float32))
+        w = np.ascontiguousarray(np.concatenate([np.asarray(p, np.float32).reshape(-1, 4) for p in waters])
+                                 if self._wo[-1] else np.zeros((1, 4), np.float32))
+        if self._ao[-1] and a.shape != self._a.shape or self._wo[-1] and w.shape != self._w.shape:
+            raise AusaxsError(ERR_ARGUMENT, "set_points needs the creation shapes")
+        z = None if z_exv is None else np.ascontiguousarray(z_exv, np.float64)
+        if z is not None and z.shape != (self.n,):
+            raise AusaxsError(ERR_ARGUMENT, "z_exv needs one value per structure")
+        check(load().ausaxs_gpu_batch_set_points(self.h, fptr(a), fptr(w), dptr(z), 1))
+
+    def set_points_device(self, atoms_dev, waters_dev, z_exv=None):
+        """As set_points from device tensors in the creation layout (float32 [rows, 4]); asynchronous."""
+        z = None if z_exv is None else np.ascontiguousarray(z_exv, np.float64)
+        check(load().ausaxs_gpu_batch_set_points(self.h, devptr(atoms_dev, C.c_float), devptr(waters_dev, C.c_float),
+                                                 dptr(z), 0))
 
     def histogram(self, index: int, bin_count: int):
         bufs = {k: np.zeros(n) for k, n in [("aa", 225 * bin_count), ("aw", 15 * bin_count), ("ww", bin_count),

@@ -37,6 +37,51 @@ constexpr int kDefaultCandidate = 5;
 std::mutex g_tune_mutex;
 std::map<std::tuple<int, long long, int, int>, int> g_tuned;
 
+// One structure's destinations for new coordinates (ausaxs_gpu_batch_set_points): its atoms are rows
+// [a0, a0 + na) of the concatenated input, its waters rows [w0, w0 + nw).
+struct PointsItem {
+    long long a0, na, w0, nw;
+    float4* raw_a;
+    float4* dense_a;
+    float4* raw_w;
+};
+
+__device__ __forceinline__ bool finite3(const float4& v) { return isfinite(v.x) && isfinite(v.y) && isfinite(v.z); }
+
+// New x, y, z for every point of every structure (block row y: structure y, y + gridDim.y, ...).  An
+// atom keeps its form-factor type: one whose input type differs from it, or a point with a
+// non-finite coordinate, is left as it was and counted in *rejected, so the per-type counts of the
+// plans (and the type rows the pair kernel indexes) always hold.
+__global__ void set_points_kernel(const PointsItem* items, int n, const float4* atoms, const float4* waters,
+                                  unsigned long long* rejected) {
+    unsigned int bad = 0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long first = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int s = blockIdx.y; s < n; s += gridDim.y) {
+        const PointsItem it = items[s];
+        for (long long k = first; k < it.na; k += stride) {
+            const float4 v = atoms[it.a0 + k];
+            const float4 old = it.raw_a[k];
+            if (__float_as_int(v.w) != __float_as_int(old.w) || !finite3(v)) {
+                ++bad;
+                continue;
+            }
+            it.raw_a[k] = v;
+            const float dense_type = it.dense_a[k].w;
+            it.dense_a[k] = make_float4(v.x, v.y, v.z, dense_type);
+        }
+        for (long long k = first; k < it.nw; k += stride) {
+            const float4 v = waters[it.w0 + k];
+            if (!finite3(v)) {
+                ++bad;
+                continue;
+            }
+            it.raw_w[k] = make_float4(v.x, v.y, v.z, it.raw_w[k].w);
+        }
+    }
+    if (bad) atomicAdd(rejected, (unsigned long long)bad);
+}
+
 }  // namespace
 
 struct Batch {
@@ -54,7 +99,11 @@ struct Batch {
     };
     std::vector<Launch> launches;
     int choice = -1;
-    DevBuf jobs, misc, zero, fin, args;  // misc: tile counters [16], overflow at [16]
+    // misc: tile counters [0, 16), overflow [16] (set from [24] at the start of every profile),
+    // points rejected by the last set_points [24] (kept across profiles)
+    DevBuf jobs, misc, zero, fin, args;
+    std::vector<long long> a_off, w_off;  // creation offsets of the concatenated atoms and waters
+    DevBuf points_items, points_in;       // set_points: destinations, staged host input
     DevBuf d_stats;                      // census of every structure (creation only)
     DevBuf arena;                        // every structure's point arrays
     PrepStats* h_stats = nullptr;        // pinned slots owned by the context
@@ -88,6 +137,7 @@ struct Batch {
     }
 
     unsigned long long* overflow() const { return misc.as<unsigned long long>() + 16; }
+    unsigned long long* rejected() const { return misc.as<unsigned long long>() + 24; }
 
     void load(const ausaxs_hist_config& c, int n, const float* atoms, const int64_t* aoff, const float* waters,
               const int64_t* woff, const float* exv, const int64_t* xoff, const double* z_exv, bool host) {
@@ -112,6 +162,8 @@ struct Batch {
             arena_bytes += 2 * pts(na) + pts(nw) + pts(nx) + 256;
         }
         arena.ensure(arena_bytes);
+        a_off.assign(aoff, aoff + n + 1);
+        w_off.assign(woff, woff + n + 1);
         size_t at = 0;
         for (int i = 0; i < n; ++i) {
             const int64_t na = aoff[i + 1] - aoff[i], nw = woff[i + 1] - woff[i];
@@ -154,7 +206,10 @@ struct Batch {
             zr.push_back({P.dev.as<unsigned long long>(P.off_acc), (long long)(P.acc_bytes / 8)});
         }
         misc.ensure(256);
-        zr.push_back({misc.as<unsigned long long>(), 32});
+        AUSAXS_CUDA(cudaMemset(misc.p, 0, 256));
+        zr.push_back({misc.as<unsigned long long>(), 16});
+        zr.push_back({overflow(), 1, rejected()});  // rejected points poison every profile until replaced
+        zr.push_back({overflow() + 1, 7});
         n_zero = (int)zr.size();
         zero.ensure(sizeof(ZeroRange) * zr.size());
         AUSAXS_CUDA(cudaMemcpy(zero.p, zr.data(), sizeof(ZeroRange) * zr.size(), cudaMemcpyHostToDevice));
@@ -316,6 +371,68 @@ struct Batch {
         C.launches += 4 + (long long)launches.size();
     }
 
+    // New coordinates for every point, in the creation layout (rows aoff[i] .. aoff[i+1] of atoms,
+    // woff[i] .. woff[i+1] of waters), with every atom's form-factor type as at creation.  The plans,
+    // job tables and captured graph stay: bins were planned from the creation coordinates, so pairs
+    // that now lie beyond them show as bin overflow in the next profile.  Host input is staged with
+    // one copy per array; host calls synchronise and report rejected points.
+    // z_exv (host, may be null: kept) replaces the structures' excluded-volume charges per atom.
+    void set_points(const float* atoms, const float* waters, const double* z_exv, bool host) {
+        if (cfg.manager != AUSAXS_MANAGER_FFAVG)
+            throw Error{AUSAXS_ERR_ARGUMENT, "new coordinates need an FFAVG batch (FFGRID dummies follow the atoms)"};
+        Ctx& C = *ctx;
+        cudaStream_t s = C.stream;
+        const int n = (int)items.size();
+        const long long na = a_off[n] - a_off[0], nw = w_off[n] - w_off[0];
+        if ((na && !atoms) || (nw && !waters)) throw Error{AUSAXS_ERR_ARGUMENT, "null point array"};
+        if (!points_items.p) {
+            std::vector<PointsItem> v(n);
+            for (int i = 0; i < n; ++i) {
+                Structure& S = *items[i];
+                v[i] = {a_off[i] - a_off[0], S.n_a, w_off[i] - w_off[0], S.n_w,
+                        S.raw_a.as<float4>(), S.dense_a.as<float4>(), S.raw_w.as<float4>()};
+            }
+            points_items.ensure(sizeof(PointsItem) * n);
+            AUSAXS_CUDA(cudaMemcpy(points_items.p, v.data(), sizeof(PointsItem) * n, cudaMemcpyHostToDevice));
+        }
+        const float4* src_a = reinterpret_cast<const float4*>(atoms) + a_off[0];
+        const float4* src_w = reinterpret_cast<const float4*>(waters) + w_off[0];
+        if (host) {
+            points_in.ensure((size_t)std::max<long long>(1, na + nw) * 16);
+            float4* in = points_in.as<float4>();
+            if (na) AUSAXS_CUDA(cudaMemcpyAsync(in, src_a, (size_t)na * 16, cudaMemcpyHostToDevice, s));
+            if (nw) AUSAXS_CUDA(cudaMemcpyAsync(in + na, src_w, (size_t)nw * 16, cudaMemcpyHostToDevice, s));
+            src_a = in;
+            src_w = in + na;
+        }
+        if (z_exv) {
+            std::vector<FinalizeFF> fins;
+            for (int i = 0; i < n; ++i) {
+                if (!std::isfinite(z_exv[i])) throw Error{AUSAXS_ERR_ARGUMENT, "non-finite z_exv"};
+                cfgs[i].z_exv = z_exv[i];
+                items[i]->plan.fin_ff.z_exv = z_exv[i];
+                fins.push_back(items[i]->plan.fin_ff);
+            }
+            // pageable source: staged before the call returns, ordered after earlier replays on s
+            AUSAXS_CUDA(cudaMemcpyAsync(fin.p, fins.data(), sizeof(FinalizeFF) * n, cudaMemcpyHostToDevice, s));
+        }
+        AUSAXS_CUDA(cudaMemsetAsync(rejected(), 0, 8, s));
+        long long most = 1;
+        for (auto& S : items) most = std::max<long long>({most, (long long)S->n_a, (long long)S->n_w});
+        const dim3 grid((unsigned)std::min<long long>(64, (most + 1023) / 1024), (unsigned)std::min(n, 65535));
+        set_points_kernel<<<grid, 256, 0, s>>>(points_items.as<PointsItem>(), n, src_a, src_w, rejected());
+        C.check_launch("set_points");
+        if (host) {
+            unsigned long long bad = 0;
+            AUSAXS_CUDA(cudaMemcpyAsync(&bad, rejected(), 8, cudaMemcpyDeviceToHost, s));
+            AUSAXS_CUDA(cudaStreamSynchronize(s));
+            if (bad)
+                throw Error{AUSAXS_ERR_ARGUMENT, std::to_string(bad) +
+                                                     " points rejected: a form-factor type differs from the batch's or a "
+                                                     "coordinate is not finite"};
+        }
+    }
+
     // times every candidate's pair launches on this batch (best of 2 after a warm-up) and keeps the fastest
     int autotune(double* times_ms, int n_times) {
         Ctx& C = *ctx;
@@ -437,10 +554,25 @@ int ausaxs_gpu_batch_profile(ausaxs_gpu_batch* b, const double* q, int32_t n_q, 
         AUSAXS_CUDA(cudaMemcpyAsync(dq, q, (size_t)n_q * 8, cudaMemcpyHostToDevice, C.stream));
         B.profile_device(dq, n_q, *params, dI);
         AUSAXS_CUDA(cudaMemcpyAsync(Iq, dI, n * n_q * 8, cudaMemcpyDeviceToHost, C.stream));
-        unsigned long long overflow = 0;
-        AUSAXS_CUDA(cudaMemcpyAsync(&overflow, B.overflow(), 8, cudaMemcpyDeviceToHost, C.stream));
+        unsigned long long flags[2] = {0, 0};
+        AUSAXS_CUDA(cudaMemcpyAsync(&flags[0], B.overflow(), 8, cudaMemcpyDeviceToHost, C.stream));
+        AUSAXS_CUDA(cudaMemcpyAsync(&flags[1], B.rejected(), 8, cudaMemcpyDeviceToHost, C.stream));
         AUSAXS_CUDA(cudaStreamSynchronize(C.stream));
-        if (overflow) throw Error{AUSAXS_ERR_BIN_OVERFLOW, "pair distances beyond bin_count * bin_width; increase settings::axes::bin_count"};
+        if (flags[1])
+            throw Error{AUSAXS_ERR_ARGUMENT, "the last ausaxs_gpu_batch_set_points rejected points (changed form-factor "
+                                             "type or non-finite coordinate)"};
+        if (flags[0])
+            throw Error{AUSAXS_ERR_BIN_OVERFLOW, "pair distances beyond the batch's bins (bin_count * bin_width, or the "
+                                                 "range planned from the creation coordinates after set_points)"};
+    });
+}
+
+int ausaxs_gpu_batch_set_points(ausaxs_gpu_batch* b, const float* atoms, const float* waters, const double* z_exv,
+                                int32_t host_pointers) {
+    return guarded([&] {
+        if (!b) throw Error{AUSAXS_ERR_ARGUMENT, "null batch"};
+        AUSAXS_CUDA(cudaSetDevice(b->impl.ctx->device));
+        b->impl.set_points(atoms, waters, z_exv, host_pointers != 0);
     });
 }
 

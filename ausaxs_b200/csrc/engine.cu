@@ -179,7 +179,7 @@ namespace {
 __global__ void zero_ranges_kernel(const ZeroRange* ranges) {
     const ZeroRange r = ranges[blockIdx.y];
     for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < r.words; k += (long long)gridDim.x * blockDim.x)
-        r.p[k] = 0;
+        r.p[k] = r.src ? r.src[k] : 0ull;
 }
 }  // namespace
 

@@ -195,10 +195,12 @@ struct Ctx {
 void append_pair_jobs(const Plan& P, int tile, bool by_class, std::vector<PairJob> (&jobs)[3], long long (&tiles)[3],
                       int (&rows)[3], int max_rows = 0, bool skip_lattice = false);
 
-// Clears n device ranges of u64 words in one launch (table in device memory).
+// Clears n device ranges of u64 words in one launch (table in device memory); a range with a
+// source is set to the source's words instead.
 struct ZeroRange {
     unsigned long long* p;
     long long words;
+    const unsigned long long* src = nullptr;
 };
 void zero_ranges_launch(const ZeroRange* ranges_dev, int n, cudaStream_t s);
 

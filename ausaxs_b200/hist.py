@@ -531,6 +531,20 @@ class BatchedProfiles:
     def autotune(self):
         return self._b.autotune()
 
+    def set_molecules(self, molecules: Sequence[Molecule]):
+        """Replace every molecule by one with the same atoms and waters in new positions (a new
+        conformation or pose; FFAvg batches): the plans and captured graph are kept, the excluded-volume
+        charges follow the new volumes."""
+        if self.grid:
+            raise _capi.AusaxsError(_capi.ERR_ARGUMENT, "new positions need an FFAvg batch")
+        molecules = list(molecules)
+        if len(molecules) != len(self.molecules):
+            raise _capi.AusaxsError(_capi.ERR_ARGUMENT, "set_molecules needs one molecule per structure")
+        parts = [m.compact_ff() for m in molecules]
+        z = [m.get_volume_grid() * RHO_WATER / m.size_atom() if m.size_atom() else 0.0 for m in molecules]
+        self._b.set_points([p[0] for p in parts], [p[1] for p in parts], z)
+        self.molecules = molecules
+
     def debye_transform(self, q=None, cw=1.0, cx=1.0, crho=1.0, dw_atomic=0.0, dw_exv=0.0, grid_width=1.0):
         """[n][nq] I(q) of every molecule (FP64 transform)."""
         q = default_q_axis() if q is None else np.ascontiguousarray(q, np.float64)

@@ -233,6 +233,16 @@ AUSAXS_API int ausaxs_gpu_structure_histogram(ausaxs_gpu_ctx* ctx, ausaxs_gpu_st
  *   pair launch) of the last profile, from events recorded inside the captured graph (waits for it).
  * ausaxs_gpu_batch_histogram: structure `index`'s histograms from the last profile, as
  *   ausaxs_gpu_structure_histogram.
+ * ausaxs_gpu_batch_set_points (FFAVG batches): new x, y, z for every atom and water, in the creation
+ *   layout (same offsets, so the same arrays' shapes); each atom's form-factor type must be the one it
+ *   was created with; z_exv (host, n_structures values, may be null: kept) replaces the FFAVG
+ *   excluded-volume charges.  Plans, job tables and the captured graph are kept, so the next profile is one
+ *   graph replay.  Bins stay those planned from the creation coordinates: a pair that now lies beyond
+ *   them is a bin overflow (error from ausaxs_gpu_batch_profile, NaN from _profile_device; create the
+ *   batch again).  A point whose type changed or that has a non-finite coordinate is left as it was
+ *   and counted: host_pointers = 1 synchronises and fails with AUSAXS_ERR_ARGUMENT, and every later
+ *   profile fails (or is NaN) until a set_points call without rejections.  host_pointers = 0 reads
+ *   device arrays and does not synchronise.
  */
 typedef struct ausaxs_gpu_batch ausaxs_gpu_batch;
 
@@ -250,6 +260,8 @@ AUSAXS_API int ausaxs_gpu_batch_profile(ausaxs_gpu_batch* b, const double* q, in
                                         const ausaxs_debye_params* params, double* Iq);
 AUSAXS_API int ausaxs_gpu_batch_pair_time(ausaxs_gpu_batch* b, double* ms);
 AUSAXS_API int ausaxs_gpu_batch_histogram(ausaxs_gpu_batch* b, int32_t index, ausaxs_hist_result* out);
+AUSAXS_API int ausaxs_gpu_batch_set_points(ausaxs_gpu_batch* b, const float* atoms, const float* waters,
+                                           const double* z_exv, int32_t host_pointers);
 
 /*
  * Fit of one free parameter of a composite histogram to measured data: fitter::SmartFitter::fit()

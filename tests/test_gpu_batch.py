@@ -86,3 +86,103 @@ def test_batch_rejects_simple_manager(gpu_ctx):
     a = np.zeros((3, 4), np.float32)
     with pytest.raises(_capi.AusaxsError):
         _capi.Batch(gpu_ctx, cfg, [a], [np.zeros((0, 4), np.float32)])
+
+
+def _moved(mols, seed, scale=0.97, jitter=0.05, volume_scale=0.9):
+    """Same atoms (types, order) and waters in new positions: a rotation about the centroid, a
+    shrink (pair distances stay inside the bins planned for the originals) and a small jitter."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for m in mols:
+        q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+        c = m.atoms.mean(axis=0) if len(m.atoms) else np.zeros(3)
+        mv = lambda p: (((p - c) @ q.T) * scale + c + rng.uniform(-jitter, jitter, p.shape)) if len(p) else p
+        out.append(hist.Molecule(atoms=mv(m.atoms), ff_types=m.ff_types.copy(), waters=mv(m.waters),
+                                 volume=m.volume * volume_scale))
+    return out
+
+
+def test_set_points_equals_a_new_batch(gpu_ctx):
+    mols = _molecules(300, SIZES)
+    q = np.linspace(0.005, 0.8, 400)
+    B = hist.BatchedProfiles(mols, bin_width=0.25, ctx=gpu_ctx)
+    I0 = B.debye_transform(q, cw=1.1, cx=0.95)
+    for k in range(2):  # two successive replacements, each a replay of the same graph
+        new = _moved(mols, 77 + k)
+        B.set_molecules(new)
+        I = B.debye_transform(q, cw=1.1, cx=0.95)
+        F = hist.BatchedProfiles(new, bin_width=0.25, ctx=gpu_ctx)
+        If = F.debye_transform(q, cw=1.1, cx=0.95)
+        np.testing.assert_allclose(I, If, rtol=1e-13, atol=0)
+        for i in range(len(new)):
+            b, f = B.histogram(i), F.histogram(i)
+            assert b["max_bin"] == f["max_bin"]
+            np.testing.assert_array_equal(b["aa"], f["aa"])
+            np.testing.assert_array_equal(b["aw"], f["aw"])
+            np.testing.assert_array_equal(b["ww"], f["ww"])
+            np.testing.assert_array_equal(b["d_axis"], f["d_axis"])
+        F.close()
+        assert np.max(np.abs(I / I0 - 1)) > 1e-6  # the profiles did change
+    # and against the oracle for the small ones
+    for i, m in enumerate(new[:6]):
+        A, W, _ = m.compact_ff()
+        o = O.hist_ff(0, A, W, None, 0.25, 8000, m.volume * 0.334 / m.size_atom())
+        Io, _ = O.debye_ff(0, o, q, cw=1.1, cx=0.95)
+        np.testing.assert_allclose(I[i], Io, rtol=1e-6)
+    B.close()
+
+
+def test_set_points_rejections_and_recovery(gpu_ctx):
+    mols = _molecules(500, [400, 1300, 90])
+    q = np.linspace(0.005, 0.5, 100)
+    B = hist.BatchedProfiles(mols, bin_width=0.25, ctx=gpu_ctx)
+    I0 = B.debye_transform(q)
+    parts = [m.compact_ff() for m in mols]
+    atoms = [p[0].copy() for p in parts]
+    waters = [p[1].copy() for p in parts]
+    bad = [a.copy() for a in atoms]
+    t = bad[1][5, 3].view(np.int32)
+    bad[1][5, 3] = np.array([3 if t != 3 else 7], np.int32).view(np.float32)[0]  # another form-factor type
+    with pytest.raises(_capi.AusaxsError) as e:
+        B._b.set_points(bad, waters)
+    assert e.value.code == _capi.ERR_ARGUMENT
+    with pytest.raises(_capi.AusaxsError) as e:  # every profile fails until valid points arrive
+        B.debye_transform(q)
+    assert e.value.code == _capi.ERR_ARGUMENT
+    wbad = [w.copy() for w in waters]
+    wbad[0][3, 1] = np.nan
+    with pytest.raises(_capi.AusaxsError):
+        B._b.set_points(atoms, wbad)
+    B._b.set_points(atoms, waters)
+    np.testing.assert_array_equal(B.debye_transform(q), I0)
+    # a structure grown beyond the bins planned for it: bin overflow, then recovery
+    grown = [a.copy() for a in atoms]
+    grown[2][:, :3] *= 3.0
+    B._b.set_points(grown, waters)
+    with pytest.raises(_capi.AusaxsError) as e:
+        B.debye_transform(q)
+    assert e.value.code == _capi.ERR_BIN_OVERFLOW
+    B._b.set_points(atoms, waters)
+    np.testing.assert_array_equal(B.debye_transform(q), I0)
+    with pytest.raises(_capi.AusaxsError):
+        B._b.set_points(atoms[:2], waters)  # not the creation shapes
+    B.close()
+
+
+def test_set_points_device_arrays(gpu_ctx):
+    import torch
+
+    mols = _molecules(600, [700, 2100])
+    q = np.linspace(0.005, 0.5, 100)
+    B = hist.BatchedProfiles(mols, bin_width=0.25, ctx=gpu_ctx)
+    B.debye_transform(q)
+    new = _moved(mols, 5, volume_scale=1.0)
+    parts = [m.compact_ff() for m in new]
+    a = torch.from_numpy(np.concatenate([p[0] for p in parts])).cuda()
+    w = torch.from_numpy(np.concatenate([p[1] for p in parts])).cuda()
+    torch.cuda.synchronize()
+    B._b.set_points_device(a, w)
+    I = B.debye_transform(q)
+    If = hist.BatchedProfiles(new, bin_width=0.25, ctx=gpu_ctx).debye_transform(q)
+    np.testing.assert_allclose(I, If, rtol=1e-13, atol=0)
+    B.close()
