@@ -39,8 +39,9 @@ __constant__ FormFactor5 c_ff[kNff] = {
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kRhoWater = 0.334;        // e / A^3 (include/core/constants/Constants.h:114)
 constexpr double kAvgRadius = 1.62;        // A (Constants.h:90)
-constexpr int kChunk = 512;
+constexpr int kChunk = 128;   // bins per sinc chunk
 constexpr int kThreads = 256;
+constexpr int kQB = kThreads / 32;  // q values per CTA: one warp each
 constexpr int kMaxRows = 264;
 
 // Excluded volume (A^3) per form_factor_t for explicit excluded volume: the reference's default set
@@ -128,48 +129,51 @@ __device__ RowTerms row_terms(const DebyeArgs& A, const RowDesc& r, const QFacto
     return t;
 }
 
-__device__ void debye_body(const DebyeArgs& A, const int k) {
-    if (k >= A.nq) return;
-    const double q = A.q[k];
+// One CTA evaluates kQB consecutive q values of one transform; warp w owns q0 + w for the per-q work
+// (form factors, the tensor-core check, the profile assembly) and all warps share the FP64 sums.
+__device__ void debye_qblock(const DebyeArgs& A, const int q0) {
+    const int nqb = min(kQB, A.nq - q0);
+    if (nqb <= 0) return;
     const int R = A.R;
     const int mb = *A.max_bin;
-    __shared__ double s_sinc[3][kChunk];
-    __shared__ double s_acc[kMaxRows];
-    __shared__ QFactors s_F;
-    __shared__ int s_fp64;
+    __shared__ double s_sinc[kQB][3][kChunk];
+    __shared__ double s_acc[kQB][kMaxRows];
+    __shared__ QFactors s_F[kQB];
+    __shared__ int s_fp64[kQB];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = kThreads >> 5;
 
-    if (threadIdx.x < kNff) s_F.f[threadIdx.x] = ff_raw(threadIdx.x, q);
-    if (threadIdx.x >= 64 && threadIdx.x < 64 + kNff) {
-        // ExvFormFactor(V).evaluate(q) = V rho_w exp(-V^(2/3)/(4 pi) q^2) (ExvFormFactor.h:20-33)
-        const double v = c_exv_volume[threadIdx.x - 64];
-        s_F.xe[threadIdx.x - 64] = v * kRhoWater * exp(-(pow(v, 2.0 / 3) / (4 * kPi)) * q * q);
-    }
-    if (threadIdx.x == 96) {
-        const double rm2 = kAvgRadius * kAvgRadius / 4;  // exv_factor (CompositeDistanceHistogramFFExplicitBase.cpp:54-57)
-        s_F.e = pow(A.cx, 3) * exp(-rm2 * (pow(A.cx, 2) - 1) * q * q);
-    }
-    if (threadIdx.x == 32) {
-        if (A.exv_model == 1) {
-            double e = pow(A.grid_volume, 2.0 / 3) / (4 * kPi);  // ExvFormFactor (ExvFormFactor.h:20-33)
-            s_F.fx = A.grid_volume * kRhoWater * exp(-e * q * q);
-        } else {
-            s_F.fx = ff_raw(kExv, q);
+    // per-q factors: lane j of warp qi computes one of them (a handful of exp each)
+    if (warp < nqb) {
+        const double q = A.q[q0 + warp];
+        QFactors& F = s_F[warp];
+        if (lane < kNff) {
+            F.f[lane] = ff_raw(lane, q);
+        } else if (lane < 2 * kNff) {
+            // ExvFormFactor(V).evaluate(q) = V rho_w exp(-V^(2/3)/(4 pi) q^2) (ExvFormFactor.h:20-33)
+            const double v = c_exv_volume[lane - kNff];
+            F.xe[lane - kNff] = v * kRhoWater * exp(-(pow(v, 2.0 / 3) / (4 * kPi)) * q * q);
+        } else if (lane == 2 * kNff) {
+            const double rm2 = kAvgRadius * kAvgRadius / 4;  // exv_factor (CompositeDistanceHistogramFFExplicitBase.cpp:54-57)
+            F.e = pow(A.cx, 3) * exp(-rm2 * (pow(A.cx, 2) - 1) * q * q);
+            if (A.exv_model == 1) {
+                const double e = pow(A.grid_volume, 2.0 / 3) / (4 * kPi);  // ExvFormFactor (ExvFormFactor.h:20-33)
+                F.fx = A.grid_volume * kRhoWater * exp(-e * q * q);
+            } else {
+                F.fx = ff_raw(kExv, q);
+            }
+        } else if (lane == 2 * kNff + 1) {
+            F.ba = (A.dw_atomic != 0 || A.dw_exv != 0) ? exp(-q * q * A.dw_atomic * A.dw_atomic * 0.5) : 1.0;
+            F.bx = (A.dw_atomic != 0 || A.dw_exv != 0) ? exp(-q * q * A.dw_exv * A.dw_exv * 0.5) : 1.0;
+            F.eq2 = exp(-q * q);
+            s_fp64[warp] = 1;
+            if (A.tc_err_est) A.tc_err_est[q0 + warp] = INFINITY;  // overwritten below when tensor-core values exist
         }
-        s_F.ba = (A.dw_atomic != 0 || A.dw_exv != 0) ? exp(-q * q * A.dw_atomic * A.dw_atomic * 0.5) : 1.0;
-        s_F.bx = (A.dw_atomic != 0 || A.dw_exv != 0) ? exp(-q * q * A.dw_exv * A.dw_exv * 0.5) : 1.0;
-        s_F.eq2 = exp(-q * q);
     }
-    for (int r = threadIdx.x; r < R; r += kThreads) s_acc[r] = 0;
+    for (int i = threadIdx.x; i < kQB * kMaxRows; i += kThreads) (&s_acc[0][0])[i] = 0;
     __syncthreads();
 
-    // With tensor-core values: keep this q unless the estimated error is above tolerance.
-    if (threadIdx.x == 0) {
-        s_fp64 = 1;
-        if (A.tc_err_est) A.tc_err_est[k] = INFINITY;  // overwritten below when tensor-core values exist
-    }
-    __syncthreads();
-    if (A.sinqd_tc && !(A.tc_error && *A.tc_error) && warp == 0) {
+    // With tensor-core values: keep a q unless its estimated error is above tolerance.
+    if (A.sinqd_tc && !(A.tc_error && *A.tc_error) && warp < nqb) {
         // Error bound of the tensor-core values, per row: c_rel * sum_b |H||S| + c_abs * sum_b |H|.
         //  * c_rel, operand representation: H to FP32 (2^-24), FP32 sinc value (sinf 2 ulp, the
         //    division 2^-24), the BF16 products dropped by the split (< 2^-25), the main+correction
@@ -180,20 +184,21 @@ __device__ void debye_body(const DebyeArgs& A, const int k) {
         //  * c_abs: the FP32 argument q*d carries 3 roundings, i.e. |dx| <= 3 * 2^-24 x, and
         //    |d sinc/dx| <= 2/x, so |d sinc| <= 1.5 * 2^-22 for every x;
         //  * 10 % slack for the FP32 bound and row sums themselves.
+        const int k = q0 + warp;
         const int per = debye_tc_split_bins(mb, A.tc_splits);
         const double c_rel = (0x1p-21 + (per / 16 + 1) * 0x1p-22) * 1.1;
         const double c_abs = 0x1p-21 * 1.1;
         const size_t plane = static_cast<size_t>(R) * A.nq;
         double I = 0, err = 0;
         for (int r = lane; r < R; r += 32) {
-            const double cf = row_terms(A, A.rows[r], s_F).in_I;
+            const double cf = row_terms(A, A.rows[r], s_F[warp]).in_I;
             double v = 0, bnd = 0, ha = 0;
             for (int z = 0; z < A.tc_splits; ++z) {
                 v += A.sinqd_tc[z * plane + static_cast<size_t>(r) * A.nq + k];
                 bnd += A.bound_tc[z * plane + static_cast<size_t>(r) * A.nq + k];
                 ha += A.habs_tc[static_cast<size_t>(z) * R + r];
             }
-            s_acc[r] = v;
+            s_acc[warp][r] = v;
             I += cf * v;
             err += fabs(cf) * (c_rel * bnd + c_abs * ha);
         }
@@ -203,43 +208,54 @@ __device__ void debye_body(const DebyeArgs& A, const int k) {
         }
         if (lane == 0) {
             bool ok = err <= A.tolerance * fabs(I);
-            s_fp64 = ok ? 0 : 1;
+            s_fp64[warp] = ok ? 0 : 1;
             if (!ok && A.fp64_columns) atomicAdd(A.fp64_columns, 1);
             if (A.tc_err_est) A.tc_err_est[k] = fabs(I) > 0 ? err / fabs(I) : INFINITY;
         }
     }
     __syncthreads();
 
-    if (s_fp64) {
-        for (int r = threadIdx.x; r < R; r += kThreads) s_acc[r] = 0;
-        __syncthreads();
+    int any = 0;
+    for (int qi = 0; qi < nqb; ++qi) any |= s_fp64[qi];
+    if (any) {
+        for (int i = threadIdx.x; i < nqb * R; i += kThreads)
+            if (s_fp64[i / R]) s_acc[i / R][i % R] = 0;
         int used_groups = 1;
         for (int r = 0; r < R; ++r) used_groups = max(used_groups, A.rows[r].group + 1);
+        __syncthreads();
         for (int c0 = 0; c0 < mb; c0 += kChunk) {
             const int cn = min(kChunk, mb - c0);
-            for (int t = threadIdx.x; t < cn; t += kThreads) {
-                s_sinc[0][t] = sinc64(q * A.axis0[c0 + t]);
-                if (used_groups > 1) s_sinc[1][t] = sinc64(q * A.axis1[c0 + t]);
-                if (used_groups > 2) s_sinc[2][t] = sinc64(q * A.axis2[c0 + t]);
+            for (int i = threadIdx.x; i < nqb * cn; i += kThreads) {
+                const int qi = i / cn, t = i - qi * cn;
+                if (!s_fp64[qi]) continue;
+                const double q = A.q[q0 + qi];
+                s_sinc[qi][0][t] = sinc64(q * A.axis0[c0 + t]);
+                if (used_groups > 1) s_sinc[qi][1][t] = sinc64(q * A.axis1[c0 + t]);
+                if (used_groups > 2) s_sinc[qi][2][t] = sinc64(q * A.axis2[c0 + t]);
             }
             __syncthreads();
-            for (int r = warp; r < R; r += nwarps) {
+            // (row, q) sums: lanes stride the chunk's bins, then a shuffle tree; chunk partials are
+            // added in bin order, so every transform of the same rows gives the same bits
+            for (int p = warp; p < R * nqb; p += nwarps) {
+                const int r = p / nqb, qi = p - r * nqb;
+                if (!s_fp64[qi]) continue;
                 const double* h = A.H + static_cast<size_t>(r) * A.nb + c0;
-                const double* s = s_sinc[A.rows[r].group];
+                const double* sv = s_sinc[qi][A.rows[r].group];
                 double acc = 0;
-                for (int t = lane; t < cn; t += 32) acc += h[t] * s[t];
+                for (int t = lane; t < cn; t += 32) acc += h[t] * sv[t];
                 for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-                if (lane == 0) s_acc[r] += acc;
+                if (lane == 0) s_acc[qi][r] += acc;
             }
             __syncthreads();
         }
     }
 
-    if (warp == 0) {
+    if (warp < nqb) {
+        const int k = q0 + warp;
         double prof[6] = {0, 0, 0, 0, 0, 0};
         for (int r = lane; r < R; r += 32) {
-            const RowTerms t = row_terms(A, A.rows[r], s_F);
-            for (int k2 = 0; k2 < t.n; ++k2) prof[t.p[k2]] += t.cf[k2] * s_acc[r];
+            const RowTerms t = row_terms(A, A.rows[r], s_F[warp]);
+            for (int k2 = 0; k2 < t.n; ++k2) prof[t.p[k2]] += t.cf[k2] * s_acc[warp][r];
         }
         for (int p = 0; p < 6; ++p)
             for (int o = 16; o > 0; o >>= 1) prof[p] += __shfl_xor_sync(0xffffffffu, prof[p], o);
@@ -264,15 +280,19 @@ __device__ void debye_body(const DebyeArgs& A, const int k) {
     }
 }
 
-__global__ void __launch_bounds__(kThreads) debye_kernel(DebyeArgs A) { debye_body(A, blockIdx.x); }
+__global__ void __launch_bounds__(kThreads) debye_kernel(DebyeArgs A) { debye_qblock(A, blockIdx.x * kQB); }
 // batched: blockIdx.y selects the structure
-__global__ void __launch_bounds__(kThreads) debye_batch_kernel(const DebyeArgs* As) { debye_body(As[blockIdx.y], blockIdx.x); }
+__global__ void __launch_bounds__(kThreads) debye_batch_kernel(const DebyeArgs* As) {
+    debye_qblock(As[blockIdx.y], blockIdx.x * kQB);
+}
 
 }  // namespace
 
-void debye_fp64_launch(const DebyeArgs& A, cudaStream_t s) { debye_kernel<<<A.nq, kThreads, 0, s>>>(A); }
+void debye_fp64_launch(const DebyeArgs& A, cudaStream_t s) {
+    debye_kernel<<<(A.nq + kQB - 1) / kQB, kThreads, 0, s>>>(A);
+}
 void debye_fp64_batch_launch(const DebyeArgs* As_dev, int n, int max_nq, cudaStream_t s) {
-    debye_batch_kernel<<<dim3(max_nq, n), kThreads, 0, s>>>(As_dev);
+    debye_batch_kernel<<<dim3((max_nq + kQB - 1) / kQB, n), kThreads, 0, s>>>(As_dev);
 }
 
 }  // namespace ausaxs_b200
