@@ -317,7 +317,9 @@ struct Batch {
         AUSAXS_CUDA(cudaEventRecordWithFlags(pair_t1, s, cudaEventRecordExternal));
         ff_finalize_batch_launch(fin.as<FinalizeFF>(), (int)items.size(), max_nb, s);
         ctx->check_launch("finalize");
-        debye_fp64_batch_launch(args.as<DebyeArgs>(), (int)items.size(), nq, s);
+        int max_R = 1;
+        for (auto& S : items) max_R = std::max(max_R, S->plan.R);
+        debye_fp64_batch_launch(args.as<DebyeArgs>(), (int)items.size(), nq, max_R, s);
         ctx->check_launch("debye");
     }
 

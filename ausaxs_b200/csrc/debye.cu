@@ -39,9 +39,14 @@ __constant__ FormFactor5 c_ff[kNff] = {
 constexpr double kPi = 3.14159265358979323846;
 constexpr double kRhoWater = 0.334;        // e / A^3 (include/core/constants/Constants.h:114)
 constexpr double kAvgRadius = 1.62;        // A (Constants.h:90)
-constexpr int kChunk = 128;   // bins per sinc chunk
 constexpr int kThreads = 256;
-constexpr int kQB = kThreads / 32;  // q values per CTA: one warp each
+constexpr int kWarps = kThreads / 32;
+constexpr int kQT = 16;                        // q values per CTA
+constexpr int kSubs = 32 / kQT;                // bin phases per warp
+constexpr int kPhases = kThreads / kQT;        // bin phases per CTA
+constexpr int kBinsPerThread = 8;              // bins of one phase per chunk
+constexpr int kCB = kPhases * kBinsPerThread;  // bins per chunk
+constexpr int kRG = 32;                        // rows per group of register accumulators
 constexpr int kMaxRows = 264;
 
 // Excluded volume (A^3) per form_factor_t for explicit excluded volume: the reference's default set
@@ -129,30 +134,42 @@ __device__ RowTerms row_terms(const DebyeArgs& A, const RowDesc& r, const QFacto
     return t;
 }
 
-// One CTA evaluates kQB consecutive q values of one transform; warp w owns q0 + w for the per-q work
-// (form factors, the tensor-core check, the profile assembly) and all warps share the FP64 sums.
-__device__ void debye_qblock(const DebyeArgs& A, const int q0) {
-    const int nqb = min(kQB, A.nq - q0);
-    if (nqb <= 0) return;
+// Shared memory of a CTA: per-q factors, the cross-warp reduction buffer, the row sums [kQT][R] and
+// the rows' distance-axis groups.
+constexpr size_t kOffRed = ((sizeof(QFactors) * kQT + 15) / 16) * 16;
+constexpr size_t kOffAcc = kOffRed + sizeof(double) * kWarps * kRG * kQT;
+__host__ __device__ constexpr size_t debye_smem(int R) { return kOffAcc + sizeof(double) * kQT * R + sizeof(int) * R; }
+
+// One CTA evaluates kQT consecutive q values of one transform.  Thread (warp w, lane l) owns q value
+// l % kQT and bin phase p = 2 w + l / kQT: it evaluates sinc(q d_b) for the bins b = p (mod 16) of each
+// 128-bin chunk once and adds H[r][b] sinc into one register accumulator per row (rows in groups of
+// 32).  A (row, q) sum is therefore 16 serial sums over the bins of one phase, in bin order, added by
+// a shuffle and then warp by warp: the same bits for a transform whether it runs alone or in a batch.
+__device__ void debye_qtile(const DebyeArgs& A, const int q0, unsigned char* smem) {
+    const int nqt = min(kQT, A.nq - q0);
+    if (nqt <= 0) return;
     const int R = A.R;
     const int mb = *A.max_bin;
-    __shared__ double s_sinc[kQB][3][kChunk];
-    __shared__ double s_acc[kQB][kMaxRows];
-    __shared__ QFactors s_F[kQB];
-    __shared__ int s_fp64[kQB];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = kThreads >> 5;
+    QFactors* s_F = reinterpret_cast<QFactors*>(smem);
+    double* s_red = reinterpret_cast<double*>(smem + kOffRed);  // [kWarps][kRG][kQT]
+    double* s_acc = reinterpret_cast<double*>(smem + kOffAcc);  // [kQT][R]
+    int* s_grp = reinterpret_cast<int*>(smem + kOffAcc + sizeof(double) * kQT * R);
+    __shared__ int s_fp64[kQT];
+    __shared__ int s_groups;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
-    // per-q factors: lane j of warp qi computes one of them (a handful of exp each)
-    if (warp < nqb) {
-        const double q = A.q[q0 + warp];
-        QFactors& F = s_F[warp];
-        if (lane < kNff) {
-            F.f[lane] = ff_raw(lane, q);
-        } else if (lane < 2 * kNff) {
+    // per-q factors: 32 per q value, one per thread (a handful of exp each)
+    for (int i = tid; i < nqt * 32; i += kThreads) {
+        const int qq = i >> 5, j = i & 31;
+        const double q = A.q[q0 + qq];
+        QFactors& F = s_F[qq];
+        if (j < kNff) {
+            F.f[j] = ff_raw(j, q);
+        } else if (j < 2 * kNff) {
             // ExvFormFactor(V).evaluate(q) = V rho_w exp(-V^(2/3)/(4 pi) q^2) (ExvFormFactor.h:20-33)
-            const double v = c_exv_volume[lane - kNff];
-            F.xe[lane - kNff] = v * kRhoWater * exp(-(pow(v, 2.0 / 3) / (4 * kPi)) * q * q);
-        } else if (lane == 2 * kNff) {
+            const double v = c_exv_volume[j - kNff];
+            F.xe[j - kNff] = v * kRhoWater * exp(-(pow(v, 2.0 / 3) / (4 * kPi)) * q * q);
+        } else if (j == 2 * kNff) {
             const double rm2 = kAvgRadius * kAvgRadius / 4;  // exv_factor (CompositeDistanceHistogramFFExplicitBase.cpp:54-57)
             F.e = pow(A.cx, 3) * exp(-rm2 * (pow(A.cx, 2) - 1) * q * q);
             if (A.exv_model == 1) {
@@ -161,19 +178,25 @@ __device__ void debye_qblock(const DebyeArgs& A, const int q0) {
             } else {
                 F.fx = ff_raw(kExv, q);
             }
-        } else if (lane == 2 * kNff + 1) {
+        } else {
             F.ba = (A.dw_atomic != 0 || A.dw_exv != 0) ? exp(-q * q * A.dw_atomic * A.dw_atomic * 0.5) : 1.0;
             F.bx = (A.dw_atomic != 0 || A.dw_exv != 0) ? exp(-q * q * A.dw_exv * A.dw_exv * 0.5) : 1.0;
             F.eq2 = exp(-q * q);
-            s_fp64[warp] = 1;
-            if (A.tc_err_est) A.tc_err_est[q0 + warp] = INFINITY;  // overwritten below when tensor-core values exist
+            s_fp64[qq] = 1;
+            if (A.tc_err_est) A.tc_err_est[q0 + qq] = INFINITY;  // overwritten below when tensor-core values exist
         }
     }
-    for (int i = threadIdx.x; i < kQB * kMaxRows; i += kThreads) (&s_acc[0][0])[i] = 0;
+    if (tid == 0) s_groups = 1;
+    for (int i = tid; i < kQT * R; i += kThreads) s_acc[i] = 0;
     __syncthreads();
+    for (int r = tid; r < R; r += kThreads) {
+        const int g = A.rows[r].group;
+        s_grp[r] = g;
+        if (g > 0) atomicMax(&s_groups, g + 1);
+    }
 
     // With tensor-core values: keep a q unless its estimated error is above tolerance.
-    if (A.sinqd_tc && !(A.tc_error && *A.tc_error) && warp < nqb) {
+    if (A.sinqd_tc && !(A.tc_error && *A.tc_error)) {
         // Error bound of the tensor-core values, per row: c_rel * sum_b |H||S| + c_abs * sum_b |H|.
         //  * c_rel, operand representation: H to FP32 (2^-24), FP32 sinc value (sinf 2 ulp, the
         //    division 2^-24), the BF16 products dropped by the split (< 2^-25), the main+correction
@@ -184,78 +207,102 @@ __device__ void debye_qblock(const DebyeArgs& A, const int q0) {
         //  * c_abs: the FP32 argument q*d carries 3 roundings, i.e. |dx| <= 3 * 2^-24 x, and
         //    |d sinc/dx| <= 2/x, so |d sinc| <= 1.5 * 2^-22 for every x;
         //  * 10 % slack for the FP32 bound and row sums themselves.
-        const int k = q0 + warp;
         const int per = debye_tc_split_bins(mb, A.tc_splits);
         const double c_rel = (0x1p-21 + (per / 16 + 1) * 0x1p-22) * 1.1;
         const double c_abs = 0x1p-21 * 1.1;
         const size_t plane = static_cast<size_t>(R) * A.nq;
-        double I = 0, err = 0;
-        for (int r = lane; r < R; r += 32) {
-            const double cf = row_terms(A, A.rows[r], s_F[warp]).in_I;
-            double v = 0, bnd = 0, ha = 0;
-            for (int z = 0; z < A.tc_splits; ++z) {
-                v += A.sinqd_tc[z * plane + static_cast<size_t>(r) * A.nq + k];
-                bnd += A.bound_tc[z * plane + static_cast<size_t>(r) * A.nq + k];
-                ha += A.habs_tc[static_cast<size_t>(z) * R + r];
+        for (int qq = warp; qq < nqt; qq += kWarps) {
+            const int k = q0 + qq;
+            double I = 0, err = 0;
+            for (int r = lane; r < R; r += 32) {
+                const double cf = row_terms(A, A.rows[r], s_F[qq]).in_I;
+                double v = 0, bnd = 0, ha = 0;
+                for (int z = 0; z < A.tc_splits; ++z) {
+                    v += A.sinqd_tc[z * plane + static_cast<size_t>(r) * A.nq + k];
+                    bnd += A.bound_tc[z * plane + static_cast<size_t>(r) * A.nq + k];
+                    ha += A.habs_tc[static_cast<size_t>(z) * R + r];
+                }
+                s_acc[qq * R + r] = v;
+                I += cf * v;
+                err += fabs(cf) * (c_rel * bnd + c_abs * ha);
             }
-            s_acc[warp][r] = v;
-            I += cf * v;
-            err += fabs(cf) * (c_rel * bnd + c_abs * ha);
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            I += __shfl_xor_sync(0xffffffffu, I, o);
-            err += __shfl_xor_sync(0xffffffffu, err, o);
-        }
-        if (lane == 0) {
-            bool ok = err <= A.tolerance * fabs(I);
-            s_fp64[warp] = ok ? 0 : 1;
-            if (!ok && A.fp64_columns) atomicAdd(A.fp64_columns, 1);
-            if (A.tc_err_est) A.tc_err_est[k] = fabs(I) > 0 ? err / fabs(I) : INFINITY;
+            for (int o = 16; o > 0; o >>= 1) {
+                I += __shfl_xor_sync(0xffffffffu, I, o);
+                err += __shfl_xor_sync(0xffffffffu, err, o);
+            }
+            if (lane == 0) {
+                bool ok = err <= A.tolerance * fabs(I);
+                s_fp64[qq] = ok ? 0 : 1;
+                if (!ok && A.fp64_columns) atomicAdd(A.fp64_columns, 1);
+                if (A.tc_err_est) A.tc_err_est[k] = fabs(I) > 0 ? err / fabs(I) : INFINITY;
+            }
         }
     }
     __syncthreads();
 
     int any = 0;
-    for (int qi = 0; qi < nqb; ++qi) any |= s_fp64[qi];
+    for (int qq = 0; qq < nqt; ++qq) any |= s_fp64[qq];
     if (any) {
-        for (int i = threadIdx.x; i < nqb * R; i += kThreads)
-            if (s_fp64[i / R]) s_acc[i / R][i % R] = 0;
-        int used_groups = 1;
-        for (int r = 0; r < R; ++r) used_groups = max(used_groups, A.rows[r].group + 1);
-        __syncthreads();
-        for (int c0 = 0; c0 < mb; c0 += kChunk) {
-            const int cn = min(kChunk, mb - c0);
-            for (int i = threadIdx.x; i < nqb * cn; i += kThreads) {
-                const int qi = i / cn, t = i - qi * cn;
-                if (!s_fp64[qi]) continue;
-                const double q = A.q[q0 + qi];
-                s_sinc[qi][0][t] = sinc64(q * A.axis0[c0 + t]);
-                if (used_groups > 1) s_sinc[qi][1][t] = sinc64(q * A.axis1[c0 + t]);
-                if (used_groups > 2) s_sinc[qi][2][t] = sinc64(q * A.axis2[c0 + t]);
+        const int qi = lane % kQT, phase = warp * kSubs + lane / kQT;
+        const bool qon = qi < nqt && s_fp64[qi] != 0;
+        const double q = qi < nqt ? A.q[q0 + qi] : 0.0;
+        const int groups = s_groups;
+        for (int rg0 = 0; rg0 < R; rg0 += kRG) {
+            const int rn = min(kRG, R - rg0);
+            double acc[kRG];
+#pragma unroll
+            for (int i = 0; i < kRG; ++i) acc[i] = 0;
+            for (int g = 0; g < groups; ++g) {
+                const double* axis = g == 0 ? A.axis0 : (g == 1 ? A.axis1 : A.axis2);
+                for (int c0 = 0; c0 < mb; c0 += kCB) {
+                    double sv[kBinsPerThread];
+#pragma unroll
+                    for (int k = 0; k < kBinsPerThread; ++k) {
+                        const int b = c0 + phase + k * kPhases;
+                        sv[k] = (qon && b < mb) ? sinc64(q * axis[b]) : 0.0;
+                    }
+#pragma unroll
+                    for (int i = 0; i < kRG; ++i) {
+                        if (i < rn && s_grp[rg0 + i] == g) {
+                            const double* h = A.H + static_cast<size_t>(rg0 + i) * A.nb;
+                            double a = acc[i];
+#pragma unroll
+                            for (int k = 0; k < kBinsPerThread; ++k) {
+                                const int b = c0 + phase + k * kPhases;
+                                if (b < mb) a += h[b] * sv[k];
+                            }
+                            acc[i] = a;
+                        }
+                    }
+                }
+            }
+            // the two phases of a warp by a shuffle, then the warps in order
+#pragma unroll
+            for (int i = 0; i < kRG; ++i) {
+                double v = acc[i];
+#pragma unroll
+                for (int o = kQT; o < 32; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane < kQT && i < rn) s_red[(warp * kRG + i) * kQT + qi] = v;
             }
             __syncthreads();
-            // (row, q) sums: lanes stride the chunk's bins, then a shuffle tree; chunk partials are
-            // added in bin order, so every transform of the same rows gives the same bits
-            for (int p = warp; p < R * nqb; p += nwarps) {
-                const int r = p / nqb, qi = p - r * nqb;
-                if (!s_fp64[qi]) continue;
-                const double* h = A.H + static_cast<size_t>(r) * A.nb + c0;
-                const double* sv = s_sinc[qi][A.rows[r].group];
-                double acc = 0;
-                for (int t = lane; t < cn; t += 32) acc += h[t] * sv[t];
-                for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-                if (lane == 0) s_acc[qi][r] += acc;
+            for (int i = tid; i < rn * kQT; i += kThreads) {
+                const int r = i / kQT, qq = i - r * kQT;
+                if (qq < nqt && s_fp64[qq]) {
+                    double v = 0;
+                    for (int w = 0; w < kWarps; ++w) v += s_red[(w * kRG + r) * kQT + qq];
+                    s_acc[qq * R + rg0 + r] = v;
+                }
             }
             __syncthreads();
         }
     }
 
-    if (warp < nqb) {
-        const int k = q0 + warp;
+    for (int qq = warp; qq < nqt; qq += kWarps) {
+        const int k = q0 + qq;
         double prof[6] = {0, 0, 0, 0, 0, 0};
         for (int r = lane; r < R; r += 32) {
-            const RowTerms t = row_terms(A, A.rows[r], s_F[warp]);
-            for (int k2 = 0; k2 < t.n; ++k2) prof[t.p[k2]] += t.cf[k2] * s_acc[warp][r];
+            const RowTerms t = row_terms(A, A.rows[r], s_F[qq]);
+            for (int k2 = 0; k2 < t.n; ++k2) prof[t.p[k2]] += t.cf[k2] * s_acc[qq * R + r];
         }
         for (int p = 0; p < 6; ++p)
             for (int o = 16; o > 0; o >>= 1) prof[p] += __shfl_xor_sync(0xffffffffu, prof[p], o);
@@ -280,19 +327,37 @@ __device__ void debye_qblock(const DebyeArgs& A, const int q0) {
     }
 }
 
-__global__ void __launch_bounds__(kThreads) debye_kernel(DebyeArgs A) { debye_qblock(A, blockIdx.x * kQB); }
+__global__ void __launch_bounds__(kThreads, 2) debye_kernel(DebyeArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    debye_qtile(A, blockIdx.x * kQT, smem);
+}
 // batched: blockIdx.y selects the structure
-__global__ void __launch_bounds__(kThreads) debye_batch_kernel(const DebyeArgs* As) {
-    debye_qblock(As[blockIdx.y], blockIdx.x * kQB);
+__global__ void __launch_bounds__(kThreads, 2) debye_batch_kernel(const DebyeArgs* As) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    debye_qtile(As[blockIdx.y], blockIdx.x * kQT, smem);
+}
+
+bool debye_configure() {
+    static bool done = false;
+    if (done) return true;
+    const int bytes = static_cast<int>(debye_smem(kMaxRows));
+    if (cudaFuncSetAttribute(debye_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess ||
+        cudaFuncSetAttribute(debye_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
+        return false;
+    done = true;
+    return true;
 }
 
 }  // namespace
 
+// (a failed configuration shows as the launch's own error, which the callers check)
 void debye_fp64_launch(const DebyeArgs& A, cudaStream_t s) {
-    debye_kernel<<<(A.nq + kQB - 1) / kQB, kThreads, 0, s>>>(A);
+    debye_configure();
+    debye_kernel<<<(A.nq + kQT - 1) / kQT, kThreads, debye_smem(A.R), s>>>(A);
 }
-void debye_fp64_batch_launch(const DebyeArgs* As_dev, int n, int max_nq, cudaStream_t s) {
-    debye_batch_kernel<<<dim3((max_nq + kQB - 1) / kQB, n), kThreads, 0, s>>>(As_dev);
+void debye_fp64_batch_launch(const DebyeArgs* As_dev, int n, int max_nq, int max_R, cudaStream_t s) {
+    debye_configure();
+    debye_batch_kernel<<<dim3((max_nq + kQT - 1) / kQT, n), kThreads, debye_smem(max_R), s>>>(As_dev);
 }
 
 }  // namespace ausaxs_b200

@@ -58,8 +58,8 @@ struct DebyeArgs {
 };
 
 void debye_fp64_launch(const DebyeArgs& A, cudaStream_t s);
-// n transforms at once (device array of arguments; max_nq >= every nq)
-void debye_fp64_batch_launch(const DebyeArgs* As_dev, int n, int max_nq, cudaStream_t s);
+// n transforms at once (device array of arguments; max_nq >= every nq, max_R >= every R)
+void debye_fp64_batch_launch(const DebyeArgs* As_dev, int n, int max_nq, int max_R, cudaStream_t s);
 
 // Split-BF16 tensor-core contraction sinqd[r][q] = sum_b H[r][b] sinc(q d_{g(r)}[b]) for all rows,
 // with the bound sum_b |H||sinc| per element (debye_tc.cu).  Returns false when the launch could not
