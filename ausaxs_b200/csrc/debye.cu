@@ -136,8 +136,12 @@ __device__ RowTerms row_terms(const DebyeArgs& A, const RowDesc& r, const QFacto
 
 // Shared memory of a CTA: per-q factors, the cross-warp reduction buffer, the row sums [kQT][R] and
 // the rows' distance-axis groups.
+// the cross-warp reduction buffer reuses the staged H chunk (the two are not live together)
 constexpr size_t kOffRed = ((sizeof(QFactors) * kQT + 15) / 16) * 16;
-constexpr size_t kOffAcc = kOffRed + sizeof(double) * kWarps * kRG * kQT;
+constexpr size_t kOffH = kOffRed;                             // staged H chunk [kRG][kCB]
+static_assert(kWarps * kRG * kQT <= kRG * kCB, "the reduction buffer must fit in the H chunk");
+constexpr size_t kOffAx = kOffH + sizeof(double) * kRG * kCB;  // staged axis chunk [kCB]
+constexpr size_t kOffAcc = kOffAx + sizeof(double) * kCB;
 __host__ __device__ constexpr size_t debye_smem(int R) { return kOffAcc + sizeof(double) * kQT * R + sizeof(int) * R; }
 
 // One CTA evaluates kQT consecutive q values of one transform.  Thread (warp w, lane l) owns q value
@@ -152,6 +156,8 @@ __device__ void debye_qtile(const DebyeArgs& A, const int q0, unsigned char* sme
     const int mb = *A.max_bin;
     QFactors* s_F = reinterpret_cast<QFactors*>(smem);
     double* s_red = reinterpret_cast<double*>(smem + kOffRed);  // [kWarps][kRG][kQT]
+    double* s_h = reinterpret_cast<double*>(smem + kOffH);      // [kRG][kCB]
+    double* s_ax = reinterpret_cast<double*>(smem + kOffAx);    // [kCB]
     double* s_acc = reinterpret_cast<double*>(smem + kOffAcc);  // [kQT][R]
     int* s_grp = reinterpret_cast<int*>(smem + kOffAcc + sizeof(double) * kQT * R);
     __shared__ int s_fp64[kQT];
@@ -255,28 +261,35 @@ __device__ void debye_qtile(const DebyeArgs& A, const int q0, unsigned char* sme
             for (int g = 0; g < groups; ++g) {
                 const double* axis = g == 0 ? A.axis0 : (g == 1 ? A.axis1 : A.axis2);
                 for (int c0 = 0; c0 < mb; c0 += kCB) {
+                    const int cn = min(kCB, mb - c0);
+                    // the chunk's rows of H and axis values, coalesced, zero past the last bin
+                    __syncthreads();
+                    for (int i = tid; i < rn * kCB; i += kThreads) {
+                        const int r = i / kCB, t = i - r * kCB;
+                        s_h[i] = t < cn ? A.H[static_cast<size_t>(rg0 + r) * A.nb + c0 + t] : 0.0;
+                    }
+                    for (int t = tid; t < kCB; t += kThreads) s_ax[t] = t < cn ? axis[c0 + t] : 0.0;
+                    __syncthreads();
                     double sv[kBinsPerThread];
 #pragma unroll
                     for (int k = 0; k < kBinsPerThread; ++k) {
-                        const int b = c0 + phase + k * kPhases;
-                        sv[k] = (qon && b < mb) ? sinc64(q * axis[b]) : 0.0;
+                        const int t = phase + k * kPhases;
+                        sv[k] = (qon && t < cn) ? sinc64(q * s_ax[t]) : 0.0;
                     }
 #pragma unroll
                     for (int i = 0; i < kRG; ++i) {
                         if (i < rn && s_grp[rg0 + i] == g) {
-                            const double* h = A.H + static_cast<size_t>(rg0 + i) * A.nb;
+                            const double* h = s_h + i * kCB + phase;
                             double a = acc[i];
 #pragma unroll
-                            for (int k = 0; k < kBinsPerThread; ++k) {
-                                const int b = c0 + phase + k * kPhases;
-                                if (b < mb) a += h[b] * sv[k];
-                            }
+                            for (int k = 0; k < kBinsPerThread; ++k) a += h[k * kPhases] * sv[k];
                             acc[i] = a;
                         }
                     }
                 }
             }
             // the two phases of a warp by a shuffle, then the warps in order
+            __syncthreads();  // every thread is done with the staged chunk the buffer overlays
 #pragma unroll
             for (int i = 0; i < kRG; ++i) {
                 double v = acc[i];

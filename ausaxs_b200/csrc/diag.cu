@@ -10,6 +10,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "../../include/ausaxs_b200_diag.h"
 
 namespace ausaxs_b200 {
@@ -21,9 +23,13 @@ constexpr int kDiagBins = 4096;  // u32 words per CTA (16 KB), a typical on-chip
 constexpr int kDiagThreads = 512;
 constexpr int kDiagUnroll = 8;
 
+// W64: 64-bit atomicAdd on an array of the same byte size (kDiagBins / 2 words)
+template <bool W64>
 __global__ void __launch_bounds__(kDiagThreads) smem_atomic_kernel(int iters, int conflict_free, unsigned* sink) {
-    __shared__ unsigned h[kDiagBins];
-    for (int k = threadIdx.x; k < kDiagBins; k += blockDim.x) h[k] = 0;
+    using T = typename std::conditional<W64, unsigned long long, unsigned>::type;
+    constexpr int kWords = W64 ? kDiagBins / 2 : kDiagBins;
+    __shared__ T h[kWords];
+    for (int k = threadIdx.x; k < kWords; k += blockDim.x) h[k] = 0;
     __syncthreads();
     const unsigned lane = threadIdx.x & 31u;
     unsigned x = 0x9E3779B9u * (blockIdx.x * blockDim.x + threadIdx.x + 1u);
@@ -32,14 +38,14 @@ __global__ void __launch_bounds__(kDiagThreads) smem_atomic_kernel(int iters, in
         for (int u = 0; u < kDiagUnroll; ++u) {
             x = x * 1664525u + 1013904223u;  // LCG (Numerical Recipes constants)
             const unsigned r = x >> 20;      // 12 random bits
-            const unsigned b = conflict_free ? (lane | ((r & (kDiagBins / 32 - 1)) << 5)) : (r & (kDiagBins - 1));
-            atomicAdd(&h[b], 1u);
+            const unsigned b = conflict_free ? (lane | ((r & (kWords / 32 - 1)) << 5)) : (r & (kWords - 1));
+            atomicAdd(&h[b], static_cast<T>(1));
         }
     }
     __syncthreads();
-    unsigned s = 0;
-    for (int k = threadIdx.x; k < kDiagBins; k += blockDim.x) s += h[k];
-    if (s == 0xFFFFFFFFu) sink[0] = s;  // keeps the atomics alive; never true in practice
+    T s = 0;
+    for (int k = threadIdx.x; k < kWords; k += blockDim.x) s += h[k];
+    if (s == static_cast<T>(0xFFFFFFFFu)) sink[0] = static_cast<unsigned>(s);  // keeps the atomics alive; never true in practice
 }
 
 int fail(int code, const char* msg) {
@@ -56,11 +62,13 @@ extern "C" int ausaxs_gpu_smem_atomic_rate(int32_t device, int32_t conflict_free
     if (!atomics_per_s) return fail(AUSAXS_ERR_ARGUMENT, "null argument");
     cudaGetLastError();
     if (cudaSetDevice(device) != cudaSuccess) return fail(AUSAXS_ERR_CUDA, "no such device");
+    const bool w64 = (conflict_free & 2) != 0;
+    const int mode = conflict_free & 1;
+    auto kernel = w64 ? smem_atomic_kernel<true> : smem_atomic_kernel<false>;
     int sms = 0, per_sm = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || sms <= 0)
         return fail(AUSAXS_ERR_CUDA, "cannot query the multiprocessor count");
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, smem_atomic_kernel, kDiagThreads, 0) != cudaSuccess ||
-        per_sm <= 0)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kDiagThreads, 0) != cudaSuccess || per_sm <= 0)
         return fail(AUSAXS_ERR_CUDA, "cannot query the occupancy");
     unsigned* sink = nullptr;
     cudaStream_t s = nullptr;
@@ -73,9 +81,9 @@ extern "C" int ausaxs_gpu_smem_atomic_rate(int32_t device, int32_t conflict_free
         cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
         rc = fail(AUSAXS_ERR_CUDA, "cannot allocate the measurement's resources");
     } else {
-        smem_atomic_kernel<<<grid, kDiagThreads, 0, s>>>(iters / 8, conflict_free, sink);  // warm-up
+        kernel<<<grid, kDiagThreads, 0, s>>>(iters / 8, mode, sink);  // warm-up
         cudaEventRecord(e0, s);
-        smem_atomic_kernel<<<grid, kDiagThreads, 0, s>>>(iters, conflict_free, sink);
+        kernel<<<grid, kDiagThreads, 0, s>>>(iters, mode, sink);
         cudaEventRecord(e1, s);
         if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&t, e0, e1) != cudaSuccess || t <= 0)
             rc = fail(AUSAXS_ERR_CUDA, cudaGetErrorString(cudaGetLastError()));
