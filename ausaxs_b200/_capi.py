@@ -182,10 +182,11 @@ def load():
         return L
 
 
-def smem_atomic_rate(device: int = 0, conflict_free: bool = True):
-    """(shared-memory atomics per second over the device, kernel milliseconds)."""
+def smem_atomic_rate(device: int = 0, conflict_free: bool = True, wide: bool = False):
+    """(shared-memory atomics per second over the device, kernel milliseconds); wide: 64-bit atomics."""
     r, ms = C.c_double(0.0), C.c_double(0.0)
-    check(load().ausaxs_gpu_smem_atomic_rate(device, int(conflict_free), C.byref(r), C.byref(ms)))
+    mode = int(bool(conflict_free)) | (2 if wide else 0)
+    check(load().ausaxs_gpu_smem_atomic_rate(device, mode, C.byref(r), C.byref(ms)))
     return r.value, ms.value
 
 
