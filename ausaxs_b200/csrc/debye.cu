@@ -41,11 +41,7 @@ constexpr double kRhoWater = 0.334;        // e / A^3 (include/core/constants/Co
 constexpr double kAvgRadius = 1.62;        // A (Constants.h:90)
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kQT = 16;                        // q values per CTA
-constexpr int kSubs = 32 / kQT;                // bin phases per warp
-constexpr int kPhases = kThreads / kQT;        // bin phases per CTA
-constexpr int kBinsPerThread = 8;              // bins of one phase per chunk
-constexpr int kCB = kPhases * kBinsPerThread;  // bins per chunk
+constexpr int kCB = 128;                       // bins per staged chunk
 constexpr int kRG = 32;                        // rows per group of register accumulators
 constexpr int kMaxRows = 264;
 
@@ -134,33 +130,46 @@ __device__ RowTerms row_terms(const DebyeArgs& A, const RowDesc& r, const QFacto
     return t;
 }
 
-// Shared memory of a CTA: per-q factors, the cross-warp reduction buffer, the row sums [kQT][R] and
-// the rows' distance-axis groups.
-// the cross-warp reduction buffer reuses the staged H chunk (the two are not live together)
-constexpr size_t kOffRed = ((sizeof(QFactors) * kQT + 15) / 16) * 16;
-constexpr size_t kOffH = kOffRed;                             // staged H chunk [kRG][kCB]
-static_assert(kWarps * kRG * kQT <= kRG * kCB, "the reduction buffer must fit in the H chunk");
-constexpr size_t kOffAx = kOffH + sizeof(double) * kRG * kCB;  // staged axis chunk [kCB]
-constexpr size_t kOffAcc = kOffAx + sizeof(double) * kCB;
-__host__ __device__ constexpr size_t debye_smem(int R) { return kOffAcc + sizeof(double) * kQT * R + sizeof(int) * R; }
+// q values per CTA by the transform's q count: 4 up to 256 q, 8 up to 1,024, 16 beyond.  The
+// decomposition depends on nq alone, so a structure's I(q) has the same bits alone or in a batch.
+constexpr int debye_qt(int nq) { return nq <= 256 ? 4 : (nq <= 1024 ? 8 : 16); }
 
-// One CTA evaluates kQT consecutive q values of one transform.  Thread (warp w, lane l) owns q value
-// l % kQT and bin phase p = 2 w + l / kQT: it evaluates sinc(q d_b) for the bins b = p (mod 16) of each
-// 128-bin chunk once and adds H[r][b] sinc into one register accumulator per row (rows in groups of
-// 32).  A (row, q) sum is therefore 16 serial sums over the bins of one phase, in bin order, added by
-// a shuffle and then warp by warp: the same bits for a transform whether it runs alone or in a batch.
+// Layout of a CTA of QT q values: thread (warp w, lane l) owns q value l % QT and bin phase
+// w * (32 / QT) + l / QT of the CTA's 256 / QT phases; a phase holds 128 QT / 256 bins of each chunk.
+// Shared memory: per-q factors, the staged H chunk (reused as the cross-warp reduction buffer), the
+// staged axis chunk, the row sums [QT][R] and the rows' distance-axis groups.
+template <int QT>
+struct QTile {
+    static constexpr int kSubs = 32 / QT;
+    static constexpr int kPhases = kThreads / QT;
+    static constexpr int kBinsPerThread = kCB / kPhases;
+    static constexpr size_t kOffRed = ((sizeof(QFactors) * QT + 15) / 16) * 16;
+    static constexpr size_t kOffH = kOffRed;
+    static constexpr size_t kOffAx = kOffH + sizeof(double) * kRG * kCB;
+    static constexpr size_t kOffAcc = kOffAx + sizeof(double) * kCB;
+    static constexpr size_t smem(int R) { return kOffAcc + sizeof(double) * QT * R + sizeof(int) * R; }
+    static_assert(kWarps * kRG * QT <= kRG * kCB, "the reduction buffer must fit in the H chunk");
+    static_assert(kBinsPerThread * kPhases == kCB, "a chunk must split evenly into phases");
+};
+
+// One CTA evaluates QT consecutive q values of one transform.  Each thread evaluates sinc(q d_b) for
+// its q value and the bins of its phase in each 128-bin chunk once and adds H[r][b] sinc into one
+// register accumulator per row (rows in groups of 32).  A (row, q) sum is therefore one serial sum per
+// phase, in bin order, the phases of a warp added by shuffles and then the warps in order.
+template <int QT>
 __device__ void debye_qtile(const DebyeArgs& A, const int q0, unsigned char* smem) {
-    const int nqt = min(kQT, A.nq - q0);
+    using T = QTile<QT>;
+    const int nqt = min(QT, A.nq - q0);
     if (nqt <= 0) return;
     const int R = A.R;
     const int mb = *A.max_bin;
     QFactors* s_F = reinterpret_cast<QFactors*>(smem);
-    double* s_red = reinterpret_cast<double*>(smem + kOffRed);  // [kWarps][kRG][kQT]
-    double* s_h = reinterpret_cast<double*>(smem + kOffH);      // [kRG][kCB]
-    double* s_ax = reinterpret_cast<double*>(smem + kOffAx);    // [kCB]
-    double* s_acc = reinterpret_cast<double*>(smem + kOffAcc);  // [kQT][R]
-    int* s_grp = reinterpret_cast<int*>(smem + kOffAcc + sizeof(double) * kQT * R);
-    __shared__ int s_fp64[kQT];
+    double* s_red = reinterpret_cast<double*>(smem + T::kOffRed);  // [kWarps][kRG][QT]
+    double* s_h = reinterpret_cast<double*>(smem + T::kOffH);      // [kRG][kCB]
+    double* s_ax = reinterpret_cast<double*>(smem + T::kOffAx);    // [kCB]
+    double* s_acc = reinterpret_cast<double*>(smem + T::kOffAcc);  // [QT][R]
+    int* s_grp = reinterpret_cast<int*>(smem + T::kOffAcc + sizeof(double) * QT * R);
+    __shared__ int s_fp64[QT];
     __shared__ int s_groups;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
@@ -193,7 +202,7 @@ __device__ void debye_qtile(const DebyeArgs& A, const int q0, unsigned char* sme
         }
     }
     if (tid == 0) s_groups = 1;
-    for (int i = tid; i < kQT * R; i += kThreads) s_acc[i] = 0;
+    for (int i = tid; i < QT * R; i += kThreads) s_acc[i] = 0;
     __syncthreads();
     for (int r = tid; r < R; r += kThreads) {
         const int g = A.rows[r].group;
@@ -249,7 +258,7 @@ __device__ void debye_qtile(const DebyeArgs& A, const int q0, unsigned char* sme
     int any = 0;
     for (int qq = 0; qq < nqt; ++qq) any |= s_fp64[qq];
     if (any) {
-        const int qi = lane % kQT, phase = warp * kSubs + lane / kQT;
+        const int qi = lane % QT, phase = warp * T::kSubs + lane / QT;
         const bool qon = qi < nqt && s_fp64[qi] != 0;
         const double q = qi < nqt ? A.q[q0 + qi] : 0.0;
         const int groups = s_groups;
@@ -270,10 +279,10 @@ __device__ void debye_qtile(const DebyeArgs& A, const int q0, unsigned char* sme
                     }
                     for (int t = tid; t < kCB; t += kThreads) s_ax[t] = t < cn ? axis[c0 + t] : 0.0;
                     __syncthreads();
-                    double sv[kBinsPerThread];
+                    double sv[T::kBinsPerThread];
 #pragma unroll
-                    for (int k = 0; k < kBinsPerThread; ++k) {
-                        const int t = phase + k * kPhases;
+                    for (int k = 0; k < T::kBinsPerThread; ++k) {
+                        const int t = phase + k * T::kPhases;
                         sv[k] = (qon && t < cn) ? sinc64(q * s_ax[t]) : 0.0;
                     }
 #pragma unroll
@@ -282,7 +291,7 @@ __device__ void debye_qtile(const DebyeArgs& A, const int q0, unsigned char* sme
                             const double* h = s_h + i * kCB + phase;
                             double a = acc[i];
 #pragma unroll
-                            for (int k = 0; k < kBinsPerThread; ++k) a += h[k * kPhases] * sv[k];
+                            for (int k = 0; k < T::kBinsPerThread; ++k) a += h[k * T::kPhases] * sv[k];
                             acc[i] = a;
                         }
                     }
@@ -294,15 +303,15 @@ __device__ void debye_qtile(const DebyeArgs& A, const int q0, unsigned char* sme
             for (int i = 0; i < kRG; ++i) {
                 double v = acc[i];
 #pragma unroll
-                for (int o = kQT; o < 32; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                if (lane < kQT && i < rn) s_red[(warp * kRG + i) * kQT + qi] = v;
+                for (int o = QT; o < 32; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                if (lane < QT && i < rn) s_red[(warp * kRG + i) * QT + qi] = v;
             }
             __syncthreads();
-            for (int i = tid; i < rn * kQT; i += kThreads) {
-                const int r = i / kQT, qq = i - r * kQT;
+            for (int i = tid; i < rn * QT; i += kThreads) {
+                const int r = i / QT, qq = i - r * QT;
                 if (qq < nqt && s_fp64[qq]) {
                     double v = 0;
-                    for (int w = 0; w < kWarps; ++w) v += s_red[(w * kRG + r) * kQT + qq];
+                    for (int w = 0; w < kWarps; ++w) v += s_red[(w * kRG + r) * QT + qq];
                     s_acc[qq * R + rg0 + r] = v;
                 }
             }
@@ -340,25 +349,28 @@ __device__ void debye_qtile(const DebyeArgs& A, const int q0, unsigned char* sme
     }
 }
 
+template <int QT>
 __global__ void __launch_bounds__(kThreads, 2) debye_kernel(DebyeArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
-    debye_qtile(A, blockIdx.x * kQT, smem);
+    debye_qtile<QT>(A, blockIdx.x * QT, smem);
 }
 // batched: blockIdx.y selects the structure
+template <int QT>
 __global__ void __launch_bounds__(kThreads, 2) debye_batch_kernel(const DebyeArgs* As) {
     extern __shared__ __align__(16) unsigned char smem[];
-    debye_qtile(As[blockIdx.y], blockIdx.x * kQT, smem);
+    debye_qtile<QT>(As[blockIdx.y], blockIdx.x * QT, smem);
 }
 
+template <int QT>
+bool debye_configure_qt() {
+    const int bytes = static_cast<int>(QTile<QT>::smem(kMaxRows));
+    return cudaFuncSetAttribute(debye_kernel<QT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess &&
+           cudaFuncSetAttribute(debye_batch_kernel<QT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
+}
 bool debye_configure() {
     static bool done = false;
-    if (done) return true;
-    const int bytes = static_cast<int>(debye_smem(kMaxRows));
-    if (cudaFuncSetAttribute(debye_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess ||
-        cudaFuncSetAttribute(debye_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
-        return false;
-    done = true;
-    return true;
+    if (!done) done = debye_configure_qt<4>() && debye_configure_qt<8>() && debye_configure_qt<16>();
+    return done;
 }
 
 }  // namespace
@@ -366,11 +378,21 @@ bool debye_configure() {
 // (a failed configuration shows as the launch's own error, which the callers check)
 void debye_fp64_launch(const DebyeArgs& A, cudaStream_t s) {
     debye_configure();
-    debye_kernel<<<(A.nq + kQT - 1) / kQT, kThreads, debye_smem(A.R), s>>>(A);
+    switch (debye_qt(A.nq)) {
+        case 4: debye_kernel<4><<<(A.nq + 3) / 4, kThreads, QTile<4>::smem(A.R), s>>>(A); break;
+        case 8: debye_kernel<8><<<(A.nq + 7) / 8, kThreads, QTile<8>::smem(A.R), s>>>(A); break;
+        default: debye_kernel<16><<<(A.nq + 15) / 16, kThreads, QTile<16>::smem(A.R), s>>>(A); break;
+    }
 }
-void debye_fp64_batch_launch(const DebyeArgs* As_dev, int n, int max_nq, int max_R, cudaStream_t s) {
+void debye_fp64_batch_launch(const DebyeArgs* As_dev, int n, int nq, int max_R, cudaStream_t s) {
     debye_configure();
-    debye_batch_kernel<<<dim3((max_nq + kQT - 1) / kQT, n), kThreads, debye_smem(max_R), s>>>(As_dev);
+    switch (debye_qt(nq)) {
+        case 4: debye_batch_kernel<4><<<dim3((nq + 3) / 4, n), kThreads, QTile<4>::smem(max_R), s>>>(As_dev); break;
+        case 8: debye_batch_kernel<8><<<dim3((nq + 7) / 8, n), kThreads, QTile<8>::smem(max_R), s>>>(As_dev); break;
+        default:
+            debye_batch_kernel<16><<<dim3((nq + 15) / 16, n), kThreads, QTile<16>::smem(max_R), s>>>(As_dev);
+            break;
+    }
 }
 
 }  // namespace ausaxs_b200
