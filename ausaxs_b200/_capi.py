@@ -44,7 +44,7 @@ EXPORTED = [
     "ausaxs_gpu_calculator_result",
     "ausaxs_gpu_batch_create", "ausaxs_gpu_batch_destroy", "ausaxs_gpu_batch_autotune", "ausaxs_gpu_batch_candidate",
     "ausaxs_gpu_batch_profile_device", "ausaxs_gpu_batch_profile", "ausaxs_gpu_batch_pair_time",
-    "ausaxs_gpu_batch_histogram", "ausaxs_gpu_batch_set_points", "ausaxs_gpu_smem_atomic_rate",
+    "ausaxs_gpu_batch_histogram", "ausaxs_gpu_batch_set_points", "ausaxs_gpu_batch_fp64_columns", "ausaxs_gpu_smem_atomic_rate",
     "ausaxs_gpu_server_create", "ausaxs_gpu_server_destroy", "ausaxs_gpu_server_admit", "ausaxs_gpu_server_release",
     "ausaxs_gpu_server_usage", "ausaxs_gpu_server_submit", "ausaxs_gpu_server_poll", "ausaxs_gpu_server_wait",
     "ausaxs_gpu_server_completed", "ausaxs_gpu_server_launch_count", "ausaxs_gpu_server_body_center", "ausaxs_gpu_server_coordinates", "ausaxs_gpu_server_histogram",
@@ -152,6 +152,7 @@ def load():
         L.ausaxs_gpu_batch_pair_time.argtypes = [vp, f64]
         L.ausaxs_gpu_batch_histogram.argtypes = [vp, C.c_int32, C.POINTER(HistResult)]
         L.ausaxs_gpu_batch_set_points.argtypes = [vp, f32, f32, f64, C.c_int32]
+        L.ausaxs_gpu_batch_fp64_columns.argtypes = [vp, i64]
         L.ausaxs_gpu_smem_atomic_rate.argtypes = [C.c_int32, C.c_int32, f64, f64]
         L.ausaxs_gpu_server_create.argtypes = [C.c_int32, C.c_int64, C.c_int32, C.c_int32, C.POINTER(vp)]
         L.ausaxs_gpu_server_destroy.argtypes = [vp]
@@ -592,6 +593,12 @@ class Batch:
 
     def profile_device(self, q_dev, nq: int, params: DebyeParams, I_dev):
         check(load().ausaxs_gpu_batch_profile_device(self.h, devptr(q_dev), nq, C.byref(params), devptr(I_dev)))
+
+    def fp64_columns(self) -> int:
+        """(structure, q) values of the last profile recomputed in FP64 (waits for it)."""
+        n = C.c_int64(0)
+        check(load().ausaxs_gpu_batch_fp64_columns(self.h, C.byref(n)))
+        return n.value
 
     def pair_time(self) -> float:
         """Device milliseconds of the last profile's pair stage (waits for it)."""

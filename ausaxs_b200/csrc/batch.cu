@@ -99,11 +99,19 @@ struct Batch {
     };
     std::vector<Launch> launches;
     int choice = -1;
-    // misc: tile counters [0, 16), overflow [16] (set from [24] at the start of every profile),
-    // points rejected by the last set_points [24] (kept across profiles)
+    // misc: tile counters [0, 16), overflow [16] (set from [24] at the start of every profile), q values
+    // recomputed in FP64 [20], points rejected by the last set_points [24] (kept across profiles)
     DevBuf jobs, misc, zero, fin, args;
     std::vector<long long> a_off, w_off;  // creation offsets of the concatenated atoms and waters
     DevBuf points_items, points_in;       // set_points: destinations, staged host input
+    // exact-accumulation tensor-core transform (debye_x.cu): Taylor tables shared by every structure,
+    // left-operand rows of all structures (largest first), per-structure partial sums and bound terms
+    struct XState {
+        bool on = false;
+        int K = 0, nch = 0, cps = 0, splits = 0, n_rows = 0;
+        double w = 0;
+        DevBuf table, cpart, rows, planes, err;
+    } x;
     DevBuf d_stats;                      // census of every structure (creation only)
     DevBuf arena;                        // every structure's point arrays
     PrepStats* h_stats = nullptr;        // pinned slots owned by the context
@@ -138,6 +146,8 @@ struct Batch {
 
     unsigned long long* overflow() const { return misc.as<unsigned long long>() + 16; }
     unsigned long long* rejected() const { return misc.as<unsigned long long>() + 24; }
+    // q values of the last profile that the FP64 transform recomputed (cleared by every replay)
+    int32_t* fp64_count() const { return reinterpret_cast<int32_t*>(misc.as<unsigned long long>() + 20); }
 
     void load(const ausaxs_hist_config& c, int n, const float* atoms, const int64_t* aoff, const float* waters,
               const int64_t* woff, const float* exv, const int64_t* xoff, const double* z_exv, bool host) {
@@ -309,7 +319,83 @@ struct Batch {
         }
     }
 
-    void enqueue_all(int nq, cudaStream_t s) {
+    // the tensor-core stage's tables, rows and partial-sum planes for q (device, nq values), and the
+    // fields of every structure's transform arguments that point at them
+    void setup_x(const double* q, int nq, std::vector<DebyeArgs>& A) {
+        std::vector<double> hq(nq);
+        AUSAXS_CUDA(cudaMemcpy(hq.data(), q, sizeof(double) * nq, cudaMemcpyDeviceToHost));
+        double qmax = 0;
+        for (double v : hq) qmax = std::max(qmax, std::fabs(v));
+        XState& X = x;
+        X.w = cfg.bin_width;
+        X.K = debye_x_order(qmax, X.w);
+        X.nch = std::max(1, (max_nb + kXChunk - 1) / kXChunk);
+        X.cps = std::max(1, std::min(X.nch, 60000 / (kXChunk * X.K)));  // exact s32 sums
+        X.splits = (X.nch + X.cps - 1) / X.cps;
+        X.table.ensure(debye_x_table_bytes(nq, X.nch, X.K));
+        const size_t ncp = debye_x_cpart_doubles(nq, X.nch);
+        X.cpart.ensure(sizeof(double) * ncp);
+        const int nqp = (int)(ncp / X.nch);
+        // per structure: values [splits][R][nq], then e1, e0, habs [splits][R]
+        std::vector<size_t> at(items.size());
+        size_t total = 0;
+        for (size_t i = 0; i < items.size(); ++i) {
+            at[i] = total;
+            const size_t R = items[i]->plan.R;
+            total += align_up((size_t)X.splits * R * nq + 3 * (size_t)X.splits * R, 32);
+        }
+        X.planes.ensure(sizeof(double) * std::max<size_t>(1, total));
+        X.err.ensure(256);
+        AUSAXS_CUDA(cudaMemset(X.err.p, 0, 256));
+        double* base = X.planes.as<double>();
+        std::vector<XRow> rows;
+        for (int i : order) {
+            Structure& S = *items[i];
+            Plan& P = S.plan;
+            const int R = P.R;
+            char* pb = P.dev.as<char>();
+            double* v = base + at[i];
+            double* e1 = v + (size_t)X.splits * R * nq;
+            double* e0 = e1 + (size_t)X.splits * R;
+            double* ha = e0 + (size_t)X.splits * R;
+            const double* axes[3] = {reinterpret_cast<const double*>(pb + P.off_d),
+                                     reinterpret_cast<const double*>(pb + P.off_dax),
+                                     reinterpret_cast<const double*>(pb + P.off_dxx)};
+            const bool grid = cfg.manager == AUSAXS_MANAGER_FFGRID;
+            for (int r = 0; r < R; ++r) {
+                const int g = grid ? P.rows_host[r].group : 0;
+                XRow xr{};
+                xr.H = reinterpret_cast<const double*>(pb + P.off_H) + (size_t)r * P.nb;
+                xr.axis = axes[g];
+                xr.max_bin = reinterpret_cast<const int32_t*>(pb + P.off_maxbin);
+                xr.out = v + (size_t)r * nq;
+                xr.e1 = e1 + r;
+                xr.e0 = e0 + r;
+                xr.habs = ha + r;
+                xr.out_z = (long long)R * nq;
+                xr.e_z = R;
+                rows.push_back(xr);
+            }
+            DebyeArgs& a = A[i];
+            a.x_v = v;
+            a.x_e1 = e1;
+            a.x_e0 = e0;
+            a.x_habs = ha;
+            a.x_splits = X.splits;
+            a.x_cpart = X.cpart.as<double>();
+            a.x_nch = X.nch;
+            a.x_nqp = nqp;
+            a.x_K = X.K;
+            a.x_ctr = debye_x_trunc(X.K, X.w);
+            a.tc_error = X.err.as<int32_t>();
+        }
+        X.n_rows = (int)rows.size();
+        X.rows.ensure(sizeof(XRow) * std::max<size_t>(1, rows.size()));
+        AUSAXS_CUDA(cudaMemcpy(X.rows.p, rows.data(), sizeof(XRow) * rows.size(), cudaMemcpyHostToDevice));
+        X.on = true;
+    }
+
+    void enqueue_all(const double* q, int nq, cudaStream_t s) {
         // external records: event-record nodes of the captured graph (a plain record in a capture only
         // orders streams), so every replay timestamps the pair stage
         AUSAXS_CUDA(cudaEventRecordWithFlags(pair_t0, s, cudaEventRecordExternal));
@@ -317,6 +403,14 @@ struct Batch {
         AUSAXS_CUDA(cudaEventRecordWithFlags(pair_t1, s, cudaEventRecordExternal));
         ff_finalize_batch_launch(fin.as<FinalizeFF>(), (int)items.size(), max_nb, s);
         ctx->check_launch("finalize");
+        if (x.on) {
+            debye_x_table_launch(q, nq, x.w, x.nch, x.K, x.table.as<unsigned char>(), x.cpart.as<double>(), s);
+            ctx->check_launch("debye_x_table");
+            if (!debye_x_launch(x.rows.as<XRow>(), x.n_rows, q, nq, x.table.as<unsigned char>(), x.nch, x.K, x.w, x.cps,
+                                x.splits, x.err.as<int32_t>(), s))
+                throw Error{AUSAXS_ERR_CUDA, "cannot launch the tensor-core Debye transform"};
+            ctx->check_launch("debye_x");
+        }
         int max_R = 1;
         for (auto& S : items) max_R = std::max(max_R, S->plan.R);
         debye_fp64_batch_launch(args.as<DebyeArgs>(), (int)items.size(), nq, max_R, s);
@@ -329,7 +423,8 @@ struct Batch {
         cudaStream_t s = C.stream;
         const ausaxs_debye_params& o = key.p;
         const bool same_p = o.cw == p.cw && o.cx == p.cx && o.crho == p.crho && o.dw_atomic == p.dw_atomic &&
-                            o.dw_exv == p.dw_exv && o.grid_width == p.grid_width;
+                            o.dw_exv == p.dw_exv && o.grid_width == p.grid_width && o.precision == p.precision &&
+                            o.tolerance == p.tolerance;
         const bool same = exec && key.q == q && key.nq == nq && key.I == I && key.choice == choice && key.s == s && same_p;
         if (!same) {
             if (exec) {
@@ -340,16 +435,18 @@ struct Batch {
             for (size_t i = 0; i < items.size(); ++i) {
                 DebyeArgs a = items[i]->debye_args(cfgs[i], q, nq, p, I + i * (size_t)nq, nullptr);
                 a.overflow = overflow();  // the batch's launches share one overflow counter
-                a.fp64_columns = nullptr;
+                a.fp64_columns = fp64_count();
                 A.push_back(a);
             }
+            x.on = false;
+            if (p.precision != 1) setup_x(q, nq, A);
             args.ensure(sizeof(DebyeArgs) * A.size());
             AUSAXS_CUDA(cudaMemcpyAsync(args.p, A.data(), sizeof(DebyeArgs) * A.size(), cudaMemcpyHostToDevice, s));
             AUSAXS_CUDA(cudaStreamSynchronize(s));
             cudaGraph_t g = nullptr;
             AUSAXS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
             try {
-                enqueue_all(nq, s);
+                enqueue_all(q, nq, s);
             } catch (...) {
                 cudaStreamEndCapture(s, &g);
                 if (g) cudaGraphDestroy(g);
@@ -566,6 +663,18 @@ int ausaxs_gpu_batch_profile(ausaxs_gpu_batch* b, const double* q, int32_t n_q, 
         if (flags[0])
             throw Error{AUSAXS_ERR_BIN_OVERFLOW, "pair distances beyond the batch's bins (bin_count * bin_width, or the "
                                                  "range planned from the creation coordinates after set_points)"};
+    });
+}
+
+int ausaxs_gpu_batch_fp64_columns(ausaxs_gpu_batch* b, int64_t* n) {
+    return guarded([&] {
+        if (!b || !n) throw Error{AUSAXS_ERR_ARGUMENT, "null argument"};
+        Batch& B = b->impl;
+        AUSAXS_CUDA(cudaSetDevice(B.ctx->device));
+        int32_t v = 0;
+        AUSAXS_CUDA(cudaMemcpyAsync(&v, B.fp64_count(), sizeof(v), cudaMemcpyDeviceToHost, B.ctx->stream));
+        AUSAXS_CUDA(cudaStreamSynchronize(B.ctx->stream));
+        *n = v;
     });
 }
 

@@ -252,6 +252,44 @@ __device__ void debye_qtile(const DebyeArgs& A, const int q0, unsigned char* sme
                 if (A.tc_err_est) A.tc_err_est[k] = fabs(I) > 0 ? err / fabs(I) : INFINITY;
             }
         }
+    } else if (A.x_v && !(A.tc_error && *A.tc_error)) {
+        // Exact-accumulation tensor-core values (debye_x.cu): per row and split the digit and dropped-
+        // pair error is at most x_e1 * Csum(q) + x_e0, Csum(q) = sum_{k,b} |C_k(b, q)| over the table;
+        // the Taylor truncation adds x_ctr q^K sum |H|.  5 % slack for the FP64 sums of the bound.
+        const size_t plane = static_cast<size_t>(R) * A.nq;
+        for (int qq = warp; qq < nqt; qq += kWarps) {
+            const int k = q0 + qq;
+            double cs = 0;
+            for (int c = lane; c < A.x_nch; c += 32) cs += A.x_cpart[static_cast<size_t>(c) * A.x_nqp + k];
+            for (int o = 16; o > 0; o >>= 1) cs += __shfl_xor_sync(0xffffffffu, cs, o);
+            const double qv = A.q[k];
+            double qK = 1;
+            for (int j = 0; j < A.x_K; ++j) qK *= qv;
+            const double trunc = A.x_ctr * qK;
+            double I = 0, err = 0;
+            for (int r = lane; r < R; r += 32) {
+                const double cf = row_terms(A, A.rows[r], s_F[qq]).in_I;
+                double v = 0, e = 0, ha = 0;
+                for (int z = 0; z < A.x_splits; ++z) {
+                    v += A.x_v[z * plane + static_cast<size_t>(r) * A.nq + k];
+                    e += A.x_e1[static_cast<size_t>(z) * R + r] * cs + A.x_e0[static_cast<size_t>(z) * R + r];
+                    ha += A.x_habs[static_cast<size_t>(z) * R + r];
+                }
+                s_acc[qq * R + r] = v;
+                I += cf * v;
+                err += fabs(cf) * (e + trunc * ha) * 1.05;
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                I += __shfl_xor_sync(0xffffffffu, I, o);
+                err += __shfl_xor_sync(0xffffffffu, err, o);
+            }
+            if (lane == 0) {
+                bool ok = err <= A.tolerance * fabs(I);
+                s_fp64[qq] = ok ? 0 : 1;
+                if (!ok && A.fp64_columns) atomicAdd(A.fp64_columns, 1);
+                if (A.tc_err_est) A.tc_err_est[k] = fabs(I) > 0 ? err / fabs(I) : INFINITY;
+            }
+        }
     }
     __syncthreads();
 

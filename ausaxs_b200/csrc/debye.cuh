@@ -55,6 +55,18 @@ struct DebyeArgs {
     double* tc_err_est;         // out: [nq] estimated relative error of the tensor-core I(q) (may be null)
     double* Iq;                 // [nq]
     double* profiles;           // [6][nq] or null
+    // exact-accumulation tensor-core partial sums from debye_x_launch, or null (debye_x.cu):
+    //   x_v [x_splits][R][nq] (FP64 values), x_e1 / x_e0 / x_habs [x_splits][R] (bound terms: the error of
+    //   a split's value is at most x_e1 * Csum(q) + x_e0, Csum(q) = sum_c x_cpart[c][q] over x_nch
+    //   table chunks), and the Taylor truncation x_ctr * q^x_K * sum_z x_habs
+    const double* x_v;
+    const double* x_e1;
+    const double* x_e0;
+    const double* x_habs;
+    int32_t x_splits;
+    const double* x_cpart;      // [x_nch][x_nqp]
+    int32_t x_nch, x_nqp, x_K;
+    double x_ctr;
 };
 
 void debye_fp64_launch(const DebyeArgs& A, cudaStream_t s);
@@ -81,6 +93,39 @@ struct TcArgs {
     int32_t* error_flag;
 };
 bool debye_tc_launch(const TcArgs& A, cudaStream_t s);
+
+// Exact-accumulation tensor-core contraction over shared Taylor tables (debye_x.cu).
+// One left-operand row: a histogram row of some structure and where its partial sums go.
+struct XRow {
+    const double* H;         // the row's bins (null: a padding row)
+    const double* axis;      // its distance axis
+    const int32_t* max_bin;  // its structure's bins in use (device)
+    double* out;             // value of split z, q value k: out[z * out_z + k]
+    double* e1;              // bound terms of split z: e1[z * e_z], e0[z * e_z], habs[z * e_z]
+    double* e0;
+    double* habs;
+    long long out_z;
+    int32_t e_z;
+    int32_t pad;
+};
+constexpr int kXChunk = 64;     // bins per table chunk
+constexpr int kXQTile = 64;     // q values per table tile
+constexpr int kXMaxOrder = 8;   // Taylor orders at most
+// Taylor orders for q values up to qmax at bin width w: the truncation (qmax w / 2)^K / (K! (K + 1))
+// below 2^-32 of sum |H| (at least 2, at most kXMaxOrder)
+int debye_x_order(double qmax, double w);
+// (w / 2)^K 1.01^K / (K! (K + 1)): times q^K sum |H|, the truncation bound (|u| <= 1.01)
+double debye_x_trunc(int K, double w);
+size_t debye_x_table_bytes(int nq, int nch, int K);
+size_t debye_x_cpart_doubles(int nq, int nch);
+size_t debye_x_smem_bytes();
+// The digit tables of C_k(b, q) for nch chunks of bins and every q (device q[nq]) and the per-chunk
+// column sums of |C_k| (cpart [nch][ceil(nq / 64) * 64])
+void debye_x_table_launch(const double* q, int nq, double w, int nch, int K, unsigned char* table, double* cpart,
+                          cudaStream_t s);
+// The contraction for n_rows rows (M tiles of 128 consecutive rows), splits K splits of cps chunks each
+bool debye_x_launch(const XRow* rows, int n_rows, const double* q, int nq, const unsigned char* table, int nch, int K,
+                    double w, int cps, int splits, int32_t* error_flag, cudaStream_t s);
 // K splits for a contraction of up to `bins` bins, R rows, nq q values and `groups` distance axes
 // (fills the SMs once)
 int debye_tc_splits(int R, int bins, int nq, int sms, int groups);

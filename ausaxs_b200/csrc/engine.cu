@@ -591,6 +591,7 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
         rd[T * T + 2 * T + 2] = {0, kRowWW, kWater, kWater};
     }
     AUSAXS_CUDA(cudaMemcpyAsync(base + P.off_rows, rd.data(), sizeof(RowDesc) * R, cudaMemcpyHostToDevice, C.stream));
+    P.rows_host = rd;
     return P;
 }
 

@@ -92,6 +92,7 @@ struct Plan {
     FinalizeFF fin_ff{};
     FinalizeMT fin_mt{};
     std::vector<JobSpec> specs;  // the structure's passes (tiled by append_pair_jobs)
+    std::vector<RowDesc> rows_host;  // the Debye rows (device copy at off_rows)
     int max_group_rows = 1;      // rows that fit on chip at once (for 512-point tiles)
     // tensor-core scratch
     DevBuf tc;

@@ -545,10 +545,16 @@ class BatchedProfiles:
         self._b.set_points([p[0] for p in parts], [p[1] for p in parts], z)
         self.molecules = molecules
 
-    def debye_transform(self, q=None, cw=1.0, cx=1.0, crho=1.0, dw_atomic=0.0, dw_exv=0.0, grid_width=1.0):
-        """[n][nq] I(q) of every molecule (FP64 transform)."""
+    def debye_transform(self, q=None, cw=1.0, cx=1.0, crho=1.0, dw_atomic=0.0, dw_exv=0.0, grid_width=1.0,
+                        precision=1, tolerance=1e-4):
+        """[n][nq] I(q) of every molecule: FP64 transform (precision 1), or the exact-accumulation
+        tensor-core transform with FP64 for every q whose error bound exceeds tolerance (0 or 2)."""
         q = default_q_axis() if q is None else np.ascontiguousarray(q, np.float64)
-        return self._b.profile(q, DebyeParams(cw, cx, crho, dw_atomic, dw_exv, grid_width, 1, 1e-5))
+        return self._b.profile(q, DebyeParams(cw, cx, crho, dw_atomic, dw_exv, grid_width, precision, tolerance))
+
+    def fp64_columns(self) -> int:
+        """(molecule, q) values of the last transform recomputed in FP64."""
+        return self._b.fp64_columns()
 
     def histogram(self, i: int) -> dict:
         """Molecule i's histograms from the last transform: raw aa/aw/ww counts by form factor and axes."""

@@ -226,13 +226,18 @@ AUSAXS_API int ausaxs_gpu_structure_histogram(ausaxs_gpu_ctx* ctx, ausaxs_gpu_st
  *   (times_ms may be null).  ausaxs_gpu_batch_candidate describes a candidate.
  * ausaxs_gpu_batch_profile_device: q and Iq[n_structures * n_q] are device pointers; enqueues one
  *   graph launch on the context's stream (the graph is captured on the first call and again when
- *   q, Iq, n_q or the parameters change).  The transform is FP64 for every q; params->precision is
- *   not used.  Any bin overflow in the batch makes every Iq NaN.
+ *   q, Iq, n_q or the parameters change).  params->precision 1: FP64 transform for every q; 0 or 2:
+ *   the exact-accumulation tensor-core transform (int8 digit products of the histogram rows and of
+ *   shared Taylor tables of sinc, s32 sums) with a rigorous error bound per q, and the FP64
+ *   transform for every q whose bound exceeds params->tolerance times |I(q)|.  Any bin overflow in
+ *   the batch makes every Iq NaN.
  * ausaxs_gpu_batch_profile: host q and Iq (synchronises; bin overflow is an error).
  * ausaxs_gpu_batch_pair_time: device milliseconds of the pair stage (accumulator clearing and every
  *   pair launch) of the last profile, from events recorded inside the captured graph (waits for it).
  * ausaxs_gpu_batch_histogram: structure `index`'s histograms from the last profile, as
  *   ausaxs_gpu_structure_histogram.
+ * ausaxs_gpu_batch_fp64_columns: (structure, q) values of the last profile that the FP64 transform
+ *   recomputed because their tensor-core error bound exceeded the tolerance (waits for the profile).
  * ausaxs_gpu_batch_set_points (FFAVG batches): new x, y, z for every atom and water, in the creation
  *   layout (same offsets, so the same arrays' shapes); each atom's form-factor type must be the one it
  *   was created with; z_exv (host, n_structures values, may be null: kept) replaces the FFAVG
@@ -260,6 +265,7 @@ AUSAXS_API int ausaxs_gpu_batch_profile(ausaxs_gpu_batch* b, const double* q, in
                                         const ausaxs_debye_params* params, double* Iq);
 AUSAXS_API int ausaxs_gpu_batch_pair_time(ausaxs_gpu_batch* b, double* ms);
 AUSAXS_API int ausaxs_gpu_batch_histogram(ausaxs_gpu_batch* b, int32_t index, ausaxs_hist_result* out);
+AUSAXS_API int ausaxs_gpu_batch_fp64_columns(ausaxs_gpu_batch* b, int64_t* n);
 AUSAXS_API int ausaxs_gpu_batch_set_points(ausaxs_gpu_batch* b, const float* atoms, const float* waters,
                                            const double* z_exv, int32_t host_pointers);
 

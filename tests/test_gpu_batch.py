@@ -186,3 +186,42 @@ def test_set_points_device_arrays(gpu_ctx):
     If = hist.BatchedProfiles(new, bin_width=0.25, ctx=gpu_ctx).debye_transform(q)
     np.testing.assert_allclose(I, If, rtol=1e-13, atol=0)
     B.close()
+
+
+@pytest.mark.parametrize("grid", [False, True])
+def test_batch_tensor_core_transform_within_tolerance(gpu_ctx, grid):
+    """The exact-accumulation tensor-core transform (int8 digit products of the histogram rows and of
+    shared Taylor tables, s32 sums) against the FP64 transform of the same histograms: within the
+    tolerance wherever it keeps its own value, equal wherever it fell back."""
+    sizes = [300, 2600, 40, 9000, 1200, 700] if not grid else [400, 1500, 90]
+    mols = _molecules(800, sizes, exv=700 if grid else 0)
+    w = 0.1 if grid else 0.25
+    q = np.linspace(0.005, 1.0 if grid else 0.8, 333)
+    B = hist.BatchedProfiles(mols, grid=grid, bin_width=w, ctx=gpu_ctx)
+    I64 = B.debye_transform(q, cw=1.1, cx=0.95)
+    Itc = B.debye_transform(q, cw=1.1, cx=0.95, precision=2, tolerance=1e-4)
+    fell_back = B.fp64_columns()
+    rel = np.abs(Itc / I64 - 1)
+    assert np.max(rel) <= 1e-4, float(np.max(rel))
+    # the bound is rigorous and tight enough that almost every value stays on the tensor cores
+    assert fell_back <= 0.05 * Itc.size, fell_back
+    # the actual deviation is far below the tolerance (integer sums, 42-bit digits, 2^-32 truncation)
+    assert np.median(rel) < 1e-8, float(np.median(rel))
+    # a tolerance nothing meets: every value recomputed in FP64, identical to the FP64 transform
+    Iall = B.debye_transform(q, cw=1.1, cx=0.95, precision=2, tolerance=1e-300)
+    assert B.fp64_columns() == Itc.size
+    np.testing.assert_array_equal(Iall, I64)
+    B.close()
+
+
+def test_batch_tensor_core_transform_after_set_points(gpu_ctx):
+    mols = _molecules(900, [500, 3000, 150])
+    q = np.linspace(0.005, 0.8, 200)
+    B = hist.BatchedProfiles(mols, bin_width=0.25, ctx=gpu_ctx)
+    B.debye_transform(q, precision=2)
+    new = _moved(mols, 3)
+    B.set_molecules(new)
+    Itc = B.debye_transform(q, precision=2)
+    I64 = hist.BatchedProfiles(new, bin_width=0.25, ctx=gpu_ctx).debye_transform(q)
+    assert np.max(np.abs(Itc / I64 - 1)) <= 1e-4
+    B.close()
