@@ -330,7 +330,14 @@ struct Batch {
         X.w = cfg.bin_width;
         X.K = debye_x_order(qmax, X.w);
         X.nch = std::max(1, (max_nb + kXChunk - 1) / kXChunk);
-        X.cps = std::max(1, std::min(X.nch, 60000 / (kXChunk * X.K)));  // exact s32 sums
+        // splits of the chunk range: at most debye_x_max_chunks per split (exact s32 sums), and
+        // enough of them for two CTAs per SM
+        long long n_rows = 0;
+        for (auto& S : items) n_rows += S->plan.R;
+        const long long tiles = (long long)((nq + kXQTile - 1) / kXQTile) * ((n_rows + 127) / 128);
+        int splits = (X.nch + debye_x_max_chunks(X.K) - 1) / debye_x_max_chunks(X.K);
+        while (splits < X.nch && tiles * splits < 2LL * ctx->sm_count) ++splits;
+        X.cps = (X.nch + splits - 1) / splits;
         X.splits = (X.nch + X.cps - 1) / X.cps;
         X.table.ensure(debye_x_table_bytes(nq, X.nch, X.K));
         const size_t ncp = debye_x_cpart_doubles(nq, X.nch);

@@ -116,6 +116,8 @@ constexpr int kXMaxOrder = 8;   // Taylor orders at most
 int debye_x_order(double qmax, double w);
 // (w / 2)^K 1.01^K / (K! (K + 1)): times q^K sum |H|, the truncation bound (|u| <= 1.01)
 double debye_x_trunc(int K, double w);
+// chunks one split may hold for K orders (its s32 sums stay exact)
+int debye_x_max_chunks(int K);
 size_t debye_x_table_bytes(int nq, int nch, int K);
 size_t debye_x_cpart_doubles(int nq, int nch);
 size_t debye_x_smem_bytes();

@@ -14,10 +14,10 @@
 // is the histogram row times powers of the in-bin offsets.
 //
 // Both operands are fixed-point numbers, one power-of-two scale per row (left) and a fixed scale 2 for
-// the table, cut into six signed base-128 digits (int8; Ozaki-style splitting).  tcgen05.mma
+// the table, cut into six base-128 digits, the leading one signed (int8; Ozaki-style splitting).  tcgen05.mma
 // kind::i8 adds the digit products of equal weight 2^-7(i+j+2) (i + j <= 5: 21 of the 36 pairs) into
 // six s32 accumulators in tensor memory.  Integer accumulation is exact, so the value's error is the
-// digit representation (2^-43 of a scale), the dropped pairs (2^-40.7 of the row scale per product)
+// digit representation (2^-43 of a scale), the dropped pairs (2^-38.67 of the row scale per product)
 // and the truncation R_K, each bounded per (row, q); the FP64 epilogue (debye.cu) adds the bounds up
 // and recomputes a q value in FP64 only when they exceed the tolerance.
 //
@@ -26,11 +26,11 @@
 //     so one bulk copy stages a (chunk, order) step; c_k from its power series below x = 2 and from
 //     the product of the series of sin(x + t) and 1 / (x + t) above;
 //   * contraction (debye_x_kernel): a CTA owns 128 rows x 64 q values of one split (a range of
-//     chunks).  Per (chunk, order): one thread starts the table block's bulk copy, every thread
-//     digitises H u^k for half a chunk of one row (an int64 fixed-point value, then six digits)
-//     into six tiles [128 rows x 64 bins], one thread issues the 42 MMAs (two K steps of 32) and
-//     commits them to an mbarrier.  Epilogue: tcgen05.ld of the six accumulators, sum_s D_s 2^-7(s+2)
-//     times the scales in FP64.  Every wait is bounded; on timeout the kernel records an error flag,
+//     chunks).  Per chunk the rows' H and u are staged in shared memory; per order k one thread
+//     starts the table block's bulk copy, every thread digitises H u^k for half a chunk of one row
+//     into six tiles [128 rows x 64 bins] and multiplies its staged values by u for the next order,
+//     one thread issues the 42 MMAs (two K steps of 32) and commits them to an mbarrier.  Epilogue:
+//     tcgen05.ld of the six accumulators, sum_s D_s 2^-7(s+2) times the scales in FP64.  Every wait is bounded; on timeout the kernel records an error flag,
 //     waits (bounded) for its copies and MMAs, frees its tensor memory and returns, and the epilogue
 //     takes FP64 for every q.
 #include <algorithm>
@@ -51,7 +51,7 @@ constexpr int kBTile = kXN * kXB;          // one digit tile of the table (4 KiB
 constexpr int kBBlock = kDigits * kBTile;  // one (q tile, chunk, order) block of the table (24 KiB)
 constexpr int kXTmemCols = 512;            // six accumulators of 64 columns
 constexpr unsigned kXSpin = 1u << 22;
-constexpr int kMaxKSteps = 75000;          // |D_s| < 28,608 per K element: s32-exact below this many
+constexpr int kMaxKSteps = 21000;          // |D_s| <= 6 * 128^2 per K element: s32-exact below 21,845
 
 __constant__ double c_inv_fact[20] = {1.0,
                                       1.0,
@@ -148,17 +148,19 @@ __device__ __forceinline__ void tmem_ld32i(uint32_t addr, int (&out)[32]) {
     for (int j = 0; j < 32; ++j) out[j] = static_cast<int>(v[j]);
 }
 
-// Six signed base-128 digits of X (|X| < 127.5 * 2^35): X = sum_i d_i 128^(5 - i), |d_i| <= 64 for
-// i > 0 (balanced remainders from the least significant end; X - d is a multiple of 128)
-__device__ __forceinline__ void digits6(long long X, int (&d)[kDigits]) {
-#pragma unroll
-    for (int i = kDigits - 1; i > 0; --i) {
-        int v = static_cast<int>(X & 127);
-        v -= v >= 64 ? 128 : 0;
-        d[i] = v;
-        X = (X - v) >> 7;
-    }
-    d[0] = static_cast<int>(X);
+// Six base-128 digits of X = rint(v), |v| < 127.5 * 2^35: X = sum_i d_i 2^(7 (5 - i)) with d_0 =
+// floor(X / 2^35) in [-128, 127] and d_1..d_5 in [0, 127], each an int8.  rint through the FP64
+// magic number 1.5 * 2^52, whose bit pattern then holds X in its low 52 bits.
+__device__ __forceinline__ void digits6(double v, int (&d)[kDigits]) {
+    const long long bits = __double_as_longlong(v + 6755399441055744.0);
+    const unsigned lo = static_cast<unsigned>(bits);
+    const int hi = static_cast<int>(bits >> 32) - 0x43380000;  // X >> 32
+    d[5] = static_cast<int>(lo & 127u);
+    d[4] = static_cast<int>((lo >> 7) & 127u);
+    d[3] = static_cast<int>((lo >> 14) & 127u);
+    d[2] = static_cast<int>((lo >> 21) & 127u);
+    d[1] = static_cast<int>(__funnelshift_r(lo, static_cast<unsigned>(hi), 28) & 127u);
+    d[0] = hi >> 3;
 }
 
 // c_k(x) = sinc^(k)(x) / k! for x >= 0; sx, cx = sin x, cos x
@@ -219,7 +221,7 @@ __global__ void __launch_bounds__(256) debye_x_table_kernel(const double* q, int
             asum += fabs(C);
             // C / 2 in fixed point with 42 fraction bits (|C| <= 1)
             int d[kDigits];
-            digits6(__double2ll_rn(C * 0x1p41), d);
+            digits6(C * 0x1p41, d);
 #pragma unroll
             for (int j = 0; j < kDigits; ++j)
                 pack[j][e >> 2] |= (static_cast<uint32_t>(d[j]) & 0xffu) << (8 * (e & 3));
@@ -256,6 +258,9 @@ __global__ void __launch_bounds__(kXThreads, 1) debye_x_kernel(XParams P) {
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char* Abuf = smem;                     // kDigits tiles [128 rows x 64 bins]
     unsigned char* Bbuf = smem + kDigits * kATile;  // one table block: kDigits tiles [64 q x 64 bins]
+    // the chunk's H u^k and u, [64 bins][128 rows] (consecutive rows in consecutive banks)
+    double* s_hu = reinterpret_cast<double*>(smem + kDigits * kATile + kBBlock);
+    double* s_u = s_hu + kXB * kXM;
     __shared__ __align__(8) unsigned long long bar_b, bar_m;
     __shared__ uint32_t s_tmem;
     __shared__ int s_fail, s_nch;
@@ -315,7 +320,7 @@ __global__ void __launch_bounds__(kXThreads, 1) debye_x_kernel(XParams P) {
         ha += s_hpart[m];
         double A = 0, mul = 0;
         if (mx > 0) {
-            // A = 2^e > mx * 128 / 126: the leading digit stays within [-127, 127]
+            // A = 2^e > mx * 128 / 126: the leading digit stays within [-128, 127]
             const int e = ilogb(mx * (128.0 / 126.0) * (1.0 + 0x1p-30)) + 1;
             A = ldexp(1.0, e);
             mul = ldexp(1.0, 42 - e);
@@ -346,34 +351,42 @@ __global__ void __launch_bounds__(kXThreads, 1) debye_x_kernel(XParams P) {
     bool first = true;
     int pending = 0;  // 1: a table copy may be in flight, 2: MMAs may be in flight
     for (int c = c_lo; c < c_hi; ++c) {
+        // ---- the chunk's H (order 0) and u of row m, bins [32 half, 32 half + 32) ----
+        // (the previous chunk's MMAs completed before the last barrier, so the buffers are free)
+#pragma unroll 4
+        for (int e = 0; e < 32; ++e) {
+            const int bl = half * 32 + e, b = c * kXB + bl;
+            double h = 0, u = 0;
+            if (b < b_hi) {
+                h = R.H[b];
+                u = (R.axis[b] - b * P.w) * two_w;
+            }
+            s_hu[bl * kXM + m] = h * mul;  // H in units of 2^-42 A
+            s_u[bl * kXM + m] = u;
+        }
         for (int k = 0; k < P.K; ++k) {
             if (tid == 0) xbulk(Bbuf, tq + (static_cast<size_t>(c) * P.K + k) * kBBlock, kBBlock, &bar_b);
-            // ---- digits of H u^k: row m, bins [32 half, 32 half + 32) of the chunk ----
+            // ---- digits of H u^k, then H u^(k+1) for the next order ----
 #pragma unroll 1
             for (int g = 0; g < 2; ++g) {
-                const int bl = half * 32 + g * 16;
+                const int bl0 = half * 32 + g * 16;
                 uint32_t pack[kDigits][4];
 #pragma unroll
                 for (int j = 0; j < kDigits; ++j) pack[j][0] = pack[j][1] = pack[j][2] = pack[j][3] = 0;
-#pragma unroll 4
+#pragma unroll
                 for (int e = 0; e < 16; ++e) {
-                    const int b = c * kXB + bl + e;
-                    double a = 0;
-                    if (b < b_hi) {
-                        const double u = (R.axis[b] - b * P.w) * two_w;
-                        double uk = 1.0;
-                        for (int j = 0; j < k; ++j) uk *= u;
-                        a = R.H[b] * uk;
-                    }
+                    const int i = (bl0 + e) * kXM + m;
+                    const double v = s_hu[i];
+                    s_hu[i] = v * s_u[i];
                     int d[kDigits];
-                    digits6(__double2ll_rn(a * mul), d);
+                    digits6(v, d);
 #pragma unroll
                     for (int j = 0; j < kDigits; ++j)
                         pack[j][e >> 2] |= (static_cast<uint32_t>(d[j]) & 0xffu) << (8 * (e & 3));
                 }
 #pragma unroll
                 for (int j = 0; j < kDigits; ++j)
-                    *reinterpret_cast<uint4*>(Abuf + j * kATile + xoff(kXM, m, bl)) =
+                    *reinterpret_cast<uint4*>(Abuf + j * kATile + xoff(kXM, m, bl0)) =
                         make_uint4(pack[j][0], pack[j][1], pack[j][2], pack[j][3]);
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -448,12 +461,13 @@ __global__ void __launch_bounds__(kXThreads, 1) debye_x_kernel(XParams P) {
                     if (qi < P.nq) Rr.out[z * Rr.out_z + qi] = acc[j] * A2;
                 }
                 if (qt == 0 && cb == 0) {
-                    // per element: digits of H u^k within 2^-43 A, of C_k within 2^-42; dropped digit
-                    // pairs (i + j >= 6) below 2^-40.67 A; sum_k |H u^k| <= K 1.01^(K-1) sum |H|
+                    // per element: digits of H u^k within 2^-43 A (one rounding of the fixed-point
+                    // value; the staged H u^k carry 2^-52 relative more), of C_k within 2^-42; dropped
+                    // digit pairs (i + j >= 6) below 2^-38.67 A; sum_k |H u^k| <= K 1.01^(K-1) sum |H|
                     const double nK = static_cast<double>(c_hi - c_lo) * kXB * P.K;
                     const double hs = s_hpart[rm];
-                    Rr.e1[z * Rr.e_z] = s_part[rm] * 0x1p-43;
-                    Rr.e0[z * Rr.e_z] = s_part[rm] * nK * 0x1p-40 + 0x1p-41 * 1.1 * P.K * hs;
+                    Rr.e1[z * Rr.e_z] = s_part[rm] * 0x1p-42;
+                    Rr.e0[z * Rr.e_z] = s_part[rm] * nK * 0x1p-38 + 0x1p-41 * 1.1 * P.K * hs;
                     Rr.habs[z * Rr.e_z] = hs;
                 }
             }
@@ -487,13 +501,17 @@ double debye_x_trunc(int K, double w) {
     return std::pow(w * 0.5 * 1.01, K) / (f * (K + 1));
 }
 
+int debye_x_max_chunks(int K) { return std::max(1, kMaxKSteps / (kXB * std::max(1, K))); }
+
 size_t debye_x_table_bytes(int nq, int nch, int K) {
     return static_cast<size_t>((nq + kXN - 1) / kXN) * nch * K * kBBlock;
 }
 
 size_t debye_x_cpart_doubles(int nq, int nch) { return static_cast<size_t>((nq + kXN - 1) / kXN) * kXN * nch; }
 
-size_t debye_x_smem_bytes() { return static_cast<size_t>(kDigits) * kATile + kBBlock + 1024; }
+size_t debye_x_smem_bytes() {
+    return static_cast<size_t>(kDigits) * kATile + kBBlock + 2 * sizeof(double) * kXB * kXM + 1024;
+}
 
 void debye_x_table_launch(const double* q, int nq, double w, int nch, int K, unsigned char* table, double* cpart,
                           cudaStream_t s) {
