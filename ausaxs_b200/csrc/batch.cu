@@ -108,9 +108,8 @@ struct Batch {
     // left-operand rows of all structures (largest first), per-structure partial sums and bound terms
     struct XState {
         bool on = false;
-        int K = 0, nch = 0, cps = 0, splits = 0, n_rows = 0;
-        double w = 0;
-        DevBuf table, cpart, rows, planes, err;
+        XPlan plan{};
+        DevBuf table, cpart, rows, planes, flags, qcache, adig, tile_off, row_scale;
     } x;
     DevBuf d_stats;                      // census of every structure (creation only)
     DevBuf arena;                        // every structure's point arrays
@@ -327,44 +326,49 @@ struct Batch {
         double qmax = 0;
         for (double v : hq) qmax = std::max(qmax, std::fabs(v));
         XState& X = x;
-        X.w = cfg.bin_width;
-        X.K = debye_x_order(qmax, X.w);
-        X.nch = std::max(1, (max_nb + kXChunk - 1) / kXChunk);
+        XPlan& XP = X.plan;
+        XP.w = cfg.bin_width;
+        XP.nq = nq;
+        XP.K = debye_x_order(qmax, XP.w);
+        XP.nch = std::max(1, (max_nb + kXChunk - 1) / kXChunk);
         // splits of the chunk range: at most debye_x_max_chunks per split (exact s32 sums), and
         // enough of them for two CTAs per SM
         long long n_rows = 0;
         for (auto& S : items) n_rows += S->plan.R;
         const long long tiles = (long long)((nq + kXQTile - 1) / kXQTile) * ((n_rows + 127) / 128);
-        int splits = (X.nch + debye_x_max_chunks(X.K) - 1) / debye_x_max_chunks(X.K);
-        while (splits < X.nch && tiles * splits < 2LL * ctx->sm_count) ++splits;
-        X.cps = (X.nch + splits - 1) / splits;
-        X.splits = (X.nch + X.cps - 1) / X.cps;
-        X.table.ensure(debye_x_table_bytes(nq, X.nch, X.K));
-        const size_t ncp = debye_x_cpart_doubles(nq, X.nch);
+        int splits = (XP.nch + debye_x_max_chunks(XP.K) - 1) / debye_x_max_chunks(XP.K);
+        while (splits < XP.nch && tiles * splits < 2LL * ctx->sm_count) ++splits;
+        XP.cps = (XP.nch + splits - 1) / splits;
+        XP.splits = (XP.nch + XP.cps - 1) / XP.cps;
+        X.table.ensure(debye_x_table_bytes(nq, XP.nch, XP.K));
+        const size_t ncp = debye_x_cpart_doubles(nq, XP.nch);
         X.cpart.ensure(sizeof(double) * ncp);
-        const int nqp = (int)(ncp / X.nch);
+        const int nqp = (int)(ncp / XP.nch);
+        X.qcache.ensure(sizeof(double) * nq);
+        AUSAXS_CUDA(cudaMemset(X.qcache.p, 0xff, sizeof(double) * nq));  // NaN: the tables are made on first use
+        X.flags.ensure(256);
+        AUSAXS_CUDA(cudaMemset(X.flags.p, 0, 256));
         // per structure: values [splits][R][nq], then e1, e0, habs [splits][R]
         std::vector<size_t> at(items.size());
         size_t total = 0;
         for (size_t i = 0; i < items.size(); ++i) {
             at[i] = total;
             const size_t R = items[i]->plan.R;
-            total += align_up((size_t)X.splits * R * nq + 3 * (size_t)X.splits * R, 32);
+            total += align_up((size_t)XP.splits * R * nq + 3 * (size_t)XP.splits * R, 32);
         }
         X.planes.ensure(sizeof(double) * std::max<size_t>(1, total));
-        X.err.ensure(256);
-        AUSAXS_CUDA(cudaMemset(X.err.p, 0, 256));
         double* base = X.planes.as<double>();
         std::vector<XRow> rows;
+        std::vector<int> row_chunks;  // chunk bound of each row (its plan's bins)
         for (int i : order) {
             Structure& S = *items[i];
             Plan& P = S.plan;
             const int R = P.R;
             char* pb = P.dev.as<char>();
             double* v = base + at[i];
-            double* e1 = v + (size_t)X.splits * R * nq;
-            double* e0 = e1 + (size_t)X.splits * R;
-            double* ha = e0 + (size_t)X.splits * R;
+            double* e1 = v + (size_t)XP.splits * R * nq;
+            double* e0 = e1 + (size_t)XP.splits * R;
+            double* ha = e0 + (size_t)XP.splits * R;
             const double* axes[3] = {reinterpret_cast<const double*>(pb + P.off_d),
                                      reinterpret_cast<const double*>(pb + P.off_dax),
                                      reinterpret_cast<const double*>(pb + P.off_dxx)};
@@ -382,23 +386,46 @@ struct Batch {
                 xr.out_z = (long long)R * nq;
                 xr.e_z = R;
                 rows.push_back(xr);
+                row_chunks.push_back((P.nb + kXChunk - 1) / kXChunk);
             }
             DebyeArgs& a = A[i];
             a.x_v = v;
             a.x_e1 = e1;
             a.x_e0 = e0;
             a.x_habs = ha;
-            a.x_splits = X.splits;
+            a.x_splits = XP.splits;
             a.x_cpart = X.cpart.as<double>();
-            a.x_nch = X.nch;
+            a.x_nch = XP.nch;
             a.x_nqp = nqp;
-            a.x_K = X.K;
-            a.x_ctr = debye_x_trunc(X.K, X.w);
-            a.tc_error = X.err.as<int32_t>();
+            a.x_K = XP.K;
+            a.x_ctr = debye_x_trunc(XP.K, XP.w);
+            a.tc_error = X.flags.as<int32_t>() + 1;
         }
-        X.n_rows = (int)rows.size();
+        XP.n_rows = (int)rows.size();
         X.rows.ensure(sizeof(XRow) * std::max<size_t>(1, rows.size()));
         AUSAXS_CUDA(cudaMemcpy(X.rows.p, rows.data(), sizeof(XRow) * rows.size(), cudaMemcpyHostToDevice));
+        // the rows' digit blocks: per M tile, its rows' largest chunk bound (capped by the table's)
+        const int n_tiles = (XP.n_rows + 127) / 128;
+        std::vector<long long> toff(n_tiles);
+        long long adig = 0;
+        for (int t = 0; t < n_tiles; ++t) {
+            int ch = 0;
+            for (int r = t * 128; r < std::min(XP.n_rows, (t + 1) * 128); ++r) ch = std::max(ch, row_chunks[r]);
+            toff[t] = adig;
+            adig += (long long)std::min(ch, XP.nch) * XP.K * (long long)debye_x_block_bytes();
+        }
+        X.adig.ensure((size_t)std::max<long long>(256, adig));
+        X.tile_off.ensure(sizeof(long long) * n_tiles);
+        AUSAXS_CUDA(cudaMemcpy(X.tile_off.p, toff.data(), sizeof(long long) * n_tiles, cudaMemcpyHostToDevice));
+        X.row_scale.ensure(sizeof(double) * XP.n_rows);
+        XP.rows = X.rows.as<XRow>();
+        XP.table = X.table.as<unsigned char>();
+        XP.cpart = X.cpart.as<double>();
+        XP.q_cached = X.qcache.as<double>();
+        XP.flags = X.flags.as<int32_t>();
+        XP.adig = X.adig.as<unsigned char>();
+        XP.tile_off = X.tile_off.as<long long>();
+        XP.row_scale = X.row_scale.as<double>();
         X.on = true;
     }
 
@@ -411,11 +438,7 @@ struct Batch {
         ff_finalize_batch_launch(fin.as<FinalizeFF>(), (int)items.size(), max_nb, s);
         ctx->check_launch("finalize");
         if (x.on) {
-            debye_x_table_launch(q, nq, x.w, x.nch, x.K, x.table.as<unsigned char>(), x.cpart.as<double>(), s);
-            ctx->check_launch("debye_x_table");
-            if (!debye_x_launch(x.rows.as<XRow>(), x.n_rows, q, nq, x.table.as<unsigned char>(), x.nch, x.K, x.w, x.cps,
-                                x.splits, x.err.as<int32_t>(), s))
-                throw Error{AUSAXS_ERR_CUDA, "cannot launch the tensor-core Debye transform"};
+            if (!debye_x_enqueue(x.plan, q, s)) throw Error{AUSAXS_ERR_CUDA, "cannot launch the tensor-core Debye transform"};
             ctx->check_launch("debye_x");
         }
         int max_R = 1;

@@ -55,7 +55,7 @@ struct DebyeArgs {
     double* tc_err_est;         // out: [nq] estimated relative error of the tensor-core I(q) (may be null)
     double* Iq;                 // [nq]
     double* profiles;           // [6][nq] or null
-    // exact-accumulation tensor-core partial sums from debye_x_launch, or null (debye_x.cu):
+    // exact-accumulation tensor-core partial sums from debye_x_enqueue, or null (debye_x.cu):
     //   x_v [x_splits][R][nq] (FP64 values), x_e1 / x_e0 / x_habs [x_splits][R] (bound terms: the error of
     //   a split's value is at most x_e1 * Csum(q) + x_e0, Csum(q) = sum_c x_cpart[c][q] over x_nch
     //   table chunks), and the Taylor truncation x_ctr * q^x_K * sum_z x_habs
@@ -93,6 +93,15 @@ struct TcArgs {
     int32_t* error_flag;
 };
 bool debye_tc_launch(const TcArgs& A, cudaStream_t s);
+// K splits for a contraction of up to `bins` bins, R rows, nq q values and `groups` distance axes
+// (fills the SMs once)
+int debye_tc_splits(int R, int bins, int nq, int sms, int groups);
+// bins of one K split when max_bin bins are in use (multiple of the 64-bin staging chunk)
+__host__ __device__ inline int debye_tc_split_bins(int max_bin, int splits) {
+    const int chunks = (max_bin + 63) / 64;
+    return ((chunks + splits - 1) / splits) * 64;
+}
+size_t debye_tc_smem_bytes();
 
 // Exact-accumulation tensor-core contraction over shared Taylor tables (debye_x.cu).
 // One left-operand row: a histogram row of some structure and where its partial sums go.
@@ -120,22 +129,23 @@ double debye_x_trunc(int K, double w);
 int debye_x_max_chunks(int K);
 size_t debye_x_table_bytes(int nq, int nch, int K);
 size_t debye_x_cpart_doubles(int nq, int nch);
-size_t debye_x_smem_bytes();
-// The digit tables of C_k(b, q) for nch chunks of bins and every q (device q[nq]) and the per-chunk
-// column sums of |C_k| (cpart [nch][ceil(nq / 64) * 64])
-void debye_x_table_launch(const double* q, int nq, double w, int nch, int K, unsigned char* table, double* cpart,
-                          cudaStream_t s);
-// The contraction for n_rows rows (M tiles of 128 consecutive rows), splits K splits of cps chunks each
-bool debye_x_launch(const XRow* rows, int n_rows, const double* q, int nq, const unsigned char* table, int nch, int K,
-                    double w, int cps, int splits, int32_t* error_flag, cudaStream_t s);
-// K splits for a contraction of up to `bins` bins, R rows, nq q values and `groups` distance axes
-// (fills the SMs once)
-int debye_tc_splits(int R, int bins, int nq, int sms, int groups);
-// bins of one K split when max_bin bins are in use (multiple of the 64-bin staging chunk)
-__host__ __device__ inline int debye_tc_split_bins(int max_bin, int splits) {
-    const int chunks = (max_bin + 63) / 64;
-    return ((chunks + splits - 1) / splits) * 64;
-}
-size_t debye_tc_smem_bytes();
+// bytes of the rows' digit block of one (M tile, chunk, order)
+size_t debye_x_block_bytes();
+// Device buffers and shape of one contraction (rows in M tiles of 128 consecutive rows).
+struct XPlan {
+    const XRow* rows;
+    int n_rows, nq, nch, K, cps, splits;
+    double w;
+    unsigned char* table;      // debye_x_table_bytes(nq, nch, K)
+    double* cpart;             // debye_x_cpart_doubles(nq, nch): per chunk and q, sum_{k, b} |C_k(b, q)|
+    double* q_cached;          // [nq]: the q the tables were made for (NaN: none yet)
+    int32_t* flags;            // [0] tables stale, [1] error (sticky: every later transform in FP64)
+    unsigned char* adig;       // the rows' digit blocks: tile t, chunk c, order k at tile_off[t] + (c K + k) block
+    const long long* tile_off;  // [M tiles]
+    double* row_scale;         // [n_rows]
+};
+// q check and tables (rebuilt only when q changed), row scales and bound terms, the rows' digits and
+// the contraction, on stream s; false when a launch could not be made
+bool debye_x_enqueue(const XPlan& X, const double* q, cudaStream_t s);
 
 }  // namespace ausaxs_b200

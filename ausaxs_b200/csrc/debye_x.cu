@@ -22,17 +22,19 @@
 // and recomputes a q value in FP64 only when they exceed the tolerance.
 //
 //   * tables (debye_x_table_kernel): for each q tile of 64 q values, chunk of 64 bins and order k, six
-//     digit tiles [64 q x 64 bins] in the no-swizzle K-major core-matrix layout, contiguous (24 KiB),
-//     so one bulk copy stages a (chunk, order) step; c_k from its power series below x = 2 and from
-//     the product of the series of sin(x + t) and 1 / (x + t) above;
+//     digit tiles [64 q x 64 bins] in the no-swizzle K-major core-matrix layout, contiguous (24 KiB);
+//     c_k from its power series below x = 2 and from the product of the series of sin(x + t) and
+//     1 / (x + t) above.  Rebuilt only when the q values change (debye_x_qcheck_kernel);
+//   * rows (debye_x_rowstat_kernel, debye_x_digits_kernel): each row's power-of-two scale and bound
+//     terms, then for every (M tile of 128 rows, chunk, order) six digit tiles [128 rows x 64 bins]
+//     of H u^k (48 KiB, contiguous), made once and read by every q tile;
 //   * contraction (debye_x_kernel): a CTA owns 128 rows x 64 q values of one split (a range of
-//     chunks).  Per chunk the rows' H and u are staged in shared memory; per order k one thread
-//     starts the table block's bulk copy, every thread digitises H u^k for half a chunk of one row
-//     into six tiles [128 rows x 64 bins] and multiplies its staged values by u for the next order,
-//     one thread issues the 42 MMAs (two K steps of 32) and commits them to an mbarrier.  Epilogue:
-//     tcgen05.ld of the six accumulators, sum_s D_s 2^-7(s+2) times the scales in FP64.  Every wait is bounded; on timeout the kernel records an error flag,
-//     waits (bounded) for its copies and MMAs, frees its tensor memory and returns, and the epilogue
-//     takes FP64 for every q.
+//     chunks).  One thread streams the split's (chunk, order) steps through two stages of shared
+//     memory by bulk copies of both digit blocks and issues each step's 42 MMAs (two K steps of 32)
+//     when its copies land, so the copy of the next step overlaps them.  Epilogue: tcgen05.ld of the
+//     six accumulators, sum_s D_s 2^-7(s+2) times the scales in FP64.  Every wait is bounded; on
+//     timeout the kernel waits (bounded) for what it has in flight, frees its tensor memory and
+//     records an error flag, and the epilogue then takes FP64 for every q.
 #include <algorithm>
 #include <cmath>
 
@@ -108,14 +110,6 @@ __device__ __forceinline__ void xbar_init(unsigned long long* bar) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(xsmem(bar)) : "memory");
 }
 
-__device__ __forceinline__ void xbulk(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(xsmem(bar)), "r"(bytes) : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     xsmem(dst)),
-                 "l"(src), "r"(bytes), "r"(xsmem(bar))
-                 : "memory");
-}
-
 __device__ __forceinline__ bool xwait(unsigned long long* bar, uint32_t parity) {
     const uint32_t a = xsmem(bar);
     for (unsigned it = 0; it < kXSpin; ++it) {
@@ -163,18 +157,33 @@ __device__ __forceinline__ void digits6(double v, int (&d)[kDigits]) {
     d[0] = hi >> 3;
 }
 
+// 1 / (2n + 1) and 1 / ((m + 1)(m + 2)) for the power series of c_k
+__constant__ double c_inv_odd[32] = {
+    1.0,        1.0 / 3,  1.0 / 5,  1.0 / 7,  1.0 / 9,  1.0 / 11, 1.0 / 13, 1.0 / 15, 1.0 / 17, 1.0 / 19, 1.0 / 21,
+    1.0 / 23,   1.0 / 25, 1.0 / 27, 1.0 / 29, 1.0 / 31, 1.0 / 33, 1.0 / 35, 1.0 / 37, 1.0 / 39, 1.0 / 41, 1.0 / 43,
+    1.0 / 45,   1.0 / 47, 1.0 / 49, 1.0 / 51, 1.0 / 53, 1.0 / 55, 1.0 / 57, 1.0 / 59, 1.0 / 61, 1.0 / 63};
+__constant__ double c_inv_pair[48] = {
+    1.0 / 2,    1.0 / 6,    1.0 / 12,   1.0 / 20,   1.0 / 30,   1.0 / 42,   1.0 / 56,   1.0 / 72,
+    1.0 / 90,   1.0 / 110,  1.0 / 132,  1.0 / 156,  1.0 / 182,  1.0 / 210,  1.0 / 240,  1.0 / 272,
+    1.0 / 306,  1.0 / 342,  1.0 / 380,  1.0 / 420,  1.0 / 462,  1.0 / 506,  1.0 / 552,  1.0 / 600,
+    1.0 / 650,  1.0 / 702,  1.0 / 756,  1.0 / 812,  1.0 / 870,  1.0 / 930,  1.0 / 992,  1.0 / 1056,
+    1.0 / 1122, 1.0 / 1190, 1.0 / 1260, 1.0 / 1332, 1.0 / 1406, 1.0 / 1482, 1.0 / 1560, 1.0 / 1640,
+    1.0 / 1722, 1.0 / 1806, 1.0 / 1892, 1.0 / 1980, 1.0 / 2070, 1.0 / 2162, 1.0 / 2256, 1.0 / 2352};
+
 // c_k(x) = sinc^(k)(x) / k! for x >= 0; sx, cx = sin x, cos x
 __device__ double sinc_coeff(double x, int k, double sx, double cx) {
     if (x < 2.0) {
         // sinc(x) = sum_n (-1)^n x^(2n) / (2n + 1)!, so c_k(x) = (1 / k!) sum_{2n >= k} (-1)^n x^(2n-k) /
-        // ((2n - k)! (2n + 1)); the terms fall below 1e-28 of the first within 18 of them
+        // ((2n - k)! (2n + 1)); with x < 2 the terms fall below 1e-20 of the first within 16 of them
         const int n0 = (k + 1) >> 1;
         int m = 2 * n0 - k;
         double t = m == 0 ? 1.0 : x;  // x^m / m!
+        const double x2 = x * x;
         double s = 0;
-        for (int n = n0; n < n0 + 18; ++n) {
-            s += ((n & 1) ? -t : t) / (2 * n + 1);
-            t *= x * x / ((m + 1) * (m + 2));
+#pragma unroll 4
+        for (int n = n0; n < n0 + 16; ++n) {
+            s += ((n & 1) ? -t : t) * c_inv_odd[n];
+            t *= x2 * c_inv_pair[m];
             m += 2;
         }
         return s * c_inv_fact[k];
@@ -191,37 +200,49 @@ __device__ double sinc_coeff(double x, int k, double sx, double cx) {
     return s;
 }
 
-// grid (q tiles, chunks); thread item = (q in tile, 16-bin group, order)
+// flags[0] = 1 when q differs bit for bit from the q the tables were made for (then copied there)
+__global__ void debye_x_qcheck_kernel(const double* q, int nq, double* q_cached, int32_t* flags) {
+    int diff = 0;
+    for (int i = threadIdx.x; i < nq; i += blockDim.x)
+        diff |= __double_as_longlong(q[i]) != __double_as_longlong(q_cached[i]);
+    diff = __syncthreads_or(diff);
+    if (diff)
+        for (int i = threadIdx.x; i < nq; i += blockDim.x) q_cached[i] = q[i];
+    if (threadIdx.x == 0) flags[0] = diff;
+}
+
+// grid (q tiles, chunks); thread = (q in tile, 16-bin group): sin and cos of its 16 arguments once,
+// then every order's digits
 __global__ void __launch_bounds__(256) debye_x_table_kernel(const double* q, int nq, double w, int nch, int K,
-                                                            unsigned char* table, double* cpart) {
-    __shared__ double s_cp[kXMaxOrder * 4][kXN];
+                                                            unsigned char* table, double* cpart,
+                                                            const int32_t* flags) {
+    if (!flags[0]) return;  // the tables hold this q grid already
+    __shared__ double s_cp[4][kXN];
     const int qt = blockIdx.x, c = blockIdx.y;
     const int nqp = gridDim.x * kXN;
-    for (int item = threadIdx.x; item < kXN * 4 * K; item += blockDim.x) {
-        const int qi = item % kXN, g = (item / kXN) % 4, k = item / (kXN * 4);
-        const int qg = qt * kXN + qi;
-        const double qv = qg < nq ? q[qg] : 0.0;
-        const double hq = qv * w * 0.5;
-        double hk = 1.0;
-        for (int j = 0; j < k; ++j) hk *= hq;  // (q w / 2)^k
+    const int qi = threadIdx.x % kXN, g = threadIdx.x / kXN;  // 256 threads: 64 q x 4 groups
+    const int qg = qt * kXN + qi;
+    const double qv = qg < nq ? q[qg] : 0.0;
+    const double hq = qv * w * 0.5;
+    double xs[16], sn[16], cs[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+        xs[e] = qv * (static_cast<double>(c * kXB + g * 16 + e) * w);
+        sn[e] = 0;
+        cs[e] = 1;
+        if (xs[e] >= 2.0) sincos(xs[e], &sn[e], &cs[e]);
+    }
+    double asum = 0, hk = 1.0;  // hk = (q w / 2)^k
+    for (int k = 0; k < K; ++k) {
         uint32_t pack[kDigits][4];
 #pragma unroll
         for (int j = 0; j < kDigits; ++j) pack[j][0] = pack[j][1] = pack[j][2] = pack[j][3] = 0;
-        double asum = 0;
-#pragma unroll 1
+#pragma unroll
         for (int e = 0; e < 16; ++e) {
-            const int b = c * kXB + g * 16 + e;
-            double C = 0;
-            if (qg < nq) {
-                const double x = qv * (static_cast<double>(b) * w);
-                double sx = 0, cx = 1;
-                if (x >= 2.0) sincos(x, &sx, &cx);
-                C = sinc_coeff(x, k, sx, cx) * hk;
-            }
+            const double C = qg < nq ? sinc_coeff(xs[e], k, sn[e], cs[e]) * hk : 0.0;
             asum += fabs(C);
-            // C / 2 in fixed point with 42 fraction bits (|C| <= 1)
             int d[kDigits];
-            digits6(C * 0x1p41, d);
+            digits6(C * 0x1p41, d);  // C / 2 in fixed point with 42 fraction bits (|C| <= 1)
 #pragma unroll
             for (int j = 0; j < kDigits; ++j)
                 pack[j][e >> 2] |= (static_cast<uint32_t>(d[j]) & 0xffu) << (8 * (e & 3));
@@ -231,107 +252,184 @@ __global__ void __launch_bounds__(256) debye_x_table_kernel(const double* q, int
         for (int j = 0; j < kDigits; ++j)
             *reinterpret_cast<uint4*>(blk + j * kBTile + xoff(kXN, qi, g * 16)) =
                 make_uint4(pack[j][0], pack[j][1], pack[j][2], pack[j][3]);
-        s_cp[k * 4 + g][qi] = asum;
+        hk *= hq;
+    }
+    s_cp[g][qi] = asum;
+    __syncthreads();
+    if (threadIdx.x < kXN)
+        cpart[static_cast<size_t>(c) * nqp + qt * kXN + threadIdx.x] =
+            s_cp[0][threadIdx.x] + s_cp[1][threadIdx.x] + s_cp[2][threadIdx.x] + s_cp[3][threadIdx.x];
+}
+
+// One warp per row: its scale A = 2^e > max_b |H| max(1, |u|)^(K-1) * 128 / 126 (row_scale[r]) and, per
+// split, sum |H| and the bound terms of its digit arithmetic (debye_x_kernel's epilogue):
+//   digits of H u^k within 2^-42 A (one rounding of the fixed-point value; the FP64 products H u^k
+//   add 2^-52 relative), of C_k within 2^-42 -- e1 = 2^-42 A multiplies sum |C_k(b, q)|;
+//   dropped digit pairs (i + j >= 6) below 2^-38.67 A per product and sum_k |H u^k| <= K 1.01^(K-1)
+//   sum |H| -- e0 = 2^-38 A n_K + 2^-41 1.1 K sum |H|, n_K the split's products of the row.
+__global__ void debye_x_rowstat_kernel(const XRow* rows, int n_rows, double w, int K, int cps, int splits,
+                                       double* row_scale) {
+    const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (r >= n_rows) return;
+    const XRow R = rows[r];
+    if (!R.H) {
+        if (lane == 0) row_scale[r] = 0;
+        return;
+    }
+    const int mb = *R.max_bin;
+    const double two_w = 2.0 / w;
+    double mx = 0;
+    for (int b = lane; b < mb; b += 32) {
+        const double u = fmax(1.0, fabs((R.axis[b] - b * w) * two_w));
+        double f = fabs(R.H[b]);
+        for (int k = 1; k < K; ++k) f *= u;
+        mx = fmax(mx, f);
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    double A = 0;
+    if (mx > 0) A = ldexp(1.0, ilogb(mx * (128.0 / 126.0) * (1.0 + 0x1p-30)) + 1);
+    if (lane == 0) row_scale[r] = A;
+    const int span = cps * kXB;
+    for (int z = 0; z < splits; ++z) {
+        const int b0 = z * span, b1 = min(mb, b0 + span);
+        double hs = 0;
+        for (int b = b0 + lane; b < b1; b += 32) hs += fabs(R.H[b]);
+        for (int o = 16; o > 0; o >>= 1) hs += __shfl_xor_sync(0xffffffffu, hs, o);
+        if (lane == 0) {
+            const double nK = b1 > b0 ? static_cast<double>((b1 - b0 + kXB - 1) / kXB) * kXB * K : 0.0;
+            R.e1[z * R.e_z] = b1 > b0 ? A * 0x1p-42 : 0.0;
+            R.e0[z * R.e_z] = A * nK * 0x1p-38 + 0x1p-41 * 1.1 * K * hs;
+            R.habs[z * R.e_z] = hs;
+        }
+    }
+}
+
+// chunks of bins an M tile needs: the largest of its rows' ceil(max_bin / 64) (CTA-wide, via shared memory)
+__device__ int tile_chunks(const XRow* rows, int n_rows, int tile, int* s_n) {
+    if (threadIdx.x == 0) *s_n = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < kXM; i += blockDim.x) {
+        const int r = tile * kXM + i;
+        if (r < n_rows && rows[r].H) atomicMax(s_n, (*rows[r].max_bin + kXB - 1) / kXB);
     }
     __syncthreads();
-    for (int qi = threadIdx.x; qi < kXN; qi += blockDim.x) {
-        double t = 0;
-        for (int i = 0; i < 4 * K; ++i) t += s_cp[i][qi];
-        cpart[static_cast<size_t>(c) * nqp + qt * kXN + qi] = t;
+    return *s_n;
+}
+
+// grid (M tiles, chunks): the digit tiles of H u^k for every order k of one (M tile, chunk), written in
+// the UMMA layout to adig + tile_off[tile] + (chunk K + k) 48 KiB
+__global__ void __launch_bounds__(kXThreads) debye_x_digits_kernel(const XRow* rows, int n_rows, double w, int K,
+                                                                   const double* row_scale,
+                                                                   const long long* tile_off, unsigned char* adig) {
+    constexpr int kPitch = kXM + 1;  // [bin][row], consecutive rows in consecutive banks
+    extern __shared__ __align__(16) unsigned char dsm[];
+    double* s_p = reinterpret_cast<double*>(dsm);  // H u^k in units of 2^-42 A
+    double* s_u = s_p + kXB * kPitch;
+    __shared__ const double* s_h[kXM];
+    __shared__ const double* s_ax[kXM];
+    __shared__ double s_mul[kXM];
+    __shared__ int s_mb[kXM];
+    __shared__ int s_n;
+    const int tile = blockIdx.x, c = blockIdx.y;
+    if (c >= tile_chunks(rows, n_rows, tile, &s_n)) return;
+    for (int i = threadIdx.x; i < kXM; i += blockDim.x) {
+        const int r = tile * kXM + i;
+        const bool on = r < n_rows && rows[r].H && row_scale[r] > 0;
+        s_h[i] = on ? rows[r].H : nullptr;
+        s_ax[i] = on ? rows[r].axis : nullptr;
+        s_mb[i] = on ? *rows[r].max_bin : 0;
+        s_mul[i] = on ? 0x1p42 / row_scale[r] : 0.0;
+    }
+    __syncthreads();
+    const double two_w = 2.0 / w;
+    for (int i = threadIdx.x; i < kXM * kXB; i += blockDim.x) {
+        const int rr = i / kXB, bl = i - rr * kXB, b = c * kXB + bl;
+        double h = 0, u = 0;
+        if (b < s_mb[rr]) {
+            h = s_h[rr][b] * s_mul[rr];
+            u = (s_ax[rr][b] - b * w) * two_w;
+        }
+        s_p[bl * kPitch + rr] = h;
+        s_u[bl * kPitch + rr] = u;
+    }
+    __syncthreads();
+    const int m = threadIdx.x & (kXM - 1), half = threadIdx.x >> 7;
+    unsigned char* base = adig + tile_off[tile] + static_cast<size_t>(c) * K * (kDigits * kATile);
+    for (int k = 0; k < K; ++k) {
+        unsigned char* blk = base + static_cast<size_t>(k) * (kDigits * kATile);
+#pragma unroll 1
+        for (int g = 0; g < 2; ++g) {
+            const int bl0 = half * 32 + g * 16;
+            uint32_t pack[kDigits][4];
+#pragma unroll
+            for (int j = 0; j < kDigits; ++j) pack[j][0] = pack[j][1] = pack[j][2] = pack[j][3] = 0;
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+                const int i = (bl0 + e) * kPitch + m;
+                const double v = s_p[i];
+                s_p[i] = v * s_u[i];
+                int d[kDigits];
+                digits6(v, d);
+#pragma unroll
+                for (int j = 0; j < kDigits; ++j)
+                    pack[j][e >> 2] |= (static_cast<uint32_t>(d[j]) & 0xffu) << (8 * (e & 3));
+            }
+#pragma unroll
+            for (int j = 0; j < kDigits; ++j)
+                *reinterpret_cast<uint4*>(blk + j * kATile + xoff(kXM, m, bl0)) =
+                    make_uint4(pack[j][0], pack[j][1], pack[j][2], pack[j][3]);
+        }
     }
 }
 
 struct XParams {
     const XRow* rows;
     int n_rows;
-    const double* q;
     int nq;
     const unsigned char* table;
-    int nch, K;
-    double w;
-    int cps;
+    const unsigned char* adig;
+    const long long* tile_off;
+    const double* row_scale;
+    int nch, K, cps;
     int32_t* error_flag;
 };
 
-// grid (q tiles, row tiles of 128, splits)
+// grid (q tiles, M tiles, splits).  One thread streams the (chunk, order) steps of the split through
+// two stages of shared memory (bulk copies of the rows' and the table's digit blocks, 72 KiB a stage)
+// and issues each step's 42 MMAs as soon as its copies land; the copy of step t + 1 overlaps the MMAs of
+// step t.  Then every warp reads its TMEM lanes and writes the FP64 values.
 __global__ void __launch_bounds__(kXThreads, 1) debye_x_kernel(XParams P) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    unsigned char* Abuf = smem;                     // kDigits tiles [128 rows x 64 bins]
-    unsigned char* Bbuf = smem + kDigits * kATile;  // one table block: kDigits tiles [64 q x 64 bins]
-    // the chunk's H u^k and u, [64 bins][128 rows] (consecutive rows in consecutive banks)
-    double* s_hu = reinterpret_cast<double*>(smem + kDigits * kATile + kBBlock);
-    double* s_u = s_hu + kXB * kXM;
-    __shared__ __align__(8) unsigned long long bar_b, bar_m;
+    constexpr int kABlock = kDigits * kATile;  // 48 KiB
+    constexpr int kStage = kABlock + kBBlock;  // 72 KiB
+    __shared__ __align__(8) unsigned long long bar_full[2], bar_mma[2];
     __shared__ uint32_t s_tmem;
-    __shared__ int s_fail, s_nch;
-    __shared__ double s_part[kXM];   // the second half's partial maximum, then the row's scale A
-    __shared__ double s_hpart[kXM];  // the second half's partial sum |H|, then the row's sum
-    __shared__ double s_mul[kXM];    // 2^42 / A: a value's fixed-point multiplier
+    __shared__ int s_fail, s_n;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int m = tid & (kXM - 1), half = tid >> 7;
-    const int qt = blockIdx.x, z = blockIdx.z;
-    const int row = blockIdx.y * kXM + m;
-    XRow R{};
-    if (row < P.n_rows) R = P.rows[row];
-    const int mb = R.H ? *R.max_bin : 0;
-    if (tid == 0) {
-        s_nch = 0;
-        s_fail = 0;
-    }
-    __syncthreads();
-    if (half == 0 && mb > 0) atomicMax(&s_nch, (mb + kXB - 1) / kXB);
-    __syncthreads();
-    const int nch = min(s_nch, P.nch);
-    const int c_lo = z * P.cps, c_hi = min(nch, c_lo + P.cps);
+    const int qt = blockIdx.x, tile = blockIdx.y, z = blockIdx.z;
     const int q0 = qt * kXN;
-    const int b_lo = c_lo * kXB, b_hi = min(c_hi * kXB, mb);  // this row's bins in the split
-    if (c_lo >= c_hi) {
+    const int nch = min(tile_chunks(P.rows, P.n_rows, tile, &s_n), P.nch);
+    const int c_lo = z * P.cps, c_hi = min(nch, c_lo + P.cps);
+    const int n_it = c_hi > c_lo ? (c_hi - c_lo) * P.K : 0;
+    if (n_it == 0) {
         // the split holds no bin of these rows: zero partial sums
-        if (R.H && half == 0) {
-            for (int j = 0; j < kXN && q0 + j < P.nq; ++j) R.out[z * R.out_z + q0 + j] = 0.0;
-            if (qt == 0) R.e1[z * R.e_z] = R.e0[z * R.e_z] = R.habs[z * R.e_z] = 0.0;
+        for (int i = tid; i < kXM; i += blockDim.x) {
+            const int r = tile * kXM + i;
+            if (r < P.n_rows && P.rows[r].H) {
+                const XRow R = P.rows[r];
+                for (int j = 0; j < kXN && q0 + j < P.nq; ++j) R.out[z * R.out_z + q0 + j] = 0.0;
+            }
         }
         return;
     }
-
-    // ---- row scale: max over the split's bins of |H| max(1, |u|)^(K-1), and sum |H| ----
-    const double two_w = 2.0 / P.w;
-    double mx = 0, ha = 0;
-    if (R.H && b_hi > b_lo) {
-        const int mid = (b_lo + b_hi) >> 1;
-        const int lo = half ? mid : b_lo, hi = half ? b_hi : mid;
-        for (int b = lo; b < hi; ++b) {
-            const double h = fabs(R.H[b]);
-            const double u = fmax(1.0, fabs((R.axis[b] - b * P.w) * two_w));
-            double f = h;
-            for (int k = 1; k < P.K; ++k) f *= u;
-            mx = fmax(mx, f);
-            ha += h;
-        }
-    }
-    if (half == 1) {
-        s_part[m] = mx;
-        s_hpart[m] = ha;
-    }
-    __syncthreads();
-    if (half == 0) {
-        mx = fmax(mx, s_part[m]);
-        ha += s_hpart[m];
-        double A = 0, mul = 0;
-        if (mx > 0) {
-            // A = 2^e > mx * 128 / 126: the leading digit stays within [-128, 127]
-            const int e = ilogb(mx * (128.0 / 126.0) * (1.0 + 0x1p-30)) + 1;
-            A = ldexp(1.0, e);
-            mul = ldexp(1.0, 42 - e);
-        }
-        s_part[m] = A;
-        s_hpart[m] = ha;
-        s_mul[m] = mul;
-    }
     if (tid == 0) {
-        xbar_init(&bar_b);
-        xbar_init(&bar_m);
+        s_fail = 0;
+        for (int st = 0; st < 2; ++st) {
+            xbar_init(&bar_full[st]);
+            xbar_init(&bar_mma[st]);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncwarp();
@@ -344,94 +442,78 @@ __global__ void __launch_bounds__(kXThreads, 1) debye_x_kernel(XParams P) {
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = s_tmem;
-    const double mul = s_mul[m];
-    const unsigned char* tq = P.table + static_cast<size_t>(qt) * P.nch * P.K * kBBlock;
 
-    uint32_t pb = 0, pm = 0;
-    bool first = true;
-    int pending = 0;  // 1: a table copy may be in flight, 2: MMAs may be in flight
-    for (int c = c_lo; c < c_hi; ++c) {
-        // ---- the chunk's H (order 0) and u of row m, bins [32 half, 32 half + 32) ----
-        // (the previous chunk's MMAs completed before the last barrier, so the buffers are free)
-#pragma unroll 4
-        for (int e = 0; e < 32; ++e) {
-            const int bl = half * 32 + e, b = c * kXB + bl;
-            double h = 0, u = 0;
-            if (b < b_hi) {
-                h = R.H[b];
-                u = (R.axis[b] - b * P.w) * two_w;
-            }
-            s_hu[bl * kXM + m] = h * mul;  // H in units of 2^-42 A
-            s_u[bl * kXM + m] = u;
-        }
-        for (int k = 0; k < P.K; ++k) {
-            if (tid == 0) xbulk(Bbuf, tq + (static_cast<size_t>(c) * P.K + k) * kBBlock, kBBlock, &bar_b);
-            // ---- digits of H u^k, then H u^(k+1) for the next order ----
-#pragma unroll 1
-            for (int g = 0; g < 2; ++g) {
-                const int bl0 = half * 32 + g * 16;
-                uint32_t pack[kDigits][4];
-#pragma unroll
-                for (int j = 0; j < kDigits; ++j) pack[j][0] = pack[j][1] = pack[j][2] = pack[j][3] = 0;
-#pragma unroll
-                for (int e = 0; e < 16; ++e) {
-                    const int i = (bl0 + e) * kXM + m;
-                    const double v = s_hu[i];
-                    s_hu[i] = v * s_u[i];
-                    int d[kDigits];
-                    digits6(v, d);
-#pragma unroll
-                    for (int j = 0; j < kDigits; ++j)
-                        pack[j][e >> 2] |= (static_cast<uint32_t>(d[j]) & 0xffu) << (8 * (e & 3));
+    if (tid == 0) {
+        const unsigned char* abase = P.adig + P.tile_off[tile];
+        const unsigned char* bbase = P.table + static_cast<size_t>(qt) * P.nch * P.K * kBBlock;
+        auto issue = [&](int it) {
+            const int st = it & 1;
+            const size_t step = static_cast<size_t>(c_lo) * P.K + it;  // chunk * K + order
+            unsigned char* dst = smem + st * kStage;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(xsmem(&bar_full[st])),
+                         "r"(kStage)
+                         : "memory");
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                             xsmem(dst)),
+                         "l"(abase + step * kABlock), "r"(kABlock), "r"(xsmem(&bar_full[st]))
+                         : "memory");
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                             xsmem(dst + kABlock)),
+                         "l"(bbase + step * kBBlock), "r"(kBBlock), "r"(xsmem(&bar_full[st]))
+                         : "memory");
+        };
+        int issued = 0, landed = 0, committed = 0, retired = 0;
+        bool ok = true;
+        issue(0);
+        issued = 1;
+        for (int it = 0; it < n_it && ok; ++it) {
+            const int st = it & 1;
+            if (it + 1 < n_it) {
+                // stage (it + 1) & 1 was read by the MMAs of step it - 1
+                if (it >= 1) {
+                    ok = xwait(&bar_mma[(it - 1) & 1], ((it - 1) >> 1) & 1);
+                    if (!ok) break;
+                    retired = it;
                 }
-#pragma unroll
-                for (int j = 0; j < kDigits; ++j)
-                    *reinterpret_cast<uint4*>(Abuf + j * kATile + xoff(kXM, m, bl0)) =
-                        make_uint4(pack[j][0], pack[j][1], pack[j][2], pack[j][3]);
+                issue(it + 1);
+                issued = it + 2;
             }
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncthreads();
-            if (tid == 0) {
-                if (!xwait(&bar_b, pb)) {
-                    s_fail = 1;  // the copy may still be in flight
-                } else {
-                    asm volatile("tcgen05.fence::after_thread_sync;");
+            ok = xwait(&bar_full[st], (it >> 1) & 1);
+            if (!ok) break;
+            landed = it + 1;
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            unsigned char* A = smem + st * kStage;
+            unsigned char* B = A + kABlock;
 #pragma unroll 1
-                    for (int ks = 0; ks < kXB / 32; ++ks) {
-                        const uint32_t ka = ks * 2 * (kXM / 8) * 128, kb = ks * 2 * (kXN / 8) * 128;
+            for (int ks = 0; ks < kXB / 32; ++ks) {
+                const uint32_t ka = ks * 2 * (kXM / 8) * 128, kb = ks * 2 * (kXN / 8) * 128;
 #pragma unroll
-                        for (int s = 0; s < kDigits; ++s)
+                for (int s = 0; s < kDigits; ++s)
 #pragma unroll
-                            for (int i = 0; i <= s; ++i) {
-                                const uint64_t da = xdesc(xsmem(Abuf + i * kATile) + ka, kXM);
-                                const uint64_t db = xdesc(xsmem(Bbuf + (s - i) * kBTile) + kb, kXN);
-                                mma_i8(tmem + s * kXN, da, db, (first && ks == 0 && i == 0) ? 0u : 1u);
-                            }
+                    for (int i = 0; i <= s; ++i) {
+                        const uint64_t da = xdesc(xsmem(A + i * kATile) + ka, kXM);
+                        const uint64_t db = xdesc(xsmem(B + (s - i) * kBTile) + kb, kXN);
+                        mma_i8(tmem + s * kXN, da, db, (it == 0 && ks == 0 && i == 0) ? 0u : 1u);
                     }
-                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                                     xsmem(&bar_m))
-                                 : "memory");
-                }
             }
-            __syncthreads();
-            if (s_fail) {
-                pending = 1;
-                break;
-            }
-            pb ^= 1u;
-            first = false;
-            if (!xwait(&bar_m, pm)) {
-                if (tid == 0) s_fail = 2;
-            }
-            pm ^= 1u;
-            __syncthreads();
-            if (s_fail) {
-                pending = 2;
-                break;
-            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             xsmem(&bar_mma[st]))
+                         : "memory");
+            committed = it + 1;
         }
-        if (s_fail) break;
+        if (ok) {
+            // the last commit completes after every earlier MMA
+            ok = xwait(&bar_mma[(n_it - 1) & 1], ((n_it - 1) >> 1) & 1);
+            if (ok) retired = n_it;
+        }
+        if (!ok) {
+            // bounded waits for what may still be in flight, then report
+            for (int it = landed; it < issued; ++it) xwait(&bar_full[it & 1], (it >> 1) & 1);
+            if (committed > retired) xwait(&bar_mma[(committed - 1) & 1], ((committed - 1) >> 1) & 1);
+            s_fail = 1;
+        }
     }
+    __syncthreads();
 
     if (!s_fail) {
         asm volatile("tcgen05.fence::after_thread_sync;");
@@ -450,33 +532,20 @@ __global__ void __launch_bounds__(kXThreads, 1) debye_x_kernel(XParams P) {
 #pragma unroll
             for (int j = 0; j < 32; ++j) acc[j] += static_cast<double>(v[j]) * wgt;
         }
-        const int rrow = blockIdx.y * kXM + rm;
-        if (rrow < P.n_rows) {
-            const XRow Rr = P.rows[rrow];
-            if (Rr.H) {
-                const double A2 = s_part[rm] * 2.0;  // row scale times the table's scale
+        const int r = tile * kXM + rm;
+        if (r < P.n_rows) {
+            const XRow R = P.rows[r];
+            if (R.H) {
+                const double A2 = P.row_scale[r] * 2.0;  // row scale times the table's scale
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
                     const int qi = q0 + cb + j;
-                    if (qi < P.nq) Rr.out[z * Rr.out_z + qi] = acc[j] * A2;
-                }
-                if (qt == 0 && cb == 0) {
-                    // per element: digits of H u^k within 2^-43 A (one rounding of the fixed-point
-                    // value; the staged H u^k carry 2^-52 relative more), of C_k within 2^-42; dropped
-                    // digit pairs (i + j >= 6) below 2^-38.67 A; sum_k |H u^k| <= K 1.01^(K-1) sum |H|
-                    const double nK = static_cast<double>(c_hi - c_lo) * kXB * P.K;
-                    const double hs = s_hpart[rm];
-                    Rr.e1[z * Rr.e_z] = s_part[rm] * 0x1p-42;
-                    Rr.e0[z * Rr.e_z] = s_part[rm] * nK * 0x1p-38 + 0x1p-41 * 1.1 * P.K * hs;
-                    Rr.habs[z * Rr.e_z] = hs;
+                    if (qi < P.nq) R.out[z * R.out_z + qi] = acc[j] * A2;
                 }
             }
         }
-    } else {
-        // bounded waits for the copies and MMAs this CTA may still have in flight
-        if (pending == 1) xwait(&bar_b, pb);
-        if (pending == 2) xwait(&bar_m, pm ^ 1u);
-        if (tid == 0) atomicExch(P.error_flag, 1);
+    } else if (tid == 0) {
+        atomicExch(P.error_flag, 1);
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
@@ -509,40 +578,42 @@ size_t debye_x_table_bytes(int nq, int nch, int K) {
 
 size_t debye_x_cpart_doubles(int nq, int nch) { return static_cast<size_t>((nq + kXN - 1) / kXN) * kXN * nch; }
 
-size_t debye_x_smem_bytes() {
-    return static_cast<size_t>(kDigits) * kATile + kBBlock + 2 * sizeof(double) * kXB * kXM + 1024;
-}
+size_t debye_x_block_bytes() { return static_cast<size_t>(kDigits) * kATile; }
 
-void debye_x_table_launch(const double* q, int nq, double w, int nch, int K, unsigned char* table, double* cpart,
-                          cudaStream_t s) {
-    if (nq <= 0 || nch <= 0) return;
-    debye_x_table_kernel<<<dim3((nq + kXN - 1) / kXN, nch), 256, 0, s>>>(q, nq, w, nch, K, table, cpart);
-}
-
-bool debye_x_launch(const XRow* rows, int n_rows, const double* q, int nq, const unsigned char* table, int nch, int K,
-                    double w, int cps, int splits, int32_t* error_flag, cudaStream_t s) {
+bool debye_x_enqueue(const XPlan& X, const double* q, cudaStream_t s) {
     static bool configured = false;
-    const size_t smem = debye_x_smem_bytes();
+    const size_t smem_mma = 2 * (static_cast<size_t>(kDigits) * kATile + kBBlock);
+    const size_t smem_dig = 2 * sizeof(double) * kXB * (kXM + 1);
     if (!configured) {
-        if (cudaFuncSetAttribute(debye_x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        if (cudaFuncSetAttribute(debye_x_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_mma) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(debye_x_digits_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_dig) !=
+                cudaSuccess)
             return false;
         configured = true;
     }
-    if (n_rows <= 0 || nq <= 0 || splits <= 0 || cps <= 0 || K < 1 || K > kXMaxOrder) return false;
-    if (static_cast<long long>(cps) * kXB * K > kMaxKSteps) return false;
+    if (X.n_rows <= 0 || X.nq <= 0 || X.splits <= 0 || X.cps <= 0 || X.K < 1 || X.K > kXMaxOrder) return false;
+    if (static_cast<long long>(X.cps) * kXB * X.K > kMaxKSteps) return false;
+    const int nqt = (X.nq + kXN - 1) / kXN, tiles = (X.n_rows + kXM - 1) / kXM;
+    debye_x_qcheck_kernel<<<1, 256, 0, s>>>(q, X.nq, X.q_cached, X.flags);
+    debye_x_table_kernel<<<dim3(nqt, X.nch), 256, 0, s>>>(q, X.nq, X.w, X.nch, X.K, X.table, X.cpart, X.flags);
+    debye_x_rowstat_kernel<<<(X.n_rows + 7) / 8, 256, 0, s>>>(X.rows, X.n_rows, X.w, X.K, X.cps, X.splits,
+                                                               X.row_scale);
+    debye_x_digits_kernel<<<dim3(tiles, X.nch), kXThreads, smem_dig, s>>>(X.rows, X.n_rows, X.w, X.K, X.row_scale,
+                                                                          X.tile_off, X.adig);
     XParams P;
-    P.rows = rows;
-    P.n_rows = n_rows;
-    P.q = q;
-    P.nq = nq;
-    P.table = table;
-    P.nch = nch;
-    P.K = K;
-    P.w = w;
-    P.cps = cps;
-    P.error_flag = error_flag;
-    const dim3 grid((nq + kXN - 1) / kXN, (n_rows + kXM - 1) / kXM, splits);
-    debye_x_kernel<<<grid, kXThreads, smem, s>>>(P);
+    P.rows = X.rows;
+    P.n_rows = X.n_rows;
+    P.nq = X.nq;
+    P.table = X.table;
+    P.adig = X.adig;
+    P.tile_off = X.tile_off;
+    P.row_scale = X.row_scale;
+    P.nch = X.nch;
+    P.K = X.K;
+    P.cps = X.cps;
+    P.error_flag = X.flags + 1;
+    debye_x_kernel<<<dim3(nqt, tiles, X.splits), kXThreads, smem_mma, s>>>(P);
     return cudaGetLastError() == cudaSuccess;
 }
 
