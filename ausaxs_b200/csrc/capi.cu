@@ -334,7 +334,7 @@ int ausaxs_gpu_ctx_tc_error_estimate(ausaxs_gpu_ctx* ctx, double* out, int32_t n
     return guarded([&] {
         if (!ctx || (nq > 0 && !out)) throw Error{AUSAXS_ERR_ARGUMENT, "null argument"};
         const auto& e = ctx->impl.last_tc_err;
-        if ((size_t)nq != e.size()) throw Error{AUSAXS_ERR_ARGUMENT, "nq differs from the last precision-0 transform"};
+        if ((size_t)nq != e.size()) throw Error{AUSAXS_ERR_ARGUMENT, "nq differs from the last tensor-core transform"};
         std::copy(e.begin(), e.end(), out);
     });
 }

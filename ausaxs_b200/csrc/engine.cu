@@ -668,13 +668,121 @@ DebyeArgs Structure::debye_args(const ausaxs_hist_config& cfg, const double* q_d
 void Structure::enqueue_debye(const ausaxs_hist_config& cfg, const double* q_dev, int nq, const ausaxs_debye_params& p,
                               double* Iq_dev, double* prof_dev) {
     DebyeArgs A = debye_args(cfg, q_dev, nq, p, Iq_dev, prof_dev);
-    run_debye(*ctx, A, cfg.manager == AUSAXS_MANAGER_FFGRID ? 7 : 1, plan.tc, p.precision);
+    run_debye(*ctx, A, cfg.manager == AUSAXS_MANAGER_FFGRID ? 7 : 1, plan.tc, p.precision, &plan.x, cfg.bin_width);
 }
 
-int run_debye(Ctx& C, DebyeArgs& A, int groups_present, DevBuf& tc, int precision) {
+// The exact tensor-core transform of A's rows: buffers (re)made when the shape changes, the tables
+// whenever the q values change (checked on the device); fills A's x fields.  false: not launched.
+static bool enqueue_debye_x(Ctx& C, DebyeArgs& A, XBufs& X, double w) {
+    cudaStream_t s = C.stream;
+    XPlan& XP = X.plan;
+    if (X.q != A.q || X.nq != A.nq || X.qmax < 0) {
+        std::vector<double> hq(A.nq);
+        AUSAXS_CUDA(cudaMemcpyAsync(hq.data(), A.q, sizeof(double) * A.nq, cudaMemcpyDeviceToHost, s));
+        AUSAXS_CUDA(cudaStreamSynchronize(s));
+        double qmax = 0;
+        for (double v : hq) qmax = std::max(qmax, std::fabs(v));
+        X.qmax = qmax;
+    }
+    const int K = debye_x_order(X.qmax, w);
+    const bool same = X.H == A.H && X.q == A.q && X.R == A.R && X.nb == A.nb && X.nq == A.nq && X.w == w && XP.K == K;
+    if (!same) {
+        XP.w = w;
+        XP.nq = A.nq;
+        XP.K = K;
+        XP.nch = std::max(1, (A.nb + kXChunk - 1) / kXChunk);
+        XP.n_rows = A.R;
+        const int tiles = (A.R + 127) / 128;
+        const long long qt = (A.nq + kXQTile - 1) / kXQTile;
+        int splits = (XP.nch + debye_x_max_chunks(K) - 1) / debye_x_max_chunks(K);
+        while (splits < XP.nch && qt * tiles * splits < 2LL * C.sm_count) ++splits;
+        XP.cps = (XP.nch + splits - 1) / splits;
+        XP.splits = (XP.nch + XP.cps - 1) / XP.cps;
+        X.table.ensure(debye_x_table_bytes(A.nq, XP.nch, K));
+        const size_t ncp = debye_x_cpart_doubles(A.nq, XP.nch);
+        X.cpart.ensure(sizeof(double) * ncp);
+        X.qcache.ensure(sizeof(double) * A.nq);
+        AUSAXS_CUDA(cudaMemsetAsync(X.qcache.p, 0xff, sizeof(double) * A.nq, s));  // NaN: tables made on first use
+        X.flags.ensure(256);
+        AUSAXS_CUDA(cudaMemsetAsync(X.flags.p, 0, 256, s));
+        const size_t nv = (size_t)XP.splits * A.R * A.nq, ne = (size_t)XP.splits * A.R;
+        X.planes.ensure(sizeof(double) * (nv + 3 * ne));
+        // rows: their distance axes from the row descriptors
+        std::vector<RowDesc> rd(A.R);
+        AUSAXS_CUDA(cudaMemcpyAsync(rd.data(), A.rows, sizeof(RowDesc) * A.R, cudaMemcpyDeviceToHost, s));
+        AUSAXS_CUDA(cudaStreamSynchronize(s));
+        double* v = X.planes.as<double>();
+        double* e1 = v + nv;
+        double* e0 = e1 + ne;
+        double* ha = e0 + ne;
+        const double* axes[3] = {A.axis0, A.axis1 ? A.axis1 : A.axis0, A.axis2 ? A.axis2 : A.axis0};
+        std::vector<XRow> rows(A.R);
+        for (int r = 0; r < A.R; ++r) {
+            XRow& xr = rows[r];
+            xr = XRow{};
+            xr.H = A.H + (size_t)r * A.nb;
+            xr.axis = axes[std::min(2, std::max(0, rd[r].group))];
+            xr.max_bin = A.max_bin;
+            xr.out = v + (size_t)r * A.nq;
+            xr.e1 = e1 + r;
+            xr.e0 = e0 + r;
+            xr.habs = ha + r;
+            xr.out_z = (long long)A.R * A.nq;
+            xr.e_z = A.R;
+        }
+        X.rows.ensure(sizeof(XRow) * A.R);
+        AUSAXS_CUDA(cudaMemcpyAsync(X.rows.p, rows.data(), sizeof(XRow) * A.R, cudaMemcpyHostToDevice, s));
+        std::vector<long long> toff(tiles);
+        for (int t = 0; t < tiles; ++t) toff[t] = (long long)t * XP.nch * K * (long long)debye_x_block_bytes();
+        X.adig.ensure((size_t)tiles * XP.nch * K * debye_x_block_bytes());
+        X.tile_off.ensure(sizeof(long long) * tiles);
+        AUSAXS_CUDA(cudaMemcpyAsync(X.tile_off.p, toff.data(), sizeof(long long) * tiles, cudaMemcpyHostToDevice, s));
+        X.row_scale.ensure(sizeof(double) * A.R);
+        AUSAXS_CUDA(cudaStreamSynchronize(s));  // the host staging vectors end here
+        XP.rows = X.rows.as<XRow>();
+        XP.table = X.table.as<unsigned char>();
+        XP.cpart = X.cpart.as<double>();
+        XP.q_cached = X.qcache.as<double>();
+        XP.flags = X.flags.as<int32_t>();
+        XP.adig = X.adig.as<unsigned char>();
+        XP.tile_off = X.tile_off.as<long long>();
+        XP.row_scale = X.row_scale.as<double>();
+        X.H = A.H;
+        X.q = A.q;
+        X.R = A.R;
+        X.nb = A.nb;
+        X.nq = A.nq;
+        X.w = w;
+    }
+    if (!debye_x_enqueue(XP, A.q, s)) return false;
+    C.check_launch("debye_x");
+    const size_t nv = (size_t)XP.splits * A.R * A.nq, ne = (size_t)XP.splits * A.R;
+    double* v = X.planes.as<double>();
+    A.x_v = v;
+    A.x_e1 = v + nv;
+    A.x_e0 = v + nv + ne;
+    A.x_habs = v + nv + 2 * ne;
+    A.x_splits = XP.splits;
+    A.x_cpart = X.cpart.as<double>();
+    A.x_nch = XP.nch;
+    A.x_nqp = (int)(debye_x_cpart_doubles(A.nq, XP.nch) / XP.nch);
+    A.x_K = XP.K;
+    A.x_ctr = debye_x_trunc(XP.K, w);
+    A.tc_error = X.flags.as<int32_t>() + 1;
+    return true;
+}
+
+int run_debye(Ctx& C, DebyeArgs& A, int groups_present, DevBuf& tc, int precision, XBufs* xb, double w) {
     precision = debye_precision(precision, A.R, A.nb, A.nq);
+    if (precision == 3 && (!xb || !(w > 0))) precision = 1;
     if (A.nq <= 0) return precision;
     cudaStream_t s = C.stream;
+    if (precision == 3) {
+        cudaEvent_t ev;
+        C.time_begin(3, &ev);
+        if (!enqueue_debye_x(C, A, *xb, w)) precision = 1;
+        C.time_end(3, ev);
+    }
     if (precision == 0) {
         // split-BF16 tensor-core contraction for every q, FP64 re-evaluation of the flagged ones
         int sms = 148;
@@ -882,7 +990,7 @@ void debye_of_host_histogram(Ctx& C, const ausaxs_hist_config& cfg, const ausaxs
     cudaStream_t s = C.stream;
     C.last_tc_err.assign(p.precision != 1 ? nq : 0, INFINITY);
     if (nq > 0) {
-        const int used = run_debye(C, A, D.groups, C.tc, p.precision);
+        const int used = run_debye(C, A, D.groups, C.tc, p.precision, &C.x, cfg.bin_width);
         int32_t ncols = 0;
         AUSAXS_CUDA(cudaMemcpyAsync(&ncols, A.fp64_columns, 4, cudaMemcpyDeviceToHost, s));
         AUSAXS_CUDA(cudaMemcpyAsync(Iq, A.Iq, (size_t)nq * 8, cudaMemcpyDeviceToHost, s));
@@ -890,7 +998,7 @@ void debye_of_host_histogram(Ctx& C, const ausaxs_hist_config& cfg, const ausaxs
         if (p.precision != 1)
             AUSAXS_CUDA(cudaMemcpyAsync(C.last_tc_err.data(), A.tc_err_est, (size_t)nq * 8, cudaMemcpyDeviceToHost, s));
         AUSAXS_CUDA(cudaStreamSynchronize(s));
-        C.last_fp64_columns = used == 0 ? ncols : nq;
+        C.last_fp64_columns = (used == 0 || used == 3) ? ncols : nq;
     }
     AUSAXS_CUDA(cudaStreamSynchronize(s));
 }

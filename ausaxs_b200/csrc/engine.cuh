@@ -64,6 +64,18 @@ struct JobSpec {
     bool lattice = false;  // the plan bins this pass with the lattice kernel (the structure's own launches)
 };
 
+// Buffers of the exact-accumulation tensor-core transform of one structure's rows (debye_x.cu), kept
+// with their shape so repeated transforms reuse tables, digit blocks and planes.
+struct XBufs {
+    DevBuf table, cpart, qcache, flags, planes, rows, adig, tile_off, row_scale;
+    XPlan plan{};
+    // shape the buffers were made for
+    const double* H = nullptr;
+    const double* q = nullptr;
+    int R = 0, nb = 0, nq = 0;
+    double w = 0, qmax = -1;
+};
+
 // Launch plan of one structure under one histogram configuration: job table, accumulator and
 // output layout, kernel shapes.  Built once, then enqueued any number of times without
 // allocation or synchronisation (so it can be captured in a CUDA graph).
@@ -97,6 +109,7 @@ struct Plan {
     // tensor-core scratch
     DevBuf tc;
     int tc_nq = 0;
+    XBufs x;
     // the dummies' self pairs by the lattice kernel (lattice.cuh): launch shape, or grid == 0
     LatticeLaunch lattice{};
     int lattice_grid = 0;
@@ -183,6 +196,7 @@ struct Ctx {
     std::shared_ptr<Hydrator> hyd;  // hydration workspace (hydrate.cuh)
     DevBuf io;                     // q / I(q) / profiles of one-shot host calls
     DevBuf tc;                     // tensor-core scratch of one-shot host calls
+    XBufs x;                       // exact tensor-core transform of one-shot host calls
     int last_fp64_columns = 0;     // q values the last host transform evaluated in FP64
     std::vector<double> last_tc_err;  // per q: estimated relative error of its tensor-core value
     void check_launch(const char* what);
@@ -205,9 +219,12 @@ struct ZeroRange {
 };
 void zero_ranges_launch(const ZeroRange* ranges_dev, int n, cudaStream_t s);
 
-// Tensor-core contraction (precision 0) followed by the FP64 epilogue, or FP64 only (precision 1);
-// precision 2 picks 0 when the contraction pays off (debye_precision).  Returns the precision used.
-int run_debye(Ctx& C, DebyeArgs& A, int groups_present, DevBuf& tc, int precision);
+// Split-BF16 tensor-core contraction (precision 0) or exact-accumulation tensor-core contraction
+// (precision 3, needs xb and the bin width w) followed by the FP64 epilogue, or FP64 only (precision
+// 1); precision 2 picks 3 when the contraction pays off (debye_precision), else 1.  Returns the
+// precision used.
+int run_debye(Ctx& C, DebyeArgs& A, int groups_present, DevBuf& tc, int precision, XBufs* xb = nullptr,
+              double w = 0);
 
 // The contraction's fixed cost (operand staging in a few CTAs, ~50 us) exceeds the FP64 transform's
 // below about 5e6 row x bin x q products (measured: 48 us against 25 us at 2.4e6, 92 + ~50 us
@@ -215,7 +232,7 @@ int run_debye(Ctx& C, DebyeArgs& A, int groups_present, DevBuf& tc, int precisio
 constexpr double kTcMinWork = 8e6;
 inline int debye_precision(int precision, int rows, int bins, int nq) {
     if (precision != 2) return precision;
-    return (double)rows * bins * nq >= kTcMinWork ? 0 : 1;
+    return (double)rows * bins * nq >= kTcMinWork ? 3 : 1;
 }
 
 // A histogram given in the reference's host layouts (ausaxs_hist_result), compacted to the rows of

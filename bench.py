@@ -699,9 +699,9 @@ def run_ours(args, rank, world, local_rank):
     cfg = mgr.config()
     A, W, X = mgr._inputs()
     pairs = pair_count(m, grid)
-    # precision 2 (default): the split-BF16 tensor-core transform where it pays off (FP64 for every q
-    # whose rigorous error bound exceeds the tolerance, the path's I(q) bar of 1e-4 relative to the
-    # FP64 transform), the FP64 transform for small ones
+    # precision 2 (default): the exact-accumulation tensor-core transform where it pays off (FP64 for
+    # every q whose rigorous error bound exceeds the tolerance, the path's I(q) bar of 1e-4 relative to
+    # the FP64 transform), the FP64 transform for small ones
     params = _capi.DebyeParams(1.0, 1.0, 1.0, 0.0, 0.0, 1.0, args.precision, args.tolerance)
     nq = len(wl.q)
     q_dev = torch.tensor(wl.q, dtype=torch.float64, device=f"cuda:{local_rank}")
@@ -1561,8 +1561,9 @@ def main():
     ap.add_argument("--atoms", type=int, default=0, help="cfg1: atoms of the globule (default 50000; smaller for profiling)")
     ap.add_argument("--structures", type=int, default=0,
                     help="cfg3: the first structures of the seeded batch (default all 256; fewer for profiling)")
-    ap.add_argument("--precision", type=int, default=2, choices=[0, 1, 2],
-                    help="Debye transform: 0 tensor cores, 1 FP64, 2 automatic (tensor cores from 8e6 row x bin x q)")
+    ap.add_argument("--precision", type=int, default=2, choices=[0, 1, 2, 3],
+                    help="Debye transform: 0 split-BF16 tensor cores, 1 FP64, 3 exact-accumulation tensor cores, "
+                         "2 automatic (3 from 8e6 row x bin x q, else 1)")
     ap.add_argument("--tolerance", type=float, default=1e-4)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

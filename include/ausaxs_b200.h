@@ -152,15 +152,18 @@ AUSAXS_API int ausaxs_gpu_histogram(ausaxs_gpu_ctx* ctx, const ausaxs_hist_confi
  * scaling, crho = solvent density scaling, Debye-Waller sigmas for atoms and exv).
  * grid_width: settings::grid::exv::width, the FFGRID dummy volume is grid_width^3.
  * precision: 0 = split-BF16 tensor-core contraction with FP64 recomputation of every q whose
- *            estimated error exceeds tolerance; 1 = FP64 on CUDA cores for every q; 2 = automatic:
- *            0 when the transform has at least 8e6 row x bin x q products (below that the
+ *            estimated error exceeds tolerance; 1 = FP64 on CUDA cores for every q; 3 = exact-
+ *            accumulation tensor-core contraction (int8 digits of the histogram rows and of Taylor
+ *            tables of sinc shared by every call on the same q grid, s32 sums) with a rigorous bound
+ *            per q and FP64 recomputation of every q whose bound exceeds tolerance; 2 = automatic:
+ *            3 when the transform has at least 8e6 row x bin x q products (below that the
  *            contraction's fixed cost exceeds the FP64 transform's), else 1.
  */
 typedef struct {
     double cw, cx, crho, dw_atomic, dw_exv;
     double grid_width;
     int32_t precision;
-    double tolerance; /* relative I(q) error target for precision 0 (default 1e-5 when <= 0) */
+    double tolerance; /* relative I(q) error target for precision 0, 2, 3 (default 1e-5 when <= 0) */
 } ausaxs_debye_params;
 
 /*

@@ -126,3 +126,54 @@ def test_automatic_precision_picks_by_size(gpu_ctx):
     h.precision = 1
     _, I1 = h.debye_transform(q)
     np.testing.assert_allclose(I2, I1, rtol=TOL)
+
+
+def _exact_pair(h, q, ctx, tolerance):
+    h.precision, h.tolerance = 1, 1e-5
+    _, I64 = h.debye_transform(q)
+    h.precision, h.tolerance = 3, tolerance
+    _, Ix = h.debye_transform(q)
+    return I64, Ix, ctx.fp64_columns(), ctx.tc_error_estimate(len(q))
+
+
+@pytest.mark.parametrize("grid", [False, True])
+def test_exact_tensor_core_transform(gpu_ctx, grid):
+    """precision 3: int8 digit products (exact s32 sums) of the histogram rows and of shared Taylor
+    tables.  The rigorous bound keeps every q on the tensor cores at the 1e-4 bar, the actual deviation
+    from the FP64 transform stays below the bound, and far below the bar."""
+    rng = np.random.default_rng(21 + grid)
+    n = 6000
+    xyz = rng.normal(0, 14, (n, 3))
+    m = hist.Molecule(atoms=xyz, ff_types=rng.choice([3, 7, 11, 12], n).astype(np.int32),
+                      waters=rng.normal(0, 17, (1200, 3)), volume=n * 18.0,
+                      exv=np.round(rng.uniform(-15, 15, (3000, 3))) if grid else None)
+    w = 0.1
+    h = (hist.HistogramManagerMTFFGrid(m, w, 8000, gpu_ctx) if grid
+         else hist.HistogramManagerMTFFAvg(m, True, w, 8000, gpu_ctx)).calculate_all()
+    if grid:
+        h.apply_excluded_volume_scaling_factor(1.07)
+    q = np.linspace(0.005, 1.0, 1000)
+    I64, Ix, n64, est = _exact_pair(h, q, gpu_ctx, TOL)
+    rel = np.abs(Ix / I64 - 1)
+    assert np.max(rel) <= TOL
+    assert n64 <= 0.02 * len(q), n64
+    kept = np.isfinite(est) & (est <= TOL)
+    assert np.all(rel[kept] <= est[kept])  # the bound holds
+    assert np.median(rel) < 1e-8
+    # repeated transforms on the same q grid reuse the tables and give the same bits
+    _, Ix2, _, _ = _exact_pair(h, q, gpu_ctx, TOL)
+    np.testing.assert_array_equal(Ix2, Ix)
+    # a new q grid at the same address (the context's staging buffer) rebuilds them
+    q2 = np.linspace(0.01, 0.9, 1000)
+    I64b, Ixb, _, _ = _exact_pair(h, q2, gpu_ctx, TOL)
+    assert np.max(np.abs(Ixb / I64b - 1)) <= TOL
+
+
+def test_exact_transform_on_golden_cases(gpu_ctx):
+    """precision 3 against the FP64 transform on every golden case (their parameters applied)."""
+    for name, h, q in _cases(gpu_ctx):
+        h.precision, h.tolerance = 1, 1e-5
+        _, I64 = h.debye_transform(q)
+        h.precision, h.tolerance = 3, TOL
+        _, I = h.debye_transform(q)
+        np.testing.assert_allclose(I, I64, rtol=TOL, err_msg=name)
