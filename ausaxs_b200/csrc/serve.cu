@@ -432,8 +432,9 @@ struct Assembly {
         C.check_launch("finalize");
         DebyeArgs A = S.debye_args(cfg, q_dev, nq, params, I_dev, nullptr);
         A.fp64_columns = nullptr;
-        debye_fp64_launch(A, s);
-        C.check_launch("debye");
+        // FP64 (precision 1), or the exact tensor-core contraction (3; 2 when it pays off) over tables
+        // kept with the assembly's plan (made when its first request runs)
+        run_debye(C, A, 1, S.plan.tc, params.precision, &S.plan.x, cfg.bin_width);
         if (fit) {
             lsq_launch(target_dev, I_dev, err_dev, nq, lsq_dev, s);
             C.check_launch("lsq");

@@ -543,7 +543,7 @@ def serving_measure(args, rank, world, local_rank, compact=False):
     chains = args.chains
     nq = 400
     q = np.linspace(0.005, 0.5, nq)
-    p = _capi.DebyeParams(1.0, 1.0, 1.0, 0.0, 0.0, 1.0, 1, 1e-5)
+    p = _capi.DebyeParams(1.0, 1.0, 1.0, 0.0, 0.0, 1.0, args.serve_precision, 1e-4 if args.serve_precision != 1 else 1e-5)
     rng = np.random.default_rng(4 + rank)
     t_gen = time.perf_counter()
     asm = [synth.assembly(1000 * rank + 40 + c) for c in range(chains)]
@@ -1557,6 +1557,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="cfg3: skip the serving sub-object")
     ap.add_argument("--serve-requests", type=int, default=0, help="serving: requests per load point (default 5 x chains)")
+    ap.add_argument("--serve-precision", type=int, default=1, choices=[1, 2, 3],
+                    help="serving: the per-move transform (1 FP64, 3 exact-accumulation tensor cores, 2 automatic)")
     ap.add_argument("--subunit", type=int, default=0, help="cfg2: atoms per subunit (default 8333; smaller for profiling)")
     ap.add_argument("--atoms", type=int, default=0, help="cfg1: atoms of the globule (default 50000; smaller for profiling)")
     ap.add_argument("--structures", type=int, default=0,

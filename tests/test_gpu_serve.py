@@ -207,3 +207,26 @@ def test_served_iq_matches_oracle_after_moves(gpu_ctx):
         # the d-axis carries the fixed-point quantisation (<= 1e-6 A): q * 1e-6 relative phase at most
         np.testing.assert_allclose(I, Io, rtol=1e-6, atol=0)
     S.close()
+
+
+def test_served_tensor_core_transform(gpu_ctx):
+    """Requests of an assembly admitted with precision 3 (the exact-accumulation tensor-core transform,
+    its tables kept with the assembly) against the same moves served with the FP64 transform: within
+    the 1e-4 bar, and the assembly's histograms identical."""
+    atoms, wats, _ = _bodies(11, [1200, 2500, 800, 1700])
+    cfg = _cfg(atoms)
+    q = np.linspace(0.005, 0.5, 400)
+    p64 = _capi.DebyeParams(1.0, 1.0, 1.0, 0.0, 0.0, 1.0, 1, 1e-5)
+    ptc = _capi.DebyeParams(1.0, 1.0, 1.0, 0.0, 0.0, 1.0, 3, 1e-4)
+    S = _capi.Server(hbm_budget=4 << 30)
+    a, _ = S.admit(cfg, atoms, wats, q, p64, margin=30.0)
+    b, _ = S.admit(cfg, atoms, wats, q, ptc, margin=30.0)
+    rng = np.random.default_rng(4)
+    for step in range(5):
+        body = int(rng.integers(0, 4))
+        R, t = _random_move(rng, S.body_center(a, body))
+        Ia, _ = S.wait(S.submit(a, body, R, t), a)
+        Ib, _ = S.wait(S.submit(b, body, R, t), b)
+        np.testing.assert_allclose(Ib, Ia, rtol=1e-4, atol=0)
+        np.testing.assert_array_equal(S.histogram(a, 8000)["aa"], S.histogram(b, 8000)["aa"])
+    S.close()
