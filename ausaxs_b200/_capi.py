@@ -45,7 +45,7 @@ EXPORTED = [
     "ausaxs_gpu_batch_create", "ausaxs_gpu_batch_destroy", "ausaxs_gpu_batch_autotune", "ausaxs_gpu_batch_candidate",
     "ausaxs_gpu_batch_profile_device", "ausaxs_gpu_batch_profile", "ausaxs_gpu_batch_pair_time",
     "ausaxs_gpu_batch_histogram", "ausaxs_gpu_batch_set_points", "ausaxs_gpu_batch_fp64_columns", "ausaxs_gpu_smem_atomic_rate",
-    "ausaxs_gpu_server_create", "ausaxs_gpu_server_destroy", "ausaxs_gpu_server_admit", "ausaxs_gpu_server_release",
+    "ausaxs_gpu_server_create", "ausaxs_gpu_server_set_policy", "ausaxs_gpu_server_destroy", "ausaxs_gpu_server_admit", "ausaxs_gpu_server_release",
     "ausaxs_gpu_server_usage", "ausaxs_gpu_server_submit", "ausaxs_gpu_server_poll", "ausaxs_gpu_server_wait",
     "ausaxs_gpu_server_completed", "ausaxs_gpu_server_launch_count", "ausaxs_gpu_server_body_center", "ausaxs_gpu_server_coordinates", "ausaxs_gpu_server_histogram",
 ]
@@ -156,6 +156,7 @@ def load():
         L.ausaxs_gpu_smem_atomic_rate.argtypes = [C.c_int32, C.c_int32, f64, f64]
         L.ausaxs_gpu_server_create.argtypes = [C.c_int32, C.c_int64, C.c_int32, C.c_int32, C.POINTER(vp)]
         L.ausaxs_gpu_server_destroy.argtypes = [vp]
+        L.ausaxs_gpu_server_set_policy.argtypes = [vp, C.c_int32]
         L.ausaxs_gpu_server_admit.argtypes = [vp, C.POINTER(HistConfig), C.c_int32, f32, i64, f32, i64, C.c_double,
                                               f64, C.c_int32, C.POINTER(DebyeParams), f64, f64, i32, i64]
         L.ausaxs_gpu_server_release.argtypes = [vp, C.c_int32]
@@ -649,6 +650,10 @@ class Server:
         self.nq = {}
         self.n_atoms = {}
         self.n_waters = {}
+
+    def set_policy(self, policy: int):
+        """0: concurrent per-assembly streams with small moves at high priority; 1: submission order."""
+        check(load().ausaxs_gpu_server_set_policy(self.h, int(policy)))
 
     def close(self):
         if getattr(self, "h", None):

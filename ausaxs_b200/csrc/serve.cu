@@ -149,11 +149,12 @@ struct Assembly {
     void sync() {
         for (auto& st : streams)
             if (st) cudaStreamSynchronize(st);
+        if (has_last) cudaEventSynchronize(last);  // a request on the server's arrival-order stream
     }
 
     // the stream of a request with this priority, ordered after the assembly's previous request
-    void select_stream(bool high) {
-        cudaStream_t st = streams[high ? 0 : 1];
+    void select_stream(bool high) { select(streams[high ? 0 : 1]); }
+    void select(cudaStream_t st) {
         if (has_last && st != C.stream) AUSAXS_CUDA(cudaStreamWaitEvent(st, last, 0));
         C.stream = st;
     }
@@ -461,6 +462,10 @@ struct Server {
     long long next_ticket = 1;
     std::vector<cudaEvent_t> events;
     long long high_priority_pairs = 0;  // moves of at most this many pairs run on high-priority streams
+    // 0: every assembly's requests on its own two streams (concurrent; small moves at high priority);
+    // 1: every request on one stream in submission order (each move has the whole GPU)
+    int policy = 0;
+    cudaStream_t fifo = nullptr;
 
     // the median move size over the bodies of every admitted assembly
     void update_priority_threshold() {
@@ -480,6 +485,7 @@ struct Server {
         for (auto& r : inflight) cudaEventDestroy(r.second.ev);
         for (auto e : events) cudaEventDestroy(e);
         asms.clear();
+        if (fifo) cudaStreamDestroy(fifo);
     }
 
     Assembly& get(int id) {
@@ -532,6 +538,13 @@ int ausaxs_gpu_server_create(int32_t device, int64_t hbm_budget_bytes, int32_t m
         s->impl.max_inflight = max_inflight;
         s->impl.slots_per_assembly = slots_per_assembly;
         *out = s;
+    });
+}
+
+int ausaxs_gpu_server_set_policy(ausaxs_gpu_server* s, int32_t policy) {
+    return guarded([&] {
+        if (!s || (policy != 0 && policy != 1)) throw Error{AUSAXS_ERR_ARGUMENT, "bad scheduling policy"};
+        s->impl.policy = policy;
     });
 }
 
@@ -603,7 +616,12 @@ int ausaxs_gpu_server_submit(ausaxs_gpu_server* s, int32_t id, int32_t body, con
             AUSAXS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         }
         try {
-            A.select_stream(body >= 0 && A.move_pairs[body] <= S.high_priority_pairs);
+            if (S.policy == 1) {
+                if (!S.fifo) AUSAXS_CUDA(cudaStreamCreateWithFlags(&S.fifo, cudaStreamNonBlocking));
+                A.select(S.fifo);
+            } else {
+                A.select_stream(body >= 0 && A.move_pairs[body] <= S.high_priority_pairs);
+            }
             A.enqueue_request(body, R, t, slot);
             AUSAXS_CUDA(cudaEventRecord(A.last, A.C.stream));
             A.has_last = true;

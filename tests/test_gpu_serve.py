@@ -230,3 +230,31 @@ def test_served_tensor_core_transform(gpu_ctx):
         np.testing.assert_allclose(Ib, Ia, rtol=1e-4, atol=0)
         np.testing.assert_array_equal(S.histogram(a, 8000)["aa"], S.histogram(b, 8000)["aa"])
     S.close()
+
+
+def test_submission_order_policy_same_results(gpu_ctx):
+    """Scheduling changes when a request runs, not what it computes: the same moves under both policies
+    give the same bits."""
+    atoms, wats, _ = _bodies(13, [900, 1400, 600])
+    others = _bodies(14, [700, 1100])
+    q = np.linspace(0.005, 0.5, 100)
+    p = _capi.DebyeParams(1.0, 1.0, 1.0, 0.0, 0.0, 1.0, 1, 1e-5)
+    rng = np.random.default_rng(5)
+    moves = [(int(rng.integers(0, 3)), synth.random_rotation(rng, 5.0), rng.uniform(-2, 2, 3)) for _ in range(6)]
+    results = []
+    for policy in (0, 1):
+        S = _capi.Server(hbm_budget=2 << 30)
+        S.set_policy(policy)
+        a, _ = S.admit(_cfg(atoms), atoms, wats, q, p)
+        b, _ = S.admit(_cfg(others[0]), others[0], others[1], q, p)
+        out = []
+        for body, R, t in moves:
+            ta = S.submit(a, body, R, t)
+            tb = S.submit(b, body % 2, R, t)  # interleaved with another assembly's requests
+            out.append(S.wait(ta, a)[0])
+            S.wait(tb, b)
+        results.append(np.array(out))
+        S.close()
+    np.testing.assert_array_equal(results[0], results[1])
+    with pytest.raises(_capi.AusaxsError):
+        _capi.Server(hbm_budget=1 << 30).set_policy(2)
