@@ -652,7 +652,8 @@ class Server:
         self.n_waters = {}
 
     def set_policy(self, policy: int):
-        """0: concurrent per-assembly streams with small moves at high priority; 1: submission order."""
+        """0: concurrent per-assembly streams with small moves at high priority; k > 0: submission order
+        over k streams (at most k moves share the device)."""
         check(load().ausaxs_gpu_server_set_policy(self.h, int(policy)))
 
     def close(self):

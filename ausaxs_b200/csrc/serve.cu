@@ -463,9 +463,11 @@ struct Server {
     std::vector<cudaEvent_t> events;
     long long high_priority_pairs = 0;  // moves of at most this many pairs run on high-priority streams
     // 0: every assembly's requests on its own two streams (concurrent; small moves at high priority);
-    // 1: every request on one stream in submission order (each move has the whole GPU)
+    // k > 0: requests in submission order, round robin over k server streams (at most k moves share
+    // the GPU; k = 1: each move has it alone)
     int policy = 0;
-    cudaStream_t fifo = nullptr;
+    std::vector<cudaStream_t> lanes;
+    size_t next_lane = 0;
 
     // the median move size over the bodies of every admitted assembly
     void update_priority_threshold() {
@@ -485,7 +487,7 @@ struct Server {
         for (auto& r : inflight) cudaEventDestroy(r.second.ev);
         for (auto e : events) cudaEventDestroy(e);
         asms.clear();
-        if (fifo) cudaStreamDestroy(fifo);
+        for (auto st : lanes) cudaStreamDestroy(st);
     }
 
     Assembly& get(int id) {
@@ -543,7 +545,7 @@ int ausaxs_gpu_server_create(int32_t device, int64_t hbm_budget_bytes, int32_t m
 
 int ausaxs_gpu_server_set_policy(ausaxs_gpu_server* s, int32_t policy) {
     return guarded([&] {
-        if (!s || (policy != 0 && policy != 1)) throw Error{AUSAXS_ERR_ARGUMENT, "bad scheduling policy"};
+        if (!s || policy < 0 || policy > 16) throw Error{AUSAXS_ERR_ARGUMENT, "bad scheduling policy"};
         s->impl.policy = policy;
     });
 }
@@ -616,9 +618,13 @@ int ausaxs_gpu_server_submit(ausaxs_gpu_server* s, int32_t id, int32_t body, con
             AUSAXS_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
         }
         try {
-            if (S.policy == 1) {
-                if (!S.fifo) AUSAXS_CUDA(cudaStreamCreateWithFlags(&S.fifo, cudaStreamNonBlocking));
-                A.select(S.fifo);
+            if (S.policy > 0) {
+                while ((int)S.lanes.size() < S.policy) {
+                    cudaStream_t st;
+                    AUSAXS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+                    S.lanes.push_back(st);
+                }
+                A.select(S.lanes[S.next_lane++ % S.policy]);
             } else {
                 A.select_stream(body >= 0 && A.move_pairs[body] <= S.high_priority_pairs);
             }

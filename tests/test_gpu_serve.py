@@ -242,7 +242,7 @@ def test_submission_order_policy_same_results(gpu_ctx):
     rng = np.random.default_rng(5)
     moves = [(int(rng.integers(0, 3)), synth.random_rotation(rng, 5.0), rng.uniform(-2, 2, 3)) for _ in range(6)]
     results = []
-    for policy in (0, 1):
+    for policy in (0, 1, 2):
         S = _capi.Server(hbm_budget=2 << 30)
         S.set_policy(policy)
         a, _ = S.admit(_cfg(atoms), atoms, wats, q, p)
@@ -256,5 +256,6 @@ def test_submission_order_policy_same_results(gpu_ctx):
         results.append(np.array(out))
         S.close()
     np.testing.assert_array_equal(results[0], results[1])
+    np.testing.assert_array_equal(results[0], results[2])
     with pytest.raises(_capi.AusaxsError):
-        _capi.Server(hbm_budget=1 << 30).set_policy(2)
+        _capi.Server(hbm_budget=1 << 30).set_policy(-1)
