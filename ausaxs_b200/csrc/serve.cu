@@ -464,8 +464,9 @@ struct Server {
     long long high_priority_pairs = 0;  // moves of at most this many pairs run on high-priority streams
     // 0: every assembly's requests on its own two streams (concurrent; small moves at high priority);
     // k > 0: requests in submission order, round robin over k server streams (at most k moves share
-    // the GPU; k = 1: each move has it alone)
-    int policy = 0;
+    // the GPU; k = 1: each move has it alone).  Two lanes by default: a move waits for at most one
+    // other, and the pair launches of two moves still fill each other's last waves.
+    int policy = 2;
     std::vector<cudaStream_t> lanes;
     size_t next_lane = 0;
 

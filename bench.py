@@ -1558,9 +1558,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true", help="cfg3: skip the serving sub-object")
     ap.add_argument("--serve-requests", type=int, default=0, help="serving: requests per load point (default 5 x chains)")
-    ap.add_argument("--serve-policy", type=int, default=0,
-                    help="serving: 0 concurrent per-assembly streams (small moves first), k > 0 submission order "
-                         "over k streams")
+    ap.add_argument("--serve-policy", type=int, default=2,
+                    help="serving: k > 0 submission order over k streams (default 2), 0 concurrent per-assembly "
+                         "streams (small moves first)")
     ap.add_argument("--serve-precision", type=int, default=1, choices=[1, 2, 3],
                     help="serving: the per-move transform (1 FP64, 3 exact-accumulation tensor cores, 2 automatic)")
     ap.add_argument("--subunit", type=int, default=0, help="cfg2: atoms per subunit (default 8333; smaller for profiling)")

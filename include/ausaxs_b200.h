@@ -464,10 +464,10 @@ typedef struct ausaxs_gpu_server ausaxs_gpu_server;
 AUSAXS_API int ausaxs_gpu_server_create(int32_t device, int64_t hbm_budget_bytes, int32_t max_inflight,
                                         int32_t slots_per_assembly, ausaxs_gpu_server** out);
 AUSAXS_API int ausaxs_gpu_server_destroy(ausaxs_gpu_server* s);
-/* Scheduling of requests: 0 (default) every assembly's requests on its own two streams, so moves of
- * different assemblies overlap on the device, moves of at most the median size at high stream
- * priority; k in [1, 16] requests in submission order, round robin over k server streams, so at most
- * k moves share the device (1: each move has it alone).  An assembly's requests stay in order. */
+/* Scheduling of requests: k in [1, 16] (default 2) requests in submission order, round robin over k
+ * server streams, so at most k moves share the device (1: each move has it alone); 0 every assembly's
+ * requests on its own two streams, so moves of all assemblies overlap on the device, moves of at most
+ * the median size at high stream priority.  An assembly's requests stay in order. */
 AUSAXS_API int ausaxs_gpu_server_set_policy(ausaxs_gpu_server* s, int32_t policy);
 AUSAXS_API int ausaxs_gpu_server_admit(ausaxs_gpu_server* s, const ausaxs_hist_config* cfg, int32_t n_bodies,
                                        const float* atoms, const int64_t* atom_offsets, const float* waters,
