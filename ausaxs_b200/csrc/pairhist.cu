@@ -244,7 +244,7 @@ struct Outer {
 
 // The count and offset arrays are indexed with the bit pattern of the magic-rounded distance
 // (kMagic + bin), their base pointers shifted by -kMagicBits.
-template <bool GENERAL, bool WEIGHTED, int ROWS, int R, bool NR>
+template <bool GENERAL, bool WEIGHTED, int ROWS, int R, int NR>
 __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, const float4* s_pts, const Outer (&o)[R],
                                            int j0, int k0, int k1, bool diag, float wsc) {
     const float inv_w = J.inv_w, c = J.c, scale = J.scale;
@@ -273,12 +273,18 @@ __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, co
                 if (tail) s = __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
             }
             const float d = NR ? pair_sqrt_nr(s) : __fsqrt_rn(s);
-            const float x = __fmul_rn(d, inv_w);
-            // rint(x) by the magic number, ties to even; distances past the last bin (also NaN, inf
-            // and x >= 2^22) are clamped to the overflow column
-            float xm = fminf(__fadd_rn(x, kMagic), bin_limit);
-            if (GENERAL && tail && __fsub_rn(x, __fsub_rn(xm, kMagic)) == 0.5f)
-                xm = fminf(__fadd_rn(xm, 1.0f), bin_limit);  // std::round: ties away from zero
+            // rint(x), x = d inv_w, by the magic number, ties to even; distances past the last bin
+            // (also NaN, inf and x >= 2^22) are clamped to the overflow column.  NR == 2: inv_w is a
+            // power of two, so d inv_w is exact and one fused multiply-add rounds it
+            float xm;
+            if (NR == 2 && !GENERAL) {
+                xm = fminf(__fmaf_rn(d, inv_w, kMagic), bin_limit);
+            } else {
+                const float x = __fmul_rn(d, inv_w);
+                xm = fminf(__fadd_rn(x, kMagic), bin_limit);
+                if (GENERAL && tail && __fsub_rn(x, __fsub_rn(xm, kMagic)) == 0.5f)
+                    xm = fminf(__fadd_rn(xm, 1.0f), bin_limit);  // std::round: ties away from zero
+            }
             const int xb = __float_as_int(xm);
             if (ROWS == kRowsSingle) {
                 shared_red_add(o[k].caddr + (static_cast<uint32_t>(xb) << 2), 1u);
@@ -305,7 +311,7 @@ __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, co
     }
 }
 
-template <int NT, int R, bool WEIGHTED, bool DREG, bool NR>
+template <int NT, int R, bool WEIGHTED, bool DREG, int NR>
 __device__ __forceinline__ void run_segments(const PairJob& J, const Onchip& S, const float4* s_pts, const Outer (&o)[R],
                                              int j0, int jn, bool general, bool diag, float wsc,
                                              OffsetRegs<NT, DREG>& Rg) {
@@ -333,7 +339,7 @@ __device__ __forceinline__ void run_segments(const PairJob& J, const Onchip& S, 
 }
 
 // DREG: the u64 offset sums live in registers (one CTA per SM; pairhist_dreg decides)
-template <int NT, int R, bool WEIGHTED, bool DREG, bool NR>
+template <int NT, int R, bool WEIGHTED, bool DREG, int NR>
 __global__ void __launch_bounds__(NT, DREG ? 1 : (512 / NT > 1 ? 512 / NT : 1)) pairhist_kernel(PairLaunch L) {
     constexpr int TILE = NT * R;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -489,7 +495,7 @@ __global__ void __launch_bounds__(NT, DREG ? 1 : (512 / NT > 1 ? 512 / NT : 1)) 
     }
 }
 
-template <int NT, int R, bool WEIGHTED, bool DREG, bool NR>
+template <int NT, int R, bool WEIGHTED, bool DREG, int NR>
 void launch_one(const PairLaunch& L, int grid, size_t smem, cudaStream_t s) {
     cudaFuncSetAttribute(pairhist_kernel<NT, R, WEIGHTED, DREG, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     pairhist_kernel<NT, R, WEIGHTED, DREG, NR><<<grid, NT, smem, s>>>(L);
@@ -497,8 +503,9 @@ void launch_one(const PairLaunch& L, int grid, size_t smem, cudaStream_t s) {
 
 template <int NT, bool WEIGHTED, bool DREG>
 void launch_nr(const PairLaunch& L, int grid, size_t smem, cudaStream_t s) {
-    if (L.nr_sqrt) launch_one<NT, kOuter, WEIGHTED, DREG, true>(L, grid, smem, s);
-    else launch_one<NT, kOuter, WEIGHTED, DREG, false>(L, grid, smem, s);
+    if (L.nr_sqrt == 2) launch_one<NT, kOuter, WEIGHTED, DREG, 2>(L, grid, smem, s);
+    else if (L.nr_sqrt == 1) launch_one<NT, kOuter, WEIGHTED, DREG, 1>(L, grid, smem, s);
+    else launch_one<NT, kOuter, WEIGHTED, DREG, 0>(L, grid, smem, s);
 }
 
 template <int TILE>
@@ -512,8 +519,8 @@ void launch_tile(const PairLaunch& L, int grid, size_t smem, cudaStream_t s) {
 
 template <int NT, int R, bool WEIGHTED, bool DREG>
 int occupancy_one(size_t smem) {
-    // both root variants share the launch shape; the exact one bounds the registers
-    auto k = pairhist_kernel<NT, R, WEIGHTED, DREG, false>;
+    // the root variants share the launch shape; the fewest resident CTAs of them bounds the launch
+    auto k = pairhist_kernel<NT, R, WEIGHTED, DREG, 0>;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
         return 1;
@@ -523,11 +530,12 @@ int occupancy_one(size_t smem) {
         cudaGetLastError();
         return 1;
     }
-    auto k2 = pairhist_kernel<NT, R, WEIGHTED, DREG, true>;
-    int n2 = 0;
-    if (cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n2, k2, NT, smem) == cudaSuccess && n2 < n)
-        n = n2;
+    for (auto k2 : {pairhist_kernel<NT, R, WEIGHTED, DREG, 1>, pairhist_kernel<NT, R, WEIGHTED, DREG, 2>}) {
+        int n2 = 0;
+        if (cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n2, k2, NT, smem) == cudaSuccess && n2 < n)
+            n = n2;
+    }
     cudaGetLastError();
     return n > 0 ? n : 1;
 }
@@ -611,6 +619,10 @@ void pairhist_launch(const PairLaunch& L0, int tile, int grid, size_t smem, cuda
         std::memcpy(&key, &L.inv_w, 4);
         auto it = g_sqrt.bins.find(key);
         L.nr_sqrt = (L.inv_w > 0 && it != g_sqrt.bins.end() && it->second >= L.smem_bins) ? 1 : 0;
+        // a power-of-two inverse width (0.25 A bins): the product d inv_w is exact, so the rounding to
+        // a bin fuses with it (one FFMA per pair instead of FMUL + FADD)
+        int e = 0;
+        if (L.nr_sqrt && std::frexp(L.inv_w, &e) == 0.5f) L.nr_sqrt = 2;
     }
     // double-buffered staging when the launch was given the room for it
     L.stages = smem >= pairhist_layout_bytes(L.smem_rows, L.smem_bins, L.weighted != 0, tile, L.dreg != 0, 2) ? 2 : 1;

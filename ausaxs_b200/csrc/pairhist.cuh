@@ -63,7 +63,8 @@ struct PairLaunch {
                                     // shared memory it is given: 2 = the next tile's copy overlaps)
     float inv_w;                    // the inverse bin width every job of the launch shares (0: unknown)
     int32_t nr_sqrt;                // 1: the Newton-Raphson root (pair_sqrt_nr), set by pairhist_launch for
-                                    // a width pair_sqrt_prepare verified (else the correctly rounded root)
+                                    // a width pair_sqrt_prepare verified (else the correctly rounded root);
+                                    // 2: that, with a power-of-two inv_w fused into the bin rounding
     int32_t max_grabs;              // > 0: a CTA takes at most this many chunks and exits (the grid
                                     // must then cover the tiles: grid * max_grabs * chunk >= total);
                                     // bounded CTAs let the block scheduler interleave other launches
