@@ -35,9 +35,11 @@ sys.path.insert(0, ROOT)
 
 import numpy as np  # noqa: E402
 
-# warp instructions per 32 pair evaluations of the pair kernel, counted by ncu on the batch's pair launches
-# (smsp__inst_executed / (shared atomics / 2), profiles/pairhist_kernel_batch_64_structures.md)
-INSTR_PER_PAIR = 34.5
+# warp instructions per 32 pair evaluations of the pair kernel at 0.25 A bins (the batch and serving
+# configurations; the bin rounding fused with the power-of-two inverse width), counted by ncu on the
+# batch's pair launches (smsp__inst_executed / (shared atomics / 2),
+# profiles/pairhist_kernel_batch_64_structures.md)
+INSTR_PER_PAIR = 33.5
 # DRAM bytes (read + write) of the pair launches of one step of the 256-structure batch: 16.6 MB per pass
 # measured by ncu on its first 64 structures (0.86M points), scaled by points to the batch's 3.66M
 BATCH_PAIR_TRAFFIC_BYTES = 7.0e7
