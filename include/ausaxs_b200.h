@@ -229,7 +229,7 @@ AUSAXS_API int ausaxs_gpu_structure_histogram(ausaxs_gpu_ctx* ctx, ausaxs_gpu_st
  *   (times_ms may be null).  ausaxs_gpu_batch_candidate describes a candidate.
  * ausaxs_gpu_batch_profile_device: q and Iq[n_structures * n_q] are device pointers; enqueues one
  *   graph launch on the context's stream (the graph is captured on the first call and again when
- *   q, Iq, n_q or the parameters change).  params->precision 1: FP64 transform for every q; 0 or 2:
+ *   q, Iq, n_q or the parameters change).  params->precision 1: FP64 transform for every q; 0, 2, 3:
  *   the exact-accumulation tensor-core transform (int8 digit products of the histogram rows and of
  *   shared Taylor tables of sinc, s32 sums) with a rigorous error bound per q, and the FP64
  *   transform for every q whose bound exceeds params->tolerance times |I(q)|.  Any bin overflow in
