@@ -122,6 +122,7 @@ struct Batch {
     cudaEvent_t pair_t0 = nullptr, pair_t1 = nullptr;
     // captured profile
     cudaGraphExec_t exec = nullptr;
+    long long graph_launches = 0;
     struct Key {
         const double* q = nullptr;
         int nq = -1;
@@ -437,9 +438,11 @@ struct Batch {
         AUSAXS_CUDA(cudaEventRecordWithFlags(pair_t1, s, cudaEventRecordExternal));
         ff_finalize_batch_launch(fin.as<FinalizeFF>(), (int)items.size(), max_nb, s);
         ctx->check_launch("finalize");
+        ctx->launches += 1;  // two kernels
         if (x.on) {
             if (!debye_x_enqueue(x.plan, q, s)) throw Error{AUSAXS_ERR_CUDA, "cannot launch the tensor-core Debye transform"};
             ctx->check_launch("debye_x");
+            ctx->launches += 4;  // five kernels
         }
         int max_R = 1;
         for (auto& S : items) max_R = std::max(max_R, S->plan.R);
@@ -475,6 +478,7 @@ struct Batch {
             AUSAXS_CUDA(cudaStreamSynchronize(s));
             cudaGraph_t g = nullptr;
             AUSAXS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            const long long launches0 = C.launches;
             try {
                 enqueue_all(q, nq, s);
             } catch (...) {
@@ -483,6 +487,8 @@ struct Batch {
                 throw;
             }
             AUSAXS_CUDA(cudaStreamEndCapture(s, &g));
+            graph_launches = C.launches - launches0;  // kernels per replay (counted as they were captured)
+            C.launches = launches0;
             cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
             cudaGraphDestroy(g);
             if (e != cudaSuccess) {
@@ -497,7 +503,7 @@ struct Batch {
             key.p = p;
         }
         AUSAXS_CUDA(cudaGraphLaunch(exec, s));
-        C.launches += 4 + (long long)launches.size();
+        C.launches += graph_launches;
     }
 
     // New coordinates for every point, in the creation layout (rows aoff[i] .. aoff[i+1] of atoms,

@@ -756,6 +756,7 @@ static bool enqueue_debye_x(Ctx& C, DebyeArgs& A, XBufs& X, double w) {
     }
     if (!debye_x_enqueue(XP, A.q, s)) return false;
     C.check_launch("debye_x");
+    C.launches += 4;  // five kernels
     const size_t nv = (size_t)XP.splits * A.R * A.nq, ne = (size_t)XP.splits * A.R;
     double* v = X.planes.as<double>();
     A.x_v = v;
