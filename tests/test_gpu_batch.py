@@ -44,10 +44,12 @@ def test_batch_equals_single_structure_ffavg(gpu_ctx):
     B.close()
 
 
-def test_batch_vs_oracle(gpu_ctx):
-    mols = _molecules(7, [300, 1200, 50])
+@pytest.mark.parametrize("precision", [1, 2])
+def test_batch_vs_oracle(gpu_ctx, precision):
+    """FP64 transform (1) and the exact-accumulation tensor-core transform (2) against the oracle."""
+    mols = _molecules(7, [300, 1200, 50, 2500])
     q = np.linspace(0.005, 0.5, 120)
-    I = hist.BatchedProfiles(mols, bin_width=0.25, ctx=gpu_ctx).debye_transform(q)
+    I = hist.BatchedProfiles(mols, bin_width=0.25, ctx=gpu_ctx).debye_transform(q, precision=precision)
     for i, m in enumerate(mols):
         A, W, _ = m.compact_ff()
         o = O.hist_ff(0, A, W, None, 0.25, 8000, m.volume * 0.334 / m.size_atom())
