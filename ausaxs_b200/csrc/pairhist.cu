@@ -501,18 +501,21 @@ void launch_one(const PairLaunch& L, int grid, size_t smem, cudaStream_t s) {
     pairhist_kernel<NT, R, WEIGHTED, DREG, NR><<<grid, NT, smem, s>>>(L);
 }
 
-template <int NT, bool WEIGHTED, bool DREG>
+template <int NT, bool WEIGHTED, bool DREG, int R = kOuter>
 void launch_nr(const PairLaunch& L, int grid, size_t smem, cudaStream_t s) {
-    if (L.nr_sqrt == 2) launch_one<NT, kOuter, WEIGHTED, DREG, 2>(L, grid, smem, s);
-    else if (L.nr_sqrt == 1) launch_one<NT, kOuter, WEIGHTED, DREG, 1>(L, grid, smem, s);
-    else launch_one<NT, kOuter, WEIGHTED, DREG, 0>(L, grid, smem, s);
+    if (L.nr_sqrt == 2) launch_one<NT, R, WEIGHTED, DREG, 2>(L, grid, smem, s);
+    else if (L.nr_sqrt == 1) launch_one<NT, R, WEIGHTED, DREG, 1>(L, grid, smem, s);
+    else launch_one<NT, R, WEIGHTED, DREG, 0>(L, grid, smem, s);
 }
 
+// Register-held offset sums mean a layout of one CTA per SM; with 1024-point tiles that CTA runs one
+// outer point per thread (1,024 threads: 32 warps per SM instead of 16), the shared memory unchanged.
 template <int TILE>
 void launch_tile(const PairLaunch& L, int grid, size_t smem, cudaStream_t s) {
     constexpr int NT = TILE / kOuter;
     // register-held offset sums exist for unweighted launches only (pairhist_dreg)
     if (L.weighted) launch_nr<NT, true, false>(L, grid, smem, s);
+    else if (L.dreg && TILE == 1024) launch_nr<TILE, false, true, 1>(L, grid, smem, s);
     else if (L.dreg) launch_nr<NT, false, true>(L, grid, smem, s);
     else launch_nr<NT, false, false>(L, grid, smem, s);
 }
@@ -572,6 +575,7 @@ SqrtVerified g_sqrt;
 }  // namespace
 
 int pairhist_ctas_per_sm(size_t smem, int tile, bool dreg, bool weighted) {
+    if (tile == 1024 && dreg && !weighted) return occupancy_one<1024, 1, false, true>(smem);
     if (tile == 1024) return occupancy_tile<1024>(smem, weighted, dreg);
     if (tile == 256) return occupancy_tile<256>(smem, weighted, dreg);
     return occupancy_tile<512>(smem, weighted, dreg);
