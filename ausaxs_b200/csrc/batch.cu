@@ -102,6 +102,8 @@ struct Batch {
     // misc: tile counters [0, 16), overflow [16] (set from [24] at the start of every profile), q values
     // recomputed in FP64 [20], points rejected by the last set_points [24] (kept across profiles)
     DevBuf jobs, misc, zero, fin, args;
+    DevBuf qfactors;      // the per-q factor table every structure's transform reads
+    DebyeArgs qf_args{};  // q and parameters of the table
     std::vector<long long> a_off, w_off;  // creation offsets of the concatenated atoms and waters
     DevBuf points_items, points_in;       // set_points: destinations, staged host input
     // exact-accumulation tensor-core transform (debye_x.cu): Taylor tables shared by every structure,
@@ -444,6 +446,9 @@ struct Batch {
             ctx->check_launch("debye_x");
             ctx->launches += 4;  // five kernels
         }
+        // every structure shares q, the parameters and the excluded-volume model: one factor table
+        debye_qfactors_launch(qf_args, qfactors.as<double>(), s);
+        ctx->check_launch("qfactors");
         int max_R = 1;
         for (auto& S : items) max_R = std::max(max_R, S->plan.R);
         debye_fp64_batch_launch(args.as<DebyeArgs>(), (int)items.size(), nq, max_R, s);
@@ -473,6 +478,9 @@ struct Batch {
             }
             x.on = false;
             if (p.precision != 1) setup_x(q, nq, A);
+            qfactors.ensure(sizeof(double) * debye_qfactors_doubles(nq));
+            qf_args = A[0];
+            for (auto& a : A) a.qf = qfactors.as<double>();
             args.ensure(sizeof(DebyeArgs) * A.size());
             AUSAXS_CUDA(cudaMemcpyAsync(args.p, A.data(), sizeof(DebyeArgs) * A.size(), cudaMemcpyHostToDevice, s));
             AUSAXS_CUDA(cudaStreamSynchronize(s));

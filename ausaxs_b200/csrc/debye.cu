@@ -9,9 +9,10 @@
 // 427-558) and CompositeDistanceHistogramFFGrid (CompositeDistanceHistogramFFGrid.cpp:37-119), or
 // I = exp(-q^2) sum_b (aa + cw aw + cw^2 ww) sinc for the Simple histogram (DistanceHistogram.cpp:54-87).
 //
-// When the split-BF16 tensor-core contraction (debye_tc.cu) has produced sinqd for all q, this kernel
-// only re-evaluates in FP64 the q values whose error estimate exceeds the tolerance: that is where
-// cancellation between bins (and between profiles) bites, typically the high-q WAXS tail.
+// When a tensor-core contraction (debye_x.cu, exact integer accumulation; debye_tc.cu, split BF16)
+// has produced sinqd for all q, this kernel adds up its error bound per q and re-evaluates in FP64
+// only the q values whose bound exceeds the tolerance: that is where cancellation between bins (and
+// between profiles) bites, typically the high-q WAXS tail.
 #include "debye.cuh"
 
 namespace ausaxs_b200 {
@@ -130,6 +131,41 @@ __device__ RowTerms row_terms(const DebyeArgs& A, const RowDesc& r, const QFacto
     return t;
 }
 
+// Factor j (0..31) of q: the 15 raw form factors, the 15 per-type excluded-volume form factors, then
+// the exv factor e and the average / grid excluded-volume form factor, then the Debye-Waller factors
+// and exp(-q^2).
+__device__ void q_factor(const DebyeArgs& A, double q, int j, QFactors& F) {
+    if (j < kNff) {
+        F.f[j] = ff_raw(j, q);
+    } else if (j < 2 * kNff) {
+        // ExvFormFactor(V).evaluate(q) = V rho_w exp(-V^(2/3)/(4 pi) q^2) (ExvFormFactor.h:20-33)
+        const double v = c_exv_volume[j - kNff];
+        F.xe[j - kNff] = v * kRhoWater * exp(-(pow(v, 2.0 / 3) / (4 * kPi)) * q * q);
+    } else if (j == 2 * kNff) {
+        const double rm2 = kAvgRadius * kAvgRadius / 4;  // exv_factor (CompositeDistanceHistogramFFExplicitBase.cpp:54-57)
+        F.e = pow(A.cx, 3) * exp(-rm2 * (pow(A.cx, 2) - 1) * q * q);
+        if (A.exv_model == 1) {
+            const double e = pow(A.grid_volume, 2.0 / 3) / (4 * kPi);  // ExvFormFactor (ExvFormFactor.h:20-33)
+            F.fx = A.grid_volume * kRhoWater * exp(-e * q * q);
+        } else {
+            F.fx = ff_raw(kExv, q);
+        }
+    } else {
+        F.ba = (A.dw_atomic != 0 || A.dw_exv != 0) ? exp(-q * q * A.dw_atomic * A.dw_atomic * 0.5) : 1.0;
+        F.bx = (A.dw_atomic != 0 || A.dw_exv != 0) ? exp(-q * q * A.dw_exv * A.dw_exv * 0.5) : 1.0;
+        F.eq2 = exp(-q * q);
+    }
+}
+
+// The per-q factor table of transforms that share q, the parameters and the excluded-volume model
+// (every structure of a batch): one thread per (q, factor)
+__global__ void debye_qfactors_kernel(DebyeArgs A, double* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.nq * 32) return;
+    QFactors& F = reinterpret_cast<QFactors*>(out)[i >> 5];
+    q_factor(A, A.q[i >> 5], i & 31, F);
+}
+
 // q values per CTA by the transform's q count: 4 up to 256 q, 8 up to 1,024, 16 beyond.  The
 // decomposition depends on nq alone, so a structure's I(q) has the same bits alone or in a batch.
 constexpr int debye_qt(int nq) { return nq <= 256 ? 4 : (nq <= 1024 ? 8 : 16); }
@@ -173,33 +209,17 @@ __device__ void debye_qtile(const DebyeArgs& A, const int q0, unsigned char* sme
     __shared__ int s_groups;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
-    // per-q factors: 32 per q value, one per thread (a handful of exp each)
-    for (int i = tid; i < nqt * 32; i += kThreads) {
-        const int qq = i >> 5, j = i & 31;
-        const double q = A.q[q0 + qq];
-        QFactors& F = s_F[qq];
-        if (j < kNff) {
-            F.f[j] = ff_raw(j, q);
-        } else if (j < 2 * kNff) {
-            // ExvFormFactor(V).evaluate(q) = V rho_w exp(-V^(2/3)/(4 pi) q^2) (ExvFormFactor.h:20-33)
-            const double v = c_exv_volume[j - kNff];
-            F.xe[j - kNff] = v * kRhoWater * exp(-(pow(v, 2.0 / 3) / (4 * kPi)) * q * q);
-        } else if (j == 2 * kNff) {
-            const double rm2 = kAvgRadius * kAvgRadius / 4;  // exv_factor (CompositeDistanceHistogramFFExplicitBase.cpp:54-57)
-            F.e = pow(A.cx, 3) * exp(-rm2 * (pow(A.cx, 2) - 1) * q * q);
-            if (A.exv_model == 1) {
-                const double e = pow(A.grid_volume, 2.0 / 3) / (4 * kPi);  // ExvFormFactor (ExvFormFactor.h:20-33)
-                F.fx = A.grid_volume * kRhoWater * exp(-e * q * q);
-            } else {
-                F.fx = ff_raw(kExv, q);
-            }
-        } else {
-            F.ba = (A.dw_atomic != 0 || A.dw_exv != 0) ? exp(-q * q * A.dw_atomic * A.dw_atomic * 0.5) : 1.0;
-            F.bx = (A.dw_atomic != 0 || A.dw_exv != 0) ? exp(-q * q * A.dw_exv * A.dw_exv * 0.5) : 1.0;
-            F.eq2 = exp(-q * q);
-            s_fp64[qq] = 1;
-            if (A.tc_err_est) A.tc_err_est[q0 + qq] = INFINITY;  // overwritten below when tensor-core values exist
-        }
+    // per-q factors: from the shared table, or 32 per q value, one per thread (a handful of exp each)
+    if (A.qf) {
+        constexpr int kWords = sizeof(QFactors) / sizeof(double);
+        for (int i = tid; i < nqt * kWords; i += kThreads)
+            reinterpret_cast<double*>(s_F)[i] = A.qf[static_cast<size_t>(q0) * kWords + i];
+    } else {
+        for (int i = tid; i < nqt * 32; i += kThreads) q_factor(A, A.q[q0 + (i >> 5)], i & 31, s_F[i >> 5]);
+    }
+    for (int qq = tid; qq < nqt; qq += kThreads) {
+        s_fp64[qq] = 1;
+        if (A.tc_err_est) A.tc_err_est[q0 + qq] = INFINITY;  // overwritten below when tensor-core values exist
     }
     if (tid == 0) s_groups = 1;
     for (int i = tid; i < QT * R; i += kThreads) s_acc[i] = 0;
@@ -412,6 +432,13 @@ bool debye_configure() {
 }
 
 }  // namespace
+
+size_t debye_qfactors_doubles(int nq) { return static_cast<size_t>(nq) * (sizeof(QFactors) / sizeof(double)); }
+
+void debye_qfactors_launch(const DebyeArgs& A, double* out, cudaStream_t s) {
+    if (A.nq <= 0) return;
+    debye_qfactors_kernel<<<(A.nq * 32 + 255) / 256, 256, 0, s>>>(A, out);
+}
 
 // (a failed configuration shows as the launch's own error, which the callers check)
 void debye_fp64_launch(const DebyeArgs& A, cudaStream_t s) {

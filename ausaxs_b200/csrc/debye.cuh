@@ -67,9 +67,16 @@ struct DebyeArgs {
     const double* x_cpart;      // [x_nch][x_nqp]
     int32_t x_nch, x_nqp, x_K;
     double x_ctr;
+    // per-q factors made by debye_qfactors_launch for transforms sharing q, the parameters and the
+    // excluded-volume model, or null (each CTA evaluates its own)
+    const double* qf;
 };
 
 void debye_fp64_launch(const DebyeArgs& A, cudaStream_t s);
+// The per-q factor table (form factors, excluded-volume and Debye-Waller factors) of A's q values and
+// parameters into out [debye_qfactors_doubles(nq)]
+size_t debye_qfactors_doubles(int nq);
+void debye_qfactors_launch(const DebyeArgs& A, double* out, cudaStream_t s);
 // n transforms at once (device array of arguments; max_nq >= every nq, max_R >= every R)
 void debye_fp64_batch_launch(const DebyeArgs* As_dev, int n, int max_nq, int max_R, cudaStream_t s);
 
