@@ -244,19 +244,19 @@ struct Outer {
 
 // The count and offset arrays are indexed with the bit pattern of the magic-rounded distance
 // (kMagic + bin), their base pointers shifted by -kMagicBits.
-template <bool GENERAL, bool WEIGHTED, int ROWS, int R, int NR>
+template <bool GENERAL, bool WEIGHTED, int ROWS, int R, int NR, bool DSUM>
 __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, const float4* s_pts, const Outer (&o)[R],
                                            int j0, int k0, int k1, bool diag, float wsc) {
     const float inv_w = J.inv_w, c = J.c, scale = J.scale;
     const float bin_limit = pair_bin_limit(J.nbins);  // kMagic + nbins: the overflow column
     const int rlo = J.row_lo, rhi = J.row_hi;
     const bool pair_rows = J.row_mode == kRowPair;
-    const bool do_d = J.dsum != nullptr;
+    constexpr bool do_d = DSUM;  // J.dsum != nullptr (a template argument: no branch per pair)
     const bool do_w = WEIGHTED && J.wsum != nullptr;
     uint32_t* const cnt = S.cnt - kMagicBits;
     // shared byte address of dacc[0] less 4 * kMagicBits (wrapping u32 arithmetic)
     const uint32_t dacc_addr = smem_addr(S.dacc) - 4u * static_cast<uint32_t>(kMagicBits);
-#pragma unroll 2
+#pragma unroll 4
     for (int jj = k0; jj < k1; ++jj) {
         const float4 b = s_pts[jj];
         const int j = j0 + jj;
@@ -319,18 +319,29 @@ __device__ __forceinline__ void run_segments(const PairJob& J, const Onchip& S, 
     const bool single = J.row_mode == kRowSingle && J.row_lo == 0 && J.row_hi >= 1;
     const int full_rows = J.row_mode == kRowPair ? J.types * J.types : (J.row_mode == kRowOuter ? J.types : 1);
     const bool offset_rows = !single && J.row_lo == 0 && J.row_hi >= full_rows;
+    const bool dsum = J.dsum != nullptr;
     for (int k0 = 0; k0 < jn; k0 += drain_segment<TILE>()) {
         const int k1 = min(jn, k0 + drain_segment<TILE>());
         if (general) {
-            if (single) tile_pairs<true, WEIGHTED, kRowsSingle, R, NR>(J, S, s_pts, o, j0, k0, k1, diag, wsc);
-            else if (offset_rows) tile_pairs<true, WEIGHTED, kRowsOffset, R, NR>(J, S, s_pts, o, j0, k0, k1, diag, wsc);
-            else tile_pairs<true, WEIGHTED, kRowsGeneric, R, NR>(J, S, s_pts, o, j0, k0, k1, diag, wsc);
+            if (dsum) {
+                if (single) tile_pairs<true, WEIGHTED, kRowsSingle, R, NR, true>(J, S, s_pts, o, j0, k0, k1, diag, wsc);
+                else if (offset_rows) tile_pairs<true, WEIGHTED, kRowsOffset, R, NR, true>(J, S, s_pts, o, j0, k0, k1, diag, wsc);
+                else tile_pairs<true, WEIGHTED, kRowsGeneric, R, NR, true>(J, S, s_pts, o, j0, k0, k1, diag, wsc);
+            } else {
+                if (single) tile_pairs<true, WEIGHTED, kRowsSingle, R, NR, false>(J, S, s_pts, o, j0, k0, k1, diag, wsc);
+                else if (offset_rows) tile_pairs<true, WEIGHTED, kRowsOffset, R, NR, false>(J, S, s_pts, o, j0, k0, k1, diag, wsc);
+                else tile_pairs<true, WEIGHTED, kRowsGeneric, R, NR, false>(J, S, s_pts, o, j0, k0, k1, diag, wsc);
+            }
+        } else if (dsum) {
+            if (single) tile_pairs<false, WEIGHTED, kRowsSingle, R, NR, true>(J, S, s_pts, o, j0, k0, k1, false, wsc);
+            else if (offset_rows) tile_pairs<false, WEIGHTED, kRowsOffset, R, NR, true>(J, S, s_pts, o, j0, k0, k1, false, wsc);
+            else tile_pairs<false, WEIGHTED, kRowsGeneric, R, NR, true>(J, S, s_pts, o, j0, k0, k1, false, wsc);
         } else {
-            if (single) tile_pairs<false, WEIGHTED, kRowsSingle, R, NR>(J, S, s_pts, o, j0, k0, k1, false, wsc);
-            else if (offset_rows) tile_pairs<false, WEIGHTED, kRowsOffset, R, NR>(J, S, s_pts, o, j0, k0, k1, false, wsc);
-            else tile_pairs<false, WEIGHTED, kRowsGeneric, R, NR>(J, S, s_pts, o, j0, k0, k1, false, wsc);
+            if (single) tile_pairs<false, WEIGHTED, kRowsSingle, R, NR, false>(J, S, s_pts, o, j0, k0, k1, false, wsc);
+            else if (offset_rows) tile_pairs<false, WEIGHTED, kRowsOffset, R, NR, false>(J, S, s_pts, o, j0, k0, k1, false, wsc);
+            else tile_pairs<false, WEIGHTED, kRowsGeneric, R, NR, false>(J, S, s_pts, o, j0, k0, k1, false, wsc);
         }
-        if (J.dsum) {
+        if (dsum) {
             __syncthreads();
             drain_offsets<NT, DREG>(S, J.nbins, Rg);
             __syncthreads();
