@@ -39,7 +39,7 @@ import numpy as np  # noqa: E402
 # configurations; the bin rounding fused with the power-of-two inverse width), counted by ncu on the
 # batch's pair launches (smsp__inst_executed / (shared atomics / 2),
 # profiles/pairhist_kernel_batch_64_structures.md)
-INSTR_PER_PAIR = 33.5
+INSTR_PER_PAIR = 31.1
 # DRAM bytes (read + write) of the pair launches of one step of the 256-structure batch: 16.6 MB per pass
 # measured by ncu on its first 64 structures (0.86M points), scaled by points to the batch's 3.66M
 BATCH_PAIR_TRAFFIC_BYTES = 7.0e7
