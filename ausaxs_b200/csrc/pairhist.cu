@@ -311,17 +311,27 @@ __device__ __forceinline__ void tile_pairs(const PairJob& J, const Onchip& S, co
     }
 }
 
-template <int NT, int R, bool WEIGHTED, bool DREG, int NR>
+// G groups of NT / G threads split the inner points of a tile: group g takes inner points
+// [g * TILE / G, (g + 1) * TILE / G); every group runs the same number of segments (the drains
+// synchronise the CTA), and a segment spans NT * R pairs per inner point of every group, so
+// drain_segment<NT * R>() keeps the 2^16-pairs-per-bin bound of the offset accumulators.
+template <int NT, int R, bool WEIGHTED, bool DREG, int NR, int G>
 __device__ __forceinline__ void run_segments(const PairJob& J, const Onchip& S, const float4* s_pts, const Outer (&o)[R],
                                              int j0, int jn, bool general, bool diag, float wsc,
                                              OffsetRegs<NT, DREG>& Rg) {
-    constexpr int TILE = NT * R;
+    constexpr int TILE = NT * R / G;
+    constexpr int H = TILE / G;  // inner points per group
+    constexpr int SEG = drain_segment<NT * R>();
     const bool single = J.row_mode == kRowSingle && J.row_lo == 0 && J.row_hi >= 1;
     const int full_rows = J.row_mode == kRowPair ? J.types * J.types : (J.row_mode == kRowOuter ? J.types : 1);
     const bool offset_rows = !single && J.row_lo == 0 && J.row_hi >= full_rows;
     const bool dsum = J.dsum != nullptr;
-    for (int k0 = 0; k0 < jn; k0 += drain_segment<TILE>()) {
-        const int k1 = min(jn, k0 + drain_segment<TILE>());
+    const int g_lo = G > 1 ? static_cast<int>(threadIdx.x / (NT / G)) * H : 0;  // this group's first inner point
+    const int g_hi = G > 1 ? min(jn, g_lo + H) : jn;
+    const int span = G > 1 ? min(jn, H) : jn;  // group 0 has the most inner points: it sets the segment count
+    for (int s0 = 0; s0 < span; s0 += SEG) {
+        const int k0 = g_lo + s0;
+        const int k1 = min(g_hi, k0 + SEG);
         if (general) {
             if (dsum) {
                 if (single) tile_pairs<true, WEIGHTED, kRowsSingle, R, NR, true>(J, S, s_pts, o, j0, k0, k1, diag, wsc);
@@ -349,10 +359,14 @@ __device__ __forceinline__ void run_segments(const PairJob& J, const Onchip& S, 
     }
 }
 
-// DREG: the u64 offset sums live in registers (one CTA per SM; pairhist_dreg decides)
-template <int NT, int R, bool WEIGHTED, bool DREG, int NR>
+// DREG: the u64 offset sums live in registers (one CTA per SM; pairhist_dreg decides).  G > 1: the
+// tile's side is NT * R / G points; G groups of NT / G threads share its outer points (R each) and
+// split its inner points (run_segments), so a one-CTA layout keeps R = 2 outer points per thread
+// (one staged inner point read per two pairs) with NT = 1024 threads on 1024-point tiles.
+template <int NT, int R, bool WEIGHTED, bool DREG, int NR, int G>
 __global__ void __launch_bounds__(NT, DREG ? 1 : (512 / NT > 1 ? 512 / NT : 1)) pairhist_kernel(PairLaunch L) {
-    constexpr int TILE = NT * R;
+    constexpr int TILE = NT * R / G;
+    constexpr int NTG = NT / G;  // threads per group
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ unsigned long long s_bar[2];
     __shared__ long long s_grab;
@@ -392,8 +406,9 @@ __global__ void __launch_bounds__(NT, DREG ? 1 : (512 / NT > 1 ? 512 / NT : 1)) 
 #pragma unroll
     for (int k = 0; k < OffsetRegs<NT, DREG>::kSlots; ++k) Rg.v[k] = 0;
     const float wsc = WEIGHTED ? *L.wscale : 0.f;
-    // lanes of a warp take outer points NT/32 apart; the warps interleave
-    const int spread = (threadIdx.x & 31) * (NT / 32) + (threadIdx.x >> 5);
+    // lanes of a warp take outer points NTG/32 apart; the warps of a group interleave
+    const int tg = static_cast<int>(threadIdx.x % NTG);
+    const int spread = (tg & 31) * (NTG / 32) + (tg >> 5);
     int cur = -1;
     long long pairs_since_flush = 0;
     unsigned phases = 0u;  // bit b: the parity of staging barrier b's next phase
@@ -458,7 +473,7 @@ __global__ void __launch_bounds__(NT, DREG ? 1 : (512 / NT > 1 ? 512 / NT : 1)) 
         const int row_begin_base = J.tail_from_outer ? J.a_base + 1 : 0;
 #pragma unroll
         for (int k = 0; k < R; ++k) {
-            o[k].i = ti * TILE + spread + k * NT;
+            o[k].i = ti * TILE + spread + k * NTG;
             o[k].active = o[k].i < J.na;
             o[k].a = o[k].active ? J.A[o[k].i] : make_float4(0.f, 0.f, 0.f, 0.f);
             const int ta = __float_as_int(o[k].a.w);
@@ -492,7 +507,7 @@ __global__ void __launch_bounds__(NT, DREG ? 1 : (512 / NT > 1 ? 512 / NT : 1)) 
         const bool has_tail = J.b_base + j0 + jn > J.tail_end - 3;  // scalar-tail partners: last 3 of a row
         const bool full = (ti + 1) * TILE <= J.na;
         const bool general = diag || has_tail || !full;
-        run_segments<NT, R, WEIGHTED, DREG, NR>(J, S, s_pts, o, j0, jn, general, diag, wsc, Rg);
+        run_segments<NT, R, WEIGHTED, DREG, NR, G>(J, S, s_pts, o, j0, jn, general, diag, wsc, Rg);
         fence_proxy_async();  // this thread's accesses to the buffer before the next bulk copy into it
         __syncthreads();      // every thread is done with the buffer
         if (!prefetch && gn < L.total_tiles) issue(gn, buf);
@@ -506,35 +521,36 @@ __global__ void __launch_bounds__(NT, DREG ? 1 : (512 / NT > 1 ? 512 / NT : 1)) 
     }
 }
 
-template <int NT, int R, bool WEIGHTED, bool DREG, int NR>
+template <int NT, int R, bool WEIGHTED, bool DREG, int NR, int G>
 void launch_one(const PairLaunch& L, int grid, size_t smem, cudaStream_t s) {
-    cudaFuncSetAttribute(pairhist_kernel<NT, R, WEIGHTED, DREG, NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    pairhist_kernel<NT, R, WEIGHTED, DREG, NR><<<grid, NT, smem, s>>>(L);
+    cudaFuncSetAttribute(pairhist_kernel<NT, R, WEIGHTED, DREG, NR, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    pairhist_kernel<NT, R, WEIGHTED, DREG, NR, G><<<grid, NT, smem, s>>>(L);
 }
 
-template <int NT, bool WEIGHTED, bool DREG, int R = kOuter>
+template <int NT, bool WEIGHTED, bool DREG, int G = 1>
 void launch_nr(const PairLaunch& L, int grid, size_t smem, cudaStream_t s) {
-    if (L.nr_sqrt == 2) launch_one<NT, R, WEIGHTED, DREG, 2>(L, grid, smem, s);
-    else if (L.nr_sqrt == 1) launch_one<NT, R, WEIGHTED, DREG, 1>(L, grid, smem, s);
-    else launch_one<NT, R, WEIGHTED, DREG, 0>(L, grid, smem, s);
+    if (L.nr_sqrt == 2) launch_one<NT, kOuter, WEIGHTED, DREG, 2, G>(L, grid, smem, s);
+    else if (L.nr_sqrt == 1) launch_one<NT, kOuter, WEIGHTED, DREG, 1, G>(L, grid, smem, s);
+    else launch_one<NT, kOuter, WEIGHTED, DREG, 0, G>(L, grid, smem, s);
 }
 
-// Register-held offset sums mean a layout of one CTA per SM; with 1024-point tiles that CTA runs one
-// outer point per thread (1,024 threads: 32 warps per SM instead of 16), the shared memory unchanged.
+// Register-held offset sums mean a layout of one CTA per SM; with 1024-point tiles that CTA runs
+// 1,024 threads in two groups that split the inner points (32 warps per SM instead of 16, still two
+// outer points per thread), the shared memory unchanged.
 template <int TILE>
 void launch_tile(const PairLaunch& L, int grid, size_t smem, cudaStream_t s) {
     constexpr int NT = TILE / kOuter;
     // register-held offset sums exist for unweighted launches only (pairhist_dreg)
     if (L.weighted) launch_nr<NT, true, false>(L, grid, smem, s);
-    else if (L.dreg && TILE == 1024) launch_nr<TILE, false, true, 1>(L, grid, smem, s);
+    else if (L.dreg && TILE == 1024) launch_nr<TILE, false, true, 2>(L, grid, smem, s);
     else if (L.dreg) launch_nr<NT, false, true>(L, grid, smem, s);
     else launch_nr<NT, false, false>(L, grid, smem, s);
 }
 
-template <int NT, int R, bool WEIGHTED, bool DREG>
+template <int NT, int R, bool WEIGHTED, bool DREG, int G = 1>
 int occupancy_one(size_t smem) {
     // the root variants share the launch shape; the fewest resident CTAs of them bounds the launch
-    auto k = pairhist_kernel<NT, R, WEIGHTED, DREG, 0>;
+    auto k = pairhist_kernel<NT, R, WEIGHTED, DREG, 0, G>;
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
         return 1;
@@ -544,7 +560,7 @@ int occupancy_one(size_t smem) {
         cudaGetLastError();
         return 1;
     }
-    for (auto k2 : {pairhist_kernel<NT, R, WEIGHTED, DREG, 1>, pairhist_kernel<NT, R, WEIGHTED, DREG, 2>}) {
+    for (auto k2 : {pairhist_kernel<NT, R, WEIGHTED, DREG, 1, G>, pairhist_kernel<NT, R, WEIGHTED, DREG, 2, G>}) {
         int n2 = 0;
         if (cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n2, k2, NT, smem) == cudaSuccess && n2 < n)
@@ -586,7 +602,7 @@ SqrtVerified g_sqrt;
 }  // namespace
 
 int pairhist_ctas_per_sm(size_t smem, int tile, bool dreg, bool weighted) {
-    if (tile == 1024 && dreg && !weighted) return occupancy_one<1024, 1, false, true>(smem);
+    if (tile == 1024 && dreg && !weighted) return occupancy_one<1024, kOuter, false, true, 2>(smem);
     if (tile == 1024) return occupancy_tile<1024>(smem, weighted, dreg);
     if (tile == 256) return occupancy_tile<256>(smem, weighted, dreg);
     return occupancy_tile<512>(smem, weighted, dreg);
