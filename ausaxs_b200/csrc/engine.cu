@@ -490,9 +490,12 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
         Plan::Group& G = P.group[P.n_launch++];
         G.tile = tile;
         G.smem = pairhist_launch_smem(group_rows[g], nb, w_launch, tile);
-        const int per_sm = pairhist_ctas_per_sm(G.smem, tile, pairhist_dreg(group_rows[g], nb, w_launch, tile), w_launch);
+        const bool dreg = pairhist_dreg(group_rows[g], nb, w_launch, tile);
+        const int groups = pairhist_groups(G.smem, tile, dreg, w_launch, group_tiles[g], C.sm_count);
+        const int per_sm = pairhist_ctas_per_sm(G.smem, tile, dreg, w_launch, groups);
         G.grid = (int)std::min<long long>((long long)C.sm_count * per_sm, std::max<long long>(1, group_tiles[g]));
         PairLaunch& L = G.launch;
+        L.groups = groups;
         L.jobs = reinterpret_cast<const PairJob*>(base + job_off);
         L.n_jobs = (int)group_jobs[g].size();
         L.total_tiles = group_tiles[g];

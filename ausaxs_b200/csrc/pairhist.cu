@@ -364,7 +364,7 @@ __device__ __forceinline__ void run_segments(const PairJob& J, const Onchip& S, 
 // split its inner points (run_segments), so a one-CTA layout keeps R = 2 outer points per thread
 // (one staged inner point read per two pairs) with NT = 1024 threads on 1024-point tiles.
 template <int NT, int R, bool WEIGHTED, bool DREG, int NR, int G>
-__global__ void __launch_bounds__(NT, DREG ? 1 : (512 / NT > 1 ? 512 / NT : 1)) pairhist_kernel(PairLaunch L) {
+__global__ void __launch_bounds__(NT, DREG ? 1 : (G > 1 ? 1024 / NT : (512 / NT > 1 ? 512 / NT : 1))) pairhist_kernel(PairLaunch L) {
     constexpr int TILE = NT * R / G;
     constexpr int NTG = NT / G;  // threads per group
     extern __shared__ __align__(16) unsigned char smem[];
@@ -544,6 +544,7 @@ void launch_tile(const PairLaunch& L, int grid, size_t smem, cudaStream_t s) {
     if (L.weighted) launch_nr<NT, true, false>(L, grid, smem, s);
     else if (L.dreg && TILE == 1024) launch_nr<TILE, false, true, 2>(L, grid, smem, s);
     else if (L.dreg) launch_nr<NT, false, true>(L, grid, smem, s);
+    else if (L.groups == 2) launch_nr<TILE, false, false, 2>(L, grid, smem, s);
     else launch_nr<NT, false, false>(L, grid, smem, s);
 }
 
@@ -571,10 +572,11 @@ int occupancy_one(size_t smem) {
 }
 
 template <int TILE>
-int occupancy_tile(size_t smem, bool weighted, bool dreg) {
+int occupancy_tile(size_t smem, bool weighted, bool dreg, int groups) {
     constexpr int NT = TILE / kOuter;
     if (weighted) return occupancy_one<NT, kOuter, true, false>(smem);
     if (dreg) return occupancy_one<NT, kOuter, false, true>(smem);
+    if (groups == 2) return occupancy_one<TILE, kOuter, false, false, 2>(smem);
     return occupancy_one<NT, kOuter, false, false>(smem);
 }
 
@@ -601,11 +603,17 @@ SqrtVerified g_sqrt;
 
 }  // namespace
 
-int pairhist_ctas_per_sm(size_t smem, int tile, bool dreg, bool weighted) {
+int pairhist_ctas_per_sm(size_t smem, int tile, bool dreg, bool weighted, int groups) {
     if (tile == 1024 && dreg && !weighted) return occupancy_one<1024, kOuter, false, true, 2>(smem);
-    if (tile == 1024) return occupancy_tile<1024>(smem, weighted, dreg);
-    if (tile == 256) return occupancy_tile<256>(smem, weighted, dreg);
-    return occupancy_tile<512>(smem, weighted, dreg);
+    if (tile == 1024) return occupancy_tile<1024>(smem, weighted, dreg, groups);
+    if (tile == 256) return occupancy_tile<256>(smem, weighted, dreg, groups);
+    return occupancy_tile<512>(smem, weighted, dreg, groups);
+}
+
+int pairhist_groups(size_t smem, int tile, bool dreg, bool weighted, long long tiles, int sm_count) {
+    if (weighted || dreg) return 1;
+    const int per_sm = pairhist_ctas_per_sm(smem, tile, false, false, 1);
+    return (tiles < (long long)sm_count * per_sm || per_sm <= 2) ? 2 : 1;
 }
 
 bool pair_sqrt_prepare(float inv_w, int bins) {

@@ -68,6 +68,9 @@ struct PairLaunch {
     int32_t max_grabs;              // > 0: a CTA takes at most this many chunks and exits (the grid
                                     // must then cover the tiles: grid * max_grabs * chunk >= total);
                                     // bounded CTAs let the block scheduler interleave other launches
+    int32_t groups;                 // 2: unweighted launches with shared-memory offset sums run tile
+                                    // threads per CTA in two groups that split every tile's inner
+                                    // points (pairhist_groups); 0 or 1: tile / kOuter threads
 };
 
 // Outer points per thread: a tile of `tile` points per side runs tile / kOuter threads.
@@ -119,8 +122,15 @@ inline size_t pairhist_launch_smem(int rows, int bins, bool weighted, int tile) 
     return pairhist_smem_bytes(rows, bins, weighted, tile, pairhist_dreg(rows, bins, weighted, tile));
 }
 
-// Resident CTAs per SM of a launch with this footprint (the runtime's occupancy of the instantiation).
-int pairhist_ctas_per_sm(size_t smem, int tile, bool dreg, bool weighted);
+// Resident CTAs per SM of a launch with this footprint (the runtime's occupancy of the instantiation;
+// groups as PairLaunch::groups).
+int pairhist_ctas_per_sm(size_t smem, int tile, bool dreg, bool weighted, int groups = 1);
+
+// Thread groups per CTA for a launch of `tiles` tiles: two groups (twice the threads on the same tile
+// and shared memory) where one group per CTA would leave CTA slots without a tile (small structures:
+// each tile then takes half the time) or would hold an SM to two CTAs (16 warps); one otherwise.
+// Launches with weighted bins or register-held offset sums keep their own layouts (1).
+int pairhist_groups(size_t smem, int tile, bool dreg, bool weighted, long long tiles, int sm_count);
 
 // Rows of [rows][bins] counts that fit on chip for `tile`-point tiles (512 covers 256 as well).
 inline int pairhist_max_rows(int bins, bool weighted, int tile = 512) {
