@@ -321,7 +321,13 @@ struct Assembly {
             max_rows = std::max(max_rows, rows[0]);
         }
         smem = pairhist_launch_smem(max_rows, nb, false, tile);
-        for (Work& Wk : work) Wk.L.dreg = pairhist_dreg(max_rows, nb, false, tile) ? 1 : 0;
+        // two thread groups per CTA (pairhist_groups): a tile of a move's short-lived CTAs takes half
+        // the time, which shortens the last wave of a move (measured: the largest body's lone move
+        // 1.43 -> 1.38 ms p50, 2.54 -> 2.21 ms max; saturated moves/s +3 %)
+        for (Work& Wk : work) {
+            Wk.L.dreg = pairhist_dreg(max_rows, nb, false, tile) ? 1 : 0;
+            Wk.L.groups = Wk.L.dreg ? 1 : 2;
+        }
         const int per_sm = pairhist_ctas_per_sm(smem, tile, pairhist_dreg(max_rows, nb, false, tile), false);
         // device tables: jobs, zero ranges, partial pointers of the master sum
         std::vector<const unsigned long long*> ptrs[3];
