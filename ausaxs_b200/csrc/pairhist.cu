@@ -364,7 +364,7 @@ __device__ __forceinline__ void run_segments(const PairJob& J, const Onchip& S, 
 // split its inner points (run_segments), so a one-CTA layout keeps R = 2 outer points per thread
 // (one staged inner point read per two pairs) with NT = 1024 threads on 1024-point tiles.
 template <int NT, int R, bool WEIGHTED, bool DREG, int NR, int G>
-__global__ void __launch_bounds__(NT, DREG ? 1 : (G > 1 ? 1024 / NT : (512 / NT > 1 ? 512 / NT : 1))) pairhist_kernel(PairLaunch L) {
+__global__ void __launch_bounds__(NT, DREG ? 1 : (WEIGHTED ? (512 / NT > 1 ? 512 / NT : 1) : 1024 / NT)) pairhist_kernel(PairLaunch L) {
     constexpr int TILE = NT * R / G;
     constexpr int NTG = NT / G;  // threads per group
     extern __shared__ __align__(16) unsigned char smem[];
