@@ -462,7 +462,7 @@ Plan& Structure::plan_for(const ausaxs_hist_config& cfg) {
         LL.dsum = weighted ? reinterpret_cast<unsigned long long*>(base + slot_ds[5]) : nullptr;
         LL.overflow = reinterpret_cast<unsigned long long*>(base + P.off_overflow);
         LL.counter = reinterpret_cast<unsigned long long*>(base + P.off_counter) + 8;  // cleared with the accumulators
-        LL.n_items = lat.G.lz * (2 * lat.G.ly - 1);
+        LL.n_items = lat.G.lz * (2 * lat.G.ly - 1) * kLatticeChunks;
         LL.pts = raw_x.as<float4>();
         LL.n_pts = n_x;
         LL.tail_fix = lattice_rules_agree(lat.s2_max, inv_w) ? 0 : 1;

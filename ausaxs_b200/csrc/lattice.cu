@@ -180,15 +180,21 @@ __global__ void __launch_bounds__(lattice_threads<W>(), 1) lattice_kernel(Lattic
         if (lane == 0) item = static_cast<int>(atomicAdd(L.counter, 1ull));
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= L.n_items) break;
-        const int dz = item / span;
-        const int dy = item - dz * span - (ly - 1);
+        // item = (line offset, z chunk): the line offset's z1 range split into kLatticeChunks parts,
+        // so the first (largest, dz = 0) offsets do not leave a long tail of lone warps
+        const int base = item / kLatticeChunks;
+        const int chunk = item - base * kLatticeChunks;
+        const int dz = base / span;
+        const int dy = base - dz * span - (ly - 1);
         if (dz == 0 && dy < 0) continue;  // the mirror image of an item with dy > 0
         const bool same = dz == 0 && dy == 0;
         uint32_t C[W];
 #pragma unroll
         for (int g = 0; g < W; ++g) C[g] = 0u;
         const int y_lo = max(0, -dy), y_hi = min(ly, ly - dy);
-        for (int z1 = 0; z1 + dz < lz; ++z1) {
+        const int z_per = (lz - dz + kLatticeChunks - 1) / kLatticeChunks;
+        const int z_begin = chunk * z_per, z_end = min(lz - dz, z_begin + z_per);
+        for (int z1 = z_begin; z1 < z_end; ++z1) {
             const int32_t* t1 = s_table + z1 * ly;
             const int32_t* t2 = s_table + (z1 + dz) * ly + dy;
             for (int y1 = y_lo; y1 < y_hi; ++y1) {

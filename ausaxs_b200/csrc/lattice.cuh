@@ -28,7 +28,7 @@ struct LatticeLaunch {
     unsigned long long* dsum;      // [nbins] or null
     unsigned long long* overflow;  // pairs beyond the last bin
     unsigned long long* counter;   // work-item counter (zeroed before the launch)
-    int n_items;                   // lz * (2 ly - 1) line offsets (dz >= 0)
+    int n_items;                   // lz * (2 ly - 1) line offsets (dz >= 0) x kLatticeChunks z ranges
     const float4* pts;             // the points themselves, in the reference's loop order
     int n_pts;
     int tail_fix;                  // the two rounding rules differ at some squared offset: correct the
@@ -39,6 +39,7 @@ struct LatticeLaunch {
 constexpr int kLatticeMinPoints = 1024;
 constexpr int kLatticeMaxWords = 8;   // lines of up to 256 lattice cells along x
 constexpr int kLatticeThreads = 512;  // lines of more than 128 cells; up to 128: 1024 threads
+constexpr int kLatticeChunks = 4;     // z ranges per line offset (work items of one warp)
 
 // Words per line of the kernel instantiation that serves a grid of `words` words (1, 2, 4 or 8).
 inline int lattice_kernel_words(int words) { return words <= 2 ? words : (words <= 4 ? 4 : 8); }
