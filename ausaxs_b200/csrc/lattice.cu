@@ -151,6 +151,43 @@ __global__ void __launch_bounds__(1024) lattice_compact_kernel(const uint32_t* g
 template <int W>
 constexpr int lattice_threads() { return W <= 4 ? 1024 : kLatticeThreads; }
 
+// Carry-save accumulation of popcounts (the Harley-Seal method) for x-shift group 0, the group with
+// the most terms (2 W per line pair): the terms are added bitwise into words of weight 1 (ones) and
+// 2 (twos) carried across line pairs, and only the words of weight 4 that fall out are popcounted.
+// POPC issues on the XU pipe at a quarter of the ALU rate and binds the kernel; group 0 this way takes
+// one POPC per four terms, the other groups keep one per term (carry-saving every group moves the
+// bound onto the ALU pipe and is slower).  The count is 4 n + 2 popc(twos) + popc(ones).
+struct CsaCount {
+    uint32_t ones, twos, n;
+};
+
+// full adder over 32 bit positions: a + b + c = 2 hi + lo
+__device__ __forceinline__ void csa(uint32_t& hi, uint32_t& lo, uint32_t a, uint32_t b, uint32_t c) {
+    const uint32_t u = a ^ b;
+    hi = (a & b) | (u & c);
+    lo = u ^ c;
+}
+
+__device__ __forceinline__ void csa_add4(CsaCount& k, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+    uint32_t t1, t2, f;
+    csa(t1, k.ones, k.ones, a, b);
+    csa(t2, k.ones, k.ones, c, d);
+    csa(f, k.twos, k.twos, t1, t2);
+    k.n += __popc(f);
+}
+
+__device__ __forceinline__ void csa_add2(CsaCount& k, uint32_t a, uint32_t b) {
+    uint32_t t1;
+    csa(t1, k.ones, k.ones, a, b);
+    const uint32_t f = k.twos & t1;
+    k.twos ^= t1;
+    k.n += __popc(f);
+}
+
+__device__ __forceinline__ uint32_t csa_total(const CsaCount& k) {
+    return 4u * k.n + 2u * static_cast<uint32_t>(__popc(k.twos)) + static_cast<uint32_t>(__popc(k.ones));
+}
+
 template <int W>
 __global__ void __launch_bounds__(lattice_threads<W>(), 1) lattice_kernel(LatticeLaunch L) {
     constexpr int NTH = lattice_threads<W>();
@@ -194,36 +231,66 @@ __global__ void __launch_bounds__(lattice_threads<W>(), 1) lattice_kernel(Lattic
         const int y_lo = max(0, -dy), y_hi = min(ly, ly - dy);
         const int z_per = (lz - dz + kLatticeChunks - 1) / kLatticeChunks;
         const int z_begin = chunk * z_per, z_end = min(lz - dz, z_begin + z_per);
-        for (int z1 = z_begin; z1 < z_end; ++z1) {
-            const int32_t* t1 = s_table + z1 * ly;
-            const int32_t* t2 = s_table + (z1 + dz) * ly + dy;
-            for (int y1 = y_lo; y1 < y_hi; ++y1) {
-                const int i1 = t1[y1];
-                if (i1 < 0) continue;
-                const int i2 = t2[y1];
-                if (i2 < 0) continue;
-                uint32_t P[W], Q[W];
+        if (!same) {
+            // two lines: for x-shift group g, the terms P[w] & (Q >> s) and Q[w] & (P >> s) of every
+            // word w, shift 32 g + lane; x-shift 0 (lane 0 of group 0) is counted once
+            CsaCount K0{0u, 0u, 0u};
+            const uint32_t not_lane0 = lane ? 0xffffffffu : 0u;
+            for (int z1 = z_begin; z1 < z_end; ++z1) {
+                const int32_t* t1 = s_table + z1 * ly;
+                const int32_t* t2 = s_table + (z1 + dz) * ly + dy;
+                for (int y1 = y_lo; y1 < y_hi; ++y1) {
+                    const int i1 = t1[y1];
+                    if (i1 < 0) continue;
+                    const int i2 = t2[y1];
+                    if (i2 < 0) continue;
+                    uint32_t P[W], Q[W], Ps[W], Qs[W];
 #pragma unroll
-                for (int w = 0; w < W; ++w) {
-                    P[w] = s_lines[i1 * W + w];
-                    Q[w] = s_lines[i2 * W + w];
+                    for (int w = 0; w < W; ++w) {
+                        P[w] = s_lines[i1 * W + w];
+                        Q[w] = s_lines[i2 * W + w];
+                    }
+#pragma unroll
+                    for (int k = 0; k < W; ++k) {
+                        Qs[k] = __funnelshift_r(Q[k], k + 1 < W ? Q[k + 1] : 0u, lane);
+                        Ps[k] = __funnelshift_r(P[k], k + 1 < W ? P[k + 1] : 0u, lane);
+                    }
+#pragma unroll
+                    for (int w = 0; w + 1 < W; w += 2)
+                        csa_add4(K0, P[w] & Qs[w], Q[w] & Ps[w] & not_lane0, P[w + 1] & Qs[w + 1],
+                                 Q[w + 1] & Ps[w + 1] & not_lane0);
+                    if (W & 1) csa_add2(K0, P[W - 1] & Qs[W - 1], Q[W - 1] & Ps[W - 1] & not_lane0);
+#pragma unroll
+                    for (int g = 1; g < W; ++g) {
+#pragma unroll
+                        for (int w = 0; w + g < W; ++w)
+                            C[g] += __popc(P[w] & Qs[w + g]) + __popc(Q[w] & Ps[w + g]);
+                    }
                 }
+            }
+            C[0] = csa_total(K0);
+        } else {
+            // a line with itself (one item per z range): the pairs x2 - x1 = s > 0 only
+            for (int z1 = z_begin; z1 < z_end; ++z1) {
+                const int32_t* t1 = s_table + z1 * ly;
+                for (int y1 = 0; y1 < ly; ++y1) {
+                    const int i1 = t1[y1];
+                    if (i1 < 0) continue;
+                    uint32_t P[W];
 #pragma unroll
-                for (int g = 0; g < W; ++g) {
+                    for (int w = 0; w < W; ++w) P[w] = s_lines[i1 * W + w];
 #pragma unroll
-                    for (int w = 0; w + g < W; ++w) {
-                        const uint32_t qn = (w + g + 1 < W) ? Q[w + g + 1] : 0u;
-                        C[g] += __popc(P[w] & __funnelshift_r(Q[w + g], qn, lane));
-                        if (!same) {
+                    for (int g = 0; g < W; ++g) {
+#pragma unroll
+                        for (int w = 0; w + g < W; ++w) {
                             const uint32_t pn = (w + g + 1 < W) ? P[w + g + 1] : 0u;
-                            const uint32_t v = __popc(Q[w] & __funnelshift_r(P[w + g], pn, lane));
-                            C[g] += (g == 0 && lane == 0) ? 0u : v;  // x-shift 0 is counted once
+                            C[g] += __popc(P[w] & __funnelshift_r(P[w + g], pn, lane));
                         }
                     }
                 }
             }
+            if (lane == 0) C[0] = 0u;  // x-shift 0 within a line: a point with itself
         }
-        if (same && lane == 0) C[0] = 0u;  // x-shift 0 within a line: a point with itself
 #pragma unroll
         for (int g = 0; g < W; ++g) {
             if (!C[g]) continue;
