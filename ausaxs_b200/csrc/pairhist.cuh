@@ -128,7 +128,8 @@ int pairhist_ctas_per_sm(size_t smem, int tile, bool dreg, bool weighted, int gr
 
 // Thread groups per CTA for a launch of `tiles` tiles: two groups (twice the threads on the same tile
 // and shared memory) where one group per CTA would leave CTA slots without a tile (small structures:
-// each tile then takes half the time) or would hold an SM to two CTAs (16 warps); one otherwise.
+// each tile then takes half the time) or would hold an SM to at most two CTAs (few warps per SM); one
+// otherwise.
 // Launches with weighted bins or register-held offset sums keep their own layouts (1).
 int pairhist_groups(size_t smem, int tile, bool dreg, bool weighted, long long tiles, int sm_count);
 
